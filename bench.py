@@ -1,0 +1,380 @@
+"""Benchmark: 3D VTI adjoint gradient (fwd + adjoint) throughput on B200.
+
+Workload (one "step" = one L2-misfit gradient evaluation of one shot, the
+three passes of objFuncGradientCij3d_f): 400 x 400 x 200 grid at 12.5 m
+(40-cell pad inside), dt = 1 ms, nt = 3000 (all 2999 levels), 12 Hz Ricker,
+200 x 200 receivers at 25 m, 4 ms trace sampling; layered VTI model with a
+Gaussian random-field perturbation; observed data from the true model, the
+gradient at the smoothed (250 m) model. Synthetic, seeded inputs.
+
+Metric: grid-point updates per second (Gpts/s): 4 wavefield-pair updates per
+time level (pass 1 forward, pass 2 forward, pass 3 source reconstruction and
+adjoint) x nx*ny*nz points x levels, summed over all ranks.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Under torchrun each rank models its own shot (weak scaling); the gradients
+are summed with one NCCL all-reduce per step. `value` is device-resident
+throughput; `e2e` goes through the host-buffer C-ABI entry point
+(vti3d_gradient_cij) with pinned host inputs and outputs.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "thesis-source-code_b200"))
+
+CONFIGS = {
+    # name: survey3d kwargs
+    "gradient400": dict(nx=400, ny=400, nz=200, nt=3000, npad=40, d=12.5, dt=1e-3, rate=4e-3,
+                        freq=12.0, rec_step=2, rec_start=0, rec_depth=25.0, src_depth=25.0,
+                        smooth_m=250.0),
+    "small": dict(nx=128, ny=128, nz=96, nt=402, npad=16, d=12.5, dt=1e-3, rate=4e-3,
+                  freq=12.0, rec_step=2, rec_start=0, rec_depth=25.0, src_depth=25.0,
+                  smooth_m=100.0),
+}
+BWD_BYTES_PER_POINT = 84  # 14 reads + 7 writes of FP32 per point (fused backward)
+FWD_BYTES_PER_POINT = 36  # 7 reads + 2 writes
+
+
+def peaks():
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        d = json.loads(f.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, device):
+        self.device, self.rows, self.proc = device, [], None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4)
+                          if len(r) > 4 + k and r[4 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def make_inputs(cfg, rank):
+    import vtib200 as V
+    import vtib200.synth as S
+    kw = dict(CONFIGS[cfg])
+    nx, ny = kw["nx"], kw["ny"]
+    # each rank's shot at its own position (weak scaling)
+    off = [(0, 0), (40, 0), (0, 40), (40, 40), (-40, 0), (0, -40), (-40, -40), (40, -40)]
+    dx, dy = off[rank % len(off)]
+    kw["src_xy"] = (nx // 2 + dx * nx // 400, ny // 2 + dy * ny // 400)
+    s = S.survey3d(**kw)
+    padb, randb = S.boundaries3d(s)
+    tv, te, td = s.extra["true"]
+    ctrue = s.cij(tv, te, td)
+    n = s.nxyz
+    # observed data use the pad boundary of the true model in the sponge pass
+    ctrue = np.concatenate([V.put_boundary(padb[k * s.nb:(k + 1) * s.nb],
+                                           ctrue[k * n:(k + 1) * n], s.nx, s.ny, s.nz, s.npad)
+                            for k in range(3)])
+    return s, s.cij(), ctrue, padb, randb
+
+
+def levels(g, flags):
+    return g.nt - 1 if flags & 1 else 1 + 64 * ((g.nt - 2) // 64)
+
+
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+    import vtib200 as V
+
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device(
+            "cuda", local))
+    s, cstart, ctrue, padb, randb = make_inputs(args.config, rank)
+    g = s.geom()
+    flags = V.OPT_FULL_STEPS
+    n = s.nxyz
+    ctx = V.Context(local)
+    plan = V.Plan3d(ctx, g, flags)
+    plan.set_wavelet(s.wavelet)
+    plan.set_receivers(s.recloc)
+    nrec = s.recloc.size // 4
+    nnt = V.nnt3d(g)
+    dobs = torch.zeros(nnt * nrec, dtype=torch.float32, device="cuda")
+    plan.set_model(ctrue[:n], ctrue[n:2 * n], ctrue[2 * n:])
+    plan.model_data(s.souloc, [0], out=dobs.data_ptr(), mem=V.MEM_DEVICE)
+    plan.set_model(cstart[:n], cstart[n:2 * n], cstart[2 * n:], padb=padb, randb=randb)
+    fg = torch.zeros(1 + 3 * n, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.ExternalStream(ctx.stream)
+
+    def step():
+        _, mis = plan.gradient(s.souloc, [0], dobs.data_ptr(), V.MEM_DEVICE, fg.data_ptr(),
+                               V.MEM_DEVICE)
+        if world > 1:
+            dist.all_reduce(fg)
+        return mis
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = ctx.launches
+    ctx.set_timing(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            mis = step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    bwd_ms, bwd_n = ctx.kernel_time("bwd3d")
+    fwd_ms, fwd_n = ctx.kernel_time("fwd3d")
+    ctx.set_timing(False)
+    launches = ctx.launches - launches0
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    M = levels(g, flags)
+    pts_per_step = 4.0 * (M - 1) * n
+    value = pts_per_step * args.steps * world / (ms / 1e3) / 1e9
+    # roofline of the dominant kernel (fused backward step)
+    upd = (s.nx - 8) * (s.ny - 8) * s.nz
+    peak, peak_kind = peaks()
+    bwd_avg = bwd_ms / max(bwd_n, 1) / 1e3
+    fwd_avg = fwd_ms / max(fwd_n, 1) / 1e3
+    achieved = BWD_BYTES_PER_POINT * upd / bwd_avg / 1e9 if bwd_n else None
+    traffic = None
+    tf = ROOT / "profiles" / "k_bwd3d_traffic.json"
+    if tf.exists():
+        traffic = json.loads(tf.read_text()).get("bytes_per_launch")
+    out = None
+    if rank == 0:
+        e2e = run_e2e(args, ctx, s, cstart, padb, randb, dobs.cpu().numpy(), flags)
+        cpu = None if args.no_cpu else cpu_baseline(s, cstart, args)
+        out = {
+            "metric": "3D VTI fwd+adjoint gradient throughput (grid-point updates/s)",
+            "value": round(value, 3), "unit": "Gpts/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded layered VTI model + GRF, Ricker source)",
+            "config": {"workload": f"3D VTI L2-misfit gradient, {args.config}: "
+                                   f"{s.nx}x{s.ny}x{s.nz} grid (pad {s.npad}), nt={s.nt}, "
+                                   f"{M} levels, {nrec} receivers, 1 shot per GPU",
+                       "grid": [s.nx, s.ny, s.nz], "nt": s.nt, "levels": M,
+                       "receivers": nrec, "shots_per_gpu": 1, "misfit": mis,
+                       "l2": "wavefields (128 MB each) larger than L2 (126 MB)"},
+            "roofline": {"bound": "hbm", "kernel": "k_bwd3d",
+                         "achieved": round(achieved, 1) if achieved else None, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4) if achieved else None,
+                         "traffic": traffic,
+                         "bytes_per_point": BWD_BYTES_PER_POINT,
+                         "avg_launch_ms": round(bwd_avg * 1e3, 4),
+                         "fwd3d": {"achieved": round(FWD_BYTES_PER_POINT * upd / fwd_avg / 1e9, 1)
+                                   if fwd_n else None,
+                                   "avg_launch_ms": round(fwd_avg * 1e3, 4)}},
+            "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": launches,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(out), flush=True)
+    plan.close()
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return out
+
+
+def run_e2e(args, ctx, s, cstart, padb, randb, dobs, flags):
+    """Same metric through the one-call host-buffer C ABI entry point."""
+    import torch
+    import vtib200 as V
+    g = s.geom()
+    n = s.nxyz
+
+    def pin(a):
+        t = torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).pin_memory()
+        return t
+
+    h_cij, h_padb, h_randb, h_dobs = pin(cstart), pin(padb), pin(randb), pin(dobs)
+    h_w, h_so, h_rec = pin(s.wavelet), pin(s.souloc), pin(s.recloc)
+    h_fg = torch.zeros(1 + 3 * n, dtype=torch.float32).pin_memory()
+    shot = np.zeros(1, dtype=np.int32)
+    lib = V.lib()
+    import ctypes as C
+    mis = C.c_double(0)
+    nrec = s.recloc.size // 4
+
+    def call():
+        ctx.check(lib.vti3d_gradient_cij(
+            ctx.handle, C.byref(g), C.c_void_p(h_cij.data_ptr()), C.c_void_p(h_padb.data_ptr()),
+            C.c_void_p(h_randb.data_ptr()), C.c_void_p(h_w.data_ptr()),
+            C.c_void_p(h_so.data_ptr()), C.c_void_p(shot.ctypes.data), 1,
+            C.c_void_p(h_rec.data_ptr()), nrec, C.c_void_p(h_dobs.data_ptr()),
+            C.c_void_p(h_fg.data_ptr()), C.byref(mis), flags))
+
+    call()  # warm-up
+    steps = max(1, min(args.steps, 2))
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        call()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    ms = max(e0.elapsed_time(e1), wall * 1e3)
+    M = levels(g, flags)
+    val = 4.0 * (M - 1) * n * steps / (ms / 1e3) / 1e9
+    bi = 4 * (cstart.size + padb.size + randb.size + dobs.size + s.wavelet.size)
+    return {"value": round(val, 3), "unit": "Gpts/s", "h2d_bytes_per_step": int(bi),
+            "d2h_bytes_per_step": int(4 * (1 + 3 * n)), "steps": steps,
+            "ms_per_step": round(ms / steps, 2),
+            "api": "vti3d_gradient_cij (host buffers, plan created per call)"}
+
+
+def cpu_baseline(s, cstart, args, target_s=15.0):
+    """FP32 oracle (C++/OpenMP restatement of the reference path) on the same
+    grid: per level 2 forward steps + 1 fused backward step."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    g = s.geom()
+    n = s.nxyz
+    c = (cstart[:n], cstart[n:2 * n], cstart[2 * n:])
+    t0 = time.perf_counter()
+    thr = O.time_forward_f32(g, *c, 1)
+    tf1 = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    O.time_backward_f32(g, *c, 1)
+    tb1 = time.perf_counter() - t0
+    k = max(1, int(target_s / (2 * tf1 + tb1)))
+    t0 = time.perf_counter()
+    O.time_forward_f32(g, *c, 2 * k)
+    tf = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    O.time_backward_f32(g, *c, k)
+    tb = time.perf_counter() - t0
+    val = 4.0 * k * n / (tf + tb) / 1e9
+    return {"value": round(val, 4), "unit": "Gpts/s", "cores": int(thr), "kind": "port",
+            "sample": f"{k} gradient levels (2k forward + k fused backward steps) on the "
+                      f"{s.nx}x{s.ny}x{s.nz} grid, FP32, {thr} OpenMP threads",
+            "seconds": round(tf + tb, 2)}
+
+
+def run_reference(args):
+    """Reference arm: the reference algorithm's CPU implementation (the FP32
+    oracle port; the reference's own CPU path needs ISPC and TBB, absent
+    here), all host threads, bounded samples of the same workload."""
+    rank = int(os.environ.get("RANK", 0))
+    if rank != 0:
+        return None
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    import vtib200.synth as S
+    kw = dict(CONFIGS[args.config])
+    s = S.survey3d(**kw)
+    cstart = s.cij()
+    g = s.geom()
+    n = s.nxyz
+    c = (cstart[:n], cstart[n:2 * n], cstart[2 * n:])
+    k = 1
+    for _ in range(args.warmup):
+        O.time_forward_f32(g, *c, 1)
+    t0 = time.perf_counter()
+    thr = 0
+    for _ in range(args.steps):
+        thr = O.time_forward_f32(g, *c, 2 * k)
+        O.time_backward_f32(g, *c, k)
+    sec = time.perf_counter() - t0
+    val = 4.0 * k * n * args.steps / sec / 1e9
+    out = {"metric": "3D VTI fwd+adjoint gradient throughput (grid-point updates/s)",
+           "value": round(val, 4), "unit": "Gpts/s", "n_gpus": int(os.environ.get(
+               "WORLD_SIZE", 1)), "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": round(sec / args.steps * 1e3, 2), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "impl": "reference",
+           "config": {"workload": f"3D VTI L2-misfit gradient, {args.config}: "
+                                  f"{s.nx}x{s.ny}x{s.nz} grid; each step = {k} gradient level "
+                                  "(2 forward + 1 fused backward step)"},
+           "cpu_baseline": {"value": round(val, 4), "unit": "Gpts/s", "cores": int(thr),
+                            "kind": "port",
+                            "sample": f"{k} level(s) per step on the full grid, FP32"},
+           "e2e": {"value": round(val, 4), "unit": "Gpts/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", default="gradient400", choices=sorted(CONFIGS))
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,174 @@
+/*
+ * vti_b200.h — C ABI of the B200-native VTI pseudo-acoustic modeling and
+ * gradient library (libvti_b200.so).
+ *
+ * Plain C types only: pointers, sizes, status codes. No CUDA or torch types
+ * appear in any signature; device pointers are passed as `void*`/`float*`
+ * together with a VTI_MEM_* tag.
+ *
+ * Array conventions follow the reference (huyleq/thesis-source-code):
+ *  - 3D arrays are x-fastest, i = ix + iy*nx + iz*nx*ny, the absorbing pad
+ *    inside nx, ny, nz (lib/vti-fwi-3d/gpu/boundary.cpp:10-46).
+ *  - 3D traces are time-fastest, data[it + ir*nnt], nnt = (nt-1)/s + 1,
+ *    s = round(sampling_rate/dt) (lib/vti-fwi-3d/gpu/modelData3d_f.cu:29-30,272).
+ *  - souloc holds 5 floats per shot (x, y, z, nr, irbegin), recloc 4 floats
+ *    per receiver (x, y, z, live flag) (objFuncGradient3d_f.cu:551-575).
+ *  - "boundary" arrays are the pad-region lists produced by getBoundary
+ *    (boundary.cpp:10-46), nb = nx*ny*nz - (nx-2npad)(ny-2npad)(nz-2npad).
+ *  - 2D arrays are i = ix + iz*nnx with nnx = nx + 2*npad
+ *    (lib/vti-fwi-2d/init.cpp:11-18); 2D traces are receiver-fastest,
+ *    data[it*nr + ir] (synthetic_f.cu:110).
+ *
+ * Every entry point returns a vti_status. On a non-OK status the context's
+ * last-error string (vti_ctx_last_error) holds a one-line reason.
+ */
+#ifndef VTI_B200_H
+#define VTI_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  VTI_OK = 0,
+  VTI_ERR_ARG = 1,        /* invalid argument (sizes, indices, null pointers) */
+  VTI_ERR_CFL = 2,        /* dt violates the scheme's stability bound */
+  VTI_ERR_OOM = 3,        /* device allocation failed */
+  VTI_ERR_DEVICE = 4,     /* a CUDA call failed; see vti_ctx_last_error */
+  VTI_ERR_TIMEOUT = 5,    /* a bounded device-side wait gave up */
+  VTI_ERR_NONFINITE = 6,  /* a wavefield or misfit became NaN/Inf */
+  VTI_ERR_UNSUPPORTED = 7 /* valid request this build does not implement */
+} vti_status;
+
+/* where a pointer lives */
+#define VTI_MEM_HOST 0
+#define VTI_MEM_DEVICE 1
+
+/* option flags (bitwise OR) */
+/* Run every time level 0..nt-1. Without it the 3D propagators run the
+ * reference pipeline's 2 + 64*floor((nt-2)/64) levels
+ * (objFuncGradient3d_f.cu:538-542), so results match it for every nt. */
+#define VTI_OPT_FULL_STEPS 1u
+/* Check wavefields for NaN/Inf after each pass (VTI_ERR_NONFINITE). */
+#define VTI_OPT_CHECK_FINITE 2u
+
+typedef struct vti_ctx vti_ctx;
+typedef struct vti3d_plan vti3d_plan;
+
+typedef struct {
+  int nx, ny, nz; /* grid including the absorbing pad; x fastest */
+  int nt;         /* time samples of the wavelet / simulation */
+  int npad;       /* pad width (sponge and random-boundary region) */
+  float ox, oy, oz, ot;
+  float dx, dy, dz, dt;
+  float sampling_rate; /* trace sampling interval (seconds) */
+} vti3d_geom;
+
+typedef struct {
+  int nx, nz; /* interior size; arrays are (nx+2npad) x (nz+2npad) */
+  int nt, npad;
+  float dx, dz, dt;
+  float rate; /* trace/snapshot sampling interval */
+  float ot;   /* time of sample 0 (<= 0) */
+} vti2d_geom;
+
+/* ---------------------------------------------------------------- context */
+/* One context per CUDA device; owns the streams and a device error word. */
+int vti_ctx_create(int device, vti_ctx** out);
+int vti_ctx_destroy(vti_ctx* ctx);
+const char* vti_status_string(int status);
+const char* vti_ctx_last_error(const vti_ctx* ctx);
+/* The CUDA stream (cudaStream_t) all work of this context is ordered on. */
+void* vti_ctx_stream(vti_ctx* ctx);
+/* Number of library kernels launched on this context so far. */
+uint64_t vti_ctx_kernel_launches(const vti_ctx* ctx);
+/* Per-kernel device timing with CUDA events on the context stream.
+ * enable != 0 starts (and clears) recording; kernel is "fwd3d", "bwd3d" or
+ * "step2d". vti_ctx_kernel_time synchronizes the stream and returns the summed
+ * device time (ms) and the number of timed launches. */
+int vti_ctx_set_timing(vti_ctx* ctx, int enable);
+int vti_ctx_kernel_time(vti_ctx* ctx, const char* kernel, double* total_ms, uint64_t* count);
+
+/* ------------------------------------------------------------- host glue */
+/* Stability bound of the leapfrog scheme: largest dt^2 * lambda_max(M) over
+ * the model, M = [[c11 Kh, c13 Kz],[c13 Kh, c33 Kz]]. Stable iff < 4. */
+double vti3d_cfl_number(const vti3d_geom* g, const float* c11, const float* c13,
+                        const float* c33);
+/* getBoundary / putBoundary / zeroBoundary (boundary.cpp:10-117). */
+void vti3d_get_boundary(float* boundary, const float* v, int nx, int ny, int nz, int npad);
+void vti3d_put_boundary(const float* boundary, float* v, int nx, int ny, int nz, int npad);
+void vti3d_zero_boundary(float* v, int nx, int ny, int nz, int npad);
+/* VEpsDel2Cij, GradCij2GradVEpsDel, dVEpsDel2dCij, checkEpsDel
+ * (lib/vti-fwi-2d/conversions.cpp:42-81, check.cpp:22-40). */
+void vti_vepsdel_to_cij(float* c11, float* c13, float* c33, const float* v, const float* eps,
+                        const float* del, float v0, float eps0, float del0, size_t n);
+void vti_grad_cij_to_vepsdel(float* gv, float* geps, float* gdel, const float* gc11,
+                             const float* gc13, const float* gc33, const float* v,
+                             const float* eps, const float* del, float v0, float eps0, float del0,
+                             size_t n);
+void vti_dvepsdel_to_dcij(float* c11, float* c13, float* c33, float* dc11, float* dc13,
+                          float* dc33, const float* v, const float* eps, const float* del,
+                          const float* dv, const float* deps, const float* ddel, float v0,
+                          float eps0, float del0, size_t n);
+int vti_check_eps_del(float* eps, float* del, float eps0, float del0, size_t n, float* mask);
+
+/* ------------------------------------------------------------ 3D plans */
+/* A plan owns the device-resident state of one 3D geometry: model (pad and
+ * random-boundary versions), wavefields, gradient accumulators, traces. */
+int vti3d_plan_create(vti_ctx* ctx, const vti3d_geom* g, unsigned flags, vti3d_plan** out);
+int vti3d_plan_destroy(vti3d_plan* plan);
+/* Model c11,c13,c33 (nxyz each, mem = VTI_MEM_*). padb / randb are the
+ * 3*nb boundary lists (c11 list, c13 list, c33 list) swapped into the pad for
+ * the sponge pass and the random-boundary passes (objFuncGradient3d_f.cu:594,786);
+ * NULL leaves the model's own pad in place. */
+int vti3d_plan_set_model(vti3d_plan* plan, const float* c11, const float* c13, const float* c33,
+                         const float* padb, const float* randb, int mem);
+/* wavelet: nt floats. */
+int vti3d_plan_set_wavelet(vti3d_plan* plan, const float* wavelet, int mem);
+/* Receivers (host): 4 floats each, the whole survey. */
+int vti3d_plan_set_receivers(vti3d_plan* plan, const float* recloc, int nrec_total);
+/* Forward modeling with the sponge (modelDataCij3d_f, modelData3d_f.cu:427):
+ * ddata gets nnt*nr traces per shot at offset nnt*irbegin. */
+int vti3d_plan_model_data(vti3d_plan* plan, const float* souloc, const int* shotid, int nshot,
+                          float* ddata, int mem);
+/* L2 misfit gradient (objFuncGradientCij3d_f, objFuncGradient3d_f.cu:361):
+ * dobs as ddata; fgcij = [misfit/2 (float), gc11, gc13, gc33] (1+3*nxyz).
+ * misfit (optional) receives the FP64 sum of squared residuals / 2. */
+int vti3d_plan_gradient(vti3d_plan* plan, const float* souloc, const int* shotid, int nshot,
+                        const float* dobs, int dobs_mem, float* fgcij, int fgcij_mem,
+                        double* misfit);
+/* Misfit only (objFuncCij3d_f, objFuncGradient3d_f.cu:1272). */
+int vti3d_plan_objfunc(vti3d_plan* plan, const float* souloc, const int* shotid, int nshot,
+                       const float* dobs, int dobs_mem, double* misfit);
+/* Device pointer of the last forward wavefield sigma_x (nxyz floats). */
+const float* vti3d_plan_wavefield(vti3d_plan* plan);
+
+/* One-call host-buffer forms (what the drop-in shim calls). */
+int vti3d_model_data_cij(vti_ctx* ctx, const vti3d_geom* g, const float* c11, const float* c13,
+                         const float* c33, const float* wavelet, const float* souloc,
+                         const int* shotid, int nshot, const float* recloc, int nrec_total,
+                         float* ddata, unsigned flags);
+int vti3d_gradient_cij(vti_ctx* ctx, const vti3d_geom* g, const float* cij, const float* padb,
+                       const float* randb, const float* wavelet, const float* souloc,
+                       const int* shotid, int nshot, const float* recloc, int nrec_total,
+                       const float* dobs, float* fgcij, double* misfit, unsigned flags);
+
+/* ------------------------------------------------------------------- 2D */
+/* synthetic_f (lib/vti-fwi-2d/synthetic_f.cu:13): data[(it/ratio)*nr + ir]. */
+int vti2d_synthetic(vti_ctx* ctx, const vti2d_geom* g, const float* c11, const float* c13,
+                    const float* c33, const float* wavelet, const int* sloc, int ns,
+                    const int* rloc, int nr, const float* taper, float* data);
+/* modeling_f (modeling_f.cu:10): sigma_h snapshots wavefield[(it/ratio)*nnxz + i]. */
+int vti2d_modeling(vti_ctx* ctx, const vti2d_geom* g, const float* c11, const float* c13,
+                   const float* c33, const float* wavelet, int slocxz, const float* taper,
+                   float* wavefield);
+/* 2D taper of lib/vti-fwi-2d/init.cpp:70-89 ((nx+2npad)*(nz+2npad) floats). */
+void vti2d_init_taper(float* taper, int nx, int nz, int npad);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VTI_B200_H */

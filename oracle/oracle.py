@@ -1,0 +1,161 @@
+"""ctypes loader for the CPU oracle (oracle/vti_oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+cpu_baseline / reference legs of bench.py, never by the library.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_build" / "liboracle.so"
+_lib = None
+VP = C.c_void_p
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        L = C.CDLL(str(LIB))
+        for suf in ("f64", "f32"):
+            f = getattr(L, f"orc3d_model_data_{suf}")
+            f.argtypes = [VP] * 8 + [C.c_int, VP, VP, VP]
+            f.restype = C.c_int
+            f = getattr(L, f"orc3d_gradient_cij_{suf}")
+            f.argtypes = [VP] * 8 + [C.c_int, VP, VP, VP, C.c_int, VP]
+            f.restype = C.c_int
+            f = getattr(L, f"orc2d_forward_{suf}")
+            f.argtypes = [VP] * 7 + [C.c_int, VP, C.c_int, VP, VP, C.c_int]
+            f.restype = C.c_int
+        L.orc3d_damping.argtypes = [C.c_int] * 4 + [VP]
+        L.orc3d_last_level.argtypes = [VP, VP]
+        L.orc3d_last_level.restype = C.c_int
+        for n in ("orc3d_time_forward_f32", "orc3d_time_backward_f32"):
+            getattr(L, n).argtypes = [VP] * 5 + [C.c_int, VP]
+            getattr(L, n).restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _geo3(g, full_steps=False):
+    ip = np.array([g.nx, g.ny, g.nz, g.nt, g.npad, 0 if full_steps else 1], dtype=np.int32)
+    fp = np.array([g.ox, g.oy, g.oz, g.ot, g.dx, g.dy, g.dz, g.dt, g.sampling_rate],
+                  dtype=np.float32)
+    return ip, fp
+
+
+def nnt3d(g):
+    s = int(np.round(np.float32(g.sampling_rate) / np.float32(g.dt)))
+    return (g.nt - 1) // s + 1
+
+
+def model_data3d(g, c11, c13, c33, wavelet, souloc, shotid, recloc, dtype=np.float64,
+                 full_steps=False, want_wavefield=False):
+    """modelDataCij3d_f restated: traces (nnt*nrec_total) and optionally the
+    last sigma_x level."""
+    ip, fp = _geo3(g, full_steps)
+    recloc = _f32(recloc).reshape(-1)
+    out = np.zeros(nnt3d(g) * (recloc.size // 4), dtype=dtype)
+    wf = np.zeros(g.nx * g.ny * g.nz, dtype=dtype) if want_wavefield else None
+    suf = "f64" if dtype == np.float64 else "f32"
+    shotid = _i32(shotid)
+    getattr(lib(), f"orc3d_model_data_{suf}")(
+        _p(ip), _p(fp), _p(_f32(c11)), _p(_f32(c13)), _p(_f32(c33)), _p(_f32(wavelet)),
+        _p(_f32(souloc)), _p(shotid), len(shotid), _p(recloc), _p(out), _p(wf))
+    return (out, wf) if want_wavefield else out
+
+
+def gradient3d(g, cij, padb, randb, wavelet, souloc, shotid, recloc, dobs, dtype=np.float64,
+               full_steps=False, misfit_only=False, want_modeled=False):
+    """objFuncGradientCij3d_f restated: fgcij = [misfit/2, gc11, gc13, gc33]."""
+    ip, fp = _geo3(g, full_steps)
+    n = g.nx * g.ny * g.nz
+    out = np.zeros(1 + 3 * n, dtype=dtype)
+    recloc = _f32(recloc).reshape(-1)
+    mod = np.zeros(nnt3d(g) * (recloc.size // 4), dtype=dtype) if want_modeled else None
+    suf = "f64" if dtype == np.float64 else "f32"
+    shotid = _i32(shotid)
+    getattr(lib(), f"orc3d_gradient_cij_{suf}")(
+        _p(ip), _p(fp), _p(_f32(cij)), _p(_f32(padb)), _p(_f32(randb)), _p(_f32(wavelet)),
+        _p(_f32(souloc)), _p(shotid), len(shotid), _p(recloc), _p(_f32(dobs)), _p(out),
+        1 if misfit_only else 0, _p(mod))
+    return (out, mod) if want_modeled else out
+
+
+def damping3d(nx, ny, nz, npad):
+    out = np.zeros(nx * ny + nz, dtype=np.float32)
+    lib().orc3d_damping(nx, ny, nz, npad, _p(out))
+    return out[: nx * ny].reshape(ny, nx), out[nx * ny:]
+
+
+def last_level(g, full_steps=False):
+    ip, fp = _geo3(g, full_steps)
+    return lib().orc3d_last_level(_p(ip), _p(fp))
+
+
+def forward2d(g, c11, c13, c33, wavelet, sloc, rloc, taper, mode=0, slocxz=None,
+              dtype=np.float64):
+    """mode 0: synthetic_f traces [rows, nr]; mode 1: modeling_f snapshots."""
+    ip = np.array([g.nx, g.nz, g.nt, g.npad], dtype=np.int32)
+    fp = np.array([g.dx, g.dz, g.dt, g.rate, g.ot], dtype=np.float32)
+    nnxz = (g.nx + 2 * g.npad) * (g.nz + 2 * g.npad)
+    suf = "f64" if dtype == np.float64 else "f32"
+    if mode == 0:
+        sloc, rloc = _i32(sloc).reshape(-1), _i32(rloc).reshape(-1)
+        nr = rloc.size // 2
+        ratio = int(np.float32(g.rate) / np.float32(g.dt) + np.float32(0.5))
+        nt_neg = int(round(abs(g.ot) / g.dt))
+        rows = (g.nt - nt_neg - 1) // ratio + 1
+        out = np.zeros(rows * nr, dtype=dtype)
+        getattr(lib(), f"orc2d_forward_{suf}")(
+            _p(ip), _p(fp), _p(_f32(c11)), _p(_f32(c13)), _p(_f32(c33)), _p(_f32(wavelet)),
+            _p(sloc), sloc.size // 4, _p(rloc), nr, _p(_f32(taper)), _p(out), 0)
+        return out.reshape(rows, nr)
+    ratio = int(np.round(np.float32(g.rate) / np.float32(g.dt)))
+    nt_neg = int(round(abs(g.ot) / g.dt))
+    rows = max((g.nt - 1 - nt_neg) // ratio + 1, 2)
+    out = np.zeros(rows * nnxz, dtype=dtype)
+    s = np.array([slocxz], dtype=np.int32)
+    getattr(lib(), f"orc2d_forward_{suf}")(
+        _p(ip), _p(fp), _p(_f32(c11)), _p(_f32(c13)), _p(_f32(c33)), _p(_f32(wavelet)), _p(s), 1,
+        None, 0, _p(_f32(taper)), _p(out), 1)
+    return out.reshape(rows, nnxz)
+
+
+def time_forward_f32(g, c11, c13, c33, nsteps):
+    """Runs nsteps FP32 forward steps; returns threads used."""
+    ip, fp = _geo3(g)
+    n = g.nx * g.ny * g.nz
+    scratch = np.zeros(4 * n, dtype=np.float32)
+    return lib().orc3d_time_forward_f32(_p(ip), _p(fp), _p(_f32(c11)), _p(_f32(c13)),
+                                        _p(_f32(c33)), nsteps, _p(scratch))
+
+
+def time_backward_f32(g, c11, c13, c33, nsteps):
+    ip, fp = _geo3(g)
+    n = g.nx * g.ny * g.nz
+    scratch = np.zeros(11 * n, dtype=np.float32)
+    return lib().orc3d_time_backward_f32(_p(ip), _p(fp), _p(_f32(c11)), _p(_f32(c13)),
+                                         _p(_f32(c33)), nsteps, _p(scratch))

@@ -1,0 +1,101 @@
+// Harness that runs the REFERENCE's own 3D GPU path (compiled from its
+// sources by oracle/build_ref.sh into oracle/_ref/ref3d) on inputs written by
+// tests/golden/make_golden.py. TEST INFRASTRUCTURE ONLY: it produces golden
+// traces and gradients that pin the oracle; nothing in the library uses it.
+//
+// usage: ref3d <dir> model|grad
+//   <dir>/params.txt : nx ny nz nt npad ox oy oz ot dx dy dz dt rate ns nrec
+//   <dir>/{souloc,recloc,wavelet,cij,padb,randb,dobs}.bin (float32)
+//   writes <dir>/ref_ddata.bin (model) or <dir>/ref_fgcij.bin (grad)
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <string>
+#include <vector>
+
+// Entry points of lib/vti-fwi-3d/gpu (wave3d.h:84-122) and lib/io/myio.cpp:15.
+void myio_init(int argc, char** argv);
+void modelDataCij3d_f(float* ddata, float* souloc, int ns, std::vector<int>& shotid,
+                      float* recloc, const float* wavelet, float* c11, float* c13, float* c33,
+                      int nx, int ny, int nz, int nt, int npad, float ox, float oy, float oz,
+                      float ot, float dx, float dy, float dz, float dt, float samplingRate,
+                      std::vector<int>& GPUs);
+void objFuncGradientCij3d_f(float* fgcij, float* souloc, int ns, std::vector<int>& shotid,
+                            float* recloc, float* wavelet, float* cij, float* padboundaryCij,
+                            float* randboundaryCij, int nx, int ny, int nz, int nt, int npad,
+                            float ox, float oy, float oz, float ot, float dx, float dy, float dz,
+                            float dt, float samplingRate, std::vector<int>& GPUs);
+
+static std::vector<float> load(const std::string& path, size_t n) {
+  std::vector<float> v(n);
+  FILE* f = std::fopen(path.c_str(), "rb");
+  if (!f || std::fread(v.data(), sizeof(float), n, f) != n) {
+    std::fprintf(stderr, "cannot read %s (%zu floats)\n", path.c_str(), n);
+    std::exit(2);
+  }
+  std::fclose(f);
+  return v;
+}
+
+static void save(const std::string& path, const float* p, size_t n) {
+  FILE* f = std::fopen(path.c_str(), "wb");
+  if (!f || std::fwrite(p, sizeof(float), n, f) != n) {
+    std::fprintf(stderr, "cannot write %s\n", path.c_str());
+    std::exit(2);
+  }
+  std::fclose(f);
+}
+
+int main(int argc, char** argv) {
+  if (argc < 3) {
+    std::fprintf(stderr, "usage: %s <dir> model|grad\n", argv[0]);
+    return 2;
+  }
+  const std::string dir = argv[1], mode = argv[2];
+  std::ifstream pf(dir + "/params.txt");
+  int nx, ny, nz, nt, npad, ns, nrec;
+  float ox, oy, oz, ot, dx, dy, dz, dt, rate;
+  if (!(pf >> nx >> ny >> nz >> nt >> npad >> ox >> oy >> oz >> ot >> dx >> dy >> dz >> dt >>
+        rate >> ns >> nrec)) {
+    std::fprintf(stderr, "bad params.txt\n");
+    return 2;
+  }
+  const size_t n = (size_t)nx * ny * nz;
+  const size_t nb = n - (size_t)(nx - 2 * npad) * (ny - 2 * npad) * (nz - 2 * npad);
+  const int st = (int)(rate / dt + 0.5f);
+  const int nnt = (nt - 1) / st + 1;
+  auto souloc = load(dir + "/souloc.bin", 5 * (size_t)ns);
+  auto recloc = load(dir + "/recloc.bin", 4 * (size_t)nrec);
+  auto wavelet = load(dir + "/wavelet.bin", nt);
+  auto cij = load(dir + "/cij.bin", 3 * n);
+  std::vector<int> shotid(ns), gpus{0};
+  for (int i = 0; i < ns; ++i) shotid[i] = i;
+  // side channel read by the reference: data=<header> (objFuncGradient3d_f.cu:760)
+  const std::string hdr = dir + "/dobs.H";
+  {
+    std::ofstream h(hdr);
+    h << "in=" << dir << "/dobs.bin\ndata_format=native_float\n";
+  }
+  std::string a0 = "ref3d", a1 = "data=" + hdr, a2 = "tpow=0", a3 = "objtype=0";
+  char* av[] = {&a0[0], &a1[0], &a2[0], &a3[0], nullptr};
+  myio_init(4, av);
+  if (mode == "model") {
+    std::vector<float> ddata((size_t)nnt * nrec, 0.f);
+    modelDataCij3d_f(ddata.data(), souloc.data(), ns, shotid, recloc.data(), wavelet.data(),
+                     cij.data(), cij.data() + n, cij.data() + 2 * n, nx, ny, nz, nt, npad, ox,
+                     oy, oz, ot, dx, dy, dz, dt, rate, gpus);
+    save(dir + "/ref_ddata.bin", ddata.data(), ddata.size());
+  } else if (mode == "grad") {
+    auto padb = load(dir + "/padb.bin", 3 * nb);
+    auto randb = load(dir + "/randb.bin", 3 * nb);
+    std::vector<float> fg(1 + 3 * n, 0.f);
+    objFuncGradientCij3d_f(fg.data(), souloc.data(), ns, shotid, recloc.data(), wavelet.data(),
+                           cij.data(), padb.data(), randb.data(), nx, ny, nz, nt, npad, ox, oy,
+                           oz, ot, dx, dy, dz, dt, rate, gpus);
+    save(dir + "/ref_fgcij.bin", fg.data(), fg.size());
+  } else {
+    std::fprintf(stderr, "unknown mode %s\n", mode.c_str());
+    return 2;
+  }
+  return 0;
+}

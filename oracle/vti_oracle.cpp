@@ -1,0 +1,545 @@
+// CPU ORACLE — TEST INFRASTRUCTURE ONLY.
+//
+// A plain C++/OpenMP restatement of the reference's VTI pseudo-acoustic
+// modeling / gradient path (huyleq/thesis-source-code, lib/vti-fwi-3d/gpu and
+// lib/vti-fwi-2d). It is the checker for the CUDA path and, in its FP32
+// instance, the timed CPU baseline. Nothing in the product library links,
+// loads or calls this file; only tests/, __graft_entry__.smoke() and the
+// cpu_baseline / reference legs of bench.py load it (through ctypes).
+//
+// Every function is templated on the arithmetic type T:
+//   T = double : the FP64 error oracle
+//   T = float  : the FP32 CPU baseline
+// Model arrays, damping tables and the scale factors dt^2/dx^2 are float
+// values in the reference, so they enter here as float and are promoted to T.
+//
+// Semantics restated (all file:line refer to the reference tree):
+//  * 3D step: lib/vti-fwi-3d/gpu/kernel3d.cu:3-74 (forward form, scale folded
+//    as dt2/dx2) and kernel3d.cu:222-298 (gradient form, dt2*(c*L/dx2)).
+//    x/y updates cover [4,n-4) (kernel3d.cu:7-10); z covers [0,nz) with zero
+//    planes outside (TopBlock/BottomBlock, kernel3d.cu:92,409).
+//  * Sponge: abc3d.cu:23-50 (profile), abc3d.cu:82-126 (applied per 4-plane
+//    z-block to next AND cur after each block's update,
+//    objFuncGradient3d_f.cu:661-662). Because blocks are processed in z
+//    order, the z-stencil of block b reads already-damped cur planes of block
+//    b-1 and undamped planes of blocks >= b. Stored values here are "once
+//    damped" (v_t); prev is read as d*v_{t-2} and the planes of the block
+//    above as d*v_{t-1}, which reproduces the reference bit-for-bit in the
+//    sequence of multiplications while writing each array once.
+//  * Time loop / source / recording: objFuncGradient3d_f.cu:605-706,
+//    modelData3d_f.cu:174-302 (source dt2*w[it-1] into next before the
+//    sponge; record 2/3 sx + 1/3 sz at it == s*j, j>=1, trace-major
+//    data[j + ir*nnt]); number of updates 64*floor((nt-2)/64)
+//    (objFuncGradient3d_f.cu:538-542, NUPDATE=64 wave3d.h:17).
+//  * Gradient: objFuncGradient3d_f.cu:361-1111 (pass 1 pad boundary + sponge
+//    + record; L2 misfit :759-771; pass 2 random boundary, no sponge;
+//    pass 3 time-reversed sigma (gradientKernel) + adjoint lambda with the
+//    FORWARD operator and the sponge + zero-lag imaging; residual injected
+//    2/3,1/3 * dt2 * linearly interpolated residual, injectRecord3d.cu:38-78).
+//  * 2D forward: lib/vti-fwi-2d/kernels.cu:452-498 (forwardCD),
+//    synthetic_f.cu:81-119, modeling_f.cu:43-82, taper kernels.cu:293-315.
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+#include <omp.h>
+
+namespace {
+
+// 8th-order second-derivative coefficients as the 3D reference writes them
+// (lib/vti-fwi-3d/gpu/wave3d.h:8-12, double literals).
+const double k3C0 = -2.84722222222, k3C1 = 1.6, k3C2 = -0.2, k3C3 = 0.02539682539,
+             k3C4 = -0.00178571428;
+// The 2D reference writes the same values as float literals
+// (lib/vti-fwi-2d/kernels.h:4-8).
+const float k2C0 = -2.84722222222f, k2C1 = 1.6f, k2C2 = -0.2f, k2C3 = 0.02539682539f,
+            k2C4 = -0.00178571428f;
+const double kTwoThird = 0.6666666666, kOneThird = 0.3333333333;  // wave3d.h:5-6
+const double kDamper = 0.95, kPi = 3.14159265359;                 // wave3d.h:4,14
+const int kNUpdate = 64;                                           // wave3d.h:17
+const int kHalf = 4;                                               // wave3d.h:19
+
+struct Geo3 {
+  int nx, ny, nz, nt, npad, ref_steps;
+  float ox, oy, oz, ot, dx, dy, dz, dt, rate;
+  long nxy() const { return (long)nx * ny; }
+  long nxyz() const { return (long)nx * ny * nz; }
+};
+
+Geo3 unpack3(const int* ip, const float* fp) {
+  Geo3 g;
+  g.nx = ip[0]; g.ny = ip[1]; g.nz = ip[2]; g.nt = ip[3]; g.npad = ip[4]; g.ref_steps = ip[5];
+  g.ox = fp[0]; g.oy = fp[1]; g.oz = fp[2]; g.ot = fp[3];
+  g.dx = fp[4]; g.dy = fp[5]; g.dz = fp[6]; g.dt = fp[7]; g.rate = fp[8];
+  return g;
+}
+
+// Last time level computed by the reference pipeline
+// (objFuncGradient3d_f.cu:538-542: it runs 2..1+64*nround).
+int last_level(const Geo3& g) {
+  if (g.ref_steps) return 1 + kNUpdate * ((g.nt - 2) / kNUpdate);
+  return g.nt - 1;
+}
+
+int sampling_step(float rate, float dt) { return (int)std::round(rate / dt); }
+
+// abc3d.cu:23-50: one-dimensional sponge profile in float.
+float damp_profile(int i, int n, int npad) {
+  float dist;
+  if (i < npad) dist = npad - i;
+  else if (i > n - npad) dist = i - n + npad;
+  else dist = 0.f;
+  return (float)(kDamper + (1. - kDamper) * std::cos(kPi * dist / npad));
+}
+
+struct Damp3 {
+  std::vector<float> xy, z;
+  Damp3(const Geo3& g) : xy(g.nxy()), z(g.nz) {
+    for (int iy = 0; iy < g.ny; ++iy) {
+      float dy = damp_profile(iy, g.ny, g.npad);
+      for (int ix = 0; ix < g.nx; ++ix) xy[ix + (long)iy * g.nx] = damp_profile(ix, g.nx, g.npad) * dy;
+    }
+    for (int iz = 0; iz < g.nz; ++iz) z[iz] = damp_profile(iz, g.nz, g.npad);
+  }
+  // abc3d.cu:93 (the abcXY variant multiplies by xy only, identical since
+  // the z profile is exactly 1.0f outside the pad).
+  float at(long ixy, int iz) const { return xy[ixy] * z[iz]; }
+};
+
+// One update of a (sigma_x, sigma_z) pair over the reference's update region.
+//   cur  : v_{t-1}            prev_next : in v_{t-2}, out v_t
+// kForwardForm: kernel3d.cu:54-69 (scale dt2/dx2 folded into the Laplacian)
+// otherwise    : kernel3d.cu:273-288 (dt2 * (c * L/dx2)).
+// damp != nullptr selects the sponge with the block-order reading rule.
+// Optional imaging (kernel3d.cu:291-293) uses lam_x/lam_z at time t-1.
+template <typename T, bool kForwardForm>
+void step3d(const Geo3& g, const float* c11, const float* c13, const float* c33, const T* cx,
+            const T* cz, T* px, T* pz, const Damp3* damp, const T* lamx, const T* lamz, T* g11,
+            T* g13, T* g33) {
+  const long nx = g.nx, ny = g.ny, nz = g.nz, nxy = g.nxy();
+  const float dx2 = g.dx * g.dx, dy2 = g.dy * g.dy, dz2 = g.dz * g.dz, dt2 = g.dt * g.dt;
+  const float sx = dt2 / dx2, sy = dt2 / dy2, sz = dt2 / dz2;
+  const T C[5] = {(T)k3C0, (T)k3C1, (T)k3C2, (T)k3C3, (T)k3C4};
+#pragma omp parallel for collapse(2) schedule(static)
+  for (long iz = 0; iz < nz; ++iz) {
+    for (long iy = kHalf; iy < ny - kHalf; ++iy) {
+      const long blk = iz / kHalf;
+      for (long ix = kHalf; ix < nx - kHalf; ++ix) {
+        const long ixy = ix + iy * nx, i = ixy + iz * nxy;
+        T lxx = C[0] * cx[i], lyy = C[0] * cx[i];
+        for (int k = 1; k <= 4; ++k) {
+          lxx += C[k] * (cx[i - k] + cx[i + k]);
+          lyy += C[k] * (cx[i - k * nx] + cx[i + k * nx]);
+        }
+        T zv[9];
+        for (int k = -4; k <= 4; ++k) {
+          long z2 = iz + k;
+          T v = 0;
+          if (z2 >= 0 && z2 < nz) {
+            v = cz[ixy + z2 * nxy];
+            if (damp && z2 / kHalf < blk) v *= (T)damp->at(ixy, (int)z2);
+          }
+          zv[k + 4] = v;
+        }
+        T lzz = C[0] * zv[4];
+        for (int k = 1; k <= 4; ++k) lzz += C[k] * (zv[4 - k] + zv[4 + k]);
+        const T d = damp ? (T)damp->at(ixy, (int)iz) : (T)1;
+        T nxv, nzv, lxy_u = 0, lz_u = 0;
+        if (kForwardForm) {
+          const T lxy = lxx * (T)sx + lyy * (T)sy, lz = lzz * (T)sz;
+          nxv = (T)c11[i] * lxy + (T)c13[i] * lz + 2 * cx[i] - d * px[i];
+          nzv = (T)c13[i] * lxy + (T)c33[i] * lz + 2 * cz[i] - d * pz[i];
+        } else {
+          lxy_u = lxx / (T)dx2 + lyy / (T)dy2;
+          lz_u = lzz / (T)dz2;
+          nxv = (T)dt2 * ((T)c11[i] * lxy_u + (T)c13[i] * lz_u) + 2 * cx[i] - d * px[i];
+          nzv = (T)dt2 * ((T)c13[i] * lxy_u + (T)c33[i] * lz_u) + 2 * cz[i] - d * pz[i];
+        }
+        px[i] = d * nxv;
+        pz[i] = d * nzv;
+        if (g11) {
+          g11[i] += lamx[i] * lxy_u;
+          g33[i] += lamz[i] * lz_u;
+          g13[i] += lamx[i] * lz_u + lamz[i] * lxy_u;
+        }
+      }
+    }
+  }
+}
+
+struct Shot3 {
+  long sidx;                 // source flat index
+  std::vector<long> ridx;    // receiver flat indices
+  std::vector<char> live;    // receiver flag != 0
+  int irbegin, nr;
+};
+
+// objFuncGradient3d_f.cu:551-575: float arithmetic, truncation toward zero.
+Shot3 make_shot3(const Geo3& g, const float* souloc, const float* recloc, int is) {
+  Shot3 s;
+  s.nr = (int)souloc[5 * is + 3];
+  s.irbegin = (int)souloc[5 * is + 4];
+  int sx = (int)((souloc[5 * is] - g.ox) / g.dx);
+  int sy = (int)((souloc[5 * is + 1] - g.oy) / g.dy);
+  int sz = (int)((souloc[5 * is + 2] - g.oz) / g.dz);
+  s.sidx = sx + (long)sy * g.nx + (long)sz * g.nxy();
+  s.ridx.resize(s.nr);
+  s.live.resize(s.nr);
+  for (int ir = 0; ir < s.nr; ++ir) {
+    int r = ir + s.irbegin;
+    int ix = (int)((recloc[4 * r] - g.ox) / g.dx);
+    int iy = (int)((recloc[4 * r + 1] - g.oy) / g.dy);
+    int iz = (int)((recloc[4 * r + 2] - g.oz) / g.dz);
+    s.ridx[ir] = ix + (long)iy * g.nx + (long)iz * g.nxy();
+    s.live[ir] = recloc[4 * r + 3] != 0.f;
+  }
+  return s;
+}
+
+// Forward propagation from the source. With damp: pass 1 of the gradient /
+// modelDataCij3d_f (records traces). Without: pass 2 (random boundary).
+// On return (cx,cz) = v_M and (px,pz) = v_{M-1}.
+template <typename T>
+void forward3d(const Geo3& g, const float* c11, const float* c13, const float* c33,
+               const float* wavelet, const Shot3& s, const Damp3* damp, T* trace /*nnt*nr or null*/,
+               std::vector<T>& cx, std::vector<T>& cz, std::vector<T>& px, std::vector<T>& pz) {
+  const long n = g.nxyz();
+  const float dt2 = g.dt * g.dt;
+  const int st = sampling_step(g.rate, g.dt);
+  const int nnt = (g.nt - 1) / st + 1;
+  const int M = last_level(g);
+  cx.assign(n, 0); cz.assign(n, 0); px.assign(n, 0); pz.assign(n, 0);
+  // "injecting source at time 0 to wavefields at time 1"
+  // (objFuncGradient3d_f.cu:605-608): assignment, no sponge.
+  const float s0 = dt2 * wavelet[0];
+  cx[s.sidx] = s0;
+  cz[s.sidx] = s0;
+  if (trace) std::fill(trace, trace + (long)nnt * s.nr, (T)0);
+  for (int it = 2; it <= M; ++it) {
+    step3d<T, true>(g, c11, c13, c33, cx.data(), cz.data(), px.data(), pz.data(), damp, nullptr,
+                    nullptr, nullptr, nullptr, nullptr);
+    // source before the sponge (objFuncGradient3d_f.cu:655-662): d*(raw+src)
+    const float src = dt2 * wavelet[it - 1];
+    const T d = damp ? (T)damp->at(s.sidx % g.nxy(), (int)(s.sidx / g.nxy())) : (T)1;
+    px[s.sidx] += d * (T)src;
+    pz[s.sidx] += d * (T)src;
+    std::swap(cx, px);
+    std::swap(cz, pz);
+    // recordData (injectRecord3d.cu:22-28) at it == s*j, j >= 1
+    if (trace && it % st == 0) {
+      int j = it / st;
+      if (j >= 1 && j < nnt)
+        for (int ir = 0; ir < s.nr; ++ir)
+          trace[j + (long)ir * nnt] =
+              (T)kTwoThird * cx[s.ridx[ir]] + (T)kOneThird * cz[s.ridx[ir]];
+    }
+  }
+  if (trace)
+    for (int ir = 0; ir < s.nr; ++ir)
+      if (!s.live[ir]) std::fill(trace + (long)ir * nnt, trace + (long)(ir + 1) * nnt, (T)0);
+}
+
+// boundary.cpp:48-84 putBoundary: scatter the pad-region list into a full array.
+void put_boundary(const float* b, float* v, int nx, int ny, int nz, int npad) {
+  size_t cb = 0, cv = 0, n = (size_t)nx * ny * npad;
+  std::memcpy(v + cv, b + cb, n * 4); cb += n; cv += n;
+  for (int iz = 0; iz < nz - 2 * npad; iz++) {
+    for (int iy = 0; iy < npad; iy++) { std::memcpy(v + cv, b + cb, nx * 4); cb += nx; cv += nx; }
+    for (int iy = 0; iy < ny - 2 * npad; iy++) {
+      std::memcpy(v + cv, b + cb, npad * 4); cb += npad; cv += nx - npad;
+      std::memcpy(v + cv, b + cb, npad * 4); cb += npad; cv += npad;
+    }
+    for (int iy = 0; iy < npad; iy++) { std::memcpy(v + cv, b + cb, nx * 4); cb += nx; cv += nx; }
+  }
+  n = (size_t)nx * ny * npad;
+  std::memcpy(v + cv, b + cb, n * 4);
+}
+
+template <typename T>
+T interp_residual(const T* res_trace, int time_index, int nnt, int st) {
+  // injectRecord3d.cu:60-78 (float f, double weights)
+  float f = float(time_index) / float(st);
+  int i = (int)f;
+  if (i >= nnt - 1) return res_trace[nnt - 1];
+  f = f - i;
+  return (T)((1. - f) * res_trace[i] + f * res_trace[i + 1]);
+}
+
+// objFuncGradientCij3d_f (objFuncGradient3d_f.cu:361-1111) for the shots in
+// shotid. fgcij[0] = misfit/2, then gc11, gc13, gc33 (nxyz each).
+// misfit_only: objFuncCij3d_f (pass 1 + misfit).
+template <typename T>
+void gradient3d(const Geo3& g, const float* cij_in, const float* padb, const float* randb,
+                const float* wavelet, const float* souloc, const int* shotid, int nshot,
+                const float* recloc, const float* dobs, T* fgcij, bool misfit_only,
+                T* modeled /*optional: nnt*nrtotal modeled traces*/) {
+  const long n = g.nxyz(), nxy = g.nxy();
+  const float dt2 = g.dt * g.dt;
+  const int st = sampling_step(g.rate, g.dt);
+  const int nnt = (g.nt - 1) / st + 1;
+  const int M = last_level(g);
+  std::vector<float> cij(cij_in, cij_in + 3 * n);
+  float *c11 = cij.data(), *c13 = c11 + n, *c33 = c13 + n;
+  const long nb = n - (long)(g.nx - 2 * g.npad) * (g.ny - 2 * g.npad) * (g.nz - 2 * g.npad);
+  if (!misfit_only) std::fill(fgcij, fgcij + 1 + 3 * n, (T)0);
+  T *g11 = fgcij + 1, *g13 = g11 + n, *g33 = g13 + n;
+  Damp3 damp(g);
+  double objfunc = 0;
+  std::vector<T> cx, cz, px, pz, lcx, lcz, lpx, lpz;
+  for (int k = 0; k < nshot; ++k) {
+    const int is = shotid[k];
+    Shot3 s = make_shot3(g, souloc, recloc, is);
+    // pass 1: pad boundary + sponge + record (objFuncGradient3d_f.cu:594-727)
+    put_boundary(padb, c11, g.nx, g.ny, g.nz, g.npad);
+    put_boundary(padb + nb, c13, g.nx, g.ny, g.nz, g.npad);
+    put_boundary(padb + 2 * nb, c33, g.nx, g.ny, g.nz, g.npad);
+    std::vector<T> res((long)nnt * s.nr);
+    forward3d<T>(g, c11, c13, c33, wavelet, s, &damp, res.data(), cx, cz, px, pz);
+    if (modeled)
+      std::copy(res.begin(), res.end(), modeled + (long)nnt * s.irbegin);
+    // L2 misfit (objFuncGradient3d_f.cu:759-771): residual = modeled - observed
+    const float* ob = dobs + (long)nnt * s.irbegin;
+    for (long i = 0; i < (long)nnt * s.nr; ++i) {
+      res[i] = res[i] - (T)ob[i];
+      objfunc += (double)(res[i] * res[i]);
+    }
+    if (misfit_only) continue;
+    // pass 2: random boundary, no sponge (objFuncGradient3d_f.cu:786-895)
+    put_boundary(randb, c11, g.nx, g.ny, g.nz, g.npad);
+    put_boundary(randb + nb, c13, g.nx, g.ny, g.nz, g.npad);
+    put_boundary(randb + 2 * nb, c33, g.nx, g.ny, g.nz, g.npad);
+    forward3d<T>(g, c11, c13, c33, wavelet, s, nullptr, nullptr, cx, cz, px, pz);
+    // flip (objFuncGradient3d_f.cu:912-914): cur = v_{M-1}, prev = v_M
+    std::swap(cx, px);
+    std::swap(cz, pz);
+    lcx.assign(n, 0); lcz.assign(n, 0); lpx.assign(n, 0); lpz.assign(n, 0);
+    // objFuncGradient3d_f.cu:922-927: adjoint seeded by assignment
+    for (int ir = 0; ir < s.nr; ++ir) {
+      T temp = (T)dt2 * res[(nnt - 1) + (long)ir * nnt];
+      lcx[s.ridx[ir]] = (T)kTwoThird * temp;
+      lcz[s.ridx[ir]] = (T)kOneThird * temp;
+    }
+    const long sxy = s.sidx % nxy;
+    const int sz = (int)(s.sidx / nxy);
+    (void)sz;
+    std::vector<T> rfine(s.nr);
+    for (int i = 0; i < M - 1; ++i) {
+      const int it = g.nt - 3 - i;  // objFuncGradient3d_f.cu:996-997
+      // sigma back one step + imaging with the current adjoint
+      step3d<T, false>(g, c11, c13, c33, cx.data(), cz.data(), px.data(), pz.data(), nullptr,
+                       lcx.data(), lcz.data(), g11, g13, g33);
+      // adjoint with the forward operator and the sponge
+      step3d<T, true>(g, c11, c13, c33, lcx.data(), lcz.data(), lpx.data(), lpz.data(), &damp,
+                      nullptr, nullptr, nullptr, nullptr, nullptr);
+      const float src = dt2 * wavelet[it + 1];  // objFuncGradient3d_f.cu:1014
+      px[s.sidx] += (T)src;
+      pz[s.sidx] += (T)src;
+      // residual injection before the sponge (injectRecord3d.cu:38-46)
+      for (int ir = 0; ir < s.nr; ++ir) {
+        T r = interp_residual<T>(res.data() + (long)ir * nnt, it + 1, nnt, st);
+        T inj = (T)dt2 * r;
+        long ri = s.ridx[ir];
+        T d = (T)damp.at(ri % nxy, (int)(ri / nxy));
+        lpx[ri] += d * ((T)kTwoThird * inj);
+        lpz[ri] += d * ((T)kOneThird * inj);
+      }
+      (void)sxy;
+      std::swap(cx, px); std::swap(cz, pz);
+      std::swap(lcx, lpx); std::swap(lcz, lpz);
+    }
+  }
+  fgcij[0] = (T)(objfunc / 2);
+}
+
+// ----------------------------------------------------------------- 2D ------
+struct Geo2 {
+  int nx, nz, nt, npad;
+  float dx, dz, dt, rate, ot;
+  int nnx() const { return nx + 2 * npad; }
+  int nnz() const { return nz + 2 * npad; }
+};
+
+Geo2 unpack2(const int* ip, const float* fp) {
+  Geo2 g;
+  g.nx = ip[0]; g.nz = ip[1]; g.nt = ip[2]; g.npad = ip[3];
+  g.dx = fp[0]; g.dz = fp[1]; g.dt = fp[2]; g.rate = fp[3]; g.ot = fp[4];
+  return g;
+}
+
+// forwardCD (kernels.cu:452-498): p0 <- 2p1 + dt2(c11 Dxx p1 + c13 Dzz q1) - p0.
+template <typename T>
+void step2d(const Geo2& g, const float* c11, const float* c13, const float* c33, const T* p1,
+            const T* q1, T* p0, T* q0) {
+  const long nnx = g.nnx(), nnz = g.nnz();
+  const float dx2 = g.dx * g.dx, dz2 = g.dz * g.dz, dt2 = g.dt * g.dt;
+  const T C[5] = {(T)k2C0, (T)k2C1, (T)k2C2, (T)k2C3, (T)k2C4};
+#pragma omp parallel for schedule(static)
+  for (long iz = kHalf; iz < nnz - kHalf; ++iz)
+    for (long ix = kHalf; ix < nnx - kHalf; ++ix) {
+      long i = ix + iz * nnx;
+      T tp = C[0] * p1[i], tq = C[0] * q1[i];
+      for (int k = 1; k <= 4; ++k) {
+        tp += C[k] * (p1[i - k] + p1[i + k]);
+        tq += C[k] * (q1[i - k * nnx] + q1[i + k * nnx]);
+      }
+      tp /= (T)dx2;
+      tq /= (T)dz2;
+      p0[i] = 2 * p1[i] + (T)dt2 * ((T)c11[i] * tp + (T)c13[i] * tq) - p0[i];
+      q0[i] = 2 * q1[i] + (T)dt2 * ((T)c13[i] * tp + (T)c33[i] * tq) - q0[i];
+    }
+}
+
+template <typename T>
+void taper2d(const Geo2& g, const float* taper, T* a) {
+  const long nnx = g.nnx(), nnz = g.nnz();
+  for (long iz = kHalf; iz < nnz - kHalf; ++iz)
+    for (long ix = kHalf; ix < nnx - kHalf; ++ix) a[ix + iz * nnx] *= (T)taper[ix + iz * nnx];
+}
+
+// synthetic_f (synthetic_f.cu:13-124) and modeling_f (modeling_f.cu:10-82).
+// mode 0: traces, data[t*nr + ir_global] = 0.5(p+q) at receivers.
+// mode 1: snapshots of p (modeling_f), out[t*nnxz + i]; the source term of
+//         modeling_f's time loop is wavelet[it-1] without dt2
+//         (modeling_f.cu:66).
+template <typename T>
+void forward2d(const Geo2& g, const float* c11, const float* c13, const float* c33,
+               const float* wavelet, const int* sloc, int is, const int* rloc, int nr_total,
+               const float* taper, T* out, int mode) {
+  const long nnx = g.nnx(), nnxz = nnx * g.nnz();
+  const float dt = g.dt, dt2 = dt * dt;
+  const int ratio = mode == 0 ? (int)(g.rate / dt + 0.5f) : (int)std::round(g.rate / dt);
+  const int ntNeg = (int)std::round(std::fabs(g.ot) / dt);
+  std::vector<T> p0(nnxz, 0), q0(nnxz, 0), p1(nnxz, 0), q1(nnxz, 0);
+  long slocxz = mode == 0 ? sloc[4 * is] + (long)sloc[4 * is + 1] * nnx : sloc[0];
+  const int nri = mode == 0 ? sloc[4 * is + 2] : 0;
+  const int ir0 = mode == 0 ? sloc[4 * is + 3] : 0;
+  auto record = [&](long row, const T* p, const T* q) {
+    if (mode == 0) {
+      for (int ir = 0; ir < nri; ++ir) {
+        long i = rloc[2 * (ir0 + ir)] + (long)rloc[2 * (ir0 + ir) + 1] * nnx;
+        out[row * nr_total + ir0 + ir] = (T)0.5f * (p[i] + q[i]);
+      }
+    } else {
+      std::copy(p, p + nnxz, out + row * nnxz);
+    }
+  };
+  p1[slocxz] += (T)(dt2 * wavelet[0]);
+  q1[slocxz] += (T)(dt2 * wavelet[0]);
+  taper2d(g, taper, p1.data());
+  taper2d(g, taper, q1.data());
+  if (ratio == 1 && g.ot == 0.f) record(1, p1.data(), q1.data());
+  for (int it = 2; it < g.nt; ++it) {
+    float t = it * dt + g.ot;
+    step2d<T>(g, c11, c13, c33, p1.data(), q1.data(), p0.data(), q0.data());
+    float src = mode == 0 ? dt2 * wavelet[it - 1] : wavelet[it - 1];
+    p0[slocxz] += (T)src;
+    q0[slocxz] += (T)src;
+    taper2d(g, taper, p1.data()); taper2d(g, taper, q1.data());
+    taper2d(g, taper, p0.data()); taper2d(g, taper, q0.data());
+    if (t >= 0.f && (it - ntNeg) % ratio == 0) record((it - ntNeg) / ratio, p0.data(), q0.data());
+    std::swap(p0, p1);
+    std::swap(q0, q1);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+// Damping tables of abc3d.cu:23-50 (nx*ny then nz floats).
+void orc3d_damping(int nx, int ny, int nz, int npad, float* out) {
+  Geo3 g{};
+  g.nx = nx; g.ny = ny; g.nz = nz; g.npad = npad;
+  Damp3 d(g);
+  std::copy(d.xy.begin(), d.xy.end(), out);
+  std::copy(d.z.begin(), d.z.end(), out + d.xy.size());
+}
+
+int orc3d_last_level(const int* ip, const float* fp) { return last_level(unpack3(ip, fp)); }
+
+#define ORC3D_MODEL(T, SUF)                                                                    \
+  int orc3d_model_data_##SUF(const int* ip, const float* fp, const float* c11, const float* c13, \
+                             const float* c33, const float* wavelet, const float* souloc,       \
+                             const int* shotid, int nshot, const float* recloc, T* ddata,       \
+                             T* final_x) {                                                      \
+    Geo3 g = unpack3(ip, fp);                                                                   \
+    Damp3 damp(g);                                                                              \
+    const int nnt = (g.nt - 1) / sampling_step(g.rate, g.dt) + 1;                               \
+    std::vector<T> cx, cz, px, pz;                                                              \
+    for (int k = 0; k < nshot; ++k) {                                                           \
+      Shot3 s = make_shot3(g, souloc, recloc, shotid[k]);                                       \
+      forward3d<T>(g, c11, c13, c33, wavelet, s, &damp, ddata + (long)nnt * s.irbegin, cx, cz,  \
+                   px, pz);                                                                     \
+      if (final_x) std::copy(cx.begin(), cx.end(), final_x);                                    \
+    }                                                                                           \
+    return 0;                                                                                   \
+  }
+ORC3D_MODEL(double, f64)
+ORC3D_MODEL(float, f32)
+
+#define ORC3D_GRAD(T, SUF)                                                                      \
+  int orc3d_gradient_cij_##SUF(const int* ip, const float* fp, const float* cij,                \
+                               const float* padb, const float* randb, const float* wavelet,     \
+                               const float* souloc, const int* shotid, int nshot,               \
+                               const float* recloc, const float* dobs, T* fgcij, int misfit_only, \
+                               T* modeled) {                                                    \
+    Geo3 g = unpack3(ip, fp);                                                                   \
+    gradient3d<T>(g, cij, padb, randb, wavelet, souloc, shotid, nshot, recloc, dobs, fgcij,     \
+                  misfit_only != 0, modeled);                                                   \
+    return 0;                                                                                   \
+  }
+ORC3D_GRAD(double, f64)
+ORC3D_GRAD(float, f32)
+
+// Time `nsteps` forward steps (forward form, sponge) of a zero-initialised
+// grid with a point source: the FP32 instance is the CPU baseline's unit of
+// work. Returns the number of threads used.
+int orc3d_time_forward_f32(const int* ip, const float* fp, const float* c11, const float* c13,
+                           const float* c33, int nsteps, float* scratch4) {
+  Geo3 g = unpack3(ip, fp);
+  Damp3 damp(g);
+  const long n = g.nxyz();
+  float *cx = scratch4, *cz = cx + n, *px = cz + n, *pz = px + n;
+  for (int it = 0; it < nsteps; ++it) {
+    step3d<float, true>(g, c11, c13, c33, cx, cz, px, pz, &damp, nullptr, nullptr, nullptr,
+                        nullptr, nullptr);
+    std::swap(cx, px);
+    std::swap(cz, pz);
+  }
+  return omp_get_max_threads();
+}
+
+// Time `nsteps` of the fused backward work (sigma back-step + imaging +
+// adjoint step with sponge), FP32.
+int orc3d_time_backward_f32(const int* ip, const float* fp, const float* c11, const float* c13,
+                            const float* c33, int nsteps, float* scratch11) {
+  Geo3 g = unpack3(ip, fp);
+  Damp3 damp(g);
+  const long n = g.nxyz();
+  float *cx = scratch11, *cz = cx + n, *px = cz + n, *pz = px + n;
+  float *lx = pz + n, *lz = lx + n, *lpx = lz + n, *lpz = lpx + n;
+  float *g11 = lpz + n, *g13 = g11 + n, *g33 = g13 + n;
+  for (int it = 0; it < nsteps; ++it) {
+    step3d<float, false>(g, c11, c13, c33, cx, cz, px, pz, nullptr, lx, lz, g11, g13, g33);
+    step3d<float, true>(g, c11, c13, c33, lx, lz, lpx, lpz, &damp, nullptr, nullptr, nullptr,
+                        nullptr, nullptr);
+    std::swap(cx, px); std::swap(cz, pz);
+    std::swap(lx, lpx); std::swap(lz, lpz);
+  }
+  return omp_get_max_threads();
+}
+
+#define ORC2D_FWD(T, SUF)                                                                      \
+  int orc2d_forward_##SUF(const int* ip, const float* fp, const float* c11, const float* c13,   \
+                          const float* c33, const float* wavelet, const int* sloc, int ns,      \
+                          const int* rloc, int nr, const float* taper, T* out, int mode) {      \
+    Geo2 g = unpack2(ip, fp);                                                                   \
+    for (int is = 0; is < (mode == 0 ? ns : 1); ++is)                                           \
+      forward2d<T>(g, c11, c13, c33, wavelet, sloc, is, rloc, nr, taper, out, mode);            \
+    return 0;                                                                                   \
+  }
+ORC2D_FWD(double, f64)
+ORC2D_FWD(float, f32)
+
+}  // extern "C"

@@ -1,0 +1,58 @@
+"""Golden cases: seeded inputs shared by make_golden.py (which runs the
+reference binaries built by oracle/build_ref.sh) and the tests (which
+regenerate the same inputs and compare against the stored outputs).
+
+Inputs are regenerated, not stored; each fixture keeps a checksum of its
+inputs so a change of generator is detected instead of silently compared.
+"""
+from __future__ import annotations
+
+import hashlib
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT / "thesis-source-code_b200"))
+
+import vtib200 as V  # noqa: E402
+import vtib200.synth as S  # noqa: E402
+
+GOLDEN = Path(__file__).resolve().parent
+
+
+def digest(*arrays) -> str:
+    h = hashlib.sha256()
+    for a in arrays:
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()[:16]
+
+
+def case3d(name: str) -> dict:
+    """3D inputs: survey (starting model), observed data source model, boundaries."""
+    if name == "g3_a":
+        # nt = 64*2+2: the reference pipeline runs every level
+        s = S.small3d(nx=40, ny=36, nz=32, nt=130, npad=8, rec_step=3, nshot=1)
+    elif name == "g3_b":
+        # nt not of the form 64k+2 (pipeline truncation) and two shots
+        s = S.small3d(nx=36, ny=40, nz=28, nt=100, npad=6, rec_step=4, nshot=2, seed=5)
+    else:
+        raise KeyError(name)
+    true = S.small3d(nx=s.nx, ny=s.ny, nz=s.nz, nt=s.nt, npad=s.npad, seed=11)
+    padb, randb = S.boundaries3d(s)
+    return {"s": s, "cij": s.cij(), "cij_true": true.cij(), "padb": padb, "randb": randb,
+            "shotid": np.arange(s.souloc.size // 5, dtype=np.int32)}
+
+
+def case2d(name: str) -> dict:
+    if name == "g2_a":
+        s = S.survey2d(nx=64, nz=40, nt=300, npad=10, d=10.0, dt=1e-3, rate=2e-3, freq=20.0,
+                       src_x=300.0, src_z=50.0, rec_z=20.0, ns=2)
+    else:
+        raise KeyError(name)
+    return {"s": s}
+
+
+CASES3D = ["g3_a", "g3_b"]
+CASES2D = ["g2_a"]

@@ -1,0 +1,104 @@
+"""Generate the golden fixtures by running the reference's own GPU code.
+
+Runs oracle/_ref/ref3d and oracle/_ref/ref2d (the unmodified reference
+sources compiled for sm_100a by oracle/build_ref.sh) on the seeded inputs of
+cases.py and stores their outputs, with input checksums, as
+tests/golden/<case>.npz. Needs a GPU; run from the repository root:
+
+    python tests/golden/make_golden.py [--out tests/golden]
+"""
+from __future__ import annotations
+
+import argparse
+import subprocess
+import sys
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE))
+import cases as K  # noqa: E402
+
+REF = K.ROOT / "oracle" / "_ref"
+
+
+def run(binary, d, mode):
+    r = subprocess.run([str(REF / binary), str(d), mode], capture_output=True, text=True,
+                       timeout=600)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout[-2000:] + r.stderr[-2000:])
+        raise SystemExit(f"{binary} {mode} failed with {r.returncode}")
+
+
+def make3d(name, out):
+    c = K.case3d(name)
+    s = c["s"]
+    g = s.geom()
+    ns = s.souloc.size // 5
+    nrec = s.recloc.size // 4
+    with tempfile.TemporaryDirectory() as td:
+        d = Path(td)
+        (d / "params.txt").write_text(
+            f"{s.nx} {s.ny} {s.nz} {s.nt} {s.npad} {g.ox!r} {g.oy!r} {g.oz!r} {g.ot!r} "
+            f"{g.dx!r} {g.dy!r} {g.dz!r} {g.dt!r} {g.sampling_rate!r} {ns} {nrec}\n")
+        for k, a in {"souloc": s.souloc, "recloc": s.recloc, "wavelet": s.wavelet,
+                     "padb": c["padb"], "randb": c["randb"]}.items():
+            np.asarray(a, dtype=np.float32).tofile(d / f"{k}.bin")
+        np.asarray(c["cij_true"], np.float32).tofile(d / "cij.bin")
+        run("ref3d", d, "model")
+        dobs = np.fromfile(d / "ref_ddata.bin", dtype=np.float32)
+        dobs.tofile(d / "dobs.bin")
+        np.asarray(c["cij"], np.float32).tofile(d / "cij.bin")
+        run("ref3d", d, "model")
+        ddata = np.fromfile(d / "ref_ddata.bin", dtype=np.float32)
+        run("ref3d", d, "grad")
+        fg = np.fromfile(d / "ref_fgcij.bin", dtype=np.float32)
+    np.savez_compressed(out / f"{name}.npz", dobs=dobs, ddata=ddata, fgcij=fg,
+                        inputs=K.digest(s.souloc, s.recloc, s.wavelet, c["cij"], c["cij_true"],
+                                        c["padb"], c["randb"]))
+    print(name, "dobs max", np.abs(dobs).max(), "misfit/2", fg[0])
+
+
+def make2d(name, out):
+    s = K.case2d(name)["s"]
+    g = s.geom()
+    ns = s.sloc.size // 4
+    nr = s.rloc.size // 2
+    with tempfile.TemporaryDirectory() as td:
+        d = Path(td)
+        (d / "params.txt").write_text(
+            f"{s.nx} {s.nz} {s.nt} {s.npad} {g.dx!r} {g.dz!r} {g.dt!r} {g.rate!r} {g.ot!r} "
+            f"{ns} {nr}\n")
+        for k in ("c11", "c13", "c33", "taper", "wavelet"):
+            np.asarray(getattr(s, k), np.float32).tofile(d / f"{k}.bin")
+        np.asarray(s.sloc, np.int32).tofile(d / "sloc.bin")
+        np.asarray(s.rloc, np.int32).tofile(d / "rloc.bin")
+        run("ref2d", d, "synthetic")
+        data = np.fromfile(d / "ref_data.bin", dtype=np.float32)
+        run("ref2d", d, "modeling")
+        w = np.fromfile(d / "ref_wavefield.bin", dtype=np.float32)
+    nnxz = (s.nx + 2 * s.npad) * (s.nz + 2 * s.npad)
+    w = w.reshape(-1, nnxz)
+    keep = np.arange(0, w.shape[0], 10)
+    np.savez_compressed(out / f"{name}.npz", data=data, snaps=w[keep], snap_rows=keep,
+                        inputs=K.digest(s.c11, s.c13, s.c33, s.taper, s.wavelet, s.sloc,
+                                        s.rloc))
+    print(name, "data max", np.abs(data).max())
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=str(HERE))
+    a = ap.parse_args()
+    out = Path(a.out)
+    out.mkdir(parents=True, exist_ok=True)
+    for n in K.CASES3D:
+        make3d(n, out)
+    for n in K.CASES2D:
+        make2d(n, out)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,44 @@
+"""GPU parity tests of the 2D forward path (synthetic_f / modeling_f)."""
+import numpy as np
+import pytest
+
+import cases as K
+import oracle as O
+from conftest import load_golden, rel_l2
+
+import vtib200 as V
+import vtib200.synth as S
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", K.CASES2D)
+def test_synthetic_matches_oracle_and_reference(ctx, name):
+    s = K.case2d(name)["s"]
+    g = s.geom()
+    d = V.synthetic_f(ctx, g, s.c11, s.c13, s.c33, s.wavelet, s.sloc, s.rloc, s.taper)
+    o = O.forward2d(g, s.c11, s.c13, s.c33, s.wavelet, s.sloc, s.rloc, s.taper)
+    assert np.abs(o).max() > 0
+    assert rel_l2(d, o) < 1e-5
+    assert rel_l2(d.reshape(-1), load_golden(name)["data"]) < 1e-5
+
+
+@pytest.mark.parametrize("name", K.CASES2D)
+def test_modeling_matches_oracle_and_reference(ctx, name):
+    s = K.case2d(name)["s"]
+    g = s.geom()
+    sxz = int(s.sloc[0] + s.sloc[1] * (s.nx + 2 * s.npad))
+    w = V.modeling_f(ctx, g, s.c11, s.c13, s.c33, s.wavelet, sxz, s.taper)
+    o = O.forward2d(g, s.c11, s.c13, s.c33, s.wavelet, None, None, s.taper, mode=1, slocxz=sxz)
+    assert rel_l2(w[: o.shape[0]], o) < 1e-5
+    gold = load_golden(name)
+    assert rel_l2(w[gold["snap_rows"]], gold["snaps"]) < 1e-5
+
+
+def test_synthetic_config_size(ctx):
+    """The 2D benchmark grid (201 x 401 + 30-cell pad, 2000 steps), one shot."""
+    s = S.survey2d()
+    g = s.geom()
+    d = V.synthetic_f(ctx, g, s.c11, s.c13, s.c33, s.wavelet, s.sloc, s.rloc, s.taper)
+    o = O.forward2d(g, s.c11, s.c13, s.c33, s.wavelet, s.sloc, s.rloc, s.taper)
+    assert rel_l2(d, o) < 1e-5

@@ -1,0 +1,139 @@
+"""GPU parity tests of the 3D path, called through the C ABI.
+
+Tolerances (relative L2): FP32 traces 1e-5 against the FP64 oracle and the
+reference's own outputs; gradients 1e-4 against the FP64 oracle.
+"""
+import numpy as np
+import pytest
+
+import cases as K
+import oracle as O
+from conftest import load_golden, rel_l2
+
+import vtib200 as V
+import vtib200.synth as S
+
+pytestmark = pytest.mark.gpu
+
+TRACE_TOL = 1e-5
+GRAD_TOL = 1e-4
+
+
+def _split(cij, n):
+    return cij[:n], cij[n:2 * n], cij[2 * n:]
+
+
+def _parts(fg, n):
+    return [fg[1 + k * n:1 + (k + 1) * n] for k in range(3)]
+
+
+@pytest.mark.parametrize("name", K.CASES3D)
+def test_model_data_matches_oracle_and_reference(ctx, name):
+    c = K.case3d(name)
+    s = c["s"]
+    g = s.geom()
+    n = s.nxyz
+    d = V.modelDataCij3d_f(ctx, g, s.souloc, c["shotid"], s.recloc, s.wavelet,
+                           *_split(c["cij_true"], n))
+    o = O.model_data3d(g, *_split(c["cij_true"], n), s.wavelet, s.souloc, c["shotid"], s.recloc)
+    assert np.abs(o).max() > 0
+    assert rel_l2(d, o) < TRACE_TOL
+    gold = load_golden(name)
+    assert rel_l2(d, gold["dobs"]) < TRACE_TOL
+
+
+@pytest.mark.parametrize("name", K.CASES3D)
+def test_gradient_matches_oracle_and_reference(ctx, name):
+    c = K.case3d(name)
+    s = c["s"]
+    g = s.geom()
+    n = s.nxyz
+    gold = load_golden(name)
+    dobs = gold["dobs"]
+    fg, mis = V.objFuncGradientCij3d_f(ctx, g, s.souloc, c["shotid"], s.recloc, s.wavelet,
+                                       c["cij"], c["padb"], c["randb"], dobs)
+    o = O.gradient3d(g, c["cij"], c["padb"], c["randb"], s.wavelet, s.souloc, c["shotid"],
+                     s.recloc, dobs)
+    assert abs(mis - o[0]) / o[0] < TRACE_TOL
+    assert abs(fg[0] - o[0]) / o[0] < TRACE_TOL
+    ref = gold["fgcij"]
+    for k, (a, b, r) in enumerate(zip(_parts(fg, n), _parts(o, n), _parts(ref, n))):
+        assert np.abs(b).max() > 0
+        assert rel_l2(a, b) < GRAD_TOL, k
+        assert rel_l2(a, r) < GRAD_TOL, k
+
+
+def test_full_steps_option(ctx):
+    c = K.case3d("g3_b")
+    s = c["s"]
+    g = s.geom()
+    n = s.nxyz
+    d = V.modelDataCij3d_f(ctx, g, s.souloc, c["shotid"], s.recloc, s.wavelet,
+                           *_split(c["cij"], n), flags=V.OPT_FULL_STEPS)
+    o = O.model_data3d(g, *_split(c["cij"], n), s.wavelet, s.souloc, c["shotid"], s.recloc,
+                       full_steps=True)
+    assert rel_l2(d, o) < TRACE_TOL
+    # the reference truncation leaves the late samples at zero
+    nnt = O.nnt3d(g)
+    tr = O.model_data3d(g, *_split(c["cij"], n), s.wavelet, s.souloc, c["shotid"], s.recloc)
+    assert not tr.reshape(-1, nnt)[:, O.last_level(g) // 2 + 1:].any()
+    assert np.abs(o.reshape(-1, nnt)[:, -5:]).max() > 0
+
+
+def test_plan_reuse_is_deterministic_and_objfunc_agrees(ctx):
+    c = K.case3d("g3_a")
+    s = c["s"]
+    g = s.geom()
+    n = s.nxyz
+    gold = load_golden("g3_a")
+    p = V.Plan3d(ctx, g)
+    p.set_model(*_split(c["cij"], n), padb=c["padb"], randb=c["randb"])
+    p.set_wavelet(s.wavelet)
+    p.set_receivers(s.recloc)
+    fg1, m1 = p.gradient(s.souloc, c["shotid"], gold["dobs"])
+    fg2, m2 = p.gradient(s.souloc, c["shotid"], gold["dobs"])
+    np.testing.assert_array_equal(fg1, fg2)
+    assert m1 == m2
+    m3 = p.objfunc(s.souloc, c["shotid"], gold["dobs"])
+    assert m3 == m1
+    p.close()
+
+
+def test_zero_residual_gives_zero_gradient(ctx):
+    """Observed data modeled by the library itself: residual and gradient are 0."""
+    s = S.small3d(nx=72, ny=64, nz=48, nt=130, npad=8, rec_step=2)
+    g = s.geom()
+    n = s.nxyz
+    padb, randb = S.boundaries3d(s)
+    cp = np.concatenate([V.put_boundary(padb[k * s.nb:(k + 1) * s.nb], s.cij()[k * n:(k + 1) * n],
+                                        s.nx, s.ny, s.nz, s.npad) for k in range(3)])
+    dobs = V.modelDataCij3d_f(ctx, g, s.souloc, [0], s.recloc, s.wavelet, *_split(cp, n))
+    assert np.abs(dobs).max() > 0
+    fg, mis = V.objFuncGradientCij3d_f(ctx, g, s.souloc, [0], s.recloc, s.wavelet, s.cij(), padb,
+                                       randb, dobs)
+    assert mis == 0.0 and fg[0] == 0.0 and not fg[1:].any()
+
+
+def test_linearity_in_wavelet_large(ctx):
+    """Size-independent property at a larger grid: traces scale with the source."""
+    s = S.small3d(nx=160, ny=144, nz=96, nt=194, npad=16, rec_step=4, d=12.5, dt=8e-4,
+                  rate=1.6e-3)
+    g = s.geom()
+    c = _split(s.cij(), s.nxyz)
+    d1 = V.modelDataCij3d_f(ctx, g, s.souloc, [0], s.recloc, s.wavelet, *c)
+    d2 = V.modelDataCij3d_f(ctx, g, s.souloc, [0], s.recloc, -2.0 * s.wavelet, *c)
+    assert np.abs(d1).max() > 0
+    assert rel_l2(d2, -2.0 * d1) < 1e-6
+
+
+def test_source_outside_update_region_is_rejected(ctx):
+    s = S.small3d(nx=24, ny=24, nz=20, nt=70, npad=4, rec_step=4)
+    g = s.geom()
+    so = s.souloc.copy()
+    so[0] = s.o + 1.25 * s.d  # ix = 1 lies in the never-updated 4-cell frame
+    with pytest.raises(V.VtiError) as e:
+        V.modelDataCij3d_f(ctx, g, so, [0], s.recloc, s.wavelet, *_split(s.cij(), s.nxyz))
+    assert e.value.status == V.VTI_ERR_ARG
+    bad = V.geom3d(8, 8, 8, 10, 2, 10.0, 10.0, 10.0, 1e-3, 2e-3)
+    with pytest.raises(V.VtiError):
+        V.Plan3d(ctx, bad)

@@ -1,0 +1,128 @@
+"""CPU tests of the C-ABI library's host side: it loads, exports every symbol
+its header declares, and its host glue matches the reference formulas."""
+import ctypes
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, rel_l2
+
+import vtib200 as V
+
+
+def header_functions():
+    txt = (ROOT / "include" / "vti_b200.h").read_text()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(vti\w+)\s*\(", txt)))
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    lib = ctypes.CDLL(str(V.LIB_PATH))
+    names = header_functions()
+    assert len(names) >= 25
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_binding_declares_only_header_symbols():
+    assert set(V.exported_symbols()) <= set(header_functions())
+
+
+def _boundary_mask(nx, ny, nz, npad):
+    m = np.ones((nz, ny, nx), dtype=bool)
+    m[npad:nz - npad, npad:ny - npad, npad:nx - npad] = False
+    return m.reshape(-1)
+
+
+@pytest.mark.parametrize("dims", [(12, 10, 9, 2), (20, 16, 14, 4), (9, 9, 9, 1)])
+def test_boundary_get_put_zero(dims):
+    nx, ny, nz, npad = dims
+    rng = np.random.default_rng(0)
+    v = rng.standard_normal(nx * ny * nz).astype(np.float32)
+    b = V.get_boundary(v, nx, ny, nz, npad)
+    mask = _boundary_mask(nx, ny, nz, npad)
+    assert b.size == mask.sum()
+    # the list holds exactly the pad-region values, in the x-fastest scan order
+    np.testing.assert_array_equal(b, v[mask])
+    w = V.put_boundary(b * 2, v, nx, ny, nz, npad)
+    np.testing.assert_array_equal(w[mask], 2 * v[mask])
+    np.testing.assert_array_equal(w[~mask], v[~mask])
+    z = V.zero_boundary(v, nx, ny, nz, npad)
+    assert not z[mask].any()
+    np.testing.assert_array_equal(z[~mask], v[~mask])
+
+
+def test_vepsdel_conversion_and_chain_rule():
+    rng = np.random.default_rng(1)
+    n = 1000
+    v = rng.uniform(1.5, 4.5, n).astype(np.float32)
+    eps = rng.uniform(0, 0.2, n).astype(np.float32)
+    dl = rng.uniform(0, 0.1, n).astype(np.float32)
+    v0, e0, d0 = 1000.0, 1.0, 1.0
+    c11, c13, c33 = V.vepsdel_to_cij(v, eps, dl, v0, e0, d0)
+    vv = (v0 * v.astype(np.float64)) ** 2
+    np.testing.assert_allclose(c33, vv, rtol=1e-6)
+    np.testing.assert_allclose(c11, vv * (1 + 2 * eps), rtol=1e-6)
+    np.testing.assert_allclose(c13, vv * np.sqrt(1 + 2 * dl), rtol=1e-6)
+    # chain rule = transpose of the Jacobian: <g, dC/dm dm> = <J^T g, dm>
+    g = [rng.standard_normal(n).astype(np.float32) for _ in range(3)]
+    gv, ge, gd = V.grad_cij_to_vepsdel(*g, v, eps, dl, v0, e0, d0)
+    h = 1e-3
+    for k, (gm, arr) in enumerate(zip((gv, ge, gd), (v, eps, dl))):
+        dm = np.zeros((3, n), dtype=np.float64)
+        dm[k] = 1.0
+        args_p = [v.astype(np.float64), eps.astype(np.float64), dl.astype(np.float64)]
+        args_m = [a.copy() for a in args_p]
+        args_p[k] = args_p[k] + h
+        args_m[k] = args_m[k] - h
+
+        def cij(a):
+            q = (v0 * a[0]) ** 2
+            return q * (1 + 2 * e0 * a[1]), q * np.sqrt(1 + 2 * d0 * a[2]), q
+
+        cp, cm = cij(args_p), cij(args_m)
+        fd = sum(g[j].astype(np.float64) * (cp[j] - cm[j]) / (2 * h) for j in range(3))
+        assert rel_l2(gm, fd) < 1e-4, k
+
+
+def test_check_eps_del_projection():
+    eps = np.array([0.1, 0.05, 0.2], dtype=np.float32)
+    dl = np.array([0.05, 0.1, 0.2], dtype=np.float32)
+    lib = V.lib()
+    mask = np.zeros(3, dtype=np.float32)
+    cnt = lib.vti_check_eps_del(V._p(eps), V._p(dl), 1.0, 1.0, 3, V._p(mask))
+    assert cnt == 1
+    assert eps[1] == dl[1]  # projected onto del == eps
+    assert list(mask) == [0.0, 2.0, 1.0]
+
+
+def test_cfl_number_matches_eigenvalues():
+    rng = np.random.default_rng(2)
+    n = 200
+    c33 = rng.uniform(1.5e3, 4.5e3, n).astype(np.float32) ** 2
+    c11 = (c33 * rng.uniform(1.0, 1.4, n)).astype(np.float32)
+    c13 = (c33 * rng.uniform(1.0, 1.2, n)).astype(np.float32)
+    g = V.geom3d(2, 2, n // 4, 10, 0, 10.0, 12.0, 8.0, 1e-3, 2e-3)
+    g.nx, g.ny, g.nz = 2, 2, n // 4
+    cfl = V.cfl_number(g, c11, c13, c33)
+    C = np.array([-2.84722222222, 1.6, -0.2, 0.02539682539, -0.00178571428])
+    s = abs(C[0] + 2 * sum(C[k] * (-1) ** k for k in range(1, 5)))
+    kh, kz = s / 10.0**2 + s / 12.0**2, s / 8.0**2
+    lam = max(np.linalg.eigvals(np.array([[a * kh, b * kz], [b * kh, c * kz]])).real.max()
+              for a, b, c in zip(c11.astype(np.float64), c13.astype(np.float64),
+                                 c33.astype(np.float64)))
+    dt2 = float(np.float32(1e-3)) ** 2
+    assert abs(cfl - lam * dt2) / (lam * dt2) < 1e-9
+
+
+def test_taper2d_profile():
+    nx, nz, npad = 20, 10, 5
+    t = V.init_taper2d(nx, nz, npad).reshape(nz + 2 * npad, nx + 2 * npad)
+    pi = np.float64(np.float32(4 * np.arctan(np.float32(1))))
+    t0 = (np.float32(0.95) + (1 - np.float64(np.float32(0.95))) *
+          np.cos(pi * (npad - 1 - np.arange(npad)) / npad)).astype(np.float32)
+    assert np.all(t[npad:-npad, npad:-npad] == 1)
+    np.testing.assert_allclose(t[nz // 2 + npad, :npad], t0, rtol=1e-7)
+    np.testing.assert_allclose(t[nz // 2 + npad, -npad:], t0[::-1], rtol=1e-7)
+    np.testing.assert_allclose(t[0, 0], t0[0] * t0[0], rtol=1e-6)

@@ -1,0 +1,106 @@
+"""CPU tests of the oracle: pinned against the reference's own GPU outputs
+(golden fixtures made by tests/golden/make_golden.py from the unmodified
+reference sources), plus self-consistency properties."""
+import numpy as np
+import pytest
+
+import cases as K
+import oracle as O
+from conftest import load_golden, rel_l2
+
+import vtib200.synth as S
+
+
+def _split(cij, n):
+    return cij[:n], cij[n:2 * n], cij[2 * n:]
+
+
+@pytest.mark.parametrize("name", K.CASES3D)
+def test_oracle_model_data_matches_reference(name):
+    c = K.case3d(name)
+    s = c["s"]
+    gold = load_golden(name)
+    assert str(gold["inputs"]) == K.digest(s.souloc, s.recloc, s.wavelet, c["cij"],
+                                           c["cij_true"], c["padb"], c["randb"])
+    g = s.geom()
+    n = s.nxyz
+    for key, cij in (("dobs", c["cij_true"]), ("ddata", c["cij"])):
+        d = O.model_data3d(g, *_split(cij, n), s.wavelet, s.souloc, c["shotid"], s.recloc)
+        assert rel_l2(d, gold[key]) < 1e-5, key
+
+
+@pytest.mark.parametrize("name", K.CASES3D)
+def test_oracle_gradient_matches_reference(name):
+    c = K.case3d(name)
+    s = c["s"]
+    gold = load_golden(name)
+    g = s.geom()
+    fg = O.gradient3d(g, c["cij"], c["padb"], c["randb"], s.wavelet, s.souloc, c["shotid"],
+                      s.recloc, gold["dobs"])
+    ref = gold["fgcij"].astype(np.float64)
+    assert abs(fg[0] - ref[0]) / abs(ref[0]) < 1e-5
+    n = s.nxyz
+    for k in range(3):
+        assert rel_l2(fg[1 + k * n:1 + (k + 1) * n], ref[1 + k * n:1 + (k + 1) * n]) < 1e-4, k
+
+
+@pytest.mark.parametrize("name", K.CASES2D)
+def test_oracle_2d_matches_reference(name):
+    s = K.case2d(name)["s"]
+    gold = load_golden(name)
+    assert str(gold["inputs"]) == K.digest(s.c11, s.c13, s.c33, s.taper, s.wavelet, s.sloc,
+                                           s.rloc)
+    g = s.geom()
+    d = O.forward2d(g, s.c11, s.c13, s.c33, s.wavelet, s.sloc, s.rloc, s.taper)
+    assert rel_l2(d.reshape(-1), gold["data"]) < 1e-5
+    w = O.forward2d(g, s.c11, s.c13, s.c33, s.wavelet, None, None, s.taper, mode=1,
+                    slocxz=int(s.sloc[0] + s.sloc[1] * (s.nx + 2 * s.npad)))
+    assert rel_l2(w[gold["snap_rows"]], gold["snaps"]) < 1e-5
+
+
+def test_oracle_fp32_tracks_fp64():
+    c = K.case3d("g3_a")
+    s = c["s"]
+    g = s.geom()
+    n = s.nxyz
+    d64 = O.model_data3d(g, *_split(c["cij"], n), s.wavelet, s.souloc, c["shotid"], s.recloc)
+    d32 = O.model_data3d(g, *_split(c["cij"], n), s.wavelet, s.souloc, c["shotid"], s.recloc,
+                         dtype=np.float32)
+    assert rel_l2(d32, d64) < 1e-5
+
+
+def test_oracle_linear_in_wavelet_and_zero_source():
+    s = S.small3d(nx=24, ny=24, nz=20, nt=70, npad=4, rec_step=4)
+    g = s.geom()
+    n = s.nxyz
+    c = _split(s.cij(), n)
+    d1 = O.model_data3d(g, *c, s.wavelet, s.souloc, [0], s.recloc)
+    d2 = O.model_data3d(g, *c, 3.0 * s.wavelet, s.souloc, [0], s.recloc)
+    # source amplitudes are float products dt2*w (as in the reference)
+    assert rel_l2(d2, 3.0 * d1) < 1e-6
+    d0 = O.model_data3d(g, *c, 0.0 * s.wavelet, s.souloc, [0], s.recloc)
+    assert not d0.any()
+
+
+def test_oracle_zero_residual_gives_zero_gradient():
+    c = K.case3d("g3_a")
+    s = c["s"]
+    g = s.geom()
+    n = s.nxyz
+    # observed data from the same model (the sponge pass models with the pad
+    # boundary swapped in) and the same code: the residual is exactly 0
+    import vtib200 as V
+    cp = np.concatenate([V.put_boundary(c["padb"][k * s.nb:(k + 1) * s.nb],
+                                        c["cij"][k * n:(k + 1) * n], s.nx, s.ny, s.nz, s.npad)
+                         for k in range(3)])
+    dobs = O.model_data3d(g, *_split(cp, n), s.wavelet, s.souloc, c["shotid"], s.recloc,
+                          dtype=np.float32)
+    fg = O.gradient3d(g, c["cij"], c["padb"], c["randb"], s.wavelet, s.souloc, c["shotid"],
+                      s.recloc, dobs, dtype=np.float32)
+    assert fg[0] == 0.0 and not fg[1:].any()
+
+
+def test_reference_truncates_levels():
+    g = S.small3d(nt=100).geom()
+    assert O.last_level(g) == 1 + 64 * ((100 - 2) // 64) == 65
+    assert O.last_level(g, full_steps=True) == 99

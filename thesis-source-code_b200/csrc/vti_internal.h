@@ -1,0 +1,152 @@
+// Internal declarations shared by the libvti_b200 translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "vti_b200.h"
+
+namespace vti {
+
+// Half width of the 8th-order stencil (lib/vti-fwi-3d/gpu/wave3d.h:19).
+constexpr int kHalo = 4;
+// z planes of zeros kept above and below every device volume so the z
+// stencil never needs a bounds test (the reference pads with zero planes in
+// its top/bottom kernels, kernel3d.cu:92,409).
+constexpr int kZPad = kHalo;
+// The reference pipeline advances 64 steps per block visit
+// (wave3d.h:17) and therefore runs 2 + 64*floor((nt-2)/64) time levels.
+constexpr int kRefUpdate = 64;
+
+// Recording / injection weights (wave3d.h:5-6).
+constexpr double kTwoThird = 0.6666666666;
+constexpr double kOneThird = 0.3333333333;
+
+// A device volume: x-fastest rows of `pitch` floats, ny rows per plane,
+// nz planes plus kZPad zero planes on each side. `origin` points at
+// element (0,0,0).
+struct Vol {
+  float* alloc = nullptr;
+  float* origin = nullptr;
+  size_t bytes = 0;
+};
+
+struct Dims3 {
+  int nx, ny, nz;
+  int pitch;          // floats per row (multiple of 32)
+  long long plane;    // floats per plane = pitch * ny
+  __host__ __device__ long long npoints() const { return (long long)nx * ny * nz; }
+  __host__ __device__ long long off(int x, int y, int z) const {
+    return (long long)z * plane + (long long)y * pitch + x;
+  }
+};
+
+}  // namespace vti
+
+namespace vti {
+// Kernels whose launches can be timed with CUDA events (vti_ctx_set_timing).
+enum TimedKernel { kTimedFwd3d = 0, kTimedBwd3d = 1, kTimedStep2d = 2, kNumTimed = 3 };
+}  // namespace vti
+
+struct vti_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string last_error;
+  uint64_t launches = 0;
+  int sm_count = 0;
+  // device status word written by kernels (0 = ok)
+  int* d_status = nullptr;
+  // optional per-kernel timing: event pairs recorded around timed launches
+  bool timing = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events[vti::kNumTimed];
+  std::vector<cudaEvent_t> event_pool;
+};
+
+namespace vti {
+// Brackets one launch with events on ctx->stream when timing is enabled.
+struct LaunchTimer {
+  vti_ctx* ctx;
+  int kind;
+  cudaEvent_t stop = nullptr;
+  LaunchTimer(vti_ctx* c, int k);
+  ~LaunchTimer();
+};
+}  // namespace vti
+
+namespace vti {
+
+// Sets ctx->last_error and returns the status.
+int fail(vti_ctx* ctx, int status, const std::string& msg);
+// Converts a CUDA error to a status (and message) if any.
+int cuda_check(vti_ctx* ctx, cudaError_t e, const char* what);
+
+#define VTI_CUDA(ctx, call)                                   \
+  do {                                                        \
+    cudaError_t e_ = (call);                                  \
+    if (e_ != cudaSuccess) return ::vti::cuda_check(ctx, e_, #call); \
+  } while (0)
+
+#define VTI_LAUNCHED(ctx, what)                                              \
+  do {                                                                       \
+    (ctx)->launches++;                                                       \
+    cudaError_t e_ = cudaGetLastError();                                     \
+    if (e_ != cudaSuccess) return ::vti::cuda_check(ctx, e_, what);          \
+  } while (0)
+
+int vol_alloc(vti_ctx* ctx, const Dims3& d, Vol* v);
+void vol_free(Vol* v);
+// Zero the whole allocation (data and pad planes).
+int vol_zero(vti_ctx* ctx, const Dims3& d, Vol* v);
+// Contiguous x-fastest host/device array <-> pitched volume.
+int vol_upload(vti_ctx* ctx, const Dims3& d, Vol* v, const float* src, int mem);
+int vol_download(vti_ctx* ctx, const Dims3& d, const Vol* v, float* dst, int mem);
+
+Dims3 make_dims(int nx, int ny, int nz);
+
+// -------------------------------------------------------------- kernels
+struct Damping {
+  const float* x;  // nx
+  const float* y;  // ny
+  const float* z;  // nz
+};
+
+struct PointSource {
+  int x = -1, y = -1, z = -1;  // grid indices; x < 0 disables
+  float amp = 0.f;             // added to next before the sponge
+};
+
+// One forward-form leapfrog step over the update region
+// (x,y in [4,n-4), all z): next written over prev.
+// damp == nullptr: no sponge (random-boundary pass).
+int launch_fwd3d(vti_ctx* ctx, const Dims3& d, const float* cx, const float* cz, float* px,
+                 float* pz, const float* c11, const float* c13, const float* c33,
+                 const Damping* damp, float sx, float sy, float sz, PointSource src);
+
+// Fused backward step: sigma back one level (gradient form, no sponge, +src),
+// adjoint lambda one level (forward form, sponge), zero-lag imaging into g.
+int launch_bwd3d(vti_ctx* ctx, const Dims3& d, const float* scx, const float* scz, float* spx,
+                 float* spz, const float* lcx, const float* lcz, float* lpx, float* lpz,
+                 const float* c11, const float* c13, const float* c33, float* g11, float* g13,
+                 float* g33, const Damping& damp, float dt2, float idx2, float idy2, float idz2,
+                 float sx, float sy, float sz, PointSource src);
+
+// Sparse receiver kernels. rec: device offsets (Dims3::off) per receiver.
+int launch_record(vti_ctx* ctx, float* trace, int nnt, int j, const float* cx, const float* cz,
+                  const long long* rec, int nr);
+int launch_inject_residual(vti_ctx* ctx, float* lx, float* lz, const float* res, int nnt,
+                           int i0, float f, int clamp_last, const long long* rec,
+                           const float* rec_damp, int nr, float dt2);
+int launch_seed_adjoint(vti_ctx* ctx, float* lx, float* lz, const float* res, int nnt,
+                        const long long* rec, const float* rec_damp, int nr, float dt2);
+int launch_set_point(vti_ctx* ctx, float* a, float* b, long long off, float value);
+// res <- modeled - observed (dead receivers: modeled zeroed first);
+// *acc += sum(res^2) in FP64. obs == nullptr: only zero the dead traces.
+int launch_residual(vti_ctx* ctx, float* trace, const float* obs, const unsigned char* live,
+                    int nnt, int nr, double* acc);
+int launch_boundary_merge(vti_ctx* ctx, const Dims3& d, int npad, const float* full,
+                          const float* blist, float* out);
+
+}  // namespace vti

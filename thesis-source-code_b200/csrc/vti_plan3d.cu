@@ -1,0 +1,551 @@
+// 3D plan: device-resident state of one grid and the three-pass gradient
+// (objFuncGradientCij3d_f, lib/vti-fwi-3d/gpu/objFuncGradient3d_f.cu:361-1111),
+// forward modeling (modelDataCij3d_f, modelData3d_f.cu:427) and the misfit
+// (objFuncCij3d_f, objFuncGradient3d_f.cu:1272).
+//
+// The reference streams 4-plane z-blocks between host and GPUs through a
+// 64-step temporal pipeline because its GPUs could not hold a shot. Here the
+// whole shot is resident in HBM; each time step is one fused kernel over the
+// volume, and the pipeline's observable conventions are kept:
+//   * number of levels: 2 + 64*floor((nt-2)/64) unless VTI_OPT_FULL_STEPS;
+//   * source dt2*w[it-1] into level it before the sponge; recording of level
+//     it at it == s*j, j >= 1 (objFuncGradient3d_f.cu:655-668);
+//   * pass 3: level it = nt-3-i of the source wavefield gets dt2*w[it+1],
+//     the adjoint gets the residual interpolated at it+1 (:958-1024).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "vti_internal.h"
+
+using namespace vti;
+
+struct vti3d_plan {
+  vti_ctx* ctx = nullptr;
+  vti3d_geom g{};
+  unsigned flags = 0;
+  Dims3 d{};
+  Vol cpad[3], crand[3];
+  bool have_rand = false;
+  Vol sx[2], sz[2], lx[2], lz[2];
+  Vol g11, g13, g33;
+  float* dampx = nullptr;  // nx + ny + nz floats, one allocation
+  float* dampy = nullptr;
+  float* dampz = nullptr;
+  std::vector<float> h_damp;  // host copy: x | y | z
+  std::vector<float> wavelet;
+  std::vector<float> recloc;
+  int nrec_total = 0;
+  // per-shot device scratch
+  long long* d_rec = nullptr;
+  float* d_rec_damp = nullptr;
+  unsigned char* d_live = nullptr;
+  size_t rec_cap = 0;
+  float* d_trace = nullptr;
+  size_t trace_cap = 0;
+  float* d_obs = nullptr;
+  size_t obs_cap = 0;
+  float* d_blist = nullptr;
+  size_t blist_cap = 0;
+  double* d_acc = nullptr;
+  int last_cur = 0;  // index into sx[] of the last forward level
+  bool have_model = false;
+};
+
+namespace {
+
+#define VTI_TRY(x)                 \
+  do {                             \
+    int st_ = (x);                 \
+    if (st_ != VTI_OK) return st_; \
+  } while (0)
+
+int sampling_step(const vti3d_geom& g) { return (int)std::round(g.sampling_rate / g.dt); }
+int nnt_of(const vti3d_geom& g) { return (g.nt - 1) / sampling_step(g) + 1; }
+int last_level(const vti3d_geom& g, unsigned flags) {
+  if (flags & VTI_OPT_FULL_STEPS) return g.nt - 1;
+  return 1 + kRefUpdate * ((g.nt - 2) / kRefUpdate);
+}
+long long boundary_count(const vti3d_geom& g) {
+  return (long long)g.nx * g.ny * g.nz -
+         (long long)(g.nx - 2 * g.npad) * (g.ny - 2 * g.npad) * (g.nz - 2 * g.npad);
+}
+
+// abc3d.cu:23-50, evaluated in the same float/double mix.
+float damp_profile(int i, int n, int npad) {
+  float dist;
+  if (i < npad) dist = npad - i;
+  else if (i > n - npad) dist = i - n + npad;
+  else dist = 0.f;
+  return (float)(0.95 + (1. - 0.95) * std::cos(3.14159265359 * dist / npad));
+}
+
+template <typename T>
+int ensure(vti_ctx* ctx, T** ptr, size_t* cap, size_t n) {
+  if (*ptr && *cap >= n) return VTI_OK;
+  if (*ptr) cudaFree(*ptr);
+  *ptr = nullptr;
+  *cap = 0;
+  VTI_CUDA(ctx, cudaMalloc((void**)ptr, std::max<size_t>(n, 1) * sizeof(T)));
+  *cap = n;
+  return VTI_OK;
+}
+
+struct ShotGeom {
+  int sx, sy, sz;
+  int nr, irbegin;
+  std::vector<long long> rec;
+  std::vector<float> rec_damp;
+  std::vector<unsigned char> live;
+};
+
+// Index arithmetic of objFuncGradient3d_f.cu:551-575 (float, truncation).
+int shot_geom(vti3d_plan* p, const float* souloc, int is, ShotGeom* s) {
+  const vti3d_geom& g = p->g;
+  const float* hx = p->h_damp.data();
+  const float* hy = hx + g.nx;
+  const float* hz = hy + g.ny;
+  s->nr = (int)souloc[5 * is + 3];
+  s->irbegin = (int)souloc[5 * is + 4];
+  s->sx = (int)((souloc[5 * is] - g.ox) / g.dx);
+  s->sy = (int)((souloc[5 * is + 1] - g.oy) / g.dy);
+  s->sz = (int)((souloc[5 * is + 2] - g.oz) / g.dz);
+  if (s->sx < kHalo || s->sx >= g.nx - kHalo || s->sy < kHalo || s->sy >= g.ny - kHalo ||
+      s->sz < 0 || s->sz >= g.nz)
+    return fail(p->ctx, VTI_ERR_ARG,
+                "source of shot " + std::to_string(is) +
+                    " lies outside the update region (x,y in [4,n-4), z in [0,nz))");
+  if (s->nr < 0 || s->irbegin < 0 || s->irbegin + s->nr > p->nrec_total)
+    return fail(p->ctx, VTI_ERR_ARG,
+                "receiver range of shot " + std::to_string(is) + " exceeds the receiver list");
+  s->rec.resize(s->nr);
+  s->rec_damp.resize(s->nr);
+  s->live.resize(s->nr);
+  for (int ir = 0; ir < s->nr; ++ir) {
+    const float* r = p->recloc.data() + 4 * (size_t)(ir + s->irbegin);
+    int ix = (int)((r[0] - g.ox) / g.dx);
+    int iy = (int)((r[1] - g.oy) / g.dy);
+    int iz = (int)((r[2] - g.oz) / g.dz);
+    if (ix < 0 || ix >= g.nx || iy < 0 || iy >= g.ny || iz < 0 || iz >= g.nz)
+      return fail(p->ctx, VTI_ERR_ARG,
+                  "receiver " + std::to_string(ir + s->irbegin) + " lies outside the grid");
+    s->rec[ir] = p->d.off(ix, iy, iz);
+    // The step kernel has already applied the sponge to next, so injected
+    // residuals are scaled by the same factor. Cells of the 4-wide x/y frame
+    // are never updated by the scheme; nothing is injected there.
+    bool inner = ix >= kHalo && ix < g.nx - kHalo && iy >= kHalo && iy < g.ny - kHalo;
+    s->rec_damp[ir] = inner ? (hx[ix] * hy[iy]) * hz[iz] : 0.f;
+    s->live[ir] = r[3] != 0.f;
+  }
+  return VTI_OK;
+}
+
+int upload_shot(vti3d_plan* p, const ShotGeom& s) {
+  vti_ctx* ctx = p->ctx;
+  size_t nr = std::max(s.nr, 1);
+  if (p->rec_cap < nr) {
+    if (p->d_rec) cudaFree(p->d_rec);
+    if (p->d_rec_damp) cudaFree(p->d_rec_damp);
+    if (p->d_live) cudaFree(p->d_live);
+    p->d_rec = nullptr;
+    p->d_rec_damp = nullptr;
+    p->d_live = nullptr;
+    p->rec_cap = 0;
+    VTI_CUDA(ctx, cudaMalloc((void**)&p->d_rec, nr * sizeof(long long)));
+    VTI_CUDA(ctx, cudaMalloc((void**)&p->d_rec_damp, nr * sizeof(float)));
+    VTI_CUDA(ctx, cudaMalloc((void**)&p->d_live, nr));
+    p->rec_cap = nr;
+  }
+  if (s.nr > 0) {
+    VTI_CUDA(ctx, cudaMemcpyAsync(p->d_rec, s.rec.data(), s.nr * sizeof(long long),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+    VTI_CUDA(ctx, cudaMemcpyAsync(p->d_rec_damp, s.rec_damp.data(), s.nr * sizeof(float),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+    VTI_CUDA(ctx, cudaMemcpyAsync(p->d_live, s.live.data(), s.nr, cudaMemcpyHostToDevice,
+                                  ctx->stream));
+  }
+  VTI_TRY(ensure(ctx, &p->d_trace, &p->trace_cap, (size_t)nnt_of(p->g) * nr));
+  // the host vectors are released when the caller's ShotGeom goes away
+  VTI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return VTI_OK;
+}
+
+// Forward propagation of one shot. sponge: pass 1 (pad-boundary model, sponge,
+// traces recorded into d_trace). Otherwise pass 2 (random-boundary model, no
+// sponge). On return sx[last_cur] holds level M and the other buffer M-1.
+int forward_pass(vti3d_plan* p, const ShotGeom& s, bool sponge) {
+  vti_ctx* ctx = p->ctx;
+  const vti3d_geom& g = p->g;
+  const Dims3& d = p->d;
+  const float dx2 = g.dx * g.dx, dy2 = g.dy * g.dy, dz2 = g.dz * g.dz, dt2 = g.dt * g.dt;
+  const float sxs = dt2 / dx2, sys = dt2 / dy2, szs = dt2 / dz2;
+  const int st = sampling_step(g), nnt = nnt_of(g), M = last_level(g, p->flags);
+  Vol* c = (sponge || !p->have_rand) ? p->cpad : p->crand;
+  Damping dmp{p->dampx, p->dampy, p->dampz};
+  for (int k = 0; k < 2; ++k) {
+    VTI_TRY(vol_zero(ctx, d, &p->sx[k]));
+    VTI_TRY(vol_zero(ctx, d, &p->sz[k]));
+  }
+  int A = 0, B = 1;
+  // "injecting source at time 0 to wavefields at time 1"
+  // (objFuncGradient3d_f.cu:605-608): assignment, no sponge.
+  VTI_TRY(launch_set_point(ctx, p->sx[A].origin, p->sz[A].origin, d.off(s.sx, s.sy, s.sz),
+                           dt2 * p->wavelet[0]));
+  if (sponge && s.nr > 0)
+    VTI_CUDA(ctx,
+             cudaMemsetAsync(p->d_trace, 0, (size_t)nnt * s.nr * sizeof(float), ctx->stream));
+  PointSource src;
+  src.x = s.sx;
+  src.y = s.sy;
+  src.z = s.sz;
+  for (int it = 2; it <= M; ++it) {
+    src.amp = dt2 * p->wavelet[it - 1];
+    VTI_TRY(launch_fwd3d(ctx, d, p->sx[A].origin, p->sz[A].origin, p->sx[B].origin,
+                         p->sz[B].origin, c[0].origin, c[1].origin, c[2].origin,
+                         sponge ? &dmp : nullptr, sxs, sys, szs, src));
+    std::swap(A, B);
+    if (sponge && it % st == 0) {
+      int j = it / st;
+      if (j >= 1 && j < nnt)
+        VTI_TRY(launch_record(ctx, p->d_trace, nnt, j, p->sx[A].origin, p->sz[A].origin,
+                              p->d_rec, s.nr));
+    }
+  }
+  p->last_cur = A;
+  return VTI_OK;
+}
+
+// Time-reversed source wavefield + adjoint + imaging (pass 3,
+// objFuncGradient3d_f.cu:910-1078). Expects sx[last_cur] = level M,
+// sx[other] = level M-1 from pass 2, and the residual in d_trace.
+int backward_pass(vti3d_plan* p, const ShotGeom& s) {
+  vti_ctx* ctx = p->ctx;
+  const vti3d_geom& g = p->g;
+  const Dims3& d = p->d;
+  const float dx2 = g.dx * g.dx, dy2 = g.dy * g.dy, dz2 = g.dz * g.dz, dt2 = g.dt * g.dt;
+  const float sxs = dt2 / dx2, sys = dt2 / dy2, szs = dt2 / dz2;
+  const float idx2 = 1.f / dx2, idy2 = 1.f / dy2, idz2 = 1.f / dz2;
+  const int st = sampling_step(g), nnt = nnt_of(g), M = last_level(g, p->flags);
+  Vol* c = p->have_rand ? p->crand : p->cpad;
+  Damping dmp{p->dampx, p->dampy, p->dampz};
+  // flip (objFuncGradient3d_f.cu:912-914): cur = level M-1, prev = level M
+  int SA = 1 - p->last_cur, SB = p->last_cur;
+  for (int k = 0; k < 2; ++k) {
+    VTI_TRY(vol_zero(ctx, d, &p->lx[k]));
+    VTI_TRY(vol_zero(ctx, d, &p->lz[k]));
+  }
+  int LA = 0, LB = 1;
+  VTI_TRY(launch_seed_adjoint(ctx, p->lx[LA].origin, p->lz[LA].origin, p->d_trace, nnt, p->d_rec,
+                              p->d_rec_damp, s.nr, dt2));
+  PointSource src;
+  src.x = s.sx;
+  src.y = s.sy;
+  src.z = s.sz;
+  for (int i = 0; i < M - 1; ++i) {
+    const int it = g.nt - 3 - i;
+    src.amp = dt2 * p->wavelet[it + 1];
+    VTI_TRY(launch_bwd3d(ctx, d, p->sx[SA].origin, p->sz[SA].origin, p->sx[SB].origin,
+                         p->sz[SB].origin, p->lx[LA].origin, p->lz[LA].origin, p->lx[LB].origin,
+                         p->lz[LB].origin, c[0].origin, c[1].origin, c[2].origin, p->g11.origin,
+                         p->g13.origin, p->g33.origin, dmp, dt2, idx2, idy2, idz2, sxs, sys, szs,
+                         src));
+    // residual interpolated at it+1 (injectRecord3d.cu:60-78)
+    const int ti = it + 1;
+    float f = float(ti) / float(st);
+    int i0 = (int)f;
+    int clamp = i0 >= nnt - 1;
+    f = f - i0;
+    VTI_TRY(launch_inject_residual(ctx, p->lx[LB].origin, p->lz[LB].origin, p->d_trace, nnt,
+                                   clamp ? 0 : i0, f, clamp, p->d_rec, p->d_rec_damp, s.nr, dt2));
+    std::swap(SA, SB);
+    std::swap(LA, LB);
+  }
+  return VTI_OK;
+}
+
+int check_geom(vti_ctx* ctx, const vti3d_geom* g) {
+  if (!g) return fail(ctx, VTI_ERR_ARG, "null geometry");
+  if (g->nx < 2 * kHalo + 1 || g->ny < 2 * kHalo + 1 || g->nz < 1 || g->nt < 3)
+    return fail(ctx, VTI_ERR_ARG, "grid too small (need nx,ny >= 9, nz >= 1, nt >= 3)");
+  if (g->npad < 1 || 2 * g->npad > g->nx || 2 * g->npad > g->ny || 2 * g->npad > g->nz)
+    return fail(ctx, VTI_ERR_ARG, "npad out of range (1 <= npad <= n/2)");
+  if (!(g->dx > 0 && g->dy > 0 && g->dz > 0 && g->dt > 0 && g->sampling_rate > 0))
+    return fail(ctx, VTI_ERR_ARG, "non-positive spacing, dt or sampling rate");
+  if ((int)std::round(g->sampling_rate / g->dt) < 1)
+    return fail(ctx, VTI_ERR_ARG, "sampling_rate < dt");
+  if ((long long)((g->nx + 31) & ~31) * g->ny >= (1LL << 31))
+    return fail(ctx, VTI_ERR_ARG, "plane too large");
+  return VTI_OK;
+}
+
+int get_obs(vti3d_plan* p, const ShotGeom& s, const float* dobs, int mem, const float** out) {
+  const int nnt = nnt_of(p->g);
+  const size_t n = (size_t)nnt * s.nr;
+  const float* src = dobs + (size_t)nnt * s.irbegin;
+  if (mem == VTI_MEM_DEVICE) {
+    *out = src;
+    return VTI_OK;
+  }
+  VTI_TRY(ensure(p->ctx, &p->d_obs, &p->obs_cap, n));
+  VTI_CUDA(p->ctx, cudaMemcpyAsync(p->d_obs, src, n * sizeof(float), cudaMemcpyHostToDevice,
+                                   p->ctx->stream));
+  *out = p->d_obs;
+  return VTI_OK;
+}
+
+int run_gradient(vti3d_plan* p, const float* souloc, const int* shotid, int nshot,
+                 const float* dobs, int dobs_mem, float* fgcij, int fgcij_mem, double* misfit,
+                 bool misfit_only) {
+  vti_ctx* ctx = p->ctx;
+  if (!p->have_model) return fail(ctx, VTI_ERR_ARG, "model not set");
+  if ((int)p->wavelet.size() != p->g.nt) return fail(ctx, VTI_ERR_ARG, "wavelet not set");
+  if (!souloc || (nshot > 0 && !shotid) || !dobs || nshot < 0)
+    return fail(ctx, VTI_ERR_ARG, "null pointer or negative shot count");
+  VTI_CUDA(ctx, cudaSetDevice(ctx->device));
+  const Dims3& d = p->d;
+  const int nnt = nnt_of(p->g);
+  if (!p->d_acc) VTI_CUDA(ctx, cudaMalloc((void**)&p->d_acc, sizeof(double)));
+  VTI_CUDA(ctx, cudaMemsetAsync(p->d_acc, 0, sizeof(double), ctx->stream));
+  if (!misfit_only) {
+    VTI_TRY(vol_zero(ctx, d, &p->g11));
+    VTI_TRY(vol_zero(ctx, d, &p->g13));
+    VTI_TRY(vol_zero(ctx, d, &p->g33));
+  }
+  for (int k = 0; k < nshot; ++k) {
+    ShotGeom s;
+    VTI_TRY(shot_geom(p, souloc, shotid[k], &s));
+    VTI_TRY(upload_shot(p, s));
+    VTI_TRY(forward_pass(p, s, true));
+    const float* obs = nullptr;
+    VTI_TRY(get_obs(p, s, dobs, dobs_mem, &obs));
+    VTI_TRY(launch_residual(ctx, p->d_trace, obs, p->d_live, nnt, s.nr, p->d_acc));
+    if (misfit_only) continue;
+    VTI_TRY(forward_pass(p, s, false));
+    VTI_TRY(backward_pass(p, s));
+    // keep host vectors alive until this shot's uploads are consumed
+    VTI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  double acc = 0;
+  VTI_CUDA(ctx, cudaMemcpyAsync(&acc, p->d_acc, sizeof(double), cudaMemcpyDeviceToHost,
+                                ctx->stream));
+  if (!misfit_only && fgcij) {
+    const size_t n = (size_t)d.npoints();
+    VTI_TRY(vol_download(ctx, d, &p->g11, fgcij + 1, fgcij_mem));
+    VTI_TRY(vol_download(ctx, d, &p->g13, fgcij + 1 + n, fgcij_mem));
+    VTI_TRY(vol_download(ctx, d, &p->g33, fgcij + 1 + 2 * n, fgcij_mem));
+  }
+  VTI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if ((p->flags & VTI_OPT_CHECK_FINITE) && !std::isfinite(acc))
+    return fail(ctx, VTI_ERR_NONFINITE, "misfit is not finite");
+  if (misfit) *misfit = acc / 2;
+  if (!misfit_only && fgcij) {
+    float f0 = (float)(acc / 2);
+    if (fgcij_mem == VTI_MEM_DEVICE)
+      VTI_CUDA(ctx, cudaMemcpy(fgcij, &f0, sizeof(float), cudaMemcpyHostToDevice));
+    else
+      fgcij[0] = f0;
+  }
+  return VTI_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int vti3d_plan_create(vti_ctx* ctx, const vti3d_geom* g, unsigned flags, vti3d_plan** out) {
+  if (!ctx || !out) return VTI_ERR_ARG;
+  *out = nullptr;
+  VTI_TRY(check_geom(ctx, g));
+  VTI_CUDA(ctx, cudaSetDevice(ctx->device));
+  vti3d_plan* p = new vti3d_plan();
+  p->ctx = ctx;
+  p->g = *g;
+  p->flags = flags;
+  p->d = make_dims(g->nx, g->ny, g->nz);
+  int st = VTI_OK;
+  Vol* vols[] = {&p->cpad[0], &p->cpad[1], &p->cpad[2], &p->sx[0], &p->sx[1], &p->sz[0],
+                 &p->sz[1],   &p->lx[0],   &p->lx[1],   &p->lz[0], &p->lz[1], &p->g11,
+                 &p->g13,     &p->g33};
+  for (Vol* v : vols)
+    if (st == VTI_OK) st = vol_alloc(ctx, p->d, v);
+  if (st == VTI_OK) {
+    p->h_damp.resize((size_t)g->nx + g->ny + g->nz);
+    for (int i = 0; i < g->nx; ++i) p->h_damp[i] = damp_profile(i, g->nx, g->npad);
+    for (int i = 0; i < g->ny; ++i) p->h_damp[g->nx + i] = damp_profile(i, g->ny, g->npad);
+    for (int i = 0; i < g->nz; ++i) p->h_damp[g->nx + g->ny + i] = damp_profile(i, g->nz, g->npad);
+    cudaError_t e = cudaMalloc((void**)&p->dampx, p->h_damp.size() * sizeof(float));
+    if (e == cudaSuccess)
+      e = cudaMemcpy(p->dampx, p->h_damp.data(), p->h_damp.size() * sizeof(float),
+                     cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) st = cuda_check(ctx, e, "damping tables");
+    p->dampy = p->dampx + g->nx;
+    p->dampz = p->dampy + g->ny;
+  }
+  if (st != VTI_OK) {
+    vti3d_plan_destroy(p);
+    return st;
+  }
+  *out = p;
+  return VTI_OK;
+}
+
+int vti3d_plan_destroy(vti3d_plan* p) {
+  if (!p) return VTI_OK;
+  cudaSetDevice(p->ctx->device);
+  cudaStreamSynchronize(p->ctx->stream);
+  for (int k = 0; k < 3; ++k) {
+    vol_free(&p->cpad[k]);
+    vol_free(&p->crand[k]);
+  }
+  for (int k = 0; k < 2; ++k) {
+    vol_free(&p->sx[k]);
+    vol_free(&p->sz[k]);
+    vol_free(&p->lx[k]);
+    vol_free(&p->lz[k]);
+  }
+  vol_free(&p->g11);
+  vol_free(&p->g13);
+  vol_free(&p->g33);
+  void* ptrs[] = {p->dampx, p->d_rec, p->d_rec_damp, p->d_live, p->d_trace,
+                  p->d_obs, p->d_blist, p->d_acc};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+  delete p;
+  return VTI_OK;
+}
+
+int vti3d_plan_set_model(vti3d_plan* p, const float* c11, const float* c13, const float* c33,
+                         const float* padb, const float* randb, int mem) {
+  if (!p) return VTI_ERR_ARG;
+  vti_ctx* ctx = p->ctx;
+  if (!c11 || !c13 || !c33) return fail(ctx, VTI_ERR_ARG, "null model array");
+  VTI_CUDA(ctx, cudaSetDevice(ctx->device));
+  const Dims3& d = p->d;
+  const float* cs[3] = {c11, c13, c33};
+  const long long nb = boundary_count(p->g);
+  if (randb) {
+    for (int k = 0; k < 3; ++k)
+      if (!p->crand[k].alloc) VTI_TRY(vol_alloc(ctx, d, &p->crand[k]));
+  }
+  if (padb || randb) VTI_TRY(ensure(ctx, &p->d_blist, &p->blist_cap, (size_t)nb));
+  for (int k = 0; k < 3; ++k) {
+    VTI_TRY(vol_upload(ctx, d, &p->cpad[k], cs[k], mem));
+    if (randb) {
+      VTI_CUDA(ctx, cudaMemcpyAsync(p->d_blist, randb + (size_t)k * nb, nb * sizeof(float),
+                                    mem == VTI_MEM_DEVICE ? cudaMemcpyDeviceToDevice
+                                                          : cudaMemcpyHostToDevice,
+                                    ctx->stream));
+      VTI_TRY(launch_boundary_merge(ctx, d, p->g.npad, p->cpad[k].origin, p->d_blist,
+                                    p->crand[k].origin));
+    }
+    if (padb) {
+      VTI_CUDA(ctx, cudaMemcpyAsync(p->d_blist, padb + (size_t)k * nb, nb * sizeof(float),
+                                    mem == VTI_MEM_DEVICE ? cudaMemcpyDeviceToDevice
+                                                          : cudaMemcpyHostToDevice,
+                                    ctx->stream));
+      VTI_TRY(launch_boundary_merge(ctx, d, p->g.npad, p->cpad[k].origin, p->d_blist,
+                                    p->cpad[k].origin));
+    }
+  }
+  VTI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  p->have_rand = randb != nullptr;
+  p->have_model = true;
+  return VTI_OK;
+}
+
+int vti3d_plan_set_wavelet(vti3d_plan* p, const float* wavelet, int mem) {
+  if (!p || !wavelet) return VTI_ERR_ARG;
+  p->wavelet.resize(p->g.nt);
+  if (mem == VTI_MEM_DEVICE) {
+    VTI_CUDA(p->ctx, cudaMemcpy(p->wavelet.data(), wavelet, p->g.nt * sizeof(float),
+                                cudaMemcpyDeviceToHost));
+  } else {
+    std::memcpy(p->wavelet.data(), wavelet, p->g.nt * sizeof(float));
+  }
+  return VTI_OK;
+}
+
+int vti3d_plan_set_receivers(vti3d_plan* p, const float* recloc, int nrec_total) {
+  if (!p || (!recloc && nrec_total > 0) || nrec_total < 0) return VTI_ERR_ARG;
+  p->recloc.assign(recloc, recloc + 4 * (size_t)nrec_total);
+  p->nrec_total = nrec_total;
+  return VTI_OK;
+}
+
+int vti3d_plan_model_data(vti3d_plan* p, const float* souloc, const int* shotid, int nshot,
+                          float* ddata, int mem) {
+  if (!p) return VTI_ERR_ARG;
+  vti_ctx* ctx = p->ctx;
+  if (!p->have_model) return fail(ctx, VTI_ERR_ARG, "model not set");
+  if ((int)p->wavelet.size() != p->g.nt) return fail(ctx, VTI_ERR_ARG, "wavelet not set");
+  if (!souloc || !ddata || (nshot > 0 && !shotid)) return fail(ctx, VTI_ERR_ARG, "null pointer");
+  VTI_CUDA(ctx, cudaSetDevice(ctx->device));
+  const int nnt = nnt_of(p->g);
+  for (int k = 0; k < nshot; ++k) {
+    ShotGeom s;
+    VTI_TRY(shot_geom(p, souloc, shotid[k], &s));
+    VTI_TRY(upload_shot(p, s));
+    VTI_TRY(forward_pass(p, s, true));
+    // modelData3d_f.cu:298-302: dead receivers give zero traces
+    VTI_TRY(launch_residual(ctx, p->d_trace, nullptr, p->d_live, nnt, s.nr, nullptr));
+    float* dst = ddata + (size_t)nnt * s.irbegin;
+    VTI_CUDA(ctx, cudaMemcpyAsync(dst, p->d_trace, (size_t)nnt * s.nr * sizeof(float),
+                                  mem == VTI_MEM_DEVICE ? cudaMemcpyDeviceToDevice
+                                                        : cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+    VTI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  return VTI_OK;
+}
+
+int vti3d_plan_gradient(vti3d_plan* p, const float* souloc, const int* shotid, int nshot,
+                        const float* dobs, int dobs_mem, float* fgcij, int fgcij_mem,
+                        double* misfit) {
+  if (!p) return VTI_ERR_ARG;
+  return run_gradient(p, souloc, shotid, nshot, dobs, dobs_mem, fgcij, fgcij_mem, misfit, false);
+}
+
+int vti3d_plan_objfunc(vti3d_plan* p, const float* souloc, const int* shotid, int nshot,
+                       const float* dobs, int dobs_mem, double* misfit) {
+  if (!p) return VTI_ERR_ARG;
+  return run_gradient(p, souloc, shotid, nshot, dobs, dobs_mem, nullptr, VTI_MEM_HOST, misfit,
+                      true);
+}
+
+const float* vti3d_plan_wavefield(vti3d_plan* p) {
+  return p ? p->sx[p->last_cur].origin : nullptr;
+}
+
+int vti3d_model_data_cij(vti_ctx* ctx, const vti3d_geom* g, const float* c11, const float* c13,
+                         const float* c33, const float* wavelet, const float* souloc,
+                         const int* shotid, int nshot, const float* recloc, int nrec_total,
+                         float* ddata, unsigned flags) {
+  vti3d_plan* p = nullptr;
+  VTI_TRY(vti3d_plan_create(ctx, g, flags, &p));
+  int st = vti3d_plan_set_model(p, c11, c13, c33, nullptr, nullptr, VTI_MEM_HOST);
+  if (st == VTI_OK) st = vti3d_plan_set_wavelet(p, wavelet, VTI_MEM_HOST);
+  if (st == VTI_OK) st = vti3d_plan_set_receivers(p, recloc, nrec_total);
+  if (st == VTI_OK) st = vti3d_plan_model_data(p, souloc, shotid, nshot, ddata, VTI_MEM_HOST);
+  vti3d_plan_destroy(p);
+  return st;
+}
+
+int vti3d_gradient_cij(vti_ctx* ctx, const vti3d_geom* g, const float* cij, const float* padb,
+                       const float* randb, const float* wavelet, const float* souloc,
+                       const int* shotid, int nshot, const float* recloc, int nrec_total,
+                       const float* dobs, float* fgcij, double* misfit, unsigned flags) {
+  if (!cij) return fail(ctx, VTI_ERR_ARG, "null cij");
+  vti3d_plan* p = nullptr;
+  VTI_TRY(vti3d_plan_create(ctx, g, flags, &p));
+  const size_t n = (size_t)g->nx * g->ny * g->nz;
+  int st = vti3d_plan_set_model(p, cij, cij + n, cij + 2 * n, padb, randb, VTI_MEM_HOST);
+  if (st == VTI_OK) st = vti3d_plan_set_wavelet(p, wavelet, VTI_MEM_HOST);
+  if (st == VTI_OK) st = vti3d_plan_set_receivers(p, recloc, nrec_total);
+  if (st == VTI_OK)
+    st = vti3d_plan_gradient(p, souloc, shotid, nshot, dobs, VTI_MEM_HOST, fgcij, VTI_MEM_HOST,
+                             misfit);
+  vti3d_plan_destroy(p);
+  return st;
+}
+
+}  // extern "C"

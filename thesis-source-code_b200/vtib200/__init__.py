@@ -1,0 +1,381 @@
+"""Python binding of libvti_b200.so (the C ABI declared in include/vti_b200.h).
+
+The library is loaded from this directory. There is no fallback: if the
+shared object is missing or fails to load, importing a compute entry point
+raises. Arrays are numpy float32/int32 (host) or raw device pointers
+(integers) tagged with ``MEM_DEVICE``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+_HERE = Path(__file__).resolve().parent
+LIB_PATH = _HERE / "libvti_b200.so"
+
+VTI_OK = 0
+VTI_ERR_ARG = 1
+VTI_ERR_CFL = 2
+VTI_ERR_OOM = 3
+VTI_ERR_DEVICE = 4
+VTI_ERR_TIMEOUT = 5
+VTI_ERR_NONFINITE = 6
+VTI_ERR_UNSUPPORTED = 7
+
+MEM_HOST = 0
+MEM_DEVICE = 1
+OPT_FULL_STEPS = 1
+OPT_CHECK_FINITE = 2
+
+
+class VtiError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"vti status {status}: {msg}")
+        self.status = status
+
+
+class Geom3d(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("nt", C.c_int),
+                ("npad", C.c_int), ("ox", C.c_float), ("oy", C.c_float), ("oz", C.c_float),
+                ("ot", C.c_float), ("dx", C.c_float), ("dy", C.c_float), ("dz", C.c_float),
+                ("dt", C.c_float), ("sampling_rate", C.c_float)]
+
+
+class Geom2d(C.Structure):
+    _fields_ = [("nx", C.c_int), ("nz", C.c_int), ("nt", C.c_int), ("npad", C.c_int),
+                ("dx", C.c_float), ("dz", C.c_float), ("dt", C.c_float), ("rate", C.c_float),
+                ("ot", C.c_float)]
+
+
+_lib = None
+
+F32P = C.POINTER(C.c_float)
+I32P = C.POINTER(C.c_int)
+VP = C.c_void_p
+
+
+def _signatures():
+    P = VP
+    return {
+        "vti_ctx_create": (C.c_int, [C.c_int, C.POINTER(VP)]),
+        "vti_ctx_destroy": (C.c_int, [P]),
+        "vti_status_string": (C.c_char_p, [C.c_int]),
+        "vti_ctx_last_error": (C.c_char_p, [P]),
+        "vti_ctx_stream": (VP, [P]),
+        "vti_ctx_kernel_launches": (C.c_uint64, [P]),
+        "vti_ctx_set_timing": (C.c_int, [P, C.c_int]),
+        "vti_ctx_kernel_time": (C.c_int, [P, C.c_char_p, C.POINTER(C.c_double),
+                                          C.POINTER(C.c_uint64)]),
+        "vti3d_cfl_number": (C.c_double, [P, P, P, P]),
+        "vti3d_get_boundary": (None, [P, P, C.c_int, C.c_int, C.c_int, C.c_int]),
+        "vti3d_put_boundary": (None, [P, P, C.c_int, C.c_int, C.c_int, C.c_int]),
+        "vti3d_zero_boundary": (None, [P, C.c_int, C.c_int, C.c_int, C.c_int]),
+        "vti_vepsdel_to_cij": (None, [P] * 6 + [C.c_float] * 3 + [C.c_size_t]),
+        "vti_grad_cij_to_vepsdel": (None, [P] * 9 + [C.c_float] * 3 + [C.c_size_t]),
+        "vti_dvepsdel_to_dcij": (None, [P] * 12 + [C.c_float] * 3 + [C.c_size_t]),
+        "vti_check_eps_del": (C.c_int, [P, P, C.c_float, C.c_float, C.c_size_t, P]),
+        "vti3d_plan_create": (C.c_int, [P, P, C.c_uint, C.POINTER(VP)]),
+        "vti3d_plan_destroy": (C.c_int, [P]),
+        "vti3d_plan_set_model": (C.c_int, [P, P, P, P, P, P, C.c_int]),
+        "vti3d_plan_set_wavelet": (C.c_int, [P, P, C.c_int]),
+        "vti3d_plan_set_receivers": (C.c_int, [P, P, C.c_int]),
+        "vti3d_plan_model_data": (C.c_int, [P, P, P, C.c_int, P, C.c_int]),
+        "vti3d_plan_gradient": (C.c_int, [P, P, P, C.c_int, P, C.c_int, P, C.c_int,
+                                          C.POINTER(C.c_double)]),
+        "vti3d_plan_objfunc": (C.c_int, [P, P, P, C.c_int, P, C.c_int, C.POINTER(C.c_double)]),
+        "vti3d_plan_wavefield": (VP, [P]),
+        "vti3d_model_data_cij": (C.c_int, [P, P, P, P, P, P, P, P, C.c_int, P, C.c_int, P,
+                                           C.c_uint]),
+        "vti3d_gradient_cij": (C.c_int, [P, P, P, P, P, P, P, P, C.c_int, P, C.c_int, P, P,
+                                         C.POINTER(C.c_double), C.c_uint]),
+        "vti2d_synthetic": (C.c_int, [P, P, P, P, P, P, P, C.c_int, P, C.c_int, P, P]),
+        "vti2d_modeling": (C.c_int, [P, P, P, P, P, P, C.c_int, P, P]),
+        "vti2d_init_taper": (None, [P, C.c_int, C.c_int, C.c_int]),
+    }
+
+
+def _declare(lib):
+    for name, (res, args) in _signatures().items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+
+
+def exported_symbols():
+    """Names of every C-ABI entry point this binding declares."""
+    return sorted(_signatures())
+
+
+def lib():
+    """Load (once) and return the shared library; raises if it is missing."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"{LIB_PATH} is missing: run `make -C thesis-source-code_b200` "
+                              "(or __graft_entry__.build())")
+        lib_ = C.CDLL(str(LIB_PATH))
+        _declare(lib_)
+        _lib = lib_
+    return _lib
+
+
+def _p(a):
+    """ctypes pointer of a contiguous numpy array, a raw int pointer, or None."""
+    if a is None:
+        return None
+    if isinstance(a, int):
+        return C.c_void_p(a)
+    if not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("array must be C-contiguous")
+    return C.c_void_p(a.ctypes.data)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+class Context:
+    """One CUDA device. Mirrors vti_ctx_create/destroy."""
+
+    def __init__(self, device: int = 0):
+        self._h = VP()
+        st = lib().vti_ctx_create(device, C.byref(self._h))
+        if st != VTI_OK:
+            raise VtiError(st, "vti_ctx_create failed (no CUDA device?)")
+
+    @property
+    def handle(self):
+        return self._h
+
+    def check(self, st: int):
+        if st != VTI_OK:
+            msg = lib().vti_ctx_last_error(self._h) or lib().vti_status_string(st)
+            raise VtiError(st, msg.decode() if isinstance(msg, bytes) else str(msg))
+
+    @property
+    def stream(self) -> int:
+        return lib().vti_ctx_stream(self._h) or 0
+
+    @property
+    def launches(self) -> int:
+        return int(lib().vti_ctx_kernel_launches(self._h))
+
+    def set_timing(self, enable: bool):
+        self.check(lib().vti_ctx_set_timing(self._h, 1 if enable else 0))
+
+    def kernel_time(self, kernel: str):
+        """(total device ms, launches) of a timed kernel: fwd3d, bwd3d, step2d."""
+        ms, cnt = C.c_double(0), C.c_uint64(0)
+        self.check(lib().vti_ctx_kernel_time(self._h, kernel.encode(), C.byref(ms),
+                                             C.byref(cnt)))
+        return ms.value, int(cnt.value)
+
+    def synchronize(self):
+        self.kernel_time("fwd3d")
+
+    def close(self):
+        if self._h:
+            lib().vti_ctx_destroy(self._h)
+            self._h = VP()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def geom3d(nx, ny, nz, nt, npad, dx, dy, dz, dt, sampling_rate, ox=0.0, oy=0.0, oz=0.0, ot=0.0):
+    return Geom3d(nx, ny, nz, nt, npad, ox, oy, oz, ot, dx, dy, dz, dt, sampling_rate)
+
+
+def geom2d(nx, nz, nt, npad, dx, dz, dt, rate, ot=0.0):
+    return Geom2d(nx, nz, nt, npad, dx, dz, dt, rate, ot)
+
+
+def nnt3d(g: Geom3d) -> int:
+    s = int(np.round(np.float32(g.sampling_rate) / np.float32(g.dt)))
+    return (g.nt - 1) // s + 1
+
+
+class Plan3d:
+    """Device-resident 3D plan (vti3d_plan_*)."""
+
+    def __init__(self, ctx: Context, g: Geom3d, flags: int = 0):
+        self.ctx, self.g = ctx, g
+        self._h = VP()
+        ctx.check(lib().vti3d_plan_create(ctx.handle, C.byref(g), flags, C.byref(self._h)))
+
+    def set_model(self, c11, c13, c33, padb=None, randb=None, mem=MEM_HOST):
+        if mem == MEM_HOST:
+            c11, c13, c33 = _f32(c11), _f32(c13), _f32(c33)
+            padb = None if padb is None else _f32(padb)
+            randb = None if randb is None else _f32(randb)
+            self._keep = (c11, c13, c33, padb, randb)
+        self.ctx.check(lib().vti3d_plan_set_model(self._h, _p(c11), _p(c13), _p(c33), _p(padb),
+                                                  _p(randb), mem))
+
+    def set_wavelet(self, w, mem=MEM_HOST):
+        if mem == MEM_HOST:
+            w = _f32(w)
+        self.ctx.check(lib().vti3d_plan_set_wavelet(self._h, _p(w), mem))
+
+    def set_receivers(self, recloc):
+        recloc = _f32(recloc).reshape(-1)
+        self.ctx.check(lib().vti3d_plan_set_receivers(self._h, _p(recloc), recloc.size // 4))
+
+    def model_data(self, souloc, shotid, out=None, mem=MEM_HOST, nrec_total=None):
+        souloc, shotid = _f32(souloc).reshape(-1), _i32(shotid)
+        if out is None:
+            nr = nrec_total if nrec_total is not None else int(
+                max(souloc[5 * s + 3] + souloc[5 * s + 4] for s in shotid))
+            out = np.zeros(nnt3d(self.g) * nr, dtype=np.float32)
+        self.ctx.check(lib().vti3d_plan_model_data(self._h, _p(souloc), _p(shotid), len(shotid),
+                                                   _p(out), mem))
+        return out
+
+    def gradient(self, souloc, shotid, dobs, dobs_mem=MEM_HOST, fgcij=None, fgcij_mem=MEM_HOST):
+        souloc, shotid = _f32(souloc).reshape(-1), _i32(shotid)
+        if dobs_mem == MEM_HOST:
+            dobs = _f32(dobs)
+        n = self.g.nx * self.g.ny * self.g.nz
+        if fgcij is None:
+            fgcij = np.zeros(1 + 3 * n, dtype=np.float32)
+        mis = C.c_double(0)
+        self.ctx.check(lib().vti3d_plan_gradient(self._h, _p(souloc), _p(shotid), len(shotid),
+                                                 _p(dobs), dobs_mem, _p(fgcij), fgcij_mem,
+                                                 C.byref(mis)))
+        return fgcij, mis.value
+
+    def objfunc(self, souloc, shotid, dobs, dobs_mem=MEM_HOST):
+        souloc, shotid = _f32(souloc).reshape(-1), _i32(shotid)
+        if dobs_mem == MEM_HOST:
+            dobs = _f32(dobs)
+        mis = C.c_double(0)
+        self.ctx.check(lib().vti3d_plan_objfunc(self._h, _p(souloc), _p(shotid), len(shotid),
+                                                _p(dobs), dobs_mem, C.byref(mis)))
+        return mis.value
+
+    def wavefield_ptr(self) -> int:
+        return lib().vti3d_plan_wavefield(self._h) or 0
+
+    def close(self):
+        if self._h:
+            lib().vti3d_plan_destroy(self._h)
+            self._h = VP()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------- reference-named API
+def modelDataCij3d_f(ctx, g: Geom3d, souloc, shotid, recloc, wavelet, c11, c13, c33, flags=0):
+    """modelDataCij3d_f (lib/vti-fwi-3d/gpu/modelData3d_f.cu:427): returns ddata."""
+    souloc, recloc = _f32(souloc).reshape(-1), _f32(recloc).reshape(-1)
+    shotid = _i32(shotid)
+    nrtot = recloc.size // 4
+    out = np.zeros(nnt3d(g) * nrtot, dtype=np.float32)
+    ctx.check(lib().vti3d_model_data_cij(ctx.handle, C.byref(g), _p(_f32(c11)), _p(_f32(c13)),
+                                         _p(_f32(c33)), _p(_f32(wavelet)), _p(souloc),
+                                         _p(shotid), len(shotid), _p(recloc), nrtot, _p(out),
+                                         flags))
+    return out
+
+
+def objFuncGradientCij3d_f(ctx, g: Geom3d, souloc, shotid, recloc, wavelet, cij, padb, randb,
+                           dobs, flags=0):
+    """objFuncGradientCij3d_f (objFuncGradient3d_f.cu:361): returns (fgcij, misfit64)."""
+    souloc, recloc = _f32(souloc).reshape(-1), _f32(recloc).reshape(-1)
+    shotid = _i32(shotid)
+    n = g.nx * g.ny * g.nz
+    fg = np.zeros(1 + 3 * n, dtype=np.float32)
+    mis = C.c_double(0)
+    ctx.check(lib().vti3d_gradient_cij(
+        ctx.handle, C.byref(g), _p(_f32(cij)), _p(None if padb is None else _f32(padb)),
+        _p(None if randb is None else _f32(randb)), _p(_f32(wavelet)), _p(souloc), _p(shotid),
+        len(shotid), _p(recloc), recloc.size // 4, _p(_f32(dobs)), _p(fg), C.byref(mis), flags))
+    return fg, mis.value
+
+
+def synthetic_f(ctx, g: Geom2d, c11, c13, c33, wavelet, sloc, rloc, taper):
+    """synthetic_f (lib/vti-fwi-2d/synthetic_f.cu:13): data[(it/ratio)*nr + ir]."""
+    sloc, rloc = _i32(sloc).reshape(-1), _i32(rloc).reshape(-1)
+    nr = rloc.size // 2
+    ratio = int(np.float32(g.rate) / np.float32(g.dt) + np.float32(0.5))
+    nt_neg = int(round(abs(g.ot) / g.dt))
+    rows = (g.nt - nt_neg - 1) // ratio + 1
+    out = np.zeros(rows * nr, dtype=np.float32)
+    ctx.check(lib().vti2d_synthetic(ctx.handle, C.byref(g), _p(_f32(c11)), _p(_f32(c13)),
+                                    _p(_f32(c33)), _p(_f32(wavelet)), _p(sloc), sloc.size // 4,
+                                    _p(rloc), nr, _p(_f32(taper)), _p(out)))
+    return out.reshape(rows, nr)
+
+
+def modeling_f(ctx, g: Geom2d, c11, c13, c33, wavelet, slocxz, taper):
+    """modeling_f (lib/vti-fwi-2d/modeling_f.cu:10): sigma_h snapshots."""
+    ratio = int(np.round(np.float32(g.rate) / np.float32(g.dt)))
+    nt_neg = int(round(abs(g.ot) / g.dt))
+    rows = (g.nt - 1 - nt_neg) // ratio + 1
+    nnxz = (g.nx + 2 * g.npad) * (g.nz + 2 * g.npad)
+    out = np.zeros(max(rows, 2) * nnxz, dtype=np.float32)
+    ctx.check(lib().vti2d_modeling(ctx.handle, C.byref(g), _p(_f32(c11)), _p(_f32(c13)),
+                                   _p(_f32(c33)), _p(_f32(wavelet)), int(slocxz),
+                                   _p(_f32(taper)), _p(out)))
+    return out.reshape(-1, nnxz)
+
+
+# ------------------------------------------------------------- host glue
+def get_boundary(v, nx, ny, nz, npad):
+    v = _f32(v)
+    nb = nx * ny * nz - (nx - 2 * npad) * (ny - 2 * npad) * (nz - 2 * npad)
+    out = np.empty(nb, dtype=np.float32)
+    lib().vti3d_get_boundary(_p(out), _p(v), nx, ny, nz, npad)
+    return out
+
+
+def put_boundary(b, v, nx, ny, nz, npad):
+    v = np.array(v, dtype=np.float32, copy=True)
+    lib().vti3d_put_boundary(_p(_f32(b)), _p(v), nx, ny, nz, npad)
+    return v
+
+
+def zero_boundary(v, nx, ny, nz, npad):
+    v = np.array(v, dtype=np.float32, copy=True)
+    lib().vti3d_zero_boundary(_p(v), nx, ny, nz, npad)
+    return v
+
+
+def vepsdel_to_cij(v, eps, dl, v0=1.0, eps0=1.0, del0=1.0):
+    v, eps, dl = _f32(v), _f32(eps), _f32(dl)
+    c11, c13, c33 = (np.empty_like(v) for _ in range(3))
+    lib().vti_vepsdel_to_cij(_p(c11), _p(c13), _p(c33), _p(v), _p(eps), _p(dl), v0, eps0, del0,
+                             v.size)
+    return c11, c13, c33
+
+
+def grad_cij_to_vepsdel(gc11, gc13, gc33, v, eps, dl, v0=1.0, eps0=1.0, del0=1.0):
+    args = [_f32(a) for a in (gc11, gc13, gc33, v, eps, dl)]
+    gv, ge, gd = (np.empty_like(args[0]) for _ in range(3))
+    lib().vti_grad_cij_to_vepsdel(_p(gv), _p(ge), _p(gd), *[_p(a) for a in args], v0, eps0,
+                                  del0, args[0].size)
+    return gv, ge, gd
+
+
+def cfl_number(g: Geom3d, c11, c13, c33):
+    return lib().vti3d_cfl_number(C.byref(g), _p(_f32(c11)), _p(_f32(c13)), _p(_f32(c33)))
+
+
+def init_taper2d(nx, nz, npad):
+    out = np.empty((nz + 2 * npad) * (nx + 2 * npad), dtype=np.float32)
+    lib().vti2d_init_taper(_p(out), nx, nz, npad)
+    return out
