@@ -54,6 +54,12 @@ typedef enum {
 #define VTI_OPT_FULL_STEPS 1u
 /* Check wavefields for NaN/Inf after each pass (VTI_ERR_NONFINITE). */
 #define VTI_OPT_CHECK_FINITE 2u
+/* Without VTI_OPT_FULL_STEPS the 3D time levels and the recorded trace
+ * samples follow the reference pipeline run on G GPUs (G = its GPUs.size(),
+ * default 1): 1 + 64*G*floor((nt-2)/(64*G)) levels, and the samples its
+ * record/transfer bookkeeping captures (modelData3d_f.cu:233-275; with a
+ * sampling step of 1 or 2 time steps it records only part of the trace). */
+#define VTI_OPT_REF_GPUS(g) ((((unsigned)(g)) & 0xffu) << 8)
 
 typedef struct vti_ctx vti_ctx;
 typedef struct vti3d_plan vti3d_plan;

@@ -59,8 +59,9 @@ def _i32(a):
     return np.ascontiguousarray(a, dtype=np.int32)
 
 
-def _geo3(g, full_steps=False):
-    ip = np.array([g.nx, g.ny, g.nz, g.nt, g.npad, 0 if full_steps else 1], dtype=np.int32)
+def _geo3(g, full_steps=False, ref_gpus=1):
+    ip = np.array([g.nx, g.ny, g.nz, g.nt, g.npad, 0 if full_steps else 1, ref_gpus],
+                  dtype=np.int32)
     fp = np.array([g.ox, g.oy, g.oz, g.ot, g.dx, g.dy, g.dz, g.dt, g.sampling_rate],
                   dtype=np.float32)
     return ip, fp

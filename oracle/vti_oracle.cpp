@@ -61,7 +61,7 @@ const int kNUpdate = 64;                                           // wave3d.h:1
 const int kHalf = 4;                                               // wave3d.h:19
 
 struct Geo3 {
-  int nx, ny, nz, nt, npad, ref_steps;
+  int nx, ny, nz, nt, npad, ref_steps, ref_gpus;
   float ox, oy, oz, ot, dx, dy, dz, dt, rate;
   long nxy() const { return (long)nx * ny; }
   long nxyz() const { return (long)nx * ny * nz; }
@@ -70,19 +70,63 @@ struct Geo3 {
 Geo3 unpack3(const int* ip, const float* fp) {
   Geo3 g;
   g.nx = ip[0]; g.ny = ip[1]; g.nz = ip[2]; g.nt = ip[3]; g.npad = ip[4]; g.ref_steps = ip[5];
+  g.ref_gpus = ip[6] < 1 ? 1 : ip[6];
   g.ox = fp[0]; g.oy = fp[1]; g.oz = fp[2]; g.ot = fp[3];
   g.dx = fp[4]; g.dy = fp[5]; g.dz = fp[6]; g.dt = fp[7]; g.rate = fp[8];
   return g;
 }
 
-// Last time level computed by the reference pipeline
-// (objFuncGradient3d_f.cu:538-542: it runs 2..1+64*nround).
+// Last time level computed by the reference pipeline on ref_gpus GPUs
+// (objFuncGradient3d_f.cu:538-542: it runs 2..1+NGPU*64*nround).
 int last_level(const Geo3& g) {
-  if (g.ref_steps) return 1 + kNUpdate * ((g.nt - 2) / kNUpdate);
+  if (g.ref_steps) return 1 + kNUpdate * g.ref_gpus * ((g.nt - 2) / (kNUpdate * g.ref_gpus));
   return g.nt - 1;
 }
 
 int sampling_step(float rate, float dt) { return (int)std::round(rate / dt); }
+
+// Trace samples the reference actually records: its host loop
+// (modelData3d_f.cu:179-296) records level it of the receiver block into
+// sample itdata only if it == s*itdata at the tick that block is updated,
+// and advances itdata two ticks later (:263-275). Replayed tick by tick.
+std::vector<int> record_schedule(const Geo3& g, int rec_block, int st, int nnt) {
+  std::vector<int> at(std::max(g.nt, 2), -1);
+  if (!g.ref_steps) {
+    for (int it = 2; it <= last_level(g); ++it)
+      if (it % st == 0 && it / st >= 1 && it / st < nnt) at[it] = it / st;
+    return at;
+  }
+  const int NG = g.ref_gpus, nb = g.nz / kHalf;
+  const int pipelen = NG * (kNUpdate + 3) + 3;
+  const int nround = (g.nt - 2) / (NG * kNUpdate);
+  const int roundlen = std::max(pipelen, nb);
+  const int nroundlen = nround * roundlen;
+  const int nk = (nround - 1) * roundlen + pipelen + nb - 1;
+  int itdata = 1, krecord = -2, ktransf = -2, rec_it = -1;
+  for (int k = 0; k < nk; k++) {
+    for (int gpu = 0; gpu < NG; gpu++) {
+      int kgpu = k - gpu * (kNUpdate + 3);
+      if (!(kgpu > 2 && kgpu <= kNUpdate + 1 + nroundlen)) continue;
+      for (int i = 0; i < kNUpdate; i++) {
+        int ib = (kgpu - 3 - i) % roundlen, iround = (kgpu - 3 - i) / roundlen;
+        if (ib >= 0 && ib < nb && iround >= 0 && iround < nround) {
+          int it = iround * NG * kNUpdate + gpu * kNUpdate + 2 + i;
+          if (ib == rec_block && it == st * itdata && itdata < nnt) {
+            krecord = k;
+            rec_it = it;
+          }
+        }
+      }
+    }
+    if (k - 1 == krecord && itdata < nnt) { krecord = -2; ktransf = k; }
+    if (k - 1 == ktransf && itdata < nnt) {
+      at[rec_it] = itdata;
+      itdata++;
+      ktransf = -2;
+    }
+  }
+  return at;
+}
 
 // abc3d.cu:23-50: one-dimensional sponge profile in float.
 float damp_profile(int i, int n, int npad) {
@@ -170,12 +214,19 @@ void step3d(const Geo3& g, const float* c11, const float* c13, const float* c33,
 
 struct Shot3 {
   long sidx;                 // source flat index
-  std::vector<long> ridx;    // receiver flat indices
+  std::vector<long> ridx;    // receiver read / residual-injection points
+  std::vector<long> seed;    // adjoint seeding points
+  std::vector<char> inner;   // receiver inside the x/y update region
   std::vector<char> live;    // receiver flag != 0
+  std::vector<int> rec_at;   // level -> recorded sample (-1: none)
   int irbegin, nr;
 };
 
-// objFuncGradient3d_f.cu:551-575: float arithmetic, truncation toward zero.
+// objFuncGradient3d_f.cu:545-575: float arithmetic, truncation toward zero.
+// Traces are read and residuals injected in the 4-plane block of the first
+// receiver of the survey (recBlock, recIndexBlock); the adjoint is seeded at
+// each receiver's own depth (recIndex, :922-927). Cells of the 4-wide x/y
+// frame are never updated by the scheme; no residual is injected there.
 Shot3 make_shot3(const Geo3& g, const float* souloc, const float* recloc, int is) {
   Shot3 s;
   s.nr = (int)souloc[5 * is + 3];
@@ -184,16 +235,24 @@ Shot3 make_shot3(const Geo3& g, const float* souloc, const float* recloc, int is
   int sy = (int)((souloc[5 * is + 1] - g.oy) / g.dy);
   int sz = (int)((souloc[5 * is + 2] - g.oz) / g.dz);
   s.sidx = sx + (long)sy * g.nx + (long)sz * g.nxy();
+  const int rec_block = (int)((recloc[2] - g.oz) / g.dz / kHalf);
   s.ridx.resize(s.nr);
+  s.seed.resize(s.nr);
+  s.inner.resize(s.nr);
   s.live.resize(s.nr);
   for (int ir = 0; ir < s.nr; ++ir) {
     int r = ir + s.irbegin;
     int ix = (int)((recloc[4 * r] - g.ox) / g.dx);
     int iy = (int)((recloc[4 * r + 1] - g.oy) / g.dy);
     int iz = (int)((recloc[4 * r + 2] - g.oz) / g.dz);
-    s.ridx[ir] = ix + (long)iy * g.nx + (long)iz * g.nxy();
+    int izr = g.ref_steps ? rec_block * kHalf + iz % kHalf : iz;
+    s.ridx[ir] = ix + (long)iy * g.nx + (long)izr * g.nxy();
+    s.seed[ir] = ix + (long)iy * g.nx + (long)iz * g.nxy();
+    s.inner[ir] = ix >= kHalf && ix < g.nx - kHalf && iy >= kHalf && iy < g.ny - kHalf;
     s.live[ir] = recloc[4 * r + 3] != 0.f;
   }
+  const int st = sampling_step(g.rate, g.dt);
+  s.rec_at = record_schedule(g, rec_block, st, (g.nt - 1) / st + 1);
   return s;
 }
 
@@ -226,13 +285,12 @@ void forward3d(const Geo3& g, const float* c11, const float* c13, const float* c
     pz[s.sidx] += d * (T)src;
     std::swap(cx, px);
     std::swap(cz, pz);
-    // recordData (injectRecord3d.cu:22-28) at it == s*j, j >= 1
-    if (trace && it % st == 0) {
-      int j = it / st;
-      if (j >= 1 && j < nnt)
-        for (int ir = 0; ir < s.nr; ++ir)
-          trace[j + (long)ir * nnt] =
-              (T)kTwoThird * cx[s.ridx[ir]] + (T)kOneThird * cz[s.ridx[ir]];
+    // recordData (injectRecord3d.cu:22-28) into the sample the reference's
+    // bookkeeping assigns to this level
+    if (trace && s.rec_at[it] >= 0) {
+      const int j = s.rec_at[it];
+      for (int ir = 0; ir < s.nr; ++ir)
+        trace[j + (long)ir * nnt] = (T)kTwoThird * cx[s.ridx[ir]] + (T)kOneThird * cz[s.ridx[ir]];
     }
   }
   if (trace)
@@ -316,9 +374,10 @@ void gradient3d(const Geo3& g, const float* cij_in, const float* padb, const flo
     lcx.assign(n, 0); lcz.assign(n, 0); lpx.assign(n, 0); lpz.assign(n, 0);
     // objFuncGradient3d_f.cu:922-927: adjoint seeded by assignment
     for (int ir = 0; ir < s.nr; ++ir) {
+      if (!s.inner[ir]) continue;
       T temp = (T)dt2 * res[(nnt - 1) + (long)ir * nnt];
-      lcx[s.ridx[ir]] = (T)kTwoThird * temp;
-      lcz[s.ridx[ir]] = (T)kOneThird * temp;
+      lcx[s.seed[ir]] = (T)kTwoThird * temp;
+      lcz[s.seed[ir]] = (T)kOneThird * temp;
     }
     const long sxy = s.sidx % nxy;
     const int sz = (int)(s.sidx / nxy);
@@ -337,6 +396,7 @@ void gradient3d(const Geo3& g, const float* cij_in, const float* padb, const flo
       pz[s.sidx] += (T)src;
       // residual injection before the sponge (injectRecord3d.cu:38-46)
       for (int ir = 0; ir < s.nr; ++ir) {
+        if (!s.inner[ir]) continue;
         T r = interp_residual<T>(res.data() + (long)ir * nnt, it + 1, nnt, st);
         T inj = (T)dt2 * r;
         long ri = s.ridx[ir];

@@ -23,6 +23,12 @@ def test_synthetic_matches_oracle_and_reference(ctx, name):
     assert rel_l2(d.reshape(-1), load_golden(name)["data"]) < 1e-5
 
 
+# Whole-wavefield snapshots carry more FP32 rounding than traces: the
+# reference's own snapshots of this case are 9.3e-6 from the FP64 oracle
+# (1.9e-5 at the last one), so two FP32 implementations may differ by 2x that.
+SNAP_TOL = 3e-5
+
+
 @pytest.mark.parametrize("name", K.CASES2D)
 def test_modeling_matches_oracle_and_reference(ctx, name):
     s = K.case2d(name)["s"]
@@ -30,9 +36,10 @@ def test_modeling_matches_oracle_and_reference(ctx, name):
     sxz = int(s.sloc[0] + s.sloc[1] * (s.nx + 2 * s.npad))
     w = V.modeling_f(ctx, g, s.c11, s.c13, s.c33, s.wavelet, sxz, s.taper)
     o = O.forward2d(g, s.c11, s.c13, s.c33, s.wavelet, None, None, s.taper, mode=1, slocxz=sxz)
-    assert rel_l2(w[: o.shape[0]], o) < 1e-5
+    assert rel_l2(w[: o.shape[0]], o) < SNAP_TOL
     gold = load_golden(name)
-    assert rel_l2(w[gold["snap_rows"]], gold["snaps"]) < 1e-5
+    assert np.abs(gold["snaps"]).max() > 0
+    assert rel_l2(w[gold["snap_rows"]], gold["snaps"]) < SNAP_TOL
 
 
 def test_synthetic_config_size(ctx):

@@ -143,9 +143,11 @@ int launch_seed_adjoint(vti_ctx* ctx, float* lx, float* lz, const float* res, in
                         const long long* rec, const float* rec_damp, int nr, float dt2);
 int launch_set_point(vti_ctx* ctx, float* a, float* b, long long off, float value);
 // res <- modeled - observed (dead receivers: modeled zeroed first);
-// *acc += sum(res^2) in FP64. obs == nullptr: only zero the dead traces.
+// acc[0] += sum(res^2) in FP64, reproducibly; acc must hold
+// 1 + residual_blocks(ctx) doubles. obs == nullptr: only zero dead traces.
 int launch_residual(vti_ctx* ctx, float* trace, const float* obs, const unsigned char* live,
                     int nnt, int nr, double* acc);
+int residual_blocks(vti_ctx* ctx);
 int launch_boundary_merge(vti_ctx* ctx, const Dims3& d, int npad, const float* full,
                           const float* blist, float* out);
 

@@ -476,9 +476,11 @@ __global__ void k_set_point(float* a, float* b, long long off, float value) {
   b[off] = value;
 }
 
-// Residual + FP64 misfit (objFuncGradient3d_f.cu:735-771).
+// Residual + FP64 misfit (objFuncGradient3d_f.cu:735-771). Each block writes
+// its partial sum; k_sum_partials adds them in a fixed order, so the misfit is
+// bitwise reproducible run to run.
 __global__ void k_residual(float* trace, const float* obs, const unsigned char* live, int nnt,
-                           int nr, double* acc) {
+                           int nr, double* partial) {
   long long n = (long long)nnt * nr;
   double s = 0.0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
@@ -493,7 +495,7 @@ __global__ void k_residual(float* trace, const float* obs, const unsigned char* 
     trace[i] = r;
     s += (double)(r * r);
   }
-  if (!acc) return;
+  if (!partial) return;
   for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
   __shared__ double ws[32];
   if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
@@ -501,8 +503,16 @@ __global__ void k_residual(float* trace, const float* obs, const unsigned char* 
   if (threadIdx.x < 32) {
     double v = threadIdx.x < (blockDim.x >> 5) ? ws[threadIdx.x] : 0.0;
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if (threadIdx.x == 0) atomicAdd(acc, v);
+    if (threadIdx.x == 0) partial[blockIdx.x] = v;
   }
+}
+
+// acc[0] += sum(partial[0..n)) in a fixed order (one warp).
+__global__ void k_sum_partials(const double* partial, int n, double* acc) {
+  double v = 0.0;
+  for (int i = threadIdx.x; i < n; i += 32) v += partial[i];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if (threadIdx.x == 0) acc[0] += v;
 }
 
 // putBoundary applied on the device: out = full, with the pad region replaced
@@ -640,13 +650,20 @@ int launch_set_point(vti_ctx* ctx, float* a, float* b, long long off, float valu
   return VTI_OK;
 }
 
+int residual_blocks(vti_ctx* ctx) { return ctx->sm_count * 8; }
+
 int launch_residual(vti_ctx* ctx, float* trace, const float* obs, const unsigned char* live,
                     int nnt, int nr, double* acc) {
   long long n = (long long)nnt * nr;
   if (n <= 0) return VTI_OK;
-  int blocks = (int)std::min<long long>((n + 255) / 256, (long long)ctx->sm_count * 8);
-  k_residual<<<blocks, 256, 0, ctx->stream>>>(trace, obs, live, nnt, nr, acc);
+  int blocks = (int)std::min<long long>((n + 255) / 256, (long long)residual_blocks(ctx));
+  // acc[0] is the running sum, acc[1 .. 1+residual_blocks) the partials
+  k_residual<<<blocks, 256, 0, ctx->stream>>>(trace, obs, live, nnt, nr, acc ? acc + 1 : nullptr);
   VTI_LAUNCHED(ctx, "k_residual");
+  if (acc) {
+    k_sum_partials<<<1, 32, 0, ctx->stream>>>(acc + 1, blocks, acc);
+    VTI_LAUNCHED(ctx, "k_sum_partials");
+  }
   return VTI_OK;
 }
 

@@ -62,9 +62,63 @@ namespace {
 
 int sampling_step(const vti3d_geom& g) { return (int)std::round(g.sampling_rate / g.dt); }
 int nnt_of(const vti3d_geom& g) { return (g.nt - 1) / sampling_step(g) + 1; }
+int ref_gpus(unsigned flags) {
+  int gpus = (int)((flags >> 8) & 0xffu);
+  return gpus < 1 ? 1 : gpus;
+}
+// objFuncGradient3d_f.cu:538-542: the pipeline runs nround rounds of
+// NGPU*64 updates starting at level 2.
 int last_level(const vti3d_geom& g, unsigned flags) {
   if (flags & VTI_OPT_FULL_STEPS) return g.nt - 1;
-  return 1 + kRefUpdate * ((g.nt - 2) / kRefUpdate);
+  const int per_round = kRefUpdate * ref_gpus(flags);
+  return 1 + per_round * ((g.nt - 2) / per_round);
+}
+
+// Which level is recorded into which trace sample. The reference records
+// level it into sample itdata only when, at the pipeline tick that updates
+// the receiver block at level it, it == s*itdata; itdata advances two ticks
+// after each record (device->host copy, then host store). This replays that
+// bookkeeping (modelData3d_f.cu:123-296, recording at :233-275) for a
+// pipeline of `ngpu` GPUs and returns rec_at[it] = sample index or -1.
+std::vector<int> reference_record_schedule(int nt, int nz, int rec_block, int st, int nnt,
+                                           int ngpu) {
+  const int NU = kRefUpdate;
+  const int nb = nz / kHalo;
+  const int pipelen = ngpu * (NU + 3) + 3;
+  const int nround = (nt - 2) / (ngpu * NU);
+  const int roundlen = std::max(pipelen, nb);
+  const int nroundlen = nround * roundlen;
+  const int nk = (nround - 1) * roundlen + pipelen + nb - 1;
+  std::vector<int> rec_at(std::max(nt, 2), -1);
+  int itdata = 1, krecord = -2, ktransf = -2, pending_it = -1;
+  for (int k = 0; k < nk; ++k) {
+    for (int gpu = 0; gpu < ngpu; ++gpu) {
+      const int kgpu = k - gpu * (NU + 3);
+      if (kgpu > 2 && kgpu <= NU + 1 + nroundlen) {
+        for (int i = 0; i < NU; ++i) {
+          const int ib = (kgpu - 3 - i) % roundlen;  // C++ truncating division,
+          const int iround = (kgpu - 3 - i) / roundlen;  // as in the reference
+          if (ib >= 0 && ib < nb && iround >= 0 && iround < nround) {
+            const int it = iround * ngpu * NU + gpu * NU + 2 + i;
+            if (ib == rec_block && it == st * itdata && itdata < nnt) {
+              krecord = k;
+              pending_it = it;
+            }
+          }
+        }
+      }
+    }
+    if (k - 1 == krecord && itdata < nnt) {
+      krecord = -2;
+      ktransf = k;
+    }
+    if (k - 1 == ktransf && itdata < nnt) {
+      if (pending_it >= 0 && pending_it < (int)rec_at.size()) rec_at[pending_it] = itdata;
+      itdata++;
+      ktransf = -2;
+    }
+  }
+  return rec_at;
 }
 long long boundary_count(const vti3d_geom& g) {
   return (long long)g.nx * g.ny * g.nz -
@@ -94,12 +148,17 @@ int ensure(vti_ctx* ctx, T** ptr, size_t* cap, size_t n) {
 struct ShotGeom {
   int sx, sy, sz;
   int nr, irbegin;
-  std::vector<long long> rec;
-  std::vector<float> rec_damp;
+  std::vector<long long> rec;   // recording / residual-injection points
+  std::vector<long long> seed;  // adjoint seeding points
+  std::vector<float> rec_damp;  // sponge factor at rec (0: frame cell, skipped)
   std::vector<unsigned char> live;
+  std::vector<int> rec_at;      // level -> trace sample (-1: not recorded)
 };
 
 // Index arithmetic of objFuncGradient3d_f.cu:551-575 (float, truncation).
+// In reference mode the receivers are read and injected inside the 4-plane
+// block of the first receiver of the survey (recBlock, :545, recIndexBlock
+// :568) and seeded at their own depth (recIndex, :567, :922-927).
 int shot_geom(vti3d_plan* p, const float* souloc, int is, ShotGeom* s) {
   const vti3d_geom& g = p->g;
   const float* hx = p->h_damp.data();
@@ -118,7 +177,12 @@ int shot_geom(vti3d_plan* p, const float* souloc, int is, ShotGeom* s) {
   if (s->nr < 0 || s->irbegin < 0 || s->irbegin + s->nr > p->nrec_total)
     return fail(p->ctx, VTI_ERR_ARG,
                 "receiver range of shot " + std::to_string(is) + " exceeds the receiver list");
+  const bool ref_mode = !(p->flags & VTI_OPT_FULL_STEPS);
+  const int st = sampling_step(g), nnt = nnt_of(g);
+  int rec_block = -1;
+  if (p->nrec_total > 0) rec_block = (int)((p->recloc[2] - g.oz) / g.dz / kHalo);
   s->rec.resize(s->nr);
+  s->seed.resize(s->nr);
   s->rec_damp.resize(s->nr);
   s->live.resize(s->nr);
   for (int ir = 0; ir < s->nr; ++ir) {
@@ -126,16 +190,27 @@ int shot_geom(vti3d_plan* p, const float* souloc, int is, ShotGeom* s) {
     int ix = (int)((r[0] - g.ox) / g.dx);
     int iy = (int)((r[1] - g.oy) / g.dy);
     int iz = (int)((r[2] - g.oz) / g.dz);
-    if (ix < 0 || ix >= g.nx || iy < 0 || iy >= g.ny || iz < 0 || iz >= g.nz)
+    int izr = ref_mode ? rec_block * kHalo + iz % kHalo : iz;
+    if (ix < 0 || ix >= g.nx || iy < 0 || iy >= g.ny || iz < 0 || iz >= g.nz || izr < 0 ||
+        izr >= g.nz)
       return fail(p->ctx, VTI_ERR_ARG,
                   "receiver " + std::to_string(ir + s->irbegin) + " lies outside the grid");
-    s->rec[ir] = p->d.off(ix, iy, iz);
+    s->rec[ir] = p->d.off(ix, iy, izr);
+    s->seed[ir] = p->d.off(ix, iy, iz);
     // The step kernel has already applied the sponge to next, so injected
     // residuals are scaled by the same factor. Cells of the 4-wide x/y frame
     // are never updated by the scheme; nothing is injected there.
     bool inner = ix >= kHalo && ix < g.nx - kHalo && iy >= kHalo && iy < g.ny - kHalo;
-    s->rec_damp[ir] = inner ? (hx[ix] * hy[iy]) * hz[iz] : 0.f;
+    s->rec_damp[ir] = inner ? (hx[ix] * hy[iy]) * hz[izr] : 0.f;
     s->live[ir] = r[3] != 0.f;
+  }
+  const int M = last_level(g, p->flags);
+  if (ref_mode) {
+    s->rec_at = reference_record_schedule(g.nt, g.nz, rec_block, st, nnt, ref_gpus(p->flags));
+  } else {
+    s->rec_at.assign(std::max(g.nt, 2), -1);
+    for (int it = 2; it <= M; ++it)
+      if (it % st == 0 && it / st >= 1 && it / st < nnt) s->rec_at[it] = it / st;
   }
   return VTI_OK;
 }
@@ -151,7 +226,8 @@ int upload_shot(vti3d_plan* p, const ShotGeom& s) {
     p->d_rec_damp = nullptr;
     p->d_live = nullptr;
     p->rec_cap = 0;
-    VTI_CUDA(ctx, cudaMalloc((void**)&p->d_rec, nr * sizeof(long long)));
+    // recording offsets [0, nr), seeding offsets [nr, 2nr)
+    VTI_CUDA(ctx, cudaMalloc((void**)&p->d_rec, 2 * nr * sizeof(long long)));
     VTI_CUDA(ctx, cudaMalloc((void**)&p->d_rec_damp, nr * sizeof(float)));
     VTI_CUDA(ctx, cudaMalloc((void**)&p->d_live, nr));
     p->rec_cap = nr;
@@ -159,6 +235,8 @@ int upload_shot(vti3d_plan* p, const ShotGeom& s) {
   if (s.nr > 0) {
     VTI_CUDA(ctx, cudaMemcpyAsync(p->d_rec, s.rec.data(), s.nr * sizeof(long long),
                                   cudaMemcpyHostToDevice, ctx->stream));
+    VTI_CUDA(ctx, cudaMemcpyAsync(p->d_rec + p->rec_cap, s.seed.data(),
+                                  s.nr * sizeof(long long), cudaMemcpyHostToDevice, ctx->stream));
     VTI_CUDA(ctx, cudaMemcpyAsync(p->d_rec_damp, s.rec_damp.data(), s.nr * sizeof(float),
                                   cudaMemcpyHostToDevice, ctx->stream));
     VTI_CUDA(ctx, cudaMemcpyAsync(p->d_live, s.live.data(), s.nr, cudaMemcpyHostToDevice,
@@ -179,7 +257,7 @@ int forward_pass(vti3d_plan* p, const ShotGeom& s, bool sponge) {
   const Dims3& d = p->d;
   const float dx2 = g.dx * g.dx, dy2 = g.dy * g.dy, dz2 = g.dz * g.dz, dt2 = g.dt * g.dt;
   const float sxs = dt2 / dx2, sys = dt2 / dy2, szs = dt2 / dz2;
-  const int st = sampling_step(g), nnt = nnt_of(g), M = last_level(g, p->flags);
+  const int nnt = nnt_of(g), M = last_level(g, p->flags);
   Vol* c = (sponge || !p->have_rand) ? p->cpad : p->crand;
   Damping dmp{p->dampx, p->dampy, p->dampz};
   for (int k = 0; k < 2; ++k) {
@@ -204,12 +282,9 @@ int forward_pass(vti3d_plan* p, const ShotGeom& s, bool sponge) {
                          p->sz[B].origin, c[0].origin, c[1].origin, c[2].origin,
                          sponge ? &dmp : nullptr, sxs, sys, szs, src));
     std::swap(A, B);
-    if (sponge && it % st == 0) {
-      int j = it / st;
-      if (j >= 1 && j < nnt)
-        VTI_TRY(launch_record(ctx, p->d_trace, nnt, j, p->sx[A].origin, p->sz[A].origin,
-                              p->d_rec, s.nr));
-    }
+    if (sponge && it < (int)s.rec_at.size() && s.rec_at[it] >= 0)
+      VTI_TRY(launch_record(ctx, p->d_trace, nnt, s.rec_at[it], p->sx[A].origin,
+                            p->sz[A].origin, p->d_rec, s.nr));
   }
   p->last_cur = A;
   return VTI_OK;
@@ -235,8 +310,8 @@ int backward_pass(vti3d_plan* p, const ShotGeom& s) {
     VTI_TRY(vol_zero(ctx, d, &p->lz[k]));
   }
   int LA = 0, LB = 1;
-  VTI_TRY(launch_seed_adjoint(ctx, p->lx[LA].origin, p->lz[LA].origin, p->d_trace, nnt, p->d_rec,
-                              p->d_rec_damp, s.nr, dt2));
+  VTI_TRY(launch_seed_adjoint(ctx, p->lx[LA].origin, p->lz[LA].origin, p->d_trace, nnt,
+                              p->d_rec + p->rec_cap, p->d_rec_damp, s.nr, dt2));
   PointSource src;
   src.x = s.sx;
   src.y = s.sy;
@@ -304,7 +379,8 @@ int run_gradient(vti3d_plan* p, const float* souloc, const int* shotid, int nsho
   VTI_CUDA(ctx, cudaSetDevice(ctx->device));
   const Dims3& d = p->d;
   const int nnt = nnt_of(p->g);
-  if (!p->d_acc) VTI_CUDA(ctx, cudaMalloc((void**)&p->d_acc, sizeof(double)));
+  if (!p->d_acc)
+    VTI_CUDA(ctx, cudaMalloc((void**)&p->d_acc, (1 + residual_blocks(ctx)) * sizeof(double)));
   VTI_CUDA(ctx, cudaMemsetAsync(p->d_acc, 0, sizeof(double), ctx->stream));
   if (!misfit_only) {
     VTI_TRY(vol_zero(ctx, d, &p->g11));

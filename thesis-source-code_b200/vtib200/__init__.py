@@ -8,7 +8,7 @@ raises. Arrays are numpy float32/int32 (host) or raw device pointers
 from __future__ import annotations
 
 import ctypes as C
-import os
+import weakref
 from pathlib import Path
 
 import numpy as np
@@ -146,6 +146,7 @@ class Context:
 
     def __init__(self, device: int = 0):
         self._h = VP()
+        self._plans = weakref.WeakSet()  # plans must be destroyed before the context
         st = lib().vti_ctx_create(device, C.byref(self._h))
         if st != VTI_OK:
             raise VtiError(st, "vti_ctx_create failed (no CUDA device?)")
@@ -182,6 +183,8 @@ class Context:
 
     def close(self):
         if self._h:
+            for p in list(self._plans):
+                p.close()
             lib().vti_ctx_destroy(self._h)
             self._h = VP()
 
@@ -212,6 +215,7 @@ class Plan3d:
         self.ctx, self.g = ctx, g
         self._h = VP()
         ctx.check(lib().vti3d_plan_create(ctx.handle, C.byref(g), flags, C.byref(self._h)))
+        ctx._plans.add(self)
 
     def set_model(self, c11, c13, c33, padb=None, randb=None, mem=MEM_HOST):
         if mem == MEM_HOST:
