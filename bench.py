@@ -42,6 +42,10 @@ CONFIGS = {
     "small": dict(nx=128, ny=128, nz=96, nt=402, npad=16, d=12.5, dt=1e-3, rate=4e-3,
                   freq=12.0, rec_step=2, rec_start=0, rec_depth=25.0, src_depth=25.0,
                   smooth_m=100.0),
+    # profiling case: every volume (34 MB) x 14 inputs exceeds the 126 MB L2
+    "mid": dict(nx=256, ny=256, nz=128, nt=130, npad=24, d=12.5, dt=1e-3, rate=4e-3,
+                freq=12.0, rec_step=2, rec_start=0, rec_depth=25.0, src_depth=25.0,
+                smooth_m=100.0),
 }
 BWD_BYTES_PER_POINT = 84  # 14 reads + 7 writes of FP32 per point (fused backward)
 FWD_BYTES_PER_POINT = 36  # 7 reads + 2 writes

@@ -149,8 +149,11 @@ int vti3d_plan_gradient(vti3d_plan* plan, const float* souloc, const int* shotid
 /* Misfit only (objFuncCij3d_f, objFuncGradient3d_f.cu:1272). */
 int vti3d_plan_objfunc(vti3d_plan* plan, const float* souloc, const int* shotid, int nshot,
                        const float* dobs, int dobs_mem, double* misfit);
-/* Device pointer of the last forward wavefield sigma_x (nxyz floats). */
+/* Device pointer of the last forward wavefield sigma_x (pitched volume). */
 const float* vti3d_plan_wavefield(vti3d_plan* plan);
+/* Copies the last forward level of sigma_x (the "wavefield" output of
+ * modelData3d_f.cu:324 / modeling3d_f.cu:266) into nxyz contiguous floats. */
+int vti3d_plan_get_wavefield(vti3d_plan* plan, float* out, int mem);
 
 /* One-call host-buffer forms (what the drop-in shim calls). */
 int vti3d_model_data_cij(vti_ctx* ctx, const vti3d_geom* g, const float* c11, const float* c13,
@@ -162,6 +165,19 @@ int vti3d_gradient_cij(vti_ctx* ctx, const vti3d_geom* g, const float* cij, cons
                        const int* shotid, int nshot, const float* recloc, int nrec_total,
                        const float* dobs, float* fgcij, double* misfit, unsigned flags);
 
+/* objFuncGradientVEpsDel (objFuncGradient3d_f.cu:249-305): gradient of the
+ * L2 misfit with respect to v, eps, del (nxyz each). padboundary_v /
+ * randboundary_v are the velocity pad-region lists (nb each); the boundary
+ * lists of eps/del are taken from the model. The gradient is zero in the pad
+ * and in the nwbottom = (wbottom-oz)/dz+1-npad planes below it; *misfit gets
+ * the float misfit/2 as a double (the reference returns fgcij[0]). */
+int vti3d_gradient_vepsdel(vti_ctx* ctx, const vti3d_geom* g, const float* v, const float* eps,
+                           const float* del, const float* padboundary_v,
+                           const float* randboundary_v, float v0, float eps0, float wbottom,
+                           const float* wavelet, const float* souloc, const int* shotid,
+                           int nshot, const float* recloc, int nrec_total, const float* dobs,
+                           float* gv, float* geps, float* gdel, double* misfit, unsigned flags);
+
 /* ------------------------------------------------------------------- 2D */
 /* synthetic_f (lib/vti-fwi-2d/synthetic_f.cu:13): data[(it/ratio)*nr + ir]. */
 int vti2d_synthetic(vti_ctx* ctx, const vti2d_geom* g, const float* c11, const float* c13,
@@ -171,6 +187,19 @@ int vti2d_synthetic(vti_ctx* ctx, const vti2d_geom* g, const float* c11, const f
 int vti2d_modeling(vti_ctx* ctx, const vti2d_geom* g, const float* c11, const float* c13,
                    const float* c33, const float* wavelet, int slocxz, const float* taper,
                    float* wavefield);
+/* objFuncGradient_f (lib/vti-fwi-2d/objFuncGradient_f.cu:15): gradient of the
+ * L2 misfit w.r.t. c11, c13, c33 (arrays (nx+2npad)*(nz+2npad)) for ns shots;
+ * observed data as synthetic_f writes them; *misfit = 0.5 * sum(res^2). */
+int vti2d_gradient(vti_ctx* ctx, const vti2d_geom* g, float* gc11, float* gc13, float* gc33,
+                   const float* data, const float* c11, const float* c13, const float* c33,
+                   const float* wavelet, const int* sloc, int ns, const int* rloc, int nr,
+                   const float* taper, double* misfit);
+/* GNhessian_f (lib/vti-fwi-2d/hessian_f.cu:575): Gauss-Newton Hessian times
+ * the model perturbation (dc11, dc13, dc33). */
+int vti2d_gn_hessian(vti_ctx* ctx, const vti2d_geom* g, float* gc11, float* gc13, float* gc33,
+                     const float* c11, const float* c13, const float* c33, const float* dc11,
+                     const float* dc13, const float* dc33, const float* wavelet, const int* sloc,
+                     int ns, const int* rloc, int nr, const float* taper);
 /* 2D taper of lib/vti-fwi-2d/init.cpp:70-89 ((nx+2npad)*(nz+2npad) floats). */
 void vti2d_init_taper(float* taper, int nx, int nz, int npad);
 

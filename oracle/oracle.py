@@ -160,3 +160,26 @@ def time_backward_f32(g, c11, c13, c33, nsteps):
     scratch = np.zeros(11 * n, dtype=np.float32)
     return lib().orc3d_time_backward_f32(_p(ip), _p(fp), _p(_f32(c11)), _p(_f32(c13)),
                                          _p(_f32(c33)), nsteps, _p(scratch))
+
+
+def gradient2d(g, c11, c13, c33, wavelet, sloc, rloc, taper, data=None, dc=None,
+               dtype=np.float64):
+    """objFuncGradient_f (dc None) or GNhessian_f (dc = (dc11, dc13, dc33))
+    restated; returns (gc11, gc13, gc33, misfit/2)."""
+    L = lib()
+    suf = "f64" if dtype == np.float64 else "f32"
+    f = getattr(L, f"orc2d_gradient_{suf}")
+    f.argtypes = [VP] * 10 + [C.c_int, VP, C.c_int, VP, VP, VP, VP, VP, C.c_int]
+    f.restype = C.c_double
+    ip = np.array([g.nx, g.nz, g.nt, g.npad], dtype=np.int32)
+    fp = np.array([g.dx, g.dz, g.dt, g.rate, g.ot], dtype=np.float32)
+    n = (g.nx + 2 * g.npad) * (g.nz + 2 * g.npad)
+    out = [np.zeros(n, dtype=dtype) for _ in range(3)]
+    sloc, rloc = _i32(sloc).reshape(-1), _i32(rloc).reshape(-1)
+    born = dc is not None
+    d11, d13, d33 = (None, None, None) if not born else tuple(_f32(x) for x in dc)
+    dat = None if data is None else _f32(data)
+    mis = f(_p(ip), _p(fp), _p(_f32(c11)), _p(_f32(c13)), _p(_f32(c33)), _p(d11), _p(d13),
+            _p(d33), _p(_f32(wavelet)), _p(sloc), sloc.size // 4, _p(rloc), rloc.size // 2,
+            _p(_f32(taper)), _p(dat), _p(out[0]), _p(out[1]), _p(out[2]), 1 if born else 0)
+    return out[0], out[1], out[2], mis

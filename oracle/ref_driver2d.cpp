@@ -20,6 +20,17 @@ void synthetic_f(float* d, const float* c11, const float* c13, const float* c33,
 void modeling_f(float* d, const float* c11, const float* c13, const float* c33,
                 const float* wavelet, int slocxz, const float* taper, int nx, int nz, int nt,
                 int npad, float dx, float dz, float dt, float rate, float ot);
+// wave.h:12 and wave.h:38
+float objFuncGradient_f(float* gc11, float* gc13, float* gc33, const float* data,
+                        const float* c11, const float* c13, const float* c33, const float* wavelet,
+                        const int* sloc, int ns, const int* rloc, int nr, const float* taper,
+                        int nx, int nz, int nt, int npad, float dx, float dz, float dt, float rate,
+                        float ot);
+void GNhessian_f(float* gc11, float* gc13, float* gc33, const float* data, const float* c11,
+                 const float* c13, const float* c33, const float* dc11, const float* dc13,
+                 const float* dc33, const float* wavelet, const int* sloc, int ns, const int* rloc,
+                 int nr, const float* taper, int nx, int nz, int nt, int npad, float dx, float dz,
+                 float dt, float rate, float ot);
 
 template <typename T>
 static std::vector<T> load(const std::string& path, size_t n) {
@@ -75,6 +86,30 @@ int main(int argc, char** argv) {
     modeling_f(w.data(), c11.data(), c13.data(), c33.data(), wavelet.data(), slocxz, taper.data(),
                nx, nz, nt, npad, dx, dz, dt, rate, ot);
     save(dir + "/ref_wavefield.bin", w.data(), w.size());
+  } else if (mode == "grad" || mode == "gnhess") {
+    // <dir>/data.bin: observed traces (grad); <dir>/dc{11,13,33}.bin (gnhess)
+    auto rloc = load<int>(dir + "/rloc.bin", 2 * (size_t)nr);
+    const int ratio = (int)(rate / dt + 0.5f);
+    const int ntneg = (int)(ot < 0 ? (-ot / dt + 0.5f) : 0);
+    const size_t rows = (nt - ntneg - 1) / ratio + 1;
+    std::vector<float> g(3 * nnxz + 1, 0.f);
+    if (mode == "grad") {
+      auto data = load<float>(dir + "/data.bin", rows * nr);
+      g[3 * nnxz] = objFuncGradient_f(g.data(), g.data() + nnxz, g.data() + 2 * nnxz,
+                                      data.data(), c11.data(), c13.data(), c33.data(),
+                                      wavelet.data(), sloc.data(), ns, rloc.data(), nr,
+                                      taper.data(), nx, nz, nt, npad, dx, dz, dt, rate, ot);
+    } else {
+      auto d11 = load<float>(dir + "/dc11.bin", nnxz);
+      auto d13 = load<float>(dir + "/dc13.bin", nnxz);
+      auto d33 = load<float>(dir + "/dc33.bin", nnxz);
+      std::vector<float> unused(rows * nr, 0.f);
+      GNhessian_f(g.data(), g.data() + nnxz, g.data() + 2 * nnxz, unused.data(), c11.data(),
+                  c13.data(), c33.data(), d11.data(), d13.data(), d33.data(), wavelet.data(),
+                  sloc.data(), ns, rloc.data(), nr, taper.data(), nx, nz, nt, npad, dx, dz, dt,
+                  rate, ot);
+    }
+    save(dir + "/ref_" + mode + ".bin", g.data(), g.size());
   } else {
     return 2;
   }

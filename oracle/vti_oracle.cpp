@@ -43,6 +43,7 @@
 #include <cstring>
 #include <vector>
 #include <algorithm>
+#include <map>
 #include <omp.h>
 
 namespace {
@@ -503,6 +504,283 @@ void forward2d(const Geo2& g, const float* c11, const float* c13, const float* c
   }
 }
 
+// --------------------------------------------- 2D gradient and GN H*v ------
+// D kernel (kernels.cu:345-387): tp = Dxx p / dx2, tq = Dzz q / dz2 on the
+// interior, zero elsewhere.
+template <typename T>
+void dop2d(const Geo2& g, const T* p, const T* q, T* tp, T* tq) {
+  const long nnx = g.nnx(), nnz = g.nnz();
+  const float dx2 = g.dx * g.dx, dz2 = g.dz * g.dz;
+  const T C[5] = {(T)k2C0, (T)k2C1, (T)k2C2, (T)k2C3, (T)k2C4};
+  std::fill(tp, tp + nnx * nnz, (T)0);
+  std::fill(tq, tq + nnx * nnz, (T)0);
+#pragma omp parallel for schedule(static)
+  for (long iz = kHalf; iz < nnz - kHalf; ++iz)
+    for (long ix = kHalf; ix < nnx - kHalf; ++ix) {
+      long i = ix + iz * nnx;
+      T a = C[0] * p[i], b = C[0] * q[i];
+      for (int k = 1; k <= 4; ++k) {
+        a += C[k] * (p[i - k] + p[i + k]);
+        b += C[k] * (q[i - k * nnx] + q[i + k * nnx]);
+      }
+      tp[i] = a / (T)dx2;
+      tq[i] = b / (T)dz2;
+    }
+}
+
+// One adjoint level on the interior. exact: backwardDC (kernels.cu:104-148),
+// p1 <- 2p0 + dt2 * D(C p0) - p1; otherwise forwardCD (kernels.cu:452-498).
+template <typename T>
+void adj2d(const Geo2& g, const float* c11, const float* c13, const float* c33, const T* p0,
+           const T* q0, T* p1, T* q1, bool exact) {
+  const long nnx = g.nnx(), nnz = g.nnz(), n = nnx * nnz;
+  const float dx2 = g.dx * g.dx, dz2 = g.dz * g.dz, dt2 = g.dt * g.dt;
+  const T C[5] = {(T)k2C0, (T)k2C1, (T)k2C2, (T)k2C3, (T)k2C4};
+  std::vector<T> a(n), b(n);
+  if (exact) {
+    for (long i = 0; i < n; ++i) {
+      a[i] = (T)c11[i] * p0[i] + (T)c13[i] * q0[i];
+      b[i] = (T)c13[i] * p0[i] + (T)c33[i] * q0[i];
+    }
+  }
+#pragma omp parallel for schedule(static)
+  for (long iz = kHalf; iz < nnz - kHalf; ++iz)
+    for (long ix = kHalf; ix < nnx - kHalf; ++ix) {
+      long i = ix + iz * nnx;
+      const T* u = exact ? a.data() : p0;
+      const T* w = exact ? b.data() : q0;
+      T tp = C[0] * u[i], tq = C[0] * w[i];
+      for (int k = 1; k <= 4; ++k) {
+        tp += C[k] * (u[i - k] + u[i + k]);
+        tq += C[k] * (w[i - k * nnx] + w[i + k * nnx]);
+      }
+      tp /= (T)dx2;
+      tq /= (T)dz2;
+      if (exact) {
+        p1[i] = 2 * p0[i] + (T)dt2 * tp - p1[i];
+        q1[i] = 2 * q0[i] + (T)dt2 * tq - q1[i];
+      } else {
+        p1[i] = 2 * p0[i] + (T)dt2 * ((T)c11[i] * tp + (T)c13[i] * tq) - p1[i];
+        q1[i] = 2 * q0[i] + (T)dt2 * ((T)c13[i] * tp + (T)c33[i] * tq) - q1[i];
+      }
+    }
+}
+
+// Which stored D(sigma) levels each backward imaging step of the 2D gradient
+// and Gauss-Newton product reads. The reference moves checkpoints through
+// three device buffers (Dpq, Dpqa, Dpqb), two pinned host buffers and a host
+// array Dp[] (objFuncGradient_f.cu:168-202 forward, :240-292 backward;
+// hessian_f.cu mirrors it). This replays those copies with labels: label t
+// means D(v_t), -1 a zero buffer. Entry 0 is the imaging of lambda(nt-1)
+// before the loop; entry 1+j the step it = nt-3-j.
+// None of these buffers is cleared between shots (only at allocation), so a
+// shot can image against checkpoints left by the previous shot on the same
+// GPU: labels therefore carry the shot, label = shot*(nt+1) + t.
+struct Pair {
+  long a, b;  // labels of Dp0 (d_Dpqa) and Dp1 (d_Dpq)
+  float f;    // weight of b
+};
+struct CkState {
+  long dq = -1, da = -1, db = -1, ha = -1, hb = -1;
+  std::vector<long> Dp;
+};
+std::vector<Pair> checkpoint_shot(CkState& S, int shot, int nt, int r) {
+  const int nnt = (nt - 1) / r + 1;
+  auto L = [&](int t) { return (long)shot * (nt + 1) + t; };
+  if (S.Dp.empty()) S.Dp.assign(std::max(nnt, 1), -1);
+  S.dq = L(1);  // D(v_1) computed at the start of every shot
+  for (int it = 2; it < nt; ++it) {
+    S.dq = L(it);
+    if (it % r == 0) {
+      if (it != nt - 1) S.da = S.dq;
+      if (it > r && it / r - 1 < nnt) S.Dp[it / r - 1] = S.ha;
+    }
+    if (it % r == 1 && it != nt - r) S.ha = S.da;
+  }
+  std::vector<Pair> out;
+  if (nnt - 3 >= 0) S.hb = S.Dp[nnt - 3];
+  {
+    float f = (nt - 2.) / r;
+    int i1 = (int)f;
+    out.push_back({S.da, S.dq, f - i1});
+  }
+  for (int it = nt - 3; it >= 0; --it) {
+    if (it % r == 0) {
+      std::swap(S.ha, S.hb);
+      S.db = S.ha;
+      if (it >= 2 * r) S.hb = S.Dp[it / r - 2];
+    }
+    if ((it + 1) % r == 0) {
+      long t = S.db;
+      S.db = S.dq;
+      S.dq = S.da;
+      S.da = t;
+    }
+    float f = (float)it / r;
+    int i1 = (int)f;
+    out.push_back({S.da, S.dq, f - i1});
+  }
+  return out;
+}
+std::vector<Pair> checkpoint_schedule(int nt, int r) {
+  CkState S;
+  return checkpoint_shot(S, 0, nt, r);
+}
+
+// gradientCrossCor (kernels.cu:438-450)
+template <typename T>
+void image2d(const Geo2& g, const T* ap, const T* aq, const T* Dp0, const T* Dq0, const T* Dp1,
+             const T* Dq1, float f, T* g11, T* g13, T* g33) {
+  const long nnx = g.nnx(), nnz = g.nnz();
+  for (long iz = kHalf; iz < nnz - kHalf; ++iz)
+    for (long ix = kHalf; ix < nnx - kHalf; ++ix) {
+      long i = ix + iz * nnx;
+      T Dp = (1 - (T)f) * (Dp0 ? Dp0[i] : 0) + (T)f * (Dp1 ? Dp1[i] : 0);
+      T Dq = (1 - (T)f) * (Dq0 ? Dq0[i] : 0) + (T)f * (Dq1 ? Dq1[i] : 0);
+      g11[i] += ap[i] * Dp;
+      g13[i] += ap[i] * Dq + aq[i] * Dp;
+      g33[i] += aq[i] * Dq;
+    }
+}
+
+// objFuncGradient_f (objFuncGradient_f.cu:15-371) when born == false;
+// GNhessian_f (hessian_f.cu:575-1010) when born == true (dc = model
+// perturbation, the Born data replace the residual, the adjoint uses the
+// forward operator). Returns 0.5 * sum of squared residuals (gradient).
+template <typename T>
+double grad2d(const Geo2& g, const float* c11, const float* c13, const float* c33,
+              const float* dc11, const float* dc13, const float* dc33, const float* wavelet,
+              const int* sloc, int ns, const int* rloc, int nr_total, const float* taper,
+              const float* data, T* g11, T* g13, T* g33, bool born) {
+  const long nnx = g.nnx(), nnxz = nnx * g.nnz();
+  const float dt = g.dt, dt2 = dt * dt;
+  const int ratio = (int)(g.rate / dt + 0.5f);
+  const int ntNeg = (int)std::round(std::fabs(g.ot) / dt);
+  const int nnt_data = (g.nt - ntNeg - 1) / ratio + 1;
+  std::fill(g11, g11 + nnxz, (T)0);
+  std::fill(g13, g13 + nnxz, (T)0);
+  std::fill(g33, g33 + nnxz, (T)0);
+  // checkpoint pairing of every shot (state carried from shot to shot)
+  std::vector<std::vector<Pair>> sched(ns);
+  {
+    CkState S;
+    for (int is = 0; is < ns; ++is) sched[is] = checkpoint_shot(S, is, g.nt, ratio);
+  }
+  std::map<long, std::pair<std::vector<T>, std::vector<T>>> ck;  // label -> (Dp, Dq)
+  for (const auto& v : sched)
+    for (const Pair& p : v) {
+      if (p.a >= 0) ck[p.a];
+      if (p.b >= 0) ck[p.b];
+    }
+  auto keep = [&](int is, int t, const std::vector<T>& a, const std::vector<T>& b) {
+    auto it = ck.find((long)is * (g.nt + 1) + t);
+    if (it != ck.end()) it->second = {a, b};
+  };
+  double objfunc = 0;
+  // the Born D buffer (d_Ddpq) is zeroed once, not per shot (hessian_f.cu:647-648)
+  std::vector<T> dtp(nnxz, 0), dtq(nnxz, 0);
+  for (int is = 0; is < ns; ++is) {
+    const long sxz = sloc[4 * is] + (long)sloc[4 * is + 1] * nnx;
+    const int nri = sloc[4 * is + 2], ir0 = sloc[4 * is + 3];
+    std::vector<long> ridx(nri);
+    for (int ir = 0; ir < nri; ++ir)
+      ridx[ir] = rloc[2 * (ir0 + ir)] + (long)rloc[2 * (ir0 + ir) + 1] * nnx;
+    std::vector<T> p0(nnxz, 0), q0(nnxz, 0), p1(nnxz, 0), q1(nnxz, 0);
+    std::vector<T> dp0(nnxz, 0), dq0(nnxz, 0), dp1(nnxz, 0), dq1(nnxz, 0);
+    std::vector<T> tp(nnxz), tq(nnxz);
+    std::vector<T> rec((long)nnt_data * nri, 0);
+    p1[sxz] = (T)(dt2 * wavelet[0]);
+    q1[sxz] = (T)(dt2 * wavelet[0]);
+    dop2d(g, p1.data(), q1.data(), tp.data(), tq.data());
+    keep(is, 1, tp, tq);
+    for (int it = 2; it < g.nt; ++it) {
+      const float t = it * dt + g.ot;
+      // forwardC with the stored D of the previous level (kernels.cu:546-556)
+      for (long i = 0; i < nnxz; ++i) {
+        long ix = i % nnx, iz = i / nnx;
+        if (ix < kHalf || ix >= nnx - kHalf || iz < kHalf || iz >= g.nnz() - kHalf) continue;
+        p0[i] = 2 * p1[i] + (T)dt2 * ((T)c11[i] * tp[i] + (T)c13[i] * tq[i]) - p0[i];
+        q0[i] = 2 * q1[i] + (T)dt2 * ((T)c13[i] * tp[i] + (T)c33[i] * tq[i]) - q0[i];
+        if (born) {
+          dp0[i] = 2 * dp1[i] + (T)dt2 * ((T)c11[i] * dtp[i] + (T)c13[i] * dtq[i]) - dp0[i];
+          dq0[i] = 2 * dq1[i] + (T)dt2 * ((T)c13[i] * dtp[i] + (T)c33[i] * dtq[i]) - dq0[i];
+          // scattering (kernels.cu:282-291) with the background D of it-1
+          dp0[i] += (T)dt2 * ((T)dc11[i] * tp[i] + (T)dc13[i] * tq[i]);
+          dq0[i] += (T)dt2 * ((T)dc13[i] * tp[i] + (T)dc33[i] * tq[i]);
+        }
+      }
+      p0[sxz] += (T)(dt2 * wavelet[it - 1]);
+      q0[sxz] += (T)(dt2 * wavelet[it - 1]);
+      taper2d(g, taper, p1.data()); taper2d(g, taper, q1.data());
+      taper2d(g, taper, p0.data()); taper2d(g, taper, q0.data());
+      if (born) {
+        taper2d(g, taper, dp1.data()); taper2d(g, taper, dq1.data());
+        taper2d(g, taper, dp0.data()); taper2d(g, taper, dq0.data());
+        dop2d(g, dp0.data(), dq0.data(), dtp.data(), dtq.data());
+      }
+      dop2d(g, p0.data(), q0.data(), tp.data(), tq.data());
+      keep(is, it, tp, tq);
+      if (t >= 0.f && (it - ntNeg) % ratio == 0) {
+        const T* a = born ? dp0.data() : p0.data();
+        const T* b = born ? dq0.data() : q0.data();
+        for (int ir = 0; ir < nri; ++ir)
+          rec[(long)((it - ntNeg) / ratio) * nri + ir] = (T)0.5f * (a[ridx[ir]] + b[ridx[ir]]);
+      }
+      std::swap(p0, p1); std::swap(q0, q1);
+      std::swap(dp0, dp1); std::swap(dq0, dq1);
+    }
+    // adjoint source: residual (gradient) or Born data (GN product)
+    if (!born) {
+      for (int t = 0; t < nnt_data; ++t)
+        for (int ir = 0; ir < nri; ++ir) {
+          T& r = rec[(long)t * nri + ir];
+          r = r - (T)data[(long)t * nr_total + ir0 + ir];
+          objfunc += (double)(r * r);
+        }
+    }
+    std::fill(p0.begin(), p0.end(), (T)0); std::fill(q0.begin(), q0.end(), (T)0);
+    std::fill(p1.begin(), p1.end(), (T)0); std::fill(q1.begin(), q1.end(), (T)0);
+    std::vector<T> b0(nri, 0), b1(nri, 0);
+    for (int ir = 0; ir < nri; ++ir) b0[ir] = rec[(long)(nnt_data - 1) * nri + ir];
+    auto inject = [&](T* p, T* q, float f) {  // injectData (kernels.cu:208-217)
+      for (int ir = 0; ir < nri; ++ir) {
+        T s = (T)0.5f * ((1 - (T)f) * b0[ir] + (T)f * b1[ir]);
+        p[ridx[ir]] += (T)dt2 * s;
+        q[ridx[ir]] += (T)dt2 * s;
+      }
+    };
+    auto img = [&](const Pair& pr, const T* ap, const T* aq) {
+      const std::vector<T>* A = pr.a >= 0 ? &ck[pr.a].first : nullptr;
+      const std::vector<T>* Aq = pr.a >= 0 ? &ck[pr.a].second : nullptr;
+      const std::vector<T>* B = pr.b >= 0 ? &ck[pr.b].first : nullptr;
+      const std::vector<T>* Bq = pr.b >= 0 ? &ck[pr.b].second : nullptr;
+      auto ptr = [](const std::vector<T>* v) { return v && !v->empty() ? v->data() : nullptr; };
+      image2d<T>(g, ap, aq, ptr(A), ptr(Aq), ptr(B), ptr(Bq), pr.f, g11, g13, g33);
+    };
+    inject(p0.data(), q0.data(), 0.f);
+    img(sched[is][0], p0.data(), q0.data());
+    int step = 1;
+    for (int it = g.nt - 3; it >= 0; --it, ++step) {
+      adj2d<T>(g, c11, c13, c33, p0.data(), q0.data(), p1.data(), q1.data(), !born);
+      if (it >= ntNeg) {
+        float f = (it - ntNeg + 1.) / ratio;
+        int i1 = (int)f;
+        if ((it - ntNeg + 2) % ratio == 0) {
+          for (int ir = 0; ir < nri; ++ir) b1[ir] = rec[(long)i1 * nri + ir];
+          std::swap(b0, b1);
+        }
+        inject(p1.data(), q1.data(), f - i1);
+      }
+      taper2d(g, taper, p1.data()); taper2d(g, taper, q1.data());
+      taper2d(g, taper, p0.data()); taper2d(g, taper, q0.data());
+      img(sched[is][step], p1.data(), q1.data());
+      std::swap(p0, p1);
+      std::swap(q0, q1);
+    }
+  }
+  return 0.5 * objfunc;
+}
+
 }  // namespace
 
 extern "C" {
@@ -601,5 +879,31 @@ int orc3d_time_backward_f32(const int* ip, const float* fp, const float* c11, co
   }
 ORC2D_FWD(double, f64)
 ORC2D_FWD(float, f32)
+
+// objFuncGradient_f (born = 0, dc = NULL) / GNhessian_f (born = 1).
+#define ORC2D_GRAD(T, SUF)                                                                      \
+  double orc2d_gradient_##SUF(const int* ip, const float* fp, const float* c11, const float* c13, \
+                              const float* c33, const float* dc11, const float* dc13,           \
+                              const float* dc33, const float* wavelet, const int* sloc, int ns,  \
+                              const int* rloc, int nr, const float* taper, const float* data,    \
+                              T* g11, T* g13, T* g33, int born) {                                \
+    Geo2 g = unpack2(ip, fp);                                                                   \
+    return grad2d<T>(g, c11, c13, c33, dc11, dc13, dc33, wavelet, sloc, ns, rloc, nr, taper,    \
+                     data, g11, g13, g33, born != 0);                                           \
+  }
+ORC2D_GRAD(double, f64)
+ORC2D_GRAD(float, f32)
+
+// The checkpoint pairing of the 2D gradient: 3 values (a, b, f) per imaging
+// step, nt-1 steps. Returns the number of steps.
+int orc2d_checkpoint_schedule(int nt, int ratio, float* out) {
+  std::vector<Pair> s = checkpoint_schedule(nt, ratio);  // first shot
+  for (size_t k = 0; k < s.size(); ++k) {
+    out[3 * k] = (float)s[k].a;
+    out[3 * k + 1] = (float)s[k].b;
+    out[3 * k + 2] = s[k].f;
+  }
+  return (int)s.size();
+}
 
 }  // extern "C"

@@ -53,12 +53,20 @@ def case3d(name: str) -> dict:
 
 
 def case2d(name: str) -> dict:
+    """2D survey (starting model), a true model for observed data, and a
+    smooth model perturbation dc for the Gauss-Newton product."""
     if name == "g2_a":
         s = S.survey2d(nx=64, nz=40, nt=300, npad=10, d=10.0, dt=1e-3, rate=2e-3, freq=20.0,
                        src_x=300.0, src_z=50.0, rec_z=20.0, ns=2)
     else:
         raise KeyError(name)
-    return {"s": s}
+    nnx, nnz = s.nx + 2 * s.npad, s.nz + 2 * s.npad
+    rng = np.random.default_rng(21)
+    bump = S.smooth(rng.standard_normal((nnz, nnx)).astype(np.float32), 4.0).reshape(-1)
+    bump *= 0.05 / np.abs(bump).max()
+    true = {k: (getattr(s, k) * (1 + bump)).astype(np.float32) for k in ("c11", "c13", "c33")}
+    dc = {k: (getattr(s, k) * bump).astype(np.float32) for k in ("c11", "c13", "c33")}
+    return {"s": s, "true": true, "dc": dc}
 
 
 CASES3D = ["g3_a", "g3_b", "g3_c"]

@@ -32,20 +32,38 @@ def run(binary, d, mode):
         raise SystemExit(f"{binary} {mode} failed with {r.returncode}")
 
 
-def make3d(name, out):
-    c = K.case3d(name)
+def write_inputs3d(c, d: Path):
+    """Case directory read by the harness oracle/ref_driver3d.cpp."""
     s = c["s"]
     g = s.geom()
     ns = s.souloc.size // 5
     nrec = s.recloc.size // 4
+    (d / "params.txt").write_text(
+        f"{s.nx} {s.ny} {s.nz} {s.nt} {s.npad} {g.ox!r} {g.oy!r} {g.oz!r} {g.ot!r} "
+        f"{g.dx!r} {g.dy!r} {g.dz!r} {g.dt!r} {g.sampling_rate!r} {ns} {nrec}\n")
+    for k, a in {"souloc": s.souloc, "recloc": s.recloc, "wavelet": s.wavelet,
+                 "padb": c["padb"], "randb": c["randb"]}.items():
+        np.asarray(a, dtype=np.float32).tofile(d / f"{k}.bin")
+
+
+def write_inputs2d(s, d: Path):
+    """Case directory read by the harness oracle/ref_driver2d.cpp."""
+    g = s.geom()
+    (d / "params.txt").write_text(
+        f"{s.nx} {s.nz} {s.nt} {s.npad} {g.dx!r} {g.dz!r} {g.dt!r} {g.rate!r} {g.ot!r} "
+        f"{s.sloc.size // 4} {s.rloc.size // 2}\n")
+    for k in ("c11", "c13", "c33", "taper", "wavelet"):
+        np.asarray(getattr(s, k), np.float32).tofile(d / f"{k}.bin")
+    np.asarray(s.sloc, np.int32).tofile(d / "sloc.bin")
+    np.asarray(s.rloc, np.int32).tofile(d / "rloc.bin")
+
+
+def make3d(name, out):
+    c = K.case3d(name)
+    s = c["s"]
     with tempfile.TemporaryDirectory() as td:
         d = Path(td)
-        (d / "params.txt").write_text(
-            f"{s.nx} {s.ny} {s.nz} {s.nt} {s.npad} {g.ox!r} {g.oy!r} {g.oz!r} {g.ot!r} "
-            f"{g.dx!r} {g.dy!r} {g.dz!r} {g.dt!r} {g.sampling_rate!r} {ns} {nrec}\n")
-        for k, a in {"souloc": s.souloc, "recloc": s.recloc, "wavelet": s.wavelet,
-                     "padb": c["padb"], "randb": c["randb"]}.items():
-            np.asarray(a, dtype=np.float32).tofile(d / f"{k}.bin")
+        write_inputs3d(c, d)
         np.asarray(c["cij_true"], np.float32).tofile(d / "cij.bin")
         run("ref3d", d, "model")
         dobs = np.fromfile(d / "ref_ddata.bin", dtype=np.float32)
@@ -62,29 +80,35 @@ def make3d(name, out):
 
 
 def make2d(name, out):
-    s = K.case2d(name)["s"]
-    g = s.geom()
-    ns = s.sloc.size // 4
-    nr = s.rloc.size // 2
+    c = K.case2d(name)
+    s = c["s"]
     with tempfile.TemporaryDirectory() as td:
         d = Path(td)
-        (d / "params.txt").write_text(
-            f"{s.nx} {s.nz} {s.nt} {s.npad} {g.dx!r} {g.dz!r} {g.dt!r} {g.rate!r} {g.ot!r} "
-            f"{ns} {nr}\n")
-        for k in ("c11", "c13", "c33", "taper", "wavelet"):
-            np.asarray(getattr(s, k), np.float32).tofile(d / f"{k}.bin")
-        np.asarray(s.sloc, np.int32).tofile(d / "sloc.bin")
-        np.asarray(s.rloc, np.int32).tofile(d / "rloc.bin")
+        write_inputs2d(s, d)
         run("ref2d", d, "synthetic")
         data = np.fromfile(d / "ref_data.bin", dtype=np.float32)
         run("ref2d", d, "modeling")
         w = np.fromfile(d / "ref_wavefield.bin", dtype=np.float32)
+        # observed data from the true model, gradient at the starting model
+        for k in ("c11", "c13", "c33"):
+            c["true"][k].tofile(d / f"{k}.bin")
+        run("ref2d", d, "synthetic")
+        dobs = np.fromfile(d / "ref_data.bin", dtype=np.float32)
+        dobs.tofile(d / "data.bin")
+        for k in ("c11", "c13", "c33"):
+            np.asarray(getattr(s, k), np.float32).tofile(d / f"{k}.bin")
+            c["dc"][k].tofile(d / f"d{k}.bin")
+        run("ref2d", d, "grad")
+        grad = np.fromfile(d / "ref_grad.bin", dtype=np.float32)
+        run("ref2d", d, "gnhess")
+        gnh = np.fromfile(d / "ref_gnhess.bin", dtype=np.float32)
     nnxz = (s.nx + 2 * s.npad) * (s.nz + 2 * s.npad)
     w = w.reshape(-1, nnxz)
     keep = np.arange(0, w.shape[0], 10)
     np.savez_compressed(out / f"{name}.npz", data=data, snaps=w[keep], snap_rows=keep,
+                        dobs=dobs, grad=grad, gnhess=gnh,
                         inputs=K.digest(s.c11, s.c13, s.c33, s.taper, s.wavelet, s.sloc,
-                                        s.rloc))
+                                        s.rloc, *c["true"].values(), *c["dc"].values()))
     print(name, "data max", np.abs(data).max())
 
 

@@ -42,6 +42,45 @@ def test_modeling_matches_oracle_and_reference(ctx, name):
     assert rel_l2(w[gold["snap_rows"]], gold["snaps"]) < SNAP_TOL
 
 
+@pytest.mark.parametrize("name", K.CASES2D)
+def test_gradient_matches_oracle_and_reference(ctx, name):
+    c = K.case2d(name)
+    s = c["s"]
+    g = s.geom()
+    n = (s.nx + 2 * s.npad) * (s.nz + 2 * s.npad)
+    gold = load_golden(name)
+    g11, g13, g33, mis = V.objFuncGradient_f(ctx, g, gold["dobs"], s.c11, s.c13, s.c33, s.wavelet,
+                                             s.sloc, s.rloc, s.taper)
+    o = O.gradient2d(g, s.c11, s.c13, s.c33, s.wavelet, s.sloc, s.rloc, s.taper,
+                     data=gold["dobs"])
+    ref = gold["grad"]
+    assert abs(mis - o[3]) / o[3] < 1e-5
+    assert abs(mis - ref[3 * n]) / ref[3 * n] < 1e-5
+    for k, a in enumerate((g11, g13, g33)):
+        assert rel_l2(a, o[k]) < 1e-4, k
+        assert rel_l2(a, ref[k * n:(k + 1) * n]) < 1e-4, k
+
+
+@pytest.mark.parametrize("name", K.CASES2D)
+def test_gn_hessian_matches_oracle_and_reference(ctx, name):
+    c = K.case2d(name)
+    s = c["s"]
+    g = s.geom()
+    n = (s.nx + 2 * s.npad) * (s.nz + 2 * s.npad)
+    dc = (c["dc"]["c11"], c["dc"]["c13"], c["dc"]["c33"])
+    h = V.GNhessian_f(ctx, g, s.c11, s.c13, s.c33, *dc, s.wavelet, s.sloc, s.rloc, s.taper)
+    o = O.gradient2d(g, s.c11, s.c13, s.c33, s.wavelet, s.sloc, s.rloc, s.taper, dc=dc)
+    ref = load_golden(name)["gnhess"]
+    for k in range(3):
+        assert rel_l2(h[k], o[k]) < 1e-4, k
+        assert rel_l2(h[k], ref[k * n:(k + 1) * n]) < 1e-4, k
+    # linear in the perturbation
+    h2 = V.GNhessian_f(ctx, g, s.c11, s.c13, s.c33, *(2 * x for x in dc), s.wavelet, s.sloc,
+                       s.rloc, s.taper)
+    for k in range(3):
+        assert rel_l2(h2[k], 2 * h[k]) < 1e-5
+
+
 def test_synthetic_config_size(ctx):
     """The 2D benchmark grid (201 x 401 + 30-cell pad, 2000 steps), one shot."""
     s = S.survey2d()

@@ -1,0 +1,78 @@
+"""Drop-in test: the harness that drives the reference's own entry points
+(oracle/ref_driver{3d,2d}.cpp: modelDataCij3d_f, objFuncGradientCij3d_f with
+the data= side channel, synthetic_f, modeling_f) is compiled against
+libvti_wave.so instead of the reference objects, and must reproduce the
+reference's golden outputs."""
+import subprocess
+import tempfile
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import cases as K
+import make_golden as MG
+from conftest import ROOT, load_golden, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+LIBDIR = ROOT / "thesis-source-code_b200" / "vtib200"
+
+
+@pytest.fixture(scope="module")
+def drivers(tmp_path_factory):
+    out = tmp_path_factory.mktemp("shim")
+    bins = {}
+    for dim in ("3d", "2d"):
+        exe = out / f"shim{dim}"
+        subprocess.run(
+            ["g++", "-O2", "-std=c++17", str(ROOT / "oracle" / f"ref_driver{dim}.cpp"),
+             str(ROOT / "tests" / "shim" / "myio_stub.cpp"), "-I", str(ROOT / "include"),
+             f"-L{LIBDIR}", "-lvti_wave", "-lvti_b200", f"-Wl,-rpath,{LIBDIR}", "-o", str(exe)],
+            check=True)
+        bins[dim] = exe
+    return bins
+
+
+def _run(exe, d, mode):
+    r = subprocess.run([str(exe), str(d), mode], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+
+
+@pytest.mark.parametrize("name", K.GRAD_CASES3D)
+def test_shim_3d_matches_reference(drivers, name):
+    c = K.case3d(name)
+    gold = load_golden(name)
+    with tempfile.TemporaryDirectory() as td:
+        d = Path(td)
+        MG.write_inputs3d(c, d)
+        np.asarray(c["cij_true"], np.float32).tofile(d / "cij.bin")
+        _run(drivers["3d"], d, "model")
+        dobs = np.fromfile(d / "ref_ddata.bin", dtype=np.float32)
+        assert rel_l2(dobs, gold["dobs"]) < 1e-5
+        np.asarray(gold["dobs"], np.float32).tofile(d / "dobs.bin")
+        np.asarray(c["cij"], np.float32).tofile(d / "cij.bin")
+        _run(drivers["3d"], d, "grad")
+        fg = np.fromfile(d / "ref_fgcij.bin", dtype=np.float32)
+    ref = gold["fgcij"]
+    assert abs(fg[0] - ref[0]) / ref[0] < 1e-5
+    n = (ref.size - 1) // 3
+    for k in range(3):
+        assert rel_l2(fg[1 + k * n:1 + (k + 1) * n], ref[1 + k * n:1 + (k + 1) * n]) < 1e-4
+
+
+@pytest.mark.parametrize("name", K.CASES2D)
+def test_shim_2d_matches_reference(drivers, name):
+    s = K.case2d(name)["s"]
+    gold = load_golden(name)
+    with tempfile.TemporaryDirectory() as td:
+        d = Path(td)
+        MG.write_inputs2d(s, d)
+        _run(drivers["2d"], d, "synthetic")
+        data = np.fromfile(d / "ref_data.bin", dtype=np.float32)
+        _run(drivers["2d"], d, "modeling")
+        w = np.fromfile(d / "ref_wavefield.bin", dtype=np.float32)
+    assert rel_l2(data, gold["data"]) < 1e-5
+    nnxz = (s.nx + 2 * s.npad) * (s.nz + 2 * s.npad)
+    w = w.reshape(-1, nnxz)
+    assert rel_l2(w[gold["snap_rows"]], gold["snaps"]) < 3e-5

@@ -52,12 +52,41 @@ def test_oracle_gradient_matches_reference(name):
         assert rel_l2(fg[1 + k * n:1 + (k + 1) * n], ref[1 + k * n:1 + (k + 1) * n]) < 1e-4, k
 
 
+def _digest2d(c):
+    s = c["s"]
+    return K.digest(s.c11, s.c13, s.c33, s.taper, s.wavelet, s.sloc, s.rloc,
+                    *c["true"].values(), *c["dc"].values())
+
+
+@pytest.mark.parametrize("name", K.CASES2D)
+def test_oracle_2d_gradient_and_gn_product_match_reference(name):
+    c = K.case2d(name)
+    s = c["s"]
+    gold = load_golden(name)
+    assert str(gold["inputs"]) == _digest2d(c)
+    g = s.geom()
+    n = (s.nx + 2 * s.npad) * (s.nz + 2 * s.npad)
+    g11, g13, g33, mis = O.gradient2d(g, s.c11, s.c13, s.c33, s.wavelet, s.sloc, s.rloc, s.taper,
+                                      data=gold["dobs"])
+    ref = gold["grad"]
+    assert abs(mis - ref[3 * n]) / ref[3 * n] < 1e-5
+    for k, a in enumerate((g11, g13, g33)):
+        assert np.abs(ref[k * n:(k + 1) * n]).max() > 0
+        assert rel_l2(a, ref[k * n:(k + 1) * n]) < 1e-4, k
+    h = O.gradient2d(g, s.c11, s.c13, s.c33, s.wavelet, s.sloc, s.rloc, s.taper,
+                     dc=(c["dc"]["c11"], c["dc"]["c13"], c["dc"]["c33"]))
+    ref = gold["gnhess"]
+    for k in range(3):
+        assert np.abs(ref[k * n:(k + 1) * n]).max() > 0
+        assert rel_l2(h[k], ref[k * n:(k + 1) * n]) < 1e-4, k
+
+
 @pytest.mark.parametrize("name", K.CASES2D)
 def test_oracle_2d_matches_reference(name):
-    s = K.case2d(name)["s"]
+    c = K.case2d(name)
+    s = c["s"]
     gold = load_golden(name)
-    assert str(gold["inputs"]) == K.digest(s.c11, s.c13, s.c33, s.taper, s.wavelet, s.sloc,
-                                           s.rloc)
+    assert str(gold["inputs"]) == _digest2d(c)
     g = s.geom()
     d = O.forward2d(g, s.c11, s.c13, s.c33, s.wavelet, s.sloc, s.rloc, s.taper)
     assert rel_l2(d.reshape(-1), gold["data"]) < 1e-5

@@ -64,6 +64,18 @@ int vol_download(vti_ctx* ctx, const Dims3& d, const Vol* v, float* dst, int mem
   return VTI_OK;
 }
 
+int check_device_status(vti_ctx* ctx) {
+  int h = 0;
+  VTI_CUDA(ctx, cudaMemcpyAsync(&h, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost,
+                                ctx->stream));
+  VTI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (h == 0) return VTI_OK;
+  VTI_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream));
+  if (h & (1 << VTI_ERR_TIMEOUT))
+    return fail(ctx, VTI_ERR_TIMEOUT, "a device-side pipeline wait timed out");
+  return fail(ctx, VTI_ERR_DEVICE, "device status word " + std::to_string(h));
+}
+
 static cudaEvent_t pool_get(vti_ctx* ctx) {
   if (!ctx->event_pool.empty()) {
     cudaEvent_t e = ctx->event_pool.back();

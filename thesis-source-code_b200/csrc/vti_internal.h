@@ -133,6 +133,36 @@ int launch_bwd3d(vti_ctx* ctx, const Dims3& d, const float* scx, const float* sc
                  float* g33, const Damping& damp, float dt2, float idx2, float idy2, float idz2,
                  float sx, float sy, float sz, PointSource src);
 
+// TMA descriptors (CUtensorMap, 128 bytes each) of one volume: 32 x 16 tiles
+// and 40 x 24 tiles (with the 4-cell halo). Plain storage keeps cuda.h out
+// of this header.
+struct TileMaps {
+  alignas(64) unsigned char plain[128];
+  alignas(64) unsigned char halo[128];
+};
+int make_tile_maps(vti_ctx* ctx, const Dims3& d, const Vol& v, TileMaps* out);
+
+// TMA-pipelined forward step (see vti_tma3d.cu).
+int launch_fwd3d_tma(vti_ctx* ctx, const Dims3& d, const TileMaps& cx, const TileMaps& cz,
+                     const TileMaps& px, const TileMaps& pz, const TileMaps& c11,
+                     const TileMaps& c13, const TileMaps& c33, const float* cz_ptr,
+                     float* px_ptr, float* pz_ptr, const Damping* damp, float sx, float sy,
+                     float sz, PointSource src);
+// TMA-pipelined fused backward step.
+int launch_bwd3d_tma(vti_ctx* ctx, const Dims3& d, const TileMaps& scx, const TileMaps& scz,
+                     const TileMaps& spx, const TileMaps& spz, const TileMaps& lcx,
+                     const TileMaps& lcz, const TileMaps& lpx, const TileMaps& lpz,
+                     const TileMaps& c11, const TileMaps& c13, const TileMaps& c33,
+                     const TileMaps& g11, const TileMaps& g13, const TileMaps& g33,
+                     const float* scz_ptr, const float* lcz_ptr, float* spx_ptr, float* spz_ptr,
+                     float* lpx_ptr, float* lpz_ptr, float* g11_ptr, float* g13_ptr,
+                     float* g33_ptr, const Damping& damp, float dt2, float idx2, float idy2,
+                     float idz2, float sx, float sy, float sz, PointSource src);
+
+// Reads (and clears) the device status word; VTI_ERR_TIMEOUT if a bounded
+// device-side wait gave up since the last check.
+int check_device_status(vti_ctx* ctx);
+
 // Sparse receiver kernels. rec: device offsets (Dims3::off) per receiver.
 int launch_record(vti_ctx* ctx, float* trace, int nnt, int j, const float* cx, const float* cz,
                   const long long* rec, int nr);

@@ -29,6 +29,9 @@ struct vti3d_plan {
   bool have_rand = false;
   Vol sx[2], sz[2], lx[2], lz[2];
   Vol g11, g13, g33;
+  // TMA descriptors of every volume
+  TileMaps m_sx[2], m_sz[2], m_lx[2], m_lz[2], m_cpad[3], m_crand[3], m_g[3];
+  bool use_tma = true;
   float* dampx = nullptr;  // nx + ny + nz floats, one allocation
   float* dampy = nullptr;
   float* dampz = nullptr;
@@ -259,6 +262,7 @@ int forward_pass(vti3d_plan* p, const ShotGeom& s, bool sponge) {
   const float sxs = dt2 / dx2, sys = dt2 / dy2, szs = dt2 / dz2;
   const int nnt = nnt_of(g), M = last_level(g, p->flags);
   Vol* c = (sponge || !p->have_rand) ? p->cpad : p->crand;
+  const TileMaps* cm = (sponge || !p->have_rand) ? p->m_cpad : p->m_crand;
   Damping dmp{p->dampx, p->dampy, p->dampz};
   for (int k = 0; k < 2; ++k) {
     VTI_TRY(vol_zero(ctx, d, &p->sx[k]));
@@ -278,9 +282,14 @@ int forward_pass(vti3d_plan* p, const ShotGeom& s, bool sponge) {
   src.z = s.sz;
   for (int it = 2; it <= M; ++it) {
     src.amp = dt2 * p->wavelet[it - 1];
-    VTI_TRY(launch_fwd3d(ctx, d, p->sx[A].origin, p->sz[A].origin, p->sx[B].origin,
-                         p->sz[B].origin, c[0].origin, c[1].origin, c[2].origin,
-                         sponge ? &dmp : nullptr, sxs, sys, szs, src));
+    if (p->use_tma)
+      VTI_TRY(launch_fwd3d_tma(ctx, d, p->m_sx[A], p->m_sz[A], p->m_sx[B], p->m_sz[B], cm[0],
+                               cm[1], cm[2], p->sz[A].origin, p->sx[B].origin, p->sz[B].origin,
+                               sponge ? &dmp : nullptr, sxs, sys, szs, src));
+    else
+      VTI_TRY(launch_fwd3d(ctx, d, p->sx[A].origin, p->sz[A].origin, p->sx[B].origin,
+                           p->sz[B].origin, c[0].origin, c[1].origin, c[2].origin,
+                           sponge ? &dmp : nullptr, sxs, sys, szs, src));
     std::swap(A, B);
     if (sponge && it < (int)s.rec_at.size() && s.rec_at[it] >= 0)
       VTI_TRY(launch_record(ctx, p->d_trace, nnt, s.rec_at[it], p->sx[A].origin,
@@ -302,6 +311,7 @@ int backward_pass(vti3d_plan* p, const ShotGeom& s) {
   const float idx2 = 1.f / dx2, idy2 = 1.f / dy2, idz2 = 1.f / dz2;
   const int st = sampling_step(g), nnt = nnt_of(g), M = last_level(g, p->flags);
   Vol* c = p->have_rand ? p->crand : p->cpad;
+  const TileMaps* cm = p->have_rand ? p->m_crand : p->m_cpad;
   Damping dmp{p->dampx, p->dampy, p->dampz};
   // flip (objFuncGradient3d_f.cu:912-914): cur = level M-1, prev = level M
   int SA = 1 - p->last_cur, SB = p->last_cur;
@@ -319,11 +329,19 @@ int backward_pass(vti3d_plan* p, const ShotGeom& s) {
   for (int i = 0; i < M - 1; ++i) {
     const int it = g.nt - 3 - i;
     src.amp = dt2 * p->wavelet[it + 1];
-    VTI_TRY(launch_bwd3d(ctx, d, p->sx[SA].origin, p->sz[SA].origin, p->sx[SB].origin,
-                         p->sz[SB].origin, p->lx[LA].origin, p->lz[LA].origin, p->lx[LB].origin,
-                         p->lz[LB].origin, c[0].origin, c[1].origin, c[2].origin, p->g11.origin,
-                         p->g13.origin, p->g33.origin, dmp, dt2, idx2, idy2, idz2, sxs, sys, szs,
-                         src));
+    if (p->use_tma)
+      VTI_TRY(launch_bwd3d_tma(
+          ctx, d, p->m_sx[SA], p->m_sz[SA], p->m_sx[SB], p->m_sz[SB], p->m_lx[LA], p->m_lz[LA],
+          p->m_lx[LB], p->m_lz[LB], cm[0], cm[1], cm[2], p->m_g[0], p->m_g[1], p->m_g[2],
+          p->sz[SA].origin, p->lz[LA].origin, p->sx[SB].origin, p->sz[SB].origin,
+          p->lx[LB].origin, p->lz[LB].origin, p->g11.origin, p->g13.origin, p->g33.origin, dmp,
+          dt2, idx2, idy2, idz2, sxs, sys, szs, src));
+    else
+      VTI_TRY(launch_bwd3d(ctx, d, p->sx[SA].origin, p->sz[SA].origin, p->sx[SB].origin,
+                           p->sz[SB].origin, p->lx[LA].origin, p->lz[LA].origin,
+                           p->lx[LB].origin, p->lz[LB].origin, c[0].origin, c[1].origin,
+                           c[2].origin, p->g11.origin, p->g13.origin, p->g33.origin, dmp, dt2,
+                           idx2, idy2, idz2, sxs, sys, szs, src));
     // residual interpolated at it+1 (injectRecord3d.cu:60-78)
     const int ti = it + 1;
     float f = float(ti) / float(st);
@@ -411,6 +429,7 @@ int run_gradient(vti3d_plan* p, const float* souloc, const int* shotid, int nsho
     VTI_TRY(vol_download(ctx, d, &p->g33, fgcij + 1 + 2 * n, fgcij_mem));
   }
   VTI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  VTI_TRY(check_device_status(ctx));
   if ((p->flags & VTI_OPT_CHECK_FINITE) && !std::isfinite(acc))
     return fail(ctx, VTI_ERR_NONFINITE, "misfit is not finite");
   if (misfit) *misfit = acc / 2;
@@ -444,6 +463,22 @@ int vti3d_plan_create(vti_ctx* ctx, const vti3d_geom* g, unsigned flags, vti3d_p
                  &p->g13,     &p->g33};
   for (Vol* v : vols)
     if (st == VTI_OK) st = vol_alloc(ctx, p->d, v);
+  {
+    const char* k = std::getenv("VTI_STEP_KERNELS");
+    p->use_tma = !(k && std::string(k) == "simt");
+  }
+  if (st == VTI_OK) {
+    for (int k = 0; k < 2 && st == VTI_OK; ++k) {
+      st = make_tile_maps(ctx, p->d, p->sx[k], &p->m_sx[k]);
+      if (st == VTI_OK) st = make_tile_maps(ctx, p->d, p->sz[k], &p->m_sz[k]);
+      if (st == VTI_OK) st = make_tile_maps(ctx, p->d, p->lx[k], &p->m_lx[k]);
+      if (st == VTI_OK) st = make_tile_maps(ctx, p->d, p->lz[k], &p->m_lz[k]);
+    }
+    for (int k = 0; k < 3 && st == VTI_OK; ++k) st = make_tile_maps(ctx, p->d, p->cpad[k], &p->m_cpad[k]);
+    if (st == VTI_OK) st = make_tile_maps(ctx, p->d, p->g11, &p->m_g[0]);
+    if (st == VTI_OK) st = make_tile_maps(ctx, p->d, p->g13, &p->m_g[1]);
+    if (st == VTI_OK) st = make_tile_maps(ctx, p->d, p->g33, &p->m_g[2]);
+  }
   if (st == VTI_OK) {
     p->h_damp.resize((size_t)g->nx + g->ny + g->nz);
     for (int i = 0; i < g->nx; ++i) p->h_damp[i] = damp_profile(i, g->nx, g->npad);
@@ -501,7 +536,10 @@ int vti3d_plan_set_model(vti3d_plan* p, const float* c11, const float* c13, cons
   const long long nb = boundary_count(p->g);
   if (randb) {
     for (int k = 0; k < 3; ++k)
-      if (!p->crand[k].alloc) VTI_TRY(vol_alloc(ctx, d, &p->crand[k]));
+      if (!p->crand[k].alloc) {
+        VTI_TRY(vol_alloc(ctx, d, &p->crand[k]));
+        VTI_TRY(make_tile_maps(ctx, d, p->crand[k], &p->m_crand[k]));
+      }
   }
   if (padb || randb) VTI_TRY(ensure(ctx, &p->d_blist, &p->blist_cap, (size_t)nb));
   for (int k = 0; k < 3; ++k) {
@@ -571,7 +609,7 @@ int vti3d_plan_model_data(vti3d_plan* p, const float* souloc, const int* shotid,
                                   ctx->stream));
     VTI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   }
-  return VTI_OK;
+  return check_device_status(ctx);
 }
 
 int vti3d_plan_gradient(vti3d_plan* p, const float* souloc, const int* shotid, int nshot,
@@ -590,6 +628,14 @@ int vti3d_plan_objfunc(vti3d_plan* p, const float* souloc, const int* shotid, in
 
 const float* vti3d_plan_wavefield(vti3d_plan* p) {
   return p ? p->sx[p->last_cur].origin : nullptr;
+}
+
+int vti3d_plan_get_wavefield(vti3d_plan* p, float* out, int mem) {
+  if (!p || !out) return VTI_ERR_ARG;
+  VTI_CUDA(p->ctx, cudaSetDevice(p->ctx->device));
+  VTI_TRY(vol_download(p->ctx, p->d, &p->sx[p->last_cur], out, mem));
+  VTI_CUDA(p->ctx, cudaStreamSynchronize(p->ctx->stream));
+  return VTI_OK;
 }
 
 int vti3d_model_data_cij(vti_ctx* ctx, const vti3d_geom* g, const float* c11, const float* c13,

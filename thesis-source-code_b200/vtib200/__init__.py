@@ -94,6 +94,12 @@ def _signatures():
         "vti2d_synthetic": (C.c_int, [P, P, P, P, P, P, P, C.c_int, P, C.c_int, P, P]),
         "vti2d_modeling": (C.c_int, [P, P, P, P, P, P, C.c_int, P, P]),
         "vti2d_init_taper": (None, [P, C.c_int, C.c_int, C.c_int]),
+        "vti2d_gradient": (C.c_int, [P] * 11 + [C.c_int, P, C.c_int, P, C.POINTER(C.c_double)]),
+        "vti2d_gn_hessian": (C.c_int, [P] * 13 + [C.c_int, P, C.c_int, P]),
+        "vti3d_plan_get_wavefield": (C.c_int, [P, P, C.c_int]),
+        "vti3d_gradient_vepsdel": (C.c_int, [P, P, P, P, P, P, P, C.c_float, C.c_float,
+                                             C.c_float, P, P, P, C.c_int, P, C.c_int, P, P, P, P,
+                                             C.POINTER(C.c_double), C.c_uint]),
     }
 
 
@@ -323,6 +329,32 @@ def synthetic_f(ctx, g: Geom2d, c11, c13, c33, wavelet, sloc, rloc, taper):
                                     _p(_f32(c33)), _p(_f32(wavelet)), _p(sloc), sloc.size // 4,
                                     _p(rloc), nr, _p(_f32(taper)), _p(out)))
     return out.reshape(rows, nr)
+
+
+def objFuncGradient_f(ctx, g: Geom2d, data, c11, c13, c33, wavelet, sloc, rloc, taper):
+    """objFuncGradient_f (lib/vti-fwi-2d/objFuncGradient_f.cu:15): (gc11, gc13, gc33, f)."""
+    sloc, rloc = _i32(sloc).reshape(-1), _i32(rloc).reshape(-1)
+    n = (g.nx + 2 * g.npad) * (g.nz + 2 * g.npad)
+    out = [np.zeros(n, dtype=np.float32) for _ in range(3)]
+    mis = C.c_double(0)
+    ctx.check(lib().vti2d_gradient(ctx.handle, C.byref(g), _p(out[0]), _p(out[1]), _p(out[2]),
+                                   _p(_f32(data)), _p(_f32(c11)), _p(_f32(c13)), _p(_f32(c33)),
+                                   _p(_f32(wavelet)), _p(sloc), sloc.size // 4, _p(rloc),
+                                   rloc.size // 2, _p(_f32(taper)), C.byref(mis)))
+    return out[0], out[1], out[2], mis.value
+
+
+def GNhessian_f(ctx, g: Geom2d, c11, c13, c33, dc11, dc13, dc33, wavelet, sloc, rloc, taper):
+    """GNhessian_f (lib/vti-fwi-2d/hessian_f.cu:575): Gauss-Newton H * dc."""
+    sloc, rloc = _i32(sloc).reshape(-1), _i32(rloc).reshape(-1)
+    n = (g.nx + 2 * g.npad) * (g.nz + 2 * g.npad)
+    out = [np.zeros(n, dtype=np.float32) for _ in range(3)]
+    ctx.check(lib().vti2d_gn_hessian(ctx.handle, C.byref(g), _p(out[0]), _p(out[1]),
+                                     _p(out[2]), _p(_f32(c11)), _p(_f32(c13)), _p(_f32(c33)),
+                                     _p(_f32(dc11)), _p(_f32(dc13)), _p(_f32(dc33)),
+                                     _p(_f32(wavelet)), _p(sloc), sloc.size // 4, _p(rloc),
+                                     rloc.size // 2, _p(_f32(taper))))
+    return out
 
 
 def modeling_f(ctx, g: Geom2d, c11, c13, c33, wavelet, slocxz, taper):
