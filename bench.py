@@ -201,10 +201,13 @@ def run_b200(args):
     bwd_avg = bwd_ms / max(bwd_n, 1) / 1e3
     fwd_avg = fwd_ms / max(fwd_n, 1) / 1e3
     achieved = BWD_BYTES_PER_POINT * upd / bwd_avg / 1e9 if bwd_n else None
+    # DRAM bytes per updated point from an ncu capture of a smaller grid
+    # (traffic grows with the points updated), scaled to this launch
     traffic = None
-    tf = ROOT / "profiles" / "k_bwd3d_traffic.json"
+    tf = ROOT / "profiles" / "k_bwd3d_tma_traffic.json"
     if tf.exists():
-        traffic = json.loads(tf.read_text()).get("bytes_per_launch")
+        per_point = json.loads(tf.read_text()).get("dram_bytes_per_point")
+        traffic = round(per_point * upd) if per_point else None
     out = None
     if rank == 0:
         e2e = run_e2e(args, ctx, s, cstart, padb, randb, dobs.cpu().numpy(), flags)
@@ -221,7 +224,7 @@ def run_b200(args):
                        "grid": [s.nx, s.ny, s.nz], "nt": s.nt, "levels": M,
                        "receivers": nrec, "shots_per_gpu": 1, "misfit": mis,
                        "l2": "wavefields (128 MB each) larger than L2 (126 MB)"},
-            "roofline": {"bound": "hbm", "kernel": "k_bwd3d",
+            "roofline": {"bound": "hbm", "kernel": "k_bwd3d_tma",
                          "achieved": round(achieved, 1) if achieved else None, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": round(achieved / peak, 4) if achieved else None,

@@ -72,7 +72,22 @@ def test_shim_2d_matches_reference(drivers, name):
         data = np.fromfile(d / "ref_data.bin", dtype=np.float32)
         _run(drivers["2d"], d, "modeling")
         w = np.fromfile(d / "ref_wavefield.bin", dtype=np.float32)
+        # objFuncGradient_f and GNhessian_f at the starting model
+        np.asarray(gold["dobs"], np.float32).tofile(d / "data.bin")
+        c = K.case2d(name)
+        for k in ("c11", "c13", "c33"):
+            c["dc"][k].tofile(d / f"d{k}.bin")
+        _run(drivers["2d"], d, "grad")
+        grad = np.fromfile(d / "ref_grad.bin", dtype=np.float32)
+        _run(drivers["2d"], d, "gnhess")
+        gnh = np.fromfile(d / "ref_gnhess.bin", dtype=np.float32)
     assert rel_l2(data, gold["data"]) < 1e-5
     nnxz = (s.nx + 2 * s.npad) * (s.nz + 2 * s.npad)
     w = w.reshape(-1, nnxz)
     assert rel_l2(w[gold["snap_rows"]], gold["snaps"]) < 3e-5
+    ref = gold["grad"]
+    assert abs(grad[3 * nnxz] - ref[3 * nnxz]) / ref[3 * nnxz] < 1e-5
+    for k in range(3):
+        sl = slice(k * nnxz, (k + 1) * nnxz)
+        assert rel_l2(grad[sl], ref[sl]) < 1e-4, k
+        assert rel_l2(gnh[sl], gold["gnhess"][sl]) < 1e-4, k

@@ -1,11 +1,15 @@
 // 3D VTI step kernels, sm_100a: TMA-staged 2.5D blocking.
 //
-// Work decomposition. The update region (x,y in [4,n-4), all z) is cut into
-// 32 x 16 columns; the (column, z-plane) pairs, z fastest, form one linear
-// sequence that is split into equal contiguous ranges, one per persistent CTA
-// (a multiple of the SM count). A CTA therefore marches down one or two
-// columns without gaps, which keeps its z register queue warm and balances
-// the load to within one plane.
+// Work decomposition. The grid is cut into 32 x 16 columns whose x origin is
+// a multiple of 32 (so every 128-byte TMA row is one L2 line; cells x < 4 and
+// x >= nx-4 are loaded as halo but not updated), y from 4. Each column is cut
+// into equal z-segments; an item is one (column, segment) pair, numbered
+// segment-major. Persistent CTAs (resident slots = SMs x CTAs per SM) take
+// items cyclically, so the CTAs of one wave start their segments together
+// and neighbouring columns walk down z in step: the halo and the 128-byte
+// lines two columns share are read from DRAM once and hit in L2 for the
+// other. The segment length is chosen on the host to balance whole waves
+// against the cost of restarting the z register queue.
 //
 // Pipeline. Warp 8 (producer) issues, for every plane of its range, TMA tile
 // loads (cp.async.bulk.tensor.3d, no multicast) of all input planes into a
@@ -22,6 +26,8 @@
 // Arithmetic and the sponge rule are those of vti_kernels3d.cu (see there);
 // the reference is lib/vti-fwi-3d/gpu/kernel3d.cu:3-74,222-298 and
 // abc3d.cu:82-126.
+#include <algorithm>
+
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -91,17 +97,22 @@ __device__ __forceinline__ void tma_load(void* dst, const CUtensorMap* map, uint
 }
 
 struct Sched {
-  int gx, gy;        // columns in x, y
+  int gx, gy;  // columns in x, y
   int nz;
-  long long total;   // gx*gy*nz plane-tiles
-  long long per_cta;
+  int seg;     // planes per segment
+  int items;   // gx * gy * ceil(nz / seg)
+  int grid;    // persistent CTAs, min(items, resident slots)
 };
 
-__device__ __forceinline__ void decode(const Sched& s, long long L, int& bx, int& by, int& z) {
-  const long long col = L / s.nz;
-  z = (int)(L - col * s.nz);
-  bx = (int)(col % s.gx);
-  by = (int)(col / s.gx);
+// Item i: segment i / (gx*gy) of column i % (gx*gy), planes [z0, z1).
+__device__ __forceinline__ void item(const Sched& s, int i, int& bx, int& by, int& z0,
+                                     int& z1) {
+  const int cols = s.gx * s.gy;
+  const int sg = i / cols, col = i - sg * cols;
+  bx = col % s.gx;
+  by = col / s.gx;
+  z0 = sg * s.seg;
+  z1 = min(s.nz, z0 + s.seg);
 }
 
 // ------------------------------------------------------------ forward
@@ -141,9 +152,6 @@ __global__ void __launch_bounds__(NTHREADS, 3)
   uint64_t* full = (uint64_t*)(smem + F_STAGES * F_STAGE_BYTES);
   uint64_t* empty = full + F_STAGES;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const long long L0 = (long long)blockIdx.x * a.sc.per_cta;
-  const long long L1 = min(L0 + a.sc.per_cta, a.sc.total);
-  if (L0 >= L1) return;
   if (threadIdx.x == 0) {
     for (int s = 0; s < F_STAGES; ++s) {
       mbar_init(&full[s], 1);
@@ -156,23 +164,30 @@ __global__ void __launch_bounds__(NTHREADS, 3)
 
   if (warp == NCW) {  // ---------------- producer
     if (lane == 0) {
-      for (long long L = L0; L < L1; ++L) {
-        const long long k = L - L0;
-        const int s = (int)(k % F_STAGES);
-        if (k >= F_STAGES && !mbar_wait(&empty[s], (uint32_t)(((k / F_STAGES) & 1) ^ 1), a.status))
-          break;
-        int bx, by, z;
-        decode(a.sc, L, bx, by, z);
-        const int x0 = kHalo + bx * TX, y0 = kHalo + by * TY, zp = z + kZPad;
-        unsigned char* st = smem + s * F_STAGE_BYTES;
-        mbar_arrive_expect_tx(&full[s], F_STAGE_BYTES);
-        tma_load(st + F_OFF_H, &m_cx, &full[s], x0 - kHalo, y0 - kHalo, zp);
-        tma_load(st + F_OFF_Z, &m_cz, &full[s], x0, y0, zp + kHalo);
-        tma_load(st + F_OFF_PX, &m_px, &full[s], x0, y0, zp);
-        tma_load(st + F_OFF_PZ, &m_pz, &full[s], x0, y0, zp);
-        tma_load(st + F_OFF_C, &m_c11, &full[s], x0, y0, zp);
-        tma_load(st + F_OFF_C + PLAIN_BYTES, &m_c13, &full[s], x0, y0, zp);
-        tma_load(st + F_OFF_C + 2 * PLAIN_BYTES, &m_c33, &full[s], x0, y0, zp);
+      long long k = 0;  // planes issued by this CTA
+      bool ok = true;
+      for (int it = blockIdx.x; ok && it < a.sc.items; it += gridDim.x) {
+        int bx, by, z0, z1;
+        item(a.sc, it, bx, by, z0, z1);
+        const int x0 = bx * TX, y0 = kHalo + by * TY;
+        for (int z = z0; z < z1; ++z, ++k) {
+          const int s = (int)(k % F_STAGES);
+          if (k >= F_STAGES &&
+              !mbar_wait(&empty[s], (uint32_t)(((k / F_STAGES) & 1) ^ 1), a.status)) {
+            ok = false;
+            break;
+          }
+          const int zp = z + kZPad;
+          unsigned char* st = smem + s * F_STAGE_BYTES;
+          mbar_arrive_expect_tx(&full[s], F_STAGE_BYTES);
+          tma_load(st + F_OFF_H, &m_cx, &full[s], x0 - kHalo, y0 - kHalo, zp);
+          tma_load(st + F_OFF_Z, &m_cz, &full[s], x0, y0, zp + kHalo);
+          tma_load(st + F_OFF_PX, &m_px, &full[s], x0, y0, zp);
+          tma_load(st + F_OFF_PZ, &m_pz, &full[s], x0, y0, zp);
+          tma_load(st + F_OFF_C, &m_c11, &full[s], x0, y0, zp);
+          tma_load(st + F_OFF_C + PLAIN_BYTES, &m_c13, &full[s], x0, y0, zp);
+          tma_load(st + F_OFF_C + 2 * PLAIN_BYTES, &m_c33, &full[s], x0, y0, zp);
+        }
       }
     }
     return;
@@ -184,85 +199,87 @@ __global__ void __launch_bounds__(NTHREADS, 3)
   float dxy[RY];
   int off[RY];
   bool valid[RY];
-  int cur_col = -1;
-  for (long long L = L0; L < L1; ++L) {
-    const long long k = L - L0;
-    const int s = (int)(k % F_STAGES);
-    int bx, by, z;
-    decode(a.sc, L, bx, by, z);
-    const int col = bx + by * a.sc.gx;
-    const int x = kHalo + bx * TX + lane;
+  long long k = 0;  // planes consumed by this CTA
+  bool ok = true;
+  for (int it = blockIdx.x; ok && it < a.sc.items; it += gridDim.x) {
+    int bx, by, z0, z1;
+    item(a.sc, it, bx, by, z0, z1);
+    const int x = bx * TX + lane;
     const int y0 = kHalo + by * TY;
-    if (col != cur_col) {  // (re)start the queue: planes z-4 .. z+3 from global
-      cur_col = col;
-#pragma unroll
-      for (int r = 0; r < RY; ++r) {
-        const int y = y0 + warp * RY + r;
-        valid[r] = x < d.nx - kHalo && y < d.ny - kHalo;
-        off[r] = y * d.pitch + x;
-        dxy[r] = (damp && valid[r]) ? a.dampx[x] * a.dampy[y] : 1.f;
-        q[r][0] = 0.f;
-#pragma unroll
-        for (int kk = 1; kk < 9; ++kk) {
-          const int zz = z - 5 + kk;
-          float v = valid[r] ? __ldg(a.cz + (long long)zz * d.plane + off[r]) : 0.f;
-          // planes of the block above z were already damped as "cur"
-          if (damp && zz >= 0 && (zz >> 2) < (z >> 2)) v *= dxy[r] * a.dampz[zz];
-          q[r][kk] = v;
-        }
-      }
-    }
-    if (!mbar_wait(&full[s], (uint32_t)((k / F_STAGES) & 1), a.status)) break;
-    const float* sh = (const float*)(smem + s * F_STAGE_BYTES + F_OFF_H);
-    const float* sq = (const float*)(smem + s * F_STAGE_BYTES + F_OFF_Z);
-    const float* spx = (const float*)(smem + s * F_STAGE_BYTES + F_OFF_PX);
-    const float* spz = (const float*)(smem + s * F_STAGE_BYTES + F_OFF_PZ);
-    const float* s11 = (const float*)(smem + s * F_STAGE_BYTES + F_OFF_C);
-    const float* s13 = s11 + TX * TY;
-    const float* s33 = s13 + TX * TY;
-    const float dz = damp ? a.dampz[z] : 1.f;
+    // start the queue: planes z0-4 .. z0+3 from global
 #pragma unroll
     for (int r = 0; r < RY; ++r) {
-      const int ry = warp * RY + r;
-      const int pi = ry * TX + lane;
+      const int y = y0 + warp * RY + r;
+      valid[r] = x >= kHalo && x < d.nx - kHalo && y < d.ny - kHalo;
+      off[r] = y * d.pitch + x;
+      dxy[r] = (damp && valid[r]) ? a.dampx[x] * a.dampy[y] : 1.f;
+      q[r][0] = 0.f;
 #pragma unroll
-      for (int kk = 0; kk < 8; ++kk) q[r][kk] = q[r][kk + 1];
-      q[r][8] = sq[pi];
-      const int sr = (ry + kHalo) * HX + lane + kHalo;
-      const float c = sh[sr];
-      const float lxx = lap9(c, sh[sr - 1], sh[sr + 1], sh[sr - 2], sh[sr + 2], sh[sr - 3],
-                             sh[sr + 3], sh[sr - 4], sh[sr + 4]);
-      const float lyy = lap9(c, sh[sr - HX], sh[sr + HX], sh[sr - 2 * HX], sh[sr + 2 * HX],
-                             sh[sr - 3 * HX], sh[sr + 3 * HX], sh[sr - 4 * HX], sh[sr + 4 * HX]);
-      const float lzz =
-          lap9(q[r][4], q[r][3], q[r][5], q[r][2], q[r][6], q[r][1], q[r][7], q[r][0], q[r][8]);
-      const float lxy = fmaf(lyy, a.sy, lxx * a.sx);
-      const float lz = lzz * a.sz;
-      const float dd = dxy[r] * dz;
-      float nxv = fmaf(s11[pi], lxy, fmaf(s13[pi], lz, 2.f * c - dd * spx[pi]));
-      float nzv = fmaf(s13[pi], lxy, fmaf(s33[pi], lz, 2.f * q[r][4] - dd * spz[pi]));
-      const int y = y0 + ry;
-      if (x == a.src.x && y == a.src.y && z == a.src.z) {
-        nxv += a.src.amp;
-        nzv += a.src.amp;
-      }
-      if (valid[r]) {
-        const long long i = (long long)z * d.plane + off[r];
-        a.px[i] = dd * nxv;
-        a.pz[i] = dd * nzv;
+      for (int kk = 1; kk < 9; ++kk) {
+        const int zz = z0 - 5 + kk;
+        float v = valid[r] ? __ldg(a.cz + (long long)zz * d.plane + off[r]) : 0.f;
+        // planes of the block above z0 were already damped as "cur"
+        if (damp && zz >= 0 && (zz >> 2) < (z0 >> 2)) v *= dxy[r] * a.dampz[zz];
+        q[r][kk] = v;
       }
     }
-    __syncwarp();
-    if (lane == 0) mbar_arrive(&empty[s]);
-    // entering the next plane: if it starts a new 4-plane block of the same
-    // column, the four planes of the block just finished become "damped cur"
-    if (damp && ((z + 1) & 3) == 0 && z + 1 < d.nz) {
+    for (int z = z0; z < z1; ++z, ++k) {
+      const int s = (int)(k % F_STAGES);
+      if (!mbar_wait(&full[s], (uint32_t)((k / F_STAGES) & 1), a.status)) {
+        ok = false;
+        break;
+      }
+      const float* sh = (const float*)(smem + s * F_STAGE_BYTES + F_OFF_H);
+      const float* sq = (const float*)(smem + s * F_STAGE_BYTES + F_OFF_Z);
+      const float* spx = (const float*)(smem + s * F_STAGE_BYTES + F_OFF_PX);
+      const float* spz = (const float*)(smem + s * F_STAGE_BYTES + F_OFF_PZ);
+      const float* s11 = (const float*)(smem + s * F_STAGE_BYTES + F_OFF_C);
+      const float* s13 = s11 + TX * TY;
+      const float* s33 = s13 + TX * TY;
+      const float dz = damp ? a.dampz[z] : 1.f;
 #pragma unroll
       for (int r = 0; r < RY; ++r) {
-        // after the shift at z+1, entries 0..3 hold planes z-3..z; they are
-        // entries 1..4 now
+        const int ry = warp * RY + r;
+        const int pi = ry * TX + lane;
 #pragma unroll
-        for (int kk = 0; kk < 4; ++kk) q[r][kk + 1] *= dxy[r] * a.dampz[z - 3 + kk];
+        for (int kk = 0; kk < 8; ++kk) q[r][kk] = q[r][kk + 1];
+        q[r][8] = sq[pi];
+        const int sr = (ry + kHalo) * HX + lane + kHalo;
+        const float c = sh[sr];
+        const float lxx = lap9(c, sh[sr - 1], sh[sr + 1], sh[sr - 2], sh[sr + 2], sh[sr - 3],
+                               sh[sr + 3], sh[sr - 4], sh[sr + 4]);
+        const float lyy = lap9(c, sh[sr - HX], sh[sr + HX], sh[sr - 2 * HX], sh[sr + 2 * HX],
+                               sh[sr - 3 * HX], sh[sr + 3 * HX], sh[sr - 4 * HX], sh[sr + 4 * HX]);
+        const float lzz =
+            lap9(q[r][4], q[r][3], q[r][5], q[r][2], q[r][6], q[r][1], q[r][7], q[r][0], q[r][8]);
+        const float lxy = fmaf(lyy, a.sy, lxx * a.sx);
+        const float lz = lzz * a.sz;
+        const float dd = dxy[r] * dz;
+        float nxv = fmaf(s11[pi], lxy, fmaf(s13[pi], lz, 2.f * c - dd * spx[pi]));
+        float nzv = fmaf(s13[pi], lxy, fmaf(s33[pi], lz, 2.f * q[r][4] - dd * spz[pi]));
+        const int y = y0 + ry;
+        if (x == a.src.x && y == a.src.y && z == a.src.z) {
+          nxv += a.src.amp;
+          nzv += a.src.amp;
+        }
+        if (valid[r]) {
+          const long long i = (long long)z * d.plane + off[r];
+          a.px[i] = dd * nxv;
+          a.pz[i] = dd * nzv;
+        }
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[s]);
+      // entering the next plane: if it starts a new 4-plane block of the same
+      // column, the four planes of the block just finished become "damped cur"
+      if (damp && ((z + 1) & 3) == 0 && z + 1 < d.nz) {
+#pragma unroll
+        for (int r = 0; r < RY; ++r) {
+          // after the shift at z+1, entries 0..3 hold planes z-3..z; they are
+          // entries 1..4 now
+#pragma unroll
+          for (int kk = 0; kk < 4; ++kk) q[r][kk + 1] *= dxy[r] * a.dampz[z - 3 + kk];
+        }
       }
     }
   }
@@ -310,9 +327,6 @@ __global__ void __launch_bounds__(NTHREADS, 2)
   uint64_t* full = (uint64_t*)(smem + B_STAGES * B_STAGE_BYTES);
   uint64_t* empty = full + B_STAGES;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const long long L0 = (long long)blockIdx.x * a.sc.per_cta;
-  const long long L1 = min(L0 + a.sc.per_cta, a.sc.total);
-  if (L0 >= L1) return;
   if (threadIdx.x == 0) {
     for (int s = 0; s < B_STAGES; ++s) {
       mbar_init(&full[s], 1);
@@ -325,31 +339,38 @@ __global__ void __launch_bounds__(NTHREADS, 2)
 
   if (warp == NCW) {  // ---------------- producer
     if (lane == 0) {
-      for (long long L = L0; L < L1; ++L) {
-        const long long k = L - L0;
-        const int s = (int)(k % B_STAGES);
-        if (k >= B_STAGES && !mbar_wait(&empty[s], (uint32_t)(((k / B_STAGES) & 1) ^ 1), a.status))
-          break;
-        int bx, by, z;
-        decode(a.sc, L, bx, by, z);
-        const int x0 = kHalo + bx * TX, y0 = kHalo + by * TY, zp = z + kZPad;
-        unsigned char* st = smem + s * B_STAGE_BYTES;
-        unsigned char* pl = st + B_OFF_P;
-        mbar_arrive_expect_tx(&full[s], B_STAGE_BYTES);
-        tma_load(st + B_OFF_SH, &m.scx, &full[s], x0 - kHalo, y0 - kHalo, zp);
-        tma_load(st + B_OFF_LH, &m.lcx, &full[s], x0 - kHalo, y0 - kHalo, zp);
-        tma_load(pl + 0 * PLAIN_BYTES, &m.scz, &full[s], x0, y0, zp + kHalo);
-        tma_load(pl + 1 * PLAIN_BYTES, &m.lcz, &full[s], x0, y0, zp + kHalo);
-        tma_load(pl + 2 * PLAIN_BYTES, &m.spx, &full[s], x0, y0, zp);
-        tma_load(pl + 3 * PLAIN_BYTES, &m.spz, &full[s], x0, y0, zp);
-        tma_load(pl + 4 * PLAIN_BYTES, &m.lpx, &full[s], x0, y0, zp);
-        tma_load(pl + 5 * PLAIN_BYTES, &m.lpz, &full[s], x0, y0, zp);
-        tma_load(pl + 6 * PLAIN_BYTES, &m.c11, &full[s], x0, y0, zp);
-        tma_load(pl + 7 * PLAIN_BYTES, &m.c13, &full[s], x0, y0, zp);
-        tma_load(pl + 8 * PLAIN_BYTES, &m.c33, &full[s], x0, y0, zp);
-        tma_load(pl + 9 * PLAIN_BYTES, &m.g11, &full[s], x0, y0, zp);
-        tma_load(pl + 10 * PLAIN_BYTES, &m.g13, &full[s], x0, y0, zp);
-        tma_load(pl + 11 * PLAIN_BYTES, &m.g33, &full[s], x0, y0, zp);
+      long long k = 0;
+      bool ok = true;
+      for (int it = blockIdx.x; ok && it < a.sc.items; it += gridDim.x) {
+        int bx, by, z0, z1;
+        item(a.sc, it, bx, by, z0, z1);
+        const int x0 = bx * TX, y0 = kHalo + by * TY;
+        for (int z = z0; z < z1; ++z, ++k) {
+          const int s = (int)(k % B_STAGES);
+          if (k >= B_STAGES &&
+              !mbar_wait(&empty[s], (uint32_t)(((k / B_STAGES) & 1) ^ 1), a.status)) {
+            ok = false;
+            break;
+          }
+          const int zp = z + kZPad;
+          unsigned char* st = smem + s * B_STAGE_BYTES;
+          unsigned char* pl = st + B_OFF_P;
+          mbar_arrive_expect_tx(&full[s], B_STAGE_BYTES);
+          tma_load(st + B_OFF_SH, &m.scx, &full[s], x0 - kHalo, y0 - kHalo, zp);
+          tma_load(st + B_OFF_LH, &m.lcx, &full[s], x0 - kHalo, y0 - kHalo, zp);
+          tma_load(pl + 0 * PLAIN_BYTES, &m.scz, &full[s], x0, y0, zp + kHalo);
+          tma_load(pl + 1 * PLAIN_BYTES, &m.lcz, &full[s], x0, y0, zp + kHalo);
+          tma_load(pl + 2 * PLAIN_BYTES, &m.spx, &full[s], x0, y0, zp);
+          tma_load(pl + 3 * PLAIN_BYTES, &m.spz, &full[s], x0, y0, zp);
+          tma_load(pl + 4 * PLAIN_BYTES, &m.lpx, &full[s], x0, y0, zp);
+          tma_load(pl + 5 * PLAIN_BYTES, &m.lpz, &full[s], x0, y0, zp);
+          tma_load(pl + 6 * PLAIN_BYTES, &m.c11, &full[s], x0, y0, zp);
+          tma_load(pl + 7 * PLAIN_BYTES, &m.c13, &full[s], x0, y0, zp);
+          tma_load(pl + 8 * PLAIN_BYTES, &m.c33, &full[s], x0, y0, zp);
+          tma_load(pl + 9 * PLAIN_BYTES, &m.g11, &full[s], x0, y0, zp);
+          tma_load(pl + 10 * PLAIN_BYTES, &m.g13, &full[s], x0, y0, zp);
+          tma_load(pl + 11 * PLAIN_BYTES, &m.g33, &full[s], x0, y0, zp);
+        }
       }
     }
     return;
@@ -359,108 +380,110 @@ __global__ void __launch_bounds__(NTHREADS, 2)
   float dxy[RY];
   int off[RY];
   bool valid[RY];
-  int cur_col = -1;
-  for (long long L = L0; L < L1; ++L) {
-    const long long k = L - L0;
-    const int s = (int)(k % B_STAGES);
-    int bx, by, z;
-    decode(a.sc, L, bx, by, z);
-    const int col = bx + by * a.sc.gx;
-    const int x = kHalo + bx * TX + lane;
+  long long k = 0;
+  bool ok = true;
+  for (int it = blockIdx.x; ok && it < a.sc.items; it += gridDim.x) {
+    int bx, by, z0, z1;
+    item(a.sc, it, bx, by, z0, z1);
+    const int x = bx * TX + lane;
     const int y0 = kHalo + by * TY;
-    if (col != cur_col) {
-      cur_col = col;
-#pragma unroll
-      for (int r = 0; r < RY; ++r) {
-        const int y = y0 + warp * RY + r;
-        valid[r] = x < d.nx - kHalo && y < d.ny - kHalo;
-        off[r] = y * d.pitch + x;
-        dxy[r] = valid[r] ? a.dampx[x] * a.dampy[y] : 1.f;
-        sq[r][0] = lq[r][0] = 0.f;
-#pragma unroll
-        for (int kk = 1; kk < 9; ++kk) {
-          const int zz = z - 5 + kk;
-          const long long i = (long long)zz * d.plane + off[r];
-          sq[r][kk] = valid[r] ? __ldg(a.scz + i) : 0.f;
-          float v = valid[r] ? __ldg(a.lcz + i) : 0.f;
-          if (zz >= 0 && (zz >> 2) < (z >> 2)) v *= dxy[r] * a.dampz[zz];
-          lq[r][kk] = v;
-        }
-      }
-    }
-    if (!mbar_wait(&full[s], (uint32_t)((k / B_STAGES) & 1), a.status)) break;
-    const unsigned char* st = smem + s * B_STAGE_BYTES;
-    const float* sh = (const float*)(st + B_OFF_SH);
-    const float* lh = (const float*)(st + B_OFF_LH);
-    const float* pl = (const float*)(st + B_OFF_P);
-    constexpr int T = TX * TY;
-    const float dz = a.dampz[z];
+    // start the queues: planes z0-4 .. z0+3 from global
 #pragma unroll
     for (int r = 0; r < RY; ++r) {
-      const int ry = warp * RY + r;
-      const int pi = ry * TX + lane;
+      const int y = y0 + warp * RY + r;
+      valid[r] = x >= kHalo && x < d.nx - kHalo && y < d.ny - kHalo;
+      off[r] = y * d.pitch + x;
+      dxy[r] = valid[r] ? a.dampx[x] * a.dampy[y] : 1.f;
+      sq[r][0] = lq[r][0] = 0.f;
 #pragma unroll
-      for (int kk = 0; kk < 8; ++kk) {
-        sq[r][kk] = sq[r][kk + 1];
-        lq[r][kk] = lq[r][kk + 1];
-      }
-      sq[r][8] = pl[0 * T + pi];
-      lq[r][8] = pl[1 * T + pi];
-      const float a11 = pl[6 * T + pi], a13 = pl[7 * T + pi], a33 = pl[8 * T + pi];
-      const int sr = (ry + kHalo) * HX + lane + kHalo;
-      const int y = y0 + ry;
-      // source wavefield back one level (gradient form)
-      const float sc = sh[sr];
-      const float sxx = lap9(sc, sh[sr - 1], sh[sr + 1], sh[sr - 2], sh[sr + 2], sh[sr - 3],
-                             sh[sr + 3], sh[sr - 4], sh[sr + 4]);
-      const float syy = lap9(sc, sh[sr - HX], sh[sr + HX], sh[sr - 2 * HX], sh[sr + 2 * HX],
-                             sh[sr - 3 * HX], sh[sr + 3 * HX], sh[sr - 4 * HX], sh[sr + 4 * HX]);
-      const float szz = lap9(sq[r][4], sq[r][3], sq[r][5], sq[r][2], sq[r][6], sq[r][1],
-                             sq[r][7], sq[r][0], sq[r][8]);
-      const float sxy_u = fmaf(syy, a.idy2, sxx * a.idx2);
-      const float sz_u = szz * a.idz2;
-      float snx = fmaf(a.dt2, fmaf(a11, sxy_u, a13 * sz_u), 2.f * sc - pl[2 * T + pi]);
-      float snz = fmaf(a.dt2, fmaf(a13, sxy_u, a33 * sz_u), 2.f * sq[r][4] - pl[3 * T + pi]);
-      if (x == a.src.x && y == a.src.y && z == a.src.z) {
-        snx += a.src.amp;
-        snz += a.src.amp;
-      }
-      // imaging with the current adjoint
-      const float lc = lh[sr];
-      const float lz0 = lq[r][4];
-      const float g11 = fmaf(lc, sxy_u, pl[9 * T + pi]);
-      const float g33 = fmaf(lz0, sz_u, pl[11 * T + pi]);
-      const float g13 = fmaf(lz0, sxy_u, fmaf(lc, sz_u, pl[10 * T + pi]));
-      // adjoint, forward form with the sponge
-      const float lxx = lap9(lc, lh[sr - 1], lh[sr + 1], lh[sr - 2], lh[sr + 2], lh[sr - 3],
-                             lh[sr + 3], lh[sr - 4], lh[sr + 4]);
-      const float lyy = lap9(lc, lh[sr - HX], lh[sr + HX], lh[sr - 2 * HX], lh[sr + 2 * HX],
-                             lh[sr - 3 * HX], lh[sr + 3 * HX], lh[sr - 4 * HX], lh[sr + 4 * HX]);
-      const float lzz = lap9(lz0, lq[r][3], lq[r][5], lq[r][2], lq[r][6], lq[r][1], lq[r][7],
-                             lq[r][0], lq[r][8]);
-      const float lxy = fmaf(lyy, a.sy, lxx * a.sx);
-      const float lzs = lzz * a.sz;
-      const float dd = dxy[r] * dz;
-      const float lnx = fmaf(a11, lxy, fmaf(a13, lzs, 2.f * lc - dd * pl[4 * T + pi]));
-      const float lnz = fmaf(a13, lxy, fmaf(a33, lzs, 2.f * lz0 - dd * pl[5 * T + pi]));
-      if (valid[r]) {
-        const long long i = (long long)z * d.plane + off[r];
-        a.spx[i] = snx;
-        a.spz[i] = snz;
-        a.lpx[i] = dd * lnx;
-        a.lpz[i] = dd * lnz;
-        a.g11[i] = g11;
-        a.g13[i] = g13;
-        a.g33[i] = g33;
+      for (int kk = 1; kk < 9; ++kk) {
+        const int zz = z0 - 5 + kk;
+        const long long i = (long long)zz * d.plane + off[r];
+        sq[r][kk] = valid[r] ? __ldg(a.scz + i) : 0.f;
+        float v = valid[r] ? __ldg(a.lcz + i) : 0.f;
+        if (zz >= 0 && (zz >> 2) < (z0 >> 2)) v *= dxy[r] * a.dampz[zz];
+        lq[r][kk] = v;
       }
     }
-    __syncwarp();
-    if (lane == 0) mbar_arrive(&empty[s]);
-    if (((z + 1) & 3) == 0 && z + 1 < d.nz) {
+    for (int z = z0; z < z1; ++z, ++k) {
+      const int s = (int)(k % B_STAGES);
+      if (!mbar_wait(&full[s], (uint32_t)((k / B_STAGES) & 1), a.status)) {
+        ok = false;
+        break;
+      }
+      const unsigned char* st = smem + s * B_STAGE_BYTES;
+      const float* sh = (const float*)(st + B_OFF_SH);
+      const float* lh = (const float*)(st + B_OFF_LH);
+      const float* pl = (const float*)(st + B_OFF_P);
+      constexpr int T = TX * TY;
+      const float dz = a.dampz[z];
 #pragma unroll
       for (int r = 0; r < RY; ++r) {
+        const int ry = warp * RY + r;
+        const int pi = ry * TX + lane;
 #pragma unroll
-        for (int kk = 0; kk < 4; ++kk) lq[r][kk + 1] *= dxy[r] * a.dampz[z - 3 + kk];
+        for (int kk = 0; kk < 8; ++kk) {
+          sq[r][kk] = sq[r][kk + 1];
+          lq[r][kk] = lq[r][kk + 1];
+        }
+        sq[r][8] = pl[0 * T + pi];
+        lq[r][8] = pl[1 * T + pi];
+        const float a11 = pl[6 * T + pi], a13 = pl[7 * T + pi], a33 = pl[8 * T + pi];
+        const int sr = (ry + kHalo) * HX + lane + kHalo;
+        const int y = y0 + ry;
+        // source wavefield back one level (gradient form)
+        const float sc = sh[sr];
+        const float sxx = lap9(sc, sh[sr - 1], sh[sr + 1], sh[sr - 2], sh[sr + 2], sh[sr - 3],
+                               sh[sr + 3], sh[sr - 4], sh[sr + 4]);
+        const float syy = lap9(sc, sh[sr - HX], sh[sr + HX], sh[sr - 2 * HX], sh[sr + 2 * HX],
+                               sh[sr - 3 * HX], sh[sr + 3 * HX], sh[sr - 4 * HX], sh[sr + 4 * HX]);
+        const float szz = lap9(sq[r][4], sq[r][3], sq[r][5], sq[r][2], sq[r][6], sq[r][1],
+                               sq[r][7], sq[r][0], sq[r][8]);
+        const float sxy_u = fmaf(syy, a.idy2, sxx * a.idx2);
+        const float sz_u = szz * a.idz2;
+        float snx = fmaf(a.dt2, fmaf(a11, sxy_u, a13 * sz_u), 2.f * sc - pl[2 * T + pi]);
+        float snz = fmaf(a.dt2, fmaf(a13, sxy_u, a33 * sz_u), 2.f * sq[r][4] - pl[3 * T + pi]);
+        if (x == a.src.x && y == a.src.y && z == a.src.z) {
+          snx += a.src.amp;
+          snz += a.src.amp;
+        }
+        // imaging with the current adjoint
+        const float lc = lh[sr];
+        const float lz0 = lq[r][4];
+        const float g11 = fmaf(lc, sxy_u, pl[9 * T + pi]);
+        const float g33 = fmaf(lz0, sz_u, pl[11 * T + pi]);
+        const float g13 = fmaf(lz0, sxy_u, fmaf(lc, sz_u, pl[10 * T + pi]));
+        // adjoint, forward form with the sponge
+        const float lxx = lap9(lc, lh[sr - 1], lh[sr + 1], lh[sr - 2], lh[sr + 2], lh[sr - 3],
+                               lh[sr + 3], lh[sr - 4], lh[sr + 4]);
+        const float lyy = lap9(lc, lh[sr - HX], lh[sr + HX], lh[sr - 2 * HX], lh[sr + 2 * HX],
+                               lh[sr - 3 * HX], lh[sr + 3 * HX], lh[sr - 4 * HX], lh[sr + 4 * HX]);
+        const float lzz = lap9(lz0, lq[r][3], lq[r][5], lq[r][2], lq[r][6], lq[r][1], lq[r][7],
+                               lq[r][0], lq[r][8]);
+        const float lxy = fmaf(lyy, a.sy, lxx * a.sx);
+        const float lzs = lzz * a.sz;
+        const float dd = dxy[r] * dz;
+        const float lnx = fmaf(a11, lxy, fmaf(a13, lzs, 2.f * lc - dd * pl[4 * T + pi]));
+        const float lnz = fmaf(a13, lxy, fmaf(a33, lzs, 2.f * lz0 - dd * pl[5 * T + pi]));
+        if (valid[r]) {
+          const long long i = (long long)z * d.plane + off[r];
+          a.spx[i] = snx;
+          a.spz[i] = snz;
+          a.lpx[i] = dd * lnx;
+          a.lpz[i] = dd * lnz;
+          a.g11[i] = g11;
+          a.g13[i] = g13;
+          a.g33[i] = g33;
+        }
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[s]);
+      if (((z + 1) & 3) == 0 && z + 1 < d.nz) {
+#pragma unroll
+        for (int r = 0; r < RY; ++r) {
+#pragma unroll
+          for (int kk = 0; kk < 4; ++kk) lq[r][kk + 1] *= dxy[r] * a.dampz[z - 3 + kk];
+        }
       }
     }
   }
@@ -480,14 +503,34 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
+// Segment length: the smallest modelled time, counted in plane-steps of one
+// CTA, waves * (seg + restart), where a wave is one item per resident slot
+// and a restart (8 queue planes read with plain loads, pipeline refill) costs
+// about kRestart plane-steps.
 Sched make_sched(vti_ctx* ctx, const Dims3& d, int ctas_per_sm) {
+  constexpr long long kRestart = 4;
   Sched s;
-  s.gx = (d.nx - 2 * kHalo + TX - 1) / TX;
+  s.gx = (d.nx - kHalo + TX - 1) / TX;  // x origins 0, 32, ...; updated x < nx-4
   s.gy = (d.ny - 2 * kHalo + TY - 1) / TY;
   s.nz = d.nz;
-  s.total = (long long)s.gx * s.gy * d.nz;
-  long long ctas = (long long)ctx->sm_count * ctas_per_sm;
-  s.per_cta = (s.total + ctas - 1) / ctas;
+  const long long cols = (long long)s.gx * s.gy;
+  const long long slots = (long long)ctx->sm_count * ctas_per_sm;
+  long long best = -1;
+  for (int nseg = 1; nseg <= d.nz; ++nseg) {
+    const int seg = (d.nz + nseg - 1) / nseg;
+    if (nseg > 1 && seg < 8) break;  // at least 8 planes per queue start
+    if (nseg > 1 && seg == (d.nz + nseg - 2) / (nseg - 1)) continue;  // same seg
+    const long long items = cols * ((d.nz + seg - 1) / seg);
+    if (items > (1LL << 30)) break;
+    const long long waves = (items + slots - 1) / slots;
+    const long long cost = waves * (seg + kRestart);
+    if (best < 0 || cost < best) {
+      best = cost;
+      s.seg = seg;
+      s.items = (int)items;
+    }
+  }
+  s.grid = (int)std::min<long long>(s.items, slots);
   return s;
 }
 
@@ -542,7 +585,7 @@ int launch_fwd3d_tma(vti_ctx* ctx, const Dims3& d, const TileMaps& cx, const Til
   a.sz = sz;
   a.src = src;
   a.status = ctx->d_status;
-  const int grid = (int)((a.sc.total + a.sc.per_cta - 1) / a.sc.per_cta);
+  const int grid = a.sc.grid;
   {
     LaunchTimer tm(ctx, kTimedFwd3d);
     k_fwd3d_tma<<<grid, NTHREADS, F_SMEM, ctx->stream>>>(*H(cx), *P(cz), *P(px), *P(pz), *P(c11),
@@ -583,7 +626,7 @@ int launch_bwd3d_tma(vti_ctx* ctx, const Dims3& d, const TileMaps& scx, const Ti
   a.sx = sx; a.sy = sy; a.sz = sz;
   a.src = src;
   a.status = ctx->d_status;
-  const int grid = (int)((a.sc.total + a.sc.per_cta - 1) / a.sc.per_cta);
+  const int grid = a.sc.grid;
   {
     LaunchTimer tm(ctx, kTimedBwd3d);
     k_bwd3d_tma<<<grid, NTHREADS, B_SMEM, ctx->stream>>>(m, a);
