@@ -183,6 +183,17 @@ int vti3d_gradient_vepsdel(vti_ctx* ctx, const vti3d_geom* g, const float* v, co
 int vti2d_synthetic(vti_ctx* ctx, const vti2d_geom* g, const float* c11, const float* c13,
                     const float* c33, const float* wavelet, const int* sloc, int ns,
                     const int* rloc, int nr, const float* taper, float* data);
+/* Same arguments and results as vti2d_synthetic, without any device
+ * allocation: all device data of a call sits in one static 40 MiB array per
+ * device (need = 8*nnx*nnz + nt + nri + rows*nri floats; larger calls return
+ * VTI_ERR_ARG). For callers that may not allocate inside a call. The first
+ * call on a device does the set-up (looks up the array's address) and should
+ * come before any stream capture. Overlapping calls on one device race on the
+ * shared array: serialise them. No counterpart in the reference. */
+int vti2d_synthetic_noalloc(vti_ctx* ctx, const vti2d_geom* g, const float* c11,
+                            const float* c13, const float* c33, const float* wavelet,
+                            const int* sloc, int ns, const int* rloc, int nr,
+                            const float* taper, float* data);
 /* modeling_f (modeling_f.cu:10): sigma_h snapshots wavefield[(it/ratio)*nnxz + i]. */
 int vti2d_modeling(vti_ctx* ctx, const vti2d_geom* g, const float* c11, const float* c13,
                    const float* c33, const float* wavelet, int slocxz, const float* taper,

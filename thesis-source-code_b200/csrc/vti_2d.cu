@@ -10,8 +10,10 @@
 // One fused kernel per time step: stencil + source + taper; receivers are
 // recorded by a small gather kernel. The source amplitudes of all steps are
 // uploaded once, so every step's launch differs only in its buffer pointers.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 
 #include "vti_internal.h"
 
@@ -266,3 +268,164 @@ int vti2d_modeling(vti_ctx* ctx, const vti2d_geom* g, const float* c11, const fl
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free synthetic traces.
+//
+// vti2d_synthetic_noalloc() computes what vti2d_synthetic() computes (same
+// kernels, same launch order, same host arithmetic) but never allocates
+// device memory: the model, the four wavefields, the source amplitudes, the
+// receiver indices and the trace rows of one shot all live in one file-scope
+// static device array of kNoAllocFloats floats (40 MiB), reserved once when
+// this module is loaded.
+//
+// Who needs it: callers that must not allocate inside a call. cudaMalloc and
+// cudaFree synchronise the whole device, so a caller that keeps other streams
+// busy (a 3D gradient running beside 2D modeling, say) would see them stall
+// at every call; a long-running job that shares the GPU can find cudaMalloc
+// failing for lack of memory hours after start-up, while a static
+// reservation either exists from the first call on or never; and hosts that
+// give the library a fixed memory budget forbid allocations inside calls.
+//
+// Limits and rules:
+//  * need = 8*nnx*nnz + nt + nri + rows*nri floats (rows =
+//    (nt-ntNeg-1)/ratio + 1, nri the largest shot's receiver count); a call
+//    that needs more than kNoAllocFloats is rejected with VTI_ERR_ARG before
+//    any work is queued. A 1000 x 1000 padded grid with nt = 4000 and 1000
+//    receivers per shot sampled every 4 steps fits.
+//  * The first call on a device (that device current) looks up the array's
+//    address with cudaGetSymbolAddress and caches it; make that first call
+//    before any stream capture begins.
+//  * The wavefields and the trace rows must start at zero for every shot;
+//    they are cleared with cudaMemsetAsync on the context stream (the model,
+//    amplitudes and receiver indices are overwritten by copies).
+//  * There is one array per device and process: calls that overlap in time on
+//    the same device (two threads, two contexts, two streams) race on it and
+//    corrupt each other's results. Serialise them.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kNoAllocFloats = (size_t)10 << 20;  // 40 MiB
+__device__ __align__(256) float g_noalloc_scratch[kNoAllocFloats];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+float* g_noalloc_ptr[kMaxDevices] = {};
+
+// Address of this device's scratch array; looked up once per device.
+int noalloc_scratch(vti_ctx* ctx, float** out) {
+  if (ctx->device < 0 || ctx->device >= kMaxDevices)
+    return fail(ctx, VTI_ERR_ARG, "device index beyond the allocation-free table");
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[ctx->device]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_check(ctx, e, "cudaGetSymbolAddress(static scratch)");
+    g_noalloc_ptr[ctx->device] = (float*)p;
+  }
+  *out = g_noalloc_ptr[ctx->device];
+  return VTI_OK;
+}
+
+}  // namespace
+
+extern "C" int vti2d_synthetic_noalloc(vti_ctx* ctx, const vti2d_geom* g, const float* c11,
+                                       const float* c13, const float* c33, const float* wavelet,
+                                       const int* sloc, int ns, const int* rloc, int nr,
+                                       const float* taper, float* data) {
+  if (!ctx || !g || !sloc || (nr > 0 && !rloc) || !c11 || !c13 || !c33 || !wavelet || !taper ||
+      !data)
+    return VTI_ERR_ARG;
+  const int nnx = g->nx + 2 * g->npad, nnz = g->nz + 2 * g->npad;
+  const long long nnxz = (long long)nnx * nnz;
+  if (nnx < 9 || nnz < 9 || g->nt < 2 || !(g->dt > 0) || !(g->rate > 0))
+    return fail(ctx, VTI_ERR_ARG, "2D geometry out of range");
+  const float dt = g->dt, dt2 = dt * dt;
+  const int ratio = (int)(g->rate / dt + 0.5f);  // as vti2d_synthetic
+  if (ratio < 1) return fail(ctx, VTI_ERR_ARG, "rate < dt");
+  const int ntNeg = (int)std::round(std::fabs(g->ot) / dt);
+  const long long rows = (g->nt - ntNeg - 1) / ratio + 1;
+  // validate every shot and size the largest before queuing anything
+  long long max_nri = 0;
+  for (int is = 0; is < ns; ++is) {
+    const int* s = sloc + 4 * is;
+    if (s[2] < 0 || s[3] < 0 || s[3] + s[2] > nr)
+      return fail(ctx, VTI_ERR_ARG, "2D shot receiver range exceeds rloc");
+    const long long src = s[0] + (long long)s[1] * nnx;
+    if (src < 0 || src >= nnxz) return fail(ctx, VTI_ERR_ARG, "2D source outside the grid");
+    for (int ir = 0; ir < s[2]; ++ir) {
+      const int x = rloc[2 * (s[3] + ir)], z = rloc[2 * (s[3] + ir) + 1];
+      if (x < 0 || x >= nnx || z < 0 || z >= nnz)
+        return fail(ctx, VTI_ERR_ARG, "2D receiver outside the grid");
+    }
+    max_nri = std::max<long long>(max_nri, s[2]);
+  }
+  const long long need = 8 * nnxz + g->nt + max_nri + rows * max_nri;
+  if (need > (long long)kNoAllocFloats) {
+    char msg[200];
+    std::snprintf(msg, sizeof msg,
+                  "allocation-free modeling needs %lld floats of static scratch, capacity %zu",
+                  need, kNoAllocFloats);
+    return fail(ctx, VTI_ERR_ARG, msg);
+  }
+  VTI_CUDA(ctx, cudaSetDevice(ctx->device));
+  float* buf = nullptr;
+  int st = noalloc_scratch(ctx, &buf);
+  if (st != VTI_OK) return st;
+  float *dc11 = buf, *dc13 = dc11 + nnxz, *dc33 = dc13 + nnxz, *dtap = dc33 + nnxz;
+  float* w[4] = {dtap + nnxz, dtap + 2 * nnxz, dtap + 3 * nnxz, dtap + 4 * nnxz};
+  float* amps = dtap + 5 * nnxz;
+  int* d_ridx = reinterpret_cast<int*>(amps + g->nt);
+  float* d_rows = amps + g->nt + max_nri;
+  cudaStream_t sm = ctx->stream;
+  VTI_CUDA(ctx, cudaMemcpyAsync(dc11, c11, nnxz * 4, cudaMemcpyHostToDevice, sm));
+  VTI_CUDA(ctx, cudaMemcpyAsync(dc13, c13, nnxz * 4, cudaMemcpyHostToDevice, sm));
+  VTI_CUDA(ctx, cudaMemcpyAsync(dc33, c33, nnxz * 4, cudaMemcpyHostToDevice, sm));
+  VTI_CUDA(ctx, cudaMemcpyAsync(dtap, taper, nnxz * 4, cudaMemcpyHostToDevice, sm));
+  std::vector<float> h_amp(g->nt, 0.f);
+  for (int it = 2; it < g->nt; ++it) h_amp[it] = dt2 * wavelet[it - 1];
+  VTI_CUDA(ctx, cudaMemcpyAsync(amps, h_amp.data(), g->nt * 4, cudaMemcpyHostToDevice, sm));
+  const float idx2 = 1.f / (g->dx * g->dx), idz2 = 1.f / (g->dz * g->dz);
+  const dim3 block(BX, BZ), grid((nnx - 8 + BX - 1) / BX, (nnz - 8 + BZ - 1) / BZ);
+  std::vector<int> ridx;
+  for (int is = 0; is < ns; ++is) {
+    const int* s = sloc + 4 * is;
+    const int slocxz = s[0] + s[1] * nnx, nri = s[2], ir0 = s[3];
+    VTI_CUDA(ctx, cudaMemsetAsync(w[0], 0, 4 * nnxz * 4, sm));  // wavefields start at zero
+    if (nri > 0) {
+      ridx.resize(nri);
+      for (int ir = 0; ir < nri; ++ir)
+        ridx[ir] = rloc[2 * (ir0 + ir)] + rloc[2 * (ir0 + ir) + 1] * nnx;
+      VTI_CUDA(ctx, cudaMemcpyAsync(d_ridx, ridx.data(), nri * sizeof(int),
+                                    cudaMemcpyHostToDevice, sm));
+      VTI_CUDA(ctx, cudaMemsetAsync(d_rows, 0, (size_t)rows * nri * 4, sm));  // row 0 stays 0
+    }
+    // time level 1: source then taper (synthetic_f.cu:86-89)
+    k_init2d<<<1, 1, 0, sm>>>(w[2], w[3], slocxz, dt2 * wavelet[0], taper[slocxz]);
+    ctx->launches++;
+    float *p1 = w[2], *q1 = w[3], *p0 = w[0], *q0 = w[1];
+    auto record = [&](long long row, const float* p, const float* q) {
+      if (nri > 0) {
+        k_record2d<<<(nri + 127) / 128, 128, 0, sm>>>(d_rows, row * nri, p, q, d_ridx, nri);
+        ctx->launches++;
+      }
+    };
+    if (ratio == 1 && g->ot == 0.f) record(1, p1, q1);
+    for (int it = 2; it < g->nt; ++it) {
+      const float t = it * dt + g->ot;
+      Step2d a{nnx, nnz, p1, q1, p0, q0, dc11, dc13, dc33, dtap, idx2, idz2, dt2, slocxz,
+               amps + it};
+      k_step2d<<<grid, block, 0, sm>>>(a);
+      ctx->launches++;
+      if (t >= 0.f && (it - ntNeg) % ratio == 0) record((it - ntNeg) / ratio, p0, q0);
+      std::swap(p0, p1);
+      std::swap(q0, q1);
+    }
+    VTI_CUDA(ctx, cudaGetLastError());
+    if (nri > 0)  // the caller's receiver-fastest layout, as vti2d_synthetic
+      VTI_CUDA(ctx, cudaMemcpy2DAsync(data + ir0, (size_t)nr * 4, d_rows, (size_t)nri * 4,
+                                      (size_t)nri * 4, rows, cudaMemcpyDeviceToHost, sm));
+  }
+  VTI_CUDA(ctx, cudaStreamSynchronize(sm));
+  return VTI_OK;
+}

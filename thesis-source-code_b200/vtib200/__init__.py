@@ -92,6 +92,7 @@ def _signatures():
         "vti3d_gradient_cij": (C.c_int, [P, P, P, P, P, P, P, P, C.c_int, P, C.c_int, P, P,
                                          C.POINTER(C.c_double), C.c_uint]),
         "vti2d_synthetic": (C.c_int, [P, P, P, P, P, P, P, C.c_int, P, C.c_int, P, P]),
+        "vti2d_synthetic_noalloc": (C.c_int, [P, P, P, P, P, P, P, C.c_int, P, C.c_int, P, P]),
         "vti2d_modeling": (C.c_int, [P, P, P, P, P, P, C.c_int, P, P]),
         "vti2d_init_taper": (None, [P, C.c_int, C.c_int, C.c_int]),
         "vti2d_gradient": (C.c_int, [P] * 11 + [C.c_int, P, C.c_int, P, C.POINTER(C.c_double)]),
