@@ -149,6 +149,14 @@ int vti3d_plan_gradient(vti3d_plan* plan, const float* souloc, const int* shotid
 /* Misfit only (objFuncCij3d_f, objFuncGradient3d_f.cu:1272). */
 int vti3d_plan_objfunc(vti3d_plan* plan, const float* souloc, const int* shotid, int nshot,
                        const float* dobs, int dobs_mem, double* misfit);
+/* Reverse-time migration (rtmCij3d_f, lib/vti-fwi-3d/gpu/rtm3d_f.cu:161-620):
+ * image (nxyz, zeroed first) = sum over shots of the zero-lag product
+ * (2/3 sx + 1/3 sz)(2/3 lx + 1/3 lz) of the back-propagated source wavefield
+ * and the receiver wavefield driven by the traces `data` (nnt x nrec_total,
+ * trace-major). Uses the random-boundary model if one was set, else the
+ * model; no sponge on the source wavefield. */
+int vti3d_plan_rtm(vti3d_plan* plan, const float* souloc, const int* shotid, int nshot,
+                   const float* data, int data_mem, float* image, int image_mem);
 /* Device pointer of the last forward wavefield sigma_x (pitched volume). */
 const float* vti3d_plan_wavefield(vti3d_plan* plan);
 /* Copies the last forward level of sigma_x (the "wavefield" output of
@@ -164,6 +172,11 @@ int vti3d_gradient_cij(vti_ctx* ctx, const vti3d_geom* g, const float* cij, cons
                        const float* randb, const float* wavelet, const float* souloc,
                        const int* shotid, int nshot, const float* recloc, int nrec_total,
                        const float* dobs, float* fgcij, double* misfit, unsigned flags);
+/* rtmCij3d_f with host buffers: the model as given (rtm3d_f.cu:161). */
+int vti3d_rtm_cij(vti_ctx* ctx, const vti3d_geom* g, const float* c11, const float* c13,
+                  const float* c33, const float* wavelet, const float* souloc, const int* shotid,
+                  int nshot, const float* recloc, int nrec_total, const float* data,
+                  float* image, unsigned flags);
 
 /* objFuncGradientVEpsDel (objFuncGradient3d_f.cu:249-305): gradient of the
  * L2 misfit with respect to v, eps, del (nxyz each). padboundary_v /
@@ -211,6 +224,14 @@ int vti2d_gn_hessian(vti_ctx* ctx, const vti2d_geom* g, float* gc11, float* gc13
                      const float* c11, const float* c13, const float* c33, const float* dc11,
                      const float* dc13, const float* dc33, const float* wavelet, const int* sloc,
                      int ns, const int* rloc, int nr, const float* taper);
+/* rtm_f (lib/vti-fwi-2d/rtm_f.cu:13): reverse-time migration of the traces
+ * data[(it/ratio)*nr + ir] (the layout vti2d_synthetic writes) into image
+ * ((nx+2npad)*(nz+2npad) floats, zeroed first, summed over shots). Dipole
+ * source and data injection; the source and the point below it must lie in
+ * the updated region. */
+int vti2d_rtm(vti_ctx* ctx, const vti2d_geom* g, float* image, const float* data,
+              const float* c11, const float* c13, const float* c33, const float* wavelet,
+              const int* sloc, int ns, const int* rloc, int nr, const float* taper);
 /* 2D taper of lib/vti-fwi-2d/init.cpp:70-89 ((nx+2npad)*(nz+2npad) floats). */
 void vti2d_init_taper(float* taper, int nx, int nz, int npad);
 

@@ -64,6 +64,19 @@ double objFuncGradientVEpsDel(float* gv, float* geps, float* gdel, float* souloc
                               float samplingRate, float v0, float eps0, float wbottom,
                               std::vector<int>& GPUs, int ngpugroup);
 
+// wave3d.h:88 — reverse-time migration of the traces in data= with the model
+// as given; recloc holds three floats (x, y, z) per receiver. Devices from gpu=.
+void rtmCij3d_f(float* image, float* souloc, int ns, std::vector<int>& shotid, float* recloc,
+                float* wavelet, float* c11, float* c13, float* c33, int nx, int ny, int nz,
+                int nt, int npad, float ox, float oy, float oz, float ot, float dx, float dy,
+                float dz, float dt, float samplingRate);
+
+// wave3d.h:90 — the same from v, eps, del; pad region and water layer zeroed.
+void rtmVEpsDel(float* image, float* souloc, int ns, std::vector<int>& shotid, float* recloc,
+                float* wavelet, float* v, float* eps, float* del, float* randboundaryV, int nx,
+                int ny, int nz, int nt, int npad, float ox, float oy, float oz, float ot,
+                float dx, float dy, float dz, float dt, float samplingRate, float wbottom);
+
 // wave3d.h:108 / :110 — forward modeling into memory, ddata[nnt*irbegin ...].
 void modelData3d_f(float* ddata, float* souloc, int ns, std::vector<int>& shotid, float* recloc,
                    const float* wavelet, float* c11, float* c13, float* c33, int nx, int ny,
@@ -121,5 +134,11 @@ void GNhessianVEpsDel(float* gv, float* geps, float* gdel, const float* d0, floa
                       const int* rloc, int nr, const float* taper, int nx, int nz, int nt,
                       int npad, float dx, float dz, float dt, float rate, float ot, float wbottom,
                       float* m);
+
+// wave.h:6 — reverse-time migration of data[(it/ratio)*nr + ir].
+void rtm_f(float* image, const float* data, const float* c11, const float* c13, const float* c33,
+           const float* wavelet, const int* sloc, int ns, const int* rloc, int nr,
+           const float* taper, int nx, int nz, int nt, int npad, float dx, float dz, float dt,
+           float rate, float ot = 0.);
 
 #endif  // VTI_WAVE_H

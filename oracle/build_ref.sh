@@ -1,8 +1,8 @@
 #!/usr/bin/env bash
 # Compiles the reference's own VTI GPU path from its sources where they lie
 # under /root/reference (read-only; nothing is copied) into oracle/_ref/:
-#   ref3d : lib/vti-fwi-3d/gpu 3D modeling + gradient (+ the host glue they link)
-#   ref2d : lib/vti-fwi-2d synthetic_f / modeling_f / objFuncGradient_f / GNhessian_f
+#   ref3d : lib/vti-fwi-3d/gpu 3D modeling, gradient, RTM (+ the host glue they link)
+#   ref2d : lib/vti-fwi-2d synthetic_f / modeling_f / objFuncGradient_f / GNhessian_f / rtm_f
 # linked with the small harnesses oracle/ref_driver{3d,2d}.cpp. Outputs go only
 # to oracle/_ref/ (git-ignored). The binaries run on a GPU host to produce the
 # golden fixtures under tests/golden/ (tests/golden/make_golden.py).
@@ -35,7 +35,7 @@ build_objs() {  # dir outdir files...
 }
 
 # 3D path (objFuncGradient3d_f.cu, modelData3d_f.cu and what they link)
-build_objs "$L3" "$OUT/obj3d" objFuncGradient3d_f.cu modelData3d_f.cu kernel3d.cu \
+build_objs "$L3" "$OUT/obj3d" objFuncGradient3d_f.cu modelData3d_f.cu rtm3d_f.cu kernel3d.cu \
   injectRecord3d.cu abc3d.cu memcpy3d.cu boundary.cpp agc.cpp cluster.cpp
 build_objs "$L2" "$OUT/obj3d" conversions.cpp check.cpp
 build_objs "$IO" "$OUT/obj3d" myio.cpp
@@ -44,7 +44,7 @@ build_objs "$IO" "$OUT/obj3d" myio.cpp
 
 # 2D path (synthetic_f.cu, modeling_f.cu)
 build_objs "$L2" "$OUT/obj2d" kernels.cu synthetic_f.cu modeling_f.cu objFuncGradient_f.cu \
-  hessian_f.cu check.cpp conversions.cpp
+  hessian_f.cu rtm_f.cu check.cpp conversions.cpp
 build_objs "$IO" "$OUT/obj2d" myio.cpp
 "$NVCC" $FLAGS -x cu -c "$HERE/ref_driver2d.cpp" -o "$OUT/obj2d/ref_driver2d.o"
 "$NVCC" $ARCH -Xcompiler -fopenmp -o "$OUT/ref2d" "$OUT"/obj2d/*.o

@@ -34,6 +34,9 @@ def lib():
             f = getattr(L, f"orc3d_gradient_cij_{suf}")
             f.argtypes = [VP] * 8 + [C.c_int, VP, VP, VP, C.c_int, VP]
             f.restype = C.c_int
+            f = getattr(L, f"orc3d_rtm_{suf}")
+            f.argtypes = [VP] * 8 + [C.c_int, VP, VP, VP]
+            f.restype = C.c_int
             f = getattr(L, f"orc2d_forward_{suf}")
             f.argtypes = [VP] * 7 + [C.c_int, VP, C.c_int, VP, VP, C.c_int]
             f.restype = C.c_int
@@ -48,7 +51,9 @@ def lib():
 
 
 def _p(a):
-    return None if a is None else C.c_void_p(a.ctypes.data)
+    # data_as keeps a reference to the array, so a temporary made by _f32()
+    # for this call lives until the call returns
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
 
 
 def _f32(a):
@@ -103,6 +108,20 @@ def gradient3d(g, cij, padb, randb, wavelet, souloc, shotid, recloc, dobs, dtype
         _p(_f32(souloc)), _p(shotid), len(shotid), _p(recloc), _p(_f32(dobs)), _p(out),
         1 if misfit_only else 0, _p(mod))
     return (out, mod) if want_modeled else out
+
+
+def rtm3d(g, c11, c13, c33, wavelet, souloc, shotid, recloc, data, dtype=np.float64,
+          full_steps=False):
+    """rtmCij3d_f restated: the zero-lag image (nxyz), summed over shots."""
+    ip, fp = _geo3(g, full_steps)
+    out = np.zeros(g.nx * g.ny * g.nz, dtype=dtype)
+    suf = "f64" if dtype == np.float64 else "f32"
+    shotid = _i32(shotid)
+    getattr(lib(), f"orc3d_rtm_{suf}")(
+        _p(ip), _p(fp), _p(_f32(c11)), _p(_f32(c13)), _p(_f32(c33)), _p(_f32(wavelet)),
+        _p(_f32(souloc)), _p(shotid), len(shotid), _p(_f32(recloc).reshape(-1)), _p(_f32(data)),
+        _p(out))
+    return out
 
 
 def damping3d(nx, ny, nz, npad):
@@ -160,6 +179,22 @@ def time_backward_f32(g, c11, c13, c33, nsteps):
     scratch = np.zeros(11 * n, dtype=np.float32)
     return lib().orc3d_time_backward_f32(_p(ip), _p(fp), _p(_f32(c11)), _p(_f32(c13)),
                                          _p(_f32(c33)), nsteps, _p(scratch))
+
+
+def rtm2d(g, c11, c13, c33, wavelet, sloc, rloc, taper, data, dtype=np.float64):
+    """rtm_f restated: the image (nnxz), summed over shots."""
+    suf = "f64" if dtype == np.float64 else "f32"
+    f = getattr(lib(), f"orc2d_rtm_{suf}")
+    f.argtypes = [VP] * 8 + [C.c_int, VP, C.c_int, VP, VP]
+    f.restype = C.c_int
+    ip = np.array([g.nx, g.nz, g.nt, g.npad], dtype=np.int32)
+    fp = np.array([g.dx, g.dz, g.dt, g.rate, g.ot], dtype=np.float32)
+    out = np.zeros((g.nx + 2 * g.npad) * (g.nz + 2 * g.npad), dtype=dtype)
+    sloc, rloc = _i32(sloc).reshape(-1), _i32(rloc).reshape(-1)
+    f(_p(ip), _p(fp), _p(_f32(c11)), _p(_f32(c13)), _p(_f32(c33)), _p(_f32(wavelet)),
+      _p(_f32(data)), _p(sloc), sloc.size // 4, _p(rloc), rloc.size // 2, _p(_f32(taper)),
+      _p(out))
+    return out
 
 
 def gradient2d(g, c11, c13, c33, wavelet, sloc, rloc, taper, data=None, dc=None,

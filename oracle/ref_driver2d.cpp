@@ -2,7 +2,7 @@
 // sources by oracle/build_ref.sh into oracle/_ref/ref2d) on inputs written by
 // tests/golden/make_golden.py. TEST INFRASTRUCTURE ONLY.
 //
-// usage: ref2d <dir> synthetic|modeling
+// usage: ref2d <dir> synthetic|modeling|grad|gnhess|rtm
 //   <dir>/params.txt : nx nz nt npad dx dz dt rate ot ns nr
 //   <dir>/{c11,c13,c33,taper,wavelet}.bin (float32), sloc.bin / rloc.bin (int32)
 #include <cstdio>
@@ -31,6 +31,11 @@ void GNhessian_f(float* gc11, float* gc13, float* gc33, const float* data, const
                  const float* dc33, const float* wavelet, const int* sloc, int ns, const int* rloc,
                  int nr, const float* taper, int nx, int nz, int nt, int npad, float dx, float dz,
                  float dt, float rate, float ot);
+
+void rtm_f(float* image, const float* data, const float* c11, const float* c13, const float* c33,
+           const float* wavelet, const int* sloc, int ns, const int* rloc, int nr,
+           const float* taper, int nx, int nz, int nt, int npad, float dx, float dz, float dt,
+           float rate, float ot);
 
 template <typename T>
 static std::vector<T> load(const std::string& path, size_t n) {
@@ -110,6 +115,17 @@ int main(int argc, char** argv) {
                   rate, ot);
     }
     save(dir + "/ref_" + mode + ".bin", g.data(), g.size());
+  } else if (mode == "rtm") {
+    // <dir>/data.bin: the traces to migrate (receiver-fastest rows)
+    auto rloc = load<int>(dir + "/rloc.bin", 2 * (size_t)nr);
+    const int ratio = (int)(rate / dt + 0.5f);
+    const int ntneg = (int)(ot < 0 ? (-ot / dt + 0.5f) : 0);
+    const size_t rows = (nt - ntneg - 1) / ratio + 1;
+    auto data = load<float>(dir + "/data.bin", rows * nr);
+    std::vector<float> image(nnxz, 0.f);
+    rtm_f(image.data(), data.data(), c11.data(), c13.data(), c33.data(), wavelet.data(),
+          sloc.data(), ns, rloc.data(), nr, taper.data(), nx, nz, nt, npad, dx, dz, dt, rate, ot);
+    save(dir + "/ref_rtm.bin", image.data(), image.size());
   } else {
     return 2;
   }

@@ -3,10 +3,11 @@
 // tests/golden/make_golden.py. TEST INFRASTRUCTURE ONLY: it produces golden
 // traces and gradients that pin the oracle; nothing in the library uses it.
 //
-// usage: ref3d <dir> model|grad
+// usage: ref3d <dir> model|grad|rtm
 //   <dir>/params.txt : nx ny nz nt npad ox oy oz ot dx dy dz dt rate ns nrec
 //   <dir>/{souloc,recloc,wavelet,cij,padb,randb,dobs}.bin (float32)
-//   writes <dir>/ref_ddata.bin (model) or <dir>/ref_fgcij.bin (grad)
+//   writes <dir>/ref_ddata.bin (model), <dir>/ref_fgcij.bin (grad) or
+//   <dir>/ref_image.bin (rtm: the traces in dobs.bin migrated with cij)
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
@@ -25,6 +26,10 @@ void objFuncGradientCij3d_f(float* fgcij, float* souloc, int ns, std::vector<int
                             float* randboundaryCij, int nx, int ny, int nz, int nt, int npad,
                             float ox, float oy, float oz, float ot, float dx, float dy, float dz,
                             float dt, float samplingRate, std::vector<int>& GPUs);
+void rtmCij3d_f(float* image, float* souloc, int ns, std::vector<int>& shotid, float* recloc,
+                float* wavelet, float* c11, float* c13, float* c33, int nx, int ny, int nz,
+                int nt, int npad, float ox, float oy, float oz, float ot, float dx, float dy,
+                float dz, float dt, float samplingRate);
 
 static std::vector<float> load(const std::string& path, size_t n) {
   std::vector<float> v(n);
@@ -48,7 +53,7 @@ static void save(const std::string& path, const float* p, size_t n) {
 
 int main(int argc, char** argv) {
   if (argc < 3) {
-    std::fprintf(stderr, "usage: %s <dir> model|grad\n", argv[0]);
+    std::fprintf(stderr, "usage: %s <dir> model|grad|rtm\n", argv[0]);
     return 2;
   }
   const std::string dir = argv[1], mode = argv[2];
@@ -76,9 +81,10 @@ int main(int argc, char** argv) {
     std::ofstream h(hdr);
     h << "in=" << dir << "/dobs.bin\ndata_format=native_float\n";
   }
-  std::string a0 = "ref3d", a1 = "data=" + hdr, a2 = "tpow=0", a3 = "objtype=0";
-  char* av[] = {&a0[0], &a1[0], &a2[0], &a3[0], nullptr};
-  myio_init(4, av);
+  // gpu= is read by rtmCij3d_f (rtm3d_f.cu:164)
+  std::string a0 = "ref3d", a1 = "data=" + hdr, a2 = "tpow=0", a3 = "objtype=0", a4 = "gpu=0";
+  char* av[] = {&a0[0], &a1[0], &a2[0], &a3[0], &a4[0], nullptr};
+  myio_init(5, av);
   if (mode == "model") {
     std::vector<float> ddata((size_t)nnt * nrec, 0.f);
     modelDataCij3d_f(ddata.data(), souloc.data(), ns, shotid, recloc.data(), wavelet.data(),
@@ -93,6 +99,16 @@ int main(int argc, char** argv) {
                            cij.data(), padb.data(), randb.data(), nx, ny, nz, nt, npad, ox, oy,
                            oz, ot, dx, dy, dz, dt, rate, gpus);
     save(dir + "/ref_fgcij.bin", fg.data(), fg.size());
+  } else if (mode == "rtm") {
+    // rtmCij3d_f reads three floats (x, y, z) per receiver (rtm3d_f.cu:347-350)
+    std::vector<float> rec3(3 * (size_t)nrec);
+    for (int ir = 0; ir < nrec; ++ir)
+      for (int k = 0; k < 3; ++k) rec3[3 * ir + k] = recloc[4 * ir + k];
+    std::vector<float> image(n, 0.f);
+    rtmCij3d_f(image.data(), souloc.data(), ns, shotid, rec3.data(), wavelet.data(), cij.data(),
+               cij.data() + n, cij.data() + 2 * n, nx, ny, nz, nt, npad, ox, oy, oz, ot, dx, dy,
+               dz, dt, rate);
+    save(dir + "/ref_image.bin", image.data(), image.size());
   } else {
     std::fprintf(stderr, "unknown mode %s\n", mode.c_str());
     return 2;

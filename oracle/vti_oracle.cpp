@@ -413,6 +413,74 @@ void gradient3d(const Geo3& g, const float* cij_in, const float* padb, const flo
   fgcij[0] = (T)(objfunc / 2);
 }
 
+// rtmCij3d_f (lib/vti-fwi-3d/gpu/rtm3d_f.cu:161-620) for the shots in shotid:
+// pass 1 propagates the source wavefield with the model as given and no
+// sponge (:378-468); after the flip (:495-497) the source wavefield steps back
+// (forward form, source re-injected with w[it+1], :585-600) while the
+// receiver wavefield is seeded with the last data sample (:509-514), stepped
+// with the forward operator, fed the data interpolated at it+1 and damped by
+// the sponge (:586-608); imagingKernel (kernel3d.cu:456-469) then adds
+// (2/3 sx + 1/3 sz)(2/3 lx + 1/3 lz) with both fields at the step's current
+// level, the receiver wavefield already damped by this step's sponge.
+// image is zeroed first and accumulates over shots (rtm3d_f.cu:175).
+template <typename T>
+void rtm3d(const Geo3& g, const float* c11, const float* c13, const float* c33,
+           const float* wavelet, const float* souloc, const int* shotid, int nshot,
+           const float* recloc, const float* data, T* image) {
+  const long n = g.nxyz(), nxy = g.nxy();
+  const float dt2 = g.dt * g.dt;
+  const int st = sampling_step(g.rate, g.dt);
+  const int nnt = (g.nt - 1) / st + 1;
+  const int M = last_level(g);
+  std::fill(image, image + n, (T)0);
+  Damp3 damp(g);
+  std::vector<T> cx, cz, px, pz, lcx, lcz, lpx, lpz;
+  for (int k = 0; k < nshot; ++k) {
+    Shot3 s = make_shot3(g, souloc, recloc, shotid[k]);
+    const float* dat = data + (long)nnt * s.irbegin;
+    forward3d<T>(g, c11, c13, c33, wavelet, s, nullptr, nullptr, cx, cz, px, pz);
+    std::swap(cx, px);
+    std::swap(cz, pz);
+    lcx.assign(n, 0); lcz.assign(n, 0); lpx.assign(n, 0); lpz.assign(n, 0);
+    for (int ir = 0; ir < s.nr; ++ir) {
+      if (!s.inner[ir]) continue;
+      T temp = (T)dt2 * (T)dat[(nnt - 1) + (long)ir * nnt];
+      lcx[s.seed[ir]] = (T)kTwoThird * temp;
+      lcz[s.seed[ir]] = (T)kOneThird * temp;
+    }
+    for (int i = 0; i < M - 1; ++i) {
+      const int it = g.nt - 3 - i;
+      step3d<T, true>(g, c11, c13, c33, cx.data(), cz.data(), px.data(), pz.data(), nullptr,
+                      nullptr, nullptr, nullptr, nullptr, nullptr);
+      const float src = dt2 * wavelet[it + 1];
+      px[s.sidx] += (T)src;
+      pz[s.sidx] += (T)src;
+      step3d<T, true>(g, c11, c13, c33, lcx.data(), lcz.data(), lpx.data(), lpz.data(), &damp,
+                      nullptr, nullptr, nullptr, nullptr, nullptr);
+      for (int ir = 0; ir < s.nr; ++ir) {
+        if (!s.inner[ir]) continue;
+        std::vector<T> tr(dat + (long)ir * nnt, dat + (long)(ir + 1) * nnt);
+        T inj = (T)dt2 * interp_residual<T>(tr.data(), it + 1, nnt, st);
+        long ri = s.ridx[ir];
+        T d = (T)damp.at(ri % nxy, (int)(ri / nxy));
+        lpx[ri] += d * ((T)kTwoThird * inj);
+        lpz[ri] += d * ((T)kOneThird * inj);
+      }
+#pragma omp parallel for collapse(2) schedule(static)
+      for (long iz = 0; iz < g.nz; ++iz)
+        for (long iy = kHalf; iy < g.ny - kHalf; ++iy)
+          for (long ix = kHalf; ix < g.nx - kHalf; ++ix) {
+            const long ixy = ix + iy * g.nx, j = ixy + iz * nxy;
+            const T d = (T)damp.at(ixy, (int)iz);
+            image[j] += ((T)kTwoThird * cx[j] + (T)kOneThird * cz[j]) *
+                        (d * ((T)kTwoThird * lcx[j] + (T)kOneThird * lcz[j]));
+          }
+      std::swap(cx, px); std::swap(cz, pz);
+      std::swap(lcx, lpx); std::swap(lcz, lpz);
+    }
+  }
+}
+
 // ----------------------------------------------------------------- 2D ------
 struct Geo2 {
   int nx, nz, nt, npad;
@@ -456,6 +524,117 @@ void taper2d(const Geo2& g, const float* taper, T* a) {
   const long nnx = g.nnx(), nnz = g.nnz();
   for (long iz = kHalf; iz < nnz - kHalf; ++iz)
     for (long ix = kHalf; ix < nnx - kHalf; ++ix) a[ix + iz * nnx] *= (T)taper[ix + iz * nnx];
+}
+
+// injectDipoleSource / injectDipoleData (kernels.cu:232-256): +a at i, -a one
+// row below.
+template <typename T>
+void dipole2d(const Geo2& g, T* p, T* q, long i, T a) {
+  p[i] += a;
+  q[i] += a;
+  p[i + g.nnx()] -= a;
+  q[i + g.nnx()] -= a;
+}
+
+// rtm_f (lib/vti-fwi-2d/rtm_f.cu:13-267): dipole source; source wavefield
+// slices 0.5(p+q) of the interior at it % ratio == 0 (and level 1 when
+// ratio == 1, recordWavefieldSlice kernels.cu:335-343) kept for the whole
+// shot; the receiver wavefield (forwardCD, data as dipoles interpolated in
+// time, taper) is imaged with imagingCrossCor (kernels.cu:414-423):
+// image += 0.5(p+q) * ((1-f) S0 + f S1). Slices never written are zero (the
+// host array is zero-initialised once, rtm_f.cu:55; the index one past the
+// last slice, read with weight 0 at the first imaging, is taken as zero).
+template <typename T>
+void rtm2d(const Geo2& g, const float* c11, const float* c13, const float* c33,
+           const float* wavelet, const float* data, const int* sloc, int ns, const int* rloc,
+           int nr_total, const float* taper, T* image) {
+  const long nnx = g.nnx(), nnz = g.nnz(), nnxz = nnx * nnz;
+  const float dt = g.dt, dt2 = dt * dt;
+  const int ratio = (int)(g.rate / dt + 0.5f);
+  const int ntNeg = (int)std::round(std::fabs(g.ot) / dt);
+  const int nnt = (g.nt - 1) / ratio + 1;
+  const int nnt_data = (g.nt - ntNeg - 1) / ratio + 1;
+  std::fill(image, image + nnxz, (T)0);
+  std::vector<T> sw((size_t)(nnt + 1) * nnxz, 0);
+  auto slice = [&](int j, const T* p, const T* q) {
+    for (long iz = kHalf; iz < nnz - kHalf; ++iz)
+      for (long ix = kHalf; ix < nnx - kHalf; ++ix) {
+        long i = ix + iz * nnx;
+        sw[(size_t)j * nnxz + i] = (T)0.5f * (p[i] + q[i]);
+      }
+  };
+  auto img = [&](const T* p, const T* q, int s0, int s1, float f) {
+    const T* A = sw.data() + (size_t)s0 * nnxz;
+    const T* B = sw.data() + (size_t)s1 * nnxz;
+    for (long iz = kHalf; iz < nnz - kHalf; ++iz)
+      for (long ix = kHalf; ix < nnx - kHalf; ++ix) {
+        long i = ix + iz * nnx;
+        T d = (1 - (T)f) * A[i] + (T)f * B[i];
+        image[i] += (T)0.5f * (p[i] + q[i]) * d;
+      }
+  };
+  for (int is = 0; is < ns; ++is) {
+    const long sxz = sloc[4 * is] + (long)sloc[4 * is + 1] * nnx;
+    const int nri = sloc[4 * is + 2], ir0 = sloc[4 * is + 3];
+    std::vector<T> p0(nnxz, 0), q0(nnxz, 0), p1(nnxz, 0), q1(nnxz, 0);
+    dipole2d<T>(g, p1.data(), q1.data(), sxz, (T)(dt2 * wavelet[0]));
+    taper2d(g, taper, p1.data());
+    taper2d(g, taper, q1.data());
+    if (ratio == 1) slice(1, p1.data(), q1.data());
+    for (int it = 2; it < g.nt; ++it) {
+      step2d<T>(g, c11, c13, c33, p1.data(), q1.data(), p0.data(), q0.data());
+      dipole2d<T>(g, p0.data(), q0.data(), sxz, (T)(dt2 * wavelet[it - 1]));
+      taper2d(g, taper, p1.data()); taper2d(g, taper, q1.data());
+      taper2d(g, taper, p0.data()); taper2d(g, taper, q0.data());
+      if (it % ratio == 0) slice(it / ratio, p0.data(), q0.data());
+      std::swap(p0, p1);
+      std::swap(q0, q1);
+    }
+    std::fill(p0.begin(), p0.end(), (T)0); std::fill(q0.begin(), q0.end(), (T)0);
+    std::fill(p1.begin(), p1.end(), (T)0); std::fill(q1.begin(), q1.end(), (T)0);
+    std::vector<float> d0(nri, 0.f), d1(nri, 0.f);
+    for (int ir = 0; ir < nri; ++ir) d0[ir] = data[(long)(nnt_data - 1) * nr_total + ir0 + ir];
+    auto inject = [&](T* p, T* q, float f) {
+      for (int ir = 0; ir < nri; ++ir) {
+        long i = rloc[2 * (ir0 + ir)] + (long)rloc[2 * (ir0 + ir) + 1] * nnx;
+        float s = 0.5f * ((1.f - f) * d0[ir] + f * d1[ir]);
+        dipole2d<T>(g, p, q, i, (T)(dt2 * s));
+      }
+    };
+    inject(p0.data(), q0.data(), 0.f);
+    taper2d(g, taper, p0.data());
+    taper2d(g, taper, q0.data());
+    float f = (g.nt - 2.) / ratio;
+    int s0 = (int)f, s1 = s0 + 1;
+    if (s1 > nnt) s1 = nnt;
+    f = f - s0;
+    img(p0.data(), q0.data(), s0, s1, f);
+    for (int it = g.nt - 3; it >= 0; --it) {
+      step2d<T>(g, c11, c13, c33, p0.data(), q0.data(), p1.data(), q1.data());
+      if (it >= ntNeg) {
+        f = (it - ntNeg + 1.) / ratio;
+        int i1 = (int)f;
+        if ((it - ntNeg + 2) % ratio == 0) {
+          for (int ir = 0; ir < nri; ++ir) d1[ir] = data[(long)i1 * nr_total + ir0 + ir];
+          std::swap(d0, d1);
+        }
+        f = f - i1;
+        inject(p1.data(), q1.data(), f);
+      }
+      taper2d(g, taper, p1.data()); taper2d(g, taper, q1.data());
+      taper2d(g, taper, p0.data()); taper2d(g, taper, q0.data());
+      f = (float)it / ratio;
+      int i1 = (int)f;
+      if ((it + 1) % ratio == 0) {
+        s1 = i1;
+        std::swap(s0, s1);
+      }
+      f = f - i1;
+      img(p1.data(), q1.data(), s0, s1, f);
+      std::swap(p0, p1);
+      std::swap(q0, q1);
+    }
+  }
 }
 
 // synthetic_f (synthetic_f.cu:13-124) and modeling_f (modeling_f.cu:10-82).
@@ -830,6 +1009,18 @@ ORC3D_MODEL(float, f32)
 ORC3D_GRAD(double, f64)
 ORC3D_GRAD(float, f32)
 
+#define ORC3D_RTM(T, SUF)                                                                      \
+  int orc3d_rtm_##SUF(const int* ip, const float* fp, const float* c11, const float* c13,       \
+                      const float* c33, const float* wavelet, const float* souloc,              \
+                      const int* shotid, int nshot, const float* recloc, const float* data,     \
+                      T* image) {                                                               \
+    Geo3 g = unpack3(ip, fp);                                                                   \
+    rtm3d<T>(g, c11, c13, c33, wavelet, souloc, shotid, nshot, recloc, data, image);           \
+    return 0;                                                                                   \
+  }
+ORC3D_RTM(double, f64)
+ORC3D_RTM(float, f32)
+
 // Time `nsteps` forward steps (forward form, sponge) of a zero-initialised
 // grid with a point source: the FP32 instance is the CPU baseline's unit of
 // work. Returns the number of threads used.
@@ -893,6 +1084,18 @@ ORC2D_FWD(float, f32)
   }
 ORC2D_GRAD(double, f64)
 ORC2D_GRAD(float, f32)
+
+#define ORC2D_RTM(T, SUF)                                                                       \
+  int orc2d_rtm_##SUF(const int* ip, const float* fp, const float* c11, const float* c13,        \
+                      const float* c33, const float* wavelet, const float* data,                 \
+                      const int* sloc, int ns, const int* rloc, int nr, const float* taper,      \
+                      T* image) {                                                                \
+    Geo2 g = unpack2(ip, fp);                                                                    \
+    rtm2d<T>(g, c11, c13, c33, wavelet, data, sloc, ns, rloc, nr, taper, image);                 \
+    return 0;                                                                                    \
+  }
+ORC2D_RTM(double, f64)
+ORC2D_RTM(float, f32)
 
 // The checkpoint pairing of the 2D gradient: 3 values (a, b, f) per imaging
 // step, nt-1 steps. Returns the number of steps.

@@ -74,3 +74,18 @@ CASES3D = ["g3_a", "g3_b", "g3_c"]
 # gradient is ~1e-35, at the FP32 underflow limit, and not a meaningful check.
 GRAD_CASES3D = ["g3_a", "g3_b"]
 CASES2D = ["g2_a"]
+# RTM fixtures (<case>_rtm.npz): the case's observed traces migrated with its
+# starting model; in 3D the model carries the random boundary, as the RTM
+# drivers pass it (rtm3d_f.cu:139-148).
+RTM_CASES3D = ["g3_a"]
+RTM_CASES2D = ["g2_a"]
+
+
+def rtm_model3d(c: dict) -> np.ndarray:
+    """cij of a 3D case with its random boundary put into the pad region."""
+    import vtib200 as V
+    s = c["s"]
+    n = s.nxyz
+    return np.concatenate([V.put_boundary(c["randb"][k * s.nb:(k + 1) * s.nb],
+                                          c["cij"][k * n:(k + 1) * n], s.nx, s.ny, s.nz,
+                                          s.npad) for k in range(3)])

@@ -112,16 +112,60 @@ def make2d(name, out):
     print(name, "data max", np.abs(data).max())
 
 
+def make_rtm3d(name, out):
+    """rtmCij3d_f of the reference: the case's observed traces (its golden
+    dobs) migrated with the starting model plus random boundary."""
+    c = K.case3d(name)
+    s = c["s"]
+    dobs = np.load(HERE / f"{name}.npz")["dobs"]
+    model = K.rtm_model3d(c)
+    with tempfile.TemporaryDirectory() as td:
+        d = Path(td)
+        write_inputs3d(c, d)
+        model.astype(np.float32).tofile(d / "cij.bin")
+        dobs.astype(np.float32).tofile(d / "dobs.bin")
+        run("ref3d", d, "rtm")
+        image = np.fromfile(d / "ref_image.bin", dtype=np.float32)
+    np.savez_compressed(out / f"{name}_rtm.npz", image=image,
+                        inputs=K.digest(s.souloc, s.recloc, s.wavelet, model, dobs))
+    print(name, "rtm image max", np.abs(image).max())
+
+
+def make_rtm2d(name, out):
+    """rtm_f of the reference: the case's observed traces (golden dobs)
+    migrated with the starting model."""
+    c = K.case2d(name)
+    s = c["s"]
+    dobs = np.load(HERE / f"{name}.npz")["dobs"]
+    with tempfile.TemporaryDirectory() as td:
+        d = Path(td)
+        write_inputs2d(s, d)
+        dobs.astype(np.float32).tofile(d / "data.bin")
+        run("ref2d", d, "rtm")
+        image = np.fromfile(d / "ref_rtm.bin", dtype=np.float32)
+    np.savez_compressed(out / f"{name}_rtm.npz", image=image,
+                        inputs=K.digest(s.c11, s.c13, s.c33, s.taper, s.wavelet, s.sloc, s.rloc,
+                                        dobs))
+    print(name, "rtm image max", np.abs(image).max())
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=str(HERE))
+    ap.add_argument("--only", choices=["all", "rtm"], default="all",
+                    help="rtm: only the RTM fixtures (needs the case fixtures)")
     a = ap.parse_args()
     out = Path(a.out)
     out.mkdir(parents=True, exist_ok=True)
-    for n in K.CASES3D:
-        make3d(n, out)
-    for n in K.CASES2D:
-        make2d(n, out)
+    if a.only == "all":
+        for n in K.CASES3D:
+            make3d(n, out)
+        for n in K.CASES2D:
+            make2d(n, out)
+    for n in K.RTM_CASES3D:
+        make_rtm3d(n, out)
+    for n in K.RTM_CASES2D:
+        make_rtm2d(n, out)
 
 
 if __name__ == "__main__":

@@ -91,3 +91,30 @@ def test_shim_2d_matches_reference(drivers, name):
         sl = slice(k * nnxz, (k + 1) * nnxz)
         assert rel_l2(grad[sl], ref[sl]) < 1e-4, k
         assert rel_l2(gnh[sl], gold["gnhess"][sl]) < 1e-4, k
+
+
+@pytest.mark.parametrize("name", K.RTM_CASES3D)
+def test_shim_rtm3d_matches_reference(drivers, name):
+    """rtmCij3d_f through the drop-in library (three floats per receiver, the
+    traces read from data=) against the reference's own image."""
+    c = K.case3d(name)
+    with tempfile.TemporaryDirectory() as td:
+        d = Path(td)
+        MG.write_inputs3d(c, d)
+        K.rtm_model3d(c).astype(np.float32).tofile(d / "cij.bin")
+        np.asarray(load_golden(name)["dobs"], np.float32).tofile(d / "dobs.bin")
+        _run(drivers["3d"], d, "rtm")
+        img = np.fromfile(d / "ref_image.bin", dtype=np.float32)
+    assert rel_l2(img, load_golden(f"{name}_rtm")["image"]) < 1e-4
+
+
+@pytest.mark.parametrize("name", K.RTM_CASES2D)
+def test_shim_rtm2d_matches_reference(drivers, name):
+    s = K.case2d(name)["s"]
+    with tempfile.TemporaryDirectory() as td:
+        d = Path(td)
+        MG.write_inputs2d(s, d)
+        np.asarray(load_golden(name)["dobs"], np.float32).tofile(d / "data.bin")
+        _run(drivers["2d"], d, "rtm")
+        img = np.fromfile(d / "ref_rtm.bin", dtype=np.float32)
+    assert rel_l2(img, load_golden(f"{name}_rtm")["image"]) < 1e-4

@@ -53,6 +53,23 @@ def test_boundary_get_put_zero(dims):
     np.testing.assert_array_equal(z[~mask], v[~mask])
 
 
+def test_converted_inputs_outlive_the_call():
+    """Float64 inputs are converted to float32 temporaries; those must stay
+    alive until the C call returns. The arrays are large enough that a freed
+    temporary is returned to the system and reading it would fault."""
+    nx, ny, nz, npad = 96, 96, 64, 12
+    rng = np.random.default_rng(3)
+    v = rng.standard_normal(nx * ny * nz).astype(np.float32)
+    b64 = rng.standard_normal(int(_boundary_mask(nx, ny, nz, npad).sum()))
+    w64 = V.put_boundary(b64, v, nx, ny, nz, npad)
+    w32 = V.put_boundary(b64.astype(np.float32), v, nx, ny, nz, npad)
+    np.testing.assert_array_equal(w64, w32)
+    g = V.geom3d(nx, ny, nz, 100, npad, 10.0, 10.0, 10.0, 1e-3, 4e-3)
+    c = np.full(nx * ny * nz, 4.0e6)
+    assert V.cfl_number(g, c, c * 0.5, c) == V.cfl_number(g, *(x.astype(np.float32)
+                                                              for x in (c, c * 0.5, c)))
+
+
 def test_vepsdel_conversion_and_chain_rule():
     rng = np.random.default_rng(1)
     n = 1000

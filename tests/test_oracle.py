@@ -107,6 +107,19 @@ def test_oracle_fp32_tracks_fp64():
     assert rel_l2(d32, d64) < 1e-5
 
 
+def test_oracle_accepts_float64_inputs():
+    """Inputs converted to float32 for the call give the float32 result (the
+    converted copies must live until the call returns)."""
+    c = K.case3d("g3_a")
+    s = c["s"]
+    g = s.geom()
+    dobs = load_golden("g3_a")["dobs"]
+    args = (g, c["cij"], c["padb"], c["randb"], s.wavelet, s.souloc, c["shotid"], s.recloc)
+    a = O.gradient3d(*args, dobs.astype(np.float32), misfit_only=True)
+    b = O.gradient3d(*args, dobs.astype(np.float64), misfit_only=True)
+    assert a[0] == b[0] and a[0] > 0
+
+
 def test_oracle_linear_in_wavelet_and_zero_source():
     s = S.small3d(nx=24, ny=24, nz=20, nt=70, npad=4, rec_step=4)
     g = s.geom()
@@ -142,3 +155,33 @@ def test_reference_truncates_levels():
     g = S.small3d(nt=100).geom()
     assert O.last_level(g) == 1 + 64 * ((100 - 2) // 64) == 65
     assert O.last_level(g, full_steps=True) == 99
+
+
+@pytest.mark.parametrize("name", K.RTM_CASES3D)
+def test_oracle_rtm3d_matches_reference(name):
+    """rtmCij3d_f restated (FP64) against the reference's own image."""
+    c = K.case3d(name)
+    s = c["s"]
+    g = s.geom()
+    n = s.nxyz
+    model = K.rtm_model3d(c)
+    dobs = load_golden(name)["dobs"]
+    gold = load_golden(f"{name}_rtm")
+    assert gold["inputs"] == K.digest(s.souloc, s.recloc, s.wavelet, model, dobs)
+    o = O.rtm3d(g, *_split(model, n), s.wavelet, s.souloc, c["shotid"], s.recloc, dobs)
+    assert np.abs(o).max() > 0
+    assert rel_l2(o, gold["image"]) < 1e-4
+
+
+@pytest.mark.parametrize("name", K.RTM_CASES2D)
+def test_oracle_rtm2d_matches_reference(name):
+    """rtm_f restated (FP64) against the reference's own image."""
+    s = K.case2d(name)["s"]
+    g = s.geom()
+    dobs = load_golden(name)["dobs"]
+    gold = load_golden(f"{name}_rtm")
+    assert gold["inputs"] == K.digest(s.c11, s.c13, s.c33, s.taper, s.wavelet, s.sloc, s.rloc,
+                                      dobs)
+    o = O.rtm2d(g, s.c11, s.c13, s.c33, s.wavelet, s.sloc, s.rloc, s.taper, dobs)
+    assert np.abs(o).max() > 0
+    assert rel_l2(o, gold["image"]) < 1e-4

@@ -118,21 +118,6 @@ struct PointSource {
   float amp = 0.f;             // added to next before the sponge
 };
 
-// One forward-form leapfrog step over the update region
-// (x,y in [4,n-4), all z): next written over prev.
-// damp == nullptr: no sponge (random-boundary pass).
-int launch_fwd3d(vti_ctx* ctx, const Dims3& d, const float* cx, const float* cz, float* px,
-                 float* pz, const float* c11, const float* c13, const float* c33,
-                 const Damping* damp, float sx, float sy, float sz, PointSource src);
-
-// Fused backward step: sigma back one level (gradient form, no sponge, +src),
-// adjoint lambda one level (forward form, sponge), zero-lag imaging into g.
-int launch_bwd3d(vti_ctx* ctx, const Dims3& d, const float* scx, const float* scz, float* spx,
-                 float* spz, const float* lcx, const float* lcz, float* lpx, float* lpz,
-                 const float* c11, const float* c13, const float* c33, float* g11, float* g13,
-                 float* g33, const Damping& damp, float dt2, float idx2, float idy2, float idz2,
-                 float sx, float sy, float sz, PointSource src);
-
 // TMA descriptors (CUtensorMap, 128 bytes each) of one volume: 32 x 16 tiles
 // and 40 x 24 tiles (with the 4-cell halo). Plain storage keeps cuda.h out
 // of this header.
@@ -142,13 +127,17 @@ struct TileMaps {
 };
 int make_tile_maps(vti_ctx* ctx, const Dims3& d, const Vol& v, TileMaps* out);
 
-// TMA-pipelined forward step (see vti_tma3d.cu).
+// One forward-form leapfrog step over the update region (x,y in [4,n-4),
+// all z), next written over prev; damp == nullptr: no sponge (random-boundary
+// pass). TMA-pipelined, see vti_tma3d.cu.
 int launch_fwd3d_tma(vti_ctx* ctx, const Dims3& d, const TileMaps& cx, const TileMaps& cz,
                      const TileMaps& px, const TileMaps& pz, const TileMaps& c11,
                      const TileMaps& c13, const TileMaps& c33, const float* cz_ptr,
                      float* px_ptr, float* pz_ptr, const Damping* damp, float sx, float sy,
                      float sz, PointSource src);
-// TMA-pipelined fused backward step.
+// Fused backward step: sigma back one level (gradient form, no sponge, +src),
+// adjoint lambda one level (forward form, sponge), zero-lag imaging into g
+// (rtm: the RTM image in g11 instead).
 int launch_bwd3d_tma(vti_ctx* ctx, const Dims3& d, const TileMaps& scx, const TileMaps& scz,
                      const TileMaps& spx, const TileMaps& spz, const TileMaps& lcx,
                      const TileMaps& lcz, const TileMaps& lpx, const TileMaps& lpz,
@@ -157,7 +146,7 @@ int launch_bwd3d_tma(vti_ctx* ctx, const Dims3& d, const TileMaps& scx, const Ti
                      const float* scz_ptr, const float* lcz_ptr, float* spx_ptr, float* spz_ptr,
                      float* lpx_ptr, float* lpz_ptr, float* g11_ptr, float* g13_ptr,
                      float* g33_ptr, const Damping& damp, float dt2, float idx2, float idy2,
-                     float idz2, float sx, float sy, float sz, PointSource src);
+                     float idz2, float sx, float sy, float sz, PointSource src, bool rtm);
 
 // Reads (and clears) the device status word; VTI_ERR_TIMEOUT if a bounded
 // device-side wait gave up since the last check.

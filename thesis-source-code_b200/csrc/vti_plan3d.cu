@@ -31,7 +31,6 @@ struct vti3d_plan {
   Vol g11, g13, g33;
   // TMA descriptors of every volume
   TileMaps m_sx[2], m_sz[2], m_lx[2], m_lz[2], m_cpad[3], m_crand[3], m_g[3];
-  bool use_tma = true;
   float* dampx = nullptr;  // nx + ny + nz floats, one allocation
   float* dampy = nullptr;
   float* dampz = nullptr;
@@ -261,7 +260,6 @@ int forward_pass(vti3d_plan* p, const ShotGeom& s, bool sponge) {
   const float dx2 = g.dx * g.dx, dy2 = g.dy * g.dy, dz2 = g.dz * g.dz, dt2 = g.dt * g.dt;
   const float sxs = dt2 / dx2, sys = dt2 / dy2, szs = dt2 / dz2;
   const int nnt = nnt_of(g), M = last_level(g, p->flags);
-  Vol* c = (sponge || !p->have_rand) ? p->cpad : p->crand;
   const TileMaps* cm = (sponge || !p->have_rand) ? p->m_cpad : p->m_crand;
   Damping dmp{p->dampx, p->dampy, p->dampz};
   for (int k = 0; k < 2; ++k) {
@@ -282,14 +280,9 @@ int forward_pass(vti3d_plan* p, const ShotGeom& s, bool sponge) {
   src.z = s.sz;
   for (int it = 2; it <= M; ++it) {
     src.amp = dt2 * p->wavelet[it - 1];
-    if (p->use_tma)
-      VTI_TRY(launch_fwd3d_tma(ctx, d, p->m_sx[A], p->m_sz[A], p->m_sx[B], p->m_sz[B], cm[0],
-                               cm[1], cm[2], p->sz[A].origin, p->sx[B].origin, p->sz[B].origin,
-                               sponge ? &dmp : nullptr, sxs, sys, szs, src));
-    else
-      VTI_TRY(launch_fwd3d(ctx, d, p->sx[A].origin, p->sz[A].origin, p->sx[B].origin,
-                           p->sz[B].origin, c[0].origin, c[1].origin, c[2].origin,
-                           sponge ? &dmp : nullptr, sxs, sys, szs, src));
+    VTI_TRY(launch_fwd3d_tma(ctx, d, p->m_sx[A], p->m_sz[A], p->m_sx[B], p->m_sz[B], cm[0],
+                             cm[1], cm[2], p->sz[A].origin, p->sx[B].origin, p->sz[B].origin,
+                             sponge ? &dmp : nullptr, sxs, sys, szs, src));
     std::swap(A, B);
     if (sponge && it < (int)s.rec_at.size() && s.rec_at[it] >= 0)
       VTI_TRY(launch_record(ctx, p->d_trace, nnt, s.rec_at[it], p->sx[A].origin,
@@ -302,7 +295,9 @@ int forward_pass(vti3d_plan* p, const ShotGeom& s, bool sponge) {
 // Time-reversed source wavefield + adjoint + imaging (pass 3,
 // objFuncGradient3d_f.cu:910-1078). Expects sx[last_cur] = level M,
 // sx[other] = level M-1 from pass 2, and the residual in d_trace.
-int backward_pass(vti3d_plan* p, const ShotGeom& s) {
+// rtm: the observed traces are in d_trace and the RTM image accumulates in
+// g11 (rtm3d_f.cu:470-620, same schedule).
+int backward_pass(vti3d_plan* p, const ShotGeom& s, bool rtm) {
   vti_ctx* ctx = p->ctx;
   const vti3d_geom& g = p->g;
   const Dims3& d = p->d;
@@ -310,7 +305,6 @@ int backward_pass(vti3d_plan* p, const ShotGeom& s) {
   const float sxs = dt2 / dx2, sys = dt2 / dy2, szs = dt2 / dz2;
   const float idx2 = 1.f / dx2, idy2 = 1.f / dy2, idz2 = 1.f / dz2;
   const int st = sampling_step(g), nnt = nnt_of(g), M = last_level(g, p->flags);
-  Vol* c = p->have_rand ? p->crand : p->cpad;
   const TileMaps* cm = p->have_rand ? p->m_crand : p->m_cpad;
   Damping dmp{p->dampx, p->dampy, p->dampz};
   // flip (objFuncGradient3d_f.cu:912-914): cur = level M-1, prev = level M
@@ -329,19 +323,12 @@ int backward_pass(vti3d_plan* p, const ShotGeom& s) {
   for (int i = 0; i < M - 1; ++i) {
     const int it = g.nt - 3 - i;
     src.amp = dt2 * p->wavelet[it + 1];
-    if (p->use_tma)
-      VTI_TRY(launch_bwd3d_tma(
-          ctx, d, p->m_sx[SA], p->m_sz[SA], p->m_sx[SB], p->m_sz[SB], p->m_lx[LA], p->m_lz[LA],
-          p->m_lx[LB], p->m_lz[LB], cm[0], cm[1], cm[2], p->m_g[0], p->m_g[1], p->m_g[2],
-          p->sz[SA].origin, p->lz[LA].origin, p->sx[SB].origin, p->sz[SB].origin,
-          p->lx[LB].origin, p->lz[LB].origin, p->g11.origin, p->g13.origin, p->g33.origin, dmp,
-          dt2, idx2, idy2, idz2, sxs, sys, szs, src));
-    else
-      VTI_TRY(launch_bwd3d(ctx, d, p->sx[SA].origin, p->sz[SA].origin, p->sx[SB].origin,
-                           p->sz[SB].origin, p->lx[LA].origin, p->lz[LA].origin,
-                           p->lx[LB].origin, p->lz[LB].origin, c[0].origin, c[1].origin,
-                           c[2].origin, p->g11.origin, p->g13.origin, p->g33.origin, dmp, dt2,
-                           idx2, idy2, idz2, sxs, sys, szs, src));
+    VTI_TRY(launch_bwd3d_tma(
+        ctx, d, p->m_sx[SA], p->m_sz[SA], p->m_sx[SB], p->m_sz[SB], p->m_lx[LA], p->m_lz[LA],
+        p->m_lx[LB], p->m_lz[LB], cm[0], cm[1], cm[2], p->m_g[0], p->m_g[1], p->m_g[2],
+        p->sz[SA].origin, p->lz[LA].origin, p->sx[SB].origin, p->sz[SB].origin,
+        p->lx[LB].origin, p->lz[LB].origin, p->g11.origin, p->g13.origin, p->g33.origin, dmp,
+        dt2, idx2, idy2, idz2, sxs, sys, szs, src, rtm));
     // residual interpolated at it+1 (injectRecord3d.cu:60-78)
     const int ti = it + 1;
     float f = float(ti) / float(st);
@@ -415,7 +402,7 @@ int run_gradient(vti3d_plan* p, const float* souloc, const int* shotid, int nsho
     VTI_TRY(launch_residual(ctx, p->d_trace, obs, p->d_live, nnt, s.nr, p->d_acc));
     if (misfit_only) continue;
     VTI_TRY(forward_pass(p, s, false));
-    VTI_TRY(backward_pass(p, s));
+    VTI_TRY(backward_pass(p, s, false));
     // keep host vectors alive until this shot's uploads are consumed
     VTI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   }
@@ -463,10 +450,6 @@ int vti3d_plan_create(vti_ctx* ctx, const vti3d_geom* g, unsigned flags, vti3d_p
                  &p->g13,     &p->g33};
   for (Vol* v : vols)
     if (st == VTI_OK) st = vol_alloc(ctx, p->d, v);
-  {
-    const char* k = std::getenv("VTI_STEP_KERNELS");
-    p->use_tma = !(k && std::string(k) == "simt");
-  }
   if (st == VTI_OK) {
     for (int k = 0; k < 2 && st == VTI_OK; ++k) {
       st = make_tile_maps(ctx, p->d, p->sx[k], &p->m_sx[k]);
@@ -648,6 +631,53 @@ int vti3d_model_data_cij(vti_ctx* ctx, const vti3d_geom* g, const float* c11, co
   if (st == VTI_OK) st = vti3d_plan_set_wavelet(p, wavelet, VTI_MEM_HOST);
   if (st == VTI_OK) st = vti3d_plan_set_receivers(p, recloc, nrec_total);
   if (st == VTI_OK) st = vti3d_plan_model_data(p, souloc, shotid, nshot, ddata, VTI_MEM_HOST);
+  vti3d_plan_destroy(p);
+  return st;
+}
+
+int vti3d_plan_rtm(vti3d_plan* p, const float* souloc, const int* shotid, int nshot,
+                   const float* data, int data_mem, float* image, int image_mem) {
+  if (!p) return VTI_ERR_ARG;
+  vti_ctx* ctx = p->ctx;
+  if (!p->have_model) return fail(ctx, VTI_ERR_ARG, "model not set");
+  if ((int)p->wavelet.size() != p->g.nt) return fail(ctx, VTI_ERR_ARG, "wavelet not set");
+  if (!souloc || (nshot > 0 && !shotid) || !data || !image || nshot < 0)
+    return fail(ctx, VTI_ERR_ARG, "null pointer or negative shot count");
+  VTI_CUDA(ctx, cudaSetDevice(ctx->device));
+  const int nnt = nnt_of(p->g);
+  // rtm3d_f.cu:175: the image is zeroed, then summed over the shots
+  VTI_TRY(vol_zero(ctx, p->d, &p->g11));
+  for (int k = 0; k < nshot; ++k) {
+    ShotGeom s;
+    VTI_TRY(shot_geom(p, souloc, shotid[k], &s));
+    VTI_TRY(upload_shot(p, s));
+    // the recorded traces drive the receiver wavefield as they are
+    // (rtm3d_f.cu:505-514, 547-566): no residual, no dead-trace masking
+    const float* obs = nullptr;
+    VTI_TRY(get_obs(p, s, data, data_mem, &obs));
+    if (s.nr > 0)
+      VTI_CUDA(ctx, cudaMemcpyAsync(p->d_trace, obs, (size_t)nnt * s.nr * sizeof(float),
+                                    cudaMemcpyDeviceToDevice, ctx->stream));
+    VTI_TRY(forward_pass(p, s, false));
+    VTI_TRY(backward_pass(p, s, true));
+    VTI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  VTI_TRY(vol_download(ctx, p->d, &p->g11, image, image_mem));
+  VTI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return check_device_status(ctx);
+}
+
+int vti3d_rtm_cij(vti_ctx* ctx, const vti3d_geom* g, const float* c11, const float* c13,
+                  const float* c33, const float* wavelet, const float* souloc, const int* shotid,
+                  int nshot, const float* recloc, int nrec_total, const float* data,
+                  float* image, unsigned flags) {
+  vti3d_plan* p = nullptr;
+  VTI_TRY(vti3d_plan_create(ctx, g, flags, &p));
+  int st = vti3d_plan_set_model(p, c11, c13, c33, nullptr, nullptr, VTI_MEM_HOST);
+  if (st == VTI_OK) st = vti3d_plan_set_wavelet(p, wavelet, VTI_MEM_HOST);
+  if (st == VTI_OK) st = vti3d_plan_set_receivers(p, recloc, nrec_total);
+  if (st == VTI_OK)
+    st = vti3d_plan_rtm(p, souloc, shotid, nshot, data, VTI_MEM_HOST, image, VTI_MEM_HOST);
   vti3d_plan_destroy(p);
   return st;
 }

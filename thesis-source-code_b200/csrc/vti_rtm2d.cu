@@ -1,0 +1,316 @@
+// 2D reverse-time migration (rtm_f, lib/vti-fwi-2d/rtm_f.cu:13-267) for
+// sm_100a.
+//
+// One step kernel serves both wavefields; both are forwardCD levels
+// (kernels.cu:452-498) with the taper of cur and next folded in as in the
+// forward-modeling kernel (stored levels are once-tapered, prev is read as
+// taper * prev):
+//   * source pass: dipole source (injectDipoleSource, kernels.cu:251-256:
+//     +a at the source, -a one row below) and, every `ratio` steps, the slice
+//     0.5(p+q) of the new level (recordWavefieldSlice, kernels.cu:335-343) into
+//     a device array holding all slices of the shot;
+//   * receiver pass: the kernel first images the current level,
+//     image += 0.5(p+q) * ((1-f) S0 + f S1) (imagingCrossCor,
+//     kernels.cu:414-423), then steps; the traces enter as dipoles
+//     interpolated in time (injectDipoleData, kernels.cu:232-244), scaled by
+//     the taper the reference applies right after the injection.
+// The slice pair and weight each level is imaged with, and the data rows
+// each injection interpolates, follow rtm_f's bookkeeping on the host.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "vti_internal.h"
+
+namespace vti {
+namespace {
+
+constexpr float kC0 = -2.84722222222f, kC1 = 1.6f, kC2 = -0.2f, kC3 = 0.02539682539f,
+                kC4 = -0.00178571428f;
+constexpr int BX = 32, BZ = 8;
+
+__device__ __forceinline__ float lap9(const float* r, int s) {
+  float v = kC0 * r[0];
+  v = fmaf(kC1, r[-s] + r[s], v);
+  v = fmaf(kC2, r[-2 * s] + r[2 * s], v);
+  v = fmaf(kC3, r[-3 * s] + r[3 * s], v);
+  v = fmaf(kC4, r[-4 * s] + r[4 * s], v);
+  return v;
+}
+
+struct RtmStep {
+  int nnx, nnz;
+  const float *p1, *q1;  // current level
+  float *p0, *q0;        // prev in / next out; null: imaging only
+  const float *c11, *c13, *c33, *taper;
+  float idx2, idz2, dt2;
+  int src;    // dipole source at src (+amp) and src + nnx (-amp); -1: none
+  float amp;
+  float* slice;  // set: 0.5(p+q) of the new level
+  float* image;  // set: image the current level against (1-f) s0 + f s1
+  const float *s0, *s1;
+  float f;
+};
+
+__global__ void __launch_bounds__(BX* BZ) k_rtm2d_step(RtmStep a) {
+  __shared__ float sp[BZ][BX + 8], sq[BZ + 8][BX];
+  const int tx = threadIdx.x, tz = threadIdx.y;
+  const int ix = kHalo + blockIdx.x * BX + tx, iz = kHalo + blockIdx.y * BZ + tz;
+  const int nnx = a.nnx, nnz = a.nnz;
+  auto ld = [&](const float* v, int x, int z) {
+    return (x < nnx && z < nnz) ? v[x + z * nnx] : 0.f;
+  };
+  sp[tz][tx + 4] = ld(a.p1, ix, iz);
+  sq[tz + 4][tx] = ld(a.q1, ix, iz);
+  if (tx < 4) {
+    sp[tz][tx] = ld(a.p1, ix - 4, iz);
+    sp[tz][tx + BX + 4] = ld(a.p1, ix + BX, iz);
+  }
+  if (tz < 4) {
+    sq[tz][tx] = ld(a.q1, ix, iz - 4);
+    sq[tz + BZ + 4][tx] = ld(a.q1, ix, iz + BZ);
+  }
+  __syncthreads();
+  if (!(ix < nnx - kHalo && iz < nnz - kHalo)) return;
+  const int i = ix + iz * nnx;
+  const float p = sp[tz][tx + 4], q = sq[tz + 4][tx];
+  if (a.image) {
+    const float d = (1.f - a.f) * a.s0[i] + a.f * a.s1[i];
+    a.image[i] += 0.5f * (p + q) * d;
+  }
+  if (!a.p0) return;
+  const float tp = lap9(&sp[tz][tx + 4], 1) * a.idx2;
+  const float tq = lap9(&sq[tz + 4][tx], BX) * a.idz2;
+  const float t = a.taper[i];
+  float pn = fmaf(a.dt2, fmaf(a.c11[i], tp, a.c13[i] * tq), 2.f * p - t * a.p0[i]);
+  float qn = fmaf(a.dt2, fmaf(a.c13[i], tp, a.c33[i] * tq), 2.f * q - t * a.q0[i]);
+  if (i == a.src) {
+    pn += a.amp;
+    qn += a.amp;
+  } else if (a.src >= 0 && i == a.src + nnx) {
+    pn -= a.amp;
+    qn -= a.amp;
+  }
+  pn *= t;
+  qn *= t;
+  a.p0[i] = pn;
+  a.q0[i] = qn;
+  if (a.slice) a.slice[i] = 0.5f * (pn + qn);
+}
+
+// injectDipoleData into a level that has already been tapered: the taper
+// factor of each point (1 in the never-updated 4-cell frame) is applied to
+// the injected value. Receivers may share points, hence the atomics.
+__global__ void k_rtm2d_inject(float* p, float* q, const float* d0, const float* d1, float f,
+                               const int* ridx, const float* taper, int nr, float dt2, int nnx,
+                               int nnz) {
+  const int ir = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ir >= nr) return;
+  const float v = dt2 * (0.5f * ((1.f - f) * (d0 ? d0[ir] : 0.f) + f * (d1 ? d1[ir] : 0.f)));
+  auto add = [&](int k, float w) {
+    const int x = k % nnx, z = k / nnx;
+    const bool in = x >= kHalo && x < nnx - kHalo && z >= kHalo && z < nnz - kHalo;
+    const float s = in ? taper[k] * w : w;
+    atomicAdd(p + k, s);
+    atomicAdd(q + k, s);
+  };
+  add(ridx[ir], v);
+  add(ridx[ir] + nnx, -v);
+}
+
+}  // namespace
+}  // namespace vti
+
+using namespace vti;
+
+extern "C" int vti2d_rtm(vti_ctx* ctx, const vti2d_geom* g, float* image, const float* data,
+                         const float* c11, const float* c13, const float* c33,
+                         const float* wavelet, const int* sloc, int ns, const int* rloc, int nr,
+                         const float* taper) {
+  if (!ctx || !g || !image || !data || !c11 || !c13 || !c33 || !wavelet || !sloc || !taper ||
+      (nr > 0 && !rloc) || ns < 0)
+    return VTI_ERR_ARG;
+  const int nnx = g->nx + 2 * g->npad, nnz = g->nz + 2 * g->npad;
+  const long long nnxz = (long long)nnx * nnz;
+  if (nnx < 9 || nnz < 10 || g->nt < 3 || !(g->dt > 0) || !(g->rate > 0))
+    return fail(ctx, VTI_ERR_ARG, "2D geometry out of range");
+  const float dt = g->dt, dt2 = dt * dt;
+  const int ratio = (int)(g->rate / dt + 0.5f);  // rtm_f.cu:16
+  if (ratio < 1) return fail(ctx, VTI_ERR_ARG, "rate < dt");
+  const int ntNeg = (int)std::round(std::fabs(g->ot) / dt);
+  const int nnt = (g->nt - 1) / ratio + 1;
+  const int nnt_data = (g->nt - ntNeg - 1) / ratio + 1;
+  // the dipole source needs both of its points inside the updated region;
+  // receivers only need theirs inside the grid
+  for (int is = 0; is < ns; ++is) {
+    const int* s = sloc + 4 * is;
+    if (s[0] < kHalo || s[0] >= nnx - kHalo || s[1] < kHalo || s[1] + 1 >= nnz - kHalo)
+      return fail(ctx, VTI_ERR_ARG, "2D RTM source (and the point below it) must lie in the "
+                                    "updated region");
+    if (s[2] < 0 || s[3] < 0 || s[3] + s[2] > nr)
+      return fail(ctx, VTI_ERR_ARG, "2D shot receiver range exceeds rloc");
+    for (int ir = 0; ir < s[2]; ++ir) {
+      const int x = rloc[2 * (s[3] + ir)], z = rloc[2 * (s[3] + ir) + 1];
+      if (x < 0 || x >= nnx || z < 0 || z + 1 >= nnz)
+        return fail(ctx, VTI_ERR_ARG, "2D receiver (and the point below it) outside the grid");
+    }
+  }
+  VTI_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t sm = ctx->stream;
+  // device buffers: model, taper, 4 wavefields, image, slices, traces, receivers
+  const size_t nslices = (size_t)nnt + 1;  // one past the last slice reads zeros
+  const size_t nfloat = 9 * (size_t)nnxz + nslices * nnxz + (size_t)nnt_data * nr;
+  float* buf = nullptr;
+  int* d_ridx = nullptr;
+  VTI_CUDA(ctx, cudaMalloc((void**)&buf, nfloat * sizeof(float)));
+  int st = VTI_OK;
+  if (cudaMalloc((void**)&d_ridx, std::max(nr, 1) * sizeof(int)) != cudaSuccess) {
+    cudaFree(buf);
+    return fail(ctx, VTI_ERR_OOM, "cannot allocate the receiver table");
+  }
+  float *dc11 = buf, *dc13 = dc11 + nnxz, *dc33 = dc13 + nnxz, *dtap = dc33 + nnxz;
+  float *p0 = dtap + nnxz, *q0 = p0 + nnxz, *p1 = q0 + nnxz, *q1 = p1 + nnxz;
+  float* dimg = q1 + nnxz;
+  float* slices = dimg + nnxz;
+  float* ddata = slices + nslices * nnxz;
+  auto done = [&](int status) {
+    cudaStreamSynchronize(sm);
+    cudaFree(buf);
+    cudaFree(d_ridx);
+    return status;
+  };
+#define RTM_CK(call)                                               \
+  do {                                                             \
+    cudaError_t e_ = (call);                                       \
+    if (e_ != cudaSuccess) return done(cuda_check(ctx, e_, #call)); \
+  } while (0)
+  RTM_CK(cudaMemcpyAsync(dc11, c11, nnxz * 4, cudaMemcpyHostToDevice, sm));
+  RTM_CK(cudaMemcpyAsync(dc13, c13, nnxz * 4, cudaMemcpyHostToDevice, sm));
+  RTM_CK(cudaMemcpyAsync(dc33, c33, nnxz * 4, cudaMemcpyHostToDevice, sm));
+  RTM_CK(cudaMemcpyAsync(dtap, taper, nnxz * 4, cudaMemcpyHostToDevice, sm));
+  if (nr > 0)
+    RTM_CK(cudaMemcpyAsync(ddata, data, (size_t)nnt_data * nr * 4, cudaMemcpyHostToDevice, sm));
+  // image and every slice start at zero (rtm_f.cu:24,55)
+  RTM_CK(cudaMemsetAsync(dimg, 0, (nnxz + nslices * nnxz) * 4, sm));
+  std::vector<int> ridx(std::max(nr, 1));
+  for (int ir = 0; ir < nr; ++ir) ridx[ir] = rloc[2 * ir] + rloc[2 * ir + 1] * nnx;
+  RTM_CK(cudaMemcpyAsync(d_ridx, ridx.data(), std::max(nr, 1) * sizeof(int),
+                         cudaMemcpyHostToDevice, sm));
+  const dim3 block(BX, BZ), grid((nnx - 8 + BX - 1) / BX, (nnz - 8 + BZ - 1) / BZ);
+  RtmStep a{};
+  a.nnx = nnx;
+  a.nnz = nnz;
+  a.c11 = dc11;
+  a.c13 = dc13;
+  a.c33 = dc33;
+  a.taper = dtap;
+  a.idx2 = 1.f / (g->dx * g->dx);
+  a.idz2 = 1.f / (g->dz * g->dz);
+  a.dt2 = dt2;
+  auto step = [&](const float* cp, const float* cq, float* np, float* nq) -> int {
+    a.p1 = cp;
+    a.q1 = cq;
+    a.p0 = np;
+    a.q0 = nq;
+    k_rtm2d_step<<<grid, block, 0, sm>>>(a);
+    ctx->launches++;
+    return cuda_check(ctx, cudaGetLastError(), "k_rtm2d_step");
+  };
+  auto slice_at = [&](int j) { return slices + (size_t)j * nnxz; };
+  for (int is = 0; is < ns; ++is) {
+    const int* s = sloc + 4 * is;
+    const int sxz = s[0] + s[1] * nnx, nri = s[2], ir0 = s[3];
+    RTM_CK(cudaMemsetAsync(p0, 0, 4 * nnxz * 4, sm));
+    // level 1 (rtm_f.cu:113-120): the dipole source, then the taper, so
+    // t * (dt2 w0) at the source and -t * (dt2 w0) below it; with ratio 1 its
+    // slice 0.5(p+q) holds the same two values (p = q there)
+    {
+      const float a0 = dt2 * wavelet[0];
+      const float v[2] = {taper[sxz] * a0, -(taper[sxz + nnx] * a0)};
+      for (float* f : {p1, q1}) {
+        RTM_CK(cudaMemcpyAsync(f + sxz, &v[0], 4, cudaMemcpyHostToDevice, sm));
+        RTM_CK(cudaMemcpyAsync(f + sxz + nnx, &v[1], 4, cudaMemcpyHostToDevice, sm));
+      }
+      if (ratio == 1) {  // a whole new slice: clear the previous shot's points
+        RTM_CK(cudaMemsetAsync(slice_at(1), 0, nnxz * 4, sm));
+        RTM_CK(cudaMemcpyAsync(slice_at(1) + sxz, &v[0], 4, cudaMemcpyHostToDevice, sm));
+        RTM_CK(cudaMemcpyAsync(slice_at(1) + sxz + nnx, &v[1], 4, cudaMemcpyHostToDevice, sm));
+      }
+      RTM_CK(cudaStreamSynchronize(sm));  // v goes out of scope
+    }
+    float *cp = p1, *cq = q1, *np = p0, *nq = q0;
+    a.image = nullptr;
+    for (int it = 2; it < g->nt; ++it) {
+      a.src = sxz;
+      a.amp = dt2 * wavelet[it - 1];
+      a.slice = (it % ratio == 0) ? slice_at(it / ratio) : nullptr;
+      st = step(cp, cq, np, nq);
+      if (st != VTI_OK) return done(st);
+      std::swap(cp, np);
+      std::swap(cq, nq);
+    }
+    // receiver pass (rtm_f.cu:152-225)
+    a.src = -1;
+    a.slice = nullptr;
+    RTM_CK(cudaMemsetAsync(p0, 0, 4 * nnxz * 4, sm));
+    cp = p0;
+    cq = q0;
+    np = p1;
+    nq = q1;
+    const float* row_base = ddata + ir0;
+    const float* d0 = row_base + (size_t)(nnt_data - 1) * nr;
+    const float* d1 = nullptr;  // zeros
+    auto inject = [&](float* p, float* q, float f) -> int {
+      if (nri <= 0) return VTI_OK;
+      k_rtm2d_inject<<<(nri + 127) / 128, 128, 0, sm>>>(p, q, d0, d1, f, d_ridx + ir0, dtap, nri,
+                                                         dt2, nnx, nnz);
+      ctx->launches++;
+      return cuda_check(ctx, cudaGetLastError(), "k_rtm2d_inject");
+    };
+    st = inject(cp, cq, 0.f);  // into the zero level, then its taper (rtm_f.cu:162-164)
+    if (st != VTI_OK) return done(st);
+    float f = (g->nt - 2.) / ratio;
+    int s0 = (int)f, s1 = std::min(s0 + 1, nnt);
+    f -= s0;
+    // the level just made is imaged by the next kernel, which reads it as cur
+    a.image = dimg;
+    a.s0 = slice_at(s0);
+    a.s1 = slice_at(s1);
+    a.f = f;
+    for (int it = g->nt - 3; it >= 0; --it) {
+      st = step(cp, cq, np, nq);  // images cur (level it+1), makes level it
+      if (st != VTI_OK) return done(st);
+      if (it >= ntNeg) {
+        float fd = (it - ntNeg + 1.) / ratio;
+        const int i1 = (int)fd;
+        if ((it - ntNeg + 2) % ratio == 0) {
+          d1 = row_base + (size_t)i1 * nr;
+          std::swap(d0, d1);
+        }
+        fd -= i1;
+        st = inject(np, nq, fd);
+        if (st != VTI_OK) return done(st);
+      }
+      float fs = (float)it / ratio;
+      const int i1 = (int)fs;
+      if ((it + 1) % ratio == 0) {
+        s1 = i1;
+        std::swap(s0, s1);
+      }
+      fs -= i1;
+      a.s0 = slice_at(s0);
+      a.s1 = slice_at(s1);
+      a.f = fs;
+      std::swap(cp, np);
+      std::swap(cq, nq);
+    }
+    // image the last level (it = 0)
+    st = step(cp, cq, nullptr, nullptr);
+    if (st != VTI_OK) return done(st);
+    a.image = nullptr;
+  }
+  RTM_CK(cudaMemcpyAsync(image, dimg, nnxz * 4, cudaMemcpyDeviceToHost, sm));
+  RTM_CK(cudaStreamSynchronize(sm));
+#undef RTM_CK
+  return done(VTI_OK);
+}

@@ -738,3 +738,103 @@ void GNhessianVEpsDel(float* gv, float* geps, float* gdel, const float* d0, floa
   std::memset(geps, 0, rows * nnx * sizeof(float));
   std::memset(gdel, 0, rows * nnx * sizeof(float));
 }
+
+// ---------------------------------------------------------------- RTM
+// rtmCij3d_f (rtm3d_f.cu:161-620): devices from gpu=, three floats (x, y, z)
+// per receiver, each shot's traces read from data= (rtm3d_f.cu:505); the
+// model is used as passed (the caller puts the random boundary in). Images of
+// the devices' shots are summed.
+void rtmCij3d_f(float* image, float* souloc, int ns, std::vector<int>& shotid, float* recloc,
+                float* wavelet, float* c11, float* c13, float* c33, int nx, int ny, int nz,
+                int nt, int npad, float ox, float oy, float oz, float ot, float dx, float dy,
+                float dz, float dt, float samplingRate) {
+  (void)ns;
+  vti3d_geom g = geom3(nx, ny, nz, nt, npad, ox, oy, oz, ot, dx, dy, dz, dt, samplingRate);
+  const size_t n = (size_t)nx * ny * nz;
+  std::memset(image, 0, n * sizeof(float));
+  const std::vector<int> gpus = gpus_from_argv();
+  const int nrec = total_receivers(souloc, shotid);
+  std::vector<float> rec4(4 * (size_t)nrec);
+  for (int ir = 0; ir < nrec; ++ir) {
+    for (int k = 0; k < 3; ++k) rec4[4 * (size_t)ir + k] = recloc[3 * (size_t)ir + k];
+    rec4[4 * (size_t)ir + 3] = 1.f;
+  }
+  std::vector<float> data;
+  int nr_read = 0;
+  if (!read_observed(souloc, shotid, g, &data, &nr_read)) return;
+  const unsigned flags = ref_flags(gpus.size());
+  std::vector<std::vector<float>> parts(gpus.size());
+  std::map<int, size_t> slot;
+  for (size_t i = 0; i < gpus.size(); ++i) slot[gpus[i]] = i;
+  over_gpus(gpus, shotid, [&](int id, const std::vector<int>& sub) {
+    Device* dev = device(id);
+    if (!dev) return false;
+    std::lock_guard<std::mutex> lk(dev->mu);
+    vti3d_plan* p = plan_for(dev, g, flags);
+    if (!p) return false;
+    std::vector<float>& img = parts[slot[id]];
+    img.assign(n, 0.f);
+    return report(dev->ctx, vti3d_plan_set_model(p, c11, c13, c33, nullptr, nullptr,
+                                                 VTI_MEM_HOST), "model") &&
+           report(dev->ctx, vti3d_plan_set_wavelet(p, wavelet, VTI_MEM_HOST), "wavelet") &&
+           report(dev->ctx, vti3d_plan_set_receivers(p, rec4.data(), nrec), "receivers") &&
+           report(dev->ctx, vti3d_plan_rtm(p, souloc, sub.data(), (int)sub.size(), data.data(),
+                                           VTI_MEM_HOST, img.data(), VTI_MEM_HOST), "rtm");
+  });
+  for (auto& img : parts)
+    if (!img.empty())
+      for (size_t i = 0; i < n; ++i) image[i] += img[i];
+}
+
+// rtmVEpsDel (rtm3d_f.cu:139-159): v, eps, del -> c_ij with unit scales,
+// migration, then the pad region and the water layer of the image zeroed.
+void rtmVEpsDel(float* image, float* souloc, int ns, std::vector<int>& shotid, float* recloc,
+                float* wavelet, float* v, float* eps, float* del, float* randboundaryV, int nx,
+                int ny, int nz, int nt, int npad, float ox, float oy, float oz, float ot,
+                float dx, float dy, float dz, float dt, float samplingRate, float wbottom) {
+  (void)randboundaryV;  // the reference leaves its putBoundary call commented out
+  const size_t nxy = (size_t)nx * ny, n = nxy * nz;
+  std::vector<float> c(3 * n);
+  vti_vepsdel_to_cij(c.data(), c.data() + n, c.data() + 2 * n, v, eps, del, 1.f, 1.f, 1.f, n);
+  rtmCij3d_f(image, souloc, ns, shotid, recloc, wavelet, c.data(), c.data() + n,
+             c.data() + 2 * n, nx, ny, nz, nt, npad, ox, oy, oz, ot, dx, dy, dz, dt,
+             samplingRate);
+  vti3d_zero_boundary(image, nx, ny, nz, npad);
+  const int nwbottom = (int)((wbottom - oz) / dz + 1 - npad);
+  if (nwbottom > 0)
+    std::memset(image + (size_t)npad * nxy, 0,
+                std::min<size_t>((size_t)nwbottom, (size_t)nz - npad) * nxy * sizeof(float));
+}
+
+// rtm_f (rtm_f.cu:13-267): shots round-robin over the gpu= devices
+// (is = pass*nGPUs + i), per-device images summed.
+void rtm_f(float* image, const float* data, const float* c11, const float* c13, const float* c33,
+           const float* wavelet, const int* sloc, int ns, const int* rloc, int nr,
+           const float* taper, int nx, int nz, int nt, int npad, float dx, float dz, float dt,
+           float rate, float ot) {
+  vti2d_geom g{nx, nz, nt, npad, dx, dz, dt, rate, ot};
+  const size_t n = (size_t)(nx + 2 * npad) * (nz + 2 * npad);
+  std::memset(image, 0, n * sizeof(float));
+  const std::vector<int> gpus = gpus_from_argv();
+  auto parts = shots_per_gpu(ns, gpus.size());
+  std::vector<std::vector<float>> img(gpus.size());
+  std::vector<std::thread> th;
+  for (size_t k = 0; k < gpus.size(); ++k) {
+    if (parts[k].empty()) continue;
+    th.emplace_back([&, k]() {
+      Device* dev = device(gpus[k]);
+      if (!dev) return;
+      std::lock_guard<std::mutex> lk(dev->mu);
+      std::vector<int> sl;
+      for (int is : parts[k]) sl.insert(sl.end(), sloc + 4 * is, sloc + 4 * is + 4);
+      img[k].assign(n, 0.f);
+      if (!report(dev->ctx, vti2d_rtm(dev->ctx, &g, img[k].data(), data, c11, c13, c33, wavelet,
+                                      sl.data(), (int)parts[k].size(), rloc, nr, taper), "rtm"))
+        img[k].clear();
+    });
+  }
+  for (auto& t : th) t.join();
+  for (auto& v : img)
+    if (!v.empty())
+      for (size_t i = 0; i < n; ++i) image[i] += v[i];
+}

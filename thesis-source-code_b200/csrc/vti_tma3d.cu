@@ -56,6 +56,11 @@ __device__ __forceinline__ float lap9(float c, float m1, float p1, float m2, flo
   return s;
 }
 
+// Two adjacent floats (8-byte aligned: x offsets are even, rows even-sized).
+__device__ __forceinline__ float2 ld2(const float* p) {
+  return *reinterpret_cast<const float2*>(p);
+}
+
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
 }
@@ -193,35 +198,44 @@ __global__ void __launch_bounds__(NTHREADS, 3)
     return;
   }
 
-  // ---------------- consumers: thread (lane, warp) owns x = x0+lane, rows 2w, 2w+1
+  // ---------------- consumers: thread (lane, warp) owns the x pair
+  // x0 + 2*(lane%16) + {0,1} of tile row 2*warp + lane/16; shared-memory reads
+  // and global stores are float2.
   const bool damp = a.dampz != nullptr;
-  float q[RY][9];
-  float dxy[RY];
-  int off[RY];
-  bool valid[RY];
+  const int ry = warp * 2 + (lane >> 4);
+  const int xo = 2 * (lane & 15);
+  const int sr = (ry + kHalo) * HX + xo + kHalo;  // centre in the halo tile
+  const int pi = ry * TX + xo;                    // centre in a plain tile
+  float q[2][9];
+  float dxy[2];
   long long k = 0;  // planes consumed by this CTA
   bool ok = true;
   for (int it = blockIdx.x; ok && it < a.sc.items; it += gridDim.x) {
     int bx, by, z0, z1;
     item(a.sc, it, bx, by, z0, z1);
-    const int x = bx * TX + lane;
-    const int y0 = kHalo + by * TY;
+    const int x = bx * TX + xo;
+    const int y = kHalo + by * TY + ry;
+    const bool vy = y < d.ny - kHalo;
+    const bool v0 = vy && x >= kHalo && x < d.nx - kHalo;
+    const bool v1 = vy && x + 1 >= kHalo && x + 1 < d.nx - kHalo;
+    const int off = y * d.pitch + x;  // x + 1 < pitch: 32 * gx <= pitch
+    dxy[0] = (damp && v0) ? a.dampx[x] * a.dampy[y] : 1.f;
+    dxy[1] = (damp && v1) ? a.dampx[x + 1] * a.dampy[y] : 1.f;
     // start the queue: planes z0-4 .. z0+3 from global
+    q[0][0] = q[1][0] = 0.f;
 #pragma unroll
-    for (int r = 0; r < RY; ++r) {
-      const int y = y0 + warp * RY + r;
-      valid[r] = x >= kHalo && x < d.nx - kHalo && y < d.ny - kHalo;
-      off[r] = y * d.pitch + x;
-      dxy[r] = (damp && valid[r]) ? a.dampx[x] * a.dampy[y] : 1.f;
-      q[r][0] = 0.f;
-#pragma unroll
-      for (int kk = 1; kk < 9; ++kk) {
-        const int zz = z0 - 5 + kk;
-        float v = valid[r] ? __ldg(a.cz + (long long)zz * d.plane + off[r]) : 0.f;
-        // planes of the block above z0 were already damped as "cur"
-        if (damp && zz >= 0 && (zz >> 2) < (z0 >> 2)) v *= dxy[r] * a.dampz[zz];
-        q[r][kk] = v;
+    for (int kk = 1; kk < 9; ++kk) {
+      const int zz = z0 - 5 + kk;
+      float2 v = (v0 || v1)
+                     ? __ldg(reinterpret_cast<const float2*>(a.cz + (long long)zz * d.plane + off))
+                     : make_float2(0.f, 0.f);
+      // planes of the block above z0 were already damped as "cur"
+      if (damp && zz >= 0 && (zz >> 2) < (z0 >> 2)) {
+        v.x *= dxy[0] * a.dampz[zz];
+        v.y *= dxy[1] * a.dampz[zz];
       }
+      q[0][kk] = v.x;
+      q[1][kk] = v.y;
     }
     for (int z = z0; z < z1; ++z, ++k) {
       const int s = (int)(k % F_STAGES);
@@ -229,56 +243,84 @@ __global__ void __launch_bounds__(NTHREADS, 3)
         ok = false;
         break;
       }
-      const float* sh = (const float*)(smem + s * F_STAGE_BYTES + F_OFF_H);
-      const float* sq = (const float*)(smem + s * F_STAGE_BYTES + F_OFF_Z);
-      const float* spx = (const float*)(smem + s * F_STAGE_BYTES + F_OFF_PX);
-      const float* spz = (const float*)(smem + s * F_STAGE_BYTES + F_OFF_PZ);
-      const float* s11 = (const float*)(smem + s * F_STAGE_BYTES + F_OFF_C);
-      const float* s13 = s11 + TX * TY;
-      const float* s33 = s13 + TX * TY;
-      const float dz = damp ? a.dampz[z] : 1.f;
+      const unsigned char* st = smem + s * F_STAGE_BYTES;
+      const float* sh = (const float*)(st + F_OFF_H) + sr;
+      const float* pl = (const float*)(st + F_OFF_Z) + pi;  // [z+4][prev x][prev z][c11][c13][c33]
+      constexpr int T = TX * TY;
 #pragma unroll
-      for (int r = 0; r < RY; ++r) {
-        const int ry = warp * RY + r;
-        const int pi = ry * TX + lane;
-#pragma unroll
-        for (int kk = 0; kk < 8; ++kk) q[r][kk] = q[r][kk + 1];
-        q[r][8] = sq[pi];
-        const int sr = (ry + kHalo) * HX + lane + kHalo;
-        const float c = sh[sr];
-        const float lxx = lap9(c, sh[sr - 1], sh[sr + 1], sh[sr - 2], sh[sr + 2], sh[sr - 3],
-                               sh[sr + 3], sh[sr - 4], sh[sr + 4]);
-        const float lyy = lap9(c, sh[sr - HX], sh[sr + HX], sh[sr - 2 * HX], sh[sr + 2 * HX],
-                               sh[sr - 3 * HX], sh[sr + 3 * HX], sh[sr - 4 * HX], sh[sr + 4 * HX]);
-        const float lzz =
-            lap9(q[r][4], q[r][3], q[r][5], q[r][2], q[r][6], q[r][1], q[r][7], q[r][0], q[r][8]);
-        const float lxy = fmaf(lyy, a.sy, lxx * a.sx);
-        const float lz = lzz * a.sz;
-        const float dd = dxy[r] * dz;
-        float nxv = fmaf(s11[pi], lxy, fmaf(s13[pi], lz, 2.f * c - dd * spx[pi]));
-        float nzv = fmaf(s13[pi], lxy, fmaf(s33[pi], lz, 2.f * q[r][4] - dd * spz[pi]));
-        const int y = y0 + ry;
-        if (x == a.src.x && y == a.src.y && z == a.src.z) {
-          nxv += a.src.amp;
-          nzv += a.src.amp;
-        }
-        if (valid[r]) {
-          const long long i = (long long)z * d.plane + off[r];
-          a.px[i] = dd * nxv;
-          a.pz[i] = dd * nzv;
-        }
+      for (int kk = 0; kk < 8; ++kk) {
+        q[0][kk] = q[0][kk + 1];
+        q[1][kk] = q[1][kk + 1];
       }
+      const float2 zq = ld2(pl);
+      q[0][8] = zq.x;
+      q[1][8] = zq.y;
+      // the row x-4 .. x+5 and the column pairs y +- 1..4
+      float r[10];
+#pragma unroll
+      for (int j = 0; j < 5; ++j) {
+        const float2 t = ld2(sh - 4 + 2 * j);
+        r[2 * j] = t.x;
+        r[2 * j + 1] = t.y;
+      }
+      float2 ym[4], yp[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        ym[j] = ld2(sh - (j + 1) * HX);
+        yp[j] = ld2(sh + (j + 1) * HX);
+      }
+      const float2 px = ld2(pl + T), pz = ld2(pl + 2 * T);
+      const float2 c11 = ld2(pl + 3 * T), c13 = ld2(pl + 4 * T), c33 = ld2(pl + 5 * T);
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[s]);
+      const float dz = damp ? a.dampz[z] : 1.f;
+      float nxv[2], nzv[2];
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        auto pick = [e](float2 v) { return e ? v.y : v.x; };
+        const float c = r[4 + e];
+        const float lxx = lap9(c, r[3 + e], r[5 + e], r[2 + e], r[6 + e], r[1 + e], r[7 + e],
+                               r[e], r[8 + e]);
+        const float lyy = lap9(c, pick(ym[0]), pick(yp[0]), pick(ym[1]), pick(yp[1]),
+                               pick(ym[2]), pick(yp[2]), pick(ym[3]), pick(yp[3]));
+        const float lzz = lap9(q[e][4], q[e][3], q[e][5], q[e][2], q[e][6], q[e][1], q[e][7],
+                               q[e][0], q[e][8]);
+        const float lxy = fmaf(lyy, a.sy, lxx * a.sx);
+        const float lz = lzz * a.sz;
+        const float dd = dxy[e] * dz;
+        const float a11 = pick(c11), a13 = pick(c13), a33 = pick(c33);
+        nxv[e] = fmaf(a11, lxy, fmaf(a13, lz, 2.f * c - dd * pick(px)));
+        nzv[e] = fmaf(a13, lxy, fmaf(a33, lz, 2.f * q[e][4] - dd * pick(pz)));
+        if (x + e == a.src.x && y == a.src.y && z == a.src.z) {
+          nxv[e] += a.src.amp;
+          nzv[e] += a.src.amp;
+        }
+        nxv[e] *= dd;
+        nzv[e] *= dd;
+      }
+      const long long i = (long long)z * d.plane + off;
+      if (v0 && v1) {
+        *reinterpret_cast<float2*>(a.px + i) = make_float2(nxv[0], nxv[1]);
+        *reinterpret_cast<float2*>(a.pz + i) = make_float2(nzv[0], nzv[1]);
+      } else {
+        if (v0) {
+          a.px[i] = nxv[0];
+          a.pz[i] = nzv[0];
+        }
+        if (v1) {
+          a.px[i + 1] = nxv[1];
+          a.pz[i + 1] = nzv[1];
+        }
+      }
       // entering the next plane: if it starts a new 4-plane block of the same
       // column, the four planes of the block just finished become "damped cur"
       if (damp && ((z + 1) & 3) == 0 && z + 1 < d.nz) {
 #pragma unroll
-        for (int r = 0; r < RY; ++r) {
+        for (int e = 0; e < 2; ++e) {
           // after the shift at z+1, entries 0..3 hold planes z-3..z; they are
           // entries 1..4 now
 #pragma unroll
-          for (int kk = 0; kk < 4; ++kk) q[r][kk + 1] *= dxy[r] * a.dampz[z - 3 + kk];
+          for (int kk = 0; kk < 4; ++kk) q[e][kk + 1] *= dxy[e] * a.dampz[z - 3 + kk];
         }
       }
     }
@@ -319,6 +361,15 @@ struct BwdMaps {
   CUtensorMap scx, scz, spx, spz, lcx, lcz, lpx, lpz, c11, c13, c33, g11, g13, g33;
 };
 
+// wave3d.h:5-6 recording / imaging weights, as float
+constexpr float kTwoThirdF = (float)kTwoThird, kOneThirdF = (float)kOneThird;
+
+// kRtm selects the imaging condition of rtmCij3d_f (kernel3d.cu:456-469,
+// rtm3d_f.cu:607-610): one image volume, kept in the g11 slot, gains
+// (2/3 sx + 1/3 sz)(2/3 lx + 1/3 lz) with both fields at the current level and
+// the adjoint already multiplied by this step's sponge; g13/g33 are neither
+// loaded nor written.
+template <bool kRtm>
 __global__ void __launch_bounds__(NTHREADS, 2)
     k_bwd3d_tma(const __grid_constant__ BwdMaps m, const BwdArgs a) {
   extern __shared__ unsigned char smem_raw[];
@@ -355,7 +406,7 @@ __global__ void __launch_bounds__(NTHREADS, 2)
           const int zp = z + kZPad;
           unsigned char* st = smem + s * B_STAGE_BYTES;
           unsigned char* pl = st + B_OFF_P;
-          mbar_arrive_expect_tx(&full[s], B_STAGE_BYTES);
+          mbar_arrive_expect_tx(&full[s], kRtm ? B_STAGE_BYTES - 2 * PLAIN_BYTES : B_STAGE_BYTES);
           tma_load(st + B_OFF_SH, &m.scx, &full[s], x0 - kHalo, y0 - kHalo, zp);
           tma_load(st + B_OFF_LH, &m.lcx, &full[s], x0 - kHalo, y0 - kHalo, zp);
           tma_load(pl + 0 * PLAIN_BYTES, &m.scz, &full[s], x0, y0, zp + kHalo);
@@ -368,42 +419,54 @@ __global__ void __launch_bounds__(NTHREADS, 2)
           tma_load(pl + 7 * PLAIN_BYTES, &m.c13, &full[s], x0, y0, zp);
           tma_load(pl + 8 * PLAIN_BYTES, &m.c33, &full[s], x0, y0, zp);
           tma_load(pl + 9 * PLAIN_BYTES, &m.g11, &full[s], x0, y0, zp);
-          tma_load(pl + 10 * PLAIN_BYTES, &m.g13, &full[s], x0, y0, zp);
-          tma_load(pl + 11 * PLAIN_BYTES, &m.g33, &full[s], x0, y0, zp);
+          if (!kRtm) {
+            tma_load(pl + 10 * PLAIN_BYTES, &m.g13, &full[s], x0, y0, zp);
+            tma_load(pl + 11 * PLAIN_BYTES, &m.g33, &full[s], x0, y0, zp);
+          }
         }
       }
     }
     return;
   }
 
-  float sq[RY][9], lq[RY][9];
-  float dxy[RY];
-  int off[RY];
-  bool valid[RY];
+  // consumers: the x pair x0 + 2*(lane%16) + {0,1} of tile row 2*warp + lane/16
+  const int ry = warp * 2 + (lane >> 4);
+  const int xo = 2 * (lane & 15);
+  const int sr = (ry + kHalo) * HX + xo + kHalo;
+  const int pi = ry * TX + xo;
+  float sq[2][9], lq[2][9];
+  float dxy[2];
   long long k = 0;
   bool ok = true;
   for (int it = blockIdx.x; ok && it < a.sc.items; it += gridDim.x) {
     int bx, by, z0, z1;
     item(a.sc, it, bx, by, z0, z1);
-    const int x = bx * TX + lane;
-    const int y0 = kHalo + by * TY;
+    const int x = bx * TX + xo;
+    const int y = kHalo + by * TY + ry;
+    const bool vy = y < d.ny - kHalo;
+    const bool v0 = vy && x >= kHalo && x < d.nx - kHalo;
+    const bool v1 = vy && x + 1 >= kHalo && x + 1 < d.nx - kHalo;
+    const int off = y * d.pitch + x;  // x + 1 < pitch: 32 * gx <= pitch
+    dxy[0] = v0 ? a.dampx[x] * a.dampy[y] : 1.f;
+    dxy[1] = v1 ? a.dampx[x + 1] * a.dampy[y] : 1.f;
     // start the queues: planes z0-4 .. z0+3 from global
+    sq[0][0] = sq[1][0] = lq[0][0] = lq[1][0] = 0.f;
 #pragma unroll
-    for (int r = 0; r < RY; ++r) {
-      const int y = y0 + warp * RY + r;
-      valid[r] = x >= kHalo && x < d.nx - kHalo && y < d.ny - kHalo;
-      off[r] = y * d.pitch + x;
-      dxy[r] = valid[r] ? a.dampx[x] * a.dampy[y] : 1.f;
-      sq[r][0] = lq[r][0] = 0.f;
-#pragma unroll
-      for (int kk = 1; kk < 9; ++kk) {
-        const int zz = z0 - 5 + kk;
-        const long long i = (long long)zz * d.plane + off[r];
-        sq[r][kk] = valid[r] ? __ldg(a.scz + i) : 0.f;
-        float v = valid[r] ? __ldg(a.lcz + i) : 0.f;
-        if (zz >= 0 && (zz >> 2) < (z0 >> 2)) v *= dxy[r] * a.dampz[zz];
-        lq[r][kk] = v;
+    for (int kk = 1; kk < 9; ++kk) {
+      const int zz = z0 - 5 + kk;
+      const long long i = (long long)zz * d.plane + off;
+      const bool any = v0 || v1;
+      const float2 sv =
+          any ? __ldg(reinterpret_cast<const float2*>(a.scz + i)) : make_float2(0.f, 0.f);
+      float2 lv = any ? __ldg(reinterpret_cast<const float2*>(a.lcz + i)) : make_float2(0.f, 0.f);
+      if (zz >= 0 && (zz >> 2) < (z0 >> 2)) {
+        lv.x *= dxy[0] * a.dampz[zz];
+        lv.y *= dxy[1] * a.dampz[zz];
       }
+      sq[0][kk] = sv.x;
+      sq[1][kk] = sv.y;
+      lq[0][kk] = lv.x;
+      lq[1][kk] = lv.y;
     }
     for (int z = z0; z < z1; ++z, ++k) {
       const int s = (int)(k % B_STAGES);
@@ -412,77 +475,128 @@ __global__ void __launch_bounds__(NTHREADS, 2)
         break;
       }
       const unsigned char* st = smem + s * B_STAGE_BYTES;
-      const float* sh = (const float*)(st + B_OFF_SH);
-      const float* lh = (const float*)(st + B_OFF_LH);
-      const float* pl = (const float*)(st + B_OFF_P);
+      const float* sh = (const float*)(st + B_OFF_SH) + sr;
+      const float* lh = (const float*)(st + B_OFF_LH) + sr;
+      const float* pl = (const float*)(st + B_OFF_P) + pi;
       constexpr int T = TX * TY;
-      const float dz = a.dampz[z];
 #pragma unroll
-      for (int r = 0; r < RY; ++r) {
-        const int ry = warp * RY + r;
-        const int pi = ry * TX + lane;
-#pragma unroll
-        for (int kk = 0; kk < 8; ++kk) {
-          sq[r][kk] = sq[r][kk + 1];
-          lq[r][kk] = lq[r][kk + 1];
-        }
-        sq[r][8] = pl[0 * T + pi];
-        lq[r][8] = pl[1 * T + pi];
-        const float a11 = pl[6 * T + pi], a13 = pl[7 * T + pi], a33 = pl[8 * T + pi];
-        const int sr = (ry + kHalo) * HX + lane + kHalo;
-        const int y = y0 + ry;
-        // source wavefield back one level (gradient form)
-        const float sc = sh[sr];
-        const float sxx = lap9(sc, sh[sr - 1], sh[sr + 1], sh[sr - 2], sh[sr + 2], sh[sr - 3],
-                               sh[sr + 3], sh[sr - 4], sh[sr + 4]);
-        const float syy = lap9(sc, sh[sr - HX], sh[sr + HX], sh[sr - 2 * HX], sh[sr + 2 * HX],
-                               sh[sr - 3 * HX], sh[sr + 3 * HX], sh[sr - 4 * HX], sh[sr + 4 * HX]);
-        const float szz = lap9(sq[r][4], sq[r][3], sq[r][5], sq[r][2], sq[r][6], sq[r][1],
-                               sq[r][7], sq[r][0], sq[r][8]);
-        const float sxy_u = fmaf(syy, a.idy2, sxx * a.idx2);
-        const float sz_u = szz * a.idz2;
-        float snx = fmaf(a.dt2, fmaf(a11, sxy_u, a13 * sz_u), 2.f * sc - pl[2 * T + pi]);
-        float snz = fmaf(a.dt2, fmaf(a13, sxy_u, a33 * sz_u), 2.f * sq[r][4] - pl[3 * T + pi]);
-        if (x == a.src.x && y == a.src.y && z == a.src.z) {
-          snx += a.src.amp;
-          snz += a.src.amp;
-        }
-        // imaging with the current adjoint
-        const float lc = lh[sr];
-        const float lz0 = lq[r][4];
-        const float g11 = fmaf(lc, sxy_u, pl[9 * T + pi]);
-        const float g33 = fmaf(lz0, sz_u, pl[11 * T + pi]);
-        const float g13 = fmaf(lz0, sxy_u, fmaf(lc, sz_u, pl[10 * T + pi]));
-        // adjoint, forward form with the sponge
-        const float lxx = lap9(lc, lh[sr - 1], lh[sr + 1], lh[sr - 2], lh[sr + 2], lh[sr - 3],
-                               lh[sr + 3], lh[sr - 4], lh[sr + 4]);
-        const float lyy = lap9(lc, lh[sr - HX], lh[sr + HX], lh[sr - 2 * HX], lh[sr + 2 * HX],
-                               lh[sr - 3 * HX], lh[sr + 3 * HX], lh[sr - 4 * HX], lh[sr + 4 * HX]);
-        const float lzz = lap9(lz0, lq[r][3], lq[r][5], lq[r][2], lq[r][6], lq[r][1], lq[r][7],
-                               lq[r][0], lq[r][8]);
-        const float lxy = fmaf(lyy, a.sy, lxx * a.sx);
-        const float lzs = lzz * a.sz;
-        const float dd = dxy[r] * dz;
-        const float lnx = fmaf(a11, lxy, fmaf(a13, lzs, 2.f * lc - dd * pl[4 * T + pi]));
-        const float lnz = fmaf(a13, lxy, fmaf(a33, lzs, 2.f * lz0 - dd * pl[5 * T + pi]));
-        if (valid[r]) {
-          const long long i = (long long)z * d.plane + off[r];
-          a.spx[i] = snx;
-          a.spz[i] = snz;
-          a.lpx[i] = dd * lnx;
-          a.lpz[i] = dd * lnz;
-          a.g11[i] = g11;
-          a.g13[i] = g13;
-          a.g33[i] = g33;
-        }
+      for (int kk = 0; kk < 8; ++kk) {
+        sq[0][kk] = sq[0][kk + 1];
+        sq[1][kk] = sq[1][kk + 1];
+        lq[0][kk] = lq[0][kk + 1];
+        lq[1][kk] = lq[1][kk + 1];
       }
+      {
+        const float2 s8 = ld2(pl), l8 = ld2(pl + T);
+        sq[0][8] = s8.x;
+        sq[1][8] = s8.y;
+        lq[0][8] = l8.x;
+        lq[1][8] = l8.y;
+      }
+      // x rows (x-4 .. x+5) and y column pairs of both halo fields
+      float rs[10], rl[10];
+#pragma unroll
+      for (int j = 0; j < 5; ++j) {
+        const float2 t = ld2(sh - 4 + 2 * j), u = ld2(lh - 4 + 2 * j);
+        rs[2 * j] = t.x;
+        rs[2 * j + 1] = t.y;
+        rl[2 * j] = u.x;
+        rl[2 * j + 1] = u.y;
+      }
+      float2 sym[4], syp[4], lym[4], lyp[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        sym[j] = ld2(sh - (j + 1) * HX);
+        syp[j] = ld2(sh + (j + 1) * HX);
+        lym[j] = ld2(lh - (j + 1) * HX);
+        lyp[j] = ld2(lh + (j + 1) * HX);
+      }
+      const float2 spx = ld2(pl + 2 * T), spz = ld2(pl + 3 * T);
+      const float2 lpx = ld2(pl + 4 * T), lpz = ld2(pl + 5 * T);
+      const float2 c11 = ld2(pl + 6 * T), c13 = ld2(pl + 7 * T), c33 = ld2(pl + 8 * T);
+      const float2 g11o = ld2(pl + 9 * T);
+      const float2 g13o = kRtm ? make_float2(0.f, 0.f) : ld2(pl + 10 * T);
+      const float2 g33o = kRtm ? make_float2(0.f, 0.f) : ld2(pl + 11 * T);
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[s]);
+      const float dz = a.dampz[z];
+      float snx[2], snz[2], lnx[2], lnz[2], g11[2], g13[2], g33[2];
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        auto pick = [e](float2 v) { return e ? v.y : v.x; };
+        const float a11 = pick(c11), a13 = pick(c13), a33 = pick(c33);
+        // source wavefield back one level (gradient form)
+        const float sc = rs[4 + e];
+        const float sxx = lap9(sc, rs[3 + e], rs[5 + e], rs[2 + e], rs[6 + e], rs[1 + e],
+                               rs[7 + e], rs[e], rs[8 + e]);
+        const float syy = lap9(sc, pick(sym[0]), pick(syp[0]), pick(sym[1]), pick(syp[1]),
+                               pick(sym[2]), pick(syp[2]), pick(sym[3]), pick(syp[3]));
+        const float szz = lap9(sq[e][4], sq[e][3], sq[e][5], sq[e][2], sq[e][6], sq[e][1],
+                               sq[e][7], sq[e][0], sq[e][8]);
+        const float sxy_u = fmaf(syy, a.idy2, sxx * a.idx2);
+        const float sz_u = szz * a.idz2;
+        snx[e] = fmaf(a.dt2, fmaf(a11, sxy_u, a13 * sz_u), 2.f * sc - pick(spx));
+        snz[e] = fmaf(a.dt2, fmaf(a13, sxy_u, a33 * sz_u), 2.f * sq[e][4] - pick(spz));
+        if (x + e == a.src.x && y == a.src.y && z == a.src.z) {
+          snx[e] += a.src.amp;
+          snz[e] += a.src.amp;
+        }
+        // imaging with the current adjoint
+        const float lc = rl[4 + e];
+        const float lz0 = lq[e][4];
+        const float dd = dxy[e] * dz;
+        if (kRtm) {
+          g11[e] = fmaf(fmaf(kTwoThirdF, sc, kOneThirdF * sq[e][4]),
+                        dd * fmaf(kTwoThirdF, lc, kOneThirdF * lz0), pick(g11o));
+        } else {
+          g11[e] = fmaf(lc, sxy_u, pick(g11o));
+          g33[e] = fmaf(lz0, sz_u, pick(g33o));
+          g13[e] = fmaf(lz0, sxy_u, fmaf(lc, sz_u, pick(g13o)));
+        }
+        // adjoint, forward form with the sponge
+        const float lxx = lap9(lc, rl[3 + e], rl[5 + e], rl[2 + e], rl[6 + e], rl[1 + e],
+                               rl[7 + e], rl[e], rl[8 + e]);
+        const float lyy = lap9(lc, pick(lym[0]), pick(lyp[0]), pick(lym[1]), pick(lyp[1]),
+                               pick(lym[2]), pick(lyp[2]), pick(lym[3]), pick(lyp[3]));
+        const float lzz = lap9(lz0, lq[e][3], lq[e][5], lq[e][2], lq[e][6], lq[e][1], lq[e][7],
+                               lq[e][0], lq[e][8]);
+        const float lxy = fmaf(lyy, a.sy, lxx * a.sx);
+        const float lzs = lzz * a.sz;
+        lnx[e] = dd * fmaf(a11, lxy, fmaf(a13, lzs, 2.f * lc - dd * pick(lpx)));
+        lnz[e] = dd * fmaf(a13, lxy, fmaf(a33, lzs, 2.f * lz0 - dd * pick(lpz)));
+      }
+      const long long i = (long long)z * d.plane + off;
+      if (v0 && v1) {
+        *reinterpret_cast<float2*>(a.spx + i) = make_float2(snx[0], snx[1]);
+        *reinterpret_cast<float2*>(a.spz + i) = make_float2(snz[0], snz[1]);
+        *reinterpret_cast<float2*>(a.lpx + i) = make_float2(lnx[0], lnx[1]);
+        *reinterpret_cast<float2*>(a.lpz + i) = make_float2(lnz[0], lnz[1]);
+        *reinterpret_cast<float2*>(a.g11 + i) = make_float2(g11[0], g11[1]);
+        if (!kRtm) {
+          *reinterpret_cast<float2*>(a.g13 + i) = make_float2(g13[0], g13[1]);
+          *reinterpret_cast<float2*>(a.g33 + i) = make_float2(g33[0], g33[1]);
+        }
+      } else {
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          if (e ? v1 : v0) {
+            a.spx[i + e] = snx[e];
+            a.spz[i + e] = snz[e];
+            a.lpx[i + e] = lnx[e];
+            a.lpz[i + e] = lnz[e];
+            a.g11[i + e] = g11[e];
+            if (!kRtm) {
+              a.g13[i + e] = g13[e];
+              a.g33[i + e] = g33[e];
+            }
+          }
+        }
+      }
       if (((z + 1) & 3) == 0 && z + 1 < d.nz) {
 #pragma unroll
-        for (int r = 0; r < RY; ++r) {
+        for (int e = 0; e < 2; ++e) {
 #pragma unroll
-          for (int kk = 0; kk < 4; ++kk) lq[r][kk + 1] *= dxy[r] * a.dampz[z - 3 + kk];
+          for (int kk = 0; kk < 4; ++kk) lq[e][kk + 1] *= dxy[e] * a.dampz[z - 3 + kk];
         }
       }
     }
@@ -603,12 +717,12 @@ int launch_bwd3d_tma(vti_ctx* ctx, const Dims3& d, const TileMaps& scx, const Ti
                      const float* scz_ptr, const float* lcz_ptr, float* spx_ptr, float* spz_ptr,
                      float* lpx_ptr, float* lpz_ptr, float* g11_ptr, float* g13_ptr,
                      float* g33_ptr, const Damping& damp, float dt2, float idx2, float idy2,
-                     float idz2, float sx, float sy, float sz, PointSource src) {
-  static bool attr[64] = {};
-  if (ctx->device >= 64 || !attr[ctx->device]) {
-    VTI_CUDA(ctx, cudaFuncSetAttribute(k_bwd3d_tma, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       B_SMEM));
-    if (ctx->device < 64) attr[ctx->device] = true;
+                     float idz2, float sx, float sy, float sz, PointSource src, bool rtm) {
+  static bool attr[2][64] = {};  // per instantiation and device
+  if (ctx->device >= 64 || !attr[rtm][ctx->device]) {
+    VTI_CUDA(ctx, cudaFuncSetAttribute(rtm ? k_bwd3d_tma<true> : k_bwd3d_tma<false>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, B_SMEM));
+    if (ctx->device < 64) attr[rtm][ctx->device] = true;
   }
   BwdMaps m;
   m.scx = *H(scx); m.scz = *P(scz); m.spx = *P(spx); m.spz = *P(spz);
@@ -629,7 +743,10 @@ int launch_bwd3d_tma(vti_ctx* ctx, const Dims3& d, const TileMaps& scx, const Ti
   const int grid = a.sc.grid;
   {
     LaunchTimer tm(ctx, kTimedBwd3d);
-    k_bwd3d_tma<<<grid, NTHREADS, B_SMEM, ctx->stream>>>(m, a);
+    if (rtm)
+      k_bwd3d_tma<true><<<grid, NTHREADS, B_SMEM, ctx->stream>>>(m, a);
+    else
+      k_bwd3d_tma<false><<<grid, NTHREADS, B_SMEM, ctx->stream>>>(m, a);
   }
   VTI_LAUNCHED(ctx, "k_bwd3d_tma");
   return VTI_OK;

@@ -86,6 +86,8 @@ def _signatures():
         "vti3d_plan_gradient": (C.c_int, [P, P, P, C.c_int, P, C.c_int, P, C.c_int,
                                           C.POINTER(C.c_double)]),
         "vti3d_plan_objfunc": (C.c_int, [P, P, P, C.c_int, P, C.c_int, C.POINTER(C.c_double)]),
+        "vti3d_plan_rtm": (C.c_int, [P, P, P, C.c_int, P, C.c_int, P, C.c_int]),
+        "vti3d_rtm_cij": (C.c_int, [P, P, P, P, P, P, P, P, C.c_int, P, C.c_int, P, P, C.c_uint]),
         "vti3d_plan_wavefield": (VP, [P]),
         "vti3d_model_data_cij": (C.c_int, [P, P, P, P, P, P, P, P, C.c_int, P, C.c_int, P,
                                            C.c_uint]),
@@ -97,6 +99,7 @@ def _signatures():
         "vti2d_init_taper": (None, [P, C.c_int, C.c_int, C.c_int]),
         "vti2d_gradient": (C.c_int, [P] * 11 + [C.c_int, P, C.c_int, P, C.POINTER(C.c_double)]),
         "vti2d_gn_hessian": (C.c_int, [P] * 13 + [C.c_int, P, C.c_int, P]),
+        "vti2d_rtm": (C.c_int, [P] * 9 + [C.c_int, P, C.c_int, P]),
         "vti3d_plan_get_wavefield": (C.c_int, [P, P, C.c_int]),
         "vti3d_gradient_vepsdel": (C.c_int, [P, P, P, P, P, P, P, C.c_float, C.c_float,
                                              C.c_float, P, P, P, C.c_int, P, C.c_int, P, P, P, P,
@@ -137,7 +140,9 @@ def _p(a):
         return C.c_void_p(a)
     if not a.flags["C_CONTIGUOUS"]:
         raise ValueError("array must be C-contiguous")
-    return C.c_void_p(a.ctypes.data)
+    # data_as keeps a reference to the array: a converted temporary such as
+    # _f32(x) stays alive until the foreign call that receives it returns
+    return a.ctypes.data_as(C.c_void_p)
 
 
 def _f32(a):
@@ -265,6 +270,17 @@ class Plan3d:
                                                  C.byref(mis)))
         return fgcij, mis.value
 
+    def rtm(self, souloc, shotid, data, data_mem=MEM_HOST, image=None, image_mem=MEM_HOST):
+        """rtmCij3d_f on the resident model: the image (nxyz)."""
+        souloc, shotid = _f32(souloc).reshape(-1), _i32(shotid)
+        if data_mem == MEM_HOST:
+            data = _f32(data)
+        if image is None:
+            image = np.zeros(self.g.nx * self.g.ny * self.g.nz, dtype=np.float32)
+        self.ctx.check(lib().vti3d_plan_rtm(self._h, _p(souloc), _p(shotid), len(shotid),
+                                            _p(data), data_mem, _p(image), image_mem))
+        return image
+
     def objfunc(self, souloc, shotid, dobs, dobs_mem=MEM_HOST):
         souloc, shotid = _f32(souloc).reshape(-1), _i32(shotid)
         if dobs_mem == MEM_HOST:
@@ -300,6 +316,18 @@ def modelDataCij3d_f(ctx, g: Geom3d, souloc, shotid, recloc, wavelet, c11, c13, 
                                          _p(_f32(c33)), _p(_f32(wavelet)), _p(souloc),
                                          _p(shotid), len(shotid), _p(recloc), nrtot, _p(out),
                                          flags))
+    return out
+
+
+def rtmCij3d_f(ctx, g: Geom3d, souloc, shotid, recloc, wavelet, c11, c13, c33, data, flags=0):
+    """rtmCij3d_f (lib/vti-fwi-3d/gpu/rtm3d_f.cu:161): returns the image (nxyz)."""
+    souloc, recloc = _f32(souloc).reshape(-1), _f32(recloc).reshape(-1)
+    shotid = _i32(shotid)
+    out = np.zeros(g.nx * g.ny * g.nz, dtype=np.float32)
+    ctx.check(lib().vti3d_rtm_cij(ctx.handle, C.byref(g), _p(_f32(c11)), _p(_f32(c13)),
+                                  _p(_f32(c33)), _p(_f32(wavelet)), _p(souloc), _p(shotid),
+                                  len(shotid), _p(recloc), recloc.size // 4, _p(_f32(data)),
+                                  _p(out), flags))
     return out
 
 
@@ -343,6 +371,16 @@ def objFuncGradient_f(ctx, g: Geom2d, data, c11, c13, c33, wavelet, sloc, rloc, 
                                    _p(_f32(wavelet)), _p(sloc), sloc.size // 4, _p(rloc),
                                    rloc.size // 2, _p(_f32(taper)), C.byref(mis)))
     return out[0], out[1], out[2], mis.value
+
+
+def rtm_f(ctx, g: Geom2d, data, c11, c13, c33, wavelet, sloc, rloc, taper):
+    """rtm_f (lib/vti-fwi-2d/rtm_f.cu:13): the migrated image (nnxz)."""
+    sloc, rloc = _i32(sloc).reshape(-1), _i32(rloc).reshape(-1)
+    out = np.zeros((g.nx + 2 * g.npad) * (g.nz + 2 * g.npad), dtype=np.float32)
+    ctx.check(lib().vti2d_rtm(ctx.handle, C.byref(g), _p(out), _p(_f32(data)), _p(_f32(c11)),
+                              _p(_f32(c13)), _p(_f32(c33)), _p(_f32(wavelet)), _p(sloc),
+                              sloc.size // 4, _p(rloc), rloc.size // 2, _p(_f32(taper))))
+    return out
 
 
 def GNhessian_f(ctx, g: Geom2d, c11, c13, c33, dc11, dc13, dc33, wavelet, sloc, rloc, taper):
