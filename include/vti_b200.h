@@ -157,6 +157,13 @@ int vti3d_plan_objfunc(vti3d_plan* plan, const float* souloc, const int* shotid,
  * model; no sponge on the source wavefield. */
 int vti3d_plan_rtm(vti3d_plan* plan, const float* souloc, const int* shotid, int nshot,
                    const float* data, int data_mem, float* image, int image_mem);
+/* Wavelet gradient (waveletGradientCij3d_f, lib/vti-fwi-3d/gpu/modelData3d_f.cu:858):
+ * gwavelet (nt) = dt2 * sum over shots and levels of lambda_x + lambda_z at the
+ * source, the adjoint wavefield driven by the traces `data` (nnt x nrec_total)
+ * with the sponge and the model's pad (the random boundary is not used). */
+int vti3d_plan_wavelet_gradient(vti3d_plan* plan, const float* souloc, const int* shotid,
+                                int nshot, const float* data, int data_mem, float* gwavelet,
+                                int mem);
 /* Device pointer of the last forward wavefield sigma_x (pitched volume). */
 const float* vti3d_plan_wavefield(vti3d_plan* plan);
 /* Copies the last forward level of sigma_x (the "wavefield" output of
@@ -172,6 +179,11 @@ int vti3d_gradient_cij(vti_ctx* ctx, const vti3d_geom* g, const float* cij, cons
                        const float* randb, const float* wavelet, const float* souloc,
                        const int* shotid, int nshot, const float* recloc, int nrec_total,
                        const float* dobs, float* fgcij, double* misfit, unsigned flags);
+/* waveletGradientCij3d_f with host buffers (modelData3d_f.cu:858). */
+int vti3d_wavelet_gradient_cij(vti_ctx* ctx, const vti3d_geom* g, const float* c11,
+                               const float* c13, const float* c33, const float* souloc,
+                               const int* shotid, int nshot, const float* recloc, int nrec_total,
+                               const float* data, float* gwavelet, unsigned flags);
 /* rtmCij3d_f with host buffers: the model as given (rtm3d_f.cu:161). */
 int vti3d_rtm_cij(vti_ctx* ctx, const vti3d_geom* g, const float* c11, const float* c13,
                   const float* c33, const float* wavelet, const float* souloc, const int* shotid,
@@ -232,6 +244,13 @@ int vti2d_gn_hessian(vti_ctx* ctx, const vti2d_geom* g, float* gc11, float* gc13
 int vti2d_rtm(vti_ctx* ctx, const vti2d_geom* g, float* image, const float* data,
               const float* c11, const float* c13, const float* c33, const float* wavelet,
               const int* sloc, int ns, const int* rloc, int nr, const float* taper);
+/* waveletGradient_f (lib/vti-fwi-2d/objFuncGradient_f.cu:373): gradient of the
+ * misfit with respect to the source wavelet (nt floats): dt2 (p + q) of the
+ * adjoint wavefield at the source for every level, the adjoint driven by the
+ * traces data[(it/ratio)*nr + ir] (injected as points). */
+int vti2d_wavelet_gradient(vti_ctx* ctx, const vti2d_geom* g, float* gwavelet, const float* data,
+                           const float* c11, const float* c13, const float* c33,
+                           const int* sloc, int ns, const int* rloc, int nr, const float* taper);
 /* 2D taper of lib/vti-fwi-2d/init.cpp:70-89 ((nx+2npad)*(nz+2npad) floats). */
 void vti2d_init_taper(float* taper, int nx, int nz, int npad);
 

@@ -77,6 +77,19 @@ void rtmVEpsDel(float* image, float* souloc, int ns, std::vector<int>& shotid, f
                 int ny, int nz, int nt, int npad, float ox, float oy, float oz, float ot,
                 float dx, float dy, float dz, float dt, float samplingRate, float wbottom);
 
+// wave3d.h:112 / :114 — gradient of the misfit w.r.t. the source wavelet (nt
+// floats), the adjoint driven by the traces in ddata (nnt*irbegin layout).
+void waveletGradient3d_f(float* gwavelet, const float* ddata, float* souloc, int ns,
+                         std::vector<int>& shotid, float* recloc, float* c11, float* c13,
+                         float* c33, int nx, int ny, int nz, int nt, int npad, float ox, float oy,
+                         float oz, float ot, float dx, float dy, float dz, float dt,
+                         float samplingRate, std::vector<int>& GPUs, int ngpugroup);
+void waveletGradientCij3d_f(float* gwavelet, const float* ddata, float* souloc, int ns,
+                            std::vector<int>& shotid, float* recloc, float* c11, float* c13,
+                            float* c33, int nx, int ny, int nz, int nt, int npad, float ox,
+                            float oy, float oz, float ot, float dx, float dy, float dz, float dt,
+                            float samplingRate, std::vector<int>& GPUs);
+
 // wave3d.h:108 / :110 — forward modeling into memory, ddata[nnt*irbegin ...].
 void modelData3d_f(float* ddata, float* souloc, int ns, std::vector<int>& shotid, float* recloc,
                    const float* wavelet, float* c11, float* c13, float* c33, int nx, int ny,
@@ -140,5 +153,11 @@ void rtm_f(float* image, const float* data, const float* c11, const float* c13, 
            const float* wavelet, const int* sloc, int ns, const int* rloc, int nr,
            const float* taper, int nx, int nz, int nt, int npad, float dx, float dz, float dt,
            float rate, float ot = 0.);
+
+// wave.h:18 — gradient w.r.t. the source wavelet (nt floats).
+void waveletGradient_f(float* gwavelet, const float* d0, const float* c11, const float* c13,
+                       const float* c33, const int* sloc, int ns, const int* rloc, int nr,
+                       const float* taper, int nx, int nz, int nt, int npad, float dx, float dz,
+                       float dt, float rate);
 
 #endif  // VTI_WAVE_H

@@ -124,6 +124,21 @@ def rtm3d(g, c11, c13, c33, wavelet, souloc, shotid, recloc, data, dtype=np.floa
     return out
 
 
+def wavelet_gradient3d(g, c11, c13, c33, souloc, shotid, recloc, data, dtype=np.float64,
+                       full_steps=False):
+    """waveletGradientCij3d_f restated: the gradient w.r.t. the wavelet (nt)."""
+    ip, fp = _geo3(g, full_steps)
+    out = np.zeros(g.nt, dtype=dtype)
+    suf = "f64" if dtype == np.float64 else "f32"
+    f = getattr(lib(), f"orc3d_wavelet_gradient_{suf}")
+    f.argtypes = [VP] * 7 + [C.c_int, VP, VP, VP]
+    f.restype = C.c_int
+    shotid = _i32(shotid)
+    f(_p(ip), _p(fp), _p(_f32(c11)), _p(_f32(c13)), _p(_f32(c33)), _p(_f32(souloc)), _p(shotid),
+      len(shotid), _p(_f32(recloc).reshape(-1)), _p(_f32(data)), _p(out))
+    return out
+
+
 def damping3d(nx, ny, nz, npad):
     out = np.zeros(nx * ny + nz, dtype=np.float32)
     lib().orc3d_damping(nx, ny, nz, npad, _p(out))
@@ -194,6 +209,21 @@ def rtm2d(g, c11, c13, c33, wavelet, sloc, rloc, taper, data, dtype=np.float64):
     f(_p(ip), _p(fp), _p(_f32(c11)), _p(_f32(c13)), _p(_f32(c33)), _p(_f32(wavelet)),
       _p(_f32(data)), _p(sloc), sloc.size // 4, _p(rloc), rloc.size // 2, _p(_f32(taper)),
       _p(out))
+    return out
+
+
+def wavelet_gradient2d(g, c11, c13, c33, sloc, rloc, taper, data, dtype=np.float64):
+    """waveletGradient_f restated: the gradient w.r.t. the wavelet (nt)."""
+    suf = "f64" if dtype == np.float64 else "f32"
+    f = getattr(lib(), f"orc2d_wavelet_gradient_{suf}")
+    f.argtypes = [VP] * 7 + [C.c_int, VP, C.c_int, VP, VP]
+    f.restype = C.c_int
+    ip = np.array([g.nx, g.nz, g.nt, g.npad], dtype=np.int32)
+    fp = np.array([g.dx, g.dz, g.dt, g.rate, g.ot], dtype=np.float32)
+    out = np.zeros(g.nt, dtype=dtype)
+    sloc, rloc = _i32(sloc).reshape(-1), _i32(rloc).reshape(-1)
+    f(_p(ip), _p(fp), _p(_f32(c11)), _p(_f32(c13)), _p(_f32(c33)), _p(_f32(data)), _p(sloc),
+      sloc.size // 4, _p(rloc), rloc.size // 2, _p(_f32(taper)), _p(out))
     return out
 
 

@@ -2,7 +2,7 @@
 // sources by oracle/build_ref.sh into oracle/_ref/ref2d) on inputs written by
 // tests/golden/make_golden.py. TEST INFRASTRUCTURE ONLY.
 //
-// usage: ref2d <dir> synthetic|modeling|grad|gnhess|rtm
+// usage: ref2d <dir> synthetic|modeling|grad|gnhess|rtm|wgrad
 //   <dir>/params.txt : nx nz nt npad dx dz dt rate ot ns nr
 //   <dir>/{c11,c13,c33,taper,wavelet}.bin (float32), sloc.bin / rloc.bin (int32)
 #include <cstdio>
@@ -36,6 +36,11 @@ void rtm_f(float* image, const float* data, const float* c11, const float* c13, 
            const float* wavelet, const int* sloc, int ns, const int* rloc, int nr,
            const float* taper, int nx, int nz, int nt, int npad, float dx, float dz, float dt,
            float rate, float ot);
+
+void waveletGradient_f(float* gwavelet, const float* d0, const float* c11, const float* c13,
+                       const float* c33, const int* sloc, int ns, const int* rloc, int nr,
+                       const float* taper, int nx, int nz, int nt, int npad, float dx, float dz,
+                       float dt, float rate);
 
 template <typename T>
 static std::vector<T> load(const std::string& path, size_t n) {
@@ -126,6 +131,16 @@ int main(int argc, char** argv) {
     rtm_f(image.data(), data.data(), c11.data(), c13.data(), c33.data(), wavelet.data(),
           sloc.data(), ns, rloc.data(), nr, taper.data(), nx, nz, nt, npad, dx, dz, dt, rate, ot);
     save(dir + "/ref_rtm.bin", image.data(), image.size());
+  } else if (mode == "wgrad") {
+    // <dir>/data.bin: the traces driving the adjoint (nnt = (nt-1)/ratio+1 rows)
+    auto rloc = load<int>(dir + "/rloc.bin", 2 * (size_t)nr);
+    const int ratio = (int)(rate / dt + 0.5);
+    const size_t rows = (nt - 1) / ratio + 1;
+    auto data = load<float>(dir + "/data.bin", rows * nr);
+    std::vector<float> gw(nt, 0.f);
+    waveletGradient_f(gw.data(), data.data(), c11.data(), c13.data(), c33.data(), sloc.data(), ns,
+                      rloc.data(), nr, taper.data(), nx, nz, nt, npad, dx, dz, dt, rate);
+    save(dir + "/ref_wgrad.bin", gw.data(), gw.size());
   } else {
     return 2;
   }

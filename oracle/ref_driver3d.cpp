@@ -3,11 +3,12 @@
 // tests/golden/make_golden.py. TEST INFRASTRUCTURE ONLY: it produces golden
 // traces and gradients that pin the oracle; nothing in the library uses it.
 //
-// usage: ref3d <dir> model|grad|rtm
+// usage: ref3d <dir> model|grad|rtm|wgrad
 //   <dir>/params.txt : nx ny nz nt npad ox oy oz ot dx dy dz dt rate ns nrec
 //   <dir>/{souloc,recloc,wavelet,cij,padb,randb,dobs}.bin (float32)
 //   writes <dir>/ref_ddata.bin (model), <dir>/ref_fgcij.bin (grad) or
-//   <dir>/ref_image.bin (rtm: the traces in dobs.bin migrated with cij)
+//   <dir>/ref_image.bin (rtm: the traces in dobs.bin migrated with cij) or
+//   <dir>/ref_wgrad.bin (wgrad: wavelet gradient driven by dobs.bin)
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
@@ -26,6 +27,11 @@ void objFuncGradientCij3d_f(float* fgcij, float* souloc, int ns, std::vector<int
                             float* randboundaryCij, int nx, int ny, int nz, int nt, int npad,
                             float ox, float oy, float oz, float ot, float dx, float dy, float dz,
                             float dt, float samplingRate, std::vector<int>& GPUs);
+void waveletGradientCij3d_f(float* gwavelet, const float* ddata, float* souloc, int ns,
+                            std::vector<int>& shotid, float* recloc, float* c11, float* c13,
+                            float* c33, int nx, int ny, int nz, int nt, int npad, float ox,
+                            float oy, float oz, float ot, float dx, float dy, float dz, float dt,
+                            float samplingRate, std::vector<int>& GPUs);
 void rtmCij3d_f(float* image, float* souloc, int ns, std::vector<int>& shotid, float* recloc,
                 float* wavelet, float* c11, float* c13, float* c33, int nx, int ny, int nz,
                 int nt, int npad, float ox, float oy, float oz, float ot, float dx, float dy,
@@ -53,7 +59,7 @@ static void save(const std::string& path, const float* p, size_t n) {
 
 int main(int argc, char** argv) {
   if (argc < 3) {
-    std::fprintf(stderr, "usage: %s <dir> model|grad|rtm\n", argv[0]);
+    std::fprintf(stderr, "usage: %s <dir> model|grad|rtm|wgrad\n", argv[0]);
     return 2;
   }
   const std::string dir = argv[1], mode = argv[2];
@@ -109,6 +115,13 @@ int main(int argc, char** argv) {
                cij.data() + n, cij.data() + 2 * n, nx, ny, nz, nt, npad, ox, oy, oz, ot, dx, dy,
                dz, dt, rate);
     save(dir + "/ref_image.bin", image.data(), image.size());
+  } else if (mode == "wgrad") {
+    auto data = load(dir + "/dobs.bin", (size_t)nnt * nrec);
+    std::vector<float> gw(nt, 0.f);
+    waveletGradientCij3d_f(gw.data(), data.data(), souloc.data(), ns, shotid, recloc.data(),
+                           cij.data(), cij.data() + n, cij.data() + 2 * n, nx, ny, nz, nt, npad,
+                           ox, oy, oz, ot, dx, dy, dz, dt, rate, gpus);
+    save(dir + "/ref_wgrad.bin", gw.data(), gw.size());
   } else {
     std::fprintf(stderr, "unknown mode %s\n", mode.c_str());
     return 2;

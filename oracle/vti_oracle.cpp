@@ -481,6 +481,57 @@ void rtm3d(const Geo3& g, const float* c11, const float* c13, const float* c33,
   }
 }
 
+// waveletGradientCij3d_f (lib/vti-fwi-3d/gpu/modelData3d_f.cu:858-1294): the
+// adjoint wavefield alone, seeded with the last data sample (:1048-1053),
+// stepped with the forward operator, fed the data interpolated at it+1 and
+// damped by the sponge; extractAdjWfldAtSouLoc (injectRecord3d.cu:9-12) adds
+// lambda_x + lambda_z of the new level at the source, as the step computed
+// it (before the residual injection and the sponge), into g[it]; finally
+// g *= dt2 (:1293). Here the undamped value is the stored one over the sponge
+// factor d at the source.
+template <typename T>
+void wavelet_grad3d(const Geo3& g, const float* c11, const float* c13, const float* c33,
+                    const float* souloc, const int* shotid, int nshot, const float* recloc,
+                    const float* data, T* gw) {
+  const long n = g.nxyz(), nxy = g.nxy();
+  const float dt2 = g.dt * g.dt;
+  const int st = sampling_step(g.rate, g.dt);
+  const int nnt = (g.nt - 1) / st + 1;
+  const int M = last_level(g);
+  std::fill(gw, gw + g.nt, (T)0);
+  Damp3 damp(g);
+  std::vector<T> lcx, lcz, lpx, lpz;
+  for (int k = 0; k < nshot; ++k) {
+    Shot3 s = make_shot3(g, souloc, recloc, shotid[k]);
+    const float* dat = data + (long)nnt * s.irbegin;
+    lcx.assign(n, 0); lcz.assign(n, 0); lpx.assign(n, 0); lpz.assign(n, 0);
+    for (int ir = 0; ir < s.nr; ++ir) {
+      if (!s.inner[ir]) continue;
+      T temp = (T)dt2 * (T)dat[(nnt - 1) + (long)ir * nnt];
+      lcx[s.seed[ir]] = (T)kTwoThird * temp;
+      lcz[s.seed[ir]] = (T)kOneThird * temp;
+    }
+    const T ds = (T)damp.at(s.sidx % nxy, (int)(s.sidx / nxy));
+    for (int i = 0; i < M - 1; ++i) {
+      const int it = g.nt - 3 - i;
+      step3d<T, true>(g, c11, c13, c33, lcx.data(), lcz.data(), lpx.data(), lpz.data(), &damp,
+                      nullptr, nullptr, nullptr, nullptr, nullptr);
+      gw[it] += (lpx[s.sidx] + lpz[s.sidx]) / ds;
+      for (int ir = 0; ir < s.nr; ++ir) {
+        if (!s.inner[ir]) continue;
+        std::vector<T> tr(dat + (long)ir * nnt, dat + (long)(ir + 1) * nnt);
+        T inj = (T)dt2 * interp_residual<T>(tr.data(), it + 1, nnt, st);
+        long ri = s.ridx[ir];
+        T d = (T)damp.at(ri % nxy, (int)(ri / nxy));
+        lpx[ri] += d * ((T)kTwoThird * inj);
+        lpz[ri] += d * ((T)kOneThird * inj);
+      }
+      std::swap(lcx, lpx); std::swap(lcz, lpz);
+    }
+  }
+  for (int it = 0; it < g.nt; ++it) gw[it] *= (T)dt2;
+}
+
 // ----------------------------------------------------------------- 2D ------
 struct Geo2 {
   int nx, nz, nt, npad;
@@ -634,6 +685,61 @@ void rtm2d(const Geo2& g, const float* c11, const float* c13, const float* c33,
       std::swap(p0, p1);
       std::swap(q0, q1);
     }
+  }
+}
+
+// waveletGradient_f (lib/vti-fwi-2d/objFuncGradient_f.cu:373-530): per shot
+// the adjoint wavefield (forwardCD, point injection of the data interpolated
+// at it+1, taper), g[it] = dt2 (p + q) at the source after the taper
+// (extractWavelet, kernels.cu:258-261; an assignment), g[nt-2] from the
+// seeded level; shots summed. ratio uses a double 0.5 here (:375). The second
+// data row of the first step is weighted 0 (the reference leaves that buffer
+// uninitialised; it is taken as zero).
+template <typename T>
+void wavelet_grad2d(const Geo2& g, const float* c11, const float* c13, const float* c33,
+                    const float* data, const int* sloc, int ns, const int* rloc, int nr_total,
+                    const float* taper, T* gw) {
+  const long nnx = g.nnx(), nnxz = nnx * g.nnz();
+  const float dt = g.dt, dt2 = dt * dt;
+  const int ratio = (int)(g.rate / dt + 0.5);
+  const int nnt = (g.nt - 1) / ratio + 1;
+  std::fill(gw, gw + g.nt, (T)0);
+  for (int is = 0; is < ns; ++is) {
+    const long sxz = sloc[4 * is] + (long)sloc[4 * is + 1] * nnx;
+    const int nri = sloc[4 * is + 2], ir0 = sloc[4 * is + 3];
+    std::vector<T> gs(g.nt, 0);
+    std::vector<T> p0(nnxz, 0), q0(nnxz, 0), p1(nnxz, 0), q1(nnxz, 0);
+    std::vector<float> d0(nri, 0.f), d1(nri, 0.f);
+    for (int ir = 0; ir < nri; ++ir) d0[ir] = data[(long)(nnt - 1) * nr_total + ir0 + ir];
+    auto inject = [&](T* p, T* q, float f) {  // injectData (kernels.cu:208-217)
+      for (int ir = 0; ir < nri; ++ir) {
+        long i = rloc[2 * (ir0 + ir)] + (long)rloc[2 * (ir0 + ir) + 1] * nnx;
+        float s = 0.5f * ((1.f - f) * d0[ir] + f * d1[ir]);
+        p[i] += (T)(dt2 * s);
+        q[i] += (T)(dt2 * s);
+      }
+    };
+    inject(p0.data(), q0.data(), 0.f);
+    taper2d(g, taper, p0.data());
+    taper2d(g, taper, q0.data());
+    gs[g.nt - 2] = (T)dt2 * (p0[sxz] + q0[sxz]);
+    for (int it = g.nt - 3; it >= 0; --it) {
+      step2d<T>(g, c11, c13, c33, p0.data(), q0.data(), p1.data(), q1.data());
+      float f = (it + 1.) / ratio;
+      int i1 = (int)f;
+      if ((it + 2) % ratio == 0) {
+        for (int ir = 0; ir < nri; ++ir) d1[ir] = data[(long)i1 * nr_total + ir0 + ir];
+        std::swap(d0, d1);
+      }
+      f = f - i1;
+      inject(p1.data(), q1.data(), f);
+      taper2d(g, taper, p0.data()); taper2d(g, taper, q0.data());
+      taper2d(g, taper, p1.data()); taper2d(g, taper, q1.data());
+      gs[it] = (T)dt2 * (p1[sxz] + q1[sxz]);
+      std::swap(p0, p1);
+      std::swap(q0, q1);
+    }
+    for (int it = 0; it < g.nt; ++it) gw[it] += gs[it];
   }
 }
 
@@ -1021,6 +1127,18 @@ ORC3D_GRAD(float, f32)
 ORC3D_RTM(double, f64)
 ORC3D_RTM(float, f32)
 
+#define ORC3D_WGRAD(T, SUF)                                                                    \
+  int orc3d_wavelet_gradient_##SUF(const int* ip, const float* fp, const float* c11,            \
+                                   const float* c13, const float* c33, const float* souloc,     \
+                                   const int* shotid, int nshot, const float* recloc,           \
+                                   const float* data, T* gw) {                                  \
+    Geo3 g = unpack3(ip, fp);                                                                   \
+    wavelet_grad3d<T>(g, c11, c13, c33, souloc, shotid, nshot, recloc, data, gw);               \
+    return 0;                                                                                   \
+  }
+ORC3D_WGRAD(double, f64)
+ORC3D_WGRAD(float, f32)
+
 // Time `nsteps` forward steps (forward form, sponge) of a zero-initialised
 // grid with a point source: the FP32 instance is the CPU baseline's unit of
 // work. Returns the number of threads used.
@@ -1096,6 +1214,18 @@ ORC2D_GRAD(float, f32)
   }
 ORC2D_RTM(double, f64)
 ORC2D_RTM(float, f32)
+
+#define ORC2D_WGRAD(T, SUF)                                                                     \
+  int orc2d_wavelet_gradient_##SUF(const int* ip, const float* fp, const float* c11,             \
+                                   const float* c13, const float* c33, const float* data,        \
+                                   const int* sloc, int ns, const int* rloc, int nr,             \
+                                   const float* taper, T* gw) {                                  \
+    Geo2 g = unpack2(ip, fp);                                                                    \
+    wavelet_grad2d<T>(g, c11, c13, c33, data, sloc, ns, rloc, nr, taper, gw);                    \
+    return 0;                                                                                    \
+  }
+ORC2D_WGRAD(double, f64)
+ORC2D_WGRAD(float, f32)
 
 // The checkpoint pairing of the 2D gradient: 3 values (a, b, f) per imaging
 // step, nt-1 steps. Returns the number of steps.

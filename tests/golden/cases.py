@@ -79,6 +79,21 @@ CASES2D = ["g2_a"]
 # drivers pass it (rtm3d_f.cu:139-148).
 RTM_CASES3D = ["g3_a"]
 RTM_CASES2D = ["g2_a"]
+# wavelet-gradient fixtures (<case>_wgrad.npz): the adjoint driven by the
+# case's observed traces; in 3D the model carries the pad boundary (the
+# sponge model), as the source-inversion drivers pass it.
+WGRAD_CASES3D = ["g3_a"]
+WGRAD_CASES2D = ["g2_a"]
+
+
+def pad_model3d(c: dict) -> np.ndarray:
+    """cij of a 3D case with its pad boundary put into the pad region."""
+    import vtib200 as V
+    s = c["s"]
+    n = s.nxyz
+    return np.concatenate([V.put_boundary(c["padb"][k * s.nb:(k + 1) * s.nb],
+                                          c["cij"][k * n:(k + 1) * n], s.nx, s.ny, s.nz,
+                                          s.npad) for k in range(3)])
 
 
 def rtm_model3d(c: dict) -> np.ndarray:

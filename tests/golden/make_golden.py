@@ -149,11 +149,45 @@ def make_rtm2d(name, out):
     print(name, "rtm image max", np.abs(image).max())
 
 
+def make_wgrad3d(name, out):
+    """waveletGradientCij3d_f of the reference, driven by the golden dobs."""
+    c = K.case3d(name)
+    s = c["s"]
+    dobs = np.load(HERE / f"{name}.npz")["dobs"]
+    model = K.pad_model3d(c)
+    with tempfile.TemporaryDirectory() as td:
+        d = Path(td)
+        write_inputs3d(c, d)
+        model.astype(np.float32).tofile(d / "cij.bin")
+        dobs.astype(np.float32).tofile(d / "dobs.bin")
+        run("ref3d", d, "wgrad")
+        gw = np.fromfile(d / "ref_wgrad.bin", dtype=np.float32)
+    np.savez_compressed(out / f"{name}_wgrad.npz", gwavelet=gw,
+                        inputs=K.digest(s.souloc, s.recloc, model, dobs))
+    print(name, "wavelet gradient max", np.abs(gw).max())
+
+
+def make_wgrad2d(name, out):
+    """waveletGradient_f of the reference, driven by the golden dobs."""
+    c = K.case2d(name)
+    s = c["s"]
+    dobs = np.load(HERE / f"{name}.npz")["dobs"]
+    with tempfile.TemporaryDirectory() as td:
+        d = Path(td)
+        write_inputs2d(s, d)
+        dobs.astype(np.float32).tofile(d / "data.bin")
+        run("ref2d", d, "wgrad")
+        gw = np.fromfile(d / "ref_wgrad.bin", dtype=np.float32)
+    np.savez_compressed(out / f"{name}_wgrad.npz", gwavelet=gw,
+                        inputs=K.digest(s.c11, s.c13, s.c33, s.taper, s.sloc, s.rloc, dobs))
+    print(name, "wavelet gradient max", np.abs(gw).max())
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=str(HERE))
-    ap.add_argument("--only", choices=["all", "rtm"], default="all",
-                    help="rtm: only the RTM fixtures (needs the case fixtures)")
+    ap.add_argument("--only", choices=["all", "rtm", "wgrad"], default="all",
+                    help="rtm / wgrad: only those fixtures (needs the case fixtures)")
     a = ap.parse_args()
     out = Path(a.out)
     out.mkdir(parents=True, exist_ok=True)
@@ -162,10 +196,16 @@ def main():
             make3d(n, out)
         for n in K.CASES2D:
             make2d(n, out)
-    for n in K.RTM_CASES3D:
-        make_rtm3d(n, out)
-    for n in K.RTM_CASES2D:
-        make_rtm2d(n, out)
+    if a.only in ("all", "rtm"):
+        for n in K.RTM_CASES3D:
+            make_rtm3d(n, out)
+        for n in K.RTM_CASES2D:
+            make_rtm2d(n, out)
+    if a.only in ("all", "wgrad"):
+        for n in K.WGRAD_CASES3D:
+            make_wgrad3d(n, out)
+        for n in K.WGRAD_CASES2D:
+            make_wgrad2d(n, out)
 
 
 if __name__ == "__main__":

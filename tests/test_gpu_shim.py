@@ -118,3 +118,28 @@ def test_shim_rtm2d_matches_reference(drivers, name):
         _run(drivers["2d"], d, "rtm")
         img = np.fromfile(d / "ref_rtm.bin", dtype=np.float32)
     assert rel_l2(img, load_golden(f"{name}_rtm")["image"]) < 1e-4
+
+
+@pytest.mark.parametrize("name", K.WGRAD_CASES3D)
+def test_shim_wavelet_gradient3d_matches_reference(drivers, name):
+    c = K.case3d(name)
+    with tempfile.TemporaryDirectory() as td:
+        d = Path(td)
+        MG.write_inputs3d(c, d)
+        K.pad_model3d(c).astype(np.float32).tofile(d / "cij.bin")
+        np.asarray(load_golden(name)["dobs"], np.float32).tofile(d / "dobs.bin")
+        _run(drivers["3d"], d, "wgrad")
+        gw = np.fromfile(d / "ref_wgrad.bin", dtype=np.float32)
+    assert rel_l2(gw, load_golden(f"{name}_wgrad")["gwavelet"]) < 1e-4
+
+
+@pytest.mark.parametrize("name", K.WGRAD_CASES2D)
+def test_shim_wavelet_gradient2d_matches_reference(drivers, name):
+    s = K.case2d(name)["s"]
+    with tempfile.TemporaryDirectory() as td:
+        d = Path(td)
+        MG.write_inputs2d(s, d)
+        np.asarray(load_golden(name)["dobs"], np.float32).tofile(d / "data.bin")
+        _run(drivers["2d"], d, "wgrad")
+        gw = np.fromfile(d / "ref_wgrad.bin", dtype=np.float32)
+    assert rel_l2(gw, load_golden(f"{name}_wgrad")["gwavelet"]) < 1e-4

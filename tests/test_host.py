@@ -143,3 +143,21 @@ def test_taper2d_profile():
     np.testing.assert_allclose(t[nz // 2 + npad, :npad], t0, rtol=1e-7)
     np.testing.assert_allclose(t[nz // 2 + npad, -npad:], t0[::-1], rtol=1e-7)
     np.testing.assert_allclose(t[0, 0], t0[0] * t0[0], rtol=1e-6)
+
+
+def header_prototypes():
+    """name -> parameter count of every function declared in vti_b200.h."""
+    txt = (ROOT / "include" / "vti_b200.h").read_text()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    out = {}
+    for m in re.finditer(r"\b(vti\w+)\s*\(([^;{]*?)\)\s*;", txt, flags=re.S):
+        params = m.group(2).strip()
+        out[m.group(1)] = 0 if params in ("", "void") else params.count(",") + 1
+    return out
+
+
+def test_binding_argument_counts_match_header():
+    protos = header_prototypes()
+    wrong = {name: (len(args), protos[name]) for name, (_, args) in V._signatures().items()
+             if name in protos and len(args) != protos[name]}
+    assert not wrong, wrong

@@ -185,3 +185,32 @@ def test_oracle_rtm2d_matches_reference(name):
     o = O.rtm2d(g, s.c11, s.c13, s.c33, s.wavelet, s.sloc, s.rloc, s.taper, dobs)
     assert np.abs(o).max() > 0
     assert rel_l2(o, gold["image"]) < 1e-4
+
+
+@pytest.mark.parametrize("name", K.WGRAD_CASES3D)
+def test_oracle_wavelet_gradient3d_matches_reference(name):
+    """waveletGradientCij3d_f restated (FP64) against the reference's output."""
+    c = K.case3d(name)
+    s = c["s"]
+    g = s.geom()
+    n = s.nxyz
+    model = K.pad_model3d(c)
+    dobs = load_golden(name)["dobs"]
+    gold = load_golden(f"{name}_wgrad")
+    assert gold["inputs"] == K.digest(s.souloc, s.recloc, model, dobs)
+    o = O.wavelet_gradient3d(g, *_split(model, n), s.souloc, c["shotid"], s.recloc, dobs)
+    assert np.abs(o).max() > 0
+    assert rel_l2(o, gold["gwavelet"]) < 1e-4
+
+
+@pytest.mark.parametrize("name", K.WGRAD_CASES2D)
+def test_oracle_wavelet_gradient2d_matches_reference(name):
+    """waveletGradient_f restated (FP64) against the reference's output."""
+    s = K.case2d(name)["s"]
+    g = s.geom()
+    dobs = load_golden(name)["dobs"]
+    gold = load_golden(f"{name}_wgrad")
+    assert gold["inputs"] == K.digest(s.c11, s.c13, s.c33, s.taper, s.sloc, s.rloc, dobs)
+    o = O.wavelet_gradient2d(g, s.c11, s.c13, s.c33, s.sloc, s.rloc, s.taper, dobs)
+    assert np.abs(o).max() > 0
+    assert rel_l2(o, gold["gwavelet"]) < 1e-4

@@ -118,6 +118,14 @@ struct PointSource {
   float amp = 0.f;             // added to next before the sponge
 };
 
+// One grid point of the new level read out by the step kernel:
+// *out += next_x + next_z as the stencil computed it (before the source and
+// the sponge). x < 0 disables.
+struct Probe {
+  int x = -1, y = -1, z = -1;
+  float* out = nullptr;
+};
+
 // TMA descriptors (CUtensorMap, 128 bytes each) of one volume: 32 x 16 tiles
 // and 40 x 24 tiles (with the 4-cell halo). Plain storage keeps cuda.h out
 // of this header.
@@ -134,7 +142,7 @@ int launch_fwd3d_tma(vti_ctx* ctx, const Dims3& d, const TileMaps& cx, const Til
                      const TileMaps& px, const TileMaps& pz, const TileMaps& c11,
                      const TileMaps& c13, const TileMaps& c33, const float* cz_ptr,
                      float* px_ptr, float* pz_ptr, const Damping* damp, float sx, float sy,
-                     float sz, PointSource src);
+                     float sz, PointSource src, Probe probe = Probe());
 // Fused backward step: sigma back one level (gradient form, no sponge, +src),
 // adjoint lambda one level (forward form, sponge), zero-lag imaging into g
 // (rtm: the RTM image in g11 instead).

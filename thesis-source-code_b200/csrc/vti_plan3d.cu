@@ -50,6 +50,8 @@ struct vti3d_plan {
   float* d_blist = nullptr;
   size_t blist_cap = 0;
   double* d_acc = nullptr;
+  float* d_gw = nullptr;  // wavelet gradient accumulator (nt)
+  size_t gw_cap = 0;
   int last_cur = 0;  // index into sx[] of the last forward level
   bool have_model = false;
 };
@@ -501,7 +503,7 @@ int vti3d_plan_destroy(vti3d_plan* p) {
   vol_free(&p->g13);
   vol_free(&p->g33);
   void* ptrs[] = {p->dampx, p->d_rec, p->d_rec_damp, p->d_live, p->d_trace,
-                  p->d_obs, p->d_blist, p->d_acc};
+                  p->d_obs, p->d_blist, p->d_acc, p->d_gw};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   delete p;
@@ -665,6 +667,87 @@ int vti3d_plan_rtm(vti3d_plan* p, const float* souloc, const int* shotid, int ns
   VTI_TRY(vol_download(ctx, p->d, &p->g11, image, image_mem));
   VTI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return check_device_status(ctx);
+}
+
+int vti3d_plan_wavelet_gradient(vti3d_plan* p, const float* souloc, const int* shotid, int nshot,
+                                const float* data, int data_mem, float* gwavelet, int mem) {
+  if (!p) return VTI_ERR_ARG;
+  vti_ctx* ctx = p->ctx;
+  if (!p->have_model) return fail(ctx, VTI_ERR_ARG, "model not set");
+  if (!souloc || (nshot > 0 && !shotid) || !data || !gwavelet || nshot < 0)
+    return fail(ctx, VTI_ERR_ARG, "null pointer or negative shot count");
+  VTI_CUDA(ctx, cudaSetDevice(ctx->device));
+  const vti3d_geom& g = p->g;
+  const Dims3& d = p->d;
+  const float dx2 = g.dx * g.dx, dy2 = g.dy * g.dy, dz2 = g.dz * g.dz, dt2 = g.dt * g.dt;
+  const float sxs = dt2 / dx2, sys = dt2 / dy2, szs = dt2 / dz2;
+  const int st = sampling_step(g), nnt = nnt_of(g), M = last_level(g, p->flags);
+  VTI_TRY(ensure(ctx, &p->d_gw, &p->gw_cap, (size_t)g.nt));
+  VTI_CUDA(ctx, cudaMemsetAsync(p->d_gw, 0, g.nt * sizeof(float), ctx->stream));
+  Damping dmp{p->dampx, p->dampy, p->dampz};
+  for (int k = 0; k < nshot; ++k) {
+    ShotGeom s;
+    VTI_TRY(shot_geom(p, souloc, shotid[k], &s));
+    VTI_TRY(upload_shot(p, s));
+    const float* obs = nullptr;
+    VTI_TRY(get_obs(p, s, data, data_mem, &obs));
+    if (s.nr > 0)
+      VTI_CUDA(ctx, cudaMemcpyAsync(p->d_trace, obs, (size_t)nnt * s.nr * sizeof(float),
+                                    cudaMemcpyDeviceToDevice, ctx->stream));
+    for (int j = 0; j < 2; ++j) {
+      VTI_TRY(vol_zero(ctx, d, &p->lx[j]));
+      VTI_TRY(vol_zero(ctx, d, &p->lz[j]));
+    }
+    int LA = 0, LB = 1;
+    VTI_TRY(launch_seed_adjoint(ctx, p->lx[LA].origin, p->lz[LA].origin, p->d_trace, nnt,
+                                p->d_rec + p->rec_cap, p->d_rec_damp, s.nr, dt2));
+    Probe probe;
+    probe.x = s.sx;
+    probe.y = s.sy;
+    probe.z = s.sz;
+    for (int i = 0; i < M - 1; ++i) {
+      const int it = g.nt - 3 - i;  // modelData3d_f.cu:1103-1104
+      probe.out = p->d_gw + it;
+      VTI_TRY(launch_fwd3d_tma(ctx, d, p->m_lx[LA], p->m_lz[LA], p->m_lx[LB], p->m_lz[LB],
+                               p->m_cpad[0], p->m_cpad[1], p->m_cpad[2], p->lz[LA].origin,
+                               p->lx[LB].origin, p->lz[LB].origin, &dmp, sxs, sys, szs,
+                               PointSource(), probe));
+      const int ti = it + 1;
+      float f = float(ti) / float(st);
+      int i0 = (int)f;
+      const int clamp = i0 >= nnt - 1;
+      f = f - i0;
+      VTI_TRY(launch_inject_residual(ctx, p->lx[LB].origin, p->lz[LB].origin, p->d_trace, nnt,
+                                     clamp ? 0 : i0, f, clamp, p->d_rec, p->d_rec_damp, s.nr,
+                                     dt2));
+      std::swap(LA, LB);
+    }
+    VTI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  std::vector<float> h(g.nt);
+  VTI_CUDA(ctx, cudaMemcpyAsync(h.data(), p->d_gw, g.nt * sizeof(float), cudaMemcpyDeviceToHost,
+                                ctx->stream));
+  VTI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  VTI_TRY(check_device_status(ctx));
+  for (float& v : h) v *= dt2;  // modelData3d_f.cu:1293
+  VTI_CUDA(ctx, cudaMemcpy(gwavelet, h.data(), g.nt * sizeof(float),
+                           mem == VTI_MEM_DEVICE ? cudaMemcpyHostToDevice : cudaMemcpyHostToHost));
+  return VTI_OK;
+}
+
+int vti3d_wavelet_gradient_cij(vti_ctx* ctx, const vti3d_geom* g, const float* c11,
+                               const float* c13, const float* c33, const float* souloc,
+                               const int* shotid, int nshot, const float* recloc, int nrec_total,
+                               const float* data, float* gwavelet, unsigned flags) {
+  vti3d_plan* p = nullptr;
+  VTI_TRY(vti3d_plan_create(ctx, g, flags, &p));
+  int st = vti3d_plan_set_model(p, c11, c13, c33, nullptr, nullptr, VTI_MEM_HOST);
+  if (st == VTI_OK) st = vti3d_plan_set_receivers(p, recloc, nrec_total);
+  if (st == VTI_OK)
+    st = vti3d_plan_wavelet_gradient(p, souloc, shotid, nshot, data, VTI_MEM_HOST, gwavelet,
+                                     VTI_MEM_HOST);
+  vti3d_plan_destroy(p);
+  return st;
 }
 
 int vti3d_rtm_cij(vti_ctx* ctx, const vti3d_geom* g, const float* c11, const float* c13,

@@ -50,6 +50,8 @@ struct RtmStep {
   float* image;  // set: image the current level against (1-f) s0 + f s1
   const float *s0, *s1;
   float f;
+  float* probe_out;  // set: *probe_out = dt2 (p + q) of the current level at probe
+  int probe;
 };
 
 __global__ void __launch_bounds__(BX* BZ) k_rtm2d_step(RtmStep a) {
@@ -78,6 +80,7 @@ __global__ void __launch_bounds__(BX* BZ) k_rtm2d_step(RtmStep a) {
     const float d = (1.f - a.f) * a.s0[i] + a.f * a.s1[i];
     a.image[i] += 0.5f * (p + q) * d;
   }
+  if (a.probe_out && i == a.probe) *a.probe_out = a.dt2 * (p + q);  // extractWavelet
   if (!a.p0) return;
   const float tp = lap9(&sp[tz][tx + 4], 1) * a.idx2;
   const float tq = lap9(&sq[tz + 4][tx], BX) * a.idz2;
@@ -98,12 +101,13 @@ __global__ void __launch_bounds__(BX* BZ) k_rtm2d_step(RtmStep a) {
   if (a.slice) a.slice[i] = 0.5f * (pn + qn);
 }
 
-// injectDipoleData into a level that has already been tapered: the taper
-// factor of each point (1 in the never-updated 4-cell frame) is applied to
-// the injected value. Receivers may share points, hence the atomics.
+// injectDipoleData (dipole != 0) or injectData (kernels.cu:208-217) into a
+// level that has already been tapered: the taper factor of each point (1 in
+// the never-updated 4-cell frame) is applied to the injected value. Receivers
+// may share points, hence the atomics.
 __global__ void k_rtm2d_inject(float* p, float* q, const float* d0, const float* d1, float f,
                                const int* ridx, const float* taper, int nr, float dt2, int nnx,
-                               int nnz) {
+                               int nnz, int dipole) {
   const int ir = blockIdx.x * blockDim.x + threadIdx.x;
   if (ir >= nr) return;
   const float v = dt2 * (0.5f * ((1.f - f) * (d0 ? d0[ir] : 0.f) + f * (d1 ? d1[ir] : 0.f)));
@@ -115,7 +119,7 @@ __global__ void k_rtm2d_inject(float* p, float* q, const float* d0, const float*
     atomicAdd(q + k, s);
   };
   add(ridx[ir], v);
-  add(ridx[ir] + nnx, -v);
+  if (dipole) add(ridx[ir] + nnx, -v);
 }
 
 }  // namespace
@@ -263,7 +267,7 @@ extern "C" int vti2d_rtm(vti_ctx* ctx, const vti2d_geom* g, float* image, const 
     auto inject = [&](float* p, float* q, float f) -> int {
       if (nri <= 0) return VTI_OK;
       k_rtm2d_inject<<<(nri + 127) / 128, 128, 0, sm>>>(p, q, d0, d1, f, d_ridx + ir0, dtap, nri,
-                                                         dt2, nnx, nnz);
+                                                         dt2, nnx, nnz, 1);
       ctx->launches++;
       return cuda_check(ctx, cudaGetLastError(), "k_rtm2d_inject");
     };
@@ -312,5 +316,142 @@ extern "C" int vti2d_rtm(vti_ctx* ctx, const vti2d_geom* g, float* image, const 
   RTM_CK(cudaMemcpyAsync(image, dimg, nnxz * 4, cudaMemcpyDeviceToHost, sm));
   RTM_CK(cudaStreamSynchronize(sm));
 #undef RTM_CK
+  return done(VTI_OK);
+}
+
+// waveletGradient_f (lib/vti-fwi-2d/objFuncGradient_f.cu:373-530): per shot the
+// adjoint wavefield driven by the traces as points (injectData), forwardCD and
+// the taper; g[it] = dt2 (p + q) at the source for every level (extractWavelet,
+// an assignment per shot, kernels.cu:258-261), g[nt-2] from the seeded level;
+// shots summed on the host in float. The step kernel reads the extracted value
+// from the finished level when it steps from it.
+extern "C" int vti2d_wavelet_gradient(vti_ctx* ctx, const vti2d_geom* g, float* gwavelet,
+                                      const float* data, const float* c11, const float* c13,
+                                      const float* c33, const int* sloc, int ns, const int* rloc,
+                                      int nr, const float* taper) {
+  if (!ctx || !g || !gwavelet || !data || !c11 || !c13 || !c33 || !sloc || !taper ||
+      (nr > 0 && !rloc) || ns < 0)
+    return VTI_ERR_ARG;
+  const int nnx = g->nx + 2 * g->npad, nnz = g->nz + 2 * g->npad;
+  const long long nnxz = (long long)nnx * nnz;
+  if (nnx < 9 || nnz < 9 || g->nt < 3 || !(g->dt > 0) || !(g->rate > 0))
+    return fail(ctx, VTI_ERR_ARG, "2D geometry out of range");
+  const float dt = g->dt, dt2 = dt * dt;
+  const int ratio = (int)(g->rate / dt + 0.5);  // objFuncGradient_f.cu:375 (double 0.5)
+  if (ratio < 1) return fail(ctx, VTI_ERR_ARG, "rate < dt");
+  const int nnt = (g->nt - 1) / ratio + 1;
+  for (int is = 0; is < ns; ++is) {
+    const int* s = sloc + 4 * is;
+    if (s[0] < kHalo || s[0] >= nnx - kHalo || s[1] < kHalo || s[1] >= nnz - kHalo)
+      return fail(ctx, VTI_ERR_ARG, "2D source must lie in the updated region");
+    if (s[2] < 0 || s[3] < 0 || s[3] + s[2] > nr)
+      return fail(ctx, VTI_ERR_ARG, "2D shot receiver range exceeds rloc");
+    for (int ir = 0; ir < s[2]; ++ir) {
+      const int x = rloc[2 * (s[3] + ir)], z = rloc[2 * (s[3] + ir) + 1];
+      if (x < 0 || x >= nnx || z < 0 || z >= nnz)
+        return fail(ctx, VTI_ERR_ARG, "2D receiver outside the grid");
+    }
+  }
+  VTI_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t sm = ctx->stream;
+  const size_t nfloat = 8 * (size_t)nnxz + (size_t)nnt * nr + g->nt;
+  float* buf = nullptr;
+  int* d_ridx = nullptr;
+  VTI_CUDA(ctx, cudaMalloc((void**)&buf, nfloat * sizeof(float)));
+  if (cudaMalloc((void**)&d_ridx, std::max(nr, 1) * sizeof(int)) != cudaSuccess) {
+    cudaFree(buf);
+    return fail(ctx, VTI_ERR_OOM, "cannot allocate the receiver table");
+  }
+  float *dc11 = buf, *dc13 = dc11 + nnxz, *dc33 = dc13 + nnxz, *dtap = dc33 + nnxz;
+  float *p0 = dtap + nnxz, *q0 = p0 + nnxz, *p1 = q0 + nnxz, *q1 = p1 + nnxz;
+  float* ddata = q1 + nnxz;
+  float* gs = ddata + (size_t)nnt * nr;
+  auto done = [&](int status) {
+    cudaStreamSynchronize(sm);
+    cudaFree(buf);
+    cudaFree(d_ridx);
+    return status;
+  };
+#define WG_CK(call)                                                 \
+  do {                                                              \
+    cudaError_t e_ = (call);                                        \
+    if (e_ != cudaSuccess) return done(cuda_check(ctx, e_, #call)); \
+  } while (0)
+  WG_CK(cudaMemcpyAsync(dc11, c11, nnxz * 4, cudaMemcpyHostToDevice, sm));
+  WG_CK(cudaMemcpyAsync(dc13, c13, nnxz * 4, cudaMemcpyHostToDevice, sm));
+  WG_CK(cudaMemcpyAsync(dc33, c33, nnxz * 4, cudaMemcpyHostToDevice, sm));
+  WG_CK(cudaMemcpyAsync(dtap, taper, nnxz * 4, cudaMemcpyHostToDevice, sm));
+  if (nr > 0)
+    WG_CK(cudaMemcpyAsync(ddata, data, (size_t)nnt * nr * 4, cudaMemcpyHostToDevice, sm));
+  std::vector<int> ridx(std::max(nr, 1));
+  for (int ir = 0; ir < nr; ++ir) ridx[ir] = rloc[2 * ir] + rloc[2 * ir + 1] * nnx;
+  WG_CK(cudaMemcpyAsync(d_ridx, ridx.data(), std::max(nr, 1) * sizeof(int),
+                        cudaMemcpyHostToDevice, sm));
+  const dim3 block(BX, BZ), grid((nnx - 8 + BX - 1) / BX, (nnz - 8 + BZ - 1) / BZ);
+  RtmStep a{};
+  a.nnx = nnx;
+  a.nnz = nnz;
+  a.c11 = dc11;
+  a.c13 = dc13;
+  a.c33 = dc33;
+  a.taper = dtap;
+  a.idx2 = 1.f / (g->dx * g->dx);
+  a.idz2 = 1.f / (g->dz * g->dz);
+  a.dt2 = dt2;
+  a.src = -1;
+  std::vector<float> acc(g->nt, 0.f), hs(g->nt);
+  for (int is = 0; is < ns; ++is) {
+    const int* s = sloc + 4 * is;
+    const int nri = s[2], ir0 = s[3];
+    WG_CK(cudaMemsetAsync(p0, 0, 4 * nnxz * 4, sm));
+    WG_CK(cudaMemsetAsync(gs, 0, g->nt * 4, sm));
+    const float* row_base = ddata + ir0;
+    const float* d0 = row_base + (size_t)(nnt - 1) * nr;
+    const float* d1 = nullptr;  // zeros
+    auto inject = [&](float* p, float* q, float f) -> int {
+      if (nri <= 0) return VTI_OK;
+      k_rtm2d_inject<<<(nri + 127) / 128, 128, 0, sm>>>(p, q, d0, d1, f, d_ridx + ir0, dtap, nri,
+                                                         dt2, nnx, nnz, 0);
+      ctx->launches++;
+      return cuda_check(ctx, cudaGetLastError(), "k_rtm2d_inject");
+    };
+    float *cp = p0, *cq = q0, *np = p1, *nq = q1;
+    int st = inject(cp, cq, 0.f);
+    if (st != VTI_OK) return done(st);
+    a.probe = s[0] + s[1] * nnx;
+    a.probe_out = gs + (g->nt - 2);
+    for (int it = g->nt - 3; it >= 0; --it) {
+      a.p1 = cp;
+      a.q1 = cq;
+      a.p0 = np;
+      a.q0 = nq;
+      k_rtm2d_step<<<grid, block, 0, sm>>>(a);  // extracts cur, makes level it
+      ctx->launches++;
+      WG_CK(cudaGetLastError());
+      float f = (it + 1.) / ratio;
+      const int i1 = (int)f;
+      if ((it + 2) % ratio == 0) {
+        d1 = row_base + (size_t)i1 * nr;
+        std::swap(d0, d1);
+      }
+      f -= i1;
+      st = inject(np, nq, f);
+      if (st != VTI_OK) return done(st);
+      a.probe_out = gs + it;
+      std::swap(cp, np);
+      std::swap(cq, nq);
+    }
+    a.p1 = cp;  // extract the last level
+    a.q1 = cq;
+    a.p0 = a.q0 = nullptr;
+    k_rtm2d_step<<<grid, block, 0, sm>>>(a);
+    ctx->launches++;
+    WG_CK(cudaGetLastError());
+    WG_CK(cudaMemcpyAsync(hs.data(), gs, g->nt * 4, cudaMemcpyDeviceToHost, sm));
+    WG_CK(cudaStreamSynchronize(sm));
+    for (int it = 0; it < g->nt; ++it) acc[it] += hs[it];
+  }
+  std::copy(acc.begin(), acc.end(), gwavelet);
+#undef WG_CK
   return done(VTI_OK);
 }

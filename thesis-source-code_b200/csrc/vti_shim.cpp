@@ -838,3 +838,107 @@ void rtm_f(float* image, const float* data, const float* c11, const float* c13, 
     if (!v.empty())
       for (size_t i = 0; i < n; ++i) image[i] += v[i];
 }
+
+// ---------------------------------------------------------- wavelet gradient
+// waveletGradientCij3d_f (modelData3d_f.cu:858-1294): the traces come in ddata
+// (nnt per receiver, shot ranges at nnt*irbegin); shots round-robin over the
+// GPUs, per-device results summed. The level count follows the pipeline of
+// GPUs.size() devices.
+void waveletGradientCij3d_f(float* gwavelet, const float* ddata, float* souloc, int ns,
+                            std::vector<int>& shotid, float* recloc, float* c11, float* c13,
+                            float* c33, int nx, int ny, int nz, int nt, int npad, float ox,
+                            float oy, float oz, float ot, float dx, float dy, float dz, float dt,
+                            float samplingRate, std::vector<int>& GPUs) {
+  (void)ns;
+  vti3d_geom g = geom3(nx, ny, nz, nt, npad, ox, oy, oz, ot, dx, dy, dz, dt, samplingRate);
+  std::memset(gwavelet, 0, nt * sizeof(float));
+  const int nrec = total_receivers(souloc, shotid);
+  const unsigned flags = ref_flags(GPUs.size());
+  std::vector<std::vector<float>> parts(GPUs.size());
+  std::map<int, size_t> slot;
+  for (size_t i = 0; i < GPUs.size(); ++i) slot[GPUs[i]] = i;
+  over_gpus(GPUs, shotid, [&](int id, const std::vector<int>& sub) {
+    Device* dev = device(id);
+    if (!dev) return false;
+    std::lock_guard<std::mutex> lk(dev->mu);
+    vti3d_plan* p = plan_for(dev, g, flags);
+    if (!p) return false;
+    std::vector<float>& gw = parts[slot[id]];
+    gw.assign(nt, 0.f);
+    return report(dev->ctx, vti3d_plan_set_model(p, c11, c13, c33, nullptr, nullptr,
+                                                 VTI_MEM_HOST), "model") &&
+           report(dev->ctx, vti3d_plan_set_receivers(p, recloc, nrec), "receivers") &&
+           report(dev->ctx, vti3d_plan_wavelet_gradient(p, souloc, sub.data(), (int)sub.size(),
+                                                        ddata, VTI_MEM_HOST, gw.data(),
+                                                        VTI_MEM_HOST), "wavelet gradient");
+  });
+  for (auto& gw : parts)
+    if (!gw.empty())
+      for (int i = 0; i < nt; ++i) gwavelet[i] += gw[i];
+}
+
+// waveletGradient3d_f (modelData3d_f.cu:810-856): contiguous shot groups, one
+// per GPU group, summed.
+void waveletGradient3d_f(float* gwavelet, const float* ddata, float* souloc, int ns,
+                         std::vector<int>& shotid, float* recloc, float* c11, float* c13,
+                         float* c33, int nx, int ny, int nz, int nt, int npad, float ox, float oy,
+                         float oz, float ot, float dx, float dy, float dz, float dt,
+                         float samplingRate, std::vector<int>& GPUs, int ngpugroup) {
+  if (ngpugroup <= 1) {
+    waveletGradientCij3d_f(gwavelet, ddata, souloc, ns, shotid, recloc, c11, c13, c33, nx, ny,
+                           nz, nt, npad, ox, oy, oz, ot, dx, dy, dz, dt, samplingRate, GPUs);
+    return;
+  }
+  const int ngpu1 = (int)GPUs.size() / ngpugroup;
+  const int nshot1 = (int)shotid.size() / ngpugroup, r = (int)shotid.size() % ngpugroup;
+  std::vector<std::vector<float>> gw(ngpugroup, std::vector<float>(nt));
+  std::vector<std::thread> th;
+  for (int i = 0; i < ngpugroup; ++i) {
+    th.emplace_back([&, i]() {
+      std::vector<int> gpus(GPUs.begin() + i * ngpu1, GPUs.begin() + (i + 1) * ngpu1);
+      int b = i < r ? i * (nshot1 + 1) : r * (nshot1 + 1) + (i - r) * nshot1;
+      int e = b + (i < r ? nshot1 + 1 : nshot1);
+      std::vector<int> sh(shotid.begin() + b, shotid.begin() + e);
+      waveletGradientCij3d_f(gw[i].data(), ddata, souloc, ns, sh, recloc, c11, c13, c33, nx, ny,
+                             nz, nt, npad, ox, oy, oz, ot, dx, dy, dz, dt, samplingRate, gpus);
+    });
+  }
+  for (auto& t : th) t.join();
+  std::memset(gwavelet, 0, nt * sizeof(float));
+  for (int i = ngpugroup - 1; i >= 0; --i)  // the reference's summation order
+    for (int j = 0; j < nt; ++j) gwavelet[j] += gw[i][j];
+}
+
+// waveletGradient_f (objFuncGradient_f.cu:373-530): shots round-robin over the
+// gpu= devices (the reference uses every visible device; the result does not
+// depend on the device count), per-device sums added.
+void waveletGradient_f(float* gwavelet, const float* d0, const float* c11, const float* c13,
+                       const float* c33, const int* sloc, int ns, const int* rloc, int nr,
+                       const float* taper, int nx, int nz, int nt, int npad, float dx, float dz,
+                       float dt, float rate) {
+  vti2d_geom g{nx, nz, nt, npad, dx, dz, dt, rate, 0.f};
+  std::memset(gwavelet, 0, nt * sizeof(float));
+  const std::vector<int> gpus = gpus_from_argv();
+  auto parts = shots_per_gpu(ns, gpus.size());
+  std::vector<std::vector<float>> gw(gpus.size());
+  std::vector<std::thread> th;
+  for (size_t k = 0; k < gpus.size(); ++k) {
+    if (parts[k].empty()) continue;
+    th.emplace_back([&, k]() {
+      Device* dev = device(gpus[k]);
+      if (!dev) return;
+      std::lock_guard<std::mutex> lk(dev->mu);
+      std::vector<int> sl;
+      for (int is : parts[k]) sl.insert(sl.end(), sloc + 4 * is, sloc + 4 * is + 4);
+      gw[k].assign(nt, 0.f);
+      if (!report(dev->ctx, vti2d_wavelet_gradient(dev->ctx, &g, gw[k].data(), d0, c11, c13, c33,
+                                                   sl.data(), (int)parts[k].size(), rloc, nr,
+                                                   taper), "wavelet gradient"))
+        gw[k].clear();
+    });
+  }
+  for (auto& t : th) t.join();
+  for (auto& v : gw)
+    if (!v.empty())
+      for (int i = 0; i < nt; ++i) gwavelet[i] += v[i];
+}

@@ -132,6 +132,7 @@ struct FwdArgs {
   const float* dampz;
   float sx, sy, sz;
   PointSource src;
+  Probe probe;
   int* status;
 };
 
@@ -145,6 +146,9 @@ constexpr int F_OFF_C = F_OFF_PZ + PLAIN_BYTES;
 constexpr int F_STAGE_BYTES = F_OFF_C + 3 * PLAIN_BYTES;  // 15872
 constexpr int F_SMEM = F_STAGES * F_STAGE_BYTES + 1024 + 2 * F_STAGES * 8;
 
+// kProbe: the probe point of FwdArgs is read out (wavelet gradient); the
+// propagation kernels are instantiated without it.
+template <bool kProbe>
 __global__ void __launch_bounds__(NTHREADS, 3)
     k_fwd3d_tma(const __grid_constant__ CUtensorMap m_cx, const __grid_constant__ CUtensorMap m_cz,
                 const __grid_constant__ CUtensorMap m_px, const __grid_constant__ CUtensorMap m_pz,
@@ -219,6 +223,9 @@ __global__ void __launch_bounds__(NTHREADS, 3)
     const bool v0 = vy && x >= kHalo && x < d.nx - kHalo;
     const bool v1 = vy && x + 1 >= kHalo && x + 1 < d.nx - kHalo;
     const int off = y * d.pitch + x;  // x + 1 < pitch: 32 * gx <= pitch
+    // which of this thread's two points (0, 1; else -1) holds the source / probe
+    const int src_e = (y == a.src.y && a.src.x >= 0) ? a.src.x - x : -1;
+    const int prb_e = (kProbe && y == a.probe.y && a.probe.x >= 0) ? a.probe.x - x : -1;
     dxy[0] = (damp && v0) ? a.dampx[x] * a.dampy[y] : 1.f;
     dxy[1] = (damp && v1) ? a.dampx[x + 1] * a.dampy[y] : 1.f;
     // start the queue: planes z0-4 .. z0+3 from global
@@ -237,7 +244,19 @@ __global__ void __launch_bounds__(NTHREADS, 3)
       q[0][kk] = v.x;
       q[1][kk] = v.y;
     }
+    // z damping factors in registers: dzr holds planes z-3..z once plane z
+    // is entered (the block transition rescales those four queue entries);
+    // the next plane's factor is fetched one plane ahead
+    float dzr[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) dzr[j] = (damp && z0 - 4 + j >= 0) ? a.dampz[z0 - 4 + j] : 1.f;
+    float dz_next = damp ? a.dampz[z0] : 1.f;
     for (int z = z0; z < z1; ++z, ++k) {
+      const float dz = dz_next;
+      if (damp && z + 1 < z1) dz_next = a.dampz[z + 1];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) dzr[j] = dzr[j + 1];
+      dzr[3] = dz;
       const int s = (int)(k % F_STAGES);
       if (!mbar_wait(&full[s], (uint32_t)((k / F_STAGES) & 1), a.status)) {
         ok = false;
@@ -273,7 +292,6 @@ __global__ void __launch_bounds__(NTHREADS, 3)
       const float2 c11 = ld2(pl + 3 * T), c13 = ld2(pl + 4 * T), c33 = ld2(pl + 5 * T);
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[s]);
-      const float dz = damp ? a.dampz[z] : 1.f;
       float nxv[2], nzv[2];
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
@@ -291,7 +309,8 @@ __global__ void __launch_bounds__(NTHREADS, 3)
         const float a11 = pick(c11), a13 = pick(c13), a33 = pick(c33);
         nxv[e] = fmaf(a11, lxy, fmaf(a13, lz, 2.f * c - dd * pick(px)));
         nzv[e] = fmaf(a13, lxy, fmaf(a33, lz, 2.f * q[e][4] - dd * pick(pz)));
-        if (x + e == a.src.x && y == a.src.y && z == a.src.z) {
+        if (kProbe && prb_e == e && z == a.probe.z) *a.probe.out += nxv[e] + nzv[e];
+        if (src_e == e && z == a.src.z) {
           nxv[e] += a.src.amp;
           nzv[e] += a.src.amp;
         }
@@ -320,7 +339,7 @@ __global__ void __launch_bounds__(NTHREADS, 3)
           // after the shift at z+1, entries 0..3 hold planes z-3..z; they are
           // entries 1..4 now
 #pragma unroll
-          for (int kk = 0; kk < 4; ++kk) q[e][kk + 1] *= dxy[e] * a.dampz[z - 3 + kk];
+          for (int kk = 0; kk < 4; ++kk) q[e][kk + 1] *= dxy[e] * dzr[kk];
         }
       }
     }
@@ -468,7 +487,17 @@ __global__ void __launch_bounds__(NTHREADS, 2)
       lq[0][kk] = lv.x;
       lq[1][kk] = lv.y;
     }
+    // z damping factors in registers (see the forward kernel)
+    float dzr[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) dzr[j] = z0 - 4 + j >= 0 ? a.dampz[z0 - 4 + j] : 1.f;
+    float dz_next = a.dampz[z0];
     for (int z = z0; z < z1; ++z, ++k) {
+      const float dz = dz_next;
+      if (z + 1 < z1) dz_next = a.dampz[z + 1];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) dzr[j] = dzr[j + 1];
+      dzr[3] = dz;
       const int s = (int)(k % B_STAGES);
       if (!mbar_wait(&full[s], (uint32_t)((k / B_STAGES) & 1), a.status)) {
         ok = false;
@@ -519,7 +548,6 @@ __global__ void __launch_bounds__(NTHREADS, 2)
       const float2 g33o = kRtm ? make_float2(0.f, 0.f) : ld2(pl + 11 * T);
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[s]);
-      const float dz = a.dampz[z];
       float snx[2], snz[2], lnx[2], lnz[2], g11[2], g13[2], g33[2];
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
@@ -596,7 +624,7 @@ __global__ void __launch_bounds__(NTHREADS, 2)
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
 #pragma unroll
-          for (int kk = 0; kk < 4; ++kk) lq[e][kk + 1] *= dxy[e] * a.dampz[z - 3 + kk];
+          for (int kk = 0; kk < 4; ++kk) lq[e][kk + 1] *= dxy[e] * dzr[kk];
         }
       }
     }
@@ -678,12 +706,14 @@ int launch_fwd3d_tma(vti_ctx* ctx, const Dims3& d, const TileMaps& cx, const Til
                      const TileMaps& px, const TileMaps& pz, const TileMaps& c11,
                      const TileMaps& c13, const TileMaps& c33, const float* cz_ptr,
                      float* px_ptr, float* pz_ptr, const Damping* damp, float sx, float sy,
-                     float sz, PointSource src) {
-  static bool attr[64] = {};  // the attribute is per device
-  if (ctx->device >= 64 || !attr[ctx->device]) {
-    VTI_CUDA(ctx, cudaFuncSetAttribute(k_fwd3d_tma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                     float sz, PointSource src, Probe probe) {
+  const bool pr = probe.x >= 0 && probe.out;
+  static bool attr[2][64] = {};  // per instantiation and device
+  if (ctx->device >= 64 || !attr[pr][ctx->device]) {
+    VTI_CUDA(ctx, cudaFuncSetAttribute(pr ? k_fwd3d_tma<true> : k_fwd3d_tma<false>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        F_SMEM));
-    if (ctx->device < 64) attr[ctx->device] = true;
+    if (ctx->device < 64) attr[pr][ctx->device] = true;
   }
   FwdArgs a;
   a.d = d;
@@ -698,11 +728,13 @@ int launch_fwd3d_tma(vti_ctx* ctx, const Dims3& d, const TileMaps& cx, const Til
   a.sy = sy;
   a.sz = sz;
   a.src = src;
+  a.probe = probe;
   a.status = ctx->d_status;
   const int grid = a.sc.grid;
   {
     LaunchTimer tm(ctx, kTimedFwd3d);
-    k_fwd3d_tma<<<grid, NTHREADS, F_SMEM, ctx->stream>>>(*H(cx), *P(cz), *P(px), *P(pz), *P(c11),
+    auto kern = pr ? k_fwd3d_tma<true> : k_fwd3d_tma<false>;
+    kern<<<grid, NTHREADS, F_SMEM, ctx->stream>>>(*H(cx), *P(cz), *P(px), *P(pz), *P(c11),
                                                          *P(c13), *P(c33), a);
   }
   VTI_LAUNCHED(ctx, "k_fwd3d_tma");

@@ -100,6 +100,9 @@ def _signatures():
         "vti2d_gradient": (C.c_int, [P] * 11 + [C.c_int, P, C.c_int, P, C.POINTER(C.c_double)]),
         "vti2d_gn_hessian": (C.c_int, [P] * 13 + [C.c_int, P, C.c_int, P]),
         "vti2d_rtm": (C.c_int, [P] * 9 + [C.c_int, P, C.c_int, P]),
+        "vti2d_wavelet_gradient": (C.c_int, [P] * 8 + [C.c_int, P, C.c_int, P]),
+        "vti3d_plan_wavelet_gradient": (C.c_int, [P, P, P, C.c_int, P, C.c_int, P, C.c_int]),
+        "vti3d_wavelet_gradient_cij": (C.c_int, [P] * 7 + [C.c_int, P, C.c_int, P, P, C.c_uint]),
         "vti3d_plan_get_wavefield": (C.c_int, [P, P, C.c_int]),
         "vti3d_gradient_vepsdel": (C.c_int, [P, P, P, P, P, P, P, C.c_float, C.c_float,
                                              C.c_float, P, P, P, C.c_int, P, C.c_int, P, P, P, P,
@@ -371,6 +374,30 @@ def objFuncGradient_f(ctx, g: Geom2d, data, c11, c13, c33, wavelet, sloc, rloc, 
                                    _p(_f32(wavelet)), _p(sloc), sloc.size // 4, _p(rloc),
                                    rloc.size // 2, _p(_f32(taper)), C.byref(mis)))
     return out[0], out[1], out[2], mis.value
+
+
+def waveletGradient_f(ctx, g: Geom2d, data, c11, c13, c33, sloc, rloc, taper):
+    """waveletGradient_f (lib/vti-fwi-2d/objFuncGradient_f.cu:373): nt floats."""
+    sloc, rloc = _i32(sloc).reshape(-1), _i32(rloc).reshape(-1)
+    out = np.zeros(g.nt, dtype=np.float32)
+    ctx.check(lib().vti2d_wavelet_gradient(ctx.handle, C.byref(g), _p(out), _p(_f32(data)),
+                                           _p(_f32(c11)), _p(_f32(c13)), _p(_f32(c33)),
+                                           _p(sloc), sloc.size // 4, _p(rloc), rloc.size // 2,
+                                           _p(_f32(taper))))
+    return out
+
+
+def waveletGradientCij3d_f(ctx, g: Geom3d, souloc, shotid, recloc, c11, c13, c33, data,
+                           flags=0):
+    """waveletGradientCij3d_f (lib/vti-fwi-3d/gpu/modelData3d_f.cu:858): nt floats."""
+    souloc, recloc = _f32(souloc).reshape(-1), _f32(recloc).reshape(-1)
+    shotid = _i32(shotid)
+    out = np.zeros(g.nt, dtype=np.float32)
+    ctx.check(lib().vti3d_wavelet_gradient_cij(ctx.handle, C.byref(g), _p(_f32(c11)),
+                                               _p(_f32(c13)), _p(_f32(c33)), _p(souloc),
+                                               _p(shotid), len(shotid), _p(recloc),
+                                               recloc.size // 4, _p(_f32(data)), _p(out), flags))
+    return out
 
 
 def rtm_f(ctx, g: Geom2d, data, c11, c13, c33, wavelet, sloc, rloc, taper):
