@@ -146,6 +146,15 @@ int vti3d_plan_model_data(vti3d_plan* plan, const float* souloc, const int* shot
 int vti3d_plan_gradient(vti3d_plan* plan, const float* souloc, const int* shotid, int nshot,
                         const float* dobs, int dobs_mem, float* fgcij, int fgcij_mem,
                         double* misfit);
+/* Misfit options of vti3d_plan_gradient (objFuncGradient3d_f.cu:743-775, the
+ * tpow= / objtype= / halfwidth= parameters of the reference): the modeled
+ * traces are multiplied by (ot + it*sampling_rate)^tpow when tpow != 0 (no
+ * chain-rule factor on the adjoint source, as in the reference); objtype 0 is
+ * the L2 misfit, any other value the AGC misfit (residualAGC, agc.cpp:62-99,
+ * energy window of 2*halfwidth+1 samples wrapping around the trace). The
+ * misfit-only entry (vti3d_plan_objfunc) stays plain L2, as objFuncCij3d_f.
+ * Defaults: 0, 0, 20. */
+int vti3d_plan_set_misfit(vti3d_plan* plan, float tpow, int objtype, int halfwidth);
 /* Misfit only (objFuncCij3d_f, objFuncGradient3d_f.cu:1272). */
 int vti3d_plan_objfunc(vti3d_plan* plan, const float* souloc, const int* shotid, int nshot,
                        const float* dobs, int dobs_mem, double* misfit);

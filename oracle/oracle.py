@@ -32,7 +32,7 @@ def lib():
             f.argtypes = [VP] * 8 + [C.c_int, VP, VP, VP]
             f.restype = C.c_int
             f = getattr(L, f"orc3d_gradient_cij_{suf}")
-            f.argtypes = [VP] * 8 + [C.c_int, VP, VP, VP, C.c_int, VP]
+            f.argtypes = [VP] * 8 + [C.c_int, VP, VP, VP, C.c_int, VP, C.c_float, C.c_int, C.c_int]
             f.restype = C.c_int
             f = getattr(L, f"orc3d_rtm_{suf}")
             f.argtypes = [VP] * 8 + [C.c_int, VP, VP, VP]
@@ -94,8 +94,10 @@ def model_data3d(g, c11, c13, c33, wavelet, souloc, shotid, recloc, dtype=np.flo
 
 
 def gradient3d(g, cij, padb, randb, wavelet, souloc, shotid, recloc, dobs, dtype=np.float64,
-               full_steps=False, misfit_only=False, want_modeled=False):
-    """objFuncGradientCij3d_f restated: fgcij = [misfit/2, gc11, gc13, gc33]."""
+               full_steps=False, misfit_only=False, want_modeled=False, tpow=0.0, objtype=0,
+               halfwidth=20):
+    """objFuncGradientCij3d_f restated: fgcij = [misfit/2, gc11, gc13, gc33];
+    tpow / objtype / halfwidth as the reference's parameters of those names."""
     ip, fp = _geo3(g, full_steps)
     n = g.nx * g.ny * g.nz
     out = np.zeros(1 + 3 * n, dtype=dtype)
@@ -106,7 +108,7 @@ def gradient3d(g, cij, padb, randb, wavelet, souloc, shotid, recloc, dobs, dtype
     getattr(lib(), f"orc3d_gradient_cij_{suf}")(
         _p(ip), _p(fp), _p(_f32(cij)), _p(_f32(padb)), _p(_f32(randb)), _p(_f32(wavelet)),
         _p(_f32(souloc)), _p(shotid), len(shotid), _p(recloc), _p(_f32(dobs)), _p(out),
-        1 if misfit_only else 0, _p(mod))
+        1 if misfit_only else 0, _p(mod), tpow, objtype, halfwidth)
     return (out, mod) if want_modeled else out
 
 

@@ -3,7 +3,7 @@
 // tests/golden/make_golden.py. TEST INFRASTRUCTURE ONLY: it produces golden
 // traces and gradients that pin the oracle; nothing in the library uses it.
 //
-// usage: ref3d <dir> model|grad|rtm|wgrad
+// usage: ref3d <dir> model|grad|rtm|wgrad [key=value ...]
 //   <dir>/params.txt : nx ny nz nt npad ox oy oz ot dx dy dz dt rate ns nrec
 //   <dir>/{souloc,recloc,wavelet,cij,padb,randb,dobs}.bin (float32)
 //   writes <dir>/ref_ddata.bin (model), <dir>/ref_fgcij.bin (grad) or
@@ -87,10 +87,14 @@ int main(int argc, char** argv) {
     std::ofstream h(hdr);
     h << "in=" << dir << "/dobs.bin\ndata_format=native_float\n";
   }
-  // gpu= is read by rtmCij3d_f (rtm3d_f.cu:164)
-  std::string a0 = "ref3d", a1 = "data=" + hdr, a2 = "tpow=0", a3 = "objtype=0", a4 = "gpu=0";
-  char* av[] = {&a0[0], &a1[0], &a2[0], &a3[0], &a4[0], nullptr};
-  myio_init(5, av);
+  // gpu= is read by rtmCij3d_f (rtm3d_f.cu:164); further key=value words on
+  // the command line (tpow=, objtype=, halfwidth=) go to the reference's argv
+  std::vector<std::string> words = {"ref3d", "data=" + hdr, "gpu=0"};
+  for (int i = 3; i < argc; ++i) words.push_back(argv[i]);
+  std::vector<char*> av;
+  for (auto& w : words) av.push_back(&w[0]);
+  av.push_back(nullptr);
+  myio_init((int)words.size(), av.data());
   if (mode == "model") {
     std::vector<float> ddata((size_t)nnt * nrec, 0.f);
     modelDataCij3d_f(ddata.data(), souloc.data(), ns, shotid, recloc.data(), wavelet.data(),

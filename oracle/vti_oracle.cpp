@@ -325,6 +325,42 @@ T interp_residual(const T* res_trace, int time_index, int nnt, int st) {
   return (T)((1. - f) * res_trace[i] + f * res_trace[i + 1]);
 }
 
+// runsum (agc.cpp:14-25): windowed sum over i-hw..i+hw, indices wrapping.
+template <typename T>
+void runsum(int nt, int hw, const T* w, T* s) {
+  for (int i = 0; i < nt; ++i) {
+    T v = 0;
+    for (int j = i - hw; j <= i + hw; ++j) v += w[j < 0 ? j + nt : (j >= nt ? j - nt : j)];
+    s[i] = v;
+  }
+}
+
+// residualAGC (agc.cpp:62-99) for one trace: d (modeled) becomes the adjoint
+// source; returns the trace's squared AGC residual.
+template <typename T>
+double agc_adjoint(int nt, int hw, T* d, const float* d0) {
+  const T eps = (T)1e-6f;
+  std::vector<T> e(nt), e0(nt), sd(nt), sd0(nt), rs(nt), drss(nt), acc(nt);
+  for (int i = 0; i < nt; ++i) {
+    e[i] = d[i] * d[i];
+    e0[i] = (T)d0[i] * (T)d0[i];
+  }
+  runsum(nt, hw, e.data(), sd.data());
+  runsum(nt, hw, e0.data(), sd0.data());
+  double fi = 0;
+  for (int i = 0; i < nt; ++i) {
+    T res = d[i] / std::sqrt(std::max(eps, sd[i])) - (T)d0[i] / std::sqrt(std::max(eps, sd0[i]));
+    fi += (double)(res * res);
+    T t1 = std::max(eps, sd[i]);
+    T t2 = res / std::sqrt(t1);
+    drss[i] = d[i] * t2 / t1;
+    rs[i] = t2;
+  }
+  runsum(nt, hw, drss.data(), acc.data());
+  for (int i = 0; i < nt; ++i) d[i] = rs[i] - d[i] * acc[i];
+  return fi;
+}
+
 // objFuncGradientCij3d_f (objFuncGradient3d_f.cu:361-1111) for the shots in
 // shotid. fgcij[0] = misfit/2, then gc11, gc13, gc33 (nxyz each).
 // misfit_only: objFuncCij3d_f (pass 1 + misfit).
@@ -332,7 +368,8 @@ template <typename T>
 void gradient3d(const Geo3& g, const float* cij_in, const float* padb, const float* randb,
                 const float* wavelet, const float* souloc, const int* shotid, int nshot,
                 const float* recloc, const float* dobs, T* fgcij, bool misfit_only,
-                T* modeled /*optional: nnt*nrtotal modeled traces*/) {
+                T* modeled /*optional: nnt*nrtotal modeled traces*/, float tpow = 0.f,
+                int objtype = 0, int halfwidth = 20) {
   const long n = g.nxyz(), nxy = g.nxy();
   const float dt2 = g.dt * g.dt;
   const int st = sampling_step(g.rate, g.dt);
@@ -357,11 +394,25 @@ void gradient3d(const Geo3& g, const float* cij_in, const float* padb, const flo
     forward3d<T>(g, c11, c13, c33, wavelet, s, &damp, res.data(), cx, cz, px, pz);
     if (modeled)
       std::copy(res.begin(), res.end(), modeled + (long)nnt * s.irbegin);
-    // L2 misfit (objFuncGradient3d_f.cu:759-771): residual = modeled - observed
+    // L2 misfit (objFuncGradient3d_f.cu:759-771): residual = modeled - observed;
+    // the gradient (not the misfit-only entry, :1579-1590) first applies the
+    // t^p gain (tpower, agc.cpp:104-116) and may use the AGC misfit instead
     const float* ob = dobs + (long)nnt * s.irbegin;
-    for (long i = 0; i < (long)nnt * s.nr; ++i) {
-      res[i] = res[i] - (T)ob[i];
-      objfunc += (double)(res[i] * res[i]);
+    if (!misfit_only && tpow != 0.f)
+      for (int ir = 0; ir < s.nr; ++ir)
+        for (int it = 0; it < nnt; ++it) {
+          float t = g.ot + it * g.rate;
+          res[it + (long)ir * nnt] *= (T)std::pow((double)t, (double)tpow);
+        }
+    if (!misfit_only && objtype != 0) {
+      for (int ir = 0; ir < s.nr; ++ir)
+        objfunc += agc_adjoint<T>(nnt, halfwidth, res.data() + (long)ir * nnt,
+                                  ob + (long)ir * nnt);
+    } else {
+      for (long i = 0; i < (long)nnt * s.nr; ++i) {
+        res[i] = res[i] - (T)ob[i];
+        objfunc += (double)(res[i] * res[i]);
+      }
     }
     if (misfit_only) continue;
     // pass 2: random boundary, no sponge (objFuncGradient3d_f.cu:786-895)
@@ -1106,10 +1157,10 @@ ORC3D_MODEL(float, f32)
                                const float* padb, const float* randb, const float* wavelet,     \
                                const float* souloc, const int* shotid, int nshot,               \
                                const float* recloc, const float* dobs, T* fgcij, int misfit_only, \
-                               T* modeled) {                                                    \
+                               T* modeled, float tpow, int objtype, int halfwidth) {             \
     Geo3 g = unpack3(ip, fp);                                                                   \
     gradient3d<T>(g, cij, padb, randb, wavelet, souloc, shotid, nshot, recloc, dobs, fgcij,     \
-                  misfit_only != 0, modeled);                                                   \
+                  misfit_only != 0, modeled, tpow, objtype, halfwidth);                         \
     return 0;                                                                                   \
   }
 ORC3D_GRAD(double, f64)

@@ -83,6 +83,10 @@ RTM_CASES2D = ["g2_a"]
 # case's observed traces; in 3D the model carries the pad boundary (the
 # sponge model), as the source-inversion drivers pass it.
 WGRAD_CASES3D = ["g3_a"]
+# gradient misfit options (<case>_misfit.npz), as the reference's tpow=,
+# objtype=, halfwidth= parameters
+MISFIT_CASES3D = ["g3_a"]
+MISFIT_OPTIONS = {"agc": {"objtype": 1, "halfwidth": 8}, "tpow": {"tpow": 2.0}}
 WGRAD_CASES2D = ["g2_a"]
 
 

@@ -24,9 +24,9 @@ import cases as K  # noqa: E402
 REF = K.ROOT / "oracle" / "_ref"
 
 
-def run(binary, d, mode):
-    r = subprocess.run([str(REF / binary), str(d), mode], capture_output=True, text=True,
-                       timeout=600)
+def run(binary, d, mode, *params):
+    r = subprocess.run([str(REF / binary), str(d), mode, *params], capture_output=True,
+                       text=True, timeout=600)
     if r.returncode != 0:
         sys.stderr.write(r.stdout[-2000:] + r.stderr[-2000:])
         raise SystemExit(f"{binary} {mode} failed with {r.returncode}")
@@ -183,10 +183,30 @@ def make_wgrad2d(name, out):
     print(name, "wavelet gradient max", np.abs(gw).max())
 
 
+def make_misfit3d(name, out):
+    """objFuncGradientCij3d_f of the reference with the tpow / AGC options."""
+    c = K.case3d(name)
+    s = c["s"]
+    dobs = np.load(HERE / f"{name}.npz")["dobs"]
+    res = {}
+    with tempfile.TemporaryDirectory() as td:
+        d = Path(td)
+        write_inputs3d(c, d)
+        dobs.astype(np.float32).tofile(d / "dobs.bin")
+        for key, opt in K.MISFIT_OPTIONS.items():
+            np.asarray(c["cij"], np.float32).tofile(d / "cij.bin")
+            run("ref3d", d, "grad", *[f"{k}={v}" for k, v in opt.items()])
+            res[f"fgcij_{key}"] = np.fromfile(d / "ref_fgcij.bin", dtype=np.float32)
+    np.savez_compressed(out / f"{name}_misfit.npz", **res,
+                        inputs=K.digest(s.souloc, s.recloc, s.wavelet, c["cij"], c["padb"],
+                                        c["randb"], dobs))
+    print(name, {k: float(v[0]) for k, v in res.items()})
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=str(HERE))
-    ap.add_argument("--only", choices=["all", "rtm", "wgrad"], default="all",
+    ap.add_argument("--only", choices=["all", "rtm", "wgrad", "misfit"], default="all",
                     help="rtm / wgrad: only those fixtures (needs the case fixtures)")
     a = ap.parse_args()
     out = Path(a.out)
@@ -201,6 +221,9 @@ def main():
             make_rtm3d(n, out)
         for n in K.RTM_CASES2D:
             make_rtm2d(n, out)
+    if a.only in ("all", "misfit"):
+        for n in K.MISFIT_CASES3D:
+            make_misfit3d(n, out)
     if a.only in ("all", "wgrad"):
         for n in K.WGRAD_CASES3D:
             make_wgrad3d(n, out)

@@ -169,3 +169,38 @@ def test_source_outside_update_region_is_rejected(ctx):
     bad = V.geom3d(8, 8, 8, 10, 2, 10.0, 10.0, 10.0, 1e-3, 2e-3)
     with pytest.raises(V.VtiError):
         V.Plan3d(ctx, bad)
+
+
+@pytest.mark.parametrize("name", K.MISFIT_CASES3D)
+@pytest.mark.parametrize("key", sorted(K.MISFIT_OPTIONS))
+def test_gradient_misfit_options_match_oracle_and_reference(ctx, name, key):
+    """tpow gain and AGC misfit of the gradient (objFuncGradient3d_f.cu:743-773)."""
+    c = K.case3d(name)
+    s = c["s"]
+    g = s.geom()
+    n = s.nxyz
+    opt = K.MISFIT_OPTIONS[key]
+    dobs = load_golden(name)["dobs"]
+    p = V.Plan3d(ctx, g)
+    try:
+        p.set_model(*_split(c["cij"], n), padb=c["padb"], randb=c["randb"])
+        p.set_wavelet(s.wavelet)
+        p.set_receivers(s.recloc)
+        p.set_misfit(**opt)
+        fg, mis = p.gradient(s.souloc, c["shotid"], dobs)
+        # the misfit-only entry stays plain L2, like objFuncCij3d_f
+        plain = p.objfunc(s.souloc, c["shotid"], dobs)
+    finally:
+        p.close()
+    o = O.gradient3d(g, c["cij"], c["padb"], c["randb"], s.wavelet, s.souloc, c["shotid"],
+                     s.recloc, dobs, **opt)
+    ref = load_golden(f"{name}_misfit")[f"fgcij_{key}"]
+    assert abs(mis - o[0]) / o[0] < TRACE_TOL
+    assert abs(fg[0] - ref[0]) / ref[0] < TRACE_TOL
+    for k, (a, b, r) in enumerate(zip(_parts(fg, n), _parts(o, n), _parts(ref, n))):
+        assert np.abs(b).max() > 0
+        assert rel_l2(a, b) < GRAD_TOL, k
+        assert rel_l2(a, r) < GRAD_TOL, k
+    l2 = O.gradient3d(g, c["cij"], c["padb"], c["randb"], s.wavelet, s.souloc, c["shotid"],
+                      s.recloc, dobs, misfit_only=True)
+    assert abs(plain - l2[0]) / l2[0] < TRACE_TOL

@@ -34,8 +34,9 @@ def drivers(tmp_path_factory):
     return bins
 
 
-def _run(exe, d, mode):
-    r = subprocess.run([str(exe), str(d), mode], capture_output=True, text=True, timeout=600)
+def _run(exe, d, mode, *params):
+    r = subprocess.run([str(exe), str(d), mode, *params], capture_output=True, text=True,
+                       timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
 
 
@@ -143,3 +144,23 @@ def test_shim_wavelet_gradient2d_matches_reference(drivers, name):
         _run(drivers["2d"], d, "wgrad")
         gw = np.fromfile(d / "ref_wgrad.bin", dtype=np.float32)
     assert rel_l2(gw, load_golden(f"{name}_wgrad")["gwavelet"]) < 1e-4
+
+
+@pytest.mark.parametrize("name", K.MISFIT_CASES3D)
+@pytest.mark.parametrize("key", sorted(K.MISFIT_OPTIONS))
+def test_shim_gradient_misfit_options_match_reference(drivers, name, key):
+    """tpow= / objtype= / halfwidth= read from the caller's argv."""
+    c = K.case3d(name)
+    opt = K.MISFIT_OPTIONS[key]
+    with tempfile.TemporaryDirectory() as td:
+        d = Path(td)
+        MG.write_inputs3d(c, d)
+        np.asarray(load_golden(name)["dobs"], np.float32).tofile(d / "dobs.bin")
+        np.asarray(c["cij"], np.float32).tofile(d / "cij.bin")
+        _run(drivers["3d"], d, "grad", *[f"{k}={v}" for k, v in opt.items()])
+        fg = np.fromfile(d / "ref_fgcij.bin", dtype=np.float32)
+    ref = load_golden(f"{name}_misfit")[f"fgcij_{key}"]
+    assert abs(fg[0] - ref[0]) / ref[0] < 1e-5
+    n = (ref.size - 1) // 3
+    for k in range(3):
+        assert rel_l2(fg[1 + k * n:1 + (k + 1) * n], ref[1 + k * n:1 + (k + 1) * n]) < 1e-4

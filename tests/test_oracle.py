@@ -214,3 +214,23 @@ def test_oracle_wavelet_gradient2d_matches_reference(name):
     o = O.wavelet_gradient2d(g, s.c11, s.c13, s.c33, s.sloc, s.rloc, s.taper, dobs)
     assert np.abs(o).max() > 0
     assert rel_l2(o, gold["gwavelet"]) < 1e-4
+
+
+@pytest.mark.parametrize("name", K.MISFIT_CASES3D)
+@pytest.mark.parametrize("key", sorted(K.MISFIT_OPTIONS))
+def test_oracle_gradient_misfit_options_match_reference(name, key):
+    """tpow gain / AGC misfit of objFuncGradientCij3d_f restated (FP64)."""
+    c = K.case3d(name)
+    s = c["s"]
+    g = s.geom()
+    dobs = load_golden(name)["dobs"]
+    gold = load_golden(f"{name}_misfit")
+    assert gold["inputs"] == K.digest(s.souloc, s.recloc, s.wavelet, c["cij"], c["padb"],
+                                      c["randb"], dobs)
+    fg = O.gradient3d(g, c["cij"], c["padb"], c["randb"], s.wavelet, s.souloc, c["shotid"],
+                      s.recloc, dobs, **K.MISFIT_OPTIONS[key])
+    ref = gold[f"fgcij_{key}"].astype(np.float64)
+    assert abs(fg[0] - ref[0]) / abs(ref[0]) < 1e-5
+    n = s.nxyz
+    for k in range(3):
+        assert rel_l2(fg[1 + k * n:1 + (k + 1) * n], ref[1 + k * n:1 + (k + 1) * n]) < 1e-4, k

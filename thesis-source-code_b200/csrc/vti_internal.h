@@ -175,6 +175,13 @@ int launch_set_point(vti_ctx* ctx, float* a, float* b, long long off, float valu
 int launch_residual(vti_ctx* ctx, float* trace, const float* obs, const unsigned char* live,
                     int nnt, int nr, double* acc);
 int residual_blocks(vti_ctx* ctx);
+// trace[it + ir*nnt] *= (ot + it*dt)^p (the reference's tpow gain).
+int launch_tpower(vti_ctx* ctx, float* trace, int nnt, int nr, float ot, float dt, float p);
+// AGC misfit: trace (modeled, dead traces already zeroed) becomes the AGC
+// adjoint source; part (nr doubles) gets the per-trace misfits and acc[0]
+// their fixed-order sum.
+int launch_agc_adjoint(vti_ctx* ctx, float* trace, const float* obs, int nnt, int nr, int hw,
+                       double* part, double* acc);
 int launch_boundary_merge(vti_ctx* ctx, const Dims3& d, int npad, const float* full,
                           const float* blist, float* out);
 

@@ -109,6 +109,75 @@ __global__ void k_sum_partials(const double* partial, int n, double* acc) {
   if (threadIdx.x == 0) acc[0] += v;
 }
 
+// tpower (lib/vti-fwi-3d/gpu/agc.cpp:104-116): trace[it + ir*nnt] *= (ot + it*dt)^p,
+// the time in float as the reference computes it.
+__global__ void k_tpower(float* trace, int nnt, int nr, float ot, float dt, float p) {
+  const long long n = (long long)nnt * nr;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int it = (int)(i % nnt);
+    const float t = ot + it * dt;
+    trace[i] *= powf(t, p);
+  }
+}
+
+// residualAGC (agc.cpp:62-99), one block per trace: AGC of the modeled and the
+// observed trace (windowed energy over it-hw..it+hw, indices wrapping around
+// the trace, runsum :14-25), residual of the two, its misfit into part[ir]
+// (float squares summed in double, fixed order), and the adjoint source
+// rs - d * runsum(d * rs / max(EPS, s)) written over the modeled trace.
+// Shared memory: 5 * nnt floats.
+constexpr float kAgcEps = 1e-6f;  // agc.cpp:10
+
+__device__ __forceinline__ float runsum_at(const float* w, int nnt, int hw, int i) {
+  float s = 0.f;
+  for (int j = i - hw; j <= i + hw; ++j) s += w[j < 0 ? j + nnt : (j >= nnt ? j - nnt : j)];
+  return s;
+}
+
+__global__ void k_agc_adjoint(float* trace, const float* obs, int nnt, int hw, double* part) {
+  extern __shared__ float sm[];
+  float* d = sm;              // modeled trace
+  float* e = d + nnt;         // d^2
+  float* e0 = e + nnt;        // d0^2
+  float* drss = e0 + nnt;     // d * rs / max(EPS, s)
+  float* rs = drss + nnt;     // res / sqrt(max(EPS, s))
+  __shared__ double red[32];
+  float* tr = trace + (long long)blockIdx.x * nnt;
+  const float* ob = obs + (long long)blockIdx.x * nnt;
+  for (int i = threadIdx.x; i < nnt; i += blockDim.x) {
+    const float v = tr[i], v0 = ob[i];
+    d[i] = v;
+    e[i] = v * v;
+    e0[i] = v0 * v0;
+  }
+  __syncthreads();
+  double fi = 0.0;
+  for (int i = threadIdx.x; i < nnt; i += blockDim.x) {
+    const float sd = runsum_at(e, nnt, hw, i), sd0 = runsum_at(e0, nnt, hw, i);
+    const float hd = d[i] / sqrtf(fmaxf(kAgcEps, sd));
+    const float hd0 = ob[i] / sqrtf(fmaxf(kAgcEps, sd0));
+    const float res = hd - hd0;
+    fi += (double)(res * res);
+    const float t1 = fmaxf(kAgcEps, sd);
+    const float t2 = res / sqrtf(t1);
+    drss[i] = d[i] * t2 / t1;
+    rs[i] = t2;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nnt; i += blockDim.x)
+    tr[i] = rs[i] - d[i] * runsum_at(drss, nnt, hw, i);
+  // block reduction of the misfit in a fixed order
+  for (int o = 16; o > 0; o >>= 1) fi += __shfl_down_sync(0xffffffffu, fi, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = fi;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x + 31) / 32; ++w) s += red[w];
+    part[blockIdx.x] = s;
+  }
+}
+
 // putBoundary applied on the device: out = full, with the pad region replaced
 // by the boundary list (order of boundary.cpp:10-46).
 __global__ void k_boundary_merge(Dims3 d, int npad, const float* full, const float* blist,
@@ -207,6 +276,32 @@ int launch_residual(vti_ctx* ctx, float* trace, const float* obs, const unsigned
     k_sum_partials<<<1, 32, 0, ctx->stream>>>(acc + 1, blocks, acc);
     VTI_LAUNCHED(ctx, "k_sum_partials");
   }
+  return VTI_OK;
+}
+
+int launch_tpower(vti_ctx* ctx, float* trace, int nnt, int nr, float ot, float dt, float p) {
+  const long long n = (long long)nnt * nr;
+  if (n <= 0) return VTI_OK;
+  const int blocks = (int)std::min<long long>((n + 255) / 256, (long long)ctx->sm_count * 8);
+  k_tpower<<<blocks, 256, 0, ctx->stream>>>(trace, nnt, nr, ot, dt, p);
+  VTI_LAUNCHED(ctx, "k_tpower");
+  return VTI_OK;
+}
+
+int launch_agc_adjoint(vti_ctx* ctx, float* trace, const float* obs, int nnt, int nr, int hw,
+                       double* part, double* acc) {
+  if (nnt <= 0 || nr <= 0) return VTI_OK;
+  const size_t smem = 5 * (size_t)nnt * sizeof(float);
+  if (smem > 200 * 1024)
+    return fail(ctx, VTI_ERR_UNSUPPORTED, "AGC misfit: trace longer than 10240 samples");
+  if (hw < 0 || 2 * hw + 1 > nnt)
+    return fail(ctx, VTI_ERR_ARG, "AGC half width must satisfy 0 <= 2*halfwidth+1 <= nnt");
+  VTI_CUDA(ctx, cudaFuncSetAttribute(k_agc_adjoint, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+  k_agc_adjoint<<<nr, 256, smem, ctx->stream>>>(trace, obs, nnt, hw, part);
+  VTI_LAUNCHED(ctx, "k_agc_adjoint");
+  k_sum_partials<<<1, 32, 0, ctx->stream>>>(part, nr, acc);
+  VTI_LAUNCHED(ctx, "k_sum_partials");
   return VTI_OK;
 }
 

@@ -52,6 +52,12 @@ struct vti3d_plan {
   double* d_acc = nullptr;
   float* d_gw = nullptr;  // wavelet gradient accumulator (nt)
   size_t gw_cap = 0;
+  double* d_part = nullptr;  // per-trace AGC misfits
+  size_t part_cap = 0;
+  // misfit options of the gradient (objFuncGradient3d_f.cu:743-775)
+  float tpow = 0.f;
+  int objtype = 0;
+  int halfwidth = 20;
   int last_cur = 0;  // index into sx[] of the last forward level
   bool have_model = false;
 };
@@ -401,7 +407,22 @@ int run_gradient(vti3d_plan* p, const float* souloc, const int* shotid, int nsho
     VTI_TRY(forward_pass(p, s, true));
     const float* obs = nullptr;
     VTI_TRY(get_obs(p, s, dobs, dobs_mem, &obs));
-    VTI_TRY(launch_residual(ctx, p->d_trace, obs, p->d_live, nnt, s.nr, p->d_acc));
+    if (misfit_only || (p->tpow == 0.f && p->objtype == 0)) {
+      VTI_TRY(launch_residual(ctx, p->d_trace, obs, p->d_live, nnt, s.nr, p->d_acc));
+    } else {
+      // objFuncGradient3d_f.cu:733-773: dead traces zeroed, t^p gain on the
+      // modeled traces, then the L2 residual or the AGC adjoint source
+      VTI_TRY(launch_residual(ctx, p->d_trace, nullptr, p->d_live, nnt, s.nr, nullptr));
+      if (p->tpow != 0.f)
+        VTI_TRY(launch_tpower(ctx, p->d_trace, nnt, s.nr, p->g.ot, p->g.sampling_rate, p->tpow));
+      if (p->objtype == 0) {
+        VTI_TRY(launch_residual(ctx, p->d_trace, obs, p->d_live, nnt, s.nr, p->d_acc));
+      } else {
+        VTI_TRY(ensure(ctx, &p->d_part, &p->part_cap, (size_t)std::max(s.nr, 1)));
+        VTI_TRY(launch_agc_adjoint(ctx, p->d_trace, obs, nnt, s.nr, p->halfwidth, p->d_part,
+                                   p->d_acc));
+      }
+    }
     if (misfit_only) continue;
     VTI_TRY(forward_pass(p, s, false));
     VTI_TRY(backward_pass(p, s, false));
@@ -503,7 +524,7 @@ int vti3d_plan_destroy(vti3d_plan* p) {
   vol_free(&p->g13);
   vol_free(&p->g33);
   void* ptrs[] = {p->dampx, p->d_rec, p->d_rec_damp, p->d_live, p->d_trace,
-                  p->d_obs, p->d_blist, p->d_acc, p->d_gw};
+                  p->d_obs, p->d_blist, p->d_acc, p->d_gw, p->d_part};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   delete p;
@@ -595,6 +616,16 @@ int vti3d_plan_model_data(vti3d_plan* p, const float* souloc, const int* shotid,
     VTI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   }
   return check_device_status(ctx);
+}
+
+int vti3d_plan_set_misfit(vti3d_plan* p, float tpow, int objtype, int halfwidth) {
+  if (!p) return VTI_ERR_ARG;
+  if (objtype != 0 && halfwidth < 0)
+    return fail(p->ctx, VTI_ERR_ARG, "AGC half width must be >= 0");
+  p->tpow = tpow;
+  p->objtype = objtype;
+  p->halfwidth = halfwidth;
+  return VTI_OK;
 }
 
 int vti3d_plan_gradient(vti3d_plan* p, const float* souloc, const int* shotid, int nshot,

@@ -243,6 +243,20 @@ bool over_gpus(const std::vector<int>& gpus, const std::vector<int>& shots, F fn
   return true;
 }
 
+// get_param("tpow"/"objtype"/"halfwidth") of objFuncGradient3d_f.cu:743-773
+struct MisfitParams {
+  float tpow = 0.f;
+  int objtype = 0;
+  int halfwidth = 20;
+};
+MisfitParams misfit_params() {
+  MisfitParams m;
+  m.tpow = float_arg("tpow", 0.f);
+  m.objtype = (int)float_arg("objtype", 0.f);
+  m.halfwidth = (int)float_arg("halfwidth", 20.f);
+  return m;
+}
+
 unsigned ref_flags(size_t ngpu) { return VTI_OPT_REF_GPUS((unsigned)(ngpu ? ngpu : 1)); }
 
 // gradient (or misfit) of `shots` on the GPUs of one pipeline group
@@ -271,6 +285,10 @@ bool gradient_group(float* fgcij, double* misfit, const float* souloc, const std
     if (misfit_only)
       return report(dev->ctx, vti3d_plan_objfunc(p, souloc, sub.data(), (int)sub.size(), dobs,
                                                  VTI_MEM_HOST, &mis[k]), "misfit");
+    const MisfitParams mp = misfit_params();
+    if (!report(dev->ctx, vti3d_plan_set_misfit(p, mp.tpow, mp.objtype, mp.halfwidth),
+                "misfit options"))
+      return false;
     parts[k].assign(1 + 3 * n, 0.f);
     return report(dev->ctx, vti3d_plan_gradient(p, souloc, sub.data(), (int)sub.size(), dobs,
                                                 VTI_MEM_HOST, parts[k].data(), VTI_MEM_HOST,
@@ -303,13 +321,6 @@ bool read_observed(const float* souloc, const std::vector<int>& shots, const vti
   return true;
 }
 
-bool unsupported_misfit() {
-  if (float_arg("tpow", 0.f) != 0.f || float_arg("objtype", 0.f) != 0.f) {
-    std::fprintf(stderr, "vti: tpow/objtype (t-power gain, AGC misfit) are not supported\n");
-    return true;
-  }
-  return false;
-}
 
 }  // namespace
 
@@ -326,7 +337,7 @@ void objFuncGradientCij3d_f(float* fgcij, float* souloc, int ns, std::vector<int
   std::vector<float> dobs;
   int nrec = 0;
   double mis = NAN;
-  if (!unsupported_misfit() && read_observed(souloc, shotid, g, &dobs, &nrec))
+  if (read_observed(souloc, shotid, g, &dobs, &nrec))
     gradient_group(fgcij, &mis, souloc, shotid, recloc, wavelet, cij, padboundaryCij,
                    randboundaryCij, g, GPUs, false, dobs.data(), nrec);
   fgcij[0] = (float)mis;
@@ -381,7 +392,7 @@ void objFuncCij3d_f(float* f, float* souloc, int ns, std::vector<int>& shotid, f
   std::vector<float> dobs;
   int nrec = 0;
   double mis = NAN;
-  if (!unsupported_misfit() && read_observed(souloc, shotid, g, &dobs, &nrec))
+  if (read_observed(souloc, shotid, g, &dobs, &nrec))
     gradient_group(nullptr, &mis, souloc, shotid, recloc, wavelet, cij, padboundaryCij, nullptr,
                    g, GPUs, true, dobs.data(), nrec);
   *f = (float)mis;

@@ -87,6 +87,7 @@ def _signatures():
                                           C.POINTER(C.c_double)]),
         "vti3d_plan_objfunc": (C.c_int, [P, P, P, C.c_int, P, C.c_int, C.POINTER(C.c_double)]),
         "vti3d_plan_rtm": (C.c_int, [P, P, P, C.c_int, P, C.c_int, P, C.c_int]),
+        "vti3d_plan_set_misfit": (C.c_int, [P, C.c_float, C.c_int, C.c_int]),
         "vti3d_rtm_cij": (C.c_int, [P, P, P, P, P, P, P, P, C.c_int, P, C.c_int, P, P, C.c_uint]),
         "vti3d_plan_wavefield": (VP, [P]),
         "vti3d_model_data_cij": (C.c_int, [P, P, P, P, P, P, P, P, C.c_int, P, C.c_int, P,
@@ -272,6 +273,11 @@ class Plan3d:
                                                  _p(dobs), dobs_mem, _p(fgcij), fgcij_mem,
                                                  C.byref(mis)))
         return fgcij, mis.value
+
+    def set_misfit(self, tpow=0.0, objtype=0, halfwidth=20):
+        """tpow gain / AGC misfit of the gradient (the reference's tpow=,
+        objtype=, halfwidth= parameters)."""
+        self.ctx.check(lib().vti3d_plan_set_misfit(self._h, tpow, objtype, halfwidth))
 
     def rtm(self, souloc, shotid, data, data_mem=MEM_HOST, image=None, image_mem=MEM_HOST):
         """rtmCij3d_f on the resident model: the image (nxyz)."""
