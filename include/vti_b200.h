@@ -253,6 +253,12 @@ int vti2d_gn_hessian(vti_ctx* ctx, const vti2d_geom* g, float* gc11, float* gc13
 int vti2d_rtm(vti_ctx* ctx, const vti2d_geom* g, float* image, const float* data,
               const float* c11, const float* c13, const float* c33, const float* wavelet,
               const int* sloc, int ns, const int* rloc, int nr, const float* taper);
+/* odcig_f (lib/vti-fwi-2d/odcig_f.cu:12): offset-domain common-image gathers,
+ * image[(h+nhx)*nnxz + i] for subsurface x offsets |h| <= nhx ((2nhx+1)*nnxz
+ * floats), the migration of vti2d_rtm with the extended imaging condition. */
+int vti2d_odcig(vti_ctx* ctx, const vti2d_geom* g, int nhx, float* image, const float* data,
+                const float* c11, const float* c13, const float* c33, const float* wavelet,
+                const int* sloc, int ns, const int* rloc, int nr, const float* taper);
 /* waveletGradient_f (lib/vti-fwi-2d/objFuncGradient_f.cu:373): gradient of the
  * misfit with respect to the source wavelet (nt floats): dt2 (p + q) of the
  * adjoint wavefield at the source for every level, the adjoint driven by the

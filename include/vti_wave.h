@@ -154,6 +154,12 @@ void rtm_f(float* image, const float* data, const float* c11, const float* c13, 
            const float* taper, int nx, int nz, int nt, int npad, float dx, float dz, float dt,
            float rate, float ot = 0.);
 
+// wave.h:16 — offset-domain common-image gathers, (2nhx+1) * nnxz floats.
+void odcig_f(float* image, const float* data, const float* c11, const float* c13,
+             const float* c33, const float* wavelet, const int* sloc, int ns, const int* rloc,
+             int nr, const float* taper, int nx, int nz, int nhx, int nt, int npad, float dx,
+             float dz, float dt, float rate, float ot = 0.);
+
 // wave.h:18 — gradient w.r.t. the source wavelet (nt floats).
 void waveletGradient_f(float* gwavelet, const float* d0, const float* c11, const float* c13,
                        const float* c33, const int* sloc, int ns, const int* rloc, int nr,

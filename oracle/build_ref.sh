@@ -44,7 +44,7 @@ build_objs "$IO" "$OUT/obj3d" myio.cpp
 
 # 2D path (synthetic_f.cu, modeling_f.cu)
 build_objs "$L2" "$OUT/obj2d" kernels.cu synthetic_f.cu modeling_f.cu objFuncGradient_f.cu \
-  hessian_f.cu rtm_f.cu check.cpp conversions.cpp
+  hessian_f.cu rtm_f.cu odcig_f.cu check.cpp conversions.cpp
 build_objs "$IO" "$OUT/obj2d" myio.cpp
 "$NVCC" $FLAGS -x cu -c "$HERE/ref_driver2d.cpp" -o "$OUT/obj2d/ref_driver2d.o"
 "$NVCC" $ARCH -Xcompiler -fopenmp -o "$OUT/ref2d" "$OUT"/obj2d/*.o

@@ -214,6 +214,23 @@ def rtm2d(g, c11, c13, c33, wavelet, sloc, rloc, taper, data, dtype=np.float64):
     return out
 
 
+def odcig2d(g, nhx, c11, c13, c33, wavelet, sloc, rloc, taper, data, dtype=np.float64):
+    """odcig_f restated: offset-domain image gathers, (2 nhx + 1) x nnxz."""
+    suf = "f64" if dtype == np.float64 else "f32"
+    f = getattr(lib(), f"orc2d_odcig_{suf}")
+    f.argtypes = [VP, VP, C.c_int] + [VP] * 6 + [C.c_int, VP, C.c_int, VP, VP]
+    f.restype = C.c_int
+    ip = np.array([g.nx, g.nz, g.nt, g.npad], dtype=np.int32)
+    fp = np.array([g.dx, g.dz, g.dt, g.rate, g.ot], dtype=np.float32)
+    nnxz = (g.nx + 2 * g.npad) * (g.nz + 2 * g.npad)
+    out = np.zeros((2 * nhx + 1) * nnxz, dtype=dtype)
+    sloc, rloc = _i32(sloc).reshape(-1), _i32(rloc).reshape(-1)
+    f(_p(ip), _p(fp), nhx, _p(_f32(c11)), _p(_f32(c13)), _p(_f32(c33)), _p(_f32(wavelet)),
+      _p(_f32(data)), _p(sloc), sloc.size // 4, _p(rloc), rloc.size // 2, _p(_f32(taper)),
+      _p(out))
+    return out.reshape(2 * nhx + 1, nnxz)
+
+
 def wavelet_gradient2d(g, c11, c13, c33, sloc, rloc, taper, data, dtype=np.float64):
     """waveletGradient_f restated: the gradient w.r.t. the wavelet (nt)."""
     suf = "f64" if dtype == np.float64 else "f32"

@@ -2,7 +2,7 @@
 // sources by oracle/build_ref.sh into oracle/_ref/ref2d) on inputs written by
 // tests/golden/make_golden.py. TEST INFRASTRUCTURE ONLY.
 //
-// usage: ref2d <dir> synthetic|modeling|grad|gnhess|rtm|wgrad
+// usage: ref2d <dir> synthetic|modeling|grad|gnhess|rtm|wgrad|odcig [nhx]
 //   <dir>/params.txt : nx nz nt npad dx dz dt rate ot ns nr
 //   <dir>/{c11,c13,c33,taper,wavelet}.bin (float32), sloc.bin / rloc.bin (int32)
 #include <cstdio>
@@ -37,6 +37,10 @@ void rtm_f(float* image, const float* data, const float* c11, const float* c13, 
            const float* taper, int nx, int nz, int nt, int npad, float dx, float dz, float dt,
            float rate, float ot);
 
+void odcig_f(float* image, const float* data, const float* c11, const float* c13,
+             const float* c33, const float* wavelet, const int* sloc, int ns, const int* rloc,
+             int nr, const float* taper, int nx, int nz, int nhx, int nt, int npad, float dx,
+             float dz, float dt, float rate, float ot);
 void waveletGradient_f(float* gwavelet, const float* d0, const float* c11, const float* c13,
                        const float* c33, const int* sloc, int ns, const int* rloc, int nr,
                        const float* taper, int nx, int nz, int nt, int npad, float dx, float dz,
@@ -131,6 +135,18 @@ int main(int argc, char** argv) {
     rtm_f(image.data(), data.data(), c11.data(), c13.data(), c33.data(), wavelet.data(),
           sloc.data(), ns, rloc.data(), nr, taper.data(), nx, nz, nt, npad, dx, dz, dt, rate, ot);
     save(dir + "/ref_rtm.bin", image.data(), image.size());
+  } else if (mode == "odcig") {
+    const int nhx = argc > 3 ? std::atoi(argv[3]) : 4;
+    auto rloc = load<int>(dir + "/rloc.bin", 2 * (size_t)nr);
+    const int ratio = (int)(rate / dt + 0.5f);
+    const int ntneg = (int)(ot < 0 ? (-ot / dt + 0.5f) : 0);
+    const size_t rows = (nt - ntneg - 1) / ratio + 1;
+    auto data = load<float>(dir + "/data.bin", rows * nr);
+    std::vector<float> image((2 * nhx + 1) * nnxz, 0.f);
+    odcig_f(image.data(), data.data(), c11.data(), c13.data(), c33.data(), wavelet.data(),
+            sloc.data(), ns, rloc.data(), nr, taper.data(), nx, nz, nhx, nt, npad, dx, dz, dt,
+            rate, ot);
+    save(dir + "/ref_odcig.bin", image.data(), image.size());
   } else if (mode == "wgrad") {
     // <dir>/data.bin: the traces driving the adjoint (nnt = (nt-1)/ratio+1 rows)
     auto rloc = load<int>(dir + "/rloc.bin", 2 * (size_t)nr);

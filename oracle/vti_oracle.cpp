@@ -646,17 +646,24 @@ void dipole2d(const Geo2& g, T* p, T* q, long i, T a) {
 // image += 0.5(p+q) * ((1-f) S0 + f S1). Slices never written are zero (the
 // host array is zero-initialised once, rtm_f.cu:55; the index one past the
 // last slice, read with weight 0 at the first imaging, is taken as zero).
+// nhx >= 0: odcig_f (lib/vti-fwi-2d/odcig_f.cu:12-232), the same migration
+// with extendedImagingCrossCor (kernels.cu:425-436): image[i + (h+nhx)*nnxz]
+// += 0.5(p+q)[i-h] * S[i+h] for |h| <= nhx over the reference kernel's threads
+// (16x16 blocks from (4,4): x in [max(4,nhx), min(nnx-nhx, 4+16*gx)), z in
+// [4, min(nnz, 4+16*gz))); its source pass injects w[it-1] without the dt2
+// factor after level 1 (odcig_f.cu:124).
 template <typename T>
 void rtm2d(const Geo2& g, const float* c11, const float* c13, const float* c33,
            const float* wavelet, const float* data, const int* sloc, int ns, const int* rloc,
-           int nr_total, const float* taper, T* image) {
+           int nr_total, const float* taper, T* image, int nhx = -1) {
   const long nnx = g.nnx(), nnz = g.nnz(), nnxz = nnx * nnz;
   const float dt = g.dt, dt2 = dt * dt;
   const int ratio = (int)(g.rate / dt + 0.5f);
   const int ntNeg = (int)std::round(std::fabs(g.ot) / dt);
   const int nnt = (g.nt - 1) / ratio + 1;
   const int nnt_data = (g.nt - ntNeg - 1) / ratio + 1;
-  std::fill(image, image + nnxz, (T)0);
+  const long nimg = nhx < 0 ? 1 : 2 * nhx + 1;
+  std::fill(image, image + nnxz * nimg, (T)0);
   std::vector<T> sw((size_t)(nnt + 1) * nnxz, 0);
   auto slice = [&](int j, const T* p, const T* q) {
     for (long iz = kHalf; iz < nnz - kHalf; ++iz)
@@ -665,9 +672,22 @@ void rtm2d(const Geo2& g, const float* c11, const float* c13, const float* c33,
         sw[(size_t)j * nnxz + i] = (T)0.5f * (p[i] + q[i]);
       }
   };
+  const long gx = (nnx - 8 + 15) / 16, gz = (nnz - 8 + 15) / 16;
   auto img = [&](const T* p, const T* q, int s0, int s1, float f) {
     const T* A = sw.data() + (size_t)s0 * nnxz;
     const T* B = sw.data() + (size_t)s1 * nnxz;
+    if (nhx >= 0) {
+      for (long iz = kHalf; iz < std::min(nnz, 4 + 16 * gz); ++iz)
+        for (long ix = std::max<long>(kHalf, nhx); ix < std::min<long>(nnx - nhx, 4 + 16 * gx);
+             ++ix) {
+          long i = ix + iz * nnx;
+          for (int h = -nhx; h <= nhx; ++h) {
+            T d = (1 - (T)f) * A[i + h] + (T)f * B[i + h];
+            image[i + (h + nhx) * nnxz] += (T)0.5f * (p[i - h] + q[i - h]) * d;
+          }
+        }
+      return;
+    }
     for (long iz = kHalf; iz < nnz - kHalf; ++iz)
       for (long ix = kHalf; ix < nnx - kHalf; ++ix) {
         long i = ix + iz * nnx;
@@ -685,7 +705,8 @@ void rtm2d(const Geo2& g, const float* c11, const float* c13, const float* c33,
     if (ratio == 1) slice(1, p1.data(), q1.data());
     for (int it = 2; it < g.nt; ++it) {
       step2d<T>(g, c11, c13, c33, p1.data(), q1.data(), p0.data(), q0.data());
-      dipole2d<T>(g, p0.data(), q0.data(), sxz, (T)(dt2 * wavelet[it - 1]));
+      dipole2d<T>(g, p0.data(), q0.data(), sxz,
+                  (T)(nhx < 0 ? dt2 * wavelet[it - 1] : wavelet[it - 1]));
       taper2d(g, taper, p1.data()); taper2d(g, taper, q1.data());
       taper2d(g, taper, p0.data()); taper2d(g, taper, q0.data());
       if (it % ratio == 0) slice(it / ratio, p0.data(), q0.data());
@@ -1265,6 +1286,18 @@ ORC2D_GRAD(float, f32)
   }
 ORC2D_RTM(double, f64)
 ORC2D_RTM(float, f32)
+
+#define ORC2D_ODCIG(T, SUF)                                                                     \
+  int orc2d_odcig_##SUF(const int* ip, const float* fp, int nhx, const float* c11,               \
+                        const float* c13, const float* c33, const float* wavelet,                \
+                        const float* data, const int* sloc, int ns, const int* rloc, int nr,     \
+                        const float* taper, T* image) {                                          \
+    Geo2 g = unpack2(ip, fp);                                                                    \
+    rtm2d<T>(g, c11, c13, c33, wavelet, data, sloc, ns, rloc, nr, taper, image, nhx);            \
+    return 0;                                                                                    \
+  }
+ORC2D_ODCIG(double, f64)
+ORC2D_ODCIG(float, f32)
 
 #define ORC2D_WGRAD(T, SUF)                                                                     \
   int orc2d_wavelet_gradient_##SUF(const int* ip, const float* fp, const float* c11,             \

@@ -88,6 +88,8 @@ WGRAD_CASES3D = ["g3_a"]
 MISFIT_CASES3D = ["g3_a"]
 MISFIT_OPTIONS = {"agc": {"objtype": 1, "halfwidth": 8}, "tpow": {"tpow": 2.0}}
 WGRAD_CASES2D = ["g2_a"]
+# offset-domain image gathers (<case>_odcig.npz): half width in x offsets
+ODCIG_CASES2D = {"g2_a": 6}
 
 
 def pad_model3d(c: dict) -> np.ndarray:

@@ -149,6 +149,24 @@ def make_rtm2d(name, out):
     print(name, "rtm image max", np.abs(image).max())
 
 
+def make_odcig2d(name, out):
+    """odcig_f of the reference: the golden dobs migrated into x-offset gathers."""
+    c = K.case2d(name)
+    s = c["s"]
+    nhx = K.ODCIG_CASES2D[name]
+    dobs = np.load(HERE / f"{name}.npz")["dobs"]
+    with tempfile.TemporaryDirectory() as td:
+        d = Path(td)
+        write_inputs2d(s, d)
+        dobs.astype(np.float32).tofile(d / "data.bin")
+        run("ref2d", d, "odcig", str(nhx))
+        image = np.fromfile(d / "ref_odcig.bin", dtype=np.float32)
+    np.savez_compressed(out / f"{name}_odcig.npz", image=image, nhx=nhx,
+                        inputs=K.digest(s.c11, s.c13, s.c33, s.taper, s.wavelet, s.sloc, s.rloc,
+                                        dobs))
+    print(name, "odcig max", np.abs(image).max())
+
+
 def make_wgrad3d(name, out):
     """waveletGradientCij3d_f of the reference, driven by the golden dobs."""
     c = K.case3d(name)
@@ -206,7 +224,7 @@ def make_misfit3d(name, out):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=str(HERE))
-    ap.add_argument("--only", choices=["all", "rtm", "wgrad", "misfit"], default="all",
+    ap.add_argument("--only", choices=["all", "rtm", "wgrad", "misfit", "odcig"], default="all",
                     help="rtm / wgrad: only those fixtures (needs the case fixtures)")
     a = ap.parse_args()
     out = Path(a.out)
@@ -221,6 +239,9 @@ def main():
             make_rtm3d(n, out)
         for n in K.RTM_CASES2D:
             make_rtm2d(n, out)
+    if a.only in ("all", "odcig"):
+        for n in K.ODCIG_CASES2D:
+            make_odcig2d(n, out)
     if a.only in ("all", "misfit"):
         for n in K.MISFIT_CASES3D:
             make_misfit3d(n, out)

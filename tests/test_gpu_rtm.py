@@ -89,3 +89,20 @@ def test_rtm2d_every_step_sampled_matches_oracle(ctx):
     o = O.rtm2d(g, s.c11, s.c13, s.c33, s.wavelet, s.sloc, s.rloc, s.taper, data)
     assert np.abs(o).max() > 0
     assert rel_l2(img, o) < IMAGE_TOL
+
+
+@pytest.mark.parametrize("name", sorted(K.ODCIG_CASES2D))
+def test_odcig2d_matches_oracle_and_reference(ctx, name):
+    """odcig_f: offset-domain common-image gathers."""
+    s = K.case2d(name)["s"]
+    g = s.geom()
+    nhx = K.ODCIG_CASES2D[name]
+    dobs = load_golden(name)["dobs"]
+    img = V.odcig_f(ctx, g, nhx, dobs, s.c11, s.c13, s.c33, s.wavelet, s.sloc, s.rloc, s.taper)
+    o = O.odcig2d(g, nhx, s.c11, s.c13, s.c33, s.wavelet, s.sloc, s.rloc, s.taper, dobs)
+    assert np.abs(o).max() > 0
+    assert rel_l2(img, o) < IMAGE_TOL
+    ref = load_golden(f"{name}_odcig")["image"].reshape(2 * nhx + 1, -1)
+    assert rel_l2(img, ref) < IMAGE_TOL
+    # every offset panel carries signal
+    assert all(np.abs(ref[h]).max() > 0 for h in range(2 * nhx + 1))

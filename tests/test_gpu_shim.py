@@ -164,3 +164,15 @@ def test_shim_gradient_misfit_options_match_reference(drivers, name, key):
     n = (ref.size - 1) // 3
     for k in range(3):
         assert rel_l2(fg[1 + k * n:1 + (k + 1) * n], ref[1 + k * n:1 + (k + 1) * n]) < 1e-4
+
+
+@pytest.mark.parametrize("name", sorted(K.ODCIG_CASES2D))
+def test_shim_odcig2d_matches_reference(drivers, name):
+    s = K.case2d(name)["s"]
+    with tempfile.TemporaryDirectory() as td:
+        d = Path(td)
+        MG.write_inputs2d(s, d)
+        np.asarray(load_golden(name)["dobs"], np.float32).tofile(d / "data.bin")
+        _run(drivers["2d"], d, "odcig", str(K.ODCIG_CASES2D[name]))
+        img = np.fromfile(d / "ref_odcig.bin", dtype=np.float32)
+    assert rel_l2(img, load_golden(f"{name}_odcig")["image"]) < 1e-4

@@ -234,3 +234,18 @@ def test_oracle_gradient_misfit_options_match_reference(name, key):
     n = s.nxyz
     for k in range(3):
         assert rel_l2(fg[1 + k * n:1 + (k + 1) * n], ref[1 + k * n:1 + (k + 1) * n]) < 1e-4, k
+
+
+@pytest.mark.parametrize("name", sorted(K.ODCIG_CASES2D))
+def test_oracle_odcig2d_matches_reference(name):
+    """odcig_f restated (FP64) against the reference's own gathers."""
+    s = K.case2d(name)["s"]
+    g = s.geom()
+    nhx = K.ODCIG_CASES2D[name]
+    dobs = load_golden(name)["dobs"]
+    gold = load_golden(f"{name}_odcig")
+    assert int(gold["nhx"]) == nhx
+    assert gold["inputs"] == K.digest(s.c11, s.c13, s.c33, s.taper, s.wavelet, s.sloc, s.rloc,
+                                      dobs)
+    o = O.odcig2d(g, nhx, s.c11, s.c13, s.c33, s.wavelet, s.sloc, s.rloc, s.taper, dobs)
+    assert rel_l2(o.reshape(-1), gold["image"]) < 1e-4

@@ -122,15 +122,37 @@ __global__ void k_rtm2d_inject(float* p, float* q, const float* d0, const float*
   if (dipole) add(ridx[ir] + nnx, -v);
 }
 
+// extendedImagingCrossCor (kernels.cu:425-436) over the reference kernel's
+// threads: image[i + (h+nhx)*nnxz] += 0.5(p+q)[i-h] * ((1-f) S0 + f S1)[i+h],
+// x in [x_lo, x_hi), z in [4, z_hi).
+__global__ void k_odcig_image(float* image, const float* p, const float* q, const float* s0,
+                              const float* s1, float f, int nnx, int nnz, int nhx, int x_lo,
+                              int x_hi, int z_hi) {
+  const int ix = x_lo + blockIdx.x * blockDim.x + threadIdx.x;
+  const int iz = kHalo + blockIdx.y * blockDim.y + threadIdx.y;
+  if (ix >= x_hi || iz >= z_hi) return;
+  const long long nnxz = (long long)nnx * nnz;
+  const int i = ix + iz * nnx;
+  for (int h = -nhx; h <= nhx; ++h) {
+    const float d = (1.f - f) * s0[i + h] + f * s1[i + h];
+    image[i + (h + nhx) * nnxz] += 0.5f * (p[i - h] + q[i - h]) * d;
+  }
+}
+
 }  // namespace
 }  // namespace vti
 
 using namespace vti;
 
-extern "C" int vti2d_rtm(vti_ctx* ctx, const vti2d_geom* g, float* image, const float* data,
-                         const float* c11, const float* c13, const float* c33,
-                         const float* wavelet, const int* sloc, int ns, const int* rloc, int nr,
-                         const float* taper) {
+namespace {
+
+// rtm_f (nhx < 0) and odcig_f (nhx >= 0, lib/vti-fwi-2d/odcig_f.cu:12-232):
+// the same passes; odcig_f images with subsurface x offsets |h| <= nhx and its
+// source pass injects w[it-1] without the dt2 factor after level 1
+// (odcig_f.cu:124).
+int rtm2d_impl(vti_ctx* ctx, const vti2d_geom* g, int nhx, float* image, const float* data,
+               const float* c11, const float* c13, const float* c33, const float* wavelet,
+               const int* sloc, int ns, const int* rloc, int nr, const float* taper) {
   if (!ctx || !g || !image || !data || !c11 || !c13 || !c33 || !wavelet || !sloc || !taper ||
       (nr > 0 && !rloc) || ns < 0)
     return VTI_ERR_ARG;
@@ -163,7 +185,10 @@ extern "C" int vti2d_rtm(vti_ctx* ctx, const vti2d_geom* g, float* image, const 
   cudaStream_t sm = ctx->stream;
   // device buffers: model, taper, 4 wavefields, image, slices, traces, receivers
   const size_t nslices = (size_t)nnt + 1;  // one past the last slice reads zeros
-  const size_t nfloat = 9 * (size_t)nnxz + nslices * nnxz + (size_t)nnt_data * nr;
+  const size_t nimg = nhx < 0 ? 1 : 2 * (size_t)nhx + 1;
+  if (nhx >= 0 && 2 * nhx + 1 > nnx)
+    return fail(ctx, VTI_ERR_ARG, "ODCIG: 2*nhx+1 exceeds the grid width");
+  const size_t nfloat = (8 + nimg) * (size_t)nnxz + nslices * nnxz + (size_t)nnt_data * nr;
   float* buf = nullptr;
   int* d_ridx = nullptr;
   VTI_CUDA(ctx, cudaMalloc((void**)&buf, nfloat * sizeof(float)));
@@ -175,7 +200,7 @@ extern "C" int vti2d_rtm(vti_ctx* ctx, const vti2d_geom* g, float* image, const 
   float *dc11 = buf, *dc13 = dc11 + nnxz, *dc33 = dc13 + nnxz, *dtap = dc33 + nnxz;
   float *p0 = dtap + nnxz, *q0 = p0 + nnxz, *p1 = q0 + nnxz, *q1 = p1 + nnxz;
   float* dimg = q1 + nnxz;
-  float* slices = dimg + nnxz;
+  float* slices = dimg + nimg * nnxz;
   float* ddata = slices + nslices * nnxz;
   auto done = [&](int status) {
     cudaStreamSynchronize(sm);
@@ -195,7 +220,7 @@ extern "C" int vti2d_rtm(vti_ctx* ctx, const vti2d_geom* g, float* image, const 
   if (nr > 0)
     RTM_CK(cudaMemcpyAsync(ddata, data, (size_t)nnt_data * nr * 4, cudaMemcpyHostToDevice, sm));
   // image and every slice start at zero (rtm_f.cu:24,55)
-  RTM_CK(cudaMemsetAsync(dimg, 0, (nnxz + nslices * nnxz) * 4, sm));
+  RTM_CK(cudaMemsetAsync(dimg, 0, (nimg * nnxz + nslices * nnxz) * 4, sm));
   std::vector<int> ridx(std::max(nr, 1));
   for (int ir = 0; ir < nr; ++ir) ridx[ir] = rloc[2 * ir] + rloc[2 * ir + 1] * nnx;
   RTM_CK(cudaMemcpyAsync(d_ridx, ridx.data(), std::max(nr, 1) * sizeof(int),
@@ -246,7 +271,7 @@ extern "C" int vti2d_rtm(vti_ctx* ctx, const vti2d_geom* g, float* image, const 
     a.image = nullptr;
     for (int it = 2; it < g->nt; ++it) {
       a.src = sxz;
-      a.amp = dt2 * wavelet[it - 1];
+      a.amp = nhx < 0 ? dt2 * wavelet[it - 1] : wavelet[it - 1];
       a.slice = (it % ratio == 0) ? slice_at(it / ratio) : nullptr;
       st = step(cp, cq, np, nq);
       if (st != VTI_OK) return done(st);
@@ -276,8 +301,24 @@ extern "C" int vti2d_rtm(vti_ctx* ctx, const vti2d_geom* g, float* image, const 
     float f = (g->nt - 2.) / ratio;
     int s0 = (int)f, s1 = std::min(s0 + 1, nnt);
     f -= s0;
-    // the level just made is imaged by the next kernel, which reads it as cur
-    a.image = dimg;
+    // extended imaging of a finished level, right after its injection
+    const int x_lo = std::max(kHalo, nhx);
+    const int x_hi = std::min(nnx - nhx, kHalo + 16 * ((nnx - 8 + 15) / 16));
+    const int z_hi = std::min(nnz, kHalo + 16 * ((nnz - 8 + 15) / 16));
+    auto odcig = [&](const float* p, const float* q, float fw) -> int {
+      if (x_hi <= x_lo) return VTI_OK;
+      const dim3 b2(32, 8), g2((x_hi - x_lo + 31) / 32, (z_hi - kHalo + 7) / 8);
+      k_odcig_image<<<g2, b2, 0, sm>>>(dimg, p, q, slice_at(s0), slice_at(s1), fw, nnx, nnz, nhx,
+                                       x_lo, x_hi, z_hi);
+      ctx->launches++;
+      return cuda_check(ctx, cudaGetLastError(), "k_odcig_image");
+    };
+    if (nhx >= 0) {
+      st = odcig(cp, cq, f);
+      if (st != VTI_OK) return done(st);
+    }
+    // RTM: the level just made is imaged by the next kernel, which reads it as cur
+    a.image = nhx < 0 ? dimg : nullptr;
     a.s0 = slice_at(s0);
     a.s1 = slice_at(s1);
     a.f = f;
@@ -305,18 +346,40 @@ extern "C" int vti2d_rtm(vti_ctx* ctx, const vti2d_geom* g, float* image, const 
       a.s0 = slice_at(s0);
       a.s1 = slice_at(s1);
       a.f = fs;
+      if (nhx >= 0) {
+        st = odcig(np, nq, fs);
+        if (st != VTI_OK) return done(st);
+      }
       std::swap(cp, np);
       std::swap(cq, nq);
     }
-    // image the last level (it = 0)
-    st = step(cp, cq, nullptr, nullptr);
-    if (st != VTI_OK) return done(st);
+    if (nhx < 0) {  // image the last level (it = 0)
+      st = step(cp, cq, nullptr, nullptr);
+      if (st != VTI_OK) return done(st);
+    }
     a.image = nullptr;
   }
-  RTM_CK(cudaMemcpyAsync(image, dimg, nnxz * 4, cudaMemcpyDeviceToHost, sm));
+  RTM_CK(cudaMemcpyAsync(image, dimg, nimg * nnxz * 4, cudaMemcpyDeviceToHost, sm));
   RTM_CK(cudaStreamSynchronize(sm));
 #undef RTM_CK
   return done(VTI_OK);
+}
+
+}  // namespace
+
+extern "C" int vti2d_rtm(vti_ctx* ctx, const vti2d_geom* g, float* image, const float* data,
+                         const float* c11, const float* c13, const float* c33,
+                         const float* wavelet, const int* sloc, int ns, const int* rloc, int nr,
+                         const float* taper) {
+  return rtm2d_impl(ctx, g, -1, image, data, c11, c13, c33, wavelet, sloc, ns, rloc, nr, taper);
+}
+
+extern "C" int vti2d_odcig(vti_ctx* ctx, const vti2d_geom* g, int nhx, float* image,
+                           const float* data, const float* c11, const float* c13,
+                           const float* c33, const float* wavelet, const int* sloc, int ns,
+                           const int* rloc, int nr, const float* taper) {
+  if (nhx < 0) return fail(ctx, VTI_ERR_ARG, "ODCIG: nhx must be >= 0");
+  return rtm2d_impl(ctx, g, nhx, image, data, c11, c13, c33, wavelet, sloc, ns, rloc, nr, taper);
 }
 
 // waveletGradient_f (lib/vti-fwi-2d/objFuncGradient_f.cu:373-530): per shot the

@@ -953,3 +953,37 @@ void waveletGradient_f(float* gwavelet, const float* d0, const float* c11, const
     if (!v.empty())
       for (int i = 0; i < nt; ++i) gwavelet[i] += v[i];
 }
+
+// odcig_f (odcig_f.cu:12-232): shots round-robin over the gpu= devices,
+// per-device gathers summed.
+void odcig_f(float* image, const float* data, const float* c11, const float* c13,
+             const float* c33, const float* wavelet, const int* sloc, int ns, const int* rloc,
+             int nr, const float* taper, int nx, int nz, int nhx, int nt, int npad, float dx,
+             float dz, float dt, float rate, float ot) {
+  vti2d_geom g{nx, nz, nt, npad, dx, dz, dt, rate, ot};
+  const size_t n = (size_t)(nx + 2 * npad) * (nz + 2 * npad) * (2 * (size_t)std::max(nhx, 0) + 1);
+  std::memset(image, 0, n * sizeof(float));
+  const std::vector<int> gpus = gpus_from_argv();
+  auto parts = shots_per_gpu(ns, gpus.size());
+  std::vector<std::vector<float>> img(gpus.size());
+  std::vector<std::thread> th;
+  for (size_t k = 0; k < gpus.size(); ++k) {
+    if (parts[k].empty()) continue;
+    th.emplace_back([&, k]() {
+      Device* dev = device(gpus[k]);
+      if (!dev) return;
+      std::lock_guard<std::mutex> lk(dev->mu);
+      std::vector<int> sl;
+      for (int is : parts[k]) sl.insert(sl.end(), sloc + 4 * is, sloc + 4 * is + 4);
+      img[k].assign(n, 0.f);
+      if (!report(dev->ctx, vti2d_odcig(dev->ctx, &g, nhx, img[k].data(), data, c11, c13, c33,
+                                        wavelet, sl.data(), (int)parts[k].size(), rloc, nr,
+                                        taper), "odcig"))
+        img[k].clear();
+    });
+  }
+  for (auto& t : th) t.join();
+  for (auto& v : img)
+    if (!v.empty())
+      for (size_t i = 0; i < n; ++i) image[i] += v[i];
+}

@@ -102,6 +102,7 @@ def _signatures():
         "vti2d_gn_hessian": (C.c_int, [P] * 13 + [C.c_int, P, C.c_int, P]),
         "vti2d_rtm": (C.c_int, [P] * 9 + [C.c_int, P, C.c_int, P]),
         "vti2d_wavelet_gradient": (C.c_int, [P] * 8 + [C.c_int, P, C.c_int, P]),
+        "vti2d_odcig": (C.c_int, [P, P, C.c_int] + [P] * 7 + [C.c_int, P, C.c_int, P]),
         "vti3d_plan_wavelet_gradient": (C.c_int, [P, P, P, C.c_int, P, C.c_int, P, C.c_int]),
         "vti3d_wavelet_gradient_cij": (C.c_int, [P] * 7 + [C.c_int, P, C.c_int, P, P, C.c_uint]),
         "vti3d_plan_get_wavefield": (C.c_int, [P, P, C.c_int]),
@@ -380,6 +381,18 @@ def objFuncGradient_f(ctx, g: Geom2d, data, c11, c13, c33, wavelet, sloc, rloc, 
                                    _p(_f32(wavelet)), _p(sloc), sloc.size // 4, _p(rloc),
                                    rloc.size // 2, _p(_f32(taper)), C.byref(mis)))
     return out[0], out[1], out[2], mis.value
+
+
+def odcig_f(ctx, g: Geom2d, nhx, data, c11, c13, c33, wavelet, sloc, rloc, taper):
+    """odcig_f (lib/vti-fwi-2d/odcig_f.cu:12): (2 nhx + 1) x nnxz gathers."""
+    sloc, rloc = _i32(sloc).reshape(-1), _i32(rloc).reshape(-1)
+    nnxz = (g.nx + 2 * g.npad) * (g.nz + 2 * g.npad)
+    out = np.zeros((2 * nhx + 1) * nnxz, dtype=np.float32)
+    ctx.check(lib().vti2d_odcig(ctx.handle, C.byref(g), nhx, _p(out), _p(_f32(data)),
+                                _p(_f32(c11)), _p(_f32(c13)), _p(_f32(c33)), _p(_f32(wavelet)),
+                                _p(sloc), sloc.size // 4, _p(rloc), rloc.size // 2,
+                                _p(_f32(taper))))
+    return out.reshape(2 * nhx + 1, nnxz)
 
 
 def waveletGradient_f(ctx, g: Geom2d, data, c11, c13, c33, sloc, rloc, taper):
