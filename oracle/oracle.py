@@ -141,6 +141,42 @@ def wavelet_gradient3d(g, c11, c13, c33, souloc, shotid, recloc, data, dtype=np.
     return out
 
 
+def _exact3d(name, g, c11, c13, c33, wavelet, souloc, shotid, recloc, extra, n_out):
+    ip, fp = _geo3(g, full_steps=True)
+    f = getattr(lib(), name)
+    f.argtypes = [VP] * 8 + [C.c_int] + [VP] * (2 + len(extra))
+    f.restype = C.c_int
+    out = np.zeros(n_out)
+    shotid = _i32(shotid)
+    f(_p(ip), _p(fp), *[_p(np.ascontiguousarray(a, dtype=np.float64)) for a in (c11, c13, c33)],
+      _p(_f32(wavelet)), _p(_f32(souloc)), _p(shotid), len(shotid), _p(_f32(recloc).reshape(-1)),
+      *[_p(np.ascontiguousarray(e, dtype=np.float64)) for e in extra], _p(out))
+    return out
+
+
+def exact_forward3d(g, c11, c13, c33, wavelet, souloc, shotid, recloc):
+    """EXACT-mode traces (self-check operator, every level up to nt-1); the
+    model is taken in FP64."""
+    nrec = np.asarray(recloc).size // 4
+    return _exact3d("orc3d_exact_forward", g, c11, c13, c33, wavelet, souloc, shotid, recloc,
+                    [], nnt3d(g) * nrec)
+
+
+def exact_born3d(g, c11, c13, c33, wavelet, souloc, shotid, recloc, dc):
+    """Derivative of the EXACT traces along dc = (dc11, dc13, dc33) stacked."""
+    nrec = np.asarray(recloc).size // 4
+    return _exact3d("orc3d_exact_born", g, c11, c13, c33, wavelet, souloc, shotid, recloc,
+                    [dc], nnt3d(g) * nrec)
+
+
+def exact_adjoint3d(g, c11, c13, c33, wavelet, souloc, shotid, recloc, res):
+    """Transpose of exact_born3d applied to traces res: with res = modeled -
+    observed, the gradient (dJ/dc11, dJ/dc13, dJ/dc33 stacked) of
+    J = 1/2 |modeled - observed|^2."""
+    return _exact3d("orc3d_exact_adjoint", g, c11, c13, c33, wavelet, souloc, shotid, recloc,
+                    [res], 3 * g.nx * g.ny * g.nz)
+
+
 def damping3d(nx, ny, nz, npad):
     out = np.zeros(nx * ny + nz, dtype=np.float32)
     lib().orc3d_damping(nx, ny, nz, npad, _p(out))

@@ -1140,6 +1140,183 @@ double grad2d(const Geo2& g, const float* c11, const float* c13, const float* c3
 
 }  // namespace
 
+// ------------------------------------------------- EXACT adjoint mode ------
+// Self-check operators. The reference's 3D gradient is not the derivative of
+// its own misfit: it propagates the adjoint with the forward operator C.L
+// (objFuncGradient3d_f.cu:1002-1010) rather than its transpose L.C (the form
+// of adjointCij, laplacian3d.ispc:166-190), rebuilds the source field through
+// a random boundary and injects time-interpolated residuals
+// (injectRecord3d.cu:60-78). EXACT mode fixes one discrete forward operator
+// and differentiates it exactly, so a dot-product test and centred finite
+// differences can check the adjoint-state machinery itself:
+//   a_0 = 0, a_1 = dt2 w[0] e_s,
+//   a_t = P D [ (2 + C L) a_{t-1} - D a_{t-2} + dt2 w[t-1] e_s ],  t = 2..M
+// with P the x/y update region, D the sponge profile (abc3d.cu:23-50) as a
+// plain diagonal, C L the forward-form VTI operator of step3d; traces
+// d_j = 2/3 a_x + 1/3 a_z at each receiver's own cell and level j*st;
+// J = 1/2 sum over live receivers of (d - dobs)^2. Its adjoint:
+//   mu_t = P D [ R^T r_t + 2 mu_{t+1} + (C L)^T mu_{t+1} - D mu_{t+2} ],
+//   (C L)^T mu = ( L_xy(c11 mu_x + c13 mu_z), L_z(c13 mu_x + c33 mu_z) ),
+//   dJ/dc11 = sum_t mu_t,x L_xy a_{t-1,x},  dJ/dc33 = sum_t mu_t,z L_z a_{t-1,z},
+//   dJ/dc13 = sum_t mu_t,x L_z a_{t-1,z} + mu_t,z L_xy a_{t-1,x}.
+// The Born operator (dJ/dc applied to a model perturbation) is the
+// linearisation of the same recursion: source term dC L a_{t-1}.
+
+// lxy <- L_xy ux, lz <- L_z uz (forward-form scaling dt2/dx2 as step3d) on
+// the update region, zero elsewhere; z reads outside [0,nz) are zero.
+template <typename T>
+void lap3d(const Geo3& g, const T* ux, const T* uz, T* lxy, T* lz) {
+  const long nx = g.nx, ny = g.ny, nz = g.nz, nxy = g.nxy();
+  const float dt2 = g.dt * g.dt;
+  const float sx = dt2 / (g.dx * g.dx), sy = dt2 / (g.dy * g.dy), sz = dt2 / (g.dz * g.dz);
+  const T C[5] = {(T)k3C0, (T)k3C1, (T)k3C2, (T)k3C3, (T)k3C4};
+  std::fill(lxy, lxy + g.nxyz(), (T)0);
+  std::fill(lz, lz + g.nxyz(), (T)0);
+#pragma omp parallel for collapse(2) schedule(static)
+  for (long iz = 0; iz < nz; ++iz)
+    for (long iy = kHalf; iy < ny - kHalf; ++iy)
+      for (long ix = kHalf; ix < nx - kHalf; ++ix) {
+        const long i = ix + iy * nx + iz * nxy;
+        T lxx = C[0] * ux[i], lyy = C[0] * ux[i], lzz = C[0] * uz[i];
+        for (int k = 1; k <= 4; ++k) {
+          lxx += C[k] * (ux[i - k] + ux[i + k]);
+          lyy += C[k] * (ux[i - k * nx] + ux[i + k * nx]);
+          lzz += C[k] * ((iz - k >= 0 ? uz[i - k * nxy] : (T)0) +
+                         (iz + k < nz ? uz[i + k * nxy] : (T)0));
+        }
+        lxy[i] = lxx * (T)sx + lyy * (T)sy;
+        lz[i] = lzz * (T)sz;
+      }
+}
+
+struct ExactShot {
+  long sidx;
+  std::vector<long> ridx;
+  std::vector<char> live;
+  int irbegin, nr;
+};
+
+ExactShot exact_shot(const Geo3& g, const float* souloc, const float* recloc, int is) {
+  Shot3 s = make_shot3(g, souloc, recloc, is);
+  return ExactShot{s.sidx, s.seed, s.live, s.irbegin, s.nr};
+}
+
+// Level recorded into sample j (0: none).
+inline int exact_level(int j, int st, int M) { return j >= 1 && j * st <= M ? j * st : 0; }
+
+template <typename T>
+struct ExactHistory {
+  std::vector<std::vector<T>> a;  // level t: x then z components (2n)
+};
+
+// Forward recursion; a.a[t] for t = 0..M. dc != nullptr: the Born field of
+// the perturbation (dc11,dc13,dc33) around the background history `bg`.
+template <typename T>
+void exact_forward3d(const Geo3& g, const T* c11, const T* c13, const T* c33,
+                     const float* wavelet, const ExactShot& s, const Damp3& damp,
+                     ExactHistory<T>& h, const ExactHistory<T>* bg = nullptr,
+                     const T* dc = nullptr) {
+  const long n = g.nxyz(), nxy = g.nxy();
+  const int M = last_level(g);
+  const float dt2 = g.dt * g.dt;
+  h.a.assign(M + 1, std::vector<T>(2 * n, (T)0));
+  if (!dc) {
+    h.a[1][s.sidx] = (T)(dt2 * wavelet[0]);
+    h.a[1][n + s.sidx] = (T)(dt2 * wavelet[0]);
+  }
+  std::vector<T> lxy(n), lz(n), bxy(n), bz(n);
+  for (int t = 2; t <= M; ++t) {
+    const T* u1 = h.a[t - 1].data();
+    const T* u2 = h.a[t - 2].data();
+    T* u = h.a[t].data();
+    lap3d<T>(g, u1, u1 + n, lxy.data(), lz.data());
+    if (dc) lap3d<T>(g, bg->a[t - 1].data(), bg->a[t - 1].data() + n, bxy.data(), bz.data());
+#pragma omp parallel for collapse(2) schedule(static)
+    for (long iz = 0; iz < g.nz; ++iz)
+      for (long iy = kHalf; iy < g.ny - kHalf; ++iy)
+        for (long ix = kHalf; ix < g.nx - kHalf; ++ix) {
+          const long ixy = ix + iy * g.nx, i = ixy + iz * nxy;
+          const T d = (T)damp.at(ixy, (int)iz);
+          T vx = c11[i] * lxy[i] + c13[i] * lz[i] + 2 * u1[i] - d * u2[i];
+          T vz = c13[i] * lxy[i] + c33[i] * lz[i] + 2 * u1[n + i] - d * u2[n + i];
+          if (dc) {
+            vx += dc[i] * bxy[i] + dc[n + i] * bz[i];
+            vz += dc[n + i] * bxy[i] + dc[2 * n + i] * bz[i];
+          }
+          u[i] = d * vx;
+          u[n + i] = d * vz;
+        }
+    if (!dc) {
+      const T d = (T)damp.at(s.sidx % nxy, (int)(s.sidx / nxy));
+      u[s.sidx] += d * (T)(dt2 * wavelet[t - 1]);
+      u[n + s.sidx] += d * (T)(dt2 * wavelet[t - 1]);
+    }
+  }
+}
+
+template <typename T>
+void exact_record3d(const Geo3& g, const ExactShot& s, const ExactHistory<T>& h, T* trace) {
+  const long n = g.nxyz();
+  const int st = sampling_step(g.rate, g.dt), nnt = (g.nt - 1) / st + 1, M = last_level(g);
+  std::fill(trace, trace + (long)nnt * s.nr, (T)0);
+  for (int j = 1; j < nnt; ++j) {
+    const int t = exact_level(j, st, M);
+    if (!t) continue;
+    for (int ir = 0; ir < s.nr; ++ir)
+      if (s.live[ir])
+        trace[j + (long)ir * nnt] = (T)kTwoThird * h.a[t][s.ridx[ir]] +
+                                    (T)kOneThird * h.a[t][n + s.ridx[ir]];
+  }
+}
+
+// Adds the adjoint-state gradient of sum_j <res_j, d_j> to grad (3n).
+template <typename T>
+void exact_adjoint3d(const Geo3& g, const T* c11, const T* c13, const T* c33,
+                     const ExactShot& s, const Damp3& damp, const ExactHistory<T>& h,
+                     const T* res, T* grad) {
+  const long n = g.nxyz(), nxy = g.nxy();
+  const int st = sampling_step(g.rate, g.dt), nnt = (g.nt - 1) / st + 1, M = last_level(g);
+  std::vector<T> mu1(2 * n, 0), mu2(2 * n, 0), mu(2 * n, 0), w(2 * n, 0);
+  std::vector<T> lxy(n), lz(n), axy(n), az(n);
+  std::vector<T> src(2 * n, 0);
+  for (int t = M; t >= 2; --t) {
+    // w = C mu_{t+1}; (lxy, lz) = (L_xy w_x, L_z w_z)
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < n; ++i) {
+      w[i] = c11[i] * mu1[i] + c13[i] * mu1[n + i];
+      w[n + i] = c13[i] * mu1[i] + c33[i] * mu1[n + i];
+    }
+    lap3d<T>(g, w.data(), w.data() + n, lxy.data(), lz.data());
+    std::fill(src.begin(), src.end(), (T)0);
+    if (t % st == 0 && t / st < nnt && exact_level(t / st, st, M) == t)
+      for (int ir = 0; ir < s.nr; ++ir)
+        if (s.live[ir]) {
+          const T r = res[t / st + (long)ir * nnt];
+          src[s.ridx[ir]] += (T)kTwoThird * r;
+          src[n + s.ridx[ir]] += (T)kOneThird * r;
+        }
+#pragma omp parallel for collapse(2) schedule(static)
+    for (long iz = 0; iz < g.nz; ++iz)
+      for (long iy = kHalf; iy < g.ny - kHalf; ++iy)
+        for (long ix = kHalf; ix < g.nx - kHalf; ++ix) {
+          const long ixy = ix + iy * g.nx, i = ixy + iz * nxy;
+          const T d = (T)damp.at(ixy, (int)iz);
+          mu[i] = d * (src[i] + 2 * mu1[i] + lxy[i] - d * mu2[i]);
+          mu[n + i] = d * (src[n + i] + 2 * mu1[n + i] + lz[i] - d * mu2[n + i]);
+        }
+    const T* a1 = h.a[t - 1].data();
+    lap3d<T>(g, a1, a1 + n, axy.data(), az.data());
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < n; ++i) {
+      grad[i] += mu[i] * axy[i];
+      grad[n + i] += mu[i] * az[i] + mu[n + i] * axy[i];
+      grad[2 * n + i] += mu[n + i] * az[i];
+    }
+    std::swap(mu2, mu1);
+    std::swap(mu1, mu);
+  }
+}
+
 extern "C" {
 
 // Damping tables of abc3d.cu:23-50 (nx*ny then nz floats).
@@ -1210,6 +1387,59 @@ ORC3D_RTM(float, f32)
   }
 ORC3D_WGRAD(double, f64)
 ORC3D_WGRAD(float, f32)
+
+// EXACT mode (self-checks, FP64). Traces of the EXACT forward operator.
+int orc3d_exact_forward(const int* ip, const float* fp, const double* c11, const double* c13,
+                        const double* c33, const float* wavelet, const float* souloc,
+                        const int* shotid, int nshot, const float* recloc, double* ddata) {
+  Geo3 g = unpack3(ip, fp);
+  Damp3 damp(g);
+  const int nnt = (g.nt - 1) / sampling_step(g.rate, g.dt) + 1;
+  ExactHistory<double> h;
+  for (int k = 0; k < nshot; ++k) {
+    ExactShot s = exact_shot(g, souloc, recloc, shotid[k]);
+    exact_forward3d<double>(g, c11, c13, c33, wavelet, s, damp, h);
+    exact_record3d<double>(g, s, h, ddata + (long)nnt * s.irbegin);
+  }
+  return 0;
+}
+
+// Born traces: the derivative of the EXACT traces along dc (3n: dc11,dc13,dc33).
+int orc3d_exact_born(const int* ip, const float* fp, const double* c11, const double* c13,
+                     const double* c33, const float* wavelet, const float* souloc,
+                     const int* shotid, int nshot, const float* recloc, const double* dc,
+                     double* ddata) {
+  Geo3 g = unpack3(ip, fp);
+  Damp3 damp(g);
+  const int nnt = (g.nt - 1) / sampling_step(g.rate, g.dt) + 1;
+  ExactHistory<double> bg, h;
+  for (int k = 0; k < nshot; ++k) {
+    ExactShot s = exact_shot(g, souloc, recloc, shotid[k]);
+    exact_forward3d<double>(g, c11, c13, c33, wavelet, s, damp, bg);
+    exact_forward3d<double>(g, c11, c13, c33, wavelet, s, damp, h, &bg, dc);
+    exact_record3d<double>(g, s, h, ddata + (long)nnt * s.irbegin);
+  }
+  return 0;
+}
+
+// Adjoint of the Born operator applied to traces `res` (grad: 3n, overwritten).
+// With res = modeled - observed it is the gradient of the EXACT misfit.
+int orc3d_exact_adjoint(const int* ip, const float* fp, const double* c11, const double* c13,
+                        const double* c33, const float* wavelet, const float* souloc,
+                        const int* shotid, int nshot, const float* recloc, const double* res,
+                        double* grad) {
+  Geo3 g = unpack3(ip, fp);
+  Damp3 damp(g);
+  const int nnt = (g.nt - 1) / sampling_step(g.rate, g.dt) + 1;
+  std::fill(grad, grad + 3 * g.nxyz(), 0.0);
+  ExactHistory<double> h;
+  for (int k = 0; k < nshot; ++k) {
+    ExactShot s = exact_shot(g, souloc, recloc, shotid[k]);
+    exact_forward3d<double>(g, c11, c13, c33, wavelet, s, damp, h);
+    exact_adjoint3d<double>(g, c11, c13, c33, s, damp, h, res + (long)nnt * s.irbegin, grad);
+  }
+  return 0;
+}
 
 // Time `nsteps` forward steps (forward form, sponge) of a zero-initialised
 // grid with a point source: the FP32 instance is the CPU baseline's unit of
