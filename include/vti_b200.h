@@ -63,6 +63,7 @@ typedef enum {
 
 typedef struct vti_ctx vti_ctx;
 typedef struct vti3d_plan vti3d_plan;
+typedef struct vti3d_batch vti3d_batch;
 
 typedef struct {
   int nx, ny, nz; /* grid including the absorbing pad; x fastest */
@@ -268,6 +269,45 @@ int vti2d_wavelet_gradient(vti_ctx* ctx, const vti2d_geom* g, float* gwavelet, c
                            const int* sloc, int ns, const int* rloc, int nr, const float* taper);
 /* 2D taper of lib/vti-fwi-2d/init.cpp:70-89 ((nx+2npad)*(nz+2npad) floats). */
 void vti2d_init_taper(float* taper, int nx, int nz, int npad);
+
+/* ------------------------------------------------- 3D batched multi-shot */
+/* A window of the model for one shot: cells [x0, x0+nx) x [y0, y0+ny) and the
+ * full z range; the window's outer npad cells are its sponge and random
+ * boundary. */
+typedef struct {
+  int x0, y0, nx, ny;
+} vti3d_window;
+/* Many shots, each on its own window, advanced together: one forward launch
+ * per time step for passes 1 and 2 of every shot, one backward launch per
+ * step for pass 3 (reference mode of vti3d_plan_gradient per shot). g is the
+ * full model grid. */
+int vti3d_batch_create(vti_ctx* ctx, const vti3d_geom* g, unsigned flags, vti3d_batch** out);
+int vti3d_batch_destroy(vti3d_batch* b);
+/* Full model c11, c13, c33 (nxyz each); kept on the device. */
+int vti3d_batch_set_model(vti3d_batch* b, const float* c11, const float* c13, const float* c33,
+                          int mem);
+int vti3d_batch_set_wavelet(vti3d_batch* b, const float* wavelet, int mem);
+/* Receiver list as vti3d_plan_set_receivers (x, y, z, flag per receiver). */
+int vti3d_batch_set_receivers(vti3d_batch* b, const float* recloc, int nrec_total);
+/* Shots: souloc 5 floats per shot (x, y, z, nrec, first receiver) in model
+ * coordinates, win one window per shot, seed of the random boundaries
+ * (generated on the device per shot). Allocates every shot's state. */
+int vti3d_batch_set_shots(vti3d_batch* b, int nshot, const float* souloc,
+                          const vti3d_window* win, unsigned seed);
+/* use_graph != 0: the time loops are captured once as CUDA graphs and
+ * replayed. seg_fwd/seg_bwd: z planes per work item (0: default schedule). */
+int vti3d_batch_set_options(vti3d_batch* b, int use_graph, int seg_fwd, int seg_bwd);
+/* Times candidate segment lengths on the current shots and keeps the fastest. */
+int vti3d_batch_autotune(vti3d_batch* b, int* seg_fwd, int* seg_bwd);
+/* Gradient of all shots: dobs as vti3d_plan_gradient (trace-major, global
+ * receiver order); fgcij = [misfit/2, gc11, gc13, gc33] over the full model,
+ * each window's gradient added without its npad x/y frame (unless that frame
+ * is the model's edge). */
+int vti3d_batch_gradient(vti3d_batch* b, const float* dobs, int dobs_mem, float* fgcij,
+                         int fgcij_mem, double* misfit);
+/* Window models of shot k (pad-boundary and random-boundary, 3 * nx*ny*nz
+ * each, host; either may be NULL). */
+int vti3d_batch_get_shot_models(vti3d_batch* b, int k, float* cpad, float* crand);
 
 #ifdef __cplusplus
 }

@@ -156,6 +156,69 @@ int launch_bwd3d_tma(vti_ctx* ctx, const Dims3& d, const TileMaps& scx, const Ti
                      float* g33_ptr, const Damping& damp, float dt2, float idx2, float idy2,
                      float idz2, float sx, float sy, float sz, PointSource src, bool rtm);
 
+// One job of a batched forward launch (k_fwd3d_tma over the items of many
+// volumes). Step s = tick - t0 of the job uses parity p = s & 1:
+// cur = cx[p]/cz[p], prev in and next out = px[p]/pz[p]; the source gets
+// amp[s] (device array).
+struct FwdJobSpec {
+  Dims3 d;
+  const TileMaps* cx[2];
+  const TileMaps* cz[2];
+  const TileMaps* px[2];
+  const TileMaps* pz[2];
+  const TileMaps* c[3];
+  const float* cz_ptr[2];
+  float* px_ptr[2];
+  float* pz_ptr[2];
+  const Damping* damp;  // null: no sponge
+  float sx, sy, sz;
+  int src_x, src_y, src_z;
+  const float* amp;
+  int t0;
+  int seg;  // planes per z-segment; 0: the single-launch schedule
+};
+// One job of a batched backward launch (roles as launch_bwd3d_tma, by parity).
+struct BwdJobSpec {
+  Dims3 d;
+  const TileMaps* scx[2];
+  const TileMaps* scz[2];
+  const TileMaps* spx[2];
+  const TileMaps* spz[2];
+  const TileMaps* lcx[2];
+  const TileMaps* lcz[2];
+  const TileMaps* lpx[2];
+  const TileMaps* lpz[2];
+  const TileMaps* c[3];
+  const TileMaps* g[3];
+  const float* scz_ptr[2];
+  const float* lcz_ptr[2];
+  float* spx_ptr[2];
+  float* spz_ptr[2];
+  float* lpx_ptr[2];
+  float* lpz_ptr[2];
+  float* g_ptr[3];
+  Damping damp;
+  float dt2, idx2, idy2, idz2, sx, sy, sz;
+  int src_x, src_y, src_z;
+  const float* amp;
+  int t0;
+  int seg;
+};
+// Descriptor sizes (64-byte aligned) and builders: write the descriptor into
+// host memory dst and return the job's item count.
+size_t fwd_job_bytes();
+size_t bwd_job_bytes();
+int build_fwd_job(vti_ctx* ctx, const FwdJobSpec& spec, void* dst, int* items);
+int build_bwd_job(vti_ctx* ctx, const BwdJobSpec& spec, void* dst, int* items);
+// One launch over the items of njobs device descriptors; base: njobs+1
+// prefix sums of their item counts (device).
+// Sets the batched kernels' launch attributes (before any stream capture).
+int prepare_batch_kernels(vti_ctx* ctx);
+int launch_fwd3d_batch(vti_ctx* ctx, const void* d_jobs, const int* d_base, int njobs, int items,
+                       int tick);
+int launch_bwd3d_batch(vti_ctx* ctx, const void* d_jobs, const int* d_base, int njobs, int items,
+                       int tick);
+
 // Reads (and clears) the device status word; VTI_ERR_TIMEOUT if a bounded
 // device-side wait gave up since the last check.
 int check_device_status(vti_ctx* ctx);

@@ -16,59 +16,13 @@
 #include <cmath>
 #include <cstring>
 
-#include "vti_internal.h"
+#include "vti_plan3d.h"
 
 using namespace vti;
+using namespace vti::p3d;
 
-struct vti3d_plan {
-  vti_ctx* ctx = nullptr;
-  vti3d_geom g{};
-  unsigned flags = 0;
-  Dims3 d{};
-  Vol cpad[3], crand[3];
-  bool have_rand = false;
-  Vol sx[2], sz[2], lx[2], lz[2];
-  Vol g11, g13, g33;
-  // TMA descriptors of every volume
-  TileMaps m_sx[2], m_sz[2], m_lx[2], m_lz[2], m_cpad[3], m_crand[3], m_g[3];
-  float* dampx = nullptr;  // nx + ny + nz floats, one allocation
-  float* dampy = nullptr;
-  float* dampz = nullptr;
-  std::vector<float> h_damp;  // host copy: x | y | z
-  std::vector<float> wavelet;
-  std::vector<float> recloc;
-  int nrec_total = 0;
-  // per-shot device scratch
-  long long* d_rec = nullptr;
-  float* d_rec_damp = nullptr;
-  unsigned char* d_live = nullptr;
-  size_t rec_cap = 0;
-  float* d_trace = nullptr;
-  size_t trace_cap = 0;
-  float* d_obs = nullptr;
-  size_t obs_cap = 0;
-  float* d_blist = nullptr;
-  size_t blist_cap = 0;
-  double* d_acc = nullptr;
-  float* d_gw = nullptr;  // wavelet gradient accumulator (nt)
-  size_t gw_cap = 0;
-  double* d_part = nullptr;  // per-trace AGC misfits
-  size_t part_cap = 0;
-  // misfit options of the gradient (objFuncGradient3d_f.cu:743-775)
-  float tpow = 0.f;
-  int objtype = 0;
-  int halfwidth = 20;
-  int last_cur = 0;  // index into sx[] of the last forward level
-  bool have_model = false;
-};
-
-namespace {
-
-#define VTI_TRY(x)                 \
-  do {                             \
-    int st_ = (x);                 \
-    if (st_ != VTI_OK) return st_; \
-  } while (0)
+namespace vti {
+namespace p3d {
 
 int sampling_step(const vti3d_geom& g) { return (int)std::round(g.sampling_rate / g.dt); }
 int nnt_of(const vti3d_geom& g) { return (g.nt - 1) / sampling_step(g) + 1; }
@@ -143,27 +97,6 @@ float damp_profile(int i, int n, int npad) {
   else dist = 0.f;
   return (float)(0.95 + (1. - 0.95) * std::cos(3.14159265359 * dist / npad));
 }
-
-template <typename T>
-int ensure(vti_ctx* ctx, T** ptr, size_t* cap, size_t n) {
-  if (*ptr && *cap >= n) return VTI_OK;
-  if (*ptr) cudaFree(*ptr);
-  *ptr = nullptr;
-  *cap = 0;
-  VTI_CUDA(ctx, cudaMalloc((void**)ptr, std::max<size_t>(n, 1) * sizeof(T)));
-  *cap = n;
-  return VTI_OK;
-}
-
-struct ShotGeom {
-  int sx, sy, sz;
-  int nr, irbegin;
-  std::vector<long long> rec;   // recording / residual-injection points
-  std::vector<long long> seed;  // adjoint seeding points
-  std::vector<float> rec_damp;  // sponge factor at rec (0: frame cell, skipped)
-  std::vector<unsigned char> live;
-  std::vector<int> rec_at;      // level -> trace sample (-1: not recorded)
-};
 
 // Index arithmetic of objFuncGradient3d_f.cu:551-575 (float, truncation).
 // In reference mode the receivers are read and injected inside the 4-plane
@@ -453,7 +386,8 @@ int run_gradient(vti3d_plan* p, const float* souloc, const int* shotid, int nsho
   return VTI_OK;
 }
 
-}  // namespace
+}  // namespace p3d
+}  // namespace vti
 
 extern "C" {
 

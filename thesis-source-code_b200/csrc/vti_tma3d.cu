@@ -27,6 +27,7 @@
 // the reference is lib/vti-fwi-3d/gpu/kernel3d.cu:3-74,222-298 and
 // abc3d.cu:82-126.
 #include <algorithm>
+#include <new>
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -34,6 +35,13 @@
 #include "vti_internal.h"
 
 namespace vti {
+
+#define VTI_TRY_ST(x)              \
+  do {                             \
+    int st_ = (x);                 \
+    if (st_ != VTI_OK) return st_; \
+  } while (0)
+
 namespace {
 
 constexpr float kC0 = -2.84722222222f, kC1 = 1.6f, kC2 = -0.2f, kC3 = 0.02539682539f,
@@ -45,6 +53,9 @@ constexpr int HX = TX + 2 * kHalo, HY = TY + 2 * kHalo;
 constexpr int PLAIN_BYTES = TX * TY * 4;  // 2048
 constexpr int HALO_BYTES = HX * HY * 4;   // 3840
 constexpr unsigned kSpinLimit = 1u << 26;
+// one 256-byte slot per consumer warp for the batched consumers' copy of the
+// job arguments
+constexpr int ARG_SLOT = 256;
 
 __device__ __forceinline__ float lap9(float c, float m1, float p1, float m2, float p2, float m3,
                                       float p3, float m4, float p4) {
@@ -120,6 +131,23 @@ __device__ __forceinline__ void item(const Sched& s, int i, int& bx, int& by, in
   z1 = min(s.nz, z0 + s.seg);
 }
 
+// Batched consumers: each warp copies its item's job arguments (global
+// memory) into its own shared-memory slot, so the item body reads them like
+// kernel parameters, without registers and without aliasing the output
+// stores. Only warp-level synchronisation: the lanes of a warp finish reading
+// the slot (previous item) before it is rewritten.
+template <typename Args>
+__device__ __forceinline__ const Args* stage_args(const Args& src, unsigned char* slot,
+                                                  int lane) {
+  static_assert(sizeof(Args) <= ARG_SLOT && sizeof(Args) % 4 == 0, "argument slot");
+  constexpr int kWords = (int)(sizeof(Args) / 4);
+  __syncwarp();
+  for (int t = lane; t < kWords; t += 32)
+    reinterpret_cast<uint32_t*>(slot)[t] = __ldg(reinterpret_cast<const uint32_t*>(&src) + t);
+  __syncwarp();
+  return reinterpret_cast<const Args*>(slot);
+}
+
 // ------------------------------------------------------------ forward
 struct FwdArgs {
   Dims3 d;
@@ -144,17 +172,212 @@ constexpr int F_OFF_PX = F_OFF_Z + PLAIN_BYTES;
 constexpr int F_OFF_PZ = F_OFF_PX + PLAIN_BYTES;
 constexpr int F_OFF_C = F_OFF_PZ + PLAIN_BYTES;
 constexpr int F_STAGE_BYTES = F_OFF_C + 3 * PLAIN_BYTES;  // 15872
-constexpr int F_SMEM = F_STAGES * F_STAGE_BYTES + 1024 + 2 * F_STAGES * 8;
+constexpr int F_SMEM = F_STAGES * F_STAGE_BYTES + 1024 + 2 * F_STAGES * 8 + NCW * ARG_SLOT;
+
+struct FwdMaps {
+  CUtensorMap cx, cz, px, pz, c11, c13, c33;
+};
+
+// A batched launch: items of job j are [base[j], base[j+1]); job j advances
+// its own step tick - t0, whose parity selects the buffer roles.
+struct JobTable {
+  const unsigned char* jobs;  // njobs descriptors of `stride` bytes
+  const int* base;            // njobs + 1 prefix sums of the jobs' items
+  int njobs, items, tick;
+};
+
+__device__ __forceinline__ int find_job(const JobTable& t, int item) {
+  int lo = 0, hi = t.njobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(t.base + mid) <= item) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+struct alignas(64) FwdJob {
+  FwdMaps m[2];  // by step parity
+  FwdArgs a[2];
+  const float* amp;  // source amplitude per step
+  int t0;
+};
+
+// Producer side of one item: TMA loads of every plane of the item's range.
+__device__ __forceinline__ bool fwd_produce(const FwdArgs& a, const FwdMaps& m, int li,
+                                            unsigned char* smem, uint64_t* full, uint64_t* empty,
+                                            long long& k) {
+  int bx, by, z0, z1;
+  item(a.sc, li, bx, by, z0, z1);
+  const int x0 = bx * TX, y0 = kHalo + by * TY;
+  for (int z = z0; z < z1; ++z, ++k) {
+    const int s = (int)(k % F_STAGES);
+    if (k >= F_STAGES && !mbar_wait(&empty[s], (uint32_t)(((k / F_STAGES) & 1) ^ 1), a.status))
+      return false;
+    const int zp = z + kZPad;
+    unsigned char* st = smem + s * F_STAGE_BYTES;
+    mbar_arrive_expect_tx(&full[s], F_STAGE_BYTES);
+    tma_load(st + F_OFF_H, &m.cx, &full[s], x0 - kHalo, y0 - kHalo, zp);
+    tma_load(st + F_OFF_Z, &m.cz, &full[s], x0, y0, zp + kHalo);
+    tma_load(st + F_OFF_PX, &m.px, &full[s], x0, y0, zp);
+    tma_load(st + F_OFF_PZ, &m.pz, &full[s], x0, y0, zp);
+    tma_load(st + F_OFF_C, &m.c11, &full[s], x0, y0, zp);
+    tma_load(st + F_OFF_C + PLAIN_BYTES, &m.c13, &full[s], x0, y0, zp);
+    tma_load(st + F_OFF_C + 2 * PLAIN_BYTES, &m.c33, &full[s], x0, y0, zp);
+  }
+  return true;
+}
+
+// Consumer side of one item. Thread (lane, warp) owns the x pair
+// x0 + 2*(lane%16) + {0,1} of tile row 2*warp + lane/16; shared-memory reads
+// and global stores are float2.
+template <bool kProbe>
+__device__ __forceinline__ bool fwd_consume(const FwdArgs& a, int li, float amp,
+                                            const unsigned char* smem, uint64_t* full,
+                                            uint64_t* empty, long long& k, int warp, int lane) {
+  const bool damp = a.dampz != nullptr;
+  const int ry = warp * 2 + (lane >> 4);
+  const int xo = 2 * (lane & 15);
+  const int sr = (ry + kHalo) * HX + xo + kHalo;  // centre in the halo tile
+  const int pi = ry * TX + xo;                    // centre in a plain tile
+  float q[2][9];
+  float dxy[2];
+  int bx, by, z0, z1;
+  item(a.sc, li, bx, by, z0, z1);
+  const int x = bx * TX + xo;
+  const int y = kHalo + by * TY + ry;
+  const bool vy = y < a.d.ny - kHalo;
+  const bool v0 = vy && x >= kHalo && x < a.d.nx - kHalo;
+  const bool v1 = vy && x + 1 >= kHalo && x + 1 < a.d.nx - kHalo;
+  const int off = y * a.d.pitch + x;  // x + 1 < pitch: 32 * gx <= pitch
+  // which of this thread's two points (0, 1; else -1) holds the source / probe
+  const int src_e = (y == a.src.y && a.src.x >= 0) ? a.src.x - x : -1;
+  const int prb_e = (kProbe && y == a.probe.y && a.probe.x >= 0) ? a.probe.x - x : -1;
+  dxy[0] = (damp && v0) ? a.dampx[x] * a.dampy[y] : 1.f;
+  dxy[1] = (damp && v1) ? a.dampx[x + 1] * a.dampy[y] : 1.f;
+  // start the queue: planes z0-4 .. z0+3 from global
+  q[0][0] = q[1][0] = 0.f;
+#pragma unroll
+  for (int kk = 1; kk < 9; ++kk) {
+    const int zz = z0 - 5 + kk;
+    float2 v = (v0 || v1)
+                   ? __ldg(reinterpret_cast<const float2*>(a.cz + (long long)zz * a.d.plane + off))
+                   : make_float2(0.f, 0.f);
+    // planes of the block above z0 were already damped as "cur"
+    if (damp && zz >= 0 && (zz >> 2) < (z0 >> 2)) {
+      v.x *= dxy[0] * a.dampz[zz];
+      v.y *= dxy[1] * a.dampz[zz];
+    }
+    q[0][kk] = v.x;
+    q[1][kk] = v.y;
+  }
+  // z damping factors in registers: dzr holds planes z-3..z once plane z
+  // is entered (the block transition rescales those four queue entries);
+  // the next plane's factor is fetched one plane ahead
+  float dzr[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) dzr[j] = (damp && z0 - 4 + j >= 0) ? a.dampz[z0 - 4 + j] : 1.f;
+  float dz_next = damp ? a.dampz[z0] : 1.f;
+  for (int z = z0; z < z1; ++z, ++k) {
+    const float dz = dz_next;
+    if (damp && z + 1 < z1) dz_next = a.dampz[z + 1];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) dzr[j] = dzr[j + 1];
+    dzr[3] = dz;
+    const int s = (int)(k % F_STAGES);
+    if (!mbar_wait(&full[s], (uint32_t)((k / F_STAGES) & 1), a.status)) return false;
+    const unsigned char* st = smem + s * F_STAGE_BYTES;
+    const float* sh = (const float*)(st + F_OFF_H) + sr;
+    const float* pl = (const float*)(st + F_OFF_Z) + pi;  // [z+4][prev x][prev z][c11][c13][c33]
+    constexpr int T = TX * TY;
+#pragma unroll
+    for (int kk = 0; kk < 8; ++kk) {
+      q[0][kk] = q[0][kk + 1];
+      q[1][kk] = q[1][kk + 1];
+    }
+    const float2 zq = ld2(pl);
+    q[0][8] = zq.x;
+    q[1][8] = zq.y;
+    // the row x-4 .. x+5 and the column pairs y +- 1..4
+    float r[10];
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+      const float2 t = ld2(sh - 4 + 2 * j);
+      r[2 * j] = t.x;
+      r[2 * j + 1] = t.y;
+    }
+    float2 ym[4], yp[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      ym[j] = ld2(sh - (j + 1) * HX);
+      yp[j] = ld2(sh + (j + 1) * HX);
+    }
+    const float2 px = ld2(pl + T), pz = ld2(pl + 2 * T);
+    const float2 c11 = ld2(pl + 3 * T), c13 = ld2(pl + 4 * T), c33 = ld2(pl + 5 * T);
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[s]);
+    float nxv[2], nzv[2];
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      auto pick = [e](float2 v) { return e ? v.y : v.x; };
+      const float c = r[4 + e];
+      const float lxx = lap9(c, r[3 + e], r[5 + e], r[2 + e], r[6 + e], r[1 + e], r[7 + e],
+                             r[e], r[8 + e]);
+      const float lyy = lap9(c, pick(ym[0]), pick(yp[0]), pick(ym[1]), pick(yp[1]),
+                             pick(ym[2]), pick(yp[2]), pick(ym[3]), pick(yp[3]));
+      const float lzz = lap9(q[e][4], q[e][3], q[e][5], q[e][2], q[e][6], q[e][1], q[e][7],
+                             q[e][0], q[e][8]);
+      const float lxy = fmaf(lyy, a.sy, lxx * a.sx);
+      const float lz = lzz * a.sz;
+      const float dd = dxy[e] * dz;
+      const float a11 = pick(c11), a13 = pick(c13), a33 = pick(c33);
+      nxv[e] = fmaf(a11, lxy, fmaf(a13, lz, 2.f * c - dd * pick(px)));
+      nzv[e] = fmaf(a13, lxy, fmaf(a33, lz, 2.f * q[e][4] - dd * pick(pz)));
+      if (kProbe && prb_e == e && z == a.probe.z) *a.probe.out += nxv[e] + nzv[e];
+      if (src_e == e && z == a.src.z) {
+        nxv[e] += amp;
+        nzv[e] += amp;
+      }
+      nxv[e] *= dd;
+      nzv[e] *= dd;
+    }
+    const long long i = (long long)z * a.d.plane + off;
+    if (v0 && v1) {
+      *reinterpret_cast<float2*>(a.px + i) = make_float2(nxv[0], nxv[1]);
+      *reinterpret_cast<float2*>(a.pz + i) = make_float2(nzv[0], nzv[1]);
+    } else {
+      if (v0) {
+        a.px[i] = nxv[0];
+        a.pz[i] = nzv[0];
+      }
+      if (v1) {
+        a.px[i + 1] = nxv[1];
+        a.pz[i + 1] = nzv[1];
+      }
+    }
+    // entering the next plane: if it starts a new 4-plane block of the same
+    // column, the four planes of the block just finished become "damped cur"
+    if (damp && ((z + 1) & 3) == 0 && z + 1 < a.d.nz) {
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        // after the shift at z+1, entries 0..3 hold planes z-3..z; they are
+        // entries 1..4 now
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) q[e][kk + 1] *= dxy[e] * dzr[kk];
+      }
+    }
+  }
+  return true;
+}
 
 // kProbe: the probe point of FwdArgs is read out (wavelet gradient); the
-// propagation kernels are instantiated without it.
-template <bool kProbe>
+// propagation kernels are instantiated without it. kBatch: the items of all
+// jobs of `jt` (descriptors in global memory) instead of the single job
+// (m0, a0).
+template <bool kProbe, bool kBatch>
 __global__ void __launch_bounds__(NTHREADS, 3)
-    k_fwd3d_tma(const __grid_constant__ CUtensorMap m_cx, const __grid_constant__ CUtensorMap m_cz,
-                const __grid_constant__ CUtensorMap m_px, const __grid_constant__ CUtensorMap m_pz,
-                const __grid_constant__ CUtensorMap m_c11,
-                const __grid_constant__ CUtensorMap m_c13,
-                const __grid_constant__ CUtensorMap m_c33, const FwdArgs a) {
+    k_fwd3d_tma(const __grid_constant__ FwdMaps m0, const __grid_constant__ FwdArgs a0,
+                const JobTable jt) {
   extern __shared__ unsigned char smem_raw[];
   unsigned char* smem =
       (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -169,180 +392,39 @@ __global__ void __launch_bounds__(NTHREADS, 3)
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  const Dims3 d = a.d;
-
+  const int items = kBatch ? jt.items : a0.sc.items;
+  long long k = 0;  // planes issued / consumed by this CTA
   if (warp == NCW) {  // ---------------- producer
     if (lane == 0) {
-      long long k = 0;  // planes issued by this CTA
-      bool ok = true;
-      for (int it = blockIdx.x; ok && it < a.sc.items; it += gridDim.x) {
-        int bx, by, z0, z1;
-        item(a.sc, it, bx, by, z0, z1);
-        const int x0 = bx * TX, y0 = kHalo + by * TY;
-        for (int z = z0; z < z1; ++z, ++k) {
-          const int s = (int)(k % F_STAGES);
-          if (k >= F_STAGES &&
-              !mbar_wait(&empty[s], (uint32_t)(((k / F_STAGES) & 1) ^ 1), a.status)) {
-            ok = false;
-            break;
-          }
-          const int zp = z + kZPad;
-          unsigned char* st = smem + s * F_STAGE_BYTES;
-          mbar_arrive_expect_tx(&full[s], F_STAGE_BYTES);
-          tma_load(st + F_OFF_H, &m_cx, &full[s], x0 - kHalo, y0 - kHalo, zp);
-          tma_load(st + F_OFF_Z, &m_cz, &full[s], x0, y0, zp + kHalo);
-          tma_load(st + F_OFF_PX, &m_px, &full[s], x0, y0, zp);
-          tma_load(st + F_OFF_PZ, &m_pz, &full[s], x0, y0, zp);
-          tma_load(st + F_OFF_C, &m_c11, &full[s], x0, y0, zp);
-          tma_load(st + F_OFF_C + PLAIN_BYTES, &m_c13, &full[s], x0, y0, zp);
-          tma_load(st + F_OFF_C + 2 * PLAIN_BYTES, &m_c33, &full[s], x0, y0, zp);
+      for (int it = blockIdx.x; it < items; it += gridDim.x) {
+        bool ok;
+        if constexpr (kBatch) {
+          const int j = find_job(jt, it);
+          const FwdJob& J = reinterpret_cast<const FwdJob*>(jt.jobs)[j];
+          const int par = (jt.tick - J.t0) & 1;
+          ok = fwd_produce(J.a[par], J.m[par], it - jt.base[j], smem, full, empty, k);
+        } else {
+          ok = fwd_produce(a0, m0, it, smem, full, empty, k);
         }
+        if (!ok) break;
       }
     }
     return;
   }
-
-  // ---------------- consumers: thread (lane, warp) owns the x pair
-  // x0 + 2*(lane%16) + {0,1} of tile row 2*warp + lane/16; shared-memory reads
-  // and global stores are float2.
-  const bool damp = a.dampz != nullptr;
-  const int ry = warp * 2 + (lane >> 4);
-  const int xo = 2 * (lane & 15);
-  const int sr = (ry + kHalo) * HX + xo + kHalo;  // centre in the halo tile
-  const int pi = ry * TX + xo;                    // centre in a plain tile
-  float q[2][9];
-  float dxy[2];
-  long long k = 0;  // planes consumed by this CTA
-  bool ok = true;
-  for (int it = blockIdx.x; ok && it < a.sc.items; it += gridDim.x) {
-    int bx, by, z0, z1;
-    item(a.sc, it, bx, by, z0, z1);
-    const int x = bx * TX + xo;
-    const int y = kHalo + by * TY + ry;
-    const bool vy = y < d.ny - kHalo;
-    const bool v0 = vy && x >= kHalo && x < d.nx - kHalo;
-    const bool v1 = vy && x + 1 >= kHalo && x + 1 < d.nx - kHalo;
-    const int off = y * d.pitch + x;  // x + 1 < pitch: 32 * gx <= pitch
-    // which of this thread's two points (0, 1; else -1) holds the source / probe
-    const int src_e = (y == a.src.y && a.src.x >= 0) ? a.src.x - x : -1;
-    const int prb_e = (kProbe && y == a.probe.y && a.probe.x >= 0) ? a.probe.x - x : -1;
-    dxy[0] = (damp && v0) ? a.dampx[x] * a.dampy[y] : 1.f;
-    dxy[1] = (damp && v1) ? a.dampx[x + 1] * a.dampy[y] : 1.f;
-    // start the queue: planes z0-4 .. z0+3 from global
-    q[0][0] = q[1][0] = 0.f;
-#pragma unroll
-    for (int kk = 1; kk < 9; ++kk) {
-      const int zz = z0 - 5 + kk;
-      float2 v = (v0 || v1)
-                     ? __ldg(reinterpret_cast<const float2*>(a.cz + (long long)zz * d.plane + off))
-                     : make_float2(0.f, 0.f);
-      // planes of the block above z0 were already damped as "cur"
-      if (damp && zz >= 0 && (zz >> 2) < (z0 >> 2)) {
-        v.x *= dxy[0] * a.dampz[zz];
-        v.y *= dxy[1] * a.dampz[zz];
-      }
-      q[0][kk] = v.x;
-      q[1][kk] = v.y;
+  unsigned char* slot = (unsigned char*)(empty + F_STAGES) + warp * ARG_SLOT;
+  for (int it = blockIdx.x; it < items; it += gridDim.x) {
+    bool ok;
+    if constexpr (kBatch) {
+      const int j = find_job(jt, it);
+      const FwdJob& J = reinterpret_cast<const FwdJob*>(jt.jobs)[j];
+      const int step = jt.tick - J.t0;
+      const FwdArgs* a = stage_args(J.a[step & 1], slot, lane);
+      ok = fwd_consume<kProbe>(*a, it - jt.base[j], __ldg(J.amp + step), smem, full, empty, k,
+                               warp, lane);
+    } else {
+      ok = fwd_consume<kProbe>(a0, it, a0.src.amp, smem, full, empty, k, warp, lane);
     }
-    // z damping factors in registers: dzr holds planes z-3..z once plane z
-    // is entered (the block transition rescales those four queue entries);
-    // the next plane's factor is fetched one plane ahead
-    float dzr[4];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) dzr[j] = (damp && z0 - 4 + j >= 0) ? a.dampz[z0 - 4 + j] : 1.f;
-    float dz_next = damp ? a.dampz[z0] : 1.f;
-    for (int z = z0; z < z1; ++z, ++k) {
-      const float dz = dz_next;
-      if (damp && z + 1 < z1) dz_next = a.dampz[z + 1];
-#pragma unroll
-      for (int j = 0; j < 3; ++j) dzr[j] = dzr[j + 1];
-      dzr[3] = dz;
-      const int s = (int)(k % F_STAGES);
-      if (!mbar_wait(&full[s], (uint32_t)((k / F_STAGES) & 1), a.status)) {
-        ok = false;
-        break;
-      }
-      const unsigned char* st = smem + s * F_STAGE_BYTES;
-      const float* sh = (const float*)(st + F_OFF_H) + sr;
-      const float* pl = (const float*)(st + F_OFF_Z) + pi;  // [z+4][prev x][prev z][c11][c13][c33]
-      constexpr int T = TX * TY;
-#pragma unroll
-      for (int kk = 0; kk < 8; ++kk) {
-        q[0][kk] = q[0][kk + 1];
-        q[1][kk] = q[1][kk + 1];
-      }
-      const float2 zq = ld2(pl);
-      q[0][8] = zq.x;
-      q[1][8] = zq.y;
-      // the row x-4 .. x+5 and the column pairs y +- 1..4
-      float r[10];
-#pragma unroll
-      for (int j = 0; j < 5; ++j) {
-        const float2 t = ld2(sh - 4 + 2 * j);
-        r[2 * j] = t.x;
-        r[2 * j + 1] = t.y;
-      }
-      float2 ym[4], yp[4];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        ym[j] = ld2(sh - (j + 1) * HX);
-        yp[j] = ld2(sh + (j + 1) * HX);
-      }
-      const float2 px = ld2(pl + T), pz = ld2(pl + 2 * T);
-      const float2 c11 = ld2(pl + 3 * T), c13 = ld2(pl + 4 * T), c33 = ld2(pl + 5 * T);
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&empty[s]);
-      float nxv[2], nzv[2];
-#pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        auto pick = [e](float2 v) { return e ? v.y : v.x; };
-        const float c = r[4 + e];
-        const float lxx = lap9(c, r[3 + e], r[5 + e], r[2 + e], r[6 + e], r[1 + e], r[7 + e],
-                               r[e], r[8 + e]);
-        const float lyy = lap9(c, pick(ym[0]), pick(yp[0]), pick(ym[1]), pick(yp[1]),
-                               pick(ym[2]), pick(yp[2]), pick(ym[3]), pick(yp[3]));
-        const float lzz = lap9(q[e][4], q[e][3], q[e][5], q[e][2], q[e][6], q[e][1], q[e][7],
-                               q[e][0], q[e][8]);
-        const float lxy = fmaf(lyy, a.sy, lxx * a.sx);
-        const float lz = lzz * a.sz;
-        const float dd = dxy[e] * dz;
-        const float a11 = pick(c11), a13 = pick(c13), a33 = pick(c33);
-        nxv[e] = fmaf(a11, lxy, fmaf(a13, lz, 2.f * c - dd * pick(px)));
-        nzv[e] = fmaf(a13, lxy, fmaf(a33, lz, 2.f * q[e][4] - dd * pick(pz)));
-        if (kProbe && prb_e == e && z == a.probe.z) *a.probe.out += nxv[e] + nzv[e];
-        if (src_e == e && z == a.src.z) {
-          nxv[e] += a.src.amp;
-          nzv[e] += a.src.amp;
-        }
-        nxv[e] *= dd;
-        nzv[e] *= dd;
-      }
-      const long long i = (long long)z * d.plane + off;
-      if (v0 && v1) {
-        *reinterpret_cast<float2*>(a.px + i) = make_float2(nxv[0], nxv[1]);
-        *reinterpret_cast<float2*>(a.pz + i) = make_float2(nzv[0], nzv[1]);
-      } else {
-        if (v0) {
-          a.px[i] = nxv[0];
-          a.pz[i] = nzv[0];
-        }
-        if (v1) {
-          a.px[i + 1] = nxv[1];
-          a.pz[i + 1] = nzv[1];
-        }
-      }
-      // entering the next plane: if it starts a new 4-plane block of the same
-      // column, the four planes of the block just finished become "damped cur"
-      if (damp && ((z + 1) & 3) == 0 && z + 1 < d.nz) {
-#pragma unroll
-        for (int e = 0; e < 2; ++e) {
-          // after the shift at z+1, entries 0..3 hold planes z-3..z; they are
-          // entries 1..4 now
-#pragma unroll
-          for (int kk = 0; kk < 4; ++kk) q[e][kk + 1] *= dxy[e] * dzr[kk];
-        }
-      }
-    }
+    if (!ok) break;
   }
 }
 
@@ -374,7 +456,7 @@ constexpr int B_OFF_SH = 0;
 constexpr int B_OFF_LH = HALO_BYTES;
 constexpr int B_OFF_P = 2 * HALO_BYTES;  // 10 plain tiles from here
 constexpr int B_STAGE_BYTES = B_OFF_P + 12 * PLAIN_BYTES;  // 32256
-constexpr int B_SMEM = B_STAGES * B_STAGE_BYTES + 1024 + 2 * B_STAGES * 8;
+constexpr int B_SMEM = B_STAGES * B_STAGE_BYTES + 1024 + 2 * B_STAGES * 8 + NCW * ARG_SLOT;
 
 struct BwdMaps {
   CUtensorMap scx, scz, spx, spz, lcx, lcz, lpx, lpz, c11, c13, c33, g11, g13, g33;
@@ -383,14 +465,238 @@ struct BwdMaps {
 // wave3d.h:5-6 recording / imaging weights, as float
 constexpr float kTwoThirdF = (float)kTwoThird, kOneThirdF = (float)kOneThird;
 
+struct alignas(64) BwdJob {
+  BwdMaps m[2];  // by step parity
+  BwdArgs a[2];
+  const float* amp;  // source amplitude per step
+  int t0;
+};
+
+template <bool kRtm>
+__device__ __forceinline__ bool bwd_produce(const BwdArgs& a, const BwdMaps& m, int li,
+                                            unsigned char* smem, uint64_t* full, uint64_t* empty,
+                                            long long& k) {
+  int bx, by, z0, z1;
+  item(a.sc, li, bx, by, z0, z1);
+  const int x0 = bx * TX, y0 = kHalo + by * TY;
+  for (int z = z0; z < z1; ++z, ++k) {
+    const int s = (int)(k % B_STAGES);
+    if (k >= B_STAGES && !mbar_wait(&empty[s], (uint32_t)(((k / B_STAGES) & 1) ^ 1), a.status))
+      return false;
+    const int zp = z + kZPad;
+    unsigned char* st = smem + s * B_STAGE_BYTES;
+    unsigned char* pl = st + B_OFF_P;
+    mbar_arrive_expect_tx(&full[s], kRtm ? B_STAGE_BYTES - 2 * PLAIN_BYTES : B_STAGE_BYTES);
+    tma_load(st + B_OFF_SH, &m.scx, &full[s], x0 - kHalo, y0 - kHalo, zp);
+    tma_load(st + B_OFF_LH, &m.lcx, &full[s], x0 - kHalo, y0 - kHalo, zp);
+    tma_load(pl + 0 * PLAIN_BYTES, &m.scz, &full[s], x0, y0, zp + kHalo);
+    tma_load(pl + 1 * PLAIN_BYTES, &m.lcz, &full[s], x0, y0, zp + kHalo);
+    tma_load(pl + 2 * PLAIN_BYTES, &m.spx, &full[s], x0, y0, zp);
+    tma_load(pl + 3 * PLAIN_BYTES, &m.spz, &full[s], x0, y0, zp);
+    tma_load(pl + 4 * PLAIN_BYTES, &m.lpx, &full[s], x0, y0, zp);
+    tma_load(pl + 5 * PLAIN_BYTES, &m.lpz, &full[s], x0, y0, zp);
+    tma_load(pl + 6 * PLAIN_BYTES, &m.c11, &full[s], x0, y0, zp);
+    tma_load(pl + 7 * PLAIN_BYTES, &m.c13, &full[s], x0, y0, zp);
+    tma_load(pl + 8 * PLAIN_BYTES, &m.c33, &full[s], x0, y0, zp);
+    tma_load(pl + 9 * PLAIN_BYTES, &m.g11, &full[s], x0, y0, zp);
+    if (!kRtm) {
+      tma_load(pl + 10 * PLAIN_BYTES, &m.g13, &full[s], x0, y0, zp);
+      tma_load(pl + 11 * PLAIN_BYTES, &m.g33, &full[s], x0, y0, zp);
+    }
+  }
+  return true;
+}
+
+// Consumers: the x pair x0 + 2*(lane%16) + {0,1} of tile row 2*warp + lane/16.
+template <bool kRtm>
+__device__ __forceinline__ bool bwd_consume(const BwdArgs& a, int li, float amp,
+                                            const unsigned char* smem, uint64_t* full,
+                                            uint64_t* empty, long long& k, int warp, int lane) {
+  const int ry = warp * 2 + (lane >> 4);
+  const int xo = 2 * (lane & 15);
+  const int sr = (ry + kHalo) * HX + xo + kHalo;
+  const int pi = ry * TX + xo;
+  float sq[2][9], lq[2][9];
+  float dxy[2];
+  int bx, by, z0, z1;
+  item(a.sc, li, bx, by, z0, z1);
+  const int x = bx * TX + xo;
+  const int y = kHalo + by * TY + ry;
+  const bool vy = y < a.d.ny - kHalo;
+  const bool v0 = vy && x >= kHalo && x < a.d.nx - kHalo;
+  const bool v1 = vy && x + 1 >= kHalo && x + 1 < a.d.nx - kHalo;
+  const int off = y * a.d.pitch + x;  // x + 1 < pitch: 32 * gx <= pitch
+  dxy[0] = v0 ? a.dampx[x] * a.dampy[y] : 1.f;
+  dxy[1] = v1 ? a.dampx[x + 1] * a.dampy[y] : 1.f;
+  // start the queues: planes z0-4 .. z0+3 from global
+  sq[0][0] = sq[1][0] = lq[0][0] = lq[1][0] = 0.f;
+#pragma unroll
+  for (int kk = 1; kk < 9; ++kk) {
+    const int zz = z0 - 5 + kk;
+    const long long i = (long long)zz * a.d.plane + off;
+    const bool any = v0 || v1;
+    const float2 sv =
+        any ? __ldg(reinterpret_cast<const float2*>(a.scz + i)) : make_float2(0.f, 0.f);
+    float2 lv = any ? __ldg(reinterpret_cast<const float2*>(a.lcz + i)) : make_float2(0.f, 0.f);
+    if (zz >= 0 && (zz >> 2) < (z0 >> 2)) {
+      lv.x *= dxy[0] * a.dampz[zz];
+      lv.y *= dxy[1] * a.dampz[zz];
+    }
+    sq[0][kk] = sv.x;
+    sq[1][kk] = sv.y;
+    lq[0][kk] = lv.x;
+    lq[1][kk] = lv.y;
+  }
+  // z damping factors in registers (see the forward kernel)
+  float dzr[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) dzr[j] = z0 - 4 + j >= 0 ? a.dampz[z0 - 4 + j] : 1.f;
+  float dz_next = a.dampz[z0];
+  for (int z = z0; z < z1; ++z, ++k) {
+    const float dz = dz_next;
+    if (z + 1 < z1) dz_next = a.dampz[z + 1];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) dzr[j] = dzr[j + 1];
+    dzr[3] = dz;
+    const int s = (int)(k % B_STAGES);
+    if (!mbar_wait(&full[s], (uint32_t)((k / B_STAGES) & 1), a.status)) return false;
+    const unsigned char* st = smem + s * B_STAGE_BYTES;
+    const float* sh = (const float*)(st + B_OFF_SH) + sr;
+    const float* lh = (const float*)(st + B_OFF_LH) + sr;
+    const float* pl = (const float*)(st + B_OFF_P) + pi;
+    constexpr int T = TX * TY;
+#pragma unroll
+    for (int kk = 0; kk < 8; ++kk) {
+      sq[0][kk] = sq[0][kk + 1];
+      sq[1][kk] = sq[1][kk + 1];
+      lq[0][kk] = lq[0][kk + 1];
+      lq[1][kk] = lq[1][kk + 1];
+    }
+    {
+      const float2 s8 = ld2(pl), l8 = ld2(pl + T);
+      sq[0][8] = s8.x;
+      sq[1][8] = s8.y;
+      lq[0][8] = l8.x;
+      lq[1][8] = l8.y;
+    }
+    // x rows (x-4 .. x+5) and y column pairs of both halo fields
+    float rs[10], rl[10];
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+      const float2 t = ld2(sh - 4 + 2 * j), u = ld2(lh - 4 + 2 * j);
+      rs[2 * j] = t.x;
+      rs[2 * j + 1] = t.y;
+      rl[2 * j] = u.x;
+      rl[2 * j + 1] = u.y;
+    }
+    float2 sym[4], syp[4], lym[4], lyp[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      sym[j] = ld2(sh - (j + 1) * HX);
+      syp[j] = ld2(sh + (j + 1) * HX);
+      lym[j] = ld2(lh - (j + 1) * HX);
+      lyp[j] = ld2(lh + (j + 1) * HX);
+    }
+    const float2 spx = ld2(pl + 2 * T), spz = ld2(pl + 3 * T);
+    const float2 lpx = ld2(pl + 4 * T), lpz = ld2(pl + 5 * T);
+    const float2 c11 = ld2(pl + 6 * T), c13 = ld2(pl + 7 * T), c33 = ld2(pl + 8 * T);
+    const float2 g11o = ld2(pl + 9 * T);
+    const float2 g13o = kRtm ? make_float2(0.f, 0.f) : ld2(pl + 10 * T);
+    const float2 g33o = kRtm ? make_float2(0.f, 0.f) : ld2(pl + 11 * T);
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[s]);
+    float snx[2], snz[2], lnx[2], lnz[2], g11[2], g13[2], g33[2];
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      auto pick = [e](float2 v) { return e ? v.y : v.x; };
+      const float a11 = pick(c11), a13 = pick(c13), a33 = pick(c33);
+      // source wavefield back one level (gradient form)
+      const float sc = rs[4 + e];
+      const float sxx = lap9(sc, rs[3 + e], rs[5 + e], rs[2 + e], rs[6 + e], rs[1 + e],
+                             rs[7 + e], rs[e], rs[8 + e]);
+      const float syy = lap9(sc, pick(sym[0]), pick(syp[0]), pick(sym[1]), pick(syp[1]),
+                             pick(sym[2]), pick(syp[2]), pick(sym[3]), pick(syp[3]));
+      const float szz = lap9(sq[e][4], sq[e][3], sq[e][5], sq[e][2], sq[e][6], sq[e][1],
+                             sq[e][7], sq[e][0], sq[e][8]);
+      const float sxy_u = fmaf(syy, a.idy2, sxx * a.idx2);
+      const float sz_u = szz * a.idz2;
+      snx[e] = fmaf(a.dt2, fmaf(a11, sxy_u, a13 * sz_u), 2.f * sc - pick(spx));
+      snz[e] = fmaf(a.dt2, fmaf(a13, sxy_u, a33 * sz_u), 2.f * sq[e][4] - pick(spz));
+      if (x + e == a.src.x && y == a.src.y && z == a.src.z) {
+        snx[e] += amp;
+        snz[e] += amp;
+      }
+      // imaging with the current adjoint
+      const float lc = rl[4 + e];
+      const float lz0 = lq[e][4];
+      const float dd = dxy[e] * dz;
+      if (kRtm) {
+        g11[e] = fmaf(fmaf(kTwoThirdF, sc, kOneThirdF * sq[e][4]),
+                      dd * fmaf(kTwoThirdF, lc, kOneThirdF * lz0), pick(g11o));
+      } else {
+        g11[e] = fmaf(lc, sxy_u, pick(g11o));
+        g33[e] = fmaf(lz0, sz_u, pick(g33o));
+        g13[e] = fmaf(lz0, sxy_u, fmaf(lc, sz_u, pick(g13o)));
+      }
+      // adjoint, forward form with the sponge
+      const float lxx = lap9(lc, rl[3 + e], rl[5 + e], rl[2 + e], rl[6 + e], rl[1 + e],
+                             rl[7 + e], rl[e], rl[8 + e]);
+      const float lyy = lap9(lc, pick(lym[0]), pick(lyp[0]), pick(lym[1]), pick(lyp[1]),
+                             pick(lym[2]), pick(lyp[2]), pick(lym[3]), pick(lyp[3]));
+      const float lzz = lap9(lz0, lq[e][3], lq[e][5], lq[e][2], lq[e][6], lq[e][1], lq[e][7],
+                             lq[e][0], lq[e][8]);
+      const float lxy = fmaf(lyy, a.sy, lxx * a.sx);
+      const float lzs = lzz * a.sz;
+      lnx[e] = dd * fmaf(a11, lxy, fmaf(a13, lzs, 2.f * lc - dd * pick(lpx)));
+      lnz[e] = dd * fmaf(a13, lxy, fmaf(a33, lzs, 2.f * lz0 - dd * pick(lpz)));
+    }
+    const long long i = (long long)z * a.d.plane + off;
+    if (v0 && v1) {
+      *reinterpret_cast<float2*>(a.spx + i) = make_float2(snx[0], snx[1]);
+      *reinterpret_cast<float2*>(a.spz + i) = make_float2(snz[0], snz[1]);
+      *reinterpret_cast<float2*>(a.lpx + i) = make_float2(lnx[0], lnx[1]);
+      *reinterpret_cast<float2*>(a.lpz + i) = make_float2(lnz[0], lnz[1]);
+      *reinterpret_cast<float2*>(a.g11 + i) = make_float2(g11[0], g11[1]);
+      if (!kRtm) {
+        *reinterpret_cast<float2*>(a.g13 + i) = make_float2(g13[0], g13[1]);
+        *reinterpret_cast<float2*>(a.g33 + i) = make_float2(g33[0], g33[1]);
+      }
+    } else {
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        if (e ? v1 : v0) {
+          a.spx[i + e] = snx[e];
+          a.spz[i + e] = snz[e];
+          a.lpx[i + e] = lnx[e];
+          a.lpz[i + e] = lnz[e];
+          a.g11[i + e] = g11[e];
+          if (!kRtm) {
+            a.g13[i + e] = g13[e];
+            a.g33[i + e] = g33[e];
+          }
+        }
+      }
+    }
+    if (((z + 1) & 3) == 0 && z + 1 < a.d.nz) {
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) lq[e][kk + 1] *= dxy[e] * dzr[kk];
+      }
+    }
+  }
+  return true;
+}
+
 // kRtm selects the imaging condition of rtmCij3d_f (kernel3d.cu:456-469,
 // rtm3d_f.cu:607-610): one image volume, kept in the g11 slot, gains
 // (2/3 sx + 1/3 sz)(2/3 lx + 1/3 lz) with both fields at the current level and
 // the adjoint already multiplied by this step's sponge; g13/g33 are neither
-// loaded nor written.
-template <bool kRtm>
+// loaded nor written. kBatch: the items of all jobs of `jt`.
+template <bool kRtm, bool kBatch>
 __global__ void __launch_bounds__(NTHREADS, 2)
-    k_bwd3d_tma(const __grid_constant__ BwdMaps m, const BwdArgs a) {
+    k_bwd3d_tma(const __grid_constant__ BwdMaps m0, const __grid_constant__ BwdArgs a0,
+                const JobTable jt) {
   extern __shared__ unsigned char smem_raw[];
   unsigned char* smem =
       (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -405,229 +711,39 @@ __global__ void __launch_bounds__(NTHREADS, 2)
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  const Dims3 d = a.d;
-
+  const int items = kBatch ? jt.items : a0.sc.items;
+  long long k = 0;
   if (warp == NCW) {  // ---------------- producer
     if (lane == 0) {
-      long long k = 0;
-      bool ok = true;
-      for (int it = blockIdx.x; ok && it < a.sc.items; it += gridDim.x) {
-        int bx, by, z0, z1;
-        item(a.sc, it, bx, by, z0, z1);
-        const int x0 = bx * TX, y0 = kHalo + by * TY;
-        for (int z = z0; z < z1; ++z, ++k) {
-          const int s = (int)(k % B_STAGES);
-          if (k >= B_STAGES &&
-              !mbar_wait(&empty[s], (uint32_t)(((k / B_STAGES) & 1) ^ 1), a.status)) {
-            ok = false;
-            break;
-          }
-          const int zp = z + kZPad;
-          unsigned char* st = smem + s * B_STAGE_BYTES;
-          unsigned char* pl = st + B_OFF_P;
-          mbar_arrive_expect_tx(&full[s], kRtm ? B_STAGE_BYTES - 2 * PLAIN_BYTES : B_STAGE_BYTES);
-          tma_load(st + B_OFF_SH, &m.scx, &full[s], x0 - kHalo, y0 - kHalo, zp);
-          tma_load(st + B_OFF_LH, &m.lcx, &full[s], x0 - kHalo, y0 - kHalo, zp);
-          tma_load(pl + 0 * PLAIN_BYTES, &m.scz, &full[s], x0, y0, zp + kHalo);
-          tma_load(pl + 1 * PLAIN_BYTES, &m.lcz, &full[s], x0, y0, zp + kHalo);
-          tma_load(pl + 2 * PLAIN_BYTES, &m.spx, &full[s], x0, y0, zp);
-          tma_load(pl + 3 * PLAIN_BYTES, &m.spz, &full[s], x0, y0, zp);
-          tma_load(pl + 4 * PLAIN_BYTES, &m.lpx, &full[s], x0, y0, zp);
-          tma_load(pl + 5 * PLAIN_BYTES, &m.lpz, &full[s], x0, y0, zp);
-          tma_load(pl + 6 * PLAIN_BYTES, &m.c11, &full[s], x0, y0, zp);
-          tma_load(pl + 7 * PLAIN_BYTES, &m.c13, &full[s], x0, y0, zp);
-          tma_load(pl + 8 * PLAIN_BYTES, &m.c33, &full[s], x0, y0, zp);
-          tma_load(pl + 9 * PLAIN_BYTES, &m.g11, &full[s], x0, y0, zp);
-          if (!kRtm) {
-            tma_load(pl + 10 * PLAIN_BYTES, &m.g13, &full[s], x0, y0, zp);
-            tma_load(pl + 11 * PLAIN_BYTES, &m.g33, &full[s], x0, y0, zp);
-          }
+      for (int it = blockIdx.x; it < items; it += gridDim.x) {
+        bool ok;
+        if constexpr (kBatch) {
+          const int j = find_job(jt, it);
+          const BwdJob& J = reinterpret_cast<const BwdJob*>(jt.jobs)[j];
+          const int par = (jt.tick - J.t0) & 1;
+          ok = bwd_produce<kRtm>(J.a[par], J.m[par], it - jt.base[j], smem, full, empty, k);
+        } else {
+          ok = bwd_produce<kRtm>(a0, m0, it, smem, full, empty, k);
         }
+        if (!ok) break;
       }
     }
     return;
   }
-
-  // consumers: the x pair x0 + 2*(lane%16) + {0,1} of tile row 2*warp + lane/16
-  const int ry = warp * 2 + (lane >> 4);
-  const int xo = 2 * (lane & 15);
-  const int sr = (ry + kHalo) * HX + xo + kHalo;
-  const int pi = ry * TX + xo;
-  float sq[2][9], lq[2][9];
-  float dxy[2];
-  long long k = 0;
-  bool ok = true;
-  for (int it = blockIdx.x; ok && it < a.sc.items; it += gridDim.x) {
-    int bx, by, z0, z1;
-    item(a.sc, it, bx, by, z0, z1);
-    const int x = bx * TX + xo;
-    const int y = kHalo + by * TY + ry;
-    const bool vy = y < d.ny - kHalo;
-    const bool v0 = vy && x >= kHalo && x < d.nx - kHalo;
-    const bool v1 = vy && x + 1 >= kHalo && x + 1 < d.nx - kHalo;
-    const int off = y * d.pitch + x;  // x + 1 < pitch: 32 * gx <= pitch
-    dxy[0] = v0 ? a.dampx[x] * a.dampy[y] : 1.f;
-    dxy[1] = v1 ? a.dampx[x + 1] * a.dampy[y] : 1.f;
-    // start the queues: planes z0-4 .. z0+3 from global
-    sq[0][0] = sq[1][0] = lq[0][0] = lq[1][0] = 0.f;
-#pragma unroll
-    for (int kk = 1; kk < 9; ++kk) {
-      const int zz = z0 - 5 + kk;
-      const long long i = (long long)zz * d.plane + off;
-      const bool any = v0 || v1;
-      const float2 sv =
-          any ? __ldg(reinterpret_cast<const float2*>(a.scz + i)) : make_float2(0.f, 0.f);
-      float2 lv = any ? __ldg(reinterpret_cast<const float2*>(a.lcz + i)) : make_float2(0.f, 0.f);
-      if (zz >= 0 && (zz >> 2) < (z0 >> 2)) {
-        lv.x *= dxy[0] * a.dampz[zz];
-        lv.y *= dxy[1] * a.dampz[zz];
-      }
-      sq[0][kk] = sv.x;
-      sq[1][kk] = sv.y;
-      lq[0][kk] = lv.x;
-      lq[1][kk] = lv.y;
+  unsigned char* slot = (unsigned char*)(empty + B_STAGES) + warp * ARG_SLOT;
+  for (int it = blockIdx.x; it < items; it += gridDim.x) {
+    bool ok;
+    if constexpr (kBatch) {
+      const int j = find_job(jt, it);
+      const BwdJob& J = reinterpret_cast<const BwdJob*>(jt.jobs)[j];
+      const int step = jt.tick - J.t0;
+      const BwdArgs* a = stage_args(J.a[step & 1], slot, lane);
+      ok = bwd_consume<kRtm>(*a, it - jt.base[j], __ldg(J.amp + step), smem, full, empty, k,
+                             warp, lane);
+    } else {
+      ok = bwd_consume<kRtm>(a0, it, a0.src.amp, smem, full, empty, k, warp, lane);
     }
-    // z damping factors in registers (see the forward kernel)
-    float dzr[4];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) dzr[j] = z0 - 4 + j >= 0 ? a.dampz[z0 - 4 + j] : 1.f;
-    float dz_next = a.dampz[z0];
-    for (int z = z0; z < z1; ++z, ++k) {
-      const float dz = dz_next;
-      if (z + 1 < z1) dz_next = a.dampz[z + 1];
-#pragma unroll
-      for (int j = 0; j < 3; ++j) dzr[j] = dzr[j + 1];
-      dzr[3] = dz;
-      const int s = (int)(k % B_STAGES);
-      if (!mbar_wait(&full[s], (uint32_t)((k / B_STAGES) & 1), a.status)) {
-        ok = false;
-        break;
-      }
-      const unsigned char* st = smem + s * B_STAGE_BYTES;
-      const float* sh = (const float*)(st + B_OFF_SH) + sr;
-      const float* lh = (const float*)(st + B_OFF_LH) + sr;
-      const float* pl = (const float*)(st + B_OFF_P) + pi;
-      constexpr int T = TX * TY;
-#pragma unroll
-      for (int kk = 0; kk < 8; ++kk) {
-        sq[0][kk] = sq[0][kk + 1];
-        sq[1][kk] = sq[1][kk + 1];
-        lq[0][kk] = lq[0][kk + 1];
-        lq[1][kk] = lq[1][kk + 1];
-      }
-      {
-        const float2 s8 = ld2(pl), l8 = ld2(pl + T);
-        sq[0][8] = s8.x;
-        sq[1][8] = s8.y;
-        lq[0][8] = l8.x;
-        lq[1][8] = l8.y;
-      }
-      // x rows (x-4 .. x+5) and y column pairs of both halo fields
-      float rs[10], rl[10];
-#pragma unroll
-      for (int j = 0; j < 5; ++j) {
-        const float2 t = ld2(sh - 4 + 2 * j), u = ld2(lh - 4 + 2 * j);
-        rs[2 * j] = t.x;
-        rs[2 * j + 1] = t.y;
-        rl[2 * j] = u.x;
-        rl[2 * j + 1] = u.y;
-      }
-      float2 sym[4], syp[4], lym[4], lyp[4];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        sym[j] = ld2(sh - (j + 1) * HX);
-        syp[j] = ld2(sh + (j + 1) * HX);
-        lym[j] = ld2(lh - (j + 1) * HX);
-        lyp[j] = ld2(lh + (j + 1) * HX);
-      }
-      const float2 spx = ld2(pl + 2 * T), spz = ld2(pl + 3 * T);
-      const float2 lpx = ld2(pl + 4 * T), lpz = ld2(pl + 5 * T);
-      const float2 c11 = ld2(pl + 6 * T), c13 = ld2(pl + 7 * T), c33 = ld2(pl + 8 * T);
-      const float2 g11o = ld2(pl + 9 * T);
-      const float2 g13o = kRtm ? make_float2(0.f, 0.f) : ld2(pl + 10 * T);
-      const float2 g33o = kRtm ? make_float2(0.f, 0.f) : ld2(pl + 11 * T);
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&empty[s]);
-      float snx[2], snz[2], lnx[2], lnz[2], g11[2], g13[2], g33[2];
-#pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        auto pick = [e](float2 v) { return e ? v.y : v.x; };
-        const float a11 = pick(c11), a13 = pick(c13), a33 = pick(c33);
-        // source wavefield back one level (gradient form)
-        const float sc = rs[4 + e];
-        const float sxx = lap9(sc, rs[3 + e], rs[5 + e], rs[2 + e], rs[6 + e], rs[1 + e],
-                               rs[7 + e], rs[e], rs[8 + e]);
-        const float syy = lap9(sc, pick(sym[0]), pick(syp[0]), pick(sym[1]), pick(syp[1]),
-                               pick(sym[2]), pick(syp[2]), pick(sym[3]), pick(syp[3]));
-        const float szz = lap9(sq[e][4], sq[e][3], sq[e][5], sq[e][2], sq[e][6], sq[e][1],
-                               sq[e][7], sq[e][0], sq[e][8]);
-        const float sxy_u = fmaf(syy, a.idy2, sxx * a.idx2);
-        const float sz_u = szz * a.idz2;
-        snx[e] = fmaf(a.dt2, fmaf(a11, sxy_u, a13 * sz_u), 2.f * sc - pick(spx));
-        snz[e] = fmaf(a.dt2, fmaf(a13, sxy_u, a33 * sz_u), 2.f * sq[e][4] - pick(spz));
-        if (x + e == a.src.x && y == a.src.y && z == a.src.z) {
-          snx[e] += a.src.amp;
-          snz[e] += a.src.amp;
-        }
-        // imaging with the current adjoint
-        const float lc = rl[4 + e];
-        const float lz0 = lq[e][4];
-        const float dd = dxy[e] * dz;
-        if (kRtm) {
-          g11[e] = fmaf(fmaf(kTwoThirdF, sc, kOneThirdF * sq[e][4]),
-                        dd * fmaf(kTwoThirdF, lc, kOneThirdF * lz0), pick(g11o));
-        } else {
-          g11[e] = fmaf(lc, sxy_u, pick(g11o));
-          g33[e] = fmaf(lz0, sz_u, pick(g33o));
-          g13[e] = fmaf(lz0, sxy_u, fmaf(lc, sz_u, pick(g13o)));
-        }
-        // adjoint, forward form with the sponge
-        const float lxx = lap9(lc, rl[3 + e], rl[5 + e], rl[2 + e], rl[6 + e], rl[1 + e],
-                               rl[7 + e], rl[e], rl[8 + e]);
-        const float lyy = lap9(lc, pick(lym[0]), pick(lyp[0]), pick(lym[1]), pick(lyp[1]),
-                               pick(lym[2]), pick(lyp[2]), pick(lym[3]), pick(lyp[3]));
-        const float lzz = lap9(lz0, lq[e][3], lq[e][5], lq[e][2], lq[e][6], lq[e][1], lq[e][7],
-                               lq[e][0], lq[e][8]);
-        const float lxy = fmaf(lyy, a.sy, lxx * a.sx);
-        const float lzs = lzz * a.sz;
-        lnx[e] = dd * fmaf(a11, lxy, fmaf(a13, lzs, 2.f * lc - dd * pick(lpx)));
-        lnz[e] = dd * fmaf(a13, lxy, fmaf(a33, lzs, 2.f * lz0 - dd * pick(lpz)));
-      }
-      const long long i = (long long)z * d.plane + off;
-      if (v0 && v1) {
-        *reinterpret_cast<float2*>(a.spx + i) = make_float2(snx[0], snx[1]);
-        *reinterpret_cast<float2*>(a.spz + i) = make_float2(snz[0], snz[1]);
-        *reinterpret_cast<float2*>(a.lpx + i) = make_float2(lnx[0], lnx[1]);
-        *reinterpret_cast<float2*>(a.lpz + i) = make_float2(lnz[0], lnz[1]);
-        *reinterpret_cast<float2*>(a.g11 + i) = make_float2(g11[0], g11[1]);
-        if (!kRtm) {
-          *reinterpret_cast<float2*>(a.g13 + i) = make_float2(g13[0], g13[1]);
-          *reinterpret_cast<float2*>(a.g33 + i) = make_float2(g33[0], g33[1]);
-        }
-      } else {
-#pragma unroll
-        for (int e = 0; e < 2; ++e) {
-          if (e ? v1 : v0) {
-            a.spx[i + e] = snx[e];
-            a.spz[i + e] = snz[e];
-            a.lpx[i + e] = lnx[e];
-            a.lpz[i + e] = lnz[e];
-            a.g11[i + e] = g11[e];
-            if (!kRtm) {
-              a.g13[i + e] = g13[e];
-              a.g33[i + e] = g33[e];
-            }
-          }
-        }
-      }
-      if (((z + 1) & 3) == 0 && z + 1 < d.nz) {
-#pragma unroll
-        for (int e = 0; e < 2; ++e) {
-#pragma unroll
-          for (int kk = 0; kk < 4; ++kk) lq[e][kk + 1] *= dxy[e] * dzr[kk];
-        }
-      }
-    }
+    if (!ok) break;
   }
 }
 
@@ -702,22 +818,34 @@ int make_tile_maps(vti_ctx* ctx, const Dims3& d, const Vol& v, TileMaps* out) {
 static const CUtensorMap* P(const TileMaps& m) { return (const CUtensorMap*)m.plain; }
 static const CUtensorMap* H(const TileMaps& m) { return (const CUtensorMap*)m.halo; }
 
-int launch_fwd3d_tma(vti_ctx* ctx, const Dims3& d, const TileMaps& cx, const TileMaps& cz,
-                     const TileMaps& px, const TileMaps& pz, const TileMaps& c11,
-                     const TileMaps& c13, const TileMaps& c33, const float* cz_ptr,
-                     float* px_ptr, float* pz_ptr, const Damping* damp, float sx, float sy,
-                     float sz, PointSource src, Probe probe) {
-  const bool pr = probe.x >= 0 && probe.out;
-  static bool attr[2][64] = {};  // per instantiation and device
-  if (ctx->device >= 64 || !attr[pr][ctx->device]) {
-    VTI_CUDA(ctx, cudaFuncSetAttribute(pr ? k_fwd3d_tma<true> : k_fwd3d_tma<false>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       F_SMEM));
-    if (ctx->device < 64) attr[pr][ctx->device] = true;
-  }
+namespace {
+
+// Segment schedule with a fixed segment length (batched jobs, autotuned).
+Sched sched_with_seg(const Dims3& d, int seg) {
+  Sched s;
+  s.gx = (d.nx - kHalo + TX - 1) / TX;
+  s.gy = (d.ny - 2 * kHalo + TY - 1) / TY;
+  s.nz = d.nz;
+  s.seg = std::max(1, std::min(seg, d.nz));
+  s.items = s.gx * s.gy * ((d.nz + s.seg - 1) / s.seg);
+  s.grid = s.items;
+  return s;
+}
+
+template <typename K>
+int set_smem_attr(vti_ctx* ctx, K kern, int bytes, bool* done) {
+  if (ctx->device < 64 && done[ctx->device]) return VTI_OK;
+  VTI_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  if (ctx->device < 64) done[ctx->device] = true;
+  return VTI_OK;
+}
+
+FwdArgs fwd_args(vti_ctx* ctx, const Dims3& d, const Sched& sc, const float* cz_ptr,
+                 float* px_ptr, float* pz_ptr, const Damping* damp, float sx, float sy,
+                 float sz, PointSource src) {
   FwdArgs a;
   a.d = d;
-  a.sc = make_sched(ctx, d, 3);
+  a.sc = sc;
   a.cz = cz_ptr;
   a.px = px_ptr;
   a.pz = pz_ptr;
@@ -728,14 +856,34 @@ int launch_fwd3d_tma(vti_ctx* ctx, const Dims3& d, const TileMaps& cx, const Til
   a.sy = sy;
   a.sz = sz;
   a.src = src;
-  a.probe = probe;
+  a.probe = Probe();
   a.status = ctx->d_status;
+  return a;
+}
+
+}  // namespace
+
+int launch_fwd3d_tma(vti_ctx* ctx, const Dims3& d, const TileMaps& cx, const TileMaps& cz,
+                     const TileMaps& px, const TileMaps& pz, const TileMaps& c11,
+                     const TileMaps& c13, const TileMaps& c33, const float* cz_ptr,
+                     float* px_ptr, float* pz_ptr, const Damping* damp, float sx, float sy,
+                     float sz, PointSource src, Probe probe) {
+  const bool pr = probe.x >= 0 && probe.out;
+  static bool attr[2][64] = {};  // per instantiation and device
+  VTI_TRY_ST(set_smem_attr(ctx, pr ? k_fwd3d_tma<true, false> : k_fwd3d_tma<false, false>,
+                           F_SMEM, attr[pr]));
+  FwdMaps m;
+  m.cx = *H(cx); m.cz = *P(cz); m.px = *P(px); m.pz = *P(pz);
+  m.c11 = *P(c11); m.c13 = *P(c13); m.c33 = *P(c33);
+  FwdArgs a = fwd_args(ctx, d, make_sched(ctx, d, 3), cz_ptr, px_ptr, pz_ptr, damp, sx, sy, sz,
+                       src);
+  a.probe = probe;
+  JobTable jt{};
   const int grid = a.sc.grid;
   {
     LaunchTimer tm(ctx, kTimedFwd3d);
-    auto kern = pr ? k_fwd3d_tma<true> : k_fwd3d_tma<false>;
-    kern<<<grid, NTHREADS, F_SMEM, ctx->stream>>>(*H(cx), *P(cz), *P(px), *P(pz), *P(c11),
-                                                         *P(c13), *P(c33), a);
+    auto kern = pr ? k_fwd3d_tma<true, false> : k_fwd3d_tma<false, false>;
+    kern<<<grid, NTHREADS, F_SMEM, ctx->stream>>>(m, a, jt);
   }
   VTI_LAUNCHED(ctx, "k_fwd3d_tma");
   return VTI_OK;
@@ -751,11 +899,8 @@ int launch_bwd3d_tma(vti_ctx* ctx, const Dims3& d, const TileMaps& scx, const Ti
                      float* g33_ptr, const Damping& damp, float dt2, float idx2, float idy2,
                      float idz2, float sx, float sy, float sz, PointSource src, bool rtm) {
   static bool attr[2][64] = {};  // per instantiation and device
-  if (ctx->device >= 64 || !attr[rtm][ctx->device]) {
-    VTI_CUDA(ctx, cudaFuncSetAttribute(rtm ? k_bwd3d_tma<true> : k_bwd3d_tma<false>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, B_SMEM));
-    if (ctx->device < 64) attr[rtm][ctx->device] = true;
-  }
+  VTI_TRY_ST(set_smem_attr(ctx, rtm ? k_bwd3d_tma<true, false> : k_bwd3d_tma<false, false>,
+                           B_SMEM, attr[rtm]));
   BwdMaps m;
   m.scx = *H(scx); m.scz = *P(scz); m.spx = *P(spx); m.spz = *P(spz);
   m.lcx = *H(lcx); m.lcz = *P(lcz); m.lpx = *P(lpx); m.lpz = *P(lpz);
@@ -772,15 +917,111 @@ int launch_bwd3d_tma(vti_ctx* ctx, const Dims3& d, const TileMaps& scx, const Ti
   a.sx = sx; a.sy = sy; a.sz = sz;
   a.src = src;
   a.status = ctx->d_status;
+  JobTable jt{};
   const int grid = a.sc.grid;
   {
     LaunchTimer tm(ctx, kTimedBwd3d);
     if (rtm)
-      k_bwd3d_tma<true><<<grid, NTHREADS, B_SMEM, ctx->stream>>>(m, a);
+      k_bwd3d_tma<true, false><<<grid, NTHREADS, B_SMEM, ctx->stream>>>(m, a, jt);
     else
-      k_bwd3d_tma<false><<<grid, NTHREADS, B_SMEM, ctx->stream>>>(m, a);
+      k_bwd3d_tma<false, false><<<grid, NTHREADS, B_SMEM, ctx->stream>>>(m, a, jt);
   }
   VTI_LAUNCHED(ctx, "k_bwd3d_tma");
+  return VTI_OK;
+}
+
+// ------------------------------------------------------------ batched jobs
+size_t fwd_job_bytes() { return sizeof(FwdJob); }
+size_t bwd_job_bytes() { return sizeof(BwdJob); }
+
+int build_fwd_job(vti_ctx* ctx, const FwdJobSpec& sp, void* dst, int* items) {
+  if (((uintptr_t)dst & 63) != 0) return fail(ctx, VTI_ERR_ARG, "job descriptor not aligned");
+  FwdJob* J = new (dst) FwdJob();
+  const Sched sc = sp.seg > 0 ? sched_with_seg(sp.d, sp.seg) : make_sched(ctx, sp.d, 3);
+  for (int p = 0; p < 2; ++p) {
+    FwdMaps& m = J->m[p];
+    m.cx = *H(*sp.cx[p]); m.cz = *P(*sp.cz[p]); m.px = *P(*sp.px[p]); m.pz = *P(*sp.pz[p]);
+    m.c11 = *P(*sp.c[0]); m.c13 = *P(*sp.c[1]); m.c33 = *P(*sp.c[2]);
+    PointSource src;
+    src.x = sp.src_x; src.y = sp.src_y; src.z = sp.src_z;
+    J->a[p] = fwd_args(ctx, sp.d, sc, sp.cz_ptr[p], sp.px_ptr[p], sp.pz_ptr[p], sp.damp, sp.sx,
+                       sp.sy, sp.sz, src);
+  }
+  J->amp = sp.amp;
+  J->t0 = sp.t0;
+  *items = sc.items;
+  return VTI_OK;
+}
+
+int build_bwd_job(vti_ctx* ctx, const BwdJobSpec& sp, void* dst, int* items) {
+  if (((uintptr_t)dst & 63) != 0) return fail(ctx, VTI_ERR_ARG, "job descriptor not aligned");
+  BwdJob* J = new (dst) BwdJob();
+  const Sched sc = sp.seg > 0 ? sched_with_seg(sp.d, sp.seg) : make_sched(ctx, sp.d, 2);
+  for (int p = 0; p < 2; ++p) {
+    BwdMaps& m = J->m[p];
+    m.scx = *H(*sp.scx[p]); m.scz = *P(*sp.scz[p]); m.spx = *P(*sp.spx[p]);
+    m.spz = *P(*sp.spz[p]);
+    m.lcx = *H(*sp.lcx[p]); m.lcz = *P(*sp.lcz[p]); m.lpx = *P(*sp.lpx[p]);
+    m.lpz = *P(*sp.lpz[p]);
+    m.c11 = *P(*sp.c[0]); m.c13 = *P(*sp.c[1]); m.c33 = *P(*sp.c[2]);
+    m.g11 = *P(*sp.g[0]); m.g13 = *P(*sp.g[1]); m.g33 = *P(*sp.g[2]);
+    BwdArgs& a = J->a[p];
+    a.d = sp.d;
+    a.sc = sc;
+    a.scz = sp.scz_ptr[p]; a.lcz = sp.lcz_ptr[p];
+    a.spx = sp.spx_ptr[p]; a.spz = sp.spz_ptr[p]; a.lpx = sp.lpx_ptr[p]; a.lpz = sp.lpz_ptr[p];
+    a.g11 = sp.g_ptr[0]; a.g13 = sp.g_ptr[1]; a.g33 = sp.g_ptr[2];
+    a.dampx = sp.damp.x; a.dampy = sp.damp.y; a.dampz = sp.damp.z;
+    a.dt2 = sp.dt2; a.idx2 = sp.idx2; a.idy2 = sp.idy2; a.idz2 = sp.idz2;
+    a.sx = sp.sx; a.sy = sp.sy; a.sz = sp.sz;
+    a.src.x = sp.src_x; a.src.y = sp.src_y; a.src.z = sp.src_z; a.src.amp = 0.f;
+    a.status = ctx->d_status;
+  }
+  J->amp = sp.amp;
+  J->t0 = sp.t0;
+  *items = sc.items;
+  return VTI_OK;
+}
+
+namespace {
+bool attr_fwd_batch[64] = {}, attr_bwd_batch[64] = {};
+}  // namespace
+
+int prepare_batch_kernels(vti_ctx* ctx) {
+  VTI_TRY_ST(set_smem_attr(ctx, k_fwd3d_tma<false, true>, F_SMEM, attr_fwd_batch));
+  VTI_TRY_ST(set_smem_attr(ctx, k_bwd3d_tma<false, true>, B_SMEM, attr_bwd_batch));
+  return VTI_OK;
+}
+
+int launch_fwd3d_batch(vti_ctx* ctx, const void* d_jobs, const int* d_base, int njobs, int items,
+                       int tick) {
+  VTI_TRY_ST(set_smem_attr(ctx, k_fwd3d_tma<false, true>, F_SMEM, attr_fwd_batch));
+  if (items <= 0 || njobs <= 0) return VTI_OK;
+  JobTable jt{(const unsigned char*)d_jobs, d_base, njobs, items, tick};
+  FwdMaps m{};
+  FwdArgs a{};
+  const int grid = std::min(items, ctx->sm_count * 3);
+  {
+    LaunchTimer tm(ctx, kTimedFwd3d);
+    k_fwd3d_tma<false, true><<<grid, NTHREADS, F_SMEM, ctx->stream>>>(m, a, jt);
+  }
+  VTI_LAUNCHED(ctx, "k_fwd3d_tma (batched)");
+  return VTI_OK;
+}
+
+int launch_bwd3d_batch(vti_ctx* ctx, const void* d_jobs, const int* d_base, int njobs, int items,
+                       int tick) {
+  VTI_TRY_ST(set_smem_attr(ctx, k_bwd3d_tma<false, true>, B_SMEM, attr_bwd_batch));
+  if (items <= 0 || njobs <= 0) return VTI_OK;
+  JobTable jt{(const unsigned char*)d_jobs, d_base, njobs, items, tick};
+  BwdMaps m{};
+  BwdArgs a{};
+  const int grid = std::min(items, ctx->sm_count * 2);
+  {
+    LaunchTimer tm(ctx, kTimedBwd3d);
+    k_bwd3d_tma<false, true><<<grid, NTHREADS, B_SMEM, ctx->stream>>>(m, a, jt);
+  }
+  VTI_LAUNCHED(ctx, "k_bwd3d_tma (batched)");
   return VTI_OK;
 }
 

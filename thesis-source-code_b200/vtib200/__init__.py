@@ -109,6 +109,16 @@ def _signatures():
         "vti3d_gradient_vepsdel": (C.c_int, [P, P, P, P, P, P, P, C.c_float, C.c_float,
                                              C.c_float, P, P, P, C.c_int, P, C.c_int, P, P, P, P,
                                              C.POINTER(C.c_double), C.c_uint]),
+        "vti3d_batch_create": (C.c_int, [P, P, C.c_uint, C.POINTER(VP)]),
+        "vti3d_batch_destroy": (C.c_int, [P]),
+        "vti3d_batch_set_model": (C.c_int, [P, P, P, P, C.c_int]),
+        "vti3d_batch_set_wavelet": (C.c_int, [P, P, C.c_int]),
+        "vti3d_batch_set_receivers": (C.c_int, [P, P, C.c_int]),
+        "vti3d_batch_set_shots": (C.c_int, [P, C.c_int, P, P, C.c_uint]),
+        "vti3d_batch_set_options": (C.c_int, [P, C.c_int, C.c_int, C.c_int]),
+        "vti3d_batch_autotune": (C.c_int, [P, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+        "vti3d_batch_gradient": (C.c_int, [P, P, C.c_int, P, C.c_int, C.POINTER(C.c_double)]),
+        "vti3d_batch_get_shot_models": (C.c_int, [P, C.c_int, P, P]),
     }
 
 
@@ -306,6 +316,80 @@ class Plan3d:
     def close(self):
         if self._h:
             lib().vti3d_plan_destroy(self._h)
+            self._h = VP()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch3d:
+    """Batched multi-shot 3D gradient (vti3d_batch_*): every shot on its own
+    window of the model, all shots advanced by one forward and one backward
+    launch per time step."""
+
+    def __init__(self, ctx: Context, g: Geom3d, flags: int = 0):
+        self.ctx, self.g = ctx, g
+        self._h = VP()
+        ctx.check(lib().vti3d_batch_create(ctx.handle, C.byref(g), flags, C.byref(self._h)))
+        ctx._plans.add(self)
+        self.windows = []
+
+    def set_model(self, c11, c13, c33, mem=MEM_HOST):
+        if mem == MEM_HOST:
+            c11, c13, c33 = _f32(c11), _f32(c13), _f32(c33)
+        self.ctx.check(lib().vti3d_batch_set_model(self._h, _p(c11), _p(c13), _p(c33), mem))
+
+    def set_wavelet(self, w, mem=MEM_HOST):
+        if mem == MEM_HOST:
+            w = _f32(w)
+        self.ctx.check(lib().vti3d_batch_set_wavelet(self._h, _p(w), mem))
+
+    def set_receivers(self, recloc):
+        recloc = _f32(recloc).reshape(-1)
+        self.ctx.check(lib().vti3d_batch_set_receivers(self._h, _p(recloc), recloc.size // 4))
+
+    def set_shots(self, souloc, windows, seed=0):
+        """souloc: 5 floats per shot; windows: (x0, y0, nx, ny) per shot."""
+        souloc = _f32(souloc).reshape(-1)
+        w = np.ascontiguousarray(np.asarray(windows, dtype=np.int32).reshape(-1, 4))
+        self.windows = [tuple(int(v) for v in r) for r in w]
+        self.ctx.check(lib().vti3d_batch_set_shots(self._h, len(w), _p(souloc), _p(w),
+                                                   seed & 0xffffffff))
+
+    def set_options(self, use_graph=False, seg_fwd=0, seg_bwd=0):
+        self.ctx.check(lib().vti3d_batch_set_options(self._h, int(use_graph), seg_fwd, seg_bwd))
+
+    def autotune(self):
+        a, b = C.c_int(0), C.c_int(0)
+        self.ctx.check(lib().vti3d_batch_autotune(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def gradient(self, dobs, dobs_mem=MEM_HOST, fgcij=None, fgcij_mem=MEM_HOST):
+        if dobs_mem == MEM_HOST:
+            dobs = _f32(dobs)
+        n = self.g.nx * self.g.ny * self.g.nz
+        if fgcij is None:
+            fgcij = np.zeros(1 + 3 * n, dtype=np.float32)
+        mis = C.c_double(0)
+        self.ctx.check(lib().vti3d_batch_gradient(self._h, _p(dobs), dobs_mem, _p(fgcij),
+                                                  fgcij_mem, C.byref(mis)))
+        return fgcij, mis.value
+
+    def shot_models(self, k):
+        """(pad-boundary, random-boundary) window models of shot k, 3*n each."""
+        x0, y0, nx, ny = self.windows[k]
+        n = nx * ny * self.g.nz
+        cpad = np.zeros(3 * n, dtype=np.float32)
+        crand = np.zeros(3 * n, dtype=np.float32)
+        self.ctx.check(lib().vti3d_batch_get_shot_models(self._h, k, _p(cpad), _p(crand)))
+        return cpad, crand
+
+    def close(self):
+        if self._h:
+            lib().vti3d_batch_destroy(self._h)
             self._h = VP()
 
     def __del__(self):

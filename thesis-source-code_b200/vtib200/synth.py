@@ -273,3 +273,48 @@ def survey2d(nx=401, nz=201, nt=2000, npad=30, d=10.0, dt=1e-3, rate=2e-3, freq=
     taper = init_taper2d(nx, nz, npad)
     return Survey2d(nx, nz, nt, npad, d, dt, rate, c11, c13, c33, wavelet, sloc.reshape(-1),
                     rloc.reshape(-1), taper)
+
+
+def batch_windows(nx, ny, nshot, amin, amax, seed=5):
+    """Per-shot windows (x0, y0, ax, ay) of a batched survey: apertures per
+    side drawn uniformly from [amin, amax] (seeded, clipped to the model),
+    window centres on a regular grid of shot positions over the model."""
+    rng = np.random.default_rng(seed)
+    g = int(np.ceil(np.sqrt(nshot)))
+    wins = []
+    for k in range(nshot):
+        ax = int(min(rng.integers(amin, amax + 1), nx))
+        ay = int(min(rng.integers(amin, amax + 1), ny))
+        cx = int((k % g + 0.5) * nx / g)
+        cy = int((k // g + 0.5) * ny / g)
+        x0 = int(np.clip(cx - ax // 2, 0, nx - ax))
+        y0 = int(np.clip(cy - ay // 2, 0, ny - ay))
+        wins.append((x0, y0, ax, ay))
+    return wins
+
+
+def batch_survey3d(s: Survey3d, windows, rec_step=2, rec_depth=None, src_depth=None):
+    """Sources and receivers of a batched survey on the model of s: one shot
+    per window, the source at the window's centre cell, receivers on every
+    rec_step-th cell of the window's interior (outside its npad frame).
+    Returns (souloc: 5 floats per shot, recloc: 4 floats per receiver, one
+    global list, each shot's receivers contiguous)."""
+    d, o, npad = s.d, s.o, s.npad
+    rz = (3 * d if rec_depth is None else rec_depth) + 0.25 * d
+    sz = (5 * d if src_depth is None else src_depth) + 0.25 * d
+    so, rec = [], []
+    for (x0, y0, ax, ay) in windows:
+        rx = np.arange(x0 + npad, x0 + ax - npad, rec_step)
+        ry = np.arange(y0 + npad, y0 + ay - npad, rec_step)
+        RX, RY = np.meshgrid(rx, ry, indexing="xy")
+        first = sum(len(r) for r in rec)
+        r = np.zeros((RX.size, 4), dtype=np.float32)
+        r[:, 0] = RX.reshape(-1) * d + o + 0.25 * d
+        r[:, 1] = RY.reshape(-1) * d + o + 0.25 * d
+        r[:, 2] = rz
+        r[:, 3] = 1.0
+        rec.append(r)
+        cx, cy = x0 + ax // 2, y0 + ay // 2
+        so.append([cx * d + o + 0.25 * d, cy * d + o + 0.25 * d, sz, RX.size, first])
+    return (np.array(so, dtype=np.float32).reshape(-1),
+            np.concatenate(rec).astype(np.float32).reshape(-1))
