@@ -187,10 +187,9 @@ struct vti3d_batch {
   std::vector<ShotGeom> geo;
   std::vector<int*> d_rec_at;
   long long cut_version = -1;  // model version cut into the windows
-  // job tables
-  unsigned char* d_jobs = nullptr;  // forward jobs, then backward jobs
-  int* d_base = nullptr;            // forward bases (2S+1), then backward (S+1)
-  int items_fwd = 0, items_bwd = 0;
+  // batched step launch plans
+  StepBatch* fwd = nullptr;         // passes 1 and 2 of every shot
+  StepBatch* bwd = nullptr;         // pass 3 of every shot
   float* d_amp = nullptr;           // forward (M-1) | backward (M-1) amplitudes
   RecJob* d_recjobs = nullptr;
   RecEntry* d_entries = nullptr;
@@ -220,11 +219,12 @@ void free_shots(vti3d_batch* b) {
   b->plans.clear();
   b->geo.clear();
   b->d_rec_at.clear();
-  void* ptrs[] = {b->d_jobs, b->d_base, b->d_amp, b->d_recjobs, b->d_entries};
+  step_batch_free(b->fwd);
+  step_batch_free(b->bwd);
+  b->fwd = b->bwd = nullptr;
+  void* ptrs[] = {b->d_amp, b->d_recjobs, b->d_entries};
   for (void* q : ptrs)
     if (q) cudaFree(q);
-  b->d_jobs = nullptr;
-  b->d_base = nullptr;
   b->d_amp = nullptr;
   b->d_recjobs = nullptr;
   b->d_entries = nullptr;
@@ -234,37 +234,44 @@ void free_shots(vti3d_batch* b) {
 
 int levels(const vti3d_batch* b) { return last_level(b->g, b->flags); }
 
-// Job descriptors, amplitudes and receiver tables of the current shots and
-// segment lengths.
+// Batched launch plans, amplitudes and receiver tables of the current shots
+// and segment lengths.
 int build_tables(vti3d_batch* b) {
   vti_ctx* ctx = b->ctx;
   free_graphs(b);
-  VTI_TRY(prepare_batch_kernels(ctx));
+  step_batch_free(b->fwd);
+  step_batch_free(b->bwd);
+  b->fwd = b->bwd = nullptr;
+  b->tables_ok = false;
   const int S = (int)b->plans.size();
   const int M = levels(b);
   const float dt2 = b->g.dt * b->g.dt;
   const float sxs = dt2 / (b->g.dx * b->g.dx), sys = dt2 / (b->g.dy * b->g.dy),
               szs = dt2 / (b->g.dz * b->g.dz);
-  const size_t fb = fwd_job_bytes(), bb = bwd_job_bytes();
-  // descriptors are 64-byte aligned (TMA maps): an aligned host staging area
-  std::vector<unsigned char> host(2 * S * fb + S * bb + 64);
-  unsigned char* h = (unsigned char*)(((uintptr_t)host.data() + 63) & ~(uintptr_t)63);
-  std::vector<int> base(2 * S + 1 + S + 1, 0);
+  const float idx2 = 1.f / (b->g.dx * b->g.dx), idy2 = 1.f / (b->g.dy * b->g.dy),
+              idz2 = 1.f / (b->g.dz * b->g.dz);
   // amplitudes: forward step s -> dt2 w[s+1]; backward step s -> dt2 w[nt-2-s]
   std::vector<float> amp(2 * (size_t)std::max(M - 1, 1), 0.f);
   for (int s = 0; s < M - 1; ++s) {
     amp[s] = dt2 * b->wavelet[s + 1];
     amp[(M - 1) + s] = dt2 * b->wavelet[b->g.nt - 2 - s];
   }
-  if (!b->d_amp) VTI_CUDA(ctx, cudaMalloc((void**)&b->d_amp, amp.size() * sizeof(float)));
+  if (b->d_amp) cudaFree(b->d_amp);
+  b->d_amp = nullptr;
+  VTI_CUDA(ctx, cudaMalloc((void**)&b->d_amp, amp.size() * sizeof(float)));
+  VTI_CUDA(ctx, cudaMemcpy(b->d_amp, amp.data(), amp.size() * sizeof(float),
+                           cudaMemcpyHostToDevice));
   const float* ampf = b->d_amp;
   const float* ampb = b->d_amp + (M - 1);
   // after the forward loop, level M is in buffer 1 - ((M-2) & 1)
   const int last_cur = 1 - ((M - 2) & 1);
-  int items = 0;
+  std::vector<FwdJobSpec> fspec;
+  std::vector<BwdJobSpec> bspec;
+  std::vector<Damping> damps(S);
   for (int k = 0; k < S; ++k) {
     vti3d_plan* p = b->plans[k];
     const ShotGeom& sg = b->geo[k];
+    damps[k] = Damping{p->dampx, p->dampy, p->dampz};
     for (int pass = 0; pass < 2; ++pass) {
       // pass 1 runs in the adjoint volumes (free until pass 3), pass 2 in sigma
       Vol* vx = pass == 0 ? p->lx : p->sx;
@@ -284,8 +291,7 @@ int build_tables(vti3d_batch* b) {
       }
       const TileMaps* cm = pass == 0 ? p->m_cpad : p->m_crand;
       for (int c = 0; c < 3; ++c) sp.c[c] = &cm[c];
-      const Damping dmp{p->dampx, p->dampy, p->dampz};  // copied into the descriptor
-      sp.damp = pass == 0 ? &dmp : nullptr;
+      sp.damp = pass == 0 ? &damps[k] : nullptr;
       sp.sx = sxs;
       sp.sy = sys;
       sp.sz = szs;
@@ -295,20 +301,8 @@ int build_tables(vti3d_batch* b) {
       sp.amp = ampf;
       sp.t0 = 0;
       sp.seg = b->seg_fwd;
-      int n = 0;
-      VTI_TRY(build_fwd_job(ctx, sp, h + (2 * k + pass) * fb, &n));
-      base[2 * k + pass] = items;
-      items += n;
+      fspec.push_back(sp);
     }
-  }
-  base[2 * S] = items;
-  b->items_fwd = items;
-  items = 0;
-  const float idx2 = 1.f / (b->g.dx * b->g.dx), idy2 = 1.f / (b->g.dy * b->g.dy),
-              idz2 = 1.f / (b->g.dz * b->g.dz);
-  for (int k = 0; k < S; ++k) {
-    vti3d_plan* p = b->plans[k];
-    const ShotGeom& sg = b->geo[k];
     BwdJobSpec sp{};
     sp.d = p->d;
     for (int par = 0; par < 2; ++par) {
@@ -336,7 +330,7 @@ int build_tables(vti3d_batch* b) {
     sp.g_ptr[0] = p->g11.origin;
     sp.g_ptr[1] = p->g13.origin;
     sp.g_ptr[2] = p->g33.origin;
-    sp.damp = Damping{p->dampx, p->dampy, p->dampz};
+    sp.damp = damps[k];
     sp.dt2 = dt2;
     sp.idx2 = idx2;
     sp.idy2 = idy2;
@@ -350,13 +344,10 @@ int build_tables(vti3d_batch* b) {
     sp.amp = ampb;
     sp.t0 = 0;
     sp.seg = b->seg_bwd;
-    int n = 0;
-    VTI_TRY(build_bwd_job(ctx, sp, h + 2 * S * fb + k * bb, &n));
-    base[2 * S + 1 + k] = items;
-    items += n;
+    bspec.push_back(sp);
   }
-  base[2 * S + 1 + S] = items;
-  b->items_bwd = items;
+  VTI_TRY(fwd_batch_build(ctx, fspec.data(), (int)fspec.size(), &b->fwd));
+  VTI_TRY(bwd_batch_build(ctx, bspec.data(), (int)bspec.size(), &b->bwd));
   // receiver tables
   std::vector<RecJob> rj(S);
   std::vector<RecEntry> ent;
@@ -387,31 +378,19 @@ int build_tables(vti3d_batch* b) {
     }
   }
   b->nentries = (int)ent.size();
-  if (b->d_jobs) cudaFree(b->d_jobs);
-  if (b->d_base) cudaFree(b->d_base);
   if (b->d_recjobs) cudaFree(b->d_recjobs);
   if (b->d_entries) cudaFree(b->d_entries);
-  b->d_jobs = nullptr;
-  b->d_base = nullptr;
   b->d_recjobs = nullptr;
   b->d_entries = nullptr;
-  const size_t jobs_bytes = 2 * (size_t)S * fb + (size_t)S * bb;
-  VTI_CUDA(ctx, cudaMalloc((void**)&b->d_jobs, jobs_bytes));
-  VTI_CUDA(ctx, cudaMalloc((void**)&b->d_base, base.size() * sizeof(int)));
   VTI_CUDA(ctx, cudaMalloc((void**)&b->d_recjobs, std::max<size_t>(rj.size(), 1) * sizeof(RecJob)));
   VTI_CUDA(ctx, cudaMalloc((void**)&b->d_entries,
                            std::max<size_t>(ent.size(), 1) * sizeof(RecEntry)));
-  VTI_CUDA(ctx, cudaMemcpy(b->d_base, base.data(), base.size() * sizeof(int),
-                           cudaMemcpyHostToDevice));
-  VTI_CUDA(ctx, cudaMemcpy(b->d_amp, amp.data(), amp.size() * sizeof(float),
-                           cudaMemcpyHostToDevice));
   if (!rj.empty())
     VTI_CUDA(ctx, cudaMemcpy(b->d_recjobs, rj.data(), rj.size() * sizeof(RecJob),
                              cudaMemcpyHostToDevice));
   if (!ent.empty())
     VTI_CUDA(ctx, cudaMemcpy(b->d_entries, ent.data(), ent.size() * sizeof(RecEntry),
                              cudaMemcpyHostToDevice));
-  VTI_CUDA(ctx, cudaMemcpy(b->d_jobs, h, jobs_bytes, cudaMemcpyHostToDevice));
   b->tables_ok = true;
   return VTI_OK;
 }
@@ -447,10 +426,10 @@ int cut_windows(vti3d_batch* b) {
 
 int forward_loop(vti3d_batch* b) {
   vti_ctx* ctx = b->ctx;
-  const int S = (int)b->plans.size(), M = levels(b);
+  const int M = levels(b);
   const int rgrid = (b->nentries + 255) / 256;
   for (int tick = 0; tick < M - 1; ++tick) {
-    VTI_TRY(launch_fwd3d_batch(ctx, b->d_jobs, b->d_base, 2 * S, b->items_fwd, tick));
+    VTI_TRY(step_batch_launch(ctx, b->fwd, tick));
     if (b->nentries > 0) {
       k_record_batch<<<rgrid, 256, 0, ctx->stream>>>(b->d_recjobs, b->d_entries, b->nentries,
                                                      tick);
@@ -462,11 +441,10 @@ int forward_loop(vti3d_batch* b) {
 
 int backward_loop(vti3d_batch* b) {
   vti_ctx* ctx = b->ctx;
-  const int S = (int)b->plans.size(), M = levels(b);
+  const int M = levels(b);
   const int rgrid = (b->nentries + 255) / 256;
-  const unsigned char* jobs = b->d_jobs + 2 * (size_t)S * fwd_job_bytes();
   for (int tick = 0; tick < M - 1; ++tick) {
-    VTI_TRY(launch_bwd3d_batch(ctx, jobs, b->d_base + 2 * S + 1, S, b->items_bwd, tick));
+    VTI_TRY(step_batch_launch(ctx, b->bwd, tick));
     if (b->nentries > 0) {
       k_inject_batch<<<rgrid, 256, 0, ctx->stream>>>(b->d_recjobs, b->d_entries, b->nentries,
                                                      tick);
@@ -498,7 +476,9 @@ int run_loop(vti3d_batch* b, int (*loop)(vti3d_batch*), cudaGraphExec_t* exec) {
     VTI_CUDA(ctx, ei);
   }
   VTI_CUDA(ctx, cudaGraphLaunch(*exec, ctx->stream));
-  ctx->launches += 2ull * (levels(b) - 1);  // kernels inside the graph
+  // kernels inside the graph: the step launches and the receiver kernel per tick
+  const StepBatch* sb = exec == &b->graph_fwd ? b->fwd : b->bwd;
+  ctx->launches += (uint64_t)(step_batch_launches(sb) + (b->nentries > 0)) * (levels(b) - 1);
   return VTI_OK;
 }
 
@@ -762,7 +742,6 @@ int vti3d_batch_autotune(vti3d_batch* b, int* seg_fwd, int* seg_bwd) {
   VTI_TRY(check_ready(b));
   VTI_CUDA(ctx, cudaSetDevice(ctx->device));
   VTI_TRY(cut_windows(b));
-  const int S = (int)b->plans.size();
   const int M = levels(b);
   const int reps = std::min(3, M - 1);
   const int nz = b->g.nz;
@@ -779,12 +758,8 @@ int vti3d_batch_autotune(vti3d_batch* b, int* seg_fwd, int* seg_bwd) {
       else b->seg_bwd = c;
       int st = build_tables(b);
       if (st != VTI_OK) break;
-      const unsigned char* jobs =
-          which == 0 ? b->d_jobs : b->d_jobs + 2 * (size_t)S * fwd_job_bytes();
       auto one = [&](int tick) {
-        return which == 0
-                   ? launch_fwd3d_batch(ctx, jobs, b->d_base, 2 * S, b->items_fwd, tick)
-                   : launch_bwd3d_batch(ctx, jobs, b->d_base + 2 * S + 1, S, b->items_bwd, tick);
+        return step_batch_launch(ctx, which == 0 ? b->fwd : b->bwd, tick);
       };
       VTI_TRY(one(0));  // warm-up
       VTI_CUDA(ctx, cudaEventRecord(e0, ctx->stream));

@@ -204,20 +204,19 @@ struct BwdJobSpec {
   int t0;
   int seg;
 };
-// Descriptor sizes (64-byte aligned) and builders: write the descriptor into
-// host memory dst and return the job's item count.
-size_t fwd_job_bytes();
-size_t bwd_job_bytes();
-int build_fwd_job(vti_ctx* ctx, const FwdJobSpec& spec, void* dst, int* items);
-int build_bwd_job(vti_ctx* ctx, const BwdJobSpec& spec, void* dst, int* items);
-// One launch over the items of njobs device descriptors; base: njobs+1
-// prefix sums of their item counts (device).
+// A batched step launch plan: the jobs' arguments as kernel parameter blocks
+// (chunks of at most 128 forward / 96 backward jobs, one launch each) and
+// their TMA descriptors on the device.
+struct StepBatch;
+int fwd_batch_build(vti_ctx* ctx, const FwdJobSpec* spec, int njobs, StepBatch** out);
+int bwd_batch_build(vti_ctx* ctx, const BwdJobSpec* spec, int njobs, StepBatch** out);
+// Launches every chunk for step `tick` on the context stream.
+int step_batch_launch(vti_ctx* ctx, StepBatch* b, int tick);
+// Kernel launches per step_batch_launch.
+int step_batch_launches(const StepBatch* b);
+void step_batch_free(StepBatch* b);
 // Sets the batched kernels' launch attributes (before any stream capture).
 int prepare_batch_kernels(vti_ctx* ctx);
-int launch_fwd3d_batch(vti_ctx* ctx, const void* d_jobs, const int* d_base, int njobs, int items,
-                       int tick);
-int launch_bwd3d_batch(vti_ctx* ctx, const void* d_jobs, const int* d_base, int njobs, int items,
-                       int tick);
 
 // Reads (and clears) the device status word; VTI_ERR_TIMEOUT if a bounded
 // device-side wait gave up since the last check.

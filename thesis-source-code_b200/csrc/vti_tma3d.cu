@@ -27,7 +27,8 @@
 // the reference is lib/vti-fwi-3d/gpu/kernel3d.cu:3-74,222-298 and
 // abc3d.cu:82-126.
 #include <algorithm>
-#include <new>
+#include <cstring>
+#include <vector>
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -53,9 +54,6 @@ constexpr int HX = TX + 2 * kHalo, HY = TY + 2 * kHalo;
 constexpr int PLAIN_BYTES = TX * TY * 4;  // 2048
 constexpr int HALO_BYTES = HX * HY * 4;   // 3840
 constexpr unsigned kSpinLimit = 1u << 26;
-// one 256-byte slot per consumer warp for the batched consumers' copy of the
-// job arguments
-constexpr int ARG_SLOT = 256;
 
 __device__ __forceinline__ float lap9(float c, float m1, float p1, float m2, float p2, float m3,
                                       float p3, float m4, float p4) {
@@ -131,35 +129,28 @@ __device__ __forceinline__ void item(const Sched& s, int i, int& bx, int& by, in
   z1 = min(s.nz, z0 + s.seg);
 }
 
-// Batched consumers: each warp copies its item's job arguments (global
-// memory) into its own shared-memory slot, so the item body reads them like
-// kernel parameters, without registers and without aliasing the output
-// stores. Only warp-level synchronisation: the lanes of a warp finish reading
-// the slot (previous item) before it is rewritten.
-template <typename Args>
-__device__ __forceinline__ const Args* stage_args(const Args& src, unsigned char* slot,
-                                                  int lane) {
-  static_assert(sizeof(Args) <= ARG_SLOT && sizeof(Args) % 4 == 0, "argument slot");
-  constexpr int kWords = (int)(sizeof(Args) / 4);
-  __syncwarp();
-  for (int t = lane; t < kWords; t += 32)
-    reinterpret_cast<uint32_t*>(slot)[t] = __ldg(reinterpret_cast<const uint32_t*>(&src) + t);
-  __syncwarp();
-  return reinterpret_cast<const Args*>(slot);
-}
-
 // ------------------------------------------------------------ forward
-struct FwdArgs {
+// Forward step arguments: the part every step of a job shares and the part
+// that alternates with the step parity (which buffer is cur / prev).
+struct FwdCommon {
   Dims3 d;
   Sched sc;
-  const float* cz;  // cur sigma_z (queue initialisation)
-  float* px;        // prev in / next out
-  float* pz;
   const float* dampx;  // null: no sponge
   const float* dampy;
   const float* dampz;
   float sx, sy, sz;
-  PointSource src;
+  PointSource src;     // amp: single launches only
+  const float* amp;    // batched: source amplitude per step
+  int t0;              // batched: tick of the job's step 0
+};
+struct FwdPar {
+  const float* cz;  // cur sigma_z (queue initialisation)
+  float* px;        // prev in / next out
+  float* pz;
+};
+struct FwdArgs {
+  FwdCommon c;
+  FwdPar p;
   Probe probe;
   int* status;
 };
@@ -172,47 +163,22 @@ constexpr int F_OFF_PX = F_OFF_Z + PLAIN_BYTES;
 constexpr int F_OFF_PZ = F_OFF_PX + PLAIN_BYTES;
 constexpr int F_OFF_C = F_OFF_PZ + PLAIN_BYTES;
 constexpr int F_STAGE_BYTES = F_OFF_C + 3 * PLAIN_BYTES;  // 15872
-constexpr int F_SMEM = F_STAGES * F_STAGE_BYTES + 1024 + 2 * F_STAGES * 8 + NCW * ARG_SLOT;
+constexpr int F_SMEM = F_STAGES * F_STAGE_BYTES + 1024 + 2 * F_STAGES * 8;
 
 struct FwdMaps {
   CUtensorMap cx, cz, px, pz, c11, c13, c33;
 };
 
-// A batched launch: items of job j are [base[j], base[j+1]); job j advances
-// its own step tick - t0, whose parity selects the buffer roles.
-struct JobTable {
-  const unsigned char* jobs;  // njobs descriptors of `stride` bytes
-  const int* base;            // njobs + 1 prefix sums of the jobs' items
-  int njobs, items, tick;
-};
-
-__device__ __forceinline__ int find_job(const JobTable& t, int item) {
-  int lo = 0, hi = t.njobs - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (__ldg(t.base + mid) <= item) lo = mid;
-    else hi = mid - 1;
-  }
-  return lo;
-}
-
-struct alignas(64) FwdJob {
-  FwdMaps m[2];  // by step parity
-  FwdArgs a[2];
-  const float* amp;  // source amplitude per step
-  int t0;
-};
-
 // Producer side of one item: TMA loads of every plane of the item's range.
-__device__ __forceinline__ bool fwd_produce(const FwdArgs& a, const FwdMaps& m, int li,
-                                            unsigned char* smem, uint64_t* full, uint64_t* empty,
-                                            long long& k) {
+__device__ __forceinline__ bool fwd_produce(const FwdCommon& a, const FwdMaps& m, int* status,
+                                            int li, unsigned char* smem, uint64_t* full,
+                                            uint64_t* empty, long long& k) {
   int bx, by, z0, z1;
   item(a.sc, li, bx, by, z0, z1);
   const int x0 = bx * TX, y0 = kHalo + by * TY;
   for (int z = z0; z < z1; ++z, ++k) {
     const int s = (int)(k % F_STAGES);
-    if (k >= F_STAGES && !mbar_wait(&empty[s], (uint32_t)(((k / F_STAGES) & 1) ^ 1), a.status))
+    if (k >= F_STAGES && !mbar_wait(&empty[s], (uint32_t)(((k / F_STAGES) & 1) ^ 1), status))
       return false;
     const int zp = z + kZPad;
     unsigned char* st = smem + s * F_STAGE_BYTES;
@@ -232,7 +198,8 @@ __device__ __forceinline__ bool fwd_produce(const FwdArgs& a, const FwdMaps& m, 
 // x0 + 2*(lane%16) + {0,1} of tile row 2*warp + lane/16; shared-memory reads
 // and global stores are float2.
 template <bool kProbe>
-__device__ __forceinline__ bool fwd_consume(const FwdArgs& a, int li, float amp,
+__device__ __forceinline__ bool fwd_consume(const FwdCommon& a, const FwdPar& bp,
+                                            const Probe& probe, int* status, int li, float amp,
                                             const unsigned char* smem, uint64_t* full,
                                             uint64_t* empty, long long& k, int warp, int lane) {
   const bool damp = a.dampz != nullptr;
@@ -252,7 +219,7 @@ __device__ __forceinline__ bool fwd_consume(const FwdArgs& a, int li, float amp,
   const int off = y * a.d.pitch + x;  // x + 1 < pitch: 32 * gx <= pitch
   // which of this thread's two points (0, 1; else -1) holds the source / probe
   const int src_e = (y == a.src.y && a.src.x >= 0) ? a.src.x - x : -1;
-  const int prb_e = (kProbe && y == a.probe.y && a.probe.x >= 0) ? a.probe.x - x : -1;
+  const int prb_e = (kProbe && y == probe.y && probe.x >= 0) ? probe.x - x : -1;
   dxy[0] = (damp && v0) ? a.dampx[x] * a.dampy[y] : 1.f;
   dxy[1] = (damp && v1) ? a.dampx[x + 1] * a.dampy[y] : 1.f;
   // start the queue: planes z0-4 .. z0+3 from global
@@ -261,7 +228,7 @@ __device__ __forceinline__ bool fwd_consume(const FwdArgs& a, int li, float amp,
   for (int kk = 1; kk < 9; ++kk) {
     const int zz = z0 - 5 + kk;
     float2 v = (v0 || v1)
-                   ? __ldg(reinterpret_cast<const float2*>(a.cz + (long long)zz * a.d.plane + off))
+                   ? __ldg(reinterpret_cast<const float2*>(bp.cz + (long long)zz * a.d.plane + off))
                    : make_float2(0.f, 0.f);
     // planes of the block above z0 were already damped as "cur"
     if (damp && zz >= 0 && (zz >> 2) < (z0 >> 2)) {
@@ -285,7 +252,7 @@ __device__ __forceinline__ bool fwd_consume(const FwdArgs& a, int li, float amp,
     for (int j = 0; j < 3; ++j) dzr[j] = dzr[j + 1];
     dzr[3] = dz;
     const int s = (int)(k % F_STAGES);
-    if (!mbar_wait(&full[s], (uint32_t)((k / F_STAGES) & 1), a.status)) return false;
+    if (!mbar_wait(&full[s], (uint32_t)((k / F_STAGES) & 1), status)) return false;
     const unsigned char* st = smem + s * F_STAGE_BYTES;
     const float* sh = (const float*)(st + F_OFF_H) + sr;
     const float* pl = (const float*)(st + F_OFF_Z) + pi;  // [z+4][prev x][prev z][c11][c13][c33]
@@ -333,7 +300,7 @@ __device__ __forceinline__ bool fwd_consume(const FwdArgs& a, int li, float amp,
       const float a11 = pick(c11), a13 = pick(c13), a33 = pick(c33);
       nxv[e] = fmaf(a11, lxy, fmaf(a13, lz, 2.f * c - dd * pick(px)));
       nzv[e] = fmaf(a13, lxy, fmaf(a33, lz, 2.f * q[e][4] - dd * pick(pz)));
-      if (kProbe && prb_e == e && z == a.probe.z) *a.probe.out += nxv[e] + nzv[e];
+      if (kProbe && prb_e == e && z == probe.z) *probe.out += nxv[e] + nzv[e];
       if (src_e == e && z == a.src.z) {
         nxv[e] += amp;
         nzv[e] += amp;
@@ -343,16 +310,16 @@ __device__ __forceinline__ bool fwd_consume(const FwdArgs& a, int li, float amp,
     }
     const long long i = (long long)z * a.d.plane + off;
     if (v0 && v1) {
-      *reinterpret_cast<float2*>(a.px + i) = make_float2(nxv[0], nxv[1]);
-      *reinterpret_cast<float2*>(a.pz + i) = make_float2(nzv[0], nzv[1]);
+      *reinterpret_cast<float2*>(bp.px + i) = make_float2(nxv[0], nxv[1]);
+      *reinterpret_cast<float2*>(bp.pz + i) = make_float2(nzv[0], nzv[1]);
     } else {
       if (v0) {
-        a.px[i] = nxv[0];
-        a.pz[i] = nzv[0];
+        bp.px[i] = nxv[0];
+        bp.pz[i] = nzv[0];
       }
       if (v1) {
-        a.px[i + 1] = nxv[1];
-        a.pz[i + 1] = nzv[1];
+        bp.px[i + 1] = nxv[1];
+        bp.pz[i + 1] = nzv[1];
       }
     }
     // entering the next plane: if it starts a new 4-plane block of the same
@@ -370,74 +337,108 @@ __device__ __forceinline__ bool fwd_consume(const FwdArgs& a, int li, float amp,
   return true;
 }
 
-// kProbe: the probe point of FwdArgs is read out (wavelet gradient); the
-// propagation kernels are instantiated without it. kBatch: the items of all
-// jobs of `jt` (descriptors in global memory) instead of the single job
-// (m0, a0).
-template <bool kProbe, bool kBatch>
-__global__ void __launch_bounds__(NTHREADS, 3)
-    k_fwd3d_tma(const __grid_constant__ FwdMaps m0, const __grid_constant__ FwdArgs a0,
-                const JobTable jt) {
-  extern __shared__ unsigned char smem_raw[];
+// Kernel prologue shared by the step kernels: 1024-aligned stage ring and
+// its full/empty mbarriers.
+template <int kStages, int kStageBytes>
+__device__ __forceinline__ unsigned char* ring_init(unsigned char* smem_raw, uint64_t*& full,
+                                                    uint64_t*& empty) {
   unsigned char* smem =
       (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  uint64_t* full = (uint64_t*)(smem + F_STAGES * F_STAGE_BYTES);
-  uint64_t* empty = full + F_STAGES;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  full = (uint64_t*)(smem + kStages * kStageBytes);
+  empty = full + kStages;
   if (threadIdx.x == 0) {
-    for (int s = 0; s < F_STAGES; ++s) {
+    for (int s = 0; s < kStages; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], NCW);
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  const int items = kBatch ? jt.items : a0.sc.items;
+  return smem;
+}
+
+// kProbe: the probe point of FwdArgs is read out (wavelet gradient); the
+// propagation kernels are instantiated without it.
+template <bool kProbe>
+__global__ void __launch_bounds__(NTHREADS, 3)
+    k_fwd3d_tma(const __grid_constant__ FwdMaps m0, const __grid_constant__ FwdArgs a0) {
+  extern __shared__ unsigned char smem_raw[];
+  uint64_t *full, *empty;
+  unsigned char* smem = ring_init<F_STAGES, F_STAGE_BYTES>(smem_raw, full, empty);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   long long k = 0;  // planes issued / consumed by this CTA
   if (warp == NCW) {  // ---------------- producer
-    if (lane == 0) {
-      for (int it = blockIdx.x; it < items; it += gridDim.x) {
-        bool ok;
-        if constexpr (kBatch) {
-          const int j = find_job(jt, it);
-          const FwdJob& J = reinterpret_cast<const FwdJob*>(jt.jobs)[j];
-          const int par = (jt.tick - J.t0) & 1;
-          ok = fwd_produce(J.a[par], J.m[par], it - jt.base[j], smem, full, empty, k);
-        } else {
-          ok = fwd_produce(a0, m0, it, smem, full, empty, k);
-        }
-        if (!ok) break;
-      }
-    }
+    if (lane == 0)
+      for (int it = blockIdx.x; it < a0.c.sc.items; it += gridDim.x)
+        if (!fwd_produce(a0.c, m0, a0.status, it, smem, full, empty, k)) break;
     return;
   }
-  unsigned char* slot = (unsigned char*)(empty + F_STAGES) + warp * ARG_SLOT;
-  for (int it = blockIdx.x; it < items; it += gridDim.x) {
-    bool ok;
-    if constexpr (kBatch) {
-      const int j = find_job(jt, it);
-      const FwdJob& J = reinterpret_cast<const FwdJob*>(jt.jobs)[j];
-      const int step = jt.tick - J.t0;
-      const FwdArgs* a = stage_args(J.a[step & 1], slot, lane);
-      ok = fwd_consume<kProbe>(*a, it - jt.base[j], __ldg(J.amp + step), smem, full, empty, k,
-                               warp, lane);
-    } else {
-      ok = fwd_consume<kProbe>(a0, it, a0.src.amp, smem, full, empty, k, warp, lane);
-    }
-    if (!ok) break;
+  for (int it = blockIdx.x; it < a0.c.sc.items; it += gridDim.x)
+    if (!fwd_consume<kProbe>(a0.c, a0.p, a0.probe, a0.status, it, a0.c.src.amp, smem, full,
+                             empty, k, warp, lane))
+      break;
+}
+
+// Batched launches: the arguments of up to kMaxFwdJobs jobs travel as kernel
+// parameters (constant bank), indexed by a job number that is uniform over
+// the CTA, so the item bodies read them as they read a single launch's
+// parameters. Job j's items are [base[j], base[j+1]); its step is
+// tick - t0, whose parity selects the buffer roles. The TMA descriptors
+// (2 per job) are in global memory.
+constexpr int kMaxFwdJobs = 128;
+constexpr int kMaxBwdJobs = 96;
+
+struct FwdBatch {
+  const FwdMaps* maps;  // [2 * job + parity]
+  int* status;
+  int njobs, items, tick;
+  int base[kMaxFwdJobs + 1];
+  FwdCommon c[kMaxFwdJobs];
+  FwdPar p[kMaxFwdJobs][2];
+};
+
+template <typename Batch>
+__device__ __forceinline__ int find_job(const Batch& b, int item) {
+  int lo = 0, hi = b.njobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (b.base[mid] <= item) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(NTHREADS, 3) k_fwd3d_batch(const __grid_constant__ FwdBatch B) {
+  extern __shared__ unsigned char smem_raw[];
+  uint64_t *full, *empty;
+  unsigned char* smem = ring_init<F_STAGES, F_STAGE_BYTES>(smem_raw, full, empty);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  long long k = 0;
+  if (warp == NCW) {
+    if (lane == 0)
+      for (int it = blockIdx.x; it < B.items; it += gridDim.x) {
+        const int j = find_job(B, it);
+        const int par = (B.tick - B.c[j].t0) & 1;
+        if (!fwd_produce(B.c[j], B.maps[2 * j + par], B.status, it - B.base[j], smem, full,
+                         empty, k))
+          break;
+      }
+    return;
+  }
+  const Probe none;
+  for (int it = blockIdx.x; it < B.items; it += gridDim.x) {
+    const int j = find_job(B, it);
+    const int step = B.tick - B.c[j].t0;
+    if (!fwd_consume<false>(B.c[j], B.p[j][step & 1], none, B.status, it - B.base[j],
+                            __ldg(B.c[j].amp + step), smem, full, empty, k, warp, lane))
+      break;
   }
 }
 
 // ------------------------------------------------------------ backward
-struct BwdArgs {
+struct BwdCommon {
   Dims3 d;
   Sched sc;
-  const float* scz;  // cur sigma_z, lambda_z (queue initialisation)
-  const float* lcz;
-  float* spx;        // prev in / next out
-  float* spz;
-  float* lpx;
-  float* lpz;
   float* g11;
   float* g13;
   float* g33;
@@ -447,6 +448,20 @@ struct BwdArgs {
   float dt2, idx2, idy2, idz2;
   float sx, sy, sz;
   PointSource src;
+  const float* amp;
+  int t0;
+};
+struct BwdPar {
+  const float* scz;  // cur sigma_z, lambda_z (queue initialisation)
+  const float* lcz;
+  float* spx;        // prev in / next out
+  float* spz;
+  float* lpx;
+  float* lpz;
+};
+struct BwdArgs {
+  BwdCommon c;
+  BwdPar p;
   int* status;
 };
 
@@ -456,7 +471,7 @@ constexpr int B_OFF_SH = 0;
 constexpr int B_OFF_LH = HALO_BYTES;
 constexpr int B_OFF_P = 2 * HALO_BYTES;  // 10 plain tiles from here
 constexpr int B_STAGE_BYTES = B_OFF_P + 12 * PLAIN_BYTES;  // 32256
-constexpr int B_SMEM = B_STAGES * B_STAGE_BYTES + 1024 + 2 * B_STAGES * 8 + NCW * ARG_SLOT;
+constexpr int B_SMEM = B_STAGES * B_STAGE_BYTES + 1024 + 2 * B_STAGES * 8;
 
 struct BwdMaps {
   CUtensorMap scx, scz, spx, spz, lcx, lcz, lpx, lpz, c11, c13, c33, g11, g13, g33;
@@ -465,23 +480,16 @@ struct BwdMaps {
 // wave3d.h:5-6 recording / imaging weights, as float
 constexpr float kTwoThirdF = (float)kTwoThird, kOneThirdF = (float)kOneThird;
 
-struct alignas(64) BwdJob {
-  BwdMaps m[2];  // by step parity
-  BwdArgs a[2];
-  const float* amp;  // source amplitude per step
-  int t0;
-};
-
 template <bool kRtm>
-__device__ __forceinline__ bool bwd_produce(const BwdArgs& a, const BwdMaps& m, int li,
-                                            unsigned char* smem, uint64_t* full, uint64_t* empty,
-                                            long long& k) {
+__device__ __forceinline__ bool bwd_produce(const BwdCommon& a, const BwdMaps& m, int* status,
+                                            int li, unsigned char* smem, uint64_t* full,
+                                            uint64_t* empty, long long& k) {
   int bx, by, z0, z1;
   item(a.sc, li, bx, by, z0, z1);
   const int x0 = bx * TX, y0 = kHalo + by * TY;
   for (int z = z0; z < z1; ++z, ++k) {
     const int s = (int)(k % B_STAGES);
-    if (k >= B_STAGES && !mbar_wait(&empty[s], (uint32_t)(((k / B_STAGES) & 1) ^ 1), a.status))
+    if (k >= B_STAGES && !mbar_wait(&empty[s], (uint32_t)(((k / B_STAGES) & 1) ^ 1), status))
       return false;
     const int zp = z + kZPad;
     unsigned char* st = smem + s * B_STAGE_BYTES;
@@ -509,9 +517,10 @@ __device__ __forceinline__ bool bwd_produce(const BwdArgs& a, const BwdMaps& m, 
 
 // Consumers: the x pair x0 + 2*(lane%16) + {0,1} of tile row 2*warp + lane/16.
 template <bool kRtm>
-__device__ __forceinline__ bool bwd_consume(const BwdArgs& a, int li, float amp,
-                                            const unsigned char* smem, uint64_t* full,
-                                            uint64_t* empty, long long& k, int warp, int lane) {
+__device__ __forceinline__ bool bwd_consume(const BwdCommon& a, const BwdPar& bp, int* status,
+                                            int li, float amp, const unsigned char* smem,
+                                            uint64_t* full, uint64_t* empty, long long& k,
+                                            int warp, int lane) {
   const int ry = warp * 2 + (lane >> 4);
   const int xo = 2 * (lane & 15);
   const int sr = (ry + kHalo) * HX + xo + kHalo;
@@ -536,8 +545,8 @@ __device__ __forceinline__ bool bwd_consume(const BwdArgs& a, int li, float amp,
     const long long i = (long long)zz * a.d.plane + off;
     const bool any = v0 || v1;
     const float2 sv =
-        any ? __ldg(reinterpret_cast<const float2*>(a.scz + i)) : make_float2(0.f, 0.f);
-    float2 lv = any ? __ldg(reinterpret_cast<const float2*>(a.lcz + i)) : make_float2(0.f, 0.f);
+        any ? __ldg(reinterpret_cast<const float2*>(bp.scz + i)) : make_float2(0.f, 0.f);
+    float2 lv = any ? __ldg(reinterpret_cast<const float2*>(bp.lcz + i)) : make_float2(0.f, 0.f);
     if (zz >= 0 && (zz >> 2) < (z0 >> 2)) {
       lv.x *= dxy[0] * a.dampz[zz];
       lv.y *= dxy[1] * a.dampz[zz];
@@ -559,7 +568,7 @@ __device__ __forceinline__ bool bwd_consume(const BwdArgs& a, int li, float amp,
     for (int j = 0; j < 3; ++j) dzr[j] = dzr[j + 1];
     dzr[3] = dz;
     const int s = (int)(k % B_STAGES);
-    if (!mbar_wait(&full[s], (uint32_t)((k / B_STAGES) & 1), a.status)) return false;
+    if (!mbar_wait(&full[s], (uint32_t)((k / B_STAGES) & 1), status)) return false;
     const unsigned char* st = smem + s * B_STAGE_BYTES;
     const float* sh = (const float*)(st + B_OFF_SH) + sr;
     const float* lh = (const float*)(st + B_OFF_LH) + sr;
@@ -652,10 +661,10 @@ __device__ __forceinline__ bool bwd_consume(const BwdArgs& a, int li, float amp,
     }
     const long long i = (long long)z * a.d.plane + off;
     if (v0 && v1) {
-      *reinterpret_cast<float2*>(a.spx + i) = make_float2(snx[0], snx[1]);
-      *reinterpret_cast<float2*>(a.spz + i) = make_float2(snz[0], snz[1]);
-      *reinterpret_cast<float2*>(a.lpx + i) = make_float2(lnx[0], lnx[1]);
-      *reinterpret_cast<float2*>(a.lpz + i) = make_float2(lnz[0], lnz[1]);
+      *reinterpret_cast<float2*>(bp.spx + i) = make_float2(snx[0], snx[1]);
+      *reinterpret_cast<float2*>(bp.spz + i) = make_float2(snz[0], snz[1]);
+      *reinterpret_cast<float2*>(bp.lpx + i) = make_float2(lnx[0], lnx[1]);
+      *reinterpret_cast<float2*>(bp.lpz + i) = make_float2(lnz[0], lnz[1]);
       *reinterpret_cast<float2*>(a.g11 + i) = make_float2(g11[0], g11[1]);
       if (!kRtm) {
         *reinterpret_cast<float2*>(a.g13 + i) = make_float2(g13[0], g13[1]);
@@ -665,10 +674,10 @@ __device__ __forceinline__ bool bwd_consume(const BwdArgs& a, int li, float amp,
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
         if (e ? v1 : v0) {
-          a.spx[i + e] = snx[e];
-          a.spz[i + e] = snz[e];
-          a.lpx[i + e] = lnx[e];
-          a.lpz[i + e] = lnz[e];
+          bp.spx[i + e] = snx[e];
+          bp.spz[i + e] = snz[e];
+          bp.lpx[i + e] = lnx[e];
+          bp.lpz[i + e] = lnz[e];
           a.g11[i + e] = g11[e];
           if (!kRtm) {
             a.g13[i + e] = g13[e];
@@ -692,60 +701,63 @@ __device__ __forceinline__ bool bwd_consume(const BwdArgs& a, int li, float amp,
 // rtm3d_f.cu:607-610): one image volume, kept in the g11 slot, gains
 // (2/3 sx + 1/3 sz)(2/3 lx + 1/3 lz) with both fields at the current level and
 // the adjoint already multiplied by this step's sponge; g13/g33 are neither
-// loaded nor written. kBatch: the items of all jobs of `jt`.
-template <bool kRtm, bool kBatch>
+// loaded nor written.
+template <bool kRtm>
 __global__ void __launch_bounds__(NTHREADS, 2)
-    k_bwd3d_tma(const __grid_constant__ BwdMaps m0, const __grid_constant__ BwdArgs a0,
-                const JobTable jt) {
+    k_bwd3d_tma(const __grid_constant__ BwdMaps m0, const __grid_constant__ BwdArgs a0) {
   extern __shared__ unsigned char smem_raw[];
-  unsigned char* smem =
-      (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  uint64_t* full = (uint64_t*)(smem + B_STAGES * B_STAGE_BYTES);
-  uint64_t* empty = full + B_STAGES;
+  uint64_t *full, *empty;
+  unsigned char* smem = ring_init<B_STAGES, B_STAGE_BYTES>(smem_raw, full, empty);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < B_STAGES; ++s) {
-      mbar_init(&full[s], 1);
-      mbar_init(&empty[s], NCW);
-    }
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  __syncthreads();
-  const int items = kBatch ? jt.items : a0.sc.items;
   long long k = 0;
-  if (warp == NCW) {  // ---------------- producer
-    if (lane == 0) {
-      for (int it = blockIdx.x; it < items; it += gridDim.x) {
-        bool ok;
-        if constexpr (kBatch) {
-          const int j = find_job(jt, it);
-          const BwdJob& J = reinterpret_cast<const BwdJob*>(jt.jobs)[j];
-          const int par = (jt.tick - J.t0) & 1;
-          ok = bwd_produce<kRtm>(J.a[par], J.m[par], it - jt.base[j], smem, full, empty, k);
-        } else {
-          ok = bwd_produce<kRtm>(a0, m0, it, smem, full, empty, k);
-        }
-        if (!ok) break;
-      }
-    }
+  if (warp == NCW) {
+    if (lane == 0)
+      for (int it = blockIdx.x; it < a0.c.sc.items; it += gridDim.x)
+        if (!bwd_produce<kRtm>(a0.c, m0, a0.status, it, smem, full, empty, k)) break;
     return;
   }
-  unsigned char* slot = (unsigned char*)(empty + B_STAGES) + warp * ARG_SLOT;
-  for (int it = blockIdx.x; it < items; it += gridDim.x) {
-    bool ok;
-    if constexpr (kBatch) {
-      const int j = find_job(jt, it);
-      const BwdJob& J = reinterpret_cast<const BwdJob*>(jt.jobs)[j];
-      const int step = jt.tick - J.t0;
-      const BwdArgs* a = stage_args(J.a[step & 1], slot, lane);
-      ok = bwd_consume<kRtm>(*a, it - jt.base[j], __ldg(J.amp + step), smem, full, empty, k,
-                             warp, lane);
-    } else {
-      ok = bwd_consume<kRtm>(a0, it, a0.src.amp, smem, full, empty, k, warp, lane);
-    }
-    if (!ok) break;
+  for (int it = blockIdx.x; it < a0.c.sc.items; it += gridDim.x)
+    if (!bwd_consume<kRtm>(a0.c, a0.p, a0.status, it, a0.c.src.amp, smem, full, empty, k, warp,
+                           lane))
+      break;
+}
+
+struct BwdBatch {
+  const BwdMaps* maps;  // [2 * job + parity]
+  int* status;
+  int njobs, items, tick;
+  int base[kMaxBwdJobs + 1];
+  BwdCommon c[kMaxBwdJobs];
+  BwdPar p[kMaxBwdJobs][2];
+};
+
+__global__ void __launch_bounds__(NTHREADS, 2) k_bwd3d_batch(const __grid_constant__ BwdBatch B) {
+  extern __shared__ unsigned char smem_raw[];
+  uint64_t *full, *empty;
+  unsigned char* smem = ring_init<B_STAGES, B_STAGE_BYTES>(smem_raw, full, empty);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  long long k = 0;
+  if (warp == NCW) {
+    if (lane == 0)
+      for (int it = blockIdx.x; it < B.items; it += gridDim.x) {
+        const int j = find_job(B, it);
+        const int par = (B.tick - B.c[j].t0) & 1;
+        if (!bwd_produce<false>(B.c[j], B.maps[2 * j + par], B.status, it - B.base[j], smem,
+                                full, empty, k))
+          break;
+      }
+    return;
+  }
+  for (int it = blockIdx.x; it < B.items; it += gridDim.x) {
+    const int j = find_job(B, it);
+    const int step = B.tick - B.c[j].t0;
+    if (!bwd_consume<false>(B.c[j], B.p[j][step & 1], B.status, it - B.base[j],
+                            __ldg(B.c[j].amp + step), smem, full, empty, k, warp, lane))
+      break;
   }
 }
+
+static_assert(sizeof(FwdBatch) <= 32000 && sizeof(BwdBatch) <= 32000, "kernel parameter size");
 
 // ------------------------------------------------------------ host side
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
@@ -840,26 +852,23 @@ int set_smem_attr(vti_ctx* ctx, K kern, int bytes, bool* done) {
   return VTI_OK;
 }
 
-FwdArgs fwd_args(vti_ctx* ctx, const Dims3& d, const Sched& sc, const float* cz_ptr,
-                 float* px_ptr, float* pz_ptr, const Damping* damp, float sx, float sy,
-                 float sz, PointSource src) {
-  FwdArgs a;
-  a.d = d;
-  a.sc = sc;
-  a.cz = cz_ptr;
-  a.px = px_ptr;
-  a.pz = pz_ptr;
-  a.dampx = damp ? damp->x : nullptr;
-  a.dampy = damp ? damp->y : nullptr;
-  a.dampz = damp ? damp->z : nullptr;
-  a.sx = sx;
-  a.sy = sy;
-  a.sz = sz;
-  a.src = src;
-  a.probe = Probe();
-  a.status = ctx->d_status;
-  return a;
+FwdCommon fwd_common(const Dims3& d, const Sched& sc, const Damping* damp, float sx, float sy,
+                     float sz, PointSource src) {
+  FwdCommon c{};
+  c.d = d;
+  c.sc = sc;
+  c.dampx = damp ? damp->x : nullptr;
+  c.dampy = damp ? damp->y : nullptr;
+  c.dampz = damp ? damp->z : nullptr;
+  c.sx = sx;
+  c.sy = sy;
+  c.sz = sz;
+  c.src = src;
+  return c;
 }
+
+bool attr_fwd[2][64] = {}, attr_bwd[2][64] = {}, attr_fwd_batch[64] = {},
+     attr_bwd_batch[64] = {};
 
 }  // namespace
 
@@ -869,21 +878,21 @@ int launch_fwd3d_tma(vti_ctx* ctx, const Dims3& d, const TileMaps& cx, const Til
                      float* px_ptr, float* pz_ptr, const Damping* damp, float sx, float sy,
                      float sz, PointSource src, Probe probe) {
   const bool pr = probe.x >= 0 && probe.out;
-  static bool attr[2][64] = {};  // per instantiation and device
-  VTI_TRY_ST(set_smem_attr(ctx, pr ? k_fwd3d_tma<true, false> : k_fwd3d_tma<false, false>,
-                           F_SMEM, attr[pr]));
+  VTI_TRY_ST(set_smem_attr(ctx, pr ? k_fwd3d_tma<true> : k_fwd3d_tma<false>, F_SMEM,
+                           attr_fwd[pr]));
   FwdMaps m;
   m.cx = *H(cx); m.cz = *P(cz); m.px = *P(px); m.pz = *P(pz);
   m.c11 = *P(c11); m.c13 = *P(c13); m.c33 = *P(c33);
-  FwdArgs a = fwd_args(ctx, d, make_sched(ctx, d, 3), cz_ptr, px_ptr, pz_ptr, damp, sx, sy, sz,
-                       src);
+  FwdArgs a{};
+  a.c = fwd_common(d, make_sched(ctx, d, 3), damp, sx, sy, sz, src);
+  a.p = FwdPar{cz_ptr, px_ptr, pz_ptr};
   a.probe = probe;
-  JobTable jt{};
-  const int grid = a.sc.grid;
+  a.status = ctx->d_status;
+  const int grid = a.c.sc.grid;
   {
     LaunchTimer tm(ctx, kTimedFwd3d);
-    auto kern = pr ? k_fwd3d_tma<true, false> : k_fwd3d_tma<false, false>;
-    kern<<<grid, NTHREADS, F_SMEM, ctx->stream>>>(m, a, jt);
+    auto kern = pr ? k_fwd3d_tma<true> : k_fwd3d_tma<false>;
+    kern<<<grid, NTHREADS, F_SMEM, ctx->stream>>>(m, a);
   }
   VTI_LAUNCHED(ctx, "k_fwd3d_tma");
   return VTI_OK;
@@ -898,131 +907,197 @@ int launch_bwd3d_tma(vti_ctx* ctx, const Dims3& d, const TileMaps& scx, const Ti
                      float* lpx_ptr, float* lpz_ptr, float* g11_ptr, float* g13_ptr,
                      float* g33_ptr, const Damping& damp, float dt2, float idx2, float idy2,
                      float idz2, float sx, float sy, float sz, PointSource src, bool rtm) {
-  static bool attr[2][64] = {};  // per instantiation and device
-  VTI_TRY_ST(set_smem_attr(ctx, rtm ? k_bwd3d_tma<true, false> : k_bwd3d_tma<false, false>,
-                           B_SMEM, attr[rtm]));
+  VTI_TRY_ST(set_smem_attr(ctx, rtm ? k_bwd3d_tma<true> : k_bwd3d_tma<false>, B_SMEM,
+                           attr_bwd[rtm]));
   BwdMaps m;
   m.scx = *H(scx); m.scz = *P(scz); m.spx = *P(spx); m.spz = *P(spz);
   m.lcx = *H(lcx); m.lcz = *P(lcz); m.lpx = *P(lpx); m.lpz = *P(lpz);
   m.c11 = *P(c11); m.c13 = *P(c13); m.c33 = *P(c33);
   m.g11 = *P(g11); m.g13 = *P(g13); m.g33 = *P(g33);
-  BwdArgs a;
-  a.d = d;
-  a.sc = make_sched(ctx, d, 2);
-  a.scz = scz_ptr; a.lcz = lcz_ptr;
-  a.spx = spx_ptr; a.spz = spz_ptr; a.lpx = lpx_ptr; a.lpz = lpz_ptr;
-  a.g11 = g11_ptr; a.g13 = g13_ptr; a.g33 = g33_ptr;
-  a.dampx = damp.x; a.dampy = damp.y; a.dampz = damp.z;
-  a.dt2 = dt2; a.idx2 = idx2; a.idy2 = idy2; a.idz2 = idz2;
-  a.sx = sx; a.sy = sy; a.sz = sz;
-  a.src = src;
+  BwdArgs a{};
+  BwdCommon& c = a.c;
+  c.d = d;
+  c.sc = make_sched(ctx, d, 2);
+  c.g11 = g11_ptr; c.g13 = g13_ptr; c.g33 = g33_ptr;
+  c.dampx = damp.x; c.dampy = damp.y; c.dampz = damp.z;
+  c.dt2 = dt2; c.idx2 = idx2; c.idy2 = idy2; c.idz2 = idz2;
+  c.sx = sx; c.sy = sy; c.sz = sz;
+  c.src = src;
+  a.p = BwdPar{scz_ptr, lcz_ptr, spx_ptr, spz_ptr, lpx_ptr, lpz_ptr};
   a.status = ctx->d_status;
-  JobTable jt{};
-  const int grid = a.sc.grid;
+  const int grid = c.sc.grid;
   {
     LaunchTimer tm(ctx, kTimedBwd3d);
     if (rtm)
-      k_bwd3d_tma<true, false><<<grid, NTHREADS, B_SMEM, ctx->stream>>>(m, a, jt);
+      k_bwd3d_tma<true><<<grid, NTHREADS, B_SMEM, ctx->stream>>>(m, a);
     else
-      k_bwd3d_tma<false, false><<<grid, NTHREADS, B_SMEM, ctx->stream>>>(m, a, jt);
+      k_bwd3d_tma<false><<<grid, NTHREADS, B_SMEM, ctx->stream>>>(m, a);
   }
   VTI_LAUNCHED(ctx, "k_bwd3d_tma");
   return VTI_OK;
 }
 
-// ------------------------------------------------------------ batched jobs
-size_t fwd_job_bytes() { return sizeof(FwdJob); }
-size_t bwd_job_bytes() { return sizeof(BwdJob); }
-
-int build_fwd_job(vti_ctx* ctx, const FwdJobSpec& sp, void* dst, int* items) {
-  if (((uintptr_t)dst & 63) != 0) return fail(ctx, VTI_ERR_ARG, "job descriptor not aligned");
-  FwdJob* J = new (dst) FwdJob();
-  const Sched sc = sp.seg > 0 ? sched_with_seg(sp.d, sp.seg) : make_sched(ctx, sp.d, 3);
-  for (int p = 0; p < 2; ++p) {
-    FwdMaps& m = J->m[p];
-    m.cx = *H(*sp.cx[p]); m.cz = *P(*sp.cz[p]); m.px = *P(*sp.px[p]); m.pz = *P(*sp.pz[p]);
-    m.c11 = *P(*sp.c[0]); m.c13 = *P(*sp.c[1]); m.c33 = *P(*sp.c[2]);
-    PointSource src;
-    src.x = sp.src_x; src.y = sp.src_y; src.z = sp.src_z;
-    J->a[p] = fwd_args(ctx, sp.d, sc, sp.cz_ptr[p], sp.px_ptr[p], sp.pz_ptr[p], sp.damp, sp.sx,
-                       sp.sy, sp.sz, src);
-  }
-  J->amp = sp.amp;
-  J->t0 = sp.t0;
-  *items = sc.items;
-  return VTI_OK;
-}
-
-int build_bwd_job(vti_ctx* ctx, const BwdJobSpec& sp, void* dst, int* items) {
-  if (((uintptr_t)dst & 63) != 0) return fail(ctx, VTI_ERR_ARG, "job descriptor not aligned");
-  BwdJob* J = new (dst) BwdJob();
-  const Sched sc = sp.seg > 0 ? sched_with_seg(sp.d, sp.seg) : make_sched(ctx, sp.d, 2);
-  for (int p = 0; p < 2; ++p) {
-    BwdMaps& m = J->m[p];
-    m.scx = *H(*sp.scx[p]); m.scz = *P(*sp.scz[p]); m.spx = *P(*sp.spx[p]);
-    m.spz = *P(*sp.spz[p]);
-    m.lcx = *H(*sp.lcx[p]); m.lcz = *P(*sp.lcz[p]); m.lpx = *P(*sp.lpx[p]);
-    m.lpz = *P(*sp.lpz[p]);
-    m.c11 = *P(*sp.c[0]); m.c13 = *P(*sp.c[1]); m.c33 = *P(*sp.c[2]);
-    m.g11 = *P(*sp.g[0]); m.g13 = *P(*sp.g[1]); m.g33 = *P(*sp.g[2]);
-    BwdArgs& a = J->a[p];
-    a.d = sp.d;
-    a.sc = sc;
-    a.scz = sp.scz_ptr[p]; a.lcz = sp.lcz_ptr[p];
-    a.spx = sp.spx_ptr[p]; a.spz = sp.spz_ptr[p]; a.lpx = sp.lpx_ptr[p]; a.lpz = sp.lpz_ptr[p];
-    a.g11 = sp.g_ptr[0]; a.g13 = sp.g_ptr[1]; a.g33 = sp.g_ptr[2];
-    a.dampx = sp.damp.x; a.dampy = sp.damp.y; a.dampz = sp.damp.z;
-    a.dt2 = sp.dt2; a.idx2 = sp.idx2; a.idy2 = sp.idy2; a.idz2 = sp.idz2;
-    a.sx = sp.sx; a.sy = sp.sy; a.sz = sp.sz;
-    a.src.x = sp.src_x; a.src.y = sp.src_y; a.src.z = sp.src_z; a.src.amp = 0.f;
-    a.status = ctx->d_status;
-  }
-  J->amp = sp.amp;
-  J->t0 = sp.t0;
-  *items = sc.items;
-  return VTI_OK;
-}
-
-namespace {
-bool attr_fwd_batch[64] = {}, attr_bwd_batch[64] = {};
-}  // namespace
+// ------------------------------------------------------------ batched steps
+// A batched step: its jobs in chunks of at most kMax*Jobs, one launch each.
+struct StepBatch {
+  bool fwd = true;
+  std::vector<FwdBatch> fb;  // host parameter blocks, one per chunk
+  std::vector<BwdBatch> bb;
+  std::vector<void*> d_maps;  // device TMA descriptors of each chunk
+  int items = 0;
+};
 
 int prepare_batch_kernels(vti_ctx* ctx) {
-  VTI_TRY_ST(set_smem_attr(ctx, k_fwd3d_tma<false, true>, F_SMEM, attr_fwd_batch));
-  VTI_TRY_ST(set_smem_attr(ctx, k_bwd3d_tma<false, true>, B_SMEM, attr_bwd_batch));
+  VTI_TRY_ST(set_smem_attr(ctx, k_fwd3d_batch, F_SMEM, attr_fwd_batch));
+  VTI_TRY_ST(set_smem_attr(ctx, k_bwd3d_batch, B_SMEM, attr_bwd_batch));
   return VTI_OK;
 }
 
-int launch_fwd3d_batch(vti_ctx* ctx, const void* d_jobs, const int* d_base, int njobs, int items,
-                       int tick) {
-  VTI_TRY_ST(set_smem_attr(ctx, k_fwd3d_tma<false, true>, F_SMEM, attr_fwd_batch));
-  if (items <= 0 || njobs <= 0) return VTI_OK;
-  JobTable jt{(const unsigned char*)d_jobs, d_base, njobs, items, tick};
-  FwdMaps m{};
-  FwdArgs a{};
-  const int grid = std::min(items, ctx->sm_count * 3);
-  {
-    LaunchTimer tm(ctx, kTimedFwd3d);
-    k_fwd3d_tma<false, true><<<grid, NTHREADS, F_SMEM, ctx->stream>>>(m, a, jt);
+void step_batch_free(StepBatch* b) {
+  if (!b) return;
+  for (void* p : b->d_maps)
+    if (p) cudaFree(p);
+  delete b;
+}
+
+int fwd_batch_build(vti_ctx* ctx, const FwdJobSpec* spec, int njobs, StepBatch** out) {
+  *out = nullptr;
+  VTI_TRY_ST(prepare_batch_kernels(ctx));
+  StepBatch* b = new StepBatch();
+  b->fwd = true;
+  for (int j0 = 0; j0 < njobs; j0 += kMaxFwdJobs) {
+    const int nj = std::min(kMaxFwdJobs, njobs - j0);
+    b->fb.emplace_back();
+    FwdBatch& B = b->fb.back();
+    std::memset(&B, 0, sizeof(B));
+    std::vector<FwdMaps> maps(2 * nj);
+    int items = 0;
+    for (int j = 0; j < nj; ++j) {
+      const FwdJobSpec& sp = spec[j0 + j];
+      const Sched sc = sp.seg > 0 ? sched_with_seg(sp.d, sp.seg) : make_sched(ctx, sp.d, 3);
+      PointSource src;
+      src.x = sp.src_x; src.y = sp.src_y; src.z = sp.src_z;
+      B.c[j] = fwd_common(sp.d, sc, sp.damp, sp.sx, sp.sy, sp.sz, src);
+      B.c[j].amp = sp.amp;
+      B.c[j].t0 = sp.t0;
+      for (int par = 0; par < 2; ++par) {
+        B.p[j][par] = FwdPar{sp.cz_ptr[par], sp.px_ptr[par], sp.pz_ptr[par]};
+        FwdMaps& m = maps[2 * j + par];
+        m.cx = *H(*sp.cx[par]); m.cz = *P(*sp.cz[par]); m.px = *P(*sp.px[par]);
+        m.pz = *P(*sp.pz[par]);
+        m.c11 = *P(*sp.c[0]); m.c13 = *P(*sp.c[1]); m.c33 = *P(*sp.c[2]);
+      }
+      B.base[j] = items;
+      items += sc.items;
+    }
+    B.base[nj] = items;
+    B.njobs = nj;
+    B.items = items;
+    B.status = ctx->d_status;
+    b->items += items;
+    void* d = nullptr;
+    cudaError_t e = cudaMalloc(&d, maps.size() * sizeof(FwdMaps));
+    if (e == cudaSuccess)
+      e = cudaMemcpy(d, maps.data(), maps.size() * sizeof(FwdMaps), cudaMemcpyHostToDevice);
+    b->d_maps.push_back(d);
+    if (e != cudaSuccess) {
+      step_batch_free(b);
+      return cuda_check(ctx, e, "batched forward descriptors");
+    }
+    B.maps = (const FwdMaps*)d;
   }
-  VTI_LAUNCHED(ctx, "k_fwd3d_tma (batched)");
+  *out = b;
   return VTI_OK;
 }
 
-int launch_bwd3d_batch(vti_ctx* ctx, const void* d_jobs, const int* d_base, int njobs, int items,
-                       int tick) {
-  VTI_TRY_ST(set_smem_attr(ctx, k_bwd3d_tma<false, true>, B_SMEM, attr_bwd_batch));
-  if (items <= 0 || njobs <= 0) return VTI_OK;
-  JobTable jt{(const unsigned char*)d_jobs, d_base, njobs, items, tick};
-  BwdMaps m{};
-  BwdArgs a{};
-  const int grid = std::min(items, ctx->sm_count * 2);
-  {
-    LaunchTimer tm(ctx, kTimedBwd3d);
-    k_bwd3d_tma<false, true><<<grid, NTHREADS, B_SMEM, ctx->stream>>>(m, a, jt);
+int bwd_batch_build(vti_ctx* ctx, const BwdJobSpec* spec, int njobs, StepBatch** out) {
+  *out = nullptr;
+  VTI_TRY_ST(prepare_batch_kernels(ctx));
+  StepBatch* b = new StepBatch();
+  b->fwd = false;
+  for (int j0 = 0; j0 < njobs; j0 += kMaxBwdJobs) {
+    const int nj = std::min(kMaxBwdJobs, njobs - j0);
+    b->bb.emplace_back();
+    BwdBatch& B = b->bb.back();
+    std::memset(&B, 0, sizeof(B));
+    std::vector<BwdMaps> maps(2 * nj);
+    int items = 0;
+    for (int j = 0; j < nj; ++j) {
+      const BwdJobSpec& sp = spec[j0 + j];
+      const Sched sc = sp.seg > 0 ? sched_with_seg(sp.d, sp.seg) : make_sched(ctx, sp.d, 2);
+      BwdCommon& c = B.c[j];
+      c.d = sp.d;
+      c.sc = sc;
+      c.g11 = sp.g_ptr[0]; c.g13 = sp.g_ptr[1]; c.g33 = sp.g_ptr[2];
+      c.dampx = sp.damp.x; c.dampy = sp.damp.y; c.dampz = sp.damp.z;
+      c.dt2 = sp.dt2; c.idx2 = sp.idx2; c.idy2 = sp.idy2; c.idz2 = sp.idz2;
+      c.sx = sp.sx; c.sy = sp.sy; c.sz = sp.sz;
+      c.src.x = sp.src_x; c.src.y = sp.src_y; c.src.z = sp.src_z; c.src.amp = 0.f;
+      c.amp = sp.amp;
+      c.t0 = sp.t0;
+      for (int par = 0; par < 2; ++par) {
+        B.p[j][par] = BwdPar{sp.scz_ptr[par], sp.lcz_ptr[par], sp.spx_ptr[par], sp.spz_ptr[par],
+                             sp.lpx_ptr[par], sp.lpz_ptr[par]};
+        BwdMaps& m = maps[2 * j + par];
+        m.scx = *H(*sp.scx[par]); m.scz = *P(*sp.scz[par]); m.spx = *P(*sp.spx[par]);
+        m.spz = *P(*sp.spz[par]);
+        m.lcx = *H(*sp.lcx[par]); m.lcz = *P(*sp.lcz[par]); m.lpx = *P(*sp.lpx[par]);
+        m.lpz = *P(*sp.lpz[par]);
+        m.c11 = *P(*sp.c[0]); m.c13 = *P(*sp.c[1]); m.c33 = *P(*sp.c[2]);
+        m.g11 = *P(*sp.g[0]); m.g13 = *P(*sp.g[1]); m.g33 = *P(*sp.g[2]);
+      }
+      B.base[j] = items;
+      items += sc.items;
+    }
+    B.base[nj] = items;
+    B.njobs = nj;
+    B.items = items;
+    B.status = ctx->d_status;
+    b->items += items;
+    void* d = nullptr;
+    cudaError_t e = cudaMalloc(&d, maps.size() * sizeof(BwdMaps));
+    if (e == cudaSuccess)
+      e = cudaMemcpy(d, maps.data(), maps.size() * sizeof(BwdMaps), cudaMemcpyHostToDevice);
+    b->d_maps.push_back(d);
+    if (e != cudaSuccess) {
+      step_batch_free(b);
+      return cuda_check(ctx, e, "batched backward descriptors");
+    }
+    B.maps = (const BwdMaps*)d;
   }
-  VTI_LAUNCHED(ctx, "k_bwd3d_tma (batched)");
+  *out = b;
   return VTI_OK;
+}
+
+int step_batch_launch(vti_ctx* ctx, StepBatch* b, int tick) {
+  if (b->fwd) {
+    for (FwdBatch& B : b->fb) {
+      if (B.items <= 0) continue;
+      B.tick = tick;
+      const int grid = std::min(B.items, ctx->sm_count * 3);
+      {
+        LaunchTimer tm(ctx, kTimedFwd3d);
+        k_fwd3d_batch<<<grid, NTHREADS, F_SMEM, ctx->stream>>>(B);
+      }
+      VTI_LAUNCHED(ctx, "k_fwd3d_batch");
+    }
+  } else {
+    for (BwdBatch& B : b->bb) {
+      if (B.items <= 0) continue;
+      B.tick = tick;
+      const int grid = std::min(B.items, ctx->sm_count * 2);
+      {
+        LaunchTimer tm(ctx, kTimedBwd3d);
+        k_bwd3d_batch<<<grid, NTHREADS, B_SMEM, ctx->stream>>>(B);
+      }
+      VTI_LAUNCHED(ctx, "k_bwd3d_batch");
+    }
+  }
+  return VTI_OK;
+}
+
+int step_batch_launches(const StepBatch* b) {
+  return (int)(b->fwd ? b->fb.size() : b->bb.size());
 }
 
 }  // namespace vti
