@@ -40,7 +40,8 @@ typedef enum {
   VTI_ERR_DEVICE = 4,     /* a CUDA call failed; see vti_ctx_last_error */
   VTI_ERR_TIMEOUT = 5,    /* a bounded device-side wait gave up */
   VTI_ERR_NONFINITE = 6,  /* a wavefield or misfit became NaN/Inf */
-  VTI_ERR_UNSUPPORTED = 7 /* valid request this build does not implement */
+  VTI_ERR_UNSUPPORTED = 7, /* valid request this build does not implement */
+  VTI_ERR_BUSY = 8         /* not now: engine memory full / job not finished */
 } vti_status;
 
 /* where a pointer lives */
@@ -308,6 +309,45 @@ int vti3d_batch_gradient(vti3d_batch* b, const float* dobs, int dobs_mem, float*
 /* Window models of shot k (pad-boundary and random-boundary, 3 * nx*ny*nz
  * each, host; either may be NULL). */
 int vti3d_batch_get_shot_models(vti3d_batch* b, int k, float* cpad, float* crand);
+
+/* ---------------------------------------------------- 3D serving engine */
+/* Continuous batching of 3D modeling and gradient jobs of different grids:
+ * jobs are admitted between time steps while their device footprint fits the
+ * engine's byte budget (VTI_ERR_BUSY otherwise); every engine tick advances
+ * every admitted job by one time level, all jobs sharing one forward and one
+ * backward launch. A job's state stays resident until its result is
+ * collected. Per job the result is that of vti3d_plan_model_data /
+ * vti3d_plan_gradient with VTI_OPT_FULL_STEPS on the job's grid. */
+typedef struct vti3d_engine vti3d_engine;
+#define VTI_JOB_MODEL 0    /* traces of one shot */
+#define VTI_JOB_GRADIENT 1 /* misfit and c11/c13/c33 gradient of one shot */
+typedef struct {
+  int kind;
+  vti3d_geom g;                   /* the job's own grid */
+  const float *c11, *c13, *c33;   /* host, nxyz each */
+  const float* wavelet;           /* host, nt */
+  const float* souloc;            /* host, 5 floats: x, y, z, nrec, 0 */
+  const float* recloc;            /* host, 4 floats per receiver */
+  int nrec;
+  const float* dobs;              /* gradient: host, nnt * nrec observed traces */
+  const float* randb;             /* gradient: host, 3*nb random-boundary lists, or NULL */
+  unsigned seed;                  /* gradient without randb: device random boundary seed */
+} vti3d_job;
+/* Device bytes a job holds while admitted. */
+size_t vti3d_engine_job_bytes(const vti3d_job* job);
+int vti3d_engine_create(vti_ctx* ctx, size_t max_bytes, vti3d_engine** out);
+int vti3d_engine_destroy(vti3d_engine* e);
+/* Admits a job (copies its inputs to the device) or returns VTI_ERR_BUSY. */
+int vti3d_engine_submit(vti3d_engine* e, const vti3d_job* job, int* id);
+/* Enqueues up to `ticks` time levels of every admitted job; *active = jobs
+ * still running. */
+int vti3d_engine_step(vti3d_engine* e, int ticks, int* active);
+/* Ids of finished jobs whose results are ready (non-blocking). */
+int vti3d_engine_poll(vti3d_engine* e, int* ids, int max_ids, int* n_done);
+/* Result of a finished job, then its device state is released: modeling:
+ * nnt*nrec traces; gradient: [misfit/2, gc11, gc13, gc33] (1 + 3 nxyz). */
+int vti3d_engine_result(vti3d_engine* e, int id, float* out, double* misfit);
+int vti3d_engine_stats(vti3d_engine* e, size_t* used_bytes, int* jobs, int* tick);
 
 #ifdef __cplusplus
 }

@@ -786,3 +786,524 @@ int vti3d_batch_autotune(vti3d_batch* b, int* seg_fwd, int* seg_bwd) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------ serving engine
+//
+// Continuous batching of 3D modeling and gradient jobs of different grids.
+// Jobs are admitted at tick boundaries while their device footprint fits the
+// engine's byte budget; every tick is one forward launch over all jobs in a
+// forward phase (modeling, or passes 1 and 2 of a gradient) and one backward
+// launch over all jobs in pass 3, so jobs that arrive while others run share
+// the launches. A job's state (model, random-boundary model, wavefields,
+// traces) stays resident until its result is collected. Per job the
+// arithmetic is that of a plan on the job's grid (vti3d_plan_model_data /
+// vti3d_plan_gradient with VTI_OPT_FULL_STEPS), whatever else runs beside it.
+
+namespace {
+
+struct EngineJob {
+  int id = 0;
+  int kind = VTI_JOB_MODEL;
+  vti3d_plan* p = nullptr;
+  ShotGeom sg;
+  int* d_rec_at = nullptr;
+  float* d_amp = nullptr;  // forward (M-1) | backward (M-1)
+  double* d_acc = nullptr;
+  cudaEvent_t done = nullptr;
+  int M = 0;
+  int phase = 0;  // 0 forward, 1 backward, 2 done
+  int t0 = 0;     // tick of the current phase's step 0
+  size_t bytes = 0;
+};
+
+size_t vol_bytes(const vti3d_geom& g) {
+  const Dims3 d = make_dims(g.nx, g.ny, g.nz);
+  return (size_t)d.plane * (d.nz + 2 * kZPad) * sizeof(float);
+}
+
+}  // namespace
+
+struct vti3d_engine {
+  vti_ctx* ctx = nullptr;
+  size_t max_bytes = 0, used = 0;
+  int tick = 0, next_id = 1;
+  std::vector<EngineJob*> jobs;
+  bool dirty = true;
+  StepBatch* fwd = nullptr;
+  StepBatch* bwd = nullptr;
+  RecJob* d_recjobs = nullptr;
+  RecEntry* d_rec = nullptr;  // recording entries of jobs in a forward phase
+  RecEntry* d_inj = nullptr;  // injection entries of jobs in pass 3
+  size_t cap_jobs = 0, cap_rec = 0, cap_inj = 0;
+  int n_rec = 0, n_inj = 0;
+  cudaStream_t copy = nullptr;
+};
+
+namespace {
+
+void engine_free_job(vti3d_engine* e, EngineJob* j) {
+  if (j->p) vti3d_plan_destroy(j->p);
+  if (j->d_rec_at) cudaFree(j->d_rec_at);
+  if (j->d_amp) cudaFree(j->d_amp);
+  if (j->d_acc) cudaFree(j->d_acc);
+  if (j->done) cudaEventDestroy(j->done);
+  e->used -= std::min(e->used, j->bytes);
+  delete j;
+}
+
+template <typename T>
+int grow(vti_ctx* ctx, T** p, size_t* cap, size_t n) {
+  if (*cap >= n && *p) return VTI_OK;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *cap = 0;
+  const size_t m = std::max<size_t>(n, 1) * 2;
+  VTI_CUDA(ctx, cudaMalloc((void**)p, m * sizeof(T)));
+  *cap = m;
+  return VTI_OK;
+}
+
+// Launch plans and receiver tables of the jobs in a forward or backward phase.
+int engine_rebuild(vti3d_engine* e) {
+  vti_ctx* ctx = e->ctx;
+  step_batch_free(e->fwd);
+  step_batch_free(e->bwd);
+  e->fwd = e->bwd = nullptr;
+  std::vector<FwdJobSpec> fspec;
+  std::vector<BwdJobSpec> bspec;
+  std::vector<Damping> damps(e->jobs.size());
+  std::vector<RecJob> rj(e->jobs.size());
+  std::vector<RecEntry> rec, inj;
+  for (size_t k = 0; k < e->jobs.size(); ++k) {
+    EngineJob* j = e->jobs[k];
+    if (j->phase > 1) continue;
+    vti3d_plan* p = j->p;
+    const vti3d_geom& g = p->g;
+    const float dt2 = g.dt * g.dt;
+    const float sxs = dt2 / (g.dx * g.dx), sys = dt2 / (g.dy * g.dy), szs = dt2 / (g.dz * g.dz);
+    damps[k] = Damping{p->dampx, p->dampy, p->dampz};
+    if (j->phase == 0) {
+      const int passes = j->kind == VTI_JOB_GRADIENT ? 2 : 1;
+      for (int pass = 0; pass < passes; ++pass) {
+        Vol* vx = pass == 0 ? p->lx : p->sx;
+        Vol* vz = pass == 0 ? p->lz : p->sz;
+        TileMaps* mx = pass == 0 ? p->m_lx : p->m_sx;
+        TileMaps* mz = pass == 0 ? p->m_lz : p->m_sz;
+        FwdJobSpec sp{};
+        sp.d = p->d;
+        for (int par = 0; par < 2; ++par) {
+          sp.cx[par] = &mx[par];
+          sp.cz[par] = &mz[par];
+          sp.px[par] = &mx[1 - par];
+          sp.pz[par] = &mz[1 - par];
+          sp.cz_ptr[par] = vz[par].origin;
+          sp.px_ptr[par] = vx[1 - par].origin;
+          sp.pz_ptr[par] = vz[1 - par].origin;
+        }
+        const TileMaps* cm = pass == 0 ? p->m_cpad : p->m_crand;
+        for (int c = 0; c < 3; ++c) sp.c[c] = &cm[c];
+        sp.damp = pass == 0 ? &damps[k] : nullptr;
+        sp.sx = sxs;
+        sp.sy = sys;
+        sp.sz = szs;
+        sp.src_x = j->sg.sx;
+        sp.src_y = j->sg.sy;
+        sp.src_z = j->sg.sz;
+        sp.amp = j->d_amp;
+        sp.t0 = j->t0;
+        sp.seg = 0;
+        fspec.push_back(sp);
+      }
+    } else {
+      const int last_cur = 1 - ((j->M - 2) & 1);
+      BwdJobSpec sp{};
+      sp.d = p->d;
+      for (int par = 0; par < 2; ++par) {
+        const int sa = last_cur ^ 1 ^ par, sb = 1 - sa;
+        const int la = par, lb = 1 - par;
+        sp.scx[par] = &p->m_sx[sa];
+        sp.scz[par] = &p->m_sz[sa];
+        sp.spx[par] = &p->m_sx[sb];
+        sp.spz[par] = &p->m_sz[sb];
+        sp.lcx[par] = &p->m_lx[la];
+        sp.lcz[par] = &p->m_lz[la];
+        sp.lpx[par] = &p->m_lx[lb];
+        sp.lpz[par] = &p->m_lz[lb];
+        sp.scz_ptr[par] = p->sz[sa].origin;
+        sp.lcz_ptr[par] = p->lz[la].origin;
+        sp.spx_ptr[par] = p->sx[sb].origin;
+        sp.spz_ptr[par] = p->sz[sb].origin;
+        sp.lpx_ptr[par] = p->lx[lb].origin;
+        sp.lpz_ptr[par] = p->lz[lb].origin;
+      }
+      for (int c = 0; c < 3; ++c) {
+        sp.c[c] = &p->m_crand[c];
+        sp.g[c] = &p->m_g[c];
+      }
+      sp.g_ptr[0] = p->g11.origin;
+      sp.g_ptr[1] = p->g13.origin;
+      sp.g_ptr[2] = p->g33.origin;
+      sp.damp = damps[k];
+      sp.dt2 = dt2;
+      sp.idx2 = 1.f / (g.dx * g.dx);
+      sp.idy2 = 1.f / (g.dy * g.dy);
+      sp.idz2 = 1.f / (g.dz * g.dz);
+      sp.sx = sxs;
+      sp.sy = sys;
+      sp.sz = szs;
+      sp.src_x = j->sg.sx;
+      sp.src_y = j->sg.sy;
+      sp.src_z = j->sg.sz;
+      sp.amp = j->d_amp + (j->M - 1);
+      sp.t0 = j->t0;
+      sp.seg = 0;
+      bspec.push_back(sp);
+    }
+    RecJob& J = rj[k];
+    for (int par = 0; par < 2; ++par) {
+      J.rx[par] = p->lx[1 - par].origin;
+      J.rz[par] = p->lz[1 - par].origin;
+      J.lx[par] = p->lx[par].origin;
+      J.lz[par] = p->lz[par].origin;
+    }
+    J.trace = p->d_trace;
+    J.rec_at = j->d_rec_at;
+    J.nnt = nnt_of(g);
+    J.st = sampling_step(g);
+    J.nt = g.nt;
+    J.t0 = j->t0;
+    J.dt2 = dt2;
+    for (int ir = 0; ir < j->sg.nr; ++ir) {
+      RecEntry en{};
+      en.off = j->sg.rec[ir];
+      en.job = (int)k;
+      en.ir = ir;
+      en.damp = j->sg.rec_damp[ir];
+      (j->phase == 0 ? rec : inj).push_back(en);
+    }
+  }
+  if (!fspec.empty()) VTI_TRY(fwd_batch_build(ctx, fspec.data(), (int)fspec.size(), &e->fwd));
+  if (!bspec.empty()) VTI_TRY(bwd_batch_build(ctx, bspec.data(), (int)bspec.size(), &e->bwd));
+  VTI_TRY(grow(ctx, &e->d_recjobs, &e->cap_jobs, rj.size()));
+  VTI_TRY(grow(ctx, &e->d_rec, &e->cap_rec, rec.size()));
+  VTI_TRY(grow(ctx, &e->d_inj, &e->cap_inj, inj.size()));
+  if (!rj.empty())
+    VTI_CUDA(ctx, cudaMemcpyAsync(e->d_recjobs, rj.data(), rj.size() * sizeof(RecJob),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+  if (!rec.empty())
+    VTI_CUDA(ctx, cudaMemcpyAsync(e->d_rec, rec.data(), rec.size() * sizeof(RecEntry),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+  if (!inj.empty())
+    VTI_CUDA(ctx, cudaMemcpyAsync(e->d_inj, inj.data(), inj.size() * sizeof(RecEntry),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+  // the host tables are released on return
+  VTI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  e->n_rec = (int)rec.size();
+  e->n_inj = (int)inj.size();
+  e->dirty = false;
+  return VTI_OK;
+}
+
+// After the tick: phase changes of jobs whose phase ran all M-1 steps.
+int engine_transitions(vti3d_engine* e) {
+  vti_ctx* ctx = e->ctx;
+  for (EngineJob* j : e->jobs) {
+    if (j->phase > 1 || e->tick - j->t0 < j->M - 1) continue;
+    vti3d_plan* p = j->p;
+    const int nnt = nnt_of(p->g);
+    const float dt2 = p->g.dt * p->g.dt;
+    if (j->phase == 0 && j->kind == VTI_JOB_GRADIENT) {
+      // residual and misfit (objFuncGradient3d_f.cu:735-771), adjoint seeded
+      VTI_TRY(launch_residual(ctx, p->d_trace, p->d_obs, p->d_live, nnt, j->sg.nr, j->d_acc));
+      for (int k = 0; k < 2; ++k) {
+        VTI_TRY(vol_zero(ctx, p->d, &p->lx[k]));
+        VTI_TRY(vol_zero(ctx, p->d, &p->lz[k]));
+      }
+      VTI_TRY(launch_seed_adjoint(ctx, p->lx[0].origin, p->lz[0].origin, p->d_trace, nnt,
+                                  p->d_rec + p->rec_cap, p->d_rec_damp, j->sg.nr, dt2));
+      j->phase = 1;
+      j->t0 = e->tick;
+    } else {
+      if (j->kind == VTI_JOB_MODEL)  // dead receivers give zero traces
+        VTI_TRY(launch_residual(ctx, p->d_trace, nullptr, p->d_live, nnt, j->sg.nr, nullptr));
+      j->phase = 2;
+      VTI_CUDA(ctx, cudaEventRecord(j->done, ctx->stream));
+    }
+    e->dirty = true;
+  }
+  return VTI_OK;
+}
+
+EngineJob* engine_find(vti3d_engine* e, int id) {
+  for (EngineJob* j : e->jobs)
+    if (j->id == id) return j;
+  return nullptr;
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t vti3d_engine_job_bytes(const vti3d_job* job) {
+  if (!job) return 0;
+  const size_t v = vol_bytes(job->g);
+  const int nvol = job->kind == VTI_JOB_GRADIENT ? 17 : 14;
+  const int st = (int)std::round(job->g.sampling_rate / job->g.dt);
+  const size_t nnt = st > 0 ? (size_t)(job->g.nt - 1) / st + 1 : 0;
+  const size_t nr = (size_t)std::max(job->nrec, 1);
+  return nvol * v + 2 * nnt * nr * sizeof(float) + nr * 32 + 2 * (size_t)job->g.nt * 8 +
+         (size_t)(job->g.nx + job->g.ny + job->g.nz) * 4;
+}
+
+int vti3d_engine_create(vti_ctx* ctx, size_t max_bytes, vti3d_engine** out) {
+  if (!ctx || !out) return VTI_ERR_ARG;
+  *out = nullptr;
+  VTI_CUDA(ctx, cudaSetDevice(ctx->device));
+  vti3d_engine* e = new vti3d_engine();
+  e->ctx = ctx;
+  e->max_bytes = max_bytes;
+  if (cudaStreamCreateWithFlags(&e->copy, cudaStreamNonBlocking) != cudaSuccess) {
+    delete e;
+    return fail(ctx, VTI_ERR_DEVICE, "copy stream");
+  }
+  *out = e;
+  return VTI_OK;
+}
+
+int vti3d_engine_destroy(vti3d_engine* e) {
+  if (!e) return VTI_OK;
+  cudaSetDevice(e->ctx->device);
+  cudaStreamSynchronize(e->ctx->stream);
+  cudaStreamSynchronize(e->copy);
+  for (EngineJob* j : e->jobs) engine_free_job(e, j);
+  step_batch_free(e->fwd);
+  step_batch_free(e->bwd);
+  void* ptrs[] = {e->d_recjobs, e->d_rec, e->d_inj};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+  cudaStreamDestroy(e->copy);
+  delete e;
+  return VTI_OK;
+}
+
+int vti3d_engine_submit(vti3d_engine* e, const vti3d_job* job, int* id) {
+  if (!e || !job || !id) return VTI_ERR_ARG;
+  vti_ctx* ctx = e->ctx;
+  *id = 0;
+  if (job->kind != VTI_JOB_MODEL && job->kind != VTI_JOB_GRADIENT)
+    return fail(ctx, VTI_ERR_ARG, "unknown job kind");
+  if (!job->c11 || !job->c13 || !job->c33 || !job->wavelet || !job->souloc ||
+      (job->nrec > 0 && !job->recloc) || (job->kind == VTI_JOB_GRADIENT && !job->dobs))
+    return fail(ctx, VTI_ERR_ARG, "null job array");
+  VTI_TRY(check_geom(ctx, &job->g));
+  const size_t bytes = vti3d_engine_job_bytes(job);
+  if (e->used + bytes > e->max_bytes)
+    return fail(ctx, VTI_ERR_BUSY, "engine memory budget full; submit again later");
+  VTI_CUDA(ctx, cudaSetDevice(ctx->device));
+  EngineJob* j = new EngineJob();
+  j->kind = job->kind;
+  j->bytes = bytes;
+  e->used += bytes;
+  int st = VTI_OK;
+  auto fail_job = [&](int s) {
+    engine_free_job(e, j);
+    return s;
+  };
+  const unsigned flags = VTI_OPT_FULL_STEPS;
+  st = vti3d_plan_create(ctx, &job->g, flags, &j->p);
+  if (st != VTI_OK) return fail_job(st);
+  vti3d_plan* p = j->p;
+  p->wavelet.assign(job->wavelet, job->wavelet + job->g.nt);
+  p->recloc.assign(job->recloc, job->recloc + 4 * (size_t)job->nrec);
+  p->nrec_total = job->nrec;
+  const Dims3& d = p->d;
+  const float* cs[3] = {job->c11, job->c13, job->c33};
+  for (int c = 0; c < 3 && st == VTI_OK; ++c) st = vol_upload(ctx, d, &p->cpad[c], cs[c], VTI_MEM_HOST);
+  if (st != VTI_OK) return fail_job(st);
+  p->have_model = true;
+  if (job->kind == VTI_JOB_GRADIENT) {
+    for (int c = 0; c < 3 && st == VTI_OK; ++c) {
+      st = vol_alloc(ctx, d, &p->crand[c]);
+      if (st == VTI_OK) st = make_tile_maps(ctx, d, p->crand[c], &p->m_crand[c]);
+    }
+    if (st != VTI_OK) return fail_job(st);
+    p->have_rand = true;
+    if (job->randb) {
+      const long long nb = boundary_count(job->g);
+      st = ensure(ctx, &p->d_blist, &p->blist_cap, (size_t)nb);
+      for (int c = 0; c < 3 && st == VTI_OK; ++c) {
+        const cudaError_t ce =
+            cudaMemcpyAsync(p->d_blist, job->randb + (size_t)c * nb, nb * sizeof(float),
+                            cudaMemcpyHostToDevice, ctx->stream);
+        st = ce == cudaSuccess ? launch_boundary_merge(ctx, d, job->g.npad, p->cpad[c].origin,
+                                                       p->d_blist, p->crand[c].origin)
+                               : cuda_check(ctx, ce, "random boundary upload");
+        if (st == VTI_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+          st = fail(ctx, VTI_ERR_DEVICE, "random boundary upload");
+      }
+    } else {
+      k_random_boundary<<<grid_for(ctx, d.npoints()), 256, 0, ctx->stream>>>(
+          p->cpad[0].origin, p->cpad[1].origin, p->cpad[2].origin, p->crand[0].origin,
+          p->crand[1].origin, p->crand[2].origin, d, job->g.npad, job->seed, 0, 0, job->g.nx,
+          job->g.ny);
+      ctx->launches++;
+      if (cudaGetLastError() != cudaSuccess) st = fail(ctx, VTI_ERR_DEVICE, "k_random_boundary");
+    }
+    if (st != VTI_OK) return fail_job(st);
+  }
+  st = shot_geom(p, job->souloc, 0, &j->sg);
+  if (st == VTI_OK) st = upload_shot(p, j->sg);
+  if (st != VTI_OK) return fail_job(st);
+  j->M = last_level(job->g, flags);
+  if (j->M < 2) return fail_job(fail(ctx, VTI_ERR_ARG, "fewer than 3 time samples"));
+  const int nnt = nnt_of(job->g);
+  const float dt2 = job->g.dt * job->g.dt;
+  std::vector<float> amp(2 * (size_t)(j->M - 1));
+  for (int s = 0; s < j->M - 1; ++s) {
+    amp[s] = dt2 * p->wavelet[s + 1];
+    amp[(j->M - 1) + s] = dt2 * p->wavelet[job->g.nt - 2 - s];
+  }
+  if (cudaMalloc((void**)&j->d_amp, amp.size() * sizeof(float)) != cudaSuccess ||
+      cudaMalloc((void**)&j->d_rec_at, j->sg.rec_at.size() * sizeof(int)) != cudaSuccess ||
+      cudaMalloc((void**)&j->d_acc, (1 + residual_blocks(ctx)) * sizeof(double)) != cudaSuccess ||
+      cudaEventCreateWithFlags(&j->done, cudaEventDisableTiming) != cudaSuccess)
+    return fail_job(fail(ctx, VTI_ERR_OOM, "job tables"));
+  if (cudaMemcpy(j->d_amp, amp.data(), amp.size() * sizeof(float), cudaMemcpyHostToDevice) !=
+          cudaSuccess ||
+      cudaMemcpy(j->d_rec_at, j->sg.rec_at.data(), j->sg.rec_at.size() * sizeof(int),
+                 cudaMemcpyHostToDevice) != cudaSuccess)
+    return fail_job(fail(ctx, VTI_ERR_DEVICE, "job tables"));
+  if (job->kind == VTI_JOB_GRADIENT) {
+    const float* obs = nullptr;
+    st = get_obs(p, j->sg, job->dobs, VTI_MEM_HOST, &obs);
+    if (st != VTI_OK) return fail_job(st);
+  }
+  // fields of step 0: level 1 holds the source (objFuncGradient3d_f.cu:605-608)
+  for (int k = 0; k < 2 && st == VTI_OK; ++k) {
+    st = vol_zero(ctx, d, &p->sx[k]);
+    if (st == VTI_OK) st = vol_zero(ctx, d, &p->sz[k]);
+    if (st == VTI_OK) st = vol_zero(ctx, d, &p->lx[k]);
+    if (st == VTI_OK) st = vol_zero(ctx, d, &p->lz[k]);
+  }
+  if (st == VTI_OK && job->kind == VTI_JOB_GRADIENT) {
+    st = vol_zero(ctx, d, &p->g11);
+    if (st == VTI_OK) st = vol_zero(ctx, d, &p->g13);
+    if (st == VTI_OK) st = vol_zero(ctx, d, &p->g33);
+  }
+  const long long o = d.off(j->sg.sx, j->sg.sy, j->sg.sz);
+  if (st == VTI_OK) st = launch_set_point(ctx, p->lx[0].origin, p->lz[0].origin, o, dt2 * p->wavelet[0]);
+  if (st == VTI_OK && job->kind == VTI_JOB_GRADIENT)
+    st = launch_set_point(ctx, p->sx[0].origin, p->sz[0].origin, o, dt2 * p->wavelet[0]);
+  if (st == VTI_OK && j->sg.nr > 0 &&
+      cudaMemsetAsync(p->d_trace, 0, (size_t)nnt * j->sg.nr * sizeof(float), ctx->stream) !=
+          cudaSuccess)
+    st = fail(ctx, VTI_ERR_DEVICE, "trace reset");
+  if (st == VTI_OK && cudaMemsetAsync(j->d_acc, 0, sizeof(double), ctx->stream) != cudaSuccess)
+    st = fail(ctx, VTI_ERR_DEVICE, "misfit reset");
+  if (st == VTI_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+    st = fail(ctx, VTI_ERR_DEVICE, "job set-up");
+  if (st != VTI_OK) return fail_job(st);
+  j->phase = 0;
+  j->t0 = e->tick;
+  j->id = e->next_id++;
+  e->jobs.push_back(j);
+  e->dirty = true;
+  *id = j->id;
+  return VTI_OK;
+}
+
+int vti3d_engine_step(vti3d_engine* e, int ticks, int* active) {
+  if (!e || ticks < 0) return VTI_ERR_ARG;
+  vti_ctx* ctx = e->ctx;
+  VTI_CUDA(ctx, cudaSetDevice(ctx->device));
+  for (int i = 0; i < ticks; ++i) {
+    bool any = false;
+    for (EngineJob* j : e->jobs) any |= j->phase <= 1;
+    if (!any) break;
+    if (e->dirty) VTI_TRY(engine_rebuild(e));
+    if (e->fwd) VTI_TRY(step_batch_launch(ctx, e->fwd, e->tick));
+    if (e->n_rec > 0) {
+      k_record_batch<<<(e->n_rec + 255) / 256, 256, 0, ctx->stream>>>(e->d_recjobs, e->d_rec,
+                                                                       e->n_rec, e->tick);
+      VTI_LAUNCHED(ctx, "k_record_batch");
+    }
+    if (e->bwd) VTI_TRY(step_batch_launch(ctx, e->bwd, e->tick));
+    if (e->n_inj > 0) {
+      k_inject_batch<<<(e->n_inj + 255) / 256, 256, 0, ctx->stream>>>(e->d_recjobs, e->d_inj,
+                                                                       e->n_inj, e->tick);
+      VTI_LAUNCHED(ctx, "k_inject_batch");
+    }
+    e->tick++;
+    VTI_TRY(engine_transitions(e));
+  }
+  if (active) {
+    int n = 0;
+    for (EngineJob* j : e->jobs) n += j->phase <= 1;
+    *active = n;
+  }
+  return VTI_OK;
+}
+
+int vti3d_engine_poll(vti3d_engine* e, int* ids, int max_ids, int* n_done) {
+  if (!e || !n_done || (max_ids > 0 && !ids)) return VTI_ERR_ARG;
+  int n = 0;
+  for (EngineJob* j : e->jobs) {
+    if (j->phase != 2 || n >= max_ids) continue;
+    const cudaError_t q = cudaEventQuery(j->done);
+    if (q == cudaSuccess) ids[n++] = j->id;
+    else if (q != cudaErrorNotReady) return cuda_check(e->ctx, q, "job completion");
+  }
+  *n_done = n;
+  return VTI_OK;
+}
+
+int vti3d_engine_result(vti3d_engine* e, int id, float* out, double* misfit) {
+  if (!e) return VTI_ERR_ARG;
+  vti_ctx* ctx = e->ctx;
+  EngineJob* j = engine_find(e, id);
+  if (!j) return fail(ctx, VTI_ERR_ARG, "unknown job id");
+  if (j->phase != 2) return fail(ctx, VTI_ERR_BUSY, "job not finished");
+  VTI_CUDA(ctx, cudaSetDevice(ctx->device));
+  vti3d_plan* p = j->p;
+  // copies on the engine's copy stream, after the job's last step only
+  VTI_CUDA(ctx, cudaStreamWaitEvent(e->copy, j->done, 0));
+  double acc = 0;
+  const int nnt = nnt_of(p->g);
+  if (j->kind == VTI_JOB_MODEL) {
+    if (out && j->sg.nr > 0)
+      VTI_CUDA(ctx, cudaMemcpyAsync(out, p->d_trace, (size_t)nnt * j->sg.nr * sizeof(float),
+                                    cudaMemcpyDeviceToHost, e->copy));
+  } else {
+    VTI_CUDA(ctx, cudaMemcpyAsync(&acc, j->d_acc, sizeof(double), cudaMemcpyDeviceToHost,
+                                  e->copy));
+    if (out) {
+      const size_t n = (size_t)p->d.npoints();
+      const Vol* gv[3] = {&p->g11, &p->g13, &p->g33};
+      for (int c = 0; c < 3; ++c)
+        VTI_CUDA(ctx, cudaMemcpy2DAsync(out + 1 + c * n, p->d.nx * sizeof(float),
+                                        gv[c]->origin, p->d.pitch * sizeof(float),
+                                        p->d.nx * sizeof(float), (size_t)p->d.ny * p->d.nz,
+                                        cudaMemcpyDeviceToHost, e->copy));
+    }
+  }
+  VTI_CUDA(ctx, cudaStreamSynchronize(e->copy));
+  if (j->kind == VTI_JOB_GRADIENT) {
+    if (misfit) *misfit = acc / 2;
+    if (out) out[0] = (float)(acc / 2);
+  }
+  // release the job's device state
+  e->jobs.erase(std::find(e->jobs.begin(), e->jobs.end(), j));
+  engine_free_job(e, j);
+  e->dirty = true;
+  return check_device_status(ctx);
+}
+
+int vti3d_engine_stats(vti3d_engine* e, size_t* used_bytes, int* jobs, int* tick) {
+  if (!e) return VTI_ERR_ARG;
+  if (used_bytes) *used_bytes = e->used;
+  if (jobs) *jobs = (int)e->jobs.size();
+  if (tick) *tick = e->tick;
+  return VTI_OK;
+}
+
+}  // extern "C"

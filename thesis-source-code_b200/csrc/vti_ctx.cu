@@ -186,6 +186,7 @@ const char* vti_status_string(int status) {
     case VTI_ERR_TIMEOUT: return "device-side wait timed out";
     case VTI_ERR_NONFINITE: return "non-finite wavefield or misfit";
     case VTI_ERR_UNSUPPORTED: return "unsupported request";
+    case VTI_ERR_BUSY: return "busy (memory budget full or job not finished)";
     default: return "unknown status";
   }
 }

@@ -24,6 +24,9 @@ VTI_ERR_DEVICE = 4
 VTI_ERR_TIMEOUT = 5
 VTI_ERR_NONFINITE = 6
 VTI_ERR_UNSUPPORTED = 7
+VTI_ERR_BUSY = 8
+JOB_MODEL = 0
+JOB_GRADIENT = 1
 
 MEM_HOST = 0
 MEM_DEVICE = 1
@@ -42,6 +45,14 @@ class Geom3d(C.Structure):
                 ("npad", C.c_int), ("ox", C.c_float), ("oy", C.c_float), ("oz", C.c_float),
                 ("ot", C.c_float), ("dx", C.c_float), ("dy", C.c_float), ("dz", C.c_float),
                 ("dt", C.c_float), ("sampling_rate", C.c_float)]
+
+
+class Job3d(C.Structure):
+    """vti3d_job: one request of the 3D serving engine."""
+    _fields_ = [("kind", C.c_int), ("g", Geom3d), ("c11", C.c_void_p), ("c13", C.c_void_p),
+                ("c33", C.c_void_p), ("wavelet", C.c_void_p), ("souloc", C.c_void_p),
+                ("recloc", C.c_void_p), ("nrec", C.c_int), ("dobs", C.c_void_p),
+                ("randb", C.c_void_p), ("seed", C.c_uint)]
 
 
 class Geom2d(C.Structure):
@@ -119,6 +130,15 @@ def _signatures():
         "vti3d_batch_autotune": (C.c_int, [P, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "vti3d_batch_gradient": (C.c_int, [P, P, C.c_int, P, C.c_int, C.POINTER(C.c_double)]),
         "vti3d_batch_get_shot_models": (C.c_int, [P, C.c_int, P, P]),
+        "vti3d_engine_job_bytes": (C.c_size_t, [P]),
+        "vti3d_engine_create": (C.c_int, [P, C.c_size_t, C.POINTER(VP)]),
+        "vti3d_engine_destroy": (C.c_int, [P]),
+        "vti3d_engine_submit": (C.c_int, [P, P, C.POINTER(C.c_int)]),
+        "vti3d_engine_step": (C.c_int, [P, C.c_int, C.POINTER(C.c_int)]),
+        "vti3d_engine_poll": (C.c_int, [P, P, C.c_int, C.POINTER(C.c_int)]),
+        "vti3d_engine_result": (C.c_int, [P, C.c_int, P, C.POINTER(C.c_double)]),
+        "vti3d_engine_stats": (C.c_int, [P, C.POINTER(C.c_size_t), C.POINTER(C.c_int),
+                                         C.POINTER(C.c_int)]),
     }
 
 
@@ -390,6 +410,81 @@ class Batch3d:
     def close(self):
         if self._h:
             lib().vti3d_batch_destroy(self._h)
+            self._h = VP()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Engine3d:
+    """3D serving engine (vti3d_engine_*): continuous batching of modeling and
+    gradient jobs of different grids under a device byte budget."""
+
+    def __init__(self, ctx: Context, max_bytes: int):
+        self.ctx = ctx
+        self._h = VP()
+        ctx.check(lib().vti3d_engine_create(ctx.handle, int(max_bytes), C.byref(self._h)))
+        ctx._plans.add(self)
+        self._jobs = {}
+
+    @staticmethod
+    def make_job(kind, g, c11, c13, c33, wavelet, souloc, recloc, dobs=None, randb=None,
+                 seed=0):
+        keep = [_f32(a) for a in (c11, c13, c33, wavelet, souloc, recloc)]
+        keep.append(None if dobs is None else _f32(dobs))
+        keep.append(None if randb is None else _f32(randb))
+        j = Job3d(kind, g, *[None if a is None else a.ctypes.data for a in keep[:6]],
+                  keep[5].size // 4, None if keep[6] is None else keep[6].ctypes.data,
+                  None if keep[7] is None else keep[7].ctypes.data, seed & 0xffffffff)
+        j._keep = keep
+        return j
+
+    def job_bytes(self, job):
+        return int(lib().vti3d_engine_job_bytes(C.byref(job)))
+
+    def submit(self, job):
+        """Job id, or None when the memory budget is full (VTI_ERR_BUSY)."""
+        jid = C.c_int(0)
+        st = lib().vti3d_engine_submit(self._h, C.byref(job), C.byref(jid))
+        if st == VTI_ERR_BUSY:
+            return None
+        self.ctx.check(st)
+        self._jobs[jid.value] = job
+        return jid.value
+
+    def step(self, ticks):
+        n = C.c_int(0)
+        self.ctx.check(lib().vti3d_engine_step(self._h, int(ticks), C.byref(n)))
+        return n.value
+
+    def poll(self, max_ids=256):
+        ids = np.zeros(max_ids, dtype=np.int32)
+        n = C.c_int(0)
+        self.ctx.check(lib().vti3d_engine_poll(self._h, _p(ids), max_ids, C.byref(n)))
+        return [int(i) for i in ids[:n.value]]
+
+    def result(self, jid):
+        job = self._jobs.pop(jid)
+        g = job.g
+        if job.kind == JOB_MODEL:
+            out = np.zeros(nnt3d(g) * job.nrec, dtype=np.float32)
+        else:
+            out = np.zeros(1 + 3 * g.nx * g.ny * g.nz, dtype=np.float32)
+        mis = C.c_double(0)
+        self.ctx.check(lib().vti3d_engine_result(self._h, jid, _p(out), C.byref(mis)))
+        return out, mis.value
+
+    def stats(self):
+        u, n, t = C.c_size_t(0), C.c_int(0), C.c_int(0)
+        self.ctx.check(lib().vti3d_engine_stats(self._h, C.byref(u), C.byref(n), C.byref(t)))
+        return u.value, n.value, t.value
+
+    def close(self):
+        if self._h:
+            lib().vti3d_engine_destroy(self._h)
             self._h = VP()
 
     def __del__(self):

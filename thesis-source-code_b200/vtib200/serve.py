@@ -1,0 +1,362 @@
+"""Request loop of the serving workload.
+
+Mixed 2D / 3D modeling and gradient requests arrive over time (seeded
+Poisson arrivals). 3D requests go to one `Engine3d` (continuous batching:
+admitted between time steps while their device footprint fits the byte
+budget, every admitted job advanced by the same launches, state resident on
+the device until collected); 2D requests run on a second context (its own
+CUDA stream) in a worker thread, so their kernels overlap the 3D launches on
+the device. An optional FWI driver interleaves L-BFGS iterations of gradient
+requests on a 3D model. The loop reports per-request latency (arrival to
+result on the host) as p50 / p99 and requests per second.
+"""
+from __future__ import annotations
+
+import queue
+import threading
+import time
+from collections import deque
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import (JOB_GRADIENT, JOB_MODEL, OPT_FULL_STEPS, Context, Engine3d, Plan3d, geom3d,
+               get_boundary, objFuncGradient_f, synthetic_f, vepsdel_to_cij)
+from . import synth as S
+
+
+@dataclass
+class Request:
+    rid: int
+    dim: int            # 2 or 3
+    kind: str           # "model" or "gradient"
+    arrival: float      # seconds after the start
+    make: object        # callable building the job (3D) or the call arguments (2D)
+    size: tuple = ()
+    t_admit: float = -1.0
+    t_done: float = -1.0
+    result: object = None
+    tag: object = None  # caller's label (FWI shot)
+
+    @property
+    def latency(self):
+        return self.t_done - self.arrival
+
+
+def _layered3d(nx, ny, nz, d, seed):
+    z = np.arange(nz) * d
+    v1, e1, d1 = S.layered(z, S.interfaces_for(nz * d, seed=seed))
+    shape = (nz, ny, nx)
+    v = np.broadcast_to(v1[:, None, None], shape).reshape(-1).astype(np.float32)
+    e = np.broadcast_to(e1[:, None, None], shape).reshape(-1).astype(np.float32)
+    dl = np.broadcast_to(d1[:, None, None], shape).reshape(-1).astype(np.float32)
+    return vepsdel_to_cij(v, e, dl)
+
+
+def job3d(kind, nx, ny, nz, nt, freq, seed, d=12.5, dt=1e-3, npad=20, rec_step=4):
+    """A 3D request: layered VTI model, source at the centre, receivers on a
+    grid 25 m below the top; gradient requests get zero observed traces (the
+    residual is the modeled data; the work does not depend on the values).
+    The pad is at most a quarter of the smallest dimension."""
+    npad = min(npad, min(nx, ny, nz) // 4)
+    o = -npad * d
+    g = geom3d(nx, ny, nz, nt, npad, d, d, d, dt, 4e-3, ox=o, oy=o, oz=o)
+    c11, c13, c33 = _layered3d(nx, ny, nz, d, seed)
+    w = S.ricker(nt, dt, freq)
+    rx = np.arange(npad, nx - npad, rec_step)
+    ry = np.arange(npad, ny - npad, rec_step)
+    RX, RY = np.meshgrid(rx, ry, indexing="xy")
+    rec = np.zeros((RX.size, 4), dtype=np.float32)
+    rec[:, 0] = RX.reshape(-1) * d + o + 0.25 * d
+    rec[:, 1] = RY.reshape(-1) * d + o + 0.25 * d
+    rec[:, 2] = (npad + 2) * d + o + 0.25 * d
+    rec[:, 3] = 1
+    so = np.array([nx // 2 * d + o + 0.25 * d, ny // 2 * d + o + 0.25 * d,
+                   (npad + 2) * d + o + 0.25 * d, RX.size, 0], dtype=np.float32)
+    nnt = (nt - 1) // 4 + 1
+    if kind == "model":
+        return Engine3d.make_job(JOB_MODEL, g, c11, c13, c33, w, so, rec)
+    return Engine3d.make_job(JOB_GRADIENT, g, c11, c13, c33, w, so, rec,
+                             dobs=np.zeros(nnt * RX.size, dtype=np.float32), seed=seed)
+
+
+def call2d(kind, nz, nx, nt, freq, seed, npad=30):
+    """A 2D request: the layered survey of lib/vti-fwi-2d's conventions."""
+    s = S.survey2d(nx=nx, nz=nz, nt=nt, npad=npad, freq=freq, seed=seed)
+    g = s.geom()
+    if kind == "model":
+        return lambda ctx: synthetic_f(ctx, g, s.c11, s.c13, s.c33, s.wavelet, s.sloc, s.rloc,
+                                       s.taper)
+    ratio = int(round(g.rate / g.dt))
+    data = np.zeros(((nt - 1) // ratio + 1, s.rloc.size // 2), dtype=np.float32)
+    return lambda ctx: objFuncGradient_f(ctx, g, data, s.c11, s.c13, s.c33, s.wavelet, s.sloc,
+                                         s.rloc, s.taper)
+
+
+def make_requests(n, rate=20.0, seed=7, size3d=((128, 128, 128), (400, 400, 200)),
+                  size2d=((201, 401), (401, 801)), nt=(2000, 4000), freq=(10.0, 15.0)):
+    """n requests with Poisson arrivals (mean `rate` per second): half 2D, half
+    3D, half modeling, half gradient; grid sizes, nt and the Ricker frequency
+    drawn uniformly in the given ranges (3D: nx, ny, nz; 2D: nz, nx)."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, size=n))
+    out = []
+    for i in range(n):
+        dim = 3 if rng.random() < 0.5 else 2
+        kind = "gradient" if rng.random() < 0.5 else "model"
+        steps = int(rng.integers(nt[0], nt[1] + 1))
+        f = float(rng.uniform(*freq))
+        if dim == 3:
+            (a, b, c), (A, B, Cc) = size3d
+            nx, ny, nz = (int(rng.integers(a, A + 1)), int(rng.integers(b, B + 1)),
+                          int(rng.integers(c, Cc + 1)))
+            mk = (lambda k=kind, x=nx, y=ny, z=nz, s=steps, ff=f, sd=seed * 1000 + i:
+                  job3d(k, x, y, z, s, ff, sd))
+            size = (nx, ny, nz, steps)
+        else:
+            (a, b), (A, B) = size2d
+            nz, nx = int(rng.integers(a, A + 1)), int(rng.integers(b, B + 1))
+            mk = (lambda k=kind, z=nz, x=nx, s=steps, ff=f, sd=seed * 1000 + i:
+                  call2d(k, z, x, s, ff, sd))
+            size = (nx, nz, steps)
+        out.append(Request(i, dim, kind, float(t[i]), mk, size))
+    return out
+
+
+@dataclass
+class FwiDriver:
+    """L-BFGS on a 3D model (c11, c13, c33 stacked) with gradients from
+    gradient requests on windows of the model, one request per shot and
+    iteration; the next iteration is submitted when the last gradient of the
+    current one has arrived. A step that raises the misfit is halved and
+    re-evaluated (at most 4 times)."""
+    g: object
+    model: np.ndarray
+    wavelet: np.ndarray
+    shots: list          # (souloc[5], recloc, dobs, window) per shot
+    iterations: int
+    memory: int = 5
+    misfits: list = field(default_factory=list)
+    step0: float = 0.0
+
+    def __post_init__(self):
+        self.s_hist, self.y_hist = [], []
+        self.x = self.model.astype(np.float64)
+        self.it = 0
+        self.g_cur = None
+        self.f_cur = None
+        self.trial = None
+        self.halvings = 0
+
+    def jobs(self, x):
+        """One gradient job per shot on its window of model x; the random
+        boundary of each window is a fixed host-generated multiplier (the
+        same for every iteration and for the plain evaluation)."""
+        g, n = self.g, self.g.nx * self.g.ny * self.g.nz
+        if not hasattr(self, "_r2"):
+            self._r2 = []
+            for k, (_, _, _, (x0, y0, wx, wy)) in enumerate(self.shots):
+                r = S.random_boundary(np.ones(wx * wy * g.nz, dtype=np.float32), wx, wy, g.nz,
+                                      g.npad, seed=101 + k)
+                self._r2.append((r * r).astype(np.float32))
+        out = []
+        for k, (so, rec, dobs, (x0, y0, wx, wy)) in enumerate(self.shots):
+            sub = geom3d(wx, wy, g.nz, g.nt, g.npad, g.dx, g.dy, g.dz, g.dt, g.sampling_rate,
+                         ox=g.ox + x0 * g.dx, oy=g.oy + y0 * g.dy, oz=g.oz)
+            c = [x[i * n:(i + 1) * n].astype(np.float32).reshape(g.nz, g.ny, g.nx)
+                 [:, y0:y0 + wy, x0:x0 + wx].reshape(-1) for i in range(3)]
+            randb = np.concatenate([get_boundary(ci * self._r2[k], wx, wy, g.nz, g.npad)
+                                    for ci in c])
+            out.append(Engine3d.make_job(JOB_GRADIENT, sub, *c, self.wavelet, so, rec,
+                                         dobs=dobs, randb=randb))
+        return out
+
+    def run_plain(self, ctx):
+        """The same iterations with the plain form: vti3d_plan_gradient of one
+        shot at a time. Returns the misfit history."""
+        jobs = self.first()
+        while jobs is not None:
+            jobs = self.update([plain_gradient(ctx, j) for j in jobs])
+        return self.misfits
+
+    def stack(self, results):
+        g, n = self.g, self.g.nx * self.g.ny * self.g.nz
+        full = np.zeros((3, g.nz, g.ny, g.nx))
+        f = 0.0
+        for (fg, mis), (_, _, _, (x0, y0, wx, wy)) in zip(results, self.shots):
+            f += mis
+            ns = wx * wy * g.nz
+            xl, xh = (0 if x0 == 0 else g.npad), (wx if x0 + wx == g.nx else wx - g.npad)
+            yl, yh = (0 if y0 == 0 else g.npad), (wy if y0 + wy == g.ny else wy - g.npad)
+            for c in range(3):
+                a = fg[1 + c * ns:1 + (c + 1) * ns].reshape(g.nz, wy, wx)
+                full[c, :, y0 + yl:y0 + yh, x0 + xl:x0 + xh] += a[:, yl:yh, xl:xh]
+        return f, full.reshape(-1)
+
+    def direction(self, grad):
+        q = grad.copy()
+        al = []
+        for s, y in reversed(list(zip(self.s_hist, self.y_hist))):
+            a = (s @ q) / (y @ s)
+            al.append(a)
+            q -= a * y
+        if self.y_hist:
+            s, y = self.s_hist[-1], self.y_hist[-1]
+            q *= (s @ y) / (y @ y)
+        else:
+            q *= self.step0 / max(np.abs(q).max(), 1e-300)
+        for (s, y), a in zip(zip(self.s_hist, self.y_hist), reversed(al)):
+            b = (y @ q) / (y @ s)
+            q += (a - b) * s
+        return -q
+
+    def first(self):
+        self.trial = self.x
+        return self.jobs(self.x)
+
+    def update(self, results):
+        """Results of the submitted jobs in; the next jobs out (None: done)."""
+        f, grad = self.stack(results)
+        if self.f_cur is None or f < self.f_cur or self.halvings >= 4:
+            if self.f_cur is not None:
+                s, y = self.trial - self.x, grad - self.g_cur
+                if s @ y > 0:
+                    self.s_hist.append(s)
+                    self.y_hist.append(y)
+                    self.s_hist, self.y_hist = self.s_hist[-self.memory:], self.y_hist[-self.memory:]
+                self.it += 1
+            self.x, self.f_cur, self.g_cur = self.trial, f, grad
+            self.misfits.append(f)
+            self.halvings = 0
+            if self.it >= self.iterations:
+                return None
+            self.p = self.direction(grad)
+            self.alpha = 1.0
+        else:
+            self.alpha *= 0.5
+            self.halvings += 1
+        self.trial = self.x + self.alpha * self.p
+        return self.jobs(self.trial)
+
+
+def plain_gradient(ctx, job):
+    """A gradient job through vti3d_plan_gradient (VTI_OPT_FULL_STEPS) on the
+    job's grid: (fgcij, misfit)."""
+    c11, c13, c33, w, so, rec, dobs, randb = job._keep
+    p = Plan3d(ctx, job.g, OPT_FULL_STEPS)
+    try:
+        p.set_model(c11, c13, c33, randb=randb)
+        p.set_wavelet(w)
+        p.set_receivers(rec)
+        return p.gradient(so, [0], dobs)
+    finally:
+        p.close()
+
+
+class Server:
+    """Continuous-batching request loop on one GPU."""
+
+    def __init__(self, device=0, max_bytes=64 << 30, chunk=16):
+        self.ctx3 = Context(device)
+        self.ctx2 = Context(device)
+        self.engine = Engine3d(self.ctx3, max_bytes)
+        self.chunk = chunk
+
+    def close(self):
+        self.engine.close()
+        self.ctx3.close()
+        self.ctx2.close()
+
+    def run(self, requests, fwi: FwiDriver | None = None, t_limit=3600.0):
+        t0 = time.perf_counter()
+        now = lambda: time.perf_counter() - t0  # noqa: E731
+        pending = deque(sorted(requests, key=lambda r: r.arrival))
+        waiting = deque()
+        q2 = queue.Queue()
+        inflight = {}
+        done = []
+        fwi_reqs = []
+
+        def worker():
+            while True:
+                r = q2.get()
+                if r is None:
+                    return
+                r.t_admit = now()
+                r.result = r.make()(self.ctx2)
+                r.t_done = now()
+                done.append(r)
+
+        th = threading.Thread(target=worker, daemon=True)
+        th.start()
+
+        def submit_fwi(jobs):
+            for k, j in enumerate(jobs):
+                r = Request(-1, 3, "gradient", now(), lambda jj=j: jj, tag=k)
+                fwi_reqs.append(r)
+                waiting.append(r)
+
+        if fwi is not None:
+            submit_fwi(fwi.first())
+        fwi_batch = {}
+        n2 = sum(r.dim == 2 for r in requests)
+        while now() < t_limit:
+            t = now()
+            while pending and pending[0].arrival <= t:
+                r = pending.popleft()
+                (q2.put(r) if r.dim == 2 else waiting.append(r))
+            refused = False
+            while waiting:
+                r = waiting[0]
+                if r.result is None and not hasattr(r, "_job"):
+                    r._job = r.make()
+                jid = self.engine.submit(r._job)
+                if jid is None:
+                    refused = True
+                    break
+                waiting.popleft()
+                r.t_admit = now()
+                inflight[jid] = r
+            active = self.engine.step(self.chunk) if inflight else 0
+            for jid in self.engine.poll():
+                r = inflight.pop(jid)
+                r.result = self.engine.result(jid)
+                r.t_done = now()
+                del r._job
+                if r.rid >= 0:
+                    done.append(r)
+                else:
+                    fwi_batch[r.tag] = r.result
+            if fwi is not None and fwi_batch and len(fwi_batch) == len(fwi.shots):
+                nxt = fwi.update([fwi_batch[k] for k in range(len(fwi.shots))])
+                fwi_batch = {}
+                if nxt is not None:
+                    submit_fwi(nxt)
+                else:
+                    fwi = None
+            n_done = sum(r.rid >= 0 for r in done)
+            if n_done == len(requests) and fwi is None and not inflight and not waiting:
+                break
+            if not active and not inflight:
+                if refused:
+                    raise RuntimeError("request larger than the engine's memory budget")
+                if waiting:
+                    continue
+                if pending:
+                    time.sleep(max(0.0, min(pending[0].arrival - now(), 0.05)))
+                elif len(done) < len(requests):
+                    time.sleep(0.002)
+        q2.put(None)
+        th.join()
+        lat = np.array([r.latency for r in done if r.rid >= 0])
+        first = min(r.arrival for r in requests) if requests else 0.0
+        last = max((r.t_done for r in done), default=first)
+        return {
+            "requests": len(requests), "done": int(len(lat)), "n2d": n2,
+            "n3d": len(requests) - n2,
+            "p50_s": float(np.percentile(lat, 50)) if len(lat) else None,
+            "p99_s": float(np.percentile(lat, 99)) if len(lat) else None,
+            "makespan_s": last - first,
+            "requests_per_s": len(lat) / max(last - first, 1e-9),
+            "fwi_requests": len(fwi_reqs),
+        }
