@@ -455,6 +455,140 @@ def run_batched(args):
     return out
 
 
+def run_served(args):
+    """Served workload: Poisson arrivals (mean 20 req/s, seed 7) of mixed
+    modeling and gradient requests, half 2D (201x401 .. 401x801) and half 3D
+    (128^3 .. 200x400x400), nt U{2000..4000}, Ricker U[10, 15] Hz, random-
+    boundary mode, served by the continuous-batching engine (3D) and a second
+    stream (2D), with L-BFGS FWI iterations (gradients of shots on windows of
+    the 400x400x200 model) interleaved. The plain form serves the same
+    requests one at a time in arrival order (3D through vti3d_plan_*, 2D the
+    same calls, one stream) and runs the same FWI iterations with
+    vti3d_plan_gradient one shot at a time."""
+    import torch
+    import vtib200 as V
+    import vtib200.serve as SV
+    import vtib200.synth as S
+
+    torch.cuda.set_device(0)
+
+    def fwi_case():
+        kw = dict(CONFIGS["gradient400"])
+        kw["nt"] = args.fwi_nt
+        s = S.survey3d(**kw)
+        tv, te, td = s.extra["true"]
+        ctrue = s.cij(tv, te, td)
+        g = s.geom()
+        wins = S.batch_windows(s.nx, s.ny, args.fwi_shots, 160, 400, seed=5)
+        souloc, recloc = S.batch_survey3d(s, wins, rec_step=2, rec_depth=25.0, src_depth=25.0)
+        ctx = V.Context(0)
+        shots = []
+        for k, (x0, y0, wx, wy) in enumerate(wins):
+            so = souloc[5 * k:5 * k + 5].copy()
+            nr, first = int(so[3]), int(so[4])
+            rec = recloc[4 * first:4 * (first + nr)].copy()
+            so[4] = 0
+            sub = V.geom3d(wx, wy, g.nz, g.nt, g.npad, g.dx, g.dy, g.dz, g.dt, g.sampling_rate,
+                           ox=g.ox + x0 * g.dx, oy=g.oy + y0 * g.dy, oz=g.oz)
+            p = V.Plan3d(ctx, sub, V.OPT_FULL_STEPS)
+            ct = ctrue.reshape(3, g.nz, g.ny, g.nx)[:, :, y0:y0 + wy, x0:x0 + wx]
+            p.set_model(*[c.reshape(-1) for c in ct])
+            p.set_wavelet(s.wavelet)
+            p.set_receivers(rec)
+            dobs = p.model_data(so, [0])
+            p.close()
+            shots.append((so, rec, dobs, (x0, y0, wx, wy)))
+        ctx.close()
+        c0 = s.cij()
+        return g, c0, s.wavelet, shots, float(np.abs(c0).max() * 2e-3)
+
+    log = lambda m: print(m, file=sys.stderr, flush=True)  # noqa: E731
+    budget = int(args.budget_gib * (1 << 30))
+
+    def serve(fwi=None):
+        srv = SV.Server(max_bytes=budget, chunk=args.chunk, keep_results=False, log=log)
+        t0 = time.perf_counter()
+        st = srv.run(SV.make_requests(args.requests, rate=20.0, seed=7) if fwi is None or
+                     args.requests_with_fwi else [], fwi=fwi)
+        st["wall_s"] = time.perf_counter() - t0
+        st["launches"] = srv.ctx3.launches + srv.ctx2.launches
+        srv.close()
+        return st
+
+    def plain_requests():
+        """One request at a time in arrival order, one stream."""
+        ctx = V.Context(0)
+        reqs_p = SV.make_requests(args.requests, rate=20.0, seed=7)
+        t0 = time.perf_counter()
+        lat = []
+        for r in reqs_p:
+            now = time.perf_counter() - t0
+            if r.arrival > now:
+                time.sleep(r.arrival - now)
+            if r.dim == 2:
+                r.make()(ctx)
+            else:
+                job = r.make()
+                if job.kind == V.JOB_MODEL:
+                    jc11, jc13, jc33, jw, jso, jrec = job._keep[:6]
+                    p = V.Plan3d(ctx, job.g, V.OPT_FULL_STEPS)
+                    p.set_model(jc11, jc13, jc33)
+                    p.set_wavelet(jw)
+                    p.set_receivers(jrec)
+                    p.model_data(jso, [0])
+                    p.close()
+                else:
+                    SV.plain_gradient(ctx, job)
+            lat.append(time.perf_counter() - t0 - r.arrival)
+            log(f"plain request {r.rid} done at {time.perf_counter() - t0:.2f} s")
+        span = time.perf_counter() - t0 - min(r.arrival for r in reqs_p)
+        ctx.close()
+        return {"requests_per_s": round(len(lat) / span, 4), "makespan_s": span,
+                "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99))}
+
+    with ClockSampler(0) as clk:
+        served = serve()
+    out = {
+        "metric": "served VTI requests: requests/s with p50/p99 latency (continuous batching)",
+        "value": round(served["requests_per_s"], 4), "unit": "requests/s", "n_gpus": 1,
+        "steps": 1, "warmup": 0, "ms_per_step": round(served["wall_s"] * 1e3, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded requests: layered VTI models, Ricker sources; zero observed "
+                "traces for request gradients, modeled traces for the FWI)",
+        "config": {"workload": f"{args.requests} requests, Poisson 20/s (seed 7), 2D 201x401.."
+                               "401x801 / 3D 128^3..200x400x400, nt U{2000..4000}, Ricker "
+                               f"U[10,15] Hz; FWI {args.fwi_iters} iterations x "
+                               f"{args.fwi_shots} shots on 400x400x200 windows, nt={args.fwi_nt}",
+                   "engine_budget_gib": args.budget_gib, "chunk_ticks": args.chunk},
+        "latency_s": {"p50": served["p50_s"], "p99": served["p99_s"]},
+        "served": served,
+        "gpu_launches": int(served["launches"]), "clocks": clk.summary(),
+    }
+    if args.plain:
+        pl = plain_requests()
+        out["plain"] = pl
+        out["speedup_vs_plain"] = round(served["requests_per_s"] / pl["requests_per_s"], 3)
+    if args.fwi_iters > 0:
+        g, c0, w, shots, step0 = fwi_case()
+        fwi = SV.FwiDriver(g, c0, w, shots, iterations=args.fwi_iters, step0=step0)
+        t0 = time.perf_counter()
+        st = serve(fwi)
+        out["fwi"] = {"misfits": fwi.misfits, "evaluations": st["fwi_requests"],
+                      "wall_s": time.perf_counter() - t0,
+                      "requests_beside": st["requests"], "p50_s": st["p50_s"],
+                      "p99_s": st["p99_s"]}
+        if args.plain:
+            ctx = V.Context(0)
+            pf = SV.FwiDriver(g, c0, w, shots, iterations=args.fwi_iters, step0=step0)
+            t0 = time.perf_counter()
+            out["fwi"]["plain_misfits"] = pf.run_plain(ctx)
+            out["fwi"]["plain_wall_s"] = time.perf_counter() - t0
+            ctx.close()
+            out["fwi"]["same_as_plain"] = out["fwi"]["plain_misfits"] == fwi.misfits
+    print(json.dumps(out), flush=True)
+    return out
+
+
 def run_reference(args):
     """Reference arm: the reference algorithm's CPU implementation (the FP32
     oracle port; the reference's own CPU path needs ISPC and TBB, absent
@@ -507,15 +641,27 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default="gradient400", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--workload", default="gradient", choices=["gradient", "batched"],
+    ap.add_argument("--workload", default="gradient", choices=["gradient", "batched", "served"],
                     help="batched: many shots on their own windows vs the plain loop")
     ap.add_argument("--shots", type=int, default=64, help="batched workload: shots")
     ap.add_argument("--plain-shots", type=int, default=3,
                     help="batched workload: shots timed in the plain per-shot loop")
     ap.add_argument("--nt", type=int, default=0, help="batched workload: time samples")
+    ap.add_argument("--requests", type=int, default=40, help="served workload: requests")
+    ap.add_argument("--budget-gib", type=float, default=100.0,
+                    help="served workload: engine device-memory budget (GiB)")
+    ap.add_argument("--fwi-iters", type=int, default=10, help="served workload: FWI iterations")
+    ap.add_argument("--fwi-shots", type=int, default=20, help="served workload: FWI shots")
+    ap.add_argument("--fwi-nt", type=int, default=1000, help="served workload: FWI time samples")
+    ap.add_argument("--plain", action="store_true", help="served workload: also the plain form")
+    ap.add_argument("--chunk", type=int, default=32, help="served workload: ticks per step")
+    ap.add_argument("--requests-with-fwi", action="store_true",
+                    help="served workload: run the requests again beside the FWI")
     args = ap.parse_args()
     if args.workload == "batched" and args.impl == "b200":
         run_batched(args)
+    elif args.workload == "served" and args.impl == "b200":
+        run_served(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -129,19 +129,20 @@ class FwiDriver:
     gradient requests on windows of the model, one request per shot and
     iteration; the next iteration is submitted when the last gradient of the
     current one has arrived. A step that raises the misfit is halved and
-    re-evaluated (at most 4 times)."""
+    re-evaluated (at most `max_halvings` times)."""
     g: object
     model: np.ndarray
     wavelet: np.ndarray
     shots: list          # (souloc[5], recloc, dobs, window) per shot
     iterations: int
-    memory: int = 5
+    memory: int = 3
+    max_halvings: int = 2
     misfits: list = field(default_factory=list)
     step0: float = 0.0
 
     def __post_init__(self):
         self.s_hist, self.y_hist = [], []
-        self.x = self.model.astype(np.float64)
+        self.x = np.array(self.model, dtype=np.float32)
         self.it = 0
         self.g_cur = None
         self.f_cur = None
@@ -181,7 +182,7 @@ class FwiDriver:
 
     def stack(self, results):
         g, n = self.g, self.g.nx * self.g.ny * self.g.nz
-        full = np.zeros((3, g.nz, g.ny, g.nx))
+        full = np.zeros((3, g.nz, g.ny, g.nx), dtype=np.float32)
         f = 0.0
         for (fg, mis), (_, _, _, (x0, y0, wx, wy)) in zip(results, self.shots):
             f += mis
@@ -194,20 +195,21 @@ class FwiDriver:
         return f, full.reshape(-1)
 
     def direction(self, grad):
+        """L-BFGS two-loop recursion; vectors in FP32, dot products in FP64."""
         q = grad.copy()
         al = []
         for s, y in reversed(list(zip(self.s_hist, self.y_hist))):
-            a = (s @ q) / (y @ s)
+            a = _dot(s, q) / _dot(y, s)
             al.append(a)
-            q -= a * y
+            q -= np.float32(a) * y
         if self.y_hist:
             s, y = self.s_hist[-1], self.y_hist[-1]
-            q *= (s @ y) / (y @ y)
+            q *= np.float32(_dot(s, y) / _dot(y, y))
         else:
-            q *= self.step0 / max(np.abs(q).max(), 1e-300)
+            q *= np.float32(self.step0 / max(float(np.abs(q).max()), 1e-300))
         for (s, y), a in zip(zip(self.s_hist, self.y_hist), reversed(al)):
-            b = (y @ q) / (y @ s)
-            q += (a - b) * s
+            b = _dot(y, q) / _dot(y, s)
+            q += np.float32(a - b) * s
         return -q
 
     def first(self):
@@ -217,10 +219,10 @@ class FwiDriver:
     def update(self, results):
         """Results of the submitted jobs in; the next jobs out (None: done)."""
         f, grad = self.stack(results)
-        if self.f_cur is None or f < self.f_cur or self.halvings >= 4:
+        if self.f_cur is None or f < self.f_cur or self.halvings >= self.max_halvings:
             if self.f_cur is not None:
                 s, y = self.trial - self.x, grad - self.g_cur
-                if s @ y > 0:
+                if _dot(s, y) > 0:
                     self.s_hist.append(s)
                     self.y_hist.append(y)
                     self.s_hist, self.y_hist = self.s_hist[-self.memory:], self.y_hist[-self.memory:]
@@ -235,8 +237,12 @@ class FwiDriver:
         else:
             self.alpha *= 0.5
             self.halvings += 1
-        self.trial = self.x + self.alpha * self.p
+        self.trial = self.x + np.float32(self.alpha) * self.p
         return self.jobs(self.trial)
+
+
+def _dot(a, b):
+    return float(np.einsum("i,i->", a, b, dtype=np.float64))
 
 
 def plain_gradient(ctx, job):
@@ -253,14 +259,29 @@ def plain_gradient(ctx, job):
         p.close()
 
 
+def _summary(res):
+    """(sum, L2 norm, misfit) of a result, for callers that keep no arrays."""
+    arrs = [a for a in (res if isinstance(res, tuple) else (res,)) if isinstance(a, np.ndarray)]
+    mis = [float(a) for a in (res if isinstance(res, tuple) else ()) if isinstance(a, float)]
+    return (sum(float(np.sum(a, dtype=np.float64)) for a in arrs),
+            sum(float(np.linalg.norm(a.reshape(-1).astype(np.float64))) for a in arrs),
+            mis[-1] if mis else None)
+
+
 class Server:
     """Continuous-batching request loop on one GPU."""
 
-    def __init__(self, device=0, max_bytes=64 << 30, chunk=16):
+    def __init__(self, device=0, max_bytes=64 << 30, chunk=16, keep_results=True, log=None):
         self.ctx3 = Context(device)
         self.ctx2 = Context(device)
         self.engine = Engine3d(self.ctx3, max_bytes)
         self.chunk = chunk
+        self.keep_results = keep_results
+        self.log = log
+
+    def _log(self, msg):
+        if self.log:
+            self.log(msg)
 
     def close(self):
         self.engine.close()
@@ -277,15 +298,30 @@ class Server:
         done = []
         fwi_reqs = []
 
+        ready = {}  # request id -> prepared 3D job (built off the stepping thread)
+        q3 = queue.Queue()
+
+        def prep():
+            while True:
+                r = q3.get()
+                if r is None:
+                    return
+                ready[id(r)] = r.make()
+
+        tp = threading.Thread(target=prep, daemon=True)
+        tp.start()
+
         def worker():
             while True:
                 r = q2.get()
                 if r is None:
                     return
                 r.t_admit = now()
-                r.result = r.make()(self.ctx2)
+                res = r.make()(self.ctx2)
+                r.result = res if self.keep_results else _summary(res)
                 r.t_done = now()
                 done.append(r)
+                self._log(f"request {r.rid} (2D {r.kind}) done at {r.t_done:.2f} s")
 
         th = threading.Thread(target=worker, daemon=True)
         th.start()
@@ -293,6 +329,7 @@ class Server:
         def submit_fwi(jobs):
             for k, j in enumerate(jobs):
                 r = Request(-1, 3, "gradient", now(), lambda jj=j: jj, tag=k)
+                r._job = j
                 fwi_reqs.append(r)
                 waiting.append(r)
 
@@ -304,12 +341,18 @@ class Server:
             t = now()
             while pending and pending[0].arrival <= t:
                 r = pending.popleft()
-                (q2.put(r) if r.dim == 2 else waiting.append(r))
+                if r.dim == 2:
+                    q2.put(r)
+                else:
+                    q3.put(r)
+                    waiting.append(r)
             refused = False
             while waiting:
                 r = waiting[0]
-                if r.result is None and not hasattr(r, "_job"):
-                    r._job = r.make()
+                if not hasattr(r, "_job"):
+                    if id(r) not in ready:
+                        break  # still being built
+                    r._job = ready.pop(id(r))
                 jid = self.engine.submit(r._job)
                 if jid is None:
                     refused = True
@@ -320,16 +363,20 @@ class Server:
             active = self.engine.step(self.chunk) if inflight else 0
             for jid in self.engine.poll():
                 r = inflight.pop(jid)
-                r.result = self.engine.result(jid)
+                res = self.engine.result(jid)
                 r.t_done = now()
                 del r._job
                 if r.rid >= 0:
+                    r.result = res if self.keep_results else _summary(res)
                     done.append(r)
+                    self._log(f"request {r.rid} ({r.dim}D {r.kind}) done at {r.t_done:.2f} s")
                 else:
-                    fwi_batch[r.tag] = r.result
+                    fwi_batch[r.tag] = res
             if fwi is not None and fwi_batch and len(fwi_batch) == len(fwi.shots):
                 nxt = fwi.update([fwi_batch[k] for k in range(len(fwi.shots))])
                 fwi_batch = {}
+                self._log(f"FWI evaluation done at {now():.2f} s, misfit {fwi.misfits[-1]:.6g}, "
+                          f"iteration {fwi.it}")
                 if nxt is not None:
                     submit_fwi(nxt)
                 else:
@@ -341,13 +388,16 @@ class Server:
                 if refused:
                     raise RuntimeError("request larger than the engine's memory budget")
                 if waiting:
+                    time.sleep(0.001)  # a job is being built
                     continue
                 if pending:
                     time.sleep(max(0.0, min(pending[0].arrival - now(), 0.05)))
                 elif len(done) < len(requests):
                     time.sleep(0.002)
         q2.put(None)
+        q3.put(None)
         th.join()
+        tp.join()
         lat = np.array([r.latency for r in done if r.rid >= 0])
         first = min(r.arrival for r in requests) if requests else 0.0
         last = max((r.t_done for r in done), default=first)
