@@ -349,6 +349,22 @@ int vti3d_engine_poll(vti3d_engine* e, int* ids, int max_ids, int* n_done);
 int vti3d_engine_result(vti3d_engine* e, int id, float* out, double* misfit);
 int vti3d_engine_stats(vti3d_engine* e, size_t* used_bytes, int* jobs, int* tick);
 
+/* ------------------------------------------- 3D Gauss-Newton product */
+/* Exact-mode 3D Gauss-Newton Hessian-vector product and gradient of one shot
+ * (no counterpart on the reference's GPU; its CPU twin has bornCij /
+ * adjointCij, lib/vti-fwi-3d/cpu/laplacian3d.ispc:132-190). Forward operator:
+ * the 3D VTI step with the sponge as a plain diagonal, every level up to
+ * nt-1, receivers at their own cells; its Born linearisation along dc and its
+ * exact discrete adjoint. Background checkpoints every `checkpoint_every`
+ * levels (0: 64), recomputed per block in the backward pass.
+ * Outputs (host, each may be NULL): hv = H dc (3*nxyz), grad = dJ/dc of
+ * J = 1/2|d - dobs|^2 (3*nxyz; needs dobs), misfit = J, traces d and Born
+ * traces (nnt*nrec each). souloc: 5 floats (x, y, z, nrec, 0). */
+int vti3d_gnhv_exact(vti_ctx* ctx, const vti3d_geom* g, const float* c11, const float* c13,
+                     const float* c33, const float* dc, const float* wavelet, const float* souloc,
+                     const float* recloc, int nrec, const float* dobs, int checkpoint_every,
+                     float* hv, float* grad, double* misfit, float* traces, float* born);
+
 #ifdef __cplusplus
 }
 #endif

@@ -177,6 +177,12 @@ def exact_adjoint3d(g, c11, c13, c33, wavelet, souloc, shotid, recloc, res):
                     [res], 3 * g.nx * g.ny * g.nz)
 
 
+def exact_gnhv3d(g, c11, c13, c33, wavelet, souloc, shotid, recloc, dc):
+    """H dc = B^T B dc in EXACT mode (B: Born operator), FP64."""
+    bd = exact_born3d(g, c11, c13, c33, wavelet, souloc, shotid, recloc, dc)
+    return exact_adjoint3d(g, c11, c13, c33, wavelet, souloc, shotid, recloc, bd)
+
+
 def damping3d(nx, ny, nz, npad):
     out = np.zeros(nx * ny + nz, dtype=np.float32)
     lib().orc3d_damping(nx, ny, nz, npad, _p(out))

@@ -136,13 +136,15 @@ struct TileMaps {
 int make_tile_maps(vti_ctx* ctx, const Dims3& d, const Vol& v, TileMaps* out);
 
 // One forward-form leapfrog step over the update region (x,y in [4,n-4),
-// all z), next written over prev; damp == nullptr: no sponge (random-boundary
-// pass). TMA-pipelined, see vti_tma3d.cu.
+// all z): next written through px_ptr/pz_ptr (prev is read through the px/pz
+// maps; the same volume for an in-place step); damp == nullptr: no sponge
+// (random-boundary pass); exact: the sponge as a plain diagonal (exact-mode
+// operator). TMA-pipelined, see vti_tma3d.cu.
 int launch_fwd3d_tma(vti_ctx* ctx, const Dims3& d, const TileMaps& cx, const TileMaps& cz,
                      const TileMaps& px, const TileMaps& pz, const TileMaps& c11,
                      const TileMaps& c13, const TileMaps& c33, const float* cz_ptr,
                      float* px_ptr, float* pz_ptr, const Damping* damp, float sx, float sy,
-                     float sz, PointSource src, Probe probe = Probe());
+                     float sz, PointSource src, Probe probe = Probe(), bool exact = false);
 // Fused backward step: sigma back one level (gradient form, no sponge, +src),
 // adjoint lambda one level (forward form, sponge), zero-lag imaging into g
 // (rtm: the RTM image in g11 instead).

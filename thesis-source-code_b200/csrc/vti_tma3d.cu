@@ -33,7 +33,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
-#include "vti_internal.h"
+#include "vti_tma_common.cuh"
 
 namespace vti {
 
@@ -44,90 +44,6 @@ namespace vti {
   } while (0)
 
 namespace {
-
-constexpr float kC0 = -2.84722222222f, kC1 = 1.6f, kC2 = -0.2f, kC3 = 0.02539682539f,
-                kC4 = -0.00178571428f;
-
-constexpr int TX = 32, TY = 16, RY = 2, NCW = TY / RY;  // consumer warps
-constexpr int NTHREADS = (NCW + 1) * 32;
-constexpr int HX = TX + 2 * kHalo, HY = TY + 2 * kHalo;
-constexpr int PLAIN_BYTES = TX * TY * 4;  // 2048
-constexpr int HALO_BYTES = HX * HY * 4;   // 3840
-constexpr unsigned kSpinLimit = 1u << 26;
-
-__device__ __forceinline__ float lap9(float c, float m1, float p1, float m2, float p2, float m3,
-                                      float p3, float m4, float p4) {
-  float s = kC0 * c;
-  s = fmaf(kC1, m1 + p1, s);
-  s = fmaf(kC2, m2 + p2, s);
-  s = fmaf(kC3, m3 + p3, s);
-  s = fmaf(kC4, m4 + p4, s);
-  return s;
-}
-
-// Two adjacent floats (8-byte aligned: x offsets are even, rows even-sized).
-__device__ __forceinline__ float2 ld2(const float* p) {
-  return *reinterpret_cast<const float2*>(p);
-}
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-               "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-      " selp.u32 %0, 1, 0, p;\n}"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// Bounded wait; false (and the status word set) if the phase never completes.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* status) {
-  for (unsigned i = 0; i < kSpinLimit; ++i)
-    if (mbar_try_wait(bar, parity)) return true;
-  atomicOr(status, 1 << VTI_ERR_TIMEOUT);
-  return false;
-}
-__device__ __forceinline__ void tma_load(void* dst, const CUtensorMap* map, uint64_t* bar, int x,
-                                         int y, int z) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(smem_u32(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
-      : "memory");
-}
-
-struct Sched {
-  int gx, gy;  // columns in x, y
-  int nz;
-  int seg;     // planes per segment
-  int items;   // gx * gy * ceil(nz / seg)
-  int grid;    // persistent CTAs, min(items, resident slots)
-};
-
-// Item i: segment i / (gx*gy) of column i % (gx*gy), planes [z0, z1).
-__device__ __forceinline__ void item(const Sched& s, int i, int& bx, int& by, int& z0,
-                                     int& z1) {
-  const int cols = s.gx * s.gy;
-  const int sg = i / cols, col = i - sg * cols;
-  bx = col % s.gx;
-  by = col / s.gx;
-  z0 = sg * s.seg;
-  z1 = min(s.nz, z0 + s.seg);
-}
 
 // ------------------------------------------------------------ forward
 // Forward step arguments: the part every step of a job shares and the part
@@ -197,7 +113,10 @@ __device__ __forceinline__ bool fwd_produce(const FwdCommon& a, const FwdMaps& m
 // Consumer side of one item. Thread (lane, warp) owns the x pair
 // x0 + 2*(lane%16) + {0,1} of tile row 2*warp + lane/16; shared-memory reads
 // and global stores are float2.
-template <bool kProbe>
+// kExact: the sponge as a plain diagonal (next = D(C L cur + 2 cur - D prev),
+// no block-order reading of the z stencil): the exact-mode forward operator
+// whose discrete adjoint the Gauss-Newton product uses.
+template <bool kProbe, bool kExact = false>
 __device__ __forceinline__ bool fwd_consume(const FwdCommon& a, const FwdPar& bp,
                                             const Probe& probe, int* status, int li, float amp,
                                             const unsigned char* smem, uint64_t* full,
@@ -231,7 +150,7 @@ __device__ __forceinline__ bool fwd_consume(const FwdCommon& a, const FwdPar& bp
                    ? __ldg(reinterpret_cast<const float2*>(bp.cz + (long long)zz * a.d.plane + off))
                    : make_float2(0.f, 0.f);
     // planes of the block above z0 were already damped as "cur"
-    if (damp && zz >= 0 && (zz >> 2) < (z0 >> 2)) {
+    if (!kExact && damp && zz >= 0 && (zz >> 2) < (z0 >> 2)) {
       v.x *= dxy[0] * a.dampz[zz];
       v.y *= dxy[1] * a.dampz[zz];
     }
@@ -324,7 +243,7 @@ __device__ __forceinline__ bool fwd_consume(const FwdCommon& a, const FwdPar& bp
     }
     // entering the next plane: if it starts a new 4-plane block of the same
     // column, the four planes of the block just finished become "damped cur"
-    if (damp && ((z + 1) & 3) == 0 && z + 1 < a.d.nz) {
+    if (!kExact && damp && ((z + 1) & 3) == 0 && z + 1 < a.d.nz) {
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
         // after the shift at z+1, entries 0..3 hold planes z-3..z; they are
@@ -337,29 +256,9 @@ __device__ __forceinline__ bool fwd_consume(const FwdCommon& a, const FwdPar& bp
   return true;
 }
 
-// Kernel prologue shared by the step kernels: 1024-aligned stage ring and
-// its full/empty mbarriers.
-template <int kStages, int kStageBytes>
-__device__ __forceinline__ unsigned char* ring_init(unsigned char* smem_raw, uint64_t*& full,
-                                                    uint64_t*& empty) {
-  unsigned char* smem =
-      (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  full = (uint64_t*)(smem + kStages * kStageBytes);
-  empty = full + kStages;
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < kStages; ++s) {
-      mbar_init(&full[s], 1);
-      mbar_init(&empty[s], NCW);
-    }
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  __syncthreads();
-  return smem;
-}
-
 // kProbe: the probe point of FwdArgs is read out (wavelet gradient); the
 // propagation kernels are instantiated without it.
-template <bool kProbe>
+template <bool kProbe, bool kExact>
 __global__ void __launch_bounds__(NTHREADS, 3)
     k_fwd3d_tma(const __grid_constant__ FwdMaps m0, const __grid_constant__ FwdArgs a0) {
   extern __shared__ unsigned char smem_raw[];
@@ -374,8 +273,8 @@ __global__ void __launch_bounds__(NTHREADS, 3)
     return;
   }
   for (int it = blockIdx.x; it < a0.c.sc.items; it += gridDim.x)
-    if (!fwd_consume<kProbe>(a0.c, a0.p, a0.probe, a0.status, it, a0.c.src.amp, smem, full,
-                             empty, k, warp, lane))
+    if (!fwd_consume<kProbe, kExact>(a0.c, a0.p, a0.probe, a0.status, it, a0.c.src.amp, smem,
+                                     full, empty, k, warp, lane))
       break;
 }
 
@@ -759,6 +658,8 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_bwd3d_batch(const __grid_consta
 
 static_assert(sizeof(FwdBatch) <= 32000 && sizeof(BwdBatch) <= 32000, "kernel parameter size");
 
+}  // namespace
+
 // ------------------------------------------------------------ host side
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -804,7 +705,6 @@ Sched make_sched(vti_ctx* ctx, const Dims3& d, int ctas_per_sm) {
   return s;
 }
 
-}  // namespace
 
 int make_tile_maps(vti_ctx* ctx, const Dims3& d, const Vol& v, TileMaps* out) {
   auto fn = encode_fn();
@@ -867,7 +767,7 @@ FwdCommon fwd_common(const Dims3& d, const Sched& sc, const Damping* damp, float
   return c;
 }
 
-bool attr_fwd[2][64] = {}, attr_bwd[2][64] = {}, attr_fwd_batch[64] = {},
+bool attr_fwd[3][64] = {}, attr_bwd[2][64] = {}, attr_fwd_batch[64] = {},
      attr_bwd_batch[64] = {};
 
 }  // namespace
@@ -876,10 +776,13 @@ int launch_fwd3d_tma(vti_ctx* ctx, const Dims3& d, const TileMaps& cx, const Til
                      const TileMaps& px, const TileMaps& pz, const TileMaps& c11,
                      const TileMaps& c13, const TileMaps& c33, const float* cz_ptr,
                      float* px_ptr, float* pz_ptr, const Damping* damp, float sx, float sy,
-                     float sz, PointSource src, Probe probe) {
+                     float sz, PointSource src, Probe probe, bool exact) {
   const bool pr = probe.x >= 0 && probe.out;
-  VTI_TRY_ST(set_smem_attr(ctx, pr ? k_fwd3d_tma<true> : k_fwd3d_tma<false>, F_SMEM,
-                           attr_fwd[pr]));
+  if (pr && exact) return fail(ctx, VTI_ERR_UNSUPPORTED, "probe with the exact-mode step");
+  auto kern = pr ? k_fwd3d_tma<true, false>
+                 : (exact ? k_fwd3d_tma<false, true> : k_fwd3d_tma<false, false>);
+  const int variant = pr ? 1 : (exact ? 2 : 0);
+  VTI_TRY_ST(set_smem_attr(ctx, kern, F_SMEM, attr_fwd[variant]));
   FwdMaps m;
   m.cx = *H(cx); m.cz = *P(cz); m.px = *P(px); m.pz = *P(pz);
   m.c11 = *P(c11); m.c13 = *P(c13); m.c33 = *P(c33);
@@ -891,7 +794,6 @@ int launch_fwd3d_tma(vti_ctx* ctx, const Dims3& d, const TileMaps& cx, const Til
   const int grid = a.c.sc.grid;
   {
     LaunchTimer tm(ctx, kTimedFwd3d);
-    auto kern = pr ? k_fwd3d_tma<true> : k_fwd3d_tma<false>;
     kern<<<grid, NTHREADS, F_SMEM, ctx->stream>>>(m, a);
   }
   VTI_LAUNCHED(ctx, "k_fwd3d_tma");

@@ -130,6 +130,8 @@ def _signatures():
         "vti3d_batch_autotune": (C.c_int, [P, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "vti3d_batch_gradient": (C.c_int, [P, P, C.c_int, P, C.c_int, C.POINTER(C.c_double)]),
         "vti3d_batch_get_shot_models": (C.c_int, [P, C.c_int, P, P]),
+        "vti3d_gnhv_exact": (C.c_int, [P] * 9 + [C.c_int, P, C.c_int, P, P,
+                                               C.POINTER(C.c_double), P, P]),
         "vti3d_engine_job_bytes": (C.c_size_t, [P]),
         "vti3d_engine_create": (C.c_int, [P, C.c_size_t, C.POINTER(VP)]),
         "vti3d_engine_destroy": (C.c_int, [P]),
@@ -492,6 +494,35 @@ class Engine3d:
             self.close()
         except Exception:
             pass
+
+
+def gnhv_exact(ctx, g: Geom3d, c11, c13, c33, wavelet, souloc, recloc, dc=None, dobs=None,
+               checkpoint_every=0, want=("hv", "grad", "traces", "born")):
+    """vti3d_gnhv_exact: exact-mode Gauss-Newton product H dc, gradient,
+    misfit and traces of one shot. Returns a dict of the requested outputs."""
+    n = g.nx * g.ny * g.nz
+    recloc = _f32(recloc).reshape(-1)
+    nrec = recloc.size // 4
+    nnt = nnt3d(g)
+    out = {}
+    hv = np.zeros(3 * n, dtype=np.float32) if "hv" in want and dc is not None else None
+    grad = np.zeros(3 * n, dtype=np.float32) if "grad" in want and dobs is not None else None
+    tr = np.zeros(nnt * nrec, dtype=np.float32) if "traces" in want else None
+    born = np.zeros(nnt * nrec, dtype=np.float32) if "born" in want and dc is not None else None
+    mis = C.c_double(0)
+    args = [_f32(c11), _f32(c13), _f32(c33), None if dc is None else _f32(dc), _f32(wavelet),
+            _f32(souloc), recloc]
+    dobs_ = None if dobs is None else _f32(dobs)
+    ctx.check(lib().vti3d_gnhv_exact(ctx.handle, C.byref(g), *[_p(a) for a in args], nrec,
+                                     _p(dobs_), checkpoint_every, _p(hv), _p(grad),
+                                     C.byref(mis) if dobs is not None else None, _p(tr),
+                                     _p(born)))
+    for k, v in (("hv", hv), ("grad", grad), ("traces", tr), ("born", born)):
+        if v is not None:
+            out[k] = v
+    if dobs is not None:
+        out["misfit"] = mis.value
+    return out
 
 
 # ------------------------------------------------------- reference-named API

@@ -129,7 +129,10 @@ class FwiDriver:
     gradient requests on windows of the model, one request per shot and
     iteration; the next iteration is submitted when the last gradient of the
     current one has arrived. A step that raises the misfit is halved and
-    re-evaluated (at most `max_halvings` times)."""
+    re-evaluated (at most `max_halvings` times); a step never changes a
+    stiffness by more than `max_step` of the largest one, and a trial model
+    whose misfit is not finite (outside the scheme's stability range) counts
+    as an increase."""
     g: object
     model: np.ndarray
     wavelet: np.ndarray
@@ -137,6 +140,7 @@ class FwiDriver:
     iterations: int
     memory: int = 3
     max_halvings: int = 2
+    max_step: float = 0.02
     misfits: list = field(default_factory=list)
     step0: float = 0.0
 
@@ -219,7 +223,10 @@ class FwiDriver:
     def update(self, results):
         """Results of the submitted jobs in; the next jobs out (None: done)."""
         f, grad = self.stack(results)
-        if self.f_cur is None or f < self.f_cur or self.halvings >= self.max_halvings:
+        if not np.isfinite(f) and self.f_cur is not None:
+            f = np.inf  # a trial model outside the stable range: halve the step
+        if self.f_cur is None or f < self.f_cur or (self.halvings >= self.max_halvings and
+                                                    np.isfinite(f)):
             if self.f_cur is not None:
                 s, y = self.trial - self.x, grad - self.g_cur
                 if _dot(s, y) > 0:
@@ -233,7 +240,10 @@ class FwiDriver:
             if self.it >= self.iterations:
                 return None
             self.p = self.direction(grad)
-            self.alpha = 1.0
+            # at most max_step (relative to the largest stiffness) per iteration
+            cap = self.max_step * float(np.abs(self.x).max())
+            pmax = float(np.abs(self.p).max())
+            self.alpha = min(1.0, cap / pmax) if pmax > 0 else 1.0
         else:
             self.alpha *= 0.5
             self.halvings += 1
