@@ -356,14 +356,19 @@ int vti3d_engine_stats(vti3d_engine* e, size_t* used_bytes, int* jobs, int* tick
  * the 3D VTI step with the sponge as a plain diagonal, every level up to
  * nt-1, receivers at their own cells; its Born linearisation along dc and its
  * exact discrete adjoint. Background checkpoints every `checkpoint_every`
- * levels (0: 64), recomputed per block in the backward pass.
+ * levels (0: 64), recomputed per block in the backward pass; with
+ * VTI_GNHV_BF16 the recomputed levels the imaging reads are kept as BF16
+ * with one FP32 scale per z plane (half the segment memory; checkpoints
+ * stay FP32, so the recomputation is exact).
  * Outputs (host, each may be NULL): hv = H dc (3*nxyz), grad = dJ/dc of
  * J = 1/2|d - dobs|^2 (3*nxyz; needs dobs), misfit = J, traces d and Born
  * traces (nnt*nrec each). souloc: 5 floats (x, y, z, nrec, 0). */
+#define VTI_GNHV_BF16 1u /* background levels of the imaging stored as BF16 + plane scales */
 int vti3d_gnhv_exact(vti_ctx* ctx, const vti3d_geom* g, const float* c11, const float* c13,
                      const float* c33, const float* dc, const float* wavelet, const float* souloc,
                      const float* recloc, int nrec, const float* dobs, int checkpoint_every,
-                     float* hv, float* grad, double* misfit, float* traces, float* born);
+                     unsigned flags, float* hv, float* grad, double* misfit, float* traces,
+                     float* born);
 
 #ifdef __cplusplus
 }

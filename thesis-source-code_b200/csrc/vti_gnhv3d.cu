@@ -28,6 +28,8 @@
 #include <cstring>
 #include <vector>
 
+#include <cuda_bf16.h>
+
 #include "vti_plan3d.h"
 #include "vti_tma_common.cuh"
 
@@ -348,6 +350,244 @@ __global__ void __launch_bounds__(NTHREADS, 2)
   }
 }
 
+// ------------------------------------------------ BF16 background storage
+// The background levels the adjoint images against are stored as bfloat16
+// with one FP32 scale per z plane (value = bf16 * scale[z + kZPad]; the
+// scale is the plane's largest magnitude, pad planes hold 0).
+__global__ void k_pack_bf16(const float* src, Dims3 d, __nv_bfloat16* dst, float* scale) {
+  const int z = blockIdx.x;
+  const float* s = src + (long long)z * d.plane;
+  __nv_bfloat16* o = dst + (long long)z * d.plane;
+  const int n = d.ny * d.pitch;
+  float m = 0.f;
+  for (int i = threadIdx.x; i < n; i += blockDim.x)
+    if (i % d.pitch < d.nx) m = fmaxf(m, fabsf(s[i]));
+  for (int off = 16; off > 0; off >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, off));
+  __shared__ float wm[32];
+  if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    float v = threadIdx.x < (blockDim.x >> 5) ? wm[threadIdx.x] : 0.f;
+    for (int off = 16; off > 0; off >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, off));
+    if (threadIdx.x == 0) wm[0] = v;
+  }
+  __syncthreads();
+  const float sc = wm[0] > 0.f ? wm[0] : 1.f;
+  const float inv = 1.f / sc;
+  if (threadIdx.x == 0) scale[z + kZPad] = sc;
+  for (int i = threadIdx.x; i < n; i += blockDim.x)
+    o[i] = __float2bfloat16_rn(i % d.pitch < d.nx ? s[i] * inv : 0.f);
+}
+
+__device__ __forceinline__ float2 ldb2(const __nv_bfloat16* p) {
+  return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(p));
+}
+
+// Adjoint step imaging against a BF16 background (stage: w halo FP32, a halo
+// BF16, w_z FP32, a_z BF16, then mu_{t+1}, mu_{t+2}, C, image FP32).
+constexpr int A_OFF_AH = HALO_BYTES;
+constexpr int A_OFF_P = A_OFF_AH + HXB * HY * 2;  // BF16 halo tile, HXB x HY
+constexpr int A_OFF_AZ = A_OFF_P + PLAIN_BYTES;
+constexpr int A_OFF_R = A_OFF_AZ + PLAIN_BYTES / 2;
+constexpr int A_STAGE_BYTES = A_OFF_R + 10 * PLAIN_BYTES;  // 29696
+constexpr int A_SMEM = G_STAGES * A_STAGE_BYTES + 1024 + 2 * G_STAGES * 8;
+static_assert(A_OFF_AH % 128 == 0 && A_OFF_P % 128 == 0 && A_OFF_AZ % 128 == 0 &&
+                  A_OFF_R % 128 == 0 && A_STAGE_BYTES % 128 == 0,
+              "TMA destinations on 128-byte boundaries");
+
+struct AdjArgsB {
+  AdjArgs f;              // as the FP32 step; az unused
+  const __nv_bfloat16* az;  // a_{t-1} z (queue start)
+  const float* sxs;       // per-plane scales of a_{t-1} x and z
+  const float* szs;
+};
+
+__global__ void __launch_bounds__(NTHREADS, 2)
+    k_adj3d_b16(const __grid_constant__ AdjMaps m, const __grid_constant__ AdjArgsB b) {
+  extern __shared__ unsigned char smem_raw[];
+  uint64_t *full, *empty;
+  unsigned char* smem = ring_init<G_STAGES, A_STAGE_BYTES>(smem_raw, full, empty);
+  const AdjArgs& a = b.f;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  long long k = 0;
+  if (warp == NCW) {
+    if (lane == 0) {
+      const CUtensorMap* maps = reinterpret_cast<const CUtensorMap*>(&m);
+      for (int it = blockIdx.x; it < a.sc.items; it += gridDim.x) {
+        int bx, by, z0, z1;
+        item(a.sc, it, bx, by, z0, z1);
+        const int x0 = bx * TX, y0 = kHalo + by * TY;
+        bool ok = true;
+        for (int z = z0; z < z1; ++z, ++k) {
+          const int s = (int)(k % G_STAGES);
+          if (k >= G_STAGES &&
+              !mbar_wait(&empty[s], (uint32_t)(((k / G_STAGES) & 1) ^ 1), a.status)) {
+            ok = false;
+            break;
+          }
+          const int zp = z + kZPad;
+          unsigned char* st = smem + s * A_STAGE_BYTES;
+          mbar_arrive_expect_tx(&full[s], A_STAGE_BYTES);
+          tma_load(st, &maps[0], &full[s], x0 - kHalo, y0 - kHalo, zp);
+          tma_load(st + A_OFF_AH, &maps[1], &full[s], x0 - 8, y0 - kHalo, zp);
+          tma_load(st + A_OFF_P, &maps[2], &full[s], x0, y0, zp + kHalo);
+          tma_load(st + A_OFF_AZ, &maps[3], &full[s], x0, y0, zp + kHalo);
+#pragma unroll
+          for (int j = 0; j < 10; ++j)
+            tma_load(st + A_OFF_R + j * PLAIN_BYTES, &maps[4 + j], &full[s], x0, y0, zp);
+        }
+        if (!ok) break;
+      }
+    }
+    return;
+  }
+  const int ry = warp * 2 + (lane >> 4);
+  const int xo = 2 * (lane & 15);
+  const int sr = (ry + kHalo) * HX + xo + kHalo;
+  const int srb = (ry + kHalo) * HXB + xo + 8;  // centre in the BF16 halo tile
+  const int pi = ry * TX + xo;
+  for (int it = blockIdx.x; it < a.sc.items; it += gridDim.x) {
+    int bx, by, z0, z1;
+    item(a.sc, it, bx, by, z0, z1);
+    const int x = bx * TX + xo;
+    const int y = kHalo + by * TY + ry;
+    const bool vy = y < a.d.ny - kHalo;
+    const bool v0 = vy && x >= kHalo && x < a.d.nx - kHalo;
+    const bool v1 = vy && x + 1 >= kHalo && x + 1 < a.d.nx - kHalo;
+    const int off = y * a.d.pitch + x;
+    float wq[2][9], aq[2][9], dxy[2];
+    queue_init(wq, a.wz, a.d, off, z0, v0 || v1);
+    aq[0][0] = aq[1][0] = 0.f;
+#pragma unroll
+    for (int kk = 1; kk < 9; ++kk) {
+      const int zz = z0 - 5 + kk;
+      const float2 v = (v0 || v1) ? ldb2(b.az + (long long)zz * a.d.plane + off)
+                                  : make_float2(0.f, 0.f);
+      const float sc = b.szs[zz + kZPad];
+      aq[0][kk] = v.x * sc;
+      aq[1][kk] = v.y * sc;
+    }
+    dxy[0] = v0 ? a.dampx[x] * a.dampy[y] : 1.f;
+    dxy[1] = v1 ? a.dampx[x + 1] * a.dampy[y] : 1.f;
+    bool ok = true;
+    for (int z = z0; z < z1; ++z, ++k) {
+      const float dz = a.dampz[z];
+      const float scx = b.sxs[z + kZPad];
+      const float scz = b.szs[z + kHalo + kZPad];
+      const int s = (int)(k % G_STAGES);
+      if (!mbar_wait(&full[s], (uint32_t)((k / G_STAGES) & 1), a.status)) {
+        ok = false;
+        break;
+      }
+      const unsigned char* st = smem + s * A_STAGE_BYTES;
+      const float* pw = (const float*)(st + A_OFF_P) + pi;
+      const __nv_bfloat16* paz = (const __nv_bfloat16*)(st + A_OFF_AZ) + pi;
+      const float* pr = (const float*)(st + A_OFF_R) + pi;
+      constexpr int T = TX * TY;
+      queue_push(wq, ld2(pw));
+      {
+        const float2 v = ldb2(paz);
+        queue_push(aq, make_float2(v.x * scz, v.y * scz));
+      }
+      Stencil2 sw;
+      sw.load((const float*)st + sr);
+      // a halo in BF16: the same stencil on the unscaled values, times the
+      // plane's scale (linear)
+      float ra[10];
+      float2 yam[4], yap[4];
+      {
+        const __nv_bfloat16* h = (const __nv_bfloat16*)(st + A_OFF_AH) + srb;
+#pragma unroll
+        for (int j = 0; j < 5; ++j) {
+          const float2 t = ldb2(h - 4 + 2 * j);
+          ra[2 * j] = t.x;
+          ra[2 * j + 1] = t.y;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          yam[j] = ldb2(h - (j + 1) * HXB);
+          yap[j] = ldb2(h + (j + 1) * HXB);
+        }
+      }
+      const float2 m1x = ld2(pr), m1z = ld2(pr + T);
+      const float2 m2x = ld2(pr + 2 * T), m2z = ld2(pr + 3 * T);
+      const float2 c11 = ld2(pr + 4 * T), c13 = ld2(pr + 5 * T), c33 = ld2(pr + 6 * T);
+      const float2 g11o = ld2(pr + 7 * T), g13o = ld2(pr + 8 * T), g33o = ld2(pr + 9 * T);
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[s]);
+      float mx[2], mz[2], wx[2], wzv[2], g11[2], g13[2], g33[2];
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        auto pick = [e](float2 v) { return e ? v.y : v.x; };
+        const float dd = dxy[e] * dz;
+        const float lxy = sw.lxy(e, a.sx, a.sy);
+        const float lz = lz_of(wq[e], a.sz);
+        mx[e] = dd * (2.f * pick(m1x) + lxy - dd * pick(m2x));
+        mz[e] = dd * (2.f * pick(m1z) + lz - dd * pick(m2z));
+        wx[e] = fmaf(pick(c11), mx[e], pick(c13) * mz[e]);
+        wzv[e] = fmaf(pick(c13), mx[e], pick(c33) * mz[e]);
+        const float c = ra[4 + e];
+        const float lxx = lap9(c, ra[3 + e], ra[5 + e], ra[2 + e], ra[6 + e], ra[1 + e],
+                               ra[7 + e], ra[e], ra[8 + e]);
+        const float lyy = lap9(c, pick(yam[0]), pick(yap[0]), pick(yam[1]), pick(yap[1]),
+                               pick(yam[2]), pick(yap[2]), pick(yam[3]), pick(yap[3]));
+        const float axy = fmaf(lyy, a.sy, lxx * a.sx) * scx;
+        const float az = lz_of(aq[e], a.sz);
+        g11[e] = fmaf(mx[e], axy, pick(g11o));
+        g13[e] = fmaf(mx[e], az, fmaf(mz[e], axy, pick(g13o)));
+        g33[e] = fmaf(mz[e], az, pick(g33o));
+      }
+      const long long i = (long long)z * a.d.plane + off;
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        if (e ? v1 : v0) {
+          a.mpx[i + e] = mx[e];
+          a.mpz[i + e] = mz[e];
+          a.wox[i + e] = wx[e];
+          a.woz[i + e] = wzv[e];
+          a.g11[i + e] = g11[e];
+          a.g13[i + e] = g13[e];
+          a.g33[i + e] = g33[e];
+        }
+      }
+    }
+    if (!ok) break;
+  }
+}
+
+__device__ __forceinline__ float lap_b16(const __nv_bfloat16* f, long long o, long long stride,
+                                         const float* sc, int z, int zstep) {
+  auto v = [&](int k) { return __bfloat162float(f[o + k * stride]) * sc[z + k * zstep + kZPad]; };
+  return lap9(v(0), v(-1), v(1), v(-2), v(2), v(-3), v(3), v(-4), v(4));
+}
+
+// k_inject_exact with the background a_{t-1} in BF16.
+__global__ void k_inject_exact_b16(float* mx, float* mz, float* wx, float* wz, float* g11,
+                                   float* g13, float* g33, const float* c11, const float* c13,
+                                   const float* c33, const __nv_bfloat16* ax,
+                                   const __nv_bfloat16* az, const float* sxs, const float* szs,
+                                   const float* res, int nnt, int j, const long long* rec,
+                                   const float* rec_damp, const unsigned char* live, int nr,
+                                   Dims3 d, float sx, float sy, float sz) {
+  const int ir = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ir >= nr || !live[ir] || rec_damp[ir] == 0.f) return;
+  const float r = res[(long long)ir * nnt + j];
+  const float dd = rec_damp[ir];
+  const float dx_ = dd * (float)(kTwoThird * r);
+  const float dz_ = dd * (float)(kOneThird * r);
+  const long long o = rec[ir];
+  const int z = (int)(o / d.plane);
+  const float axy = fmaf(lap_b16(ax, o, d.pitch, sxs, z, 0), sy, lap_b16(ax, o, 1, sxs, z, 0) * sx);
+  const float azz = lap_b16(az, o, d.plane, szs, z, 1) * sz;
+  atomicAdd(mx + o, dx_);
+  atomicAdd(mz + o, dz_);
+  atomicAdd(wx + o, fmaf(c11[o], dx_, c13[o] * dz_));
+  atomicAdd(wz + o, fmaf(c13[o], dx_, c33[o] * dz_));
+  atomicAdd(g11 + o, dx_ * axy);
+  atomicAdd(g13 + o, fmaf(dx_, azz, dz_ * axy));
+  atomicAdd(g33 + o, dz_ * azz);
+}
+
 __device__ __forceinline__ float lap_at(const float* f, long long o, long long stride) {
   return lap9(f[o], f[o - stride], f[o + stride], f[o - 2 * stride], f[o + 2 * stride],
               f[o - 3 * stride], f[o + 3 * stride], f[o - 4 * stride], f[o + 4 * stride]);
@@ -389,6 +629,14 @@ struct VolM {
   TileMaps m;
 };
 
+// A BF16 volume (layout of Vol, 2-byte elements) with its per-plane scales.
+struct VolB {
+  void* alloc = nullptr;
+  __nv_bfloat16* origin = nullptr;
+  float* scale = nullptr;  // nz + 2 kZPad
+  TileMaps m;
+};
+
 bool attr_born[64] = {}, attr_adj[64] = {};
 
 int smem_attr(vti_ctx* ctx, const void* kern, bool* done) {
@@ -411,8 +659,15 @@ struct GnState {
   std::vector<VolM> seg;       // (K+1) levels x (x, z)
   VolM mu[2][2][2], w[2][2][2];  // [image][buffer][x, z]
   VolM img[2][3];
+  VolM ring[3][2];            // BF16 mode: FP32 levels of the recomputation
+  std::vector<VolB> segb;     // BF16 mode: (K+1) levels x (x, z)
   float* damp = nullptr;
   ~GnState() {
+    for (auto& x : segb) {
+      if (x.alloc) cudaFree(x.alloc);
+      if (x.scale) cudaFree(x.scale);
+    }
+    for (auto& r : ring) for (auto& x : r) vol_free(&x.v);
     auto fr = [](VolM& x) { vol_free(&x.v); };
     for (auto& x : c) fr(x);
     for (auto& x : dc) fr(x);
@@ -429,6 +684,16 @@ struct GnState {
     VTI_TRY(vol_alloc(ctx, d, &x->v));
     VTI_TRY(vol_zero(ctx, d, &x->v));
     return make_tile_maps(ctx, d, x->v, &x->m);
+  }
+  int alloc(VolB* x) {
+    const size_t n = (size_t)d.plane * (d.nz + 2 * kZPad);
+    if (cudaMalloc(&x->alloc, n * 2) != cudaSuccess ||
+        cudaMalloc((void**)&x->scale, (d.nz + 2 * kZPad) * sizeof(float)) != cudaSuccess)
+      return fail(ctx, VTI_ERR_OOM, "BF16 segment");
+    VTI_CUDA(ctx, cudaMemsetAsync(x->alloc, 0, n * 2, ctx->stream));
+    VTI_CUDA(ctx, cudaMemsetAsync(x->scale, 0, (d.nz + 2 * kZPad) * sizeof(float), ctx->stream));
+    x->origin = (__nv_bfloat16*)x->alloc + (size_t)kZPad * d.plane;
+    return make_tile_maps_typed(ctx, d, x->alloc, 2, &x->m);
   }
 };
 
@@ -521,6 +786,67 @@ int launch_adj(GnState& S, int im, int cur, int slot) {
   return VTI_OK;
 }
 
+bool attr_adjb[64] = {};
+
+int launch_adj_b16(GnState& S, int im, int cur, int slot) {
+  vti_ctx* ctx = S.ctx;
+  if (!(ctx->device < 64 && attr_adjb[ctx->device])) {
+    VTI_CUDA(ctx, cudaFuncSetAttribute(k_adj3d_b16, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       A_SMEM));
+    if (ctx->device < 64) attr_adjb[ctx->device] = true;
+  }
+  const int nx_ = 1 - cur;
+  const VolB& ax = S.segb[2 * slot];
+  const VolB& az = S.segb[2 * slot + 1];
+  AdjMaps m;
+  m.wx = HM(S.w[im][cur][0].m);
+  m.ax = HM(ax.m);
+  m.wz = PM(S.w[im][cur][1].m);
+  m.az = PM(az.m);
+  m.m1x = PM(S.mu[im][cur][0].m);
+  m.m1z = PM(S.mu[im][cur][1].m);
+  m.mpx = PM(S.mu[im][nx_][0].m);
+  m.mpz = PM(S.mu[im][nx_][1].m);
+  m.c11 = PM(S.c[0].m); m.c13 = PM(S.c[1].m); m.c33 = PM(S.c[2].m);
+  m.g11 = PM(S.img[im][0].m); m.g13 = PM(S.img[im][1].m); m.g33 = PM(S.img[im][2].m);
+  const float dt2 = S.g.dt * S.g.dt;
+  AdjArgsB b{};
+  AdjArgs& x = b.f;
+  x.d = S.d;
+  x.sc = make_sched(ctx, S.d, 2);
+  x.wz = S.w[im][cur][1].v.origin;
+  x.az = nullptr;
+  x.mpx = S.mu[im][nx_][0].v.origin;
+  x.mpz = S.mu[im][nx_][1].v.origin;
+  x.wox = S.w[im][nx_][0].v.origin;
+  x.woz = S.w[im][nx_][1].v.origin;
+  x.g11 = S.img[im][0].v.origin;
+  x.g13 = S.img[im][1].v.origin;
+  x.g33 = S.img[im][2].v.origin;
+  x.dampx = S.damp;
+  x.dampy = S.damp + S.g.nx;
+  x.dampz = S.damp + S.g.nx + S.g.ny;
+  x.sx = dt2 / (S.g.dx * S.g.dx);
+  x.sy = dt2 / (S.g.dy * S.g.dy);
+  x.sz = dt2 / (S.g.dz * S.g.dz);
+  x.status = ctx->d_status;
+  b.az = az.origin;
+  b.sxs = ax.scale;
+  b.szs = az.scale;
+  {
+    LaunchTimer tm(ctx, kTimedBwd3d);
+    k_adj3d_b16<<<x.sc.grid, NTHREADS, A_SMEM, ctx->stream>>>(m, b);
+  }
+  VTI_LAUNCHED(ctx, "k_adj3d_b16");
+  return VTI_OK;
+}
+
+int pack(GnState& S, const VolM& src, VolB& dst) {
+  k_pack_bf16<<<S.d.nz, 256, 0, S.ctx->stream>>>(src.v.origin, S.d, dst.origin, dst.scale);
+  VTI_LAUNCHED(S.ctx, "k_pack_bf16");
+  return VTI_OK;
+}
+
 int copy_vol(vti_ctx* ctx, const Vol& src, Vol* dst) {
   VTI_CUDA(ctx, cudaMemcpyAsync(dst->alloc, src.alloc, src.bytes, cudaMemcpyDeviceToDevice,
                                 ctx->stream));
@@ -537,8 +863,10 @@ extern "C" {
 int vti3d_gnhv_exact(vti_ctx* ctx, const vti3d_geom* g, const float* c11, const float* c13,
                      const float* c33, const float* dc, const float* wavelet, const float* souloc,
                      const float* recloc, int nrec, const float* dobs, int checkpoint_every,
-                     float* hv, float* grad, double* misfit, float* traces, float* born) {
+                     unsigned gn_flags, float* hv, float* grad, double* misfit, float* traces,
+                     float* born) {
   if (!ctx || !g) return VTI_ERR_ARG;
+  const bool b16 = (gn_flags & VTI_GNHV_BF16) != 0;
   VTI_TRY(p3d::check_geom(ctx, g));
   if (!c11 || !c13 || !c33 || !wavelet || !souloc || (nrec > 0 && !recloc))
     return fail(ctx, VTI_ERR_ARG, "null input");
@@ -590,8 +918,15 @@ int vti3d_gnhv_exact(vti_ctx* ctx, const vti3d_geom* g, const float* c11, const 
   const int nblk = (M - 1 + K - 1) / K;
   S.ck.resize(4 * (size_t)nblk);
   for (auto& x : S.ck) VTI_TRY(vol_alloc(ctx, S.d, &x.v));
-  S.seg.resize(2 * (size_t)(K + 1));
-  for (auto& x : S.seg) VTI_TRY(S.alloc(&x));
+  if (b16) {
+    for (auto& r : S.ring)
+      for (auto& x : r) VTI_TRY(S.alloc(&x));
+    S.segb.resize(2 * (size_t)(K + 1));
+    for (auto& x : S.segb) VTI_TRY(S.alloc(&x));
+  } else {
+    S.seg.resize(2 * (size_t)(K + 1));
+    for (auto& x : S.seg) VTI_TRY(S.alloc(&x));
+  }
   // traces: background, Born
   float* d_tr = p->d_trace;  // nnt * nr (the plan's buffer)
   float* d_born = nullptr;
@@ -668,31 +1003,51 @@ int vti3d_gnhv_exact(vti_ctx* ctx, const vti3d_geom* g, const float* c11, const 
   for (int blk = nblk - 1; blk >= 0; --blk) {
     const int k0 = 1 + blk * K;             // first level a_{t-1} of the block
     const int k1 = std::min(k0 + K - 1, M - 1);  // last
-    // slots: s holds level k0 - 1 + s
-    VTI_TRY(copy_vol(ctx, S.ck[4 * blk + 0].v, &S.seg[0].v));
-    VTI_TRY(copy_vol(ctx, S.ck[4 * blk + 1].v, &S.seg[1].v));
-    VTI_TRY(copy_vol(ctx, S.ck[4 * blk + 2].v, &S.seg[2].v));
-    VTI_TRY(copy_vol(ctx, S.ck[4 * blk + 3].v, &S.seg[3].v));
+    // slots: s holds level k0 - 1 + s (FP32 segment, or BF16 segment fed
+    // from a 3-level FP32 ring, level L in ring slot L % 3)
+    auto lvl = [&](int L) -> VolM* { return b16 ? S.ring[L % 3] : &S.seg[2 * (L - (k0 - 1))]; };
+    for (int f = 0; f < 2; ++f) {
+      VTI_TRY(copy_vol(ctx, S.ck[4 * blk + f].v, &lvl(k0 - 1)[f].v));
+      VTI_TRY(copy_vol(ctx, S.ck[4 * blk + 2 + f].v, &lvl(k0)[f].v));
+    }
+    if (b16)
+      for (int f = 0; f < 2; ++f) {
+        VTI_TRY(pack(S, lvl(k0 - 1)[f], S.segb[f]));
+        VTI_TRY(pack(S, lvl(k0)[f], S.segb[2 + f]));
+      }
     Damping dmp{S.damp, S.damp + g->nx, S.damp + g->nx + g->ny};
     for (int t = k0 + 1; t <= k1; ++t) {
-      const int s = t - (k0 - 1);
       PointSource ps;
       ps.x = sg.sx; ps.y = sg.sy; ps.z = sg.sz; ps.amp = dt2 * wavelet[t - 1];
-      const VolM* cx = &S.seg[2 * (s - 1)];
-      const VolM* px = &S.seg[2 * (s - 2)];
-      VolM* nx_ = &S.seg[2 * s];
+      const VolM* cx = lvl(t - 1);
+      const VolM* px = lvl(t - 2);
+      VolM* nx_ = lvl(t);
       VTI_TRY(launch_fwd3d_tma(ctx, S.d, cx[0].m, cx[1].m, px[0].m, px[1].m, S.c[0].m, S.c[1].m,
                                S.c[2].m, cx[1].v.origin, nx_[0].v.origin, nx_[1].v.origin, &dmp,
                                sxs, sys, szs, ps, Probe(), true));
+      if (b16) {
+        const int sl = t - (k0 - 1);
+        VTI_TRY(pack(S, nx_[0], S.segb[2 * sl]));
+        VTI_TRY(pack(S, nx_[1], S.segb[2 * sl + 1]));
+      }
     }
     for (int tm1 = k1; tm1 >= k0; --tm1) {
       const int t = tm1 + 1;
       const int slot = tm1 - (k0 - 1);
       for (int im = 0; im < 2; ++im) {
         if (!want[im]) continue;
-        VTI_TRY(launch_adj(S, im, mcur, slot));
+        VTI_TRY(b16 ? launch_adj_b16(S, im, mcur, slot) : launch_adj(S, im, mcur, slot));
         const int nb = 1 - mcur;  // mu_t / w_t were written there
-        if (t < (int)sg.rec_at.size() && sg.rec_at[t] >= 0 && sg.nr > 0) {
+        if (b16 && t < (int)sg.rec_at.size() && sg.rec_at[t] >= 0 && sg.nr > 0) {
+          k_inject_exact_b16<<<(sg.nr + 127) / 128, 128, 0, ctx->stream>>>(
+              S.mu[im][nb][0].v.origin, S.mu[im][nb][1].v.origin, S.w[im][nb][0].v.origin,
+              S.w[im][nb][1].v.origin, S.img[im][0].v.origin, S.img[im][1].v.origin,
+              S.img[im][2].v.origin, S.c[0].v.origin, S.c[1].v.origin, S.c[2].v.origin,
+              S.segb[2 * slot].origin, S.segb[2 * slot + 1].origin, S.segb[2 * slot].scale,
+              S.segb[2 * slot + 1].scale, src[im], nnt, sg.rec_at[t], p->d_rec, p->d_rec_damp,
+              p->d_live, sg.nr, S.d, sxs, sys, szs);
+          VTI_LAUNCHED(ctx, "k_inject_exact_b16");
+        } else if (t < (int)sg.rec_at.size() && sg.rec_at[t] >= 0 && sg.nr > 0) {
           k_inject_exact<<<(sg.nr + 127) / 128, 128, 0, ctx->stream>>>(
               S.mu[im][nb][0].v.origin, S.mu[im][nb][1].v.origin, S.w[im][nb][0].v.origin,
               S.w[im][nb][1].v.origin, S.img[im][0].v.origin, S.img[im][1].v.origin,

@@ -134,6 +134,10 @@ struct TileMaps {
   alignas(64) unsigned char halo[128];
 };
 int make_tile_maps(vti_ctx* ctx, const Dims3& d, const Vol& v, TileMaps* out);
+// The same over a volume of `elem_bytes` (4: float, 2: bfloat16) elements
+// with the layout of Vol (alloc = start of the pad planes).
+int make_tile_maps_typed(vti_ctx* ctx, const Dims3& d, void* alloc, int elem_bytes,
+                         TileMaps* out);
 
 // One forward-form leapfrog step over the update region (x,y in [4,n-4),
 // all z): next written through px_ptr/pz_ptr (prev is read through the px/pz

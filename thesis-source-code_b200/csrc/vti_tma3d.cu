@@ -707,18 +707,28 @@ Sched make_sched(vti_ctx* ctx, const Dims3& d, int ctas_per_sm) {
 
 
 int make_tile_maps(vti_ctx* ctx, const Dims3& d, const Vol& v, TileMaps* out) {
+  return make_tile_maps_typed(ctx, d, v.alloc, 4, out);
+}
+
+int make_tile_maps_typed(vti_ctx* ctx, const Dims3& d, void* alloc, int elem_bytes,
+                         TileMaps* out) {
   auto fn = encode_fn();
   if (!fn) return fail(ctx, VTI_ERR_DEVICE, "cuTensorMapEncodeTiled unavailable");
+  if (elem_bytes != 4 && elem_bytes != 2) return fail(ctx, VTI_ERR_ARG, "element size");
+  const CUtensorMapDataType ty =
+      elem_bytes == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
   cuuint64_t dims[3] = {(cuuint64_t)d.nx, (cuuint64_t)d.ny, (cuuint64_t)(d.nz + 2 * kZPad)};
-  cuuint64_t strides[2] = {(cuuint64_t)d.pitch * 4, (cuuint64_t)d.plane * 4};
+  cuuint64_t strides[2] = {(cuuint64_t)d.pitch * elem_bytes, (cuuint64_t)d.plane * elem_bytes};
   cuuint32_t estr[3] = {1, 1, 1};
   cuuint32_t box_plain[3] = {TX, TY, 1};
-  cuuint32_t box_halo[3] = {HX, HY, 1};
-  CUresult r1 = fn((CUtensorMap*)out->plain, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, v.alloc, dims,
+  // TMA x coordinates must be multiples of 16 bytes: a BF16 halo tile starts
+  // 8 cells (16 bytes) left of the column and is 16 cells wider (HXB)
+  cuuint32_t box_halo[3] = {elem_bytes == 4 ? (cuuint32_t)HX : (cuuint32_t)HXB, HY, 1};
+  CUresult r1 = fn((CUtensorMap*)out->plain, ty, 3, alloc, dims,
                    strides, box_plain, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  CUresult r2 = fn((CUtensorMap*)out->halo, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, v.alloc, dims,
+  CUresult r2 = fn((CUtensorMap*)out->halo, ty, 3, alloc, dims,
                    strides, box_halo, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);

@@ -29,6 +29,8 @@ constexpr float kC0 = -2.84722222222f, kC1 = 1.6f, kC2 = -0.2f, kC3 = 0.02539682
 constexpr int TX = 32, TY = 16, RY = 2, NCW = TY / RY;  // consumer warps
 constexpr int NTHREADS = (NCW + 1) * 32;
 constexpr int HX = TX + 2 * kHalo, HY = TY + 2 * kHalo;
+// BF16 halo tiles: x from x0-8 so the TMA x coordinate is 16-byte aligned
+constexpr int HXB = TX + 16;
 constexpr int PLAIN_BYTES = TX * TY * 4;  // 2048
 constexpr int HALO_BYTES = HX * HY * 4;   // 3840
 constexpr unsigned kSpinLimit = 1u << 26;

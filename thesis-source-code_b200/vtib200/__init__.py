@@ -130,7 +130,7 @@ def _signatures():
         "vti3d_batch_autotune": (C.c_int, [P, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "vti3d_batch_gradient": (C.c_int, [P, P, C.c_int, P, C.c_int, C.POINTER(C.c_double)]),
         "vti3d_batch_get_shot_models": (C.c_int, [P, C.c_int, P, P]),
-        "vti3d_gnhv_exact": (C.c_int, [P] * 9 + [C.c_int, P, C.c_int, P, P,
+        "vti3d_gnhv_exact": (C.c_int, [P] * 9 + [C.c_int, P, C.c_int, C.c_uint, P, P,
                                                C.POINTER(C.c_double), P, P]),
         "vti3d_engine_job_bytes": (C.c_size_t, [P]),
         "vti3d_engine_create": (C.c_int, [P, C.c_size_t, C.POINTER(VP)]),
@@ -496,8 +496,11 @@ class Engine3d:
             pass
 
 
+GNHV_BF16 = 1
+
+
 def gnhv_exact(ctx, g: Geom3d, c11, c13, c33, wavelet, souloc, recloc, dc=None, dobs=None,
-               checkpoint_every=0, want=("hv", "grad", "traces", "born")):
+               checkpoint_every=0, want=("hv", "grad", "traces", "born"), flags=0):
     """vti3d_gnhv_exact: exact-mode Gauss-Newton product H dc, gradient,
     misfit and traces of one shot. Returns a dict of the requested outputs."""
     n = g.nx * g.ny * g.nz
@@ -514,7 +517,7 @@ def gnhv_exact(ctx, g: Geom3d, c11, c13, c33, wavelet, souloc, recloc, dc=None, 
             _f32(souloc), recloc]
     dobs_ = None if dobs is None else _f32(dobs)
     ctx.check(lib().vti3d_gnhv_exact(ctx.handle, C.byref(g), *[_p(a) for a in args], nrec,
-                                     _p(dobs_), checkpoint_every, _p(hv), _p(grad),
+                                     _p(dobs_), checkpoint_every, flags, _p(hv), _p(grad),
                                      C.byref(mis) if dobs is not None else None, _p(tr),
                                      _p(born)))
     for k, v in (("hv", hv), ("grad", grad), ("traces", tr), ("born", born)):
