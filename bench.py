@@ -589,6 +589,128 @@ def run_served(args):
     return out
 
 
+def run_gnhv(args):
+    """Exact-mode 3D Gauss-Newton H*v plus gradient of one shot (the mixed-
+    precision workload): 300 x 600 x 600 at 10 m, nt = 4000 with dt = 0.75 ms
+    (1 ms violates the CFL bound for v = 4500 m/s, eps = 0.2, delta = 0.1),
+    layered VTI model + Gaussian random field, 12 Hz Ricker, receivers every
+    4 cells at 20 m, input vector a seeded Gaussian random field (seed 6) of
+    1 % of the model; background checkpoints every K levels in FP32, the
+    levels the imaging reads stored as BF16 with per-z-plane FP32 scales,
+    misfit in FP64. The error against the FP64 oracle is measured on a
+    reduced grid of the same construction (the oracle keeps every level in
+    host memory)."""
+    import torch
+    import vtib200 as V
+    import vtib200.synth as S
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    torch.cuda.set_device(0)
+    nx, ny, nz = args.gn_grid
+    nt = args.nt or 4000
+
+    def case(nx, ny, nz, nt, npad):
+        s = S.survey3d(nx=nx, ny=ny, nz=nz, nt=nt, npad=npad, d=10.0, dt=7.5e-4, rate=4e-3,
+                       freq=12.0, rec_step=4, rec_start=npad, rec_depth=20.0, src_depth=20.0,
+                       corr=200.0, smooth_m=None)
+        n = s.nxyz
+        c = s.cij()
+        dc = (S.grf((nz, ny, nx), 200.0 / 10.0, 1.0, 4.0, 6).reshape(-1) * c.reshape(3, -1)
+              * 1e-2).reshape(-1).astype(np.float32)
+        # observed data: the model with a 2 % smooth velocity perturbation
+        vt = s.v * (1 + S.grf((nz, ny, nx), 20.0, 0.02, 0.04, 8).reshape(-1))
+        ct = s.cij(vt, s.eps, s.dl)
+        return s, c, ct, dc
+
+    ctx = V.Context(0)
+    s, c, ct, dc = case(nx, ny, nz, nt, 40)
+    g = s.geom()
+    n = s.nxyz
+    so = s.souloc[:5].copy()
+    so[3], so[4] = s.recloc.size // 4, 0
+    cs = [c[k * n:(k + 1) * n] for k in range(3)]
+    log = lambda m: print(m, file=sys.stderr, flush=True)  # noqa: E731
+    log("model ready")
+    dobs = V.gnhv_exact(ctx, g, *[ct[k * n:(k + 1) * n] for k in range(3)], s.wavelet, so,
+                        s.recloc, checkpoint_every=args.gn_k, want=("traces",))["traces"]
+    log("observed traces ready")
+    launches0 = ctx.launches
+    ctx.set_timing(True)
+    with ClockSampler(0) as clk:
+        t0 = time.perf_counter()
+        out = V.gnhv_exact(ctx, g, *cs, s.wavelet, so, s.recloc, dc=dc, dobs=dobs,
+                           checkpoint_every=args.gn_k, want=("hv", "grad"), flags=V.GNHV_BF16)
+        wall = time.perf_counter() - t0
+    adj_ms, adj_n = ctx.kernel_time("bwd3d")
+    fwd_ms, fwd_n = ctx.kernel_time("fwd3d")
+    ctx.set_timing(False)
+    launches = ctx.launches - launches0
+    ctx.close()
+    M = nt - 1
+    # pair updates per level: background + Born, recomputation, two adjoints
+    pts = 5.0 * (M - 1) * n
+    upd = (nx - 8) * (ny - 8) * nz
+    peak, peak_kind = peaks()
+    adj_avg = adj_ms / max(adj_n, 1) / 1e3
+    achieved = 80 * upd / adj_avg / 1e9 if adj_n else None
+    log("reduced grid vs the FP64 oracle")
+    r = args.gn_check
+    sr, cr, ctr, dcr = case(r[0], r[1], r[2], args.gn_check_nt, 8)
+    gr = sr.geom()
+    nr_ = sr.nxyz
+    sor = sr.souloc[:5].copy()
+    sor[3], sor[4] = sr.recloc.size // 4, 0
+    csr = [cr[k * nr_:(k + 1) * nr_] for k in range(3)]
+    c64 = [a.astype(np.float64) for a in csr]
+    ctx = V.Context(0)
+    dob = O.exact_forward3d(gr, *[ctr[k * nr_:(k + 1) * nr_].astype(np.float64)
+                                  for k in range(3)], sr.wavelet, sor, [0], sr.recloc)
+    gpu = V.gnhv_exact(ctx, gr, *csr, sr.wavelet, sor, sr.recloc, dc=dcr,
+                       dobs=dob.astype(np.float32), checkpoint_every=16, flags=V.GNHV_BF16)
+    ctx.close()
+    tr = O.exact_forward3d(gr, *c64, sr.wavelet, sor, [0], sr.recloc)
+    bo = O.exact_born3d(gr, *c64, sr.wavelet, sor, [0], sr.recloc, dcr)
+    grad = O.exact_adjoint3d(gr, *c64, sr.wavelet, sor, [0], sr.recloc, tr - dob)
+    hv = O.exact_adjoint3d(gr, *c64, sr.wavelet, sor, [0], sr.recloc, bo)
+
+    def rel(a, b):
+        b = np.asarray(b, dtype=np.float64)
+        return float(np.linalg.norm(np.asarray(a, dtype=np.float64) - b) / np.linalg.norm(b))
+
+    errs = {"traces": rel(gpu["traces"], tr), "born_traces": rel(gpu["born"], bo),
+            "gradient": rel(gpu["grad"], grad), "hv": rel(gpu["hv"], hv),
+            "misfit": abs(gpu["misfit"] - 0.5 * float((tr - dob) @ (tr - dob))) /
+            (0.5 * float((tr - dob) @ (tr - dob))),
+            "grid": list(r), "nt": args.gn_check_nt}
+    res = {
+        "metric": "3D exact-mode Gauss-Newton H*v + gradient (grid-point updates/s)",
+        "value": round(pts / wall / 1e9, 3), "unit": "Gpts/s", "n_gpus": 1, "steps": 1,
+        "warmup": 0, "ms_per_step": round(wall * 1e3, 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (BF16 stored background)",
+        "data": "synthetic (seeded layered VTI + GRF model, GRF input vector)",
+        "config": {"workload": f"GN H*v + gradient, {nx}x{ny}x{nz} at 10 m, nt={nt}, dt=0.75 ms, "
+                               f"checkpoints every {args.gn_k} levels, BF16 background",
+                   "grid": [nx, ny, nz], "nt": nt, "receivers": int(s.recloc.size // 4),
+                   "checkpoint_every": args.gn_k, "misfit": out["misfit"],
+                   "updates_per_level": "5 (background+Born, recomputation, 2 adjoints)"},
+        "roofline": {"bound": "hbm", "kernel": "k_adj3d_b16",
+                     "achieved": round(achieved, 1) if achieved else None, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4) if achieved else None, "traffic": None,
+                     "bytes_per_point": 80, "avg_launch_ms": round(adj_avg * 1e3, 4),
+                     "forward_kernels_ms": round(fwd_ms, 1), "forward_launches": int(fwd_n)},
+        "error_vs_fp64_oracle": errs,
+        "e2e": {"value": round(pts / wall / 1e9, 3), "unit": "Gpts/s",
+                "h2d_bytes_per_step": int(4 * (6 * n + dobs.size)),
+                "d2h_bytes_per_step": int(4 * 6 * n),
+                "api": "vti3d_gnhv_exact (host buffers)"},
+        "gpu_launches": int(launches), "clocks": clk.summary(),
+    }
+    print(json.dumps(res), flush=True)
+    return res
+
+
 def run_reference(args):
     """Reference arm: the reference algorithm's CPU implementation (the FP32
     oracle port; the reference's own CPU path needs ISPC and TBB, absent
@@ -641,7 +763,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default="gradient400", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--workload", default="gradient", choices=["gradient", "batched", "served"],
+    ap.add_argument("--workload", default="gradient",
+                    choices=["gradient", "batched", "served", "gnhv"],
                     help="batched: many shots on their own windows vs the plain loop")
     ap.add_argument("--shots", type=int, default=64, help="batched workload: shots")
     ap.add_argument("--plain-shots", type=int, default=3,
@@ -657,8 +780,16 @@ def main():
     ap.add_argument("--chunk", type=int, default=32, help="served workload: ticks per step")
     ap.add_argument("--requests-with-fwi", action="store_true",
                     help="served workload: run the requests again beside the FWI")
+    ap.add_argument("--gn-grid", type=int, nargs=3, default=[600, 600, 300],
+                    help="gnhv workload: nx ny nz")
+    ap.add_argument("--gn-k", type=int, default=126, help="gnhv workload: checkpoint interval")
+    ap.add_argument("--gn-check", type=int, nargs=3, default=[44, 56, 40],
+                    help="gnhv workload: reduced grid of the FP64 oracle check")
+    ap.add_argument("--gn-check-nt", type=int, default=300)
     args = ap.parse_args()
-    if args.workload == "batched" and args.impl == "b200":
+    if args.workload == "gnhv" and args.impl == "b200":
+        run_gnhv(args)
+    elif args.workload == "batched" and args.impl == "b200":
         run_batched(args)
     elif args.workload == "served" and args.impl == "b200":
         run_served(args)

@@ -1150,12 +1150,17 @@ double grad2d(const Geo2& g, const float* c11, const float* c13, const float* c3
 // and differentiates it exactly, so a dot-product test and centred finite
 // differences can check the adjoint-state machinery itself:
 //   a_0 = 0, a_1 = dt2 w[0] e_s,
-//   a_t = P D [ (2 + C L) a_{t-1} - D a_{t-2} + dt2 w[t-1] e_s ],  t = 2..M
+//   a_t = P [ D ((2 + C L) a_{t-1} + dt2 w[t-1] e_s) - (2D - 1) a_{t-2} ],  t = 2..M
 // with P the x/y update region, D the sponge profile (abc3d.cu:23-50) as a
-// plain diagonal, C L the forward-form VTI operator of step3d; traces
-// d_j = 2/3 a_x + 1/3 a_z at each receiver's own cell and level j*st;
-// J = 1/2 sum over live receivers of (d - dobs)^2. Its adjoint:
-//   mu_t = P D [ R^T r_t + 2 mu_{t+1} + (C L)^T mu_{t+1} - D mu_{t+2} ],
+// diagonal, C L the forward-form VTI operator of step3d. The damping is the
+// centred form u'' + g u' = C L u with D = 1/(1 + g dt/2), which is
+// energy-stable for any D <= 1 (the reference's form, D applied to next and
+// again to cur, subtracts D^2 a_{t-2}; equal to first order in 1 - D, and
+// without the block-order reading it grew without bound over 4000 steps of a
+// 600x600x300 grid). Traces d_j = 2/3 a_x + 1/3 a_z at each receiver's own
+// cell and level j*st; J = 1/2 sum over live receivers of (d - dobs)^2. Its
+// adjoint:
+//   mu_t = P [ D (R^T r_t + 2 mu_{t+1} + (C L)^T mu_{t+1}) - (2D - 1) mu_{t+2} ],
 //   (C L)^T mu = ( L_xy(c11 mu_x + c13 mu_z), L_z(c13 mu_x + c33 mu_z) ),
 //   dJ/dc11 = sum_t mu_t,x L_xy a_{t-1,x},  dJ/dc33 = sum_t mu_t,z L_z a_{t-1,z},
 //   dJ/dc13 = sum_t mu_t,x L_z a_{t-1,z} + mu_t,z L_xy a_{t-1,x}.
@@ -1237,14 +1242,14 @@ void exact_forward3d(const Geo3& g, const T* c11, const T* c13, const T* c33,
         for (long ix = kHalf; ix < g.nx - kHalf; ++ix) {
           const long ixy = ix + iy * g.nx, i = ixy + iz * nxy;
           const T d = (T)damp.at(ixy, (int)iz);
-          T vx = c11[i] * lxy[i] + c13[i] * lz[i] + 2 * u1[i] - d * u2[i];
-          T vz = c13[i] * lxy[i] + c33[i] * lz[i] + 2 * u1[n + i] - d * u2[n + i];
+          T vx = c11[i] * lxy[i] + c13[i] * lz[i] + 2 * u1[i];
+          T vz = c13[i] * lxy[i] + c33[i] * lz[i] + 2 * u1[n + i];
           if (dc) {
             vx += dc[i] * bxy[i] + dc[n + i] * bz[i];
             vz += dc[n + i] * bxy[i] + dc[2 * n + i] * bz[i];
           }
-          u[i] = d * vx;
-          u[n + i] = d * vz;
+          u[i] = d * vx - (2 * d - 1) * u2[i];
+          u[n + i] = d * vz - (2 * d - 1) * u2[n + i];
         }
     if (!dc) {
       const T d = (T)damp.at(s.sidx % nxy, (int)(s.sidx / nxy));
@@ -1301,8 +1306,8 @@ void exact_adjoint3d(const Geo3& g, const T* c11, const T* c13, const T* c33,
         for (long ix = kHalf; ix < g.nx - kHalf; ++ix) {
           const long ixy = ix + iy * g.nx, i = ixy + iz * nxy;
           const T d = (T)damp.at(ixy, (int)iz);
-          mu[i] = d * (src[i] + 2 * mu1[i] + lxy[i] - d * mu2[i]);
-          mu[n + i] = d * (src[n + i] + 2 * mu1[n + i] + lz[i] - d * mu2[n + i]);
+          mu[i] = d * (src[i] + 2 * mu1[i] + lxy[i]) - (2 * d - 1) * mu2[i];
+          mu[n + i] = d * (src[n + i] + 2 * mu1[n + i] + lz[i]) - (2 * d - 1) * mu2[n + i];
         }
     const T* a1 = h.a[t - 1].data();
     lap3d<T>(g, a1, a1 + n, axy.data(), az.data());

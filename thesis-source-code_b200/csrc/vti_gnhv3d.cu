@@ -6,10 +6,11 @@
 // exact-mode operators, whose discrete adjoint is exact (the checks are the
 // dot-product and finite-difference tests of the oracle's EXACT mode):
 //   a_0 = 0, a_1 = dt2 w[0] e_s,
-//   a_t = P D [ (2 + C L) a_{t-1} - D a_{t-2} + dt2 w[t-1] e_s ],      t = 2..M
-//   da_t = P D [ (2 + C L) da_{t-1} - D da_{t-2} + dC L a_{t-1} ]       (Born)
+//   a_t = P [ D ((2 + C L) a_{t-1} + dt2 w[t-1] e_s) - (2D - 1) a_{t-2} ],  t = 2..M
+//   da_t = P [ D ((2 + C L) da_{t-1} + dC L a_{t-1}) - (2D - 1) da_{t-2} ]  (Born)
+//   (centred damping, energy-stable for D <= 1)
 //   traces d_j = 2/3 a_x + 1/3 a_z at the receivers' cells, level j*st;
-//   mu_t = P D [ R^T r_t + 2 mu_{t+1} + (C L)^T mu_{t+1} - D mu_{t+2} ],
+//   mu_t = P [ D (R^T r_t + 2 mu_{t+1} + (C L)^T mu_{t+1}) - (2D - 1) mu_{t+2} ],
 //   (C L)^T mu = (L_xy w_x, L_z w_z), w = C mu,
 //   image += (mu_x L_xy a_{t-1}, mu_x L_z a_{t-1} + mu_z L_xy a_{t-1}, mu_z L_z a_{t-1}).
 // With r = d - d_obs the image is the gradient of J = 1/2 |d - d_obs|^2; with
@@ -208,21 +209,24 @@ __global__ void __launch_bounds__(NTHREADS, 2)
         // background: the exact forward step (same expression as k_fwd3d_tma)
         const float lxy = sa.lxy(e, a.sx, a.sy);
         const float lz = lz_of(aq[e], a.sz);
-        anx[e] = fmaf(a11, lxy, fmaf(a13, lz, 2.f * sa.r[4 + e] - dd * pick(apx)));
-        anz[e] = fmaf(a13, lxy, fmaf(a33, lz, 2.f * aq[e][4] - dd * pick(apz)));
+        const float pc = 2.f * dd - 1.f;  // centred damping: - (2D - 1) prev
+        anx[e] = fmaf(a11, lxy, fmaf(a13, lz, 2.f * sa.r[4 + e]));
+        anz[e] = fmaf(a13, lxy, fmaf(a33, lz, 2.f * aq[e][4]));
         if (x + e == a.src.x && y == a.src.y && z == a.src.z) {
           anx[e] += a.src.amp;
           anz[e] += a.src.amp;
         }
-        anx[e] *= dd;
-        anz[e] *= dd;
+        anx[e] = fmaf(dd, anx[e], -pc * pick(apx));
+        anz[e] = fmaf(dd, anz[e], -pc * pick(apz));
         // Born field: same operator plus the scattering source dC L a_{t-1}
         const float blxy = sb.lxy(e, a.sx, a.sy);
         const float blz = lz_of(bq[e], a.sz);
         const float sx_ = fmaf(pick(d11), lxy, pick(d13) * lz);
         const float sz_ = fmaf(pick(d13), lxy, pick(d33) * lz);
-        bnx[e] = dd * (fmaf(a11, blxy, fmaf(a13, blz, 2.f * sb.r[4 + e] - dd * pick(bpx))) + sx_);
-        bnz[e] = dd * (fmaf(a13, blxy, fmaf(a33, blz, 2.f * bq[e][4] - dd * pick(bpz))) + sz_);
+        bnx[e] = fmaf(dd, fmaf(a11, blxy, fmaf(a13, blz, 2.f * sb.r[4 + e])) + sx_,
+                      -pc * pick(bpx));
+        bnz[e] = fmaf(dd, fmaf(a13, blxy, fmaf(a33, blz, 2.f * bq[e][4])) + sz_,
+                      -pc * pick(bpz));
       }
       const long long i = (long long)z * a.d.plane + off;
 #pragma unroll
@@ -322,8 +326,8 @@ __global__ void __launch_bounds__(NTHREADS, 2)
         const float dd = dxy[e] * dz;
         const float lxy = sw.lxy(e, a.sx, a.sy);   // L_xy w_x
         const float lz = lz_of(wq[e], a.sz);         // L_z w_z
-        mx[e] = dd * (2.f * pick(m1x) + lxy - dd * pick(m2x));
-        mz[e] = dd * (2.f * pick(m1z) + lz - dd * pick(m2z));
+        mx[e] = fmaf(dd, 2.f * pick(m1x) + lxy, -(2.f * dd - 1.f) * pick(m2x));
+        mz[e] = fmaf(dd, 2.f * pick(m1z) + lz, -(2.f * dd - 1.f) * pick(m2z));
         wx[e] = fmaf(pick(c11), mx[e], pick(c13) * mz[e]);
         wzv[e] = fmaf(pick(c13), mx[e], pick(c33) * mz[e]);
         const float axy = sa.lxy(e, a.sx, a.sy);   // L_xy a_{t-1,x}
@@ -522,8 +526,8 @@ __global__ void __launch_bounds__(NTHREADS, 2)
         const float dd = dxy[e] * dz;
         const float lxy = sw.lxy(e, a.sx, a.sy);
         const float lz = lz_of(wq[e], a.sz);
-        mx[e] = dd * (2.f * pick(m1x) + lxy - dd * pick(m2x));
-        mz[e] = dd * (2.f * pick(m1z) + lz - dd * pick(m2z));
+        mx[e] = fmaf(dd, 2.f * pick(m1x) + lxy, -(2.f * dd - 1.f) * pick(m2x));
+        mz[e] = fmaf(dd, 2.f * pick(m1z) + lz, -(2.f * dd - 1.f) * pick(m2z));
         wx[e] = fmaf(pick(c11), mx[e], pick(c13) * mz[e]);
         wzv[e] = fmaf(pick(c13), mx[e], pick(c33) * mz[e]);
         const float c = ra[4 + e];

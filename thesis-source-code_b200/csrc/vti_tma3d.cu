@@ -113,9 +113,10 @@ __device__ __forceinline__ bool fwd_produce(const FwdCommon& a, const FwdMaps& m
 // Consumer side of one item. Thread (lane, warp) owns the x pair
 // x0 + 2*(lane%16) + {0,1} of tile row 2*warp + lane/16; shared-memory reads
 // and global stores are float2.
-// kExact: the sponge as a plain diagonal (next = D(C L cur + 2 cur - D prev),
-// no block-order reading of the z stencil): the exact-mode forward operator
-// whose discrete adjoint the Gauss-Newton product uses.
+// kExact: the exact-mode forward operator whose discrete adjoint the
+// Gauss-Newton product uses: centred damping next = D (C L cur + 2 cur + src)
+// - (2D - 1) prev (energy-stable for D <= 1), no block-order reading of the
+// z stencil.
 template <bool kProbe, bool kExact = false>
 __device__ __forceinline__ bool fwd_consume(const FwdCommon& a, const FwdPar& bp,
                                             const Probe& probe, int* status, int li, float amp,
@@ -217,15 +218,27 @@ __device__ __forceinline__ bool fwd_consume(const FwdCommon& a, const FwdPar& bp
       const float lz = lzz * a.sz;
       const float dd = dxy[e] * dz;
       const float a11 = pick(c11), a13 = pick(c13), a33 = pick(c33);
-      nxv[e] = fmaf(a11, lxy, fmaf(a13, lz, 2.f * c - dd * pick(px)));
-      nzv[e] = fmaf(a13, lxy, fmaf(a33, lz, 2.f * q[e][4] - dd * pick(pz)));
-      if (kProbe && prb_e == e && z == probe.z) *probe.out += nxv[e] + nzv[e];
-      if (src_e == e && z == a.src.z) {
-        nxv[e] += amp;
-        nzv[e] += amp;
+      if (kExact) {
+        // centred damping: D (C L cur + 2 cur + src) - (2D - 1) prev
+        nxv[e] = fmaf(a11, lxy, fmaf(a13, lz, 2.f * c));
+        nzv[e] = fmaf(a13, lxy, fmaf(a33, lz, 2.f * q[e][4]));
+        if (src_e == e && z == a.src.z) {
+          nxv[e] += amp;
+          nzv[e] += amp;
+        }
+        nxv[e] = fmaf(dd, nxv[e], -(2.f * dd - 1.f) * pick(px));
+        nzv[e] = fmaf(dd, nzv[e], -(2.f * dd - 1.f) * pick(pz));
+      } else {
+        nxv[e] = fmaf(a11, lxy, fmaf(a13, lz, 2.f * c - dd * pick(px)));
+        nzv[e] = fmaf(a13, lxy, fmaf(a33, lz, 2.f * q[e][4] - dd * pick(pz)));
+        if (kProbe && prb_e == e && z == probe.z) *probe.out += nxv[e] + nzv[e];
+        if (src_e == e && z == a.src.z) {
+          nxv[e] += amp;
+          nzv[e] += amp;
+        }
+        nxv[e] *= dd;
+        nzv[e] *= dd;
       }
-      nxv[e] *= dd;
-      nzv[e] *= dd;
     }
     const long long i = (long long)z * a.d.plane + off;
     if (v0 && v1) {
