@@ -270,6 +270,14 @@ int vti2d_wavelet_gradient(vti_ctx* ctx, const vti2d_geom* g, float* gwavelet, c
                            const int* sloc, int ns, const int* rloc, int nr, const float* taper);
 /* 2D taper of lib/vti-fwi-2d/init.cpp:70-89 ((nx+2npad)*(nz+2npad) floats). */
 void vti2d_init_taper(float* taper, int nx, int nz, int npad);
+/* Random boundary (lib/random-boundary/randomBound.h:48, RandomMY; randomB.x
+ * calls it with bval = 1, eval = 0.2): field (n1 fastest, n3 = 1 for 2D) is
+ * multiplied, inside the pad of width `pad`, by per-cluster random factors;
+ * clusters grow by a random walk continued with probability pct_g; random
+ * numbers from the C library's rand() after srand(seed), in the reference's
+ * order (host code). */
+int vti_random_boundary(float* field, int n1, int n2, int n3, int pad, float pct_g, int seed,
+                        float bval, float eval);
 
 /* ------------------------------------------------- 3D batched multi-shot */
 /* A window of the model for one shot: cells [x0, x0+nx) x [y0, y0+ny) and the

@@ -3,6 +3,7 @@
 # under /root/reference (read-only; nothing is copied) into oracle/_ref/:
 #   ref3d : lib/vti-fwi-3d/gpu 3D modeling, gradient, RTM (+ the host glue they link)
 #   ref2d : lib/vti-fwi-2d synthetic_f / modeling_f / objFuncGradient_f / GNhessian_f / rtm_f
+#   ref_randb : lib/random-boundary's generator (CPU)
 # linked with the small harnesses oracle/ref_driver{3d,2d}.cpp. Outputs go only
 # to oracle/_ref/ (git-ignored). The binaries run on a GPU host to produce the
 # golden fixtures under tests/golden/ (tests/golden/make_golden.py).
@@ -48,4 +49,6 @@ build_objs "$L2" "$OUT/obj2d" kernels.cu synthetic_f.cu modeling_f.cu objFuncGra
 build_objs "$IO" "$OUT/obj2d" myio.cpp
 "$NVCC" $FLAGS -x cu -c "$HERE/ref_driver2d.cpp" -o "$OUT/obj2d/ref_driver2d.o"
 "$NVCC" $ARCH -Xcompiler -fopenmp -o "$OUT/ref2d" "$OUT"/obj2d/*.o
-echo "built $OUT/ref3d $OUT/ref2d"
+# random-boundary generator (host code, lib/random-boundary/randomBound.h)
+g++ -O2 -std=c++14 -w -I"$REF/lib/random-boundary" "$HERE/ref_randb.cpp" -o "$OUT/ref_randb"
+echo "built $OUT/ref3d $OUT/ref2d $OUT/ref_randb"

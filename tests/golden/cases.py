@@ -110,3 +110,15 @@ def rtm_model3d(c: dict) -> np.ndarray:
     return np.concatenate([V.put_boundary(c["randb"][k * s.nb:(k + 1) * s.nb],
                                           c["cij"][k * n:(k + 1) * n], s.nx, s.ny, s.nz,
                                           s.npad) for k in range(3)])
+
+
+# Random-boundary generator cases: (n1, n2, n3, pad, pctG, seed); n3 = 1 is 2D.
+RANDB_CASES = {"rb3_a": (40, 36, 30, 8, 0.9, 2017), "rb3_b": (48, 40, 36, 10, 0.6, 77),
+               "rb2_a": (120, 80, 1, 20, 0.99, 5)}
+
+
+def randb_input(name: str) -> np.ndarray:
+    """Seeded velocity field of a random-boundary case."""
+    n1, n2, n3, pad, pct, seed = RANDB_CASES[name]
+    rng = np.random.default_rng(1234 + n1 + n3)
+    return (1500 + 3000 * rng.random(n1 * n2 * n3)).astype(np.float32)

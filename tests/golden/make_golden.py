@@ -221,10 +221,29 @@ def make_misfit3d(name, out):
     print(name, {k: float(v[0]) for k, v in res.items()})
 
 
+def make_randb(name, out):
+    """The reference's random-boundary generator (oracle/_ref/ref_randb, host
+    code; no GPU needed) on a seeded field."""
+    n1, n2, n3, pad, pct, seed = K.RANDB_CASES[name]
+    v = K.randb_input(name)
+    with tempfile.TemporaryDirectory() as td:
+        fi, fo = Path(td) / "in.f32", Path(td) / "out.f32"
+        v.tofile(fi)
+        r = subprocess.run([str(REF / "ref_randb"), str(fi), str(fo), str(n1), str(n2), str(n3),
+                            str(pad), str(pct), str(seed)], capture_output=True, text=True,
+                           timeout=600)
+        if r.returncode != 0:
+            raise RuntimeError(r.stderr)
+        w = np.fromfile(fo, dtype=np.float32)
+    np.savez_compressed(out / f"{name}.npz", field=w, input_digest=K.digest(v))
+    print("wrote", name)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=str(HERE))
-    ap.add_argument("--only", choices=["all", "rtm", "wgrad", "misfit", "odcig"], default="all",
+    ap.add_argument("--only", choices=["all", "rtm", "wgrad", "misfit", "odcig", "randb"],
+                    default="all",
                     help="rtm / wgrad: only those fixtures (needs the case fixtures)")
     a = ap.parse_args()
     out = Path(a.out)
@@ -245,6 +264,9 @@ def main():
     if a.only in ("all", "misfit"):
         for n in K.MISFIT_CASES3D:
             make_misfit3d(n, out)
+    if a.only in ("all", "randb"):
+        for n in K.RANDB_CASES:
+            make_randb(n, out)
     if a.only in ("all", "wgrad"):
         for n in K.WGRAD_CASES3D:
             make_wgrad3d(n, out)

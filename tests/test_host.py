@@ -6,7 +6,8 @@ import re
 import numpy as np
 import pytest
 
-from conftest import ROOT, rel_l2
+import cases as K
+from conftest import ROOT, load_golden, rel_l2
 
 import vtib200 as V
 
@@ -161,3 +162,22 @@ def test_binding_argument_counts_match_header():
     wrong = {name: (len(args), protos[name]) for name, (_, args) in V._signatures().items()
              if name in protos and len(args) != protos[name]}
     assert not wrong, wrong
+
+
+@pytest.mark.parametrize("name", sorted(K.RANDB_CASES))
+def test_random_boundary_matches_reference_generator(name):
+    """vti_random_boundary reproduces the reference's random-boundary
+    generator (lib/random-boundary/randomBound.h:48, as randomB.x calls it)
+    bit for bit: same C library rand() sequence, same cluster walk."""
+    n1, n2, n3, pad, pct, seed = K.RANDB_CASES[name]
+    v = K.randb_input(name)
+    gold = load_golden(name)
+    assert str(gold["input_digest"]) == K.digest(v)
+    out = V.random_boundary_ref(v, n1, n2, n3, pad, pct, seed)
+    np.testing.assert_array_equal(out, gold["field"])
+    # only the pad changes, and the velocity is only lowered
+    inner = V.zero_boundary(np.ones(v.size, dtype=np.float32), n1, n2, n3, pad) if n3 > 1 else None
+    r = out / v
+    assert r.max() <= 1.0 and r.min() > 0.2 / 3
+    if inner is not None:
+        assert np.all(r[inner == 1] == 1.0)

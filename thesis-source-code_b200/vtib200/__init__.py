@@ -109,6 +109,8 @@ def _signatures():
         "vti2d_synthetic_noalloc": (C.c_int, [P, P, P, P, P, P, P, C.c_int, P, C.c_int, P, P]),
         "vti2d_modeling": (C.c_int, [P, P, P, P, P, P, C.c_int, P, P]),
         "vti2d_init_taper": (None, [P, C.c_int, C.c_int, C.c_int]),
+        "vti_random_boundary": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
+                                          C.c_int, C.c_float, C.c_float]),
         "vti2d_gradient": (C.c_int, [P] * 11 + [C.c_int, P, C.c_int, P, C.POINTER(C.c_double)]),
         "vti2d_gn_hessian": (C.c_int, [P] * 13 + [C.c_int, P, C.c_int, P]),
         "vti2d_rtm": (C.c_int, [P] * 9 + [C.c_int, P, C.c_int, P]),
@@ -707,6 +709,16 @@ def grad_cij_to_vepsdel(gc11, gc13, gc33, v, eps, dl, v0=1.0, eps0=1.0, del0=1.0
 
 def cfl_number(g: Geom3d, c11, c13, c33):
     return lib().vti3d_cfl_number(C.byref(g), _p(_f32(c11)), _p(_f32(c13)), _p(_f32(c33)))
+
+
+def random_boundary_ref(v, n1, n2, n3, pad, pct_g=0.9, seed=2017, bval=1.0, eval_=0.2):
+    """vti_random_boundary: the reference generator's random boundary of v
+    (randomB.x defaults bval=1, eval=0.2); returns a new array."""
+    out = np.array(v, dtype=np.float32, copy=True).reshape(-1)
+    st = lib().vti_random_boundary(_p(out), n1, n2, n3, pad, pct_g, seed, bval, eval_)
+    if st != VTI_OK:
+        raise VtiError(st, "vti_random_boundary: invalid arguments")
+    return out
 
 
 def init_taper2d(nx, nz, npad):
