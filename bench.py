@@ -506,7 +506,8 @@ def run_served(args):
     budget = int(args.budget_gib * (1 << 30))
 
     def serve(fwi=None):
-        srv = SV.Server(max_bytes=budget, chunk=args.chunk, keep_results=False, log=log)
+        srv = SV.Server(max_bytes=budget, chunk=args.chunk, keep_results=False, log=log,
+                        policy=args.policy)
         t0 = time.perf_counter()
         st = srv.run(SV.make_requests(args.requests, rate=20.0, seed=7) if fwi is None or
                      args.requests_with_fwi else [], fwi=fwi)
@@ -559,7 +560,8 @@ def run_served(args):
                                "401x801 / 3D 128^3..200x400x400, nt U{2000..4000}, Ricker "
                                f"U[10,15] Hz; FWI {args.fwi_iters} iterations x "
                                f"{args.fwi_shots} shots on 400x400x200 windows, nt={args.fwi_nt}",
-                   "engine_budget_gib": args.budget_gib, "chunk_ticks": args.chunk},
+                   "engine_budget_gib": args.budget_gib, "chunk_ticks": args.chunk,
+                   "policy": args.policy},
         "latency_s": {"p50": served["p50_s"], "p99": served["p99_s"]},
         "served": served,
         "gpu_launches": int(served["launches"]), "clocks": clk.summary(),
@@ -778,6 +780,8 @@ def main():
     ap.add_argument("--fwi-nt", type=int, default=1000, help="served workload: FWI time samples")
     ap.add_argument("--plain", action="store_true", help="served workload: also the plain form")
     ap.add_argument("--chunk", type=int, default=32, help="served workload: ticks per step")
+    ap.add_argument("--policy", default="sjf", choices=["sjf", "fifo"],
+                    help="served workload: admission policy of the engine")
     ap.add_argument("--requests-with-fwi", action="store_true",
                     help="served workload: run the requests again beside the FWI")
     ap.add_argument("--gn-grid", type=int, nargs=3, default=[600, 600, 300],

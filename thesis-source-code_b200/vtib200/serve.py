@@ -269,6 +269,17 @@ def plain_gradient(ctx, job):
         p.close()
 
 
+def _points(job):
+    return job.g.nx * job.g.ny * job.g.nz
+
+
+def _work(r):
+    """Estimated device work of a 3D request: points x time steps x the
+    wavefield-pair updates per step (1 modeling, 4 gradient)."""
+    j = r._job
+    return _points(j) * j.g.nt * (4 if j.kind == JOB_GRADIENT else 1)
+
+
 def _summary(res):
     """(sum, L2 norm, misfit) of a result, for callers that keep no arrays."""
     arrs = [a for a in (res if isinstance(res, tuple) else (res,)) if isinstance(a, np.ndarray)]
@@ -281,13 +292,22 @@ def _summary(res):
 class Server:
     """Continuous-batching request loop on one GPU."""
 
-    def __init__(self, device=0, max_bytes=64 << 30, chunk=16, keep_results=True, log=None):
+    def __init__(self, device=0, max_bytes=64 << 30, chunk=16, keep_results=True, log=None,
+                 policy="sjf", max_active_points=24_000_000):
+        """policy "sjf": waiting 3D jobs are admitted shortest (grid points x
+        time steps x passes) first, and only while the grid points of the
+        jobs in flight stay within max_active_points (a larger job runs
+        alone): a launch that already fills the GPU gains nothing from more
+        jobs, which would only share its time. policy "fifo": arrival order,
+        no cap (memory budget only)."""
         self.ctx3 = Context(device)
         self.ctx2 = Context(device)
         self.engine = Engine3d(self.ctx3, max_bytes)
         self.chunk = chunk
         self.keep_results = keep_results
         self.log = log
+        self.policy = policy
+        self.max_active_points = max_active_points
 
     def _log(self, msg):
         if self.log:
@@ -357,23 +377,36 @@ class Server:
                     q3.put(r)
                     waiting.append(r)
             refused = False
-            while waiting:
-                r = waiting[0]
-                if not hasattr(r, "_job"):
-                    if id(r) not in ready:
-                        break  # still being built
+            for r in waiting:
+                if not hasattr(r, "_job") and id(r) in ready:
                     r._job = ready.pop(id(r))
+            if self.policy == "sjf":
+                order = sorted((r for r in waiting if hasattr(r, "_job")), key=_work)
+            else:
+                order = []
+                for r in waiting:  # arrival order up to the first job still being built
+                    if not hasattr(r, "_job"):
+                        break
+                    order.append(r)
+            active_pts = sum(_points(x._job) for x in inflight.values())
+            for r in order:
+                pts = _points(r._job)
+                if (self.policy == "sjf" and inflight and
+                        active_pts + pts > self.max_active_points):
+                    break
                 jid = self.engine.submit(r._job)
                 if jid is None:
                     refused = True
                     break
-                waiting.popleft()
+                waiting.remove(r)
                 r.t_admit = now()
                 inflight[jid] = r
+                active_pts += pts
             active = self.engine.step(self.chunk) if inflight else 0
             for jid in self.engine.poll():
-                r = inflight.pop(jid)
+                r = inflight[jid]
                 res = self.engine.result(jid)
+                del inflight[jid]
                 r.t_done = now()
                 del r._job
                 if r.rid >= 0:
