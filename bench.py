@@ -713,6 +713,90 @@ def run_gnhv(args):
     return res
 
 
+def run_forward2d(args):
+    """Plain 2D VTI forward modeling (synthetic_f) of one shot: nz = 201 x
+    nx = 401 at 10 m plus a 30-cell pad, dt = 1 ms, 2000 steps, five flat
+    layers (v 1500-4500 m/s, eps 0-0.2, delta 0-0.1, seeded interfaces) with a
+    -10 % Gaussian velocity anomaly, 15 Hz Ricker at (z 20 m, x 2000 m), 401
+    receivers at 20 m; the pad's velocity randomised by the reference's
+    random-boundary generator (seed 2, pctG 0.9). Timed on the GPU
+    (vti2d_synthetic, host buffers in and out) next to the FP32 oracle on the
+    host cores (the reference's 2D path has no CPU implementation)."""
+    import torch
+    import vtib200 as V
+    import vtib200.synth as S
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    torch.cuda.set_device(0)
+    s = S.survey2d(nx=401, nz=201, nt=2000, npad=30, d=10.0, dt=1e-3, rate=2e-3, freq=15.0,
+                   src_x=2000.0, src_z=20.0, rec_z=20.0, seed=1)
+    nnx, nnz = s.nx + 2 * s.npad, s.nz + 2 * s.npad
+    # velocity of the layered model back from c33 = v^2, randomised pad, back to c
+    v = np.sqrt(s.c33).astype(np.float32)
+    eps = ((s.c11 / s.c33 - 1) / 2).astype(np.float32)
+    dl = ((np.square(s.c13 / s.c33) - 1) / 2).astype(np.float32)
+    vr = V.random_boundary_ref(v, nnx, nnz, 1, s.npad, 0.9, 2)
+    c11, c13, c33 = V.vepsdel_to_cij(vr, eps, dl)
+    g = s.geom()
+    ctx = V.Context(0)
+    for _ in range(args.warmup):
+        V.synthetic_f(ctx, g, c11, c13, c33, s.wavelet, s.sloc, s.rloc, s.taper)
+    with ClockSampler(0) as clk:
+        ctx.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            tr = V.synthetic_f(ctx, g, c11, c13, c33, s.wavelet, s.sloc, s.rloc, s.taper)
+        ctx.synchronize()
+        wall = (time.perf_counter() - t0) / args.steps
+    ctx.set_timing(True)
+    launches0 = ctx.launches
+    V.synthetic_f(ctx, g, c11, c13, c33, s.wavelet, s.sloc, s.rloc, s.taper)
+    step_ms, step_n = ctx.kernel_time("step2d")
+    ctx.set_timing(False)
+    launches = ctx.launches - launches0
+    snap = V.modeling_f(ctx, g, c11, c13, c33, s.wavelet, int(s.sloc[0] + s.sloc[1] * nnx),
+                        s.taper)
+    ctx.close()
+    pts = (s.nt - 2) * nnx * nnz
+    # CPU: the FP32 oracle of the same shot, all host threads
+    t0 = time.perf_counter()
+    o = O.forward2d(g, c11, c13, c33, s.wavelet, s.sloc, s.rloc, s.taper, dtype=np.float32)
+    cpu_s = time.perf_counter() - t0
+    o64 = O.forward2d(g, c11, c13, c33, s.wavelet, s.sloc, s.rloc, s.taper)
+    err = float(np.linalg.norm(tr.astype(np.float64) - o64) / np.linalg.norm(o64))
+    upd = (nnx - 8) * (nnz - 8)
+    avg = step_ms / max(step_n, 1) / 1e3
+    peak, peak_kind = peaks()
+    res = {
+        "metric": "2D VTI forward modeling throughput (grid-point updates/s)",
+        "value": round(pts / wall / 1e9, 3), "unit": "Gpts/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(wall * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded layered VTI model, reference random boundary)",
+        "config": {"workload": "2D synthetic_f, 401 x 201 + 30-cell pad, nt 2000, dt 1 ms, "
+                               "401 receivers, one shot",
+                   "grid": [nnx, nnz], "nt": s.nt, "traces_rel_l2_vs_fp64_oracle": err,
+                   "final_snapshot_max": float(np.abs(snap[-1]).max())},
+        "roofline": {"bound": "hbm", "kernel": "k_step2d",
+                     "achieved": round(36 * upd / avg / 1e9, 1) if step_n else None,
+                     "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": round(36 * upd / avg / 1e9 / peak, 4) if step_n else None,
+                     "traffic": None, "bytes_per_point": 36,
+                     "avg_launch_ms": round(avg * 1e3, 5),
+                     "note": "the whole 2D state (11 arrays x 0.48 MB) fits in L2"},
+        "cpu_baseline": {"value": round(pts / cpu_s / 1e9, 4), "unit": "Gpts/s",
+                         "cores": os.cpu_count(), "kind": "port",
+                         "sample": "the same shot (all 2000 steps), FP32 oracle"},
+        "e2e": {"value": round(pts / wall / 1e9, 3), "unit": "Gpts/s",
+                "h2d_bytes_per_step": int(4 * (4 * nnx * nnz + s.nt)),
+                "d2h_bytes_per_step": int(tr.nbytes), "api": "vti2d_synthetic (host buffers)"},
+        "gpu_launches": int(launches), "clocks": clk.summary(),
+    }
+    print(json.dumps(res), flush=True)
+    return res
+
+
 def run_reference(args):
     """Reference arm: the reference algorithm's CPU implementation (the FP32
     oracle port; the reference's own CPU path needs ISPC and TBB, absent
@@ -766,7 +850,7 @@ def main():
     ap.add_argument("--config", default="gradient400", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--workload", default="gradient",
-                    choices=["gradient", "batched", "served", "gnhv"],
+                    choices=["gradient", "batched", "served", "gnhv", "forward2d"],
                     help="batched: many shots on their own windows vs the plain loop")
     ap.add_argument("--shots", type=int, default=64, help="batched workload: shots")
     ap.add_argument("--plain-shots", type=int, default=3,
@@ -793,6 +877,8 @@ def main():
     args = ap.parse_args()
     if args.workload == "gnhv" and args.impl == "b200":
         run_gnhv(args)
+    elif args.workload == "forward2d" and args.impl == "b200":
+        run_forward2d(args)
     elif args.workload == "batched" and args.impl == "b200":
         run_batched(args)
     elif args.workload == "served" and args.impl == "b200":
