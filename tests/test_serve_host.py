@@ -1,0 +1,106 @@
+"""CPU tests of the serving loop's host logic (vtib200.serve): the request
+generator, the L-BFGS driver (on a quadratic, with the engine replaced by an
+exact evaluator) and the stacking of window gradients into the model."""
+import numpy as np
+
+import vtib200 as V
+import vtib200.serve as SV
+
+
+def test_requests_follow_the_configured_mix():
+    reqs = SV.make_requests(400, rate=20.0, seed=7)
+    t = np.array([r.arrival for r in reqs])
+    assert np.all(np.diff(t) > 0)
+    gaps = np.diff(np.concatenate([[0.0], t]))
+    assert abs(gaps.mean() - 1 / 20.0) < 0.01  # Poisson, mean 20 per second
+    dims = np.array([r.dim for r in reqs])
+    kinds = np.array([r.kind == "gradient" for r in reqs])
+    assert 0.4 < (dims == 3).mean() < 0.6 and 0.4 < kinds.mean() < 0.6
+    for r in reqs:
+        if r.dim == 3:
+            nx, ny, nz, nt = r.size
+            assert 128 <= nx <= 400 and 128 <= ny <= 400 and 128 <= nz <= 200
+        else:
+            nx, nz, nt = r.size
+            assert 401 <= nx <= 801 and 201 <= nz <= 401
+        assert 2000 <= nt <= 4000
+    # the same seed gives the same requests
+    again = SV.make_requests(400, rate=20.0, seed=7)
+    assert [(r.dim, r.kind, r.arrival, r.size) for r in again] == \
+           [(r.dim, r.kind, r.arrival, r.size) for r in reqs]
+
+
+class _Quadratic(SV.FwiDriver):
+    """FwiDriver whose 'gradient jobs' are evaluated exactly on the host:
+    J(x) = 1/2 (x - x*)^T A (x - x*) split over shots (one window each)."""
+
+    def jobs(self, x):
+        return [x.copy() for _ in self.shots]
+
+    def stack(self, results):
+        f = sum(r[1] for r in results)
+        g = sum(r[0] for r in results)
+        return f, g
+
+
+def _evaluate(x, A, xs, nshot):
+    r = x.astype(np.float64) - xs
+    f = 0.5 * r @ (A @ r) / nshot
+    g = (A @ r / nshot).astype(np.float32)
+    return g, f
+
+
+def test_lbfgs_driver_converges_on_a_quadratic():
+    rng = np.random.default_rng(3)
+    n = 40
+    Q, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    A = Q @ np.diag(np.linspace(1.0, 20.0, n)) @ Q.T
+    xs = rng.standard_normal(n) + 5.0
+    x0 = np.full(n, 5.0, dtype=np.float32)
+    shots = [None] * 3
+    drv = _Quadratic(None, x0, None, shots, iterations=25, step0=0.5, max_step=1.0)
+    jobs = drv.first()
+    while jobs is not None:
+        jobs = drv.update([_evaluate(j, A, xs, len(shots)) for j in jobs])
+    f = np.array(drv.misfits)
+    assert f[-1] < 1e-4 * f[0]
+    assert np.all(np.diff(f) <= 1e-12 * f[0])  # accepted steps never raise the misfit
+
+
+def test_lbfgs_step_is_capped_and_nonfinite_trials_are_rejected():
+    n = 8
+    A = np.eye(n)
+    xs = np.full(n, 100.0)
+    x0 = np.ones(n, dtype=np.float32)
+    drv = _Quadratic(None, x0, None, [None], iterations=2, step0=1000.0, max_step=0.02)
+    jobs = drv.first()
+    jobs = drv.update([_evaluate(j, A, xs, 1) for j in jobs])
+    step = jobs[0] - x0
+    assert np.abs(step).max() <= 0.02 * np.abs(x0).max() * (1 + 1e-6)
+    # a trial whose misfit is not finite is halved, not accepted
+    before = drv.trial.copy()
+    nxt = drv.update([(np.zeros(n, dtype=np.float32), float("nan"))])
+    assert drv.misfits[-1] == drv.misfits[0] and len(drv.misfits) == 1
+    assert np.allclose(nxt[0] - drv.x, 0.5 * (before - drv.x))
+
+
+def test_window_gradients_are_stacked_without_their_frames():
+    """Window (x0, y0, nx, ny) contributes x in [x0 + pad, x0 + nx - pad) and
+    likewise in y, except that a frame lying on the model's edge counts."""
+    g = V.geom3d(20, 18, 6, 10, 3, 10.0, 10.0, 10.0, 1e-3, 2e-3)
+    # window 0: x [0, 9), y [0, 7); window 1 (reaches the far edges): x [7, 20), y [5, 18)
+    wins = [(0, 0, 12, 10), (4, 2, 16, 16)]
+    drv = SV.FwiDriver(g, np.zeros(3 * 20 * 18 * 6, dtype=np.float32), None,
+                       [(None, None, None, w) for w in wins], iterations=1)
+    res = []
+    for (x0, y0, wx, wy) in wins:
+        res.append((np.ones(1 + 3 * wx * wy * g.nz, dtype=np.float32), 1.5))
+    f, full = drv.stack(res)
+    assert f == 3.0
+    a = full.reshape(3, 6, 18, 20)
+    for c in range(3):
+        for z in (0, 5):
+            expect = {(0, 0): 1, (6, 8): 2, (6, 3): 1, (8, 8): 1, (8, 3): 0, (17, 19): 1,
+                      (3, 15): 0}
+            for (y, x), v in expect.items():
+                assert a[c, z, y, x] == v, (c, z, y, x)
