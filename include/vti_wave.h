@@ -140,6 +140,16 @@ void GNhessian_f(float* gc11, float* gc13, float* gc33, const float* data, const
                  int nr, const float* taper, int nx, int nz, int nt, int npad, float dx, float dz,
                  float dt, float rate, float ot);
 
+// wave.h:38 (hessians.cu:28) — GN H*v w.r.t. c11, c13, c33 scaled by c110, c130,
+// c330: the bound check of checkCij (check.cpp:6-20, c13 lowered to 0.99 of
+// sqrt(c110 c11 c330 c33)/c130 where above it, mask m), scaled model and
+// perturbation, GNhessian_f, water-bottom rows zeroed, result scaled back.
+void GNhessianCij(float* gc11, float* gc13, float* gc33, const float* d0, float* c11, float* c13,
+                  float* c33, const float* dc11, const float* dc13, const float* dc33, float c110,
+                  float c130, float c330, const float* wavelet, const int* sloc, int ns,
+                  const int* rloc, int nr, const float* taper, int nx, int nz, int nt, int npad,
+                  float dx, float dz, float dt, float rate, float ot, float wbottom, float* m);
+
 // wave.h:46 (hessians.cu:72) — same w.r.t. v, eps, del.
 void GNhessianVEpsDel(float* gv, float* geps, float* gdel, const float* d0, float* v, float* eps,
                       float* del, const float* dv, const float* deps, const float* ddel, float v0,

@@ -46,6 +46,12 @@ void waveletGradient_f(float* gwavelet, const float* d0, const float* c11, const
                        const float* taper, int nx, int nz, int nt, int npad, float dx, float dz,
                        float dt, float rate);
 
+#ifdef VTI_SHIM
+// Built against libvti_wave.so only: the Gauss-Newton operator classes of
+// lib/vti-fwi-2d/HessianOp.h (declared with the same layout).
+#include "vti_hessian_op.h"
+#endif
+
 template <typename T>
 static std::vector<T> load(const std::string& path, size_t n) {
   std::vector<T> v(n);
@@ -124,6 +130,26 @@ int main(int argc, char** argv) {
                   rate, ot);
     }
     save(dir + "/ref_" + mode + ".bin", g.data(), g.size());
+#ifdef VTI_SHIM
+  } else if (mode == "gnhessop") {
+    // GNHessianOpCij (c110 = c130 = c330 = 1, no water-bottom rows beyond the
+    // pad): forward without and adjoint with accumulation
+    auto rloc = load<int>(dir + "/rloc.bin", 2 * (size_t)nr);
+    std::vector<float> dc(3 * nnxz);
+    const char* names[3] = {"/dc11.bin", "/dc13.bin", "/dc33.bin"};
+    for (int k = 0; k < 3; ++k) {
+      auto part = load<float>(dir + names[k], nnxz);
+      std::copy(part.begin(), part.end(), dc.begin() + k * nnxz);
+    }
+    std::vector<float> mask(nnxz), out(6 * nnxz, 0.f), d0(1, 0.f);
+    GNHessianOpCij op(d0.data(), c11.data(), c13.data(), c33.data(), 1.f, 1.f, 1.f,
+                      wavelet.data(), sloc.data(), ns, rloc.data(), nr, taper.data(), nx, nz, nt,
+                      npad, dx, dz, dt, rate, ot, 0.f, mask.data());
+    op.forward(false, dc.data(), out.data());
+    std::copy(out.begin(), out.begin() + 3 * nnxz, out.begin() + 3 * nnxz);
+    op.adjoint(true, out.data() + 3 * nnxz, dc.data());
+    save(dir + "/ref_gnhessop.bin", out.data(), out.size());
+#endif
   } else if (mode == "rtm") {
     // <dir>/data.bin: the traces to migrate (receiver-fastest rows)
     auto rloc = load<int>(dir + "/rloc.bin", 2 * (size_t)nr);

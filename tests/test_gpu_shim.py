@@ -26,7 +26,8 @@ def drivers(tmp_path_factory):
     for dim in ("3d", "2d"):
         exe = out / f"shim{dim}"
         subprocess.run(
-            ["g++", "-O2", "-std=c++17", str(ROOT / "oracle" / f"ref_driver{dim}.cpp"),
+            ["g++", "-O2", "-std=c++17", "-DVTI_SHIM",
+             str(ROOT / "oracle" / f"ref_driver{dim}.cpp"),
              str(ROOT / "tests" / "shim" / "myio_stub.cpp"), "-I", str(ROOT / "include"),
              f"-L{LIBDIR}", "-lvti_wave", "-lvti_b200", f"-Wl,-rpath,{LIBDIR}", "-o", str(exe)],
             check=True)
@@ -82,6 +83,9 @@ def test_shim_2d_matches_reference(drivers, name):
         grad = np.fromfile(d / "ref_grad.bin", dtype=np.float32)
         _run(drivers["2d"], d, "gnhess")
         gnh = np.fromfile(d / "ref_gnhess.bin", dtype=np.float32)
+        # the Gauss-Newton operator classes (HessianOp.h) through the shim
+        _run(drivers["2d"], d, "gnhessop")
+        op = np.fromfile(d / "ref_gnhessop.bin", dtype=np.float32)
     assert rel_l2(data, gold["data"]) < 1e-5
     nnxz = (s.nx + 2 * s.npad) * (s.nz + 2 * s.npad)
     w = w.reshape(-1, nnxz)
@@ -92,6 +96,13 @@ def test_shim_2d_matches_reference(drivers, name):
         sl = slice(k * nnxz, (k + 1) * nnxz)
         assert rel_l2(grad[sl], ref[sl]) < 1e-4, k
         assert rel_l2(gnh[sl], gold["gnhess"][sl]) < 1e-4, k
+        # GNHessianOpCij: GNhessianCij (scales 1) = GNhessian_f with the pad
+        # rows (npad + 0/dz + 1) zeroed; adjoint(add) doubles it
+        ref_op = np.array(gold["gnhess"][sl], dtype=np.float32).reshape(-1, s.nx + 2 * s.npad)
+        ref_op[:s.npad + 1] = 0
+        assert rel_l2(op[sl], ref_op.reshape(-1)) < 1e-4, k
+        np.testing.assert_array_equal(op[3 * nnxz + k * nnxz:3 * nnxz + (k + 1) * nnxz],
+                                      2 * op[sl])
 
 
 @pytest.mark.parametrize("name", K.RTM_CASES3D)

@@ -10,6 +10,7 @@
 // count (VTI_OPT_REF_GPUS), so numbers match the reference run on those GPUs.
 // Errors are printed to stderr and, like the reference, do not throw; misfits
 // are then NaN.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -25,6 +26,7 @@
 #include <vector>
 
 #include "vti_b200.h"
+#include "vti_hessian_op.h"
 #include "vti_wave.h"
 
 // Recorded by the caller's myio_init(); weak so the shim also links without it.
@@ -748,6 +750,98 @@ void GNhessianVEpsDel(float* gv, float* geps, float* gdel, const float* d0, floa
   std::memset(gv, 0, rows * nnx * sizeof(float));
   std::memset(geps, 0, rows * nnx * sizeof(float));
   std::memset(gdel, 0, rows * nnx * sizeof(float));
+}
+
+// hessians.cu:28-45 and checkCij (check.cpp:6-20).
+void GNhessianCij(float* gc11, float* gc13, float* gc33, const float* d0, float* c11, float* c13,
+                  float* c33, const float* dc11, const float* dc13, const float* dc33, float c110,
+                  float c130, float c330, const float* wavelet, const int* sloc, int ns,
+                  const int* rloc, int nr, const float* taper, int nx, int nz, int nt, int npad,
+                  float dx, float dz, float dt, float rate, float ot, float wbottom, float* m) {
+  const int nnx = nx + 2 * npad, nnz = nz + 2 * npad;
+  const size_t n = (size_t)nnx * nnz;
+  int count = 0;
+  std::memset(m, 0, n * sizeof(float));
+  for (size_t i = 0; i < n; ++i) {
+    const float bound = std::sqrt(c110 * c11[i] * c330 * c33[i]) / c130;
+    if (c13[i] > bound) {
+      c13[i] = (float)(0.99 * bound);
+      ++count;
+      m[i] = 1.f;
+    }
+  }
+  std::fprintf(stderr, "Modified models at %d points\n", count);
+  std::vector<float> c(3 * n), dc(3 * n);
+  for (size_t i = 0; i < n; ++i) {
+    c[i] = c11[i] * c110;
+    c[n + i] = c13[i] * c130;
+    c[2 * n + i] = c33[i] * c330;
+    dc[i] = dc11[i] * c110;
+    dc[n + i] = dc13[i] * c130;
+    dc[2 * n + i] = dc33[i] * c330;
+  }
+  GNhessian_f(gc11, gc13, gc33, d0, c.data(), c.data() + n, c.data() + 2 * n, dc.data(),
+              dc.data() + n, dc.data() + 2 * n, wavelet, sloc, ns, rloc, nr, taper, nx, nz, nt,
+              npad, dx, dz, dt, rate, ot);
+  const size_t rows = std::min<size_t>((size_t)(int)(npad + wbottom / dz + 1), (size_t)nnz);
+  float* gs[3] = {gc11, gc13, gc33};
+  const float sc[3] = {c110, c130, c330};
+  for (int k = 0; k < 3; ++k) {
+    std::memset(gs[k], 0, rows * nnx * sizeof(float));
+    for (size_t i = 0; i < n; ++i) gs[k][i] *= sc[k];
+  }
+}
+
+// Operator interface of the GN Hessian (HessianOp.cu:29-51, 77-99): the
+// product is symmetric, so forward and adjoint are the same call; add = true
+// accumulates into the output.
+namespace {
+template <typename F>
+void apply_op(bool add, long long size, float* out, F&& product) {
+  if (!add) {
+    product(out);
+    return;
+  }
+  std::vector<float> t((size_t)size, 0.f);
+  product(t.data());
+  for (long long i = 0; i < size; ++i) out[i] += t[i];
+}
+}  // namespace
+
+void GNHessianOpCij::forward(bool add, const float* model, float* data) {
+  const long long n = (long long)(_nx + 2 * _npad) * (_nz + 2 * _npad);
+  apply_op(add, _dataSize, data, [&](float* o) {
+    GNhessianCij(o, o + n, o + 2 * n, _d0, _c11, _c13, _c33, model, model + n, model + 2 * n,
+                 _c110, _c130, _c330, _wavelet, _sloc, _ns, _rloc, _nr, _taper, _nx, _nz, _nt,
+                 _npad, _dx, _dz, _dt, _rate, _ot, _wbottom, _m);
+  });
+}
+
+void GNHessianOpCij::adjoint(bool add, float* model, const float* data) {
+  const long long n = (long long)(_nx + 2 * _npad) * (_nz + 2 * _npad);
+  apply_op(add, _modelSize, model, [&](float* o) {
+    GNhessianCij(o, o + n, o + 2 * n, _d0, _c11, _c13, _c33, data, data + n, data + 2 * n,
+                 _c110, _c130, _c330, _wavelet, _sloc, _ns, _rloc, _nr, _taper, _nx, _nz, _nt,
+                 _npad, _dx, _dz, _dt, _rate, _ot, _wbottom, _m);
+  });
+}
+
+void GNHessianOpVEpsDel::forward(bool add, const float* model, float* data) {
+  const long long n = (long long)(_nx + 2 * _npad) * (_nz + 2 * _npad);
+  apply_op(add, _dataSize, data, [&](float* o) {
+    GNhessianVEpsDel(o, o + n, o + 2 * n, _d0, _v, _eps, _del, model, model + n, model + 2 * n,
+                     _v0, _eps0, _del0, _wavelet, _sloc, _ns, _rloc, _nr, _taper, _nx, _nz, _nt,
+                     _npad, _dx, _dz, _dt, _rate, _ot, _wbottom, _m);
+  });
+}
+
+void GNHessianOpVEpsDel::adjoint(bool add, float* model, const float* data) {
+  const long long n = (long long)(_nx + 2 * _npad) * (_nz + 2 * _npad);
+  apply_op(add, _modelSize, model, [&](float* o) {
+    GNhessianVEpsDel(o, o + n, o + 2 * n, _d0, _v, _eps, _del, data, data + n, data + 2 * n,
+                     _v0, _eps0, _del0, _wavelet, _sloc, _ns, _rloc, _nr, _taper, _nx, _nz, _nt,
+                     _npad, _dx, _dz, _dt, _rate, _ot, _wbottom, _m);
+  });
 }
 
 // ---------------------------------------------------------------- RTM
