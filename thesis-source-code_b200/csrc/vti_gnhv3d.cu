@@ -24,7 +24,10 @@
 // exact forward step into a segment buffer, then the adjoint step (w = C mu
 // carried as its own field, so the transposed operator is a plain stencil
 // of w) images against a_{t-1} from the segment. Both adjoints (gradient and
-// H dc) share the recomputation.
+// H dc) share the recomputation. The images are summed blockwise: FP32 within
+// a checkpoint block, FP64 across blocks (compensated accumulation at one
+// FP64 read-modify-write per point per block instead of a compensation term
+// per step).
 #include <algorithm>
 #include <cstring>
 #include <vector>
@@ -625,6 +628,23 @@ __global__ void k_inject_exact(float* mx, float* mz, float* wx, float* wz, float
   atomicAdd(g33 + o, dz_ * azz);
 }
 
+// Blocked summation of the images: the FP32 sums of one checkpoint block are
+// added into FP64 master images and cleared (k_fold); the result is rounded
+// back once (k_unfold). n = the volume's planes x plane floats from origin.
+__global__ void k_fold(double* master, float* img, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    master[i] += (double)img[i];
+    img[i] = 0.f;
+  }
+}
+
+__global__ void k_unfold(const double* master, float* img, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    img[i] = (float)master[i];
+}
+
 const CUtensorMap& PM(const TileMaps& m) { return *(const CUtensorMap*)m.plain; }
 const CUtensorMap& HM(const TileMaps& m) { return *(const CUtensorMap*)m.halo; }
 
@@ -663,6 +683,7 @@ struct GnState {
   std::vector<VolM> seg;       // (K+1) levels x (x, z)
   VolM mu[2][2][2], w[2][2][2];  // [image][buffer][x, z]
   VolM img[2][3];
+  double* master[2][3] = {};  // FP64 sums of the images (blocked summation)
   VolM ring[3][2];            // BF16 mode: FP32 levels of the recomputation
   std::vector<VolB> segb;     // BF16 mode: (K+1) levels x (x, z)
   float* damp = nullptr;
@@ -672,6 +693,9 @@ struct GnState {
       if (x.scale) cudaFree(x.scale);
     }
     for (auto& r : ring) for (auto& x : r) vol_free(&x.v);
+    for (auto& i : master)
+      for (double* q : i)
+        if (q) cudaFree(q);
     auto fr = [](VolM& x) { vol_free(&x.v); };
     for (auto& x : c) fr(x);
     for (auto& x : dc) fr(x);
@@ -1000,8 +1024,15 @@ int vti3d_gnhv_exact(vti_ctx* ctx, const vti3d_geom* g, const float* c11, const 
         VTI_TRY(S.alloc(&S.mu[im][bf][f]));
         VTI_TRY(S.alloc(&S.w[im][bf][f]));
       }
-    for (int k = 0; k < 3; ++k) VTI_TRY(S.alloc(&S.img[im][k]));
+    for (int k = 0; k < 3; ++k) {
+      VTI_TRY(S.alloc(&S.img[im][k]));
+      VTI_CUDA(ctx, cudaMalloc((void**)&S.master[im][k], (size_t)S.d.plane * S.d.nz * sizeof(double)));
+      VTI_CUDA(ctx, cudaMemsetAsync(S.master[im][k], 0,
+                                    (size_t)S.d.plane * S.d.nz * sizeof(double), ctx->stream));
+    }
   }
+  const long long nimg = S.d.plane * S.d.nz;
+  const int fgrid = (int)std::min<long long>((nimg + 255) / 256, ctx->sm_count * 8LL);
   int mcur = 0;  // mu_{t+1} / w_{t+1} buffer (both images step together)
   const float sxs = dt2 / (g->dx * g->dx), sys = dt2 / (g->dy * g->dy), szs = dt2 / (g->dz * g->dz);
   for (int blk = nblk - 1; blk >= 0; --blk) {
@@ -1063,7 +1094,20 @@ int vti3d_gnhv_exact(vti_ctx* ctx, const vti3d_geom* g, const float* c11, const 
       }
       mcur = 1 - mcur;
     }
+    // this block's FP32 image sums into the FP64 masters
+    for (int im = 0; im < 2; ++im)
+      if (want[im])
+        for (int k = 0; k < 3; ++k) {
+          k_fold<<<fgrid, 256, 0, ctx->stream>>>(S.master[im][k], S.img[im][k].v.origin, nimg);
+          VTI_LAUNCHED(ctx, "k_fold");
+        }
   }
+  for (int im = 0; im < 2; ++im)
+    if (want[im])
+      for (int k = 0; k < 3; ++k) {
+        k_unfold<<<fgrid, 256, 0, ctx->stream>>>(S.master[im][k], S.img[im][k].v.origin, nimg);
+        VTI_LAUNCHED(ctx, "k_unfold");
+      }
   const size_t n = (size_t)S.d.npoints();
   float* outs[2] = {grad, hv};
   for (int im = 0; im < 2; ++im)
