@@ -25,9 +25,9 @@
 // carried as its own field, so the transposed operator is a plain stencil
 // of w) images against a_{t-1} from the segment. Both adjoints (gradient and
 // H dc) share the recomputation. The images are summed blockwise: FP32 within
-// a checkpoint block, FP64 across blocks (compensated accumulation at one
-// FP64 read-modify-write per point per block instead of a compensation term
-// per step).
+// a checkpoint block, Kahan-compensated FP32 across blocks (one compensated
+// read-modify-write per point per block instead of a compensation term per
+// step).
 #include <algorithm>
 #include <cstring>
 #include <vector>
@@ -628,21 +628,25 @@ __global__ void k_inject_exact(float* mx, float* mz, float* wx, float* wz, float
   atomicAdd(g33 + o, dz_ * azz);
 }
 
-// Blocked summation of the images: the FP32 sums of one checkpoint block are
-// added into FP64 master images and cleared (k_fold); the result is rounded
-// back once (k_unfold). n = the volume's planes x plane floats from origin.
-__global__ void k_fold(double* master, float* img, long long n) {
+// Blocked, compensated summation of the images: the FP32 sums of one
+// checkpoint block are added into an FP32 master with a Kahan compensation
+// term (k_fold) and cleared; the master is the result (k_unfold copies it
+// back). n = the volume's planes x plane floats from origin.
+__global__ void k_fold(float* master, float* comp, float* img, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
-    master[i] += (double)img[i];
+    const float y = img[i] - comp[i];
+    const float t = master[i] + y;
+    comp[i] = __fsub_rn(__fsub_rn(t, master[i]), y);
+    master[i] = t;
     img[i] = 0.f;
   }
 }
 
-__global__ void k_unfold(const double* master, float* img, long long n) {
+__global__ void k_unfold(const float* master, float* img, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
-    img[i] = (float)master[i];
+    img[i] = master[i];
 }
 
 const CUtensorMap& PM(const TileMaps& m) { return *(const CUtensorMap*)m.plain; }
@@ -683,7 +687,8 @@ struct GnState {
   std::vector<VolM> seg;       // (K+1) levels x (x, z)
   VolM mu[2][2][2], w[2][2][2];  // [image][buffer][x, z]
   VolM img[2][3];
-  double* master[2][3] = {};  // FP64 sums of the images (blocked summation)
+  float* master[2][3] = {};   // compensated FP32 sums of the images: master
+  float* comp[2][3] = {};     // and Kahan compensation
   VolM ring[3][2];            // BF16 mode: FP32 levels of the recomputation
   std::vector<VolB> segb;     // BF16 mode: (K+1) levels x (x, z)
   float* damp = nullptr;
@@ -694,7 +699,10 @@ struct GnState {
     }
     for (auto& r : ring) for (auto& x : r) vol_free(&x.v);
     for (auto& i : master)
-      for (double* q : i)
+      for (float* q : i)
+        if (q) cudaFree(q);
+    for (auto& i : comp)
+      for (float* q : i)
         if (q) cudaFree(q);
     auto fr = [](VolM& x) { vol_free(&x.v); };
     for (auto& x : c) fr(x);
@@ -1026,9 +1034,11 @@ int vti3d_gnhv_exact(vti_ctx* ctx, const vti3d_geom* g, const float* c11, const 
       }
     for (int k = 0; k < 3; ++k) {
       VTI_TRY(S.alloc(&S.img[im][k]));
-      VTI_CUDA(ctx, cudaMalloc((void**)&S.master[im][k], (size_t)S.d.plane * S.d.nz * sizeof(double)));
-      VTI_CUDA(ctx, cudaMemsetAsync(S.master[im][k], 0,
-                                    (size_t)S.d.plane * S.d.nz * sizeof(double), ctx->stream));
+      const size_t nb = (size_t)S.d.plane * S.d.nz * sizeof(float);
+      VTI_CUDA(ctx, cudaMalloc((void**)&S.master[im][k], nb));
+      VTI_CUDA(ctx, cudaMalloc((void**)&S.comp[im][k], nb));
+      VTI_CUDA(ctx, cudaMemsetAsync(S.master[im][k], 0, nb, ctx->stream));
+      VTI_CUDA(ctx, cudaMemsetAsync(S.comp[im][k], 0, nb, ctx->stream));
     }
   }
   const long long nimg = S.d.plane * S.d.nz;
@@ -1094,11 +1104,12 @@ int vti3d_gnhv_exact(vti_ctx* ctx, const vti3d_geom* g, const float* c11, const 
       }
       mcur = 1 - mcur;
     }
-    // this block's FP32 image sums into the FP64 masters
+    // this block's FP32 image sums into the compensated masters
     for (int im = 0; im < 2; ++im)
       if (want[im])
         for (int k = 0; k < 3; ++k) {
-          k_fold<<<fgrid, 256, 0, ctx->stream>>>(S.master[im][k], S.img[im][k].v.origin, nimg);
+          k_fold<<<fgrid, 256, 0, ctx->stream>>>(S.master[im][k], S.comp[im][k],
+                                                 S.img[im][k].v.origin, nimg);
           VTI_LAUNCHED(ctx, "k_fold");
         }
   }
