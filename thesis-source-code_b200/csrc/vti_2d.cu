@@ -210,6 +210,13 @@ int run2d(vti_ctx* ctx, const vti2d_geom* g, const float* c11, const float* c13,
     }
   }
   dim3 block(BX, BZ), grid((nnx - 8 + BX - 1) / BX, (nnz - 8 + BZ - 1) / BZ);
+  // The trace-recording time loop (every node a kernel) is captured as one
+  // CUDA graph: a 2D step is a few microseconds of work, so per-launch
+  // overhead is most of its cost. With per-kernel timing on, or snapshots
+  // copied to the host (modeling), the launches are issued directly.
+  const bool use_graph = mode == 0 && !ctx->timing;
+  cudaGraph_t graph = nullptr;
+  if (use_graph) CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
   for (int it = 2; it < g->nt; ++it) {
     float t = it * dt + g->ot;
     Step2d a{nnx, nnz, p1, q1, p0, q0, dc11, dc13, dc33, dtap, 1.f / dx2, 1.f / dz2, dt2,
@@ -222,12 +229,26 @@ int run2d(vti_ctx* ctx, const vti2d_geom* g, const float* c11, const float* c13,
     if (t >= 0.f && (it - ntNeg) % ratio == 0) {
       st = snapshot((it - ntNeg) / ratio, p0, q0);
       if (st != VTI_OK) {
+        if (use_graph) {
+          cudaStreamEndCapture(ctx->stream, &graph);
+          if (graph) cudaGraphDestroy(graph);
+        }
         cleanup();
         return st;
       }
     }
     std::swap(p0, p1);
     std::swap(q0, q1);
+  }
+  if (use_graph) {
+    CK(cudaStreamEndCapture(ctx->stream, &graph));
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    CK(ei);
+    const cudaError_t el = cudaGraphLaunch(exec, ctx->stream);
+    cudaGraphExecDestroy(exec);  // released once the launch completes
+    CK(el);
   }
   CK(cudaGetLastError());
   if (mode == 0 && nri > 0) {
