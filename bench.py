@@ -293,7 +293,8 @@ def run_e2e(args, ctx, s, cstart, padb, randb, dobs, flags):
     return {"value": round(val, 3), "unit": "Gpts/s", "h2d_bytes_per_step": int(bi),
             "d2h_bytes_per_step": int(4 * (1 + 3 * n)), "steps": steps,
             "ms_per_step": round(ms / steps, 2),
-            "api": "vti3d_gradient_cij (host buffers, plan created per call)"}
+            "api": "vti3d_gradient_cij (host buffers; the context keeps the plan "
+                   "between calls of the same geometry)"}
 
 
 def cpu_baseline(s, cstart, args, target_s=15.0):

@@ -181,7 +181,15 @@ const float* vti3d_plan_wavefield(vti3d_plan* plan);
  * modelData3d_f.cu:324 / modeling3d_f.cu:266) into nxyz contiguous floats. */
 int vti3d_plan_get_wavefield(vti3d_plan* plan, float* out, int mem);
 
-/* One-call host-buffer forms (what the drop-in shim calls). */
+/* One-call host-buffer forms (what the drop-in shim calls). The context keeps
+ * the plan of the last 3D one-call form (device volumes, tensor maps) and
+ * reuses it while the next call has the same geometry and flags: every call
+ * rewrites the model, wavelet and receivers and zeroes the wavefields and
+ * accumulators, so results do not depend on the calls before. A call that
+ * fails drops the kept plan. vti_ctx_set_plan_cache(ctx, 0) frees the kept
+ * plan and makes each call create and free its own (the reference's
+ * behaviour); 1 (the default) turns keeping back on. */
+int vti_ctx_set_plan_cache(vti_ctx* ctx, int enable);
 int vti3d_model_data_cij(vti_ctx* ctx, const vti3d_geom* g, const float* c11, const float* c13,
                          const float* c33, const float* wavelet, const float* souloc,
                          const int* shotid, int nshot, const float* recloc, int nrec_total,

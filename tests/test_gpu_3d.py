@@ -131,6 +131,38 @@ def test_plan_reuse_is_deterministic_and_objfunc_agrees(ctx):
         p.close()
 
 
+def test_one_call_forms_keep_no_state_between_calls(ctx):
+    """The context keeps the plan of the one-call forms while the geometry and
+    flags repeat (gradient with a random boundary, modeling without one,
+    another model): every output equals that of calls with their own plan."""
+    c = K.case3d("g3_a")
+    s = c["s"]
+    g = s.geom()
+    n = s.nxyz
+    dobs = load_golden("g3_a")["dobs"]
+
+    def run():
+        fa, ma = V.objFuncGradientCij3d_f(ctx, g, s.souloc, c["shotid"], s.recloc, s.wavelet,
+                                          c["cij"], c["padb"], c["randb"], dobs)
+        d = V.modelDataCij3d_f(ctx, g, s.souloc, c["shotid"], s.recloc, s.wavelet,
+                               *_split(c["cij_true"], n))
+        fb, mb = V.objFuncGradientCij3d_f(ctx, g, s.souloc, c["shotid"], s.recloc, s.wavelet,
+                                          c["cij_true"], c["padb"], c["randb"], dobs)
+        return fa, ma, d, fb, mb
+
+    kept = run()
+    again = run()
+    ctx.set_plan_cache(False)
+    try:
+        fresh = run()
+    finally:
+        ctx.set_plan_cache(True)
+    assert np.abs(kept[2]).max() > 0 and kept[1] > 0 and kept[4] != kept[1]
+    for a, b, r in zip(kept, again, fresh):
+        np.testing.assert_array_equal(a, r)
+        np.testing.assert_array_equal(b, r)
+
+
 def test_zero_residual_gives_zero_gradient(ctx):
     """Observed data modeled by the library itself: residual and gradient are 0."""
     s = S.small3d(nx=72, ny=64, nz=48, nt=130, npad=8, rec_step=2)

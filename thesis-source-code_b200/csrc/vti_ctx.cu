@@ -165,6 +165,7 @@ int vti_ctx_create(int device, vti_ctx** out) {
 int vti_ctx_destroy(vti_ctx* ctx) {
   if (!ctx) return VTI_OK;
   cudaSetDevice(ctx->device);
+  vti_ctx_set_plan_cache(ctx, 0);
   if (ctx->stream) {
     cudaStreamSynchronize(ctx->stream);
     release_events(ctx);

@@ -63,6 +63,11 @@ struct vti_ctx {
   bool timing = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events[vti::kNumTimed];
   std::vector<cudaEvent_t> event_pool;
+  // plan kept by the one-call 3D forms while their geometry and flags repeat
+  bool plan_cache = true;
+  vti3d_plan* cached_plan = nullptr;
+  vti3d_geom cached_geom{};
+  unsigned cached_flags = 0;
 };
 
 namespace vti {

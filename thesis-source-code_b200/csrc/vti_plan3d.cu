@@ -386,10 +386,51 @@ int run_gradient(vti3d_plan* p, const float* souloc, const int* shotid, int nsho
   return VTI_OK;
 }
 
+// Plan of a one-call form: the context's kept plan when geometry and flags
+// match it, else a new one (kept in its place when keeping is on).
+int one_call_plan(vti_ctx* ctx, const vti3d_geom* g, unsigned flags, vti3d_plan** out) {
+  if (!ctx || !g || !out) return VTI_ERR_ARG;
+  if (ctx->plan_cache && ctx->cached_plan && ctx->cached_flags == flags &&
+      std::memcmp(&ctx->cached_geom, g, sizeof(vti3d_geom)) == 0) {
+    *out = ctx->cached_plan;
+    return VTI_OK;
+  }
+  if (ctx->cached_plan) {
+    vti3d_plan_destroy(ctx->cached_plan);
+    ctx->cached_plan = nullptr;
+  }
+  VTI_TRY(vti3d_plan_create(ctx, g, flags, out));
+  if (ctx->plan_cache) {
+    ctx->cached_plan = *out;
+    ctx->cached_geom = *g;
+    ctx->cached_flags = flags;
+  }
+  return VTI_OK;
+}
+
+// End of a one-call form: a plan that is not kept, or that saw an error, is
+// freed.
+int one_call_done(vti_ctx* ctx, vti3d_plan* p, int st) {
+  if (p == ctx->cached_plan && st == VTI_OK) return st;
+  if (p == ctx->cached_plan) ctx->cached_plan = nullptr;
+  vti3d_plan_destroy(p);
+  return st;
+}
+
 }  // namespace p3d
 }  // namespace vti
 
 extern "C" {
+
+int vti_ctx_set_plan_cache(vti_ctx* ctx, int enable) {
+  if (!ctx) return VTI_ERR_ARG;
+  ctx->plan_cache = enable != 0;
+  if (!ctx->plan_cache && ctx->cached_plan) {
+    vti3d_plan_destroy(ctx->cached_plan);
+    ctx->cached_plan = nullptr;
+  }
+  return VTI_OK;
+}
 
 int vti3d_plan_create(vti_ctx* ctx, const vti3d_geom* g, unsigned flags, vti3d_plan** out) {
   if (!ctx || !out) return VTI_ERR_ARG;
@@ -593,13 +634,12 @@ int vti3d_model_data_cij(vti_ctx* ctx, const vti3d_geom* g, const float* c11, co
                          const int* shotid, int nshot, const float* recloc, int nrec_total,
                          float* ddata, unsigned flags) {
   vti3d_plan* p = nullptr;
-  VTI_TRY(vti3d_plan_create(ctx, g, flags, &p));
+  VTI_TRY(one_call_plan(ctx, g, flags, &p));
   int st = vti3d_plan_set_model(p, c11, c13, c33, nullptr, nullptr, VTI_MEM_HOST);
   if (st == VTI_OK) st = vti3d_plan_set_wavelet(p, wavelet, VTI_MEM_HOST);
   if (st == VTI_OK) st = vti3d_plan_set_receivers(p, recloc, nrec_total);
   if (st == VTI_OK) st = vti3d_plan_model_data(p, souloc, shotid, nshot, ddata, VTI_MEM_HOST);
-  vti3d_plan_destroy(p);
-  return st;
+  return one_call_done(ctx, p, st);
 }
 
 int vti3d_plan_rtm(vti3d_plan* p, const float* souloc, const int* shotid, int nshot,
@@ -705,14 +745,13 @@ int vti3d_wavelet_gradient_cij(vti_ctx* ctx, const vti3d_geom* g, const float* c
                                const int* shotid, int nshot, const float* recloc, int nrec_total,
                                const float* data, float* gwavelet, unsigned flags) {
   vti3d_plan* p = nullptr;
-  VTI_TRY(vti3d_plan_create(ctx, g, flags, &p));
+  VTI_TRY(one_call_plan(ctx, g, flags, &p));
   int st = vti3d_plan_set_model(p, c11, c13, c33, nullptr, nullptr, VTI_MEM_HOST);
   if (st == VTI_OK) st = vti3d_plan_set_receivers(p, recloc, nrec_total);
   if (st == VTI_OK)
     st = vti3d_plan_wavelet_gradient(p, souloc, shotid, nshot, data, VTI_MEM_HOST, gwavelet,
                                      VTI_MEM_HOST);
-  vti3d_plan_destroy(p);
-  return st;
+  return one_call_done(ctx, p, st);
 }
 
 int vti3d_rtm_cij(vti_ctx* ctx, const vti3d_geom* g, const float* c11, const float* c13,
@@ -720,14 +759,13 @@ int vti3d_rtm_cij(vti_ctx* ctx, const vti3d_geom* g, const float* c11, const flo
                   int nshot, const float* recloc, int nrec_total, const float* data,
                   float* image, unsigned flags) {
   vti3d_plan* p = nullptr;
-  VTI_TRY(vti3d_plan_create(ctx, g, flags, &p));
+  VTI_TRY(one_call_plan(ctx, g, flags, &p));
   int st = vti3d_plan_set_model(p, c11, c13, c33, nullptr, nullptr, VTI_MEM_HOST);
   if (st == VTI_OK) st = vti3d_plan_set_wavelet(p, wavelet, VTI_MEM_HOST);
   if (st == VTI_OK) st = vti3d_plan_set_receivers(p, recloc, nrec_total);
   if (st == VTI_OK)
     st = vti3d_plan_rtm(p, souloc, shotid, nshot, data, VTI_MEM_HOST, image, VTI_MEM_HOST);
-  vti3d_plan_destroy(p);
-  return st;
+  return one_call_done(ctx, p, st);
 }
 
 int vti3d_gradient_cij(vti_ctx* ctx, const vti3d_geom* g, const float* cij, const float* padb,
@@ -736,7 +774,7 @@ int vti3d_gradient_cij(vti_ctx* ctx, const vti3d_geom* g, const float* cij, cons
                        const float* dobs, float* fgcij, double* misfit, unsigned flags) {
   if (!cij) return fail(ctx, VTI_ERR_ARG, "null cij");
   vti3d_plan* p = nullptr;
-  VTI_TRY(vti3d_plan_create(ctx, g, flags, &p));
+  VTI_TRY(one_call_plan(ctx, g, flags, &p));
   const size_t n = (size_t)g->nx * g->ny * g->nz;
   int st = vti3d_plan_set_model(p, cij, cij + n, cij + 2 * n, padb, randb, VTI_MEM_HOST);
   if (st == VTI_OK) st = vti3d_plan_set_wavelet(p, wavelet, VTI_MEM_HOST);
@@ -744,8 +782,7 @@ int vti3d_gradient_cij(vti_ctx* ctx, const vti3d_geom* g, const float* cij, cons
   if (st == VTI_OK)
     st = vti3d_plan_gradient(p, souloc, shotid, nshot, dobs, VTI_MEM_HOST, fgcij, VTI_MEM_HOST,
                              misfit);
-  vti3d_plan_destroy(p);
-  return st;
+  return one_call_done(ctx, p, st);
 }
 
 }  // extern "C"
