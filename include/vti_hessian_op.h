@@ -7,13 +7,7 @@
 #ifndef VTI_HESSIAN_OP_H
 #define VTI_HESSIAN_OP_H
 
-class Operator {
- public:
-  Operator(long long modelSize, long long dataSize) : _modelSize(modelSize), _dataSize(dataSize) {}
-  virtual void forward(bool add, const float* model, float* data) = 0;
-  virtual void adjoint(bool add, float* model, const float* data) = 0;
-  long long _modelSize, _dataSize;
-};
+#include "vti_operator.h"
 
 class GNHessianOpCij : public Operator {
  public:

@@ -3,7 +3,8 @@
 // tests/golden/make_golden.py. TEST INFRASTRUCTURE ONLY: it produces golden
 // traces and gradients that pin the oracle; nothing in the library uses it.
 //
-// usage: ref3d <dir> model|grad|rtm|wgrad [key=value ...]
+// usage: ref3d <dir> model|grad|rtm|wgrad|modop [key=value ...] (modop: built with
+//   -DVTI_SHIM against libvti_wave.so, which provides ModelingOp3d)
 //   <dir>/params.txt : nx ny nz nt npad ox oy oz ot dx dy dz dt rate ns nrec
 //   <dir>/{souloc,recloc,wavelet,cij,padb,randb,dobs}.bin (float32)
 //   writes <dir>/ref_ddata.bin (model), <dir>/ref_fgcij.bin (grad) or
@@ -14,6 +15,12 @@
 #include <fstream>
 #include <string>
 #include <vector>
+
+#ifdef VTI_SHIM
+// built against libvti_wave.so: the source-inversion operator class
+// (ModelingOp3d.h) is available as well (mode modop)
+#include "vti_modeling_op3d.h"
+#endif
 
 // Entry points of lib/vti-fwi-3d/gpu (wave3d.h:84-122) and lib/io/myio.cpp:15.
 void myio_init(int argc, char** argv);
@@ -126,6 +133,27 @@ int main(int argc, char** argv) {
                            cij.data(), cij.data() + n, cij.data() + 2 * n, nx, ny, nz, nt, npad,
                            ox, oy, oz, ot, dx, dy, dz, dt, rate, gpus);
     save(dir + "/ref_wgrad.bin", gw.data(), gw.size());
+#ifdef VTI_SHIM
+  } else if (mode == "modop") {
+    // ModelingOp3d (ModelingOp3d.cu:12-33) with and without add: forward of
+    // the wavelet -> ref_modop_fwd.bin, forward added onto ones ->
+    // ref_modop_fwd_add.bin, adjoint of dobs.bin -> ref_modop_adj.bin,
+    // adjoint added onto ones -> ref_modop_adj_add.bin
+    ModelingOp3d op(souloc.data(), ns, shotid, recloc.data(), cij.data(), cij.data() + n,
+                    cij.data() + 2 * n, nx, ny, nz, nt, npad, ox, oy, oz, ot, dx, dy, dz, dt,
+                    rate, gpus, 1);
+    auto data = load(dir + "/dobs.bin", (size_t)nnt * nrec);
+    std::vector<float> d0((size_t)op._dataSize, 0.f), d1((size_t)op._dataSize, 1.f);
+    std::vector<float> m0((size_t)op._modelSize, 0.f), m1((size_t)op._modelSize, 1.f);
+    op.forward(false, wavelet.data(), d0.data());
+    op.forward(true, wavelet.data(), d1.data());
+    op.adjoint(false, m0.data(), data.data());
+    op.adjoint(true, m1.data(), data.data());
+    save(dir + "/ref_modop_fwd.bin", d0.data(), d0.size());
+    save(dir + "/ref_modop_fwd_add.bin", d1.data(), d1.size());
+    save(dir + "/ref_modop_adj.bin", m0.data(), m0.size());
+    save(dir + "/ref_modop_adj_add.bin", m1.data(), m1.size());
+#endif
   } else {
     std::fprintf(stderr, "unknown mode %s\n", mode.c_str());
     return 2;

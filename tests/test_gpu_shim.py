@@ -145,6 +145,35 @@ def test_shim_wavelet_gradient3d_matches_reference(drivers, name):
     assert rel_l2(gw, load_golden(f"{name}_wgrad")["gwavelet"]) < 1e-4
 
 
+@pytest.mark.parametrize("name", K.WGRAD_CASES3D)
+def test_shim_modeling_operator3d(drivers, name):
+    """ModelingOp3d (ModelingOp3d.cu:12-33) from the reference's header layout:
+    forward = modelData3d_f of the wavelet (the reference's traces), adjoint =
+    waveletGradient3d_f (the reference's wavelet gradient), add accumulates."""
+    c = K.case3d(name)
+    gold = load_golden(name)
+    with tempfile.TemporaryDirectory() as td:
+        d = Path(td)
+        MG.write_inputs3d(c, d)
+        np.asarray(gold["dobs"], np.float32).tofile(d / "dobs.bin")
+        np.asarray(c["cij_true"], np.float32).tofile(d / "cij.bin")
+        _run(drivers["3d"], d, "model")
+        _run(drivers["3d"], d, "modop")
+        ddata = np.fromfile(d / "ref_ddata.bin", dtype=np.float32)
+        fwd = np.fromfile(d / "ref_modop_fwd.bin", dtype=np.float32)
+        fwd_add = np.fromfile(d / "ref_modop_fwd_add.bin", dtype=np.float32)
+        K.pad_model3d(c).astype(np.float32).tofile(d / "cij.bin")
+        _run(drivers["3d"], d, "modop")
+        adj = np.fromfile(d / "ref_modop_adj.bin", dtype=np.float32)
+        adj_add = np.fromfile(d / "ref_modop_adj_add.bin", dtype=np.float32)
+    np.testing.assert_array_equal(fwd, ddata)
+    assert rel_l2(fwd, gold["dobs"]) < 1e-5
+    np.testing.assert_array_equal(fwd_add, np.float32(1) + fwd)
+    assert adj.size == c["s"].nt
+    assert rel_l2(adj, load_golden(f"{name}_wgrad")["gwavelet"]) < 1e-4
+    np.testing.assert_array_equal(adj_add, np.float32(1) + adj)
+
+
 @pytest.mark.parametrize("name", K.WGRAD_CASES2D)
 def test_shim_wavelet_gradient2d_matches_reference(drivers, name):
     s = K.case2d(name)["s"]

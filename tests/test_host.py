@@ -30,6 +30,24 @@ def test_binding_declares_only_header_symbols():
     assert set(V.exported_symbols()) <= set(header_functions())
 
 
+@pytest.mark.parametrize("dim", ["3d", "2d"])
+def test_reference_harness_links_against_the_shim(dim, tmp_path):
+    """The harness that drives the reference's C++ entry points and operator
+    classes (oracle/ref_driver{3d,2d}.cpp) compiles against include/ and links
+    to libvti_wave.so alone: every entry it calls is exported with the
+    reference's C++ signature. Nothing is run."""
+    import subprocess
+    libdir = V.LIB_PATH.parent
+    exe = tmp_path / f"shim{dim}"
+    r = subprocess.run(
+        ["g++", "-O0", "-std=c++17", "-DVTI_SHIM", str(ROOT / "oracle" / f"ref_driver{dim}.cpp"),
+         str(ROOT / "tests" / "shim" / "myio_stub.cpp"), "-I", str(ROOT / "include"),
+         f"-L{libdir}", "-lvti_wave", "-lvti_b200", f"-Wl,-rpath,{libdir}", "-o", str(exe)],
+        capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-3000:]
+    assert exe.exists()
+
+
 def _boundary_mask(nx, ny, nz, npad):
     m = np.ones((nz, ny, nx), dtype=bool)
     m[npad:nz - npad, npad:ny - npad, npad:nx - npad] = False

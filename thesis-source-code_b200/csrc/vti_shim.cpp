@@ -27,6 +27,7 @@
 
 #include "vti_b200.h"
 #include "vti_hessian_op.h"
+#include "vti_modeling_op3d.h"
 #include "vti_wave.h"
 
 // Recorded by the caller's myio_init(); weak so the shim also links without it.
@@ -1012,6 +1013,25 @@ void waveletGradient3d_f(float* gwavelet, const float* ddata, float* souloc, int
   std::memset(gwavelet, 0, nt * sizeof(float));
   for (int i = ngpugroup - 1; i >= 0; --i)  // the reference's summation order
     for (int j = 0; j < nt; ++j) gwavelet[j] += gw[i][j];
+}
+
+// Source-inversion operator (ModelingOp3d.cu:12-33): traces of the wavelet
+// `model`, and the wavelet gradient of the traces `data`; add = true
+// accumulates.
+void ModelingOp3d::forward(bool add, const float* model, float* data) {
+  apply_op(add, _dataSize, data, [&](float* o) {
+    modelData3d_f(o, _souloc, _ns, _shotid, _recloc, model, _c11, _c13, _c33, _nx, _ny, _nz, _nt,
+                  _npad, _ox, _oy, _oz, _ot, _dx, _dy, _dz, _dt, _samplingRate, _GPUs,
+                  _ngpugroup);
+  });
+}
+
+void ModelingOp3d::adjoint(bool add, float* model, const float* data) {
+  apply_op(add, _modelSize, model, [&](float* o) {
+    waveletGradient3d_f(o, data, _souloc, _ns, _shotid, _recloc, _c11, _c13, _c33, _nx, _ny, _nz,
+                        _nt, _npad, _ox, _oy, _oz, _ot, _dx, _dy, _dz, _dt, _samplingRate, _GPUs,
+                        _ngpugroup);
+  });
 }
 
 // waveletGradient_f (objFuncGradient_f.cu:373-530): shots round-robin over the
