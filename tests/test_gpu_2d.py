@@ -88,3 +88,27 @@ def test_synthetic_config_size(ctx):
     d = V.synthetic_f(ctx, g, s.c11, s.c13, s.c33, s.wavelet, s.sloc, s.rloc, s.taper)
     o = O.forward2d(g, s.c11, s.c13, s.c33, s.wavelet, s.sloc, s.rloc, s.taper)
     assert rel_l2(d, o) < 1e-5
+
+
+@pytest.mark.parametrize("kw", [
+    dict(),  # the benchmark grid: 461 x 261, 16 CTAs of 16 rows, source in exchanged rows
+    dict(nx=97, nz=37, nt=240, npad=9, d=10.0, dt=1e-3, rate=1e-3, freq=20.0, src_x=480.0,
+         src_z=120.0, rec_z=0.0, ns=2),  # ragged rows, every step sampled, source in exchanged rows
+    dict(nx=1100, nz=24, nt=120, npad=8, d=10.0, dt=1e-3, rate=2e-3, freq=15.0, src_x=5000.0,
+         src_z=100.0, rec_z=20.0),  # wider than one cluster: per-step path either way
+])
+def test_resident_traces_equal_per_step_traces(ctx, kw):
+    """The shared-memory resident launch (one cluster per shot) and the
+    per-step launches compute every point with the same operations: the
+    traces are bitwise equal."""
+    s = S.survey2d(**kw)
+    g = s.geom()
+    args = (ctx, g, s.c11, s.c13, s.c33, s.wavelet, s.sloc, s.rloc, s.taper)
+    res = V.synthetic_f(*args)
+    ctx.set_2d_resident(False)
+    try:
+        step = V.synthetic_f(*args)
+    finally:
+        ctx.set_2d_resident(True)
+    assert np.abs(step).max() > 0
+    np.testing.assert_array_equal(res, step)

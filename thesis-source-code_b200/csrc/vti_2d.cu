@@ -14,6 +14,9 @@
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <utility>
+
+#include <cooperative_groups.h>
 
 #include "vti_internal.h"
 
@@ -41,6 +44,12 @@ struct Step2d {
   const float* amp;  // device pointer to the source amplitude of this step
 };
 
+// Launched as a programmatic dependent launch: the model and taper (fixed for
+// the whole run) are read before griddepcontrol.wait, which returns once the
+// previous kernel of the stream (the step that wrote cur, or a recording) has
+// completed and its writes are visible; prev, which that step read as its cur,
+// is read and overwritten only after it. Launched normally, the wait returns
+// at once.
 __global__ void __launch_bounds__(BX* BZ) k_step2d(Step2d a) {
   __shared__ float sp[BZ][BX + 8];
   __shared__ float sq[BZ + 8][BX];
@@ -49,6 +58,20 @@ __global__ void __launch_bounds__(BX* BZ) k_step2d(Step2d a) {
   const int iz = kHalo + blockIdx.y * BZ + tz;
   const bool valid = ix < a.nnx - kHalo && iz < a.nnz - kHalo;
   const int i = ix + iz * a.nnx;
+  float t = 0.f, c11 = 0.f, c13 = 0.f, c33 = 0.f;
+  if (valid) {
+    t = __ldg(a.taper + i);
+    c11 = __ldg(a.c11 + i);
+    c13 = __ldg(a.c13 + i);
+    c33 = __ldg(a.c33 + i);
+  }
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  float p0 = 0.f, q0 = 0.f;
+  if (valid) {
+    p0 = a.p0[i];
+    q0 = a.q0[i];
+  }
   // stage p rows (x halo) and q columns (z halo); out-of-range lanes load 0
   auto ldp = [&](int x) { return (x < a.nnx && iz < a.nnz) ? a.p1[x + iz * a.nnx] : 0.f; };
   auto ldq = [&](int z) { return (ix < a.nnx && z < a.nnz) ? a.q1[ix + z * a.nnx] : 0.f; };
@@ -77,9 +100,8 @@ __global__ void __launch_bounds__(BX* BZ) k_step2d(Step2d a) {
   tq = fmaf(kC4, sq[tz][tx] + sq[tz + 8][tx], tq);
   tp *= a.idx2;
   tq *= a.idz2;
-  const float t = a.taper[i];
-  float pn = fmaf(a.dt2, fmaf(a.c11[i], tp, a.c13[i] * tq), 2.f * r[0] - t * a.p0[i]);
-  float qn = fmaf(a.dt2, fmaf(a.c13[i], tp, a.c33[i] * tq), 2.f * sq[tz + 4][tx] - t * a.q0[i]);
+  float pn = fmaf(a.dt2, fmaf(c11, tp, c13 * tq), 2.f * r[0] - t * p0);
+  float qn = fmaf(a.dt2, fmaf(c13, tp, c33 * tq), 2.f * sq[tz + 4][tx] - t * q0);
   if (i == a.src) {
     const float s = *a.amp;
     pn += s;
@@ -92,6 +114,8 @@ __global__ void __launch_bounds__(BX* BZ) k_step2d(Step2d a) {
 // recordData (kernels.cu:317-324): 0.5(p+q) at receivers into row `row`.
 __global__ void k_record2d(float* data, long long row_off, const float* p, const float* q,
                            const int* ridx, int nr) {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   int ir = blockIdx.x * blockDim.x + threadIdx.x;
   if (ir < nr) {
     int i = ridx[ir];
@@ -105,10 +129,319 @@ __global__ void k_init2d(float* p, float* q, int src, float value, float taper_a
   q[src] = value * taper_at_src;
 }
 
+// ---------------------------------------------------------------- resident
+// The whole 2D state of one shot held in the shared memory of one thread-block
+// cluster for all time steps (one launch per shot). CTA r of the cluster owns
+// update rows z in [4 + r*R, 4 + r*R + nr) and keeps, in rows of W floats
+// (W = nnx rounded up to even), p at two levels (R rows each), q at two
+// levels with 4 halo rows above and below (R + 8 rows each), and the taper
+// and c13 of its rows. Every step each point is updated exactly as in
+// k_step2d (same operations in the same order), the new q of the first and
+// last 4 owned rows is also stored into the neighbours' halo rows (distributed
+// shared memory), and one cluster barrier closes the step. Thread t < S*NP
+// (NP = ceil(X/2) column pairs of the X = nnx - 8 update columns, S =
+// blockDim / NP segments) owns the columns x0 = 4 + 2*(t % NP) and x0 + 1
+// (when x0 + 1 < nnx - 4) over up to kResRows consecutive rows of its CTA:
+// 64-bit shared loads serve both columns, c11 and c33 stay in registers, q's z
+// stencil runs as a register queue.
+constexpr int kResThreads = 512, kResRows = 8, kResMaxCluster = 16;
+
+struct Res2d {
+  int nnx, nnz, nt;
+  int W;             // shared-memory row stride (floats, even)
+  int rows_per_cta;  // R
+  int seg_rows;      // rows per thread segment
+  int segs;          // S
+  const float* c11;
+  const float* c13;
+  const float* c33;
+  const float* taper;
+  float idx2, idz2, dt2;
+  int src_x, src_z;
+  float init_value;     // dt2 * wavelet[0], level 1 at the source before the taper
+  const float* amp;     // amp[it]: source term of level it
+  const int* rec_row;   // trace row recorded at level it, -1 none
+  const int* rx;        // receiver columns and rows
+  const int* rz;
+  int nri;
+  float* data;          // rows x nri
+};
+
+// 32-bit shared::cluster address of `p` (this CTA's shared memory) in the
+// shared memory of cluster CTA `rank`, and stores there.
+__device__ __forceinline__ uint32_t cluster_addr(const float* p, int rank) {
+  const uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void st_cluster(uint32_t addr, float v) {
+  asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(addr), "f"(v) : "memory");
+}
+__device__ __forceinline__ void st_cluster2(uint32_t addr, float2 v) {
+  asm volatile("st.shared::cluster.v2.f32 [%0], {%1, %2};" ::"r"(addr), "f"(v.x), "f"(v.y)
+               : "memory");
+}
+
+__device__ __forceinline__ void res_record(const Res2d& a, int row, const float* p, const float* q,
+                                           int zr0, int nr) {
+  for (int ir = threadIdx.x; ir < a.nri; ir += blockDim.x) {
+    const int x = __ldg(a.rx + ir), lz = __ldg(a.rz + ir) - zr0;
+    // cells outside the update region stay 0, as the zeroed trace rows
+    if (lz >= 0 && lz < nr && x >= kHalo && x < a.nnx - kHalo)
+      a.data[(long long)row * a.nri + ir] = 0.5f * (p[lz * a.W + x] + q[(lz + 4) * a.W + x]);
+  }
+}
+
+__global__ void __launch_bounds__(kResThreads, 1)
+    k_synth2d_resident(const __grid_constant__ Res2d a) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  extern __shared__ __align__(16) float sm[];
+  const int rank = (int)cl.block_rank();
+  const int ncta = (int)cl.num_blocks();
+  const int nnx = a.nnx, W = a.W;
+  const int R = a.rows_per_cta;
+  const int zr0 = kHalo + rank * R;
+  const int nr = min(R, a.nnz - 2 * kHalo - rank * R);
+  // float offsets of the slots in sm
+  const int oP0 = 0, oP1 = R * W, oQ0 = 2 * R * W, oQ1 = oQ0 + (R + 8) * W;
+  const int oT = oQ1 + (R + 8) * W, oM13 = oT + R * W;
+  for (int i = threadIdx.x; i < oT; i += blockDim.x) sm[i] = 0.f;
+  for (int i = threadIdx.x; i < nr * nnx; i += blockDim.x) {
+    const int row = i / nnx, col = i - row * nnx;
+    sm[oT + row * W + col] = __ldg(a.taper + zr0 * nnx + i);
+    sm[oM13 + row * W + col] = __ldg(a.c13 + zr0 * nnx + i);
+  }
+  __syncthreads();
+  // level 1 (slot 1): the source after the taper (synthetic_f.cu:86-89); every
+  // CTA writes its own copy, halo rows included
+  if (threadIdx.x == 0) {
+    const float v = a.init_value * __ldg(a.taper + a.src_x + a.src_z * nnx);
+    const int lz = a.src_z - zr0;
+    if (lz >= 0 && lz < nr) sm[oP1 + lz * W + a.src_x] = v;
+    if (lz >= -4 && lz < nr + 4) sm[oQ1 + (lz + 4) * W + a.src_x] = v;
+  }
+  // this thread's column pair and rows
+  const int NP = (nnx - 2 * kHalo + 1) / 2;
+  const int t = threadIdx.x;
+  const bool active = t < a.segs * NP;
+  const int seg = active ? t / NP : 0;
+  const int x = kHalo + 2 * (active ? t % NP : 0);
+  const bool two = x + 1 < nnx - kHalo;  // the second column is updated
+  const int r0 = seg * a.seg_rows;
+  const int cnt = active ? max(0, min(a.seg_rows, nr - r0)) : 0;
+  float2 m11[kResRows], m33[kResRows];
+#pragma unroll
+  for (int j = 0; j < kResRows; ++j) {
+    const int i = x + (zr0 + r0 + j) * nnx;
+    const bool v = j < cnt;
+    m11[j] = make_float2(v ? __ldg(a.c11 + i) : 0.f, v && two ? __ldg(a.c11 + i + 1) : 0.f);
+    m33[j] = make_float2(v ? __ldg(a.c33 + i) : 0.f, v && two ? __ldg(a.c33 + i + 1) : 0.f);
+  }
+  const int src_e = a.src_x - x;  // 0 or 1 when the source is in this thread's columns
+  const bool src_mine = cnt > 0 && (src_e == 0 || (src_e == 1 && two)) &&
+                        a.src_z >= zr0 + r0 && a.src_z < zr0 + r0 + cnt;
+  // Q slot 0 of the CTA above (rank - 1) and below (rank + 1); slot 1 lies
+  // qslot bytes further
+  const uint32_t up0 = rank > 0 ? cluster_addr(sm + oQ0, rank - 1) : 0u;
+  const uint32_t dn0 = rank + 1 < ncta ? cluster_addr(sm + oQ0, rank + 1) : 0u;
+  const uint32_t qslot = (uint32_t)((oQ1 - oQ0) * sizeof(float));
+  // every CTA of the cluster is running and initialised before any remote store
+  cl.sync();
+  if (a.nt > 1 && __ldg(a.rec_row + 1) >= 0)
+    res_record(a, __ldg(a.rec_row + 1), sm + oP1, sm + oQ1, zr0, nr);
+  int cur = 1;
+  float amp_next = a.nt > 2 ? __ldg(a.amp + 2) : 0.f;
+  for (int it = 2; it < a.nt; ++it) {
+    const int nxt = cur ^ 1;
+    const float amp = amp_next;
+    if (it + 1 < a.nt) amp_next = __ldg(a.amp + it + 1);
+    if (cnt > 0) {
+      const float* Pc = sm + (cur ? oP1 : oP0) + x;
+      const float* Qc = sm + (cur ? oQ1 : oQ0) + 4 * W + x;  // row = owned row, -4 .. nr+3
+      float* Pn = sm + (nxt ? oP1 : oP0) + x;
+      float* Qn = sm + (nxt ? oQ1 : oQ0) + 4 * W + x;
+      const float* Tr = sm + oT + x;
+      const float* Cr = sm + oM13 + x;
+      const uint32_t up = up0 + (nxt ? qslot : 0u) + 4u * (uint32_t)x;
+      const uint32_t dn = dn0 + (nxt ? qslot : 0u) + 4u * (uint32_t)x;
+      float2 qz[9];
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+        qz[k + 1] = *reinterpret_cast<const float2*>(Qc + (r0 - 4 + k) * W);
+#pragma unroll
+      for (int j = 0; j < kResRows; ++j) {
+        if (j < cnt) {
+          const int lr = r0 + j;
+#pragma unroll
+          for (int k = 0; k < 8; ++k) qz[k] = qz[k + 1];
+          qz[8] = *reinterpret_cast<const float2*>(Qc + (lr + 4) * W);
+          const float* pr = Pc + lr * W;
+          float v[10];
+#pragma unroll
+          for (int k = 0; k < 5; ++k) {
+            const float2 u = *reinterpret_cast<const float2*>(pr - 4 + 2 * k);
+            v[2 * k] = u.x;
+            v[2 * k + 1] = u.y;
+          }
+          const int o = lr * W;
+          const float2 pp = *reinterpret_cast<const float2*>(Pn + o);
+          const float2 qp = *reinterpret_cast<const float2*>(Qn + o);
+          const float2 tt = *reinterpret_cast<const float2*>(Tr + o);
+          const float2 cc = *reinterpret_cast<const float2*>(Cr + o);
+          float pn[2], qn[2];
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            auto pick = [e](float2 w) { return e ? w.y : w.x; };
+            const float* r = v + 4 + e;
+            float tp = kC0 * r[0];
+            tp = fmaf(kC1, r[-1] + r[1], tp);
+            tp = fmaf(kC2, r[-2] + r[2], tp);
+            tp = fmaf(kC3, r[-3] + r[3], tp);
+            tp = fmaf(kC4, r[-4] + r[4], tp);
+            float tq = kC0 * pick(qz[4]);
+            tq = fmaf(kC1, pick(qz[3]) + pick(qz[5]), tq);
+            tq = fmaf(kC2, pick(qz[2]) + pick(qz[6]), tq);
+            tq = fmaf(kC3, pick(qz[1]) + pick(qz[7]), tq);
+            tq = fmaf(kC4, pick(qz[0]) + pick(qz[8]), tq);
+            tp *= a.idx2;
+            tq *= a.idz2;
+            const float tj = pick(tt), c13 = pick(cc);
+            float a_ = fmaf(a.dt2, fmaf(pick(m11[j]), tp, c13 * tq), 2.f * r[0] - tj * pick(pp));
+            float b_ =
+                fmaf(a.dt2, fmaf(c13, tp, pick(m33[j]) * tq), 2.f * pick(qz[4]) - tj * pick(qp));
+            if (src_mine && src_e == e && zr0 + lr == a.src_z) {
+              a_ += amp;
+              b_ += amp;
+            }
+            pn[e] = tj * a_;
+            qn[e] = tj * b_;
+          }
+          const float2 q2 = make_float2(qn[0], qn[1]);
+          // halo rows of the neighbours: my first 4 rows are the bottom halo
+          // of rank - 1 (which owns R rows), my last 4 the top halo of rank + 1
+          const bool to_up = lr < 4 && rank > 0;
+          const bool to_dn = lr >= nr - 4 && rank + 1 < ncta;
+          if (two) {
+            *reinterpret_cast<float2*>(Pn + o) = make_float2(pn[0], pn[1]);
+            *reinterpret_cast<float2*>(Qn + o) = q2;
+            if (to_up) st_cluster2(up + 4u * (uint32_t)((R + 4 + lr) * W), q2);
+            if (to_dn) st_cluster2(dn + 4u * (uint32_t)((lr - nr + 4) * W), q2);
+          } else {
+            Pn[o] = pn[0];
+            Qn[o] = qn[0];
+            if (to_up) st_cluster(up + 4u * (uint32_t)((R + 4 + lr) * W), qn[0]);
+            if (to_dn) st_cluster(dn + 4u * (uint32_t)((lr - nr + 4) * W), qn[0]);
+          }
+        }
+      }
+    }
+    cl.sync();
+    const int row = __ldg(a.rec_row + it);
+    if (row >= 0)
+      res_record(a, row, sm + (nxt ? oP1 : oP0), sm + (nxt ? oQ1 : oQ0), zr0, nr);
+    cur = nxt;
+  }
+  // no CTA leaves while a neighbour may still read its memory
+  cl.sync();
+}
+
+// Launch with programmatic stream serialization: the kernel may start while
+// the previous kernel of the stream runs; its griddepcontrol.wait orders its
+// dependent reads and writes after that kernel.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, cudaStream_t s,
+                       Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
+
 struct Dev2d {
   float* buf = nullptr;  // c11 c13 c33 taper p0 q0 p1 q1 amps
   size_t n = 0;
 };
+
+// Cluster shape of the resident path for an nnx x nnz grid: the largest
+// cluster (most SMs) whose CTAs each own >= 4 rows, whose threads each own
+// <= kResRows rows of one column pair, whose shared memory fits one CTA and
+// which the device can schedule. false: the grid does not fit one cluster.
+struct ResShape {
+  int ctas = 0, rows = 0, segs = 0, seg_rows = 0, W = 0;
+  size_t smem = 0;
+};
+bool attr_res[64] = {};
+
+bool resident_shape(vti_ctx* ctx, int nnx, int nnz, ResShape* out) {
+  constexpr size_t kMaxSmem = 227 * 1024;
+  const int NP = (nnx - 2 * kHalo + 1) / 2, rows = nnz - 2 * kHalo;
+  const int W = (nnx + 1) & ~1;
+  if (NP < 1 || rows < 4 || NP > kResThreads) return false;
+  if (ctx->device < 64 && !attr_res[ctx->device]) {
+    if (cudaFuncSetAttribute(k_synth2d_resident, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kMaxSmem) != cudaSuccess ||
+        cudaFuncSetAttribute(k_synth2d_resident,
+                             cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    attr_res[ctx->device] = true;
+  }
+  const int S = kResThreads / NP;
+  for (int C = kResMaxCluster; C >= 1; --C) {
+    const int R = (rows + C - 1) / C;
+    const int last = rows - (C - 1) * R;
+    if (R < 4 || last < 4) continue;
+    const int RS = (R + S - 1) / S;
+    const size_t smem = (size_t)(6 * R + 16) * W * sizeof(float);
+    if (RS > kResRows || smem > kMaxSmem) return false;  // fewer CTAs only need more
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(C);
+    cfg.blockDim = dim3(kResThreads);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = C;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int nclusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&nclusters, k_synth2d_resident, &cfg) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    if (nclusters < 1) continue;
+    *out = ResShape{C, R, S, RS, W, smem};
+    return true;
+  }
+  return false;
+}
+
+cudaError_t launch_resident(const ResShape& sh, const Res2d& a, cudaStream_t stream) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(sh.ctas);
+  cfg.blockDim = dim3(kResThreads);
+  cfg.dynamicSmemBytes = sh.smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = sh.ctas;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_synth2d_resident, a);
+}
 
 }  // namespace
 }  // namespace vti
@@ -116,6 +449,23 @@ struct Dev2d {
 using namespace vti;
 
 namespace {
+
+// The context's 2D scratch, grown (never shrunk) to `bytes`; freed with the
+// context.
+int scratch2d(vti_ctx* ctx, size_t bytes, float** out) {
+  if (ctx->scratch2d_bytes < bytes) {
+    if (ctx->scratch2d) {
+      VTI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+      cudaFree(ctx->scratch2d);
+      ctx->scratch2d = nullptr;
+      ctx->scratch2d_bytes = 0;
+    }
+    VTI_CUDA(ctx, cudaMalloc((void**)&ctx->scratch2d, bytes));
+    ctx->scratch2d_bytes = bytes;
+  }
+  *out = ctx->scratch2d;
+  return VTI_OK;
+}
 
 int run2d(vti_ctx* ctx, const vti2d_geom* g, const float* c11, const float* c13, const float* c33,
           const float* wavelet, const float* taper, int slocxz, const int* rloc, int nri,
@@ -131,24 +481,36 @@ int run2d(vti_ctx* ctx, const vti2d_geom* g, const float* c11, const float* c13,
   const int ratio = mode == 0 ? (int)(g->rate / dt + 0.5f) : (int)std::round(g->rate / dt);
   if (ratio < 1) return fail(ctx, VTI_ERR_ARG, "rate < dt");
   const int ntNeg = (int)std::round(std::fabs(g->ot) / dt);
+  // trace row (or snapshot) taken at each level, -1 none (synthetic_f.cu:95-110)
+  std::vector<int> rec_row(g->nt, -1);
+  if (ratio == 1 && g->ot == 0.f) rec_row[1] = 1;
+  for (int it = 2; it < g->nt; ++it) {
+    float t = it * dt + g->ot;
+    if (t >= 0.f && (it - ntNeg) % ratio == 0) rec_row[it] = (it - ntNeg) / ratio;
+  }
   VTI_CUDA(ctx, cudaSetDevice(ctx->device));
-  // device buffers: 4 model/taper + 4 wavefields + nt amplitudes + receivers + output rows
+  // device buffers (the context's 2D scratch, kept between calls): 4
+  // model/taper + 4 wavefields + nt amplitudes, then ints (trace row per
+  // level, receiver columns and rows, or flat receiver indices), then the
+  // output rows
   const long long nrows_out = mode == 0 ? (g->nt - ntNeg - 1) / ratio + 1 : 0;
+  const int nrec = mode == 0 ? std::max(nri, 0) : 0;
+  const size_t nbuf = 8 * (size_t)nnxz + g->nt;
+  const size_t n_ints = (size_t)g->nt + 2 * (size_t)nrec;
+  const size_t n_data = (size_t)nrows_out * nrec;
   float* buf = nullptr;
-  size_t nbuf = 8 * (size_t)nnxz + g->nt;
-  VTI_CUDA(ctx, cudaMalloc((void**)&buf, nbuf * sizeof(float)));
+  {
+    const int sst = scratch2d(ctx, (nbuf + n_ints + n_data) * sizeof(float), &buf);
+    if (sst != VTI_OK) return sst;
+  }
   float *dc11 = buf, *dc13 = dc11 + nnxz, *dc33 = dc13 + nnxz, *dtap = dc33 + nnxz;
   float* w[4] = {dtap + nnxz, dtap + 2 * nnxz, dtap + 3 * nnxz, dtap + 4 * nnxz};
   float* amps = dtap + 5 * nnxz;
-  int* d_ridx = nullptr;
-  float* d_data = nullptr;
+  int* d_ints = reinterpret_cast<int*>(buf + nbuf);
+  int* d_ridx = d_ints;
+  float* d_data = nrec > 0 ? buf + nbuf + n_ints : nullptr;
   int st = VTI_OK;
-  auto cleanup = [&]() {
-    cudaStreamSynchronize(ctx->stream);
-    cudaFree(buf);
-    if (d_ridx) cudaFree(d_ridx);
-    if (d_data) cudaFree(d_data);
-  };
+  auto cleanup = [&]() { cudaStreamSynchronize(ctx->stream); };
 #define CK(call)                                  \
   do {                                            \
     cudaError_t e_ = (call);                      \
@@ -178,12 +540,43 @@ int run2d(vti_ctx* ctx, const vti2d_geom* g, const float* c11, const float* c13,
       }
       ridx[ir] = x + z * nnx;
     }
-    CK(cudaMalloc((void**)&d_ridx, nri * sizeof(int)));
-    CK(cudaMemcpyAsync(d_ridx, ridx.data(), nri * sizeof(int), cudaMemcpyHostToDevice,
-                       ctx->stream));
-    CK(cudaMalloc((void**)&d_data, (size_t)nrows_out * nri * sizeof(float)));
     CK(cudaMemsetAsync(d_data, 0, (size_t)nrows_out * nri * sizeof(float), ctx->stream));
   }
+  // Traces of a grid that fits one thread-block cluster: one launch runs all
+  // levels with the state in shared memory (k_synth2d_resident). The source
+  // must lie in the update region (a source outside it keeps its level-1
+  // value in one buffer only, which the per-step path below reproduces).
+  const int src_x = slocxz % nnx, src_z = slocxz / nnx;
+  ResShape shape;
+  if (mode == 0 && ctx->resident2d && src_x >= kHalo && src_x < nnx - kHalo && src_z >= kHalo &&
+      src_z < nnz - kHalo && resident_shape(ctx, nnx, nnz, &shape)) {
+    std::vector<int> hi(rec_row);
+    hi.resize(g->nt + 2 * (size_t)nri);
+    for (int ir = 0; ir < nri; ++ir) {
+      hi[g->nt + ir] = ridx[ir] % nnx;
+      hi[g->nt + nri + ir] = ridx[ir] / nnx;
+    }
+    CK(cudaMemcpyAsync(d_ints, hi.data(), hi.size() * sizeof(int), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    Res2d a{nnx, nnz, g->nt, shape.W, shape.rows, shape.seg_rows, shape.segs, dc11, dc13, dc33, dtap,
+            1.f / dx2, 1.f / dz2, dt2, src_x, src_z, dt2 * wavelet[0], amps, d_ints,
+            d_ints + g->nt, d_ints + g->nt + nri, nri, d_data};
+    {
+      LaunchTimer tm(ctx, kTimedStep2d);
+      CK(launch_resident(shape, a, ctx->stream));
+    }
+    ctx->launches++;
+    CK(cudaGetLastError());
+    if (nri > 0)
+      CK(cudaMemcpy2DAsync(out + ir0, (size_t)nr_total * 4, d_data, (size_t)nri * 4,
+                           (size_t)nri * 4, nrows_out, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    cleanup();
+    return VTI_OK;
+  }
+  if (nrec > 0)
+    CK(cudaMemcpyAsync(d_ridx, ridx.data(), nri * sizeof(int), cudaMemcpyHostToDevice,
+                       ctx->stream));
   // time level 1: source then taper (synthetic_f.cu:86-89)
   k_init2d<<<1, 1, 0, ctx->stream>>>(w[2], w[3], slocxz, dt2 * wavelet[0], taper[slocxz]);
   ctx->launches++;
@@ -191,8 +584,9 @@ int run2d(vti_ctx* ctx, const vti2d_geom* g, const float* c11, const float* c13,
   auto snapshot = [&](long long row, const float* p, const float* q) -> int {
     if (mode == 0) {
       if (nri > 0) {
-        k_record2d<<<(nri + 127) / 128, 128, 0, ctx->stream>>>(d_data, row * nri, p, q, d_ridx,
-                                                                nri);
+        cudaError_t e = launch_pdl(k_record2d, dim3((nri + 127) / 128), dim3(128), ctx->stream,
+                                   d_data, row * nri, p, q, (const int*)d_ridx, nri);
+        if (e != cudaSuccess) return cuda_check(ctx, e, "k_record2d launch");
         ctx->launches++;
       }
     } else {
@@ -202,8 +596,8 @@ int run2d(vti_ctx* ctx, const vti2d_geom* g, const float* c11, const float* c13,
     }
     return VTI_OK;
   };
-  if (ratio == 1 && g->ot == 0.f) {
-    st = snapshot(1, p1, q1);
+  if (rec_row[1] >= 0) {
+    st = snapshot(rec_row[1], p1, q1);
     if (st != VTI_OK) {
       cleanup();
       return st;
@@ -218,24 +612,22 @@ int run2d(vti_ctx* ctx, const vti2d_geom* g, const float* c11, const float* c13,
   cudaGraph_t graph = nullptr;
   if (use_graph) CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
   for (int it = 2; it < g->nt; ++it) {
-    float t = it * dt + g->ot;
     Step2d a{nnx, nnz, p1, q1, p0, q0, dc11, dc13, dc33, dtap, 1.f / dx2, 1.f / dz2, dt2,
              slocxz, amps + it};
     {
       LaunchTimer tm(ctx, kTimedStep2d);
-      k_step2d<<<grid, block, 0, ctx->stream>>>(a);
+      const cudaError_t e = launch_pdl(k_step2d, grid, block, ctx->stream, a);
+      st = e == cudaSuccess ? VTI_OK : cuda_check(ctx, e, "k_step2d launch");
     }
     ctx->launches++;
-    if (t >= 0.f && (it - ntNeg) % ratio == 0) {
-      st = snapshot((it - ntNeg) / ratio, p0, q0);
-      if (st != VTI_OK) {
-        if (use_graph) {
-          cudaStreamEndCapture(ctx->stream, &graph);
-          if (graph) cudaGraphDestroy(graph);
-        }
-        cleanup();
-        return st;
+    if (st == VTI_OK && rec_row[it] >= 0) st = snapshot(rec_row[it], p0, q0);
+    if (st != VTI_OK) {
+      if (use_graph) {
+        cudaStreamEndCapture(ctx->stream, &graph);
+        if (graph) cudaGraphDestroy(graph);
       }
+      cleanup();
+      return st;
     }
     std::swap(p0, p1);
     std::swap(q0, q1);

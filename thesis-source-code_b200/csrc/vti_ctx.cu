@@ -173,7 +173,14 @@ int vti_ctx_destroy(vti_ctx* ctx) {
     cudaStreamDestroy(ctx->stream);
   }
   if (ctx->d_status) cudaFree(ctx->d_status);
+  if (ctx->scratch2d) cudaFree(ctx->scratch2d);
   delete ctx;
+  return VTI_OK;
+}
+
+int vti_ctx_set_2d_resident(vti_ctx* ctx, int enable) {
+  if (!ctx) return VTI_ERR_ARG;
+  ctx->resident2d = enable != 0;
   return VTI_OK;
 }
 

@@ -63,6 +63,11 @@ struct vti_ctx {
   bool timing = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events[vti::kNumTimed];
   std::vector<cudaEvent_t> event_pool;
+  // 2D traces of grids that fit one thread-block cluster run shared-memory resident
+  bool resident2d = true;
+  // device scratch of the 2D forward forms, kept between calls
+  float* scratch2d = nullptr;
+  size_t scratch2d_bytes = 0;
   // plan kept by the one-call 3D forms while their geometry and flags repeat
   bool plan_cache = true;
   vti3d_plan* cached_plan = nullptr;

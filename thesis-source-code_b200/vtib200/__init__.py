@@ -79,6 +79,7 @@ def _signatures():
         "vti_ctx_kernel_launches": (C.c_uint64, [P]),
         "vti_ctx_set_timing": (C.c_int, [P, C.c_int]),
         "vti_ctx_set_plan_cache": (C.c_int, [P, C.c_int]),
+        "vti_ctx_set_2d_resident": (C.c_int, [P, C.c_int]),
         "vti_ctx_kernel_time": (C.c_int, [P, C.c_char_p, C.POINTER(C.c_double),
                                           C.POINTER(C.c_uint64)]),
         "vti3d_cfl_number": (C.c_double, [P, P, P, P]),
@@ -222,6 +223,10 @@ class Context:
 
     def set_timing(self, enable: bool):
         self.check(lib().vti_ctx_set_timing(self._h, 1 if enable else 0))
+
+    def set_2d_resident(self, enable: bool):
+        """Shared-memory resident 2D traces where the grid fits one cluster (default)."""
+        self.check(lib().vti_ctx_set_2d_resident(self._h, 1 if enable else 0))
 
     def set_plan_cache(self, enable: bool):
         """Keep (default) or free the plan of the one-call 3D forms between calls."""
