@@ -789,9 +789,9 @@ def run_forward2d(args):
                      "traffic": 0 if resident else None, "bytes_per_point": 36,
                      "avg_step_ms": round(avg * 1e3, 5),
                      "note": ("one launch per shot: the wavefields, taper and c13 stay in the "
-                              "shared memory of one 16-CTA cluster for all steps, so no "
-                              "per-step DRAM traffic and a frac above 1; the bound is "
-                              "instruction issue on the cluster's 16 SMs")
+                              "shared memory of one 16-CTA cluster for all steps, so there "
+                              "is no per-step DRAM traffic; the bound is instruction issue "
+                              "on the cluster's 16 SMs, not HBM")
                      if resident else "the whole 2D state (11 arrays x 0.48 MB) fits in L2"},
         "cpu_baseline": {"value": round(pts / cpu_s / 1e9, 4), "unit": "Gpts/s",
                          "cores": os.cpu_count(), "kind": "port",

@@ -193,6 +193,100 @@ __device__ __forceinline__ void res_record(const Res2d& a, int row, const float*
   }
 }
 
+// One thread's rows of one level (k_synth2d_resident).
+struct ResRows {
+  const float* Pc;  // cur p, q (q rows -4 .. nr+3), next p, q, taper, c13: at column x
+  const float* Qc;
+  float* Pn;
+  float* Qn;
+  const float* Tr;
+  const float* Cr;
+  uint32_t up, dn;  // the neighbours' next-q slots at column x (shared::cluster)
+  int W, r0, cnt, nr, R;
+  bool to_up, to_dn, two;
+  int src_row, src_e;
+  float amp;
+};
+
+template <bool kFull>
+__device__ __forceinline__ void res_rows(const Res2d& a, const ResRows& rr,
+                                         const float2 (&m11)[kResRows],
+                                         const float2 (&m33)[kResRows]) {
+  const int W = rr.W;
+  float2 qz[9];
+#pragma unroll
+  for (int k = 0; k < 8; ++k)
+    qz[k + 1] = *reinterpret_cast<const float2*>(rr.Qc + (rr.r0 - 4 + k) * W);
+#pragma unroll
+  for (int j = 0; j < kResRows; ++j) {
+    if (kFull || j < rr.cnt) {
+      const int lr = rr.r0 + j;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) qz[k] = qz[k + 1];
+      qz[8] = *reinterpret_cast<const float2*>(rr.Qc + (lr + 4) * W);
+      const float* pr = rr.Pc + lr * W;
+      float v[10];
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        const float2 u = *reinterpret_cast<const float2*>(pr - 4 + 2 * k);
+        v[2 * k] = u.x;
+        v[2 * k + 1] = u.y;
+      }
+      const int o = lr * W;
+      const float2 pp = *reinterpret_cast<const float2*>(rr.Pn + o);
+      const float2 qp = *reinterpret_cast<const float2*>(rr.Qn + o);
+      const float2 tt = *reinterpret_cast<const float2*>(rr.Tr + o);
+      const float2 cc = *reinterpret_cast<const float2*>(rr.Cr + o);
+      float pn[2], qn[2];
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        auto pick = [e](float2 w) { return e ? w.y : w.x; };
+        const float* r = v + 4 + e;
+        float tp = kC0 * r[0];
+        tp = fmaf(kC1, r[-1] + r[1], tp);
+        tp = fmaf(kC2, r[-2] + r[2], tp);
+        tp = fmaf(kC3, r[-3] + r[3], tp);
+        tp = fmaf(kC4, r[-4] + r[4], tp);
+        float tq = kC0 * pick(qz[4]);
+        tq = fmaf(kC1, pick(qz[3]) + pick(qz[5]), tq);
+        tq = fmaf(kC2, pick(qz[2]) + pick(qz[6]), tq);
+        tq = fmaf(kC3, pick(qz[1]) + pick(qz[7]), tq);
+        tq = fmaf(kC4, pick(qz[0]) + pick(qz[8]), tq);
+        tp *= a.idx2;
+        tq *= a.idz2;
+        const float tj = pick(tt), c13 = pick(cc);
+        float a_ = fmaf(a.dt2, fmaf(pick(m11[j]), tp, c13 * tq), 2.f * r[0] - tj * pick(pp));
+        float b_ =
+            fmaf(a.dt2, fmaf(c13, tp, pick(m33[j]) * tq), 2.f * pick(qz[4]) - tj * pick(qp));
+        if (lr == rr.src_row && e == rr.src_e) {
+          a_ += rr.amp;
+          b_ += rr.amp;
+        }
+        pn[e] = tj * a_;
+        qn[e] = tj * b_;
+      }
+      const float2 q2 = make_float2(qn[0], qn[1]);
+      // halo rows of the neighbours: my first 4 rows are the bottom halo of
+      // rank - 1 (which owns R rows), my last 4 the top halo of rank + 1
+      const bool to_up = rr.to_up && lr < 4;
+      const bool to_dn = rr.to_dn && lr >= rr.nr - 4;
+      const uint32_t ua = rr.up + 4u * (uint32_t)((rr.R + 4 + lr) * W);
+      const uint32_t da = rr.dn + 4u * (uint32_t)((lr - rr.nr + 4) * W);
+      if (rr.two) {
+        *reinterpret_cast<float2*>(rr.Pn + o) = make_float2(pn[0], pn[1]);
+        *reinterpret_cast<float2*>(rr.Qn + o) = q2;
+        if (to_up) st_cluster2(ua, q2);
+        if (to_dn) st_cluster2(da, q2);
+      } else {
+        rr.Pn[o] = pn[0];
+        rr.Qn[o] = qn[0];
+        if (to_up) st_cluster(ua, qn[0]);
+        if (to_dn) st_cluster(da, qn[0]);
+      }
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kResThreads, 1)
     k_synth2d_resident(const __grid_constant__ Res2d a) {
   namespace cg = cooperative_groups;
@@ -231,6 +325,11 @@ __global__ void __launch_bounds__(kResThreads, 1)
   const bool two = x + 1 < nnx - kHalo;  // the second column is updated
   const int r0 = seg * a.seg_rows;
   const int cnt = active ? max(0, min(a.seg_rows, nr - r0)) : 0;
+  const int src_e = a.src_x - x;  // 0 or 1 when the source is in this thread's columns
+  const bool src_mine = cnt > 0 && (src_e == 0 || (src_e == 1 && two)) &&
+                        a.src_z >= zr0 + r0 && a.src_z < zr0 + r0 + cnt;
+  const int src_row = src_mine ? a.src_z - zr0 : -1;  // owned row of the source
+  // c11 and c33 of the thread's rows
   float2 m11[kResRows], m33[kResRows];
 #pragma unroll
   for (int j = 0; j < kResRows; ++j) {
@@ -239,9 +338,6 @@ __global__ void __launch_bounds__(kResThreads, 1)
     m11[j] = make_float2(v ? __ldg(a.c11 + i) : 0.f, v && two ? __ldg(a.c11 + i + 1) : 0.f);
     m33[j] = make_float2(v ? __ldg(a.c33 + i) : 0.f, v && two ? __ldg(a.c33 + i + 1) : 0.f);
   }
-  const int src_e = a.src_x - x;  // 0 or 1 when the source is in this thread's columns
-  const bool src_mine = cnt > 0 && (src_e == 0 || (src_e == 1 && two)) &&
-                        a.src_z >= zr0 + r0 && a.src_z < zr0 + r0 + cnt;
   // Q slot 0 of the CTA above (rank - 1) and below (rank + 1); slot 1 lies
   // qslot bytes further
   const uint32_t up0 = rank > 0 ? cluster_addr(sm + oQ0, rank - 1) : 0u;
@@ -258,84 +354,31 @@ __global__ void __launch_bounds__(kResThreads, 1)
     const float amp = amp_next;
     if (it + 1 < a.nt) amp_next = __ldg(a.amp + it + 1);
     if (cnt > 0) {
-      const float* Pc = sm + (cur ? oP1 : oP0) + x;
-      const float* Qc = sm + (cur ? oQ1 : oQ0) + 4 * W + x;  // row = owned row, -4 .. nr+3
-      float* Pn = sm + (nxt ? oP1 : oP0) + x;
-      float* Qn = sm + (nxt ? oQ1 : oQ0) + 4 * W + x;
-      const float* Tr = sm + oT + x;
-      const float* Cr = sm + oM13 + x;
-      const uint32_t up = up0 + (nxt ? qslot : 0u) + 4u * (uint32_t)x;
-      const uint32_t dn = dn0 + (nxt ? qslot : 0u) + 4u * (uint32_t)x;
-      float2 qz[9];
-#pragma unroll
-      for (int k = 0; k < 8; ++k)
-        qz[k + 1] = *reinterpret_cast<const float2*>(Qc + (r0 - 4 + k) * W);
-#pragma unroll
-      for (int j = 0; j < kResRows; ++j) {
-        if (j < cnt) {
-          const int lr = r0 + j;
-#pragma unroll
-          for (int k = 0; k < 8; ++k) qz[k] = qz[k + 1];
-          qz[8] = *reinterpret_cast<const float2*>(Qc + (lr + 4) * W);
-          const float* pr = Pc + lr * W;
-          float v[10];
-#pragma unroll
-          for (int k = 0; k < 5; ++k) {
-            const float2 u = *reinterpret_cast<const float2*>(pr - 4 + 2 * k);
-            v[2 * k] = u.x;
-            v[2 * k + 1] = u.y;
-          }
-          const int o = lr * W;
-          const float2 pp = *reinterpret_cast<const float2*>(Pn + o);
-          const float2 qp = *reinterpret_cast<const float2*>(Qn + o);
-          const float2 tt = *reinterpret_cast<const float2*>(Tr + o);
-          const float2 cc = *reinterpret_cast<const float2*>(Cr + o);
-          float pn[2], qn[2];
-#pragma unroll
-          for (int e = 0; e < 2; ++e) {
-            auto pick = [e](float2 w) { return e ? w.y : w.x; };
-            const float* r = v + 4 + e;
-            float tp = kC0 * r[0];
-            tp = fmaf(kC1, r[-1] + r[1], tp);
-            tp = fmaf(kC2, r[-2] + r[2], tp);
-            tp = fmaf(kC3, r[-3] + r[3], tp);
-            tp = fmaf(kC4, r[-4] + r[4], tp);
-            float tq = kC0 * pick(qz[4]);
-            tq = fmaf(kC1, pick(qz[3]) + pick(qz[5]), tq);
-            tq = fmaf(kC2, pick(qz[2]) + pick(qz[6]), tq);
-            tq = fmaf(kC3, pick(qz[1]) + pick(qz[7]), tq);
-            tq = fmaf(kC4, pick(qz[0]) + pick(qz[8]), tq);
-            tp *= a.idx2;
-            tq *= a.idz2;
-            const float tj = pick(tt), c13 = pick(cc);
-            float a_ = fmaf(a.dt2, fmaf(pick(m11[j]), tp, c13 * tq), 2.f * r[0] - tj * pick(pp));
-            float b_ =
-                fmaf(a.dt2, fmaf(c13, tp, pick(m33[j]) * tq), 2.f * pick(qz[4]) - tj * pick(qp));
-            if (src_mine && src_e == e && zr0 + lr == a.src_z) {
-              a_ += amp;
-              b_ += amp;
-            }
-            pn[e] = tj * a_;
-            qn[e] = tj * b_;
-          }
-          const float2 q2 = make_float2(qn[0], qn[1]);
-          // halo rows of the neighbours: my first 4 rows are the bottom halo
-          // of rank - 1 (which owns R rows), my last 4 the top halo of rank + 1
-          const bool to_up = lr < 4 && rank > 0;
-          const bool to_dn = lr >= nr - 4 && rank + 1 < ncta;
-          if (two) {
-            *reinterpret_cast<float2*>(Pn + o) = make_float2(pn[0], pn[1]);
-            *reinterpret_cast<float2*>(Qn + o) = q2;
-            if (to_up) st_cluster2(up + 4u * (uint32_t)((R + 4 + lr) * W), q2);
-            if (to_dn) st_cluster2(dn + 4u * (uint32_t)((lr - nr + 4) * W), q2);
-          } else {
-            Pn[o] = pn[0];
-            Qn[o] = qn[0];
-            if (to_up) st_cluster(up + 4u * (uint32_t)((R + 4 + lr) * W), qn[0]);
-            if (to_dn) st_cluster(dn + 4u * (uint32_t)((lr - nr + 4) * W), qn[0]);
-          }
-        }
-      }
+      ResRows rr;
+      rr.Pc = sm + (cur ? oP1 : oP0) + x;
+      rr.Qc = sm + (cur ? oQ1 : oQ0) + 4 * W + x;  // row = owned row, -4 .. nr+3
+      rr.Pn = sm + (nxt ? oP1 : oP0) + x;
+      rr.Qn = sm + (nxt ? oQ1 : oQ0) + 4 * W + x;
+      rr.Tr = sm + oT + x;
+      rr.Cr = sm + oM13 + x;
+      rr.up = up0 + (nxt ? qslot : 0u) + 4u * (uint32_t)x;
+      rr.dn = dn0 + (nxt ? qslot : 0u) + 4u * (uint32_t)x;
+      rr.W = W;
+      rr.r0 = r0;
+      rr.cnt = cnt;
+      rr.nr = nr;
+      rr.R = R;
+      rr.to_up = rank > 0;
+      rr.to_dn = rank + 1 < ncta;
+      rr.two = two;
+      rr.src_row = src_row;
+      rr.src_e = src_e;
+      rr.amp = amp;
+      // threads with a full segment run the rows without per-row guards
+      if (cnt == kResRows)
+        res_rows<true>(a, rr, m11, m33);
+      else
+        res_rows<false>(a, rr, m11, m33);
     }
     cl.sync();
     const int row = __ldg(a.rec_row + it);
