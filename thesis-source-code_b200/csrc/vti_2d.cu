@@ -19,6 +19,7 @@
 #include <cooperative_groups.h>
 
 #include "vti_internal.h"
+#include "vti_pair.cuh"
 
 namespace vti {
 namespace {
@@ -43,6 +44,26 @@ struct Step2d {
   int src;        // flat index of the source
   const float* amp;  // device pointer to the source amplitude of this step
 };
+
+// The operation sequence of one 2D update, written with explicit rounding
+// (no contraction by the compiler), so that the per-level kernel and the
+// resident kernel (scalar or packed pairs) compute bitwise the same values:
+// lap = C0 c + C1 (m1 + p1) + ... (forwardCD, kernels.cu:452-498),
+// next = dt2 (ca * lap_h * idx2 + cb * lap_v * idz2) + (2 cur - taper prev).
+__device__ __forceinline__ float lap2d(float c, float m1, float p1, float m2, float p2, float m3,
+                                       float p3, float m4, float p4) {
+  float s = __fmul_rn(kC0, c);
+  s = __fmaf_rn(kC1, __fadd_rn(m1, p1), s);
+  s = __fmaf_rn(kC2, __fadd_rn(m2, p2), s);
+  s = __fmaf_rn(kC3, __fadd_rn(m3, p3), s);
+  s = __fmaf_rn(kC4, __fadd_rn(m4, p4), s);
+  return s;
+}
+__device__ __forceinline__ float update2d(float dt2, float ca, float cb, float tp, float tq,
+                                          float cur, float t, float prev) {
+  return __fmaf_rn(dt2, __fmaf_rn(ca, tp, __fmul_rn(cb, tq)),
+                   __fsub_rn(__fmul_rn(2.f, cur), __fmul_rn(t, prev)));
+}
 
 // Launched as a programmatic dependent launch: the model and taper (fixed for
 // the whole run) are read before griddepcontrol.wait, which returns once the
@@ -88,27 +109,21 @@ __global__ void __launch_bounds__(BX* BZ) k_step2d(Step2d a) {
   __syncthreads();
   if (!valid) return;
   const float* r = &sp[tz][tx + 4];
-  float tp = kC0 * r[0];
-  tp = fmaf(kC1, r[-1] + r[1], tp);
-  tp = fmaf(kC2, r[-2] + r[2], tp);
-  tp = fmaf(kC3, r[-3] + r[3], tp);
-  tp = fmaf(kC4, r[-4] + r[4], tp);
-  float tq = kC0 * sq[tz + 4][tx];
-  tq = fmaf(kC1, sq[tz + 3][tx] + sq[tz + 5][tx], tq);
-  tq = fmaf(kC2, sq[tz + 2][tx] + sq[tz + 6][tx], tq);
-  tq = fmaf(kC3, sq[tz + 1][tx] + sq[tz + 7][tx], tq);
-  tq = fmaf(kC4, sq[tz][tx] + sq[tz + 8][tx], tq);
-  tp *= a.idx2;
-  tq *= a.idz2;
-  float pn = fmaf(a.dt2, fmaf(c11, tp, c13 * tq), 2.f * r[0] - t * p0);
-  float qn = fmaf(a.dt2, fmaf(c13, tp, c33 * tq), 2.f * sq[tz + 4][tx] - t * q0);
+  const float tp = __fmul_rn(lap2d(r[0], r[-1], r[1], r[-2], r[2], r[-3], r[3], r[-4], r[4]),
+                             a.idx2);
+  const float tq = __fmul_rn(lap2d(sq[tz + 4][tx], sq[tz + 3][tx], sq[tz + 5][tx],
+                                   sq[tz + 2][tx], sq[tz + 6][tx], sq[tz + 1][tx],
+                                   sq[tz + 7][tx], sq[tz][tx], sq[tz + 8][tx]),
+                             a.idz2);
+  float pn = update2d(a.dt2, c11, c13, tp, tq, r[0], t, p0);
+  float qn = update2d(a.dt2, c13, c33, tp, tq, sq[tz + 4][tx], t, q0);
   if (i == a.src) {
     const float s = *a.amp;
-    pn += s;
-    qn += s;
+    pn = __fadd_rn(pn, s);
+    qn = __fadd_rn(qn, s);
   }
-  a.p0[i] = t * pn;
-  a.q0[i] = t * qn;
+  a.p0[i] = __fmul_rn(t, pn);
+  a.q0[i] = __fmul_rn(t, qn);
 }
 
 // recordData (kernels.cu:317-324): 0.5(p+q) at receivers into row `row`.
@@ -237,35 +252,33 @@ __device__ __forceinline__ void res_rows(const Res2d& a, const ResRows& rr,
       const float2 qp = *reinterpret_cast<const float2*>(rr.Qn + o);
       const float2 tt = *reinterpret_cast<const float2*>(rr.Tr + o);
       const float2 cc = *reinterpret_cast<const float2*>(rr.Cr + o);
-      float pn[2], qn[2];
-#pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        auto pick = [e](float2 w) { return e ? w.y : w.x; };
-        const float* r = v + 4 + e;
-        float tp = kC0 * r[0];
-        tp = fmaf(kC1, r[-1] + r[1], tp);
-        tp = fmaf(kC2, r[-2] + r[2], tp);
-        tp = fmaf(kC3, r[-3] + r[3], tp);
-        tp = fmaf(kC4, r[-4] + r[4], tp);
-        float tq = kC0 * pick(qz[4]);
-        tq = fmaf(kC1, pick(qz[3]) + pick(qz[5]), tq);
-        tq = fmaf(kC2, pick(qz[2]) + pick(qz[6]), tq);
-        tq = fmaf(kC3, pick(qz[1]) + pick(qz[7]), tq);
-        tq = fmaf(kC4, pick(qz[0]) + pick(qz[8]), tq);
-        tp *= a.idx2;
-        tq *= a.idz2;
-        const float tj = pick(tt), c13 = pick(cc);
-        float a_ = fmaf(a.dt2, fmaf(pick(m11[j]), tp, c13 * tq), 2.f * r[0] - tj * pick(pp));
-        float b_ =
-            fmaf(a.dt2, fmaf(c13, tp, pick(m33[j]) * tq), 2.f * pick(qz[4]) - tj * pick(qp));
-        if (lr == rr.src_row && e == rr.src_e) {
-          a_ += rr.amp;
-          b_ += rr.amp;
+      // the sequence of lap2d / update2d on packed pairs; the x stencil per
+      // lane (its neighbour pairs straddle the loaded float2s)
+      float2 tp2 = make_float2(lap2d(v[4], v[3], v[5], v[2], v[6], v[1], v[7], v[0], v[8]),
+                               lap2d(v[5], v[4], v[6], v[3], v[7], v[2], v[8], v[1], v[9]));
+      float2 tq2 = mul2(splat(kC0), qz[4]);
+      tq2 = fma2(splat(kC1), add2(qz[3], qz[5]), tq2);
+      tq2 = fma2(splat(kC2), add2(qz[2], qz[6]), tq2);
+      tq2 = fma2(splat(kC3), add2(qz[1], qz[7]), tq2);
+      tq2 = fma2(splat(kC4), add2(qz[0], qz[8]), tq2);
+      tp2 = mul2(tp2, splat(a.idx2));
+      tq2 = mul2(tq2, splat(a.idz2));
+      const float2 dt2 = splat(a.dt2), two = splat(2.f);
+      float2 a2 = fma2(dt2, fma2(m11[j], tp2, mul2(cc, tq2)),
+                       sub2(mul2(two, make_float2(v[4], v[5])), mul2(tt, pp)));
+      float2 b2 = fma2(dt2, fma2(cc, tp2, mul2(m33[j], tq2)), sub2(mul2(two, qz[4]), mul2(tt, qp)));
+      if (lr == rr.src_row) {
+        if (rr.src_e == 0) {
+          a2.x = __fadd_rn(a2.x, rr.amp);
+          b2.x = __fadd_rn(b2.x, rr.amp);
+        } else {
+          a2.y = __fadd_rn(a2.y, rr.amp);
+          b2.y = __fadd_rn(b2.y, rr.amp);
         }
-        pn[e] = tj * a_;
-        qn[e] = tj * b_;
       }
-      const float2 q2 = make_float2(qn[0], qn[1]);
+      const float2 p2 = mul2(tt, a2);
+      const float2 q2 = mul2(tt, b2);
+      const float pn[2] = {p2.x, p2.y}, qn[2] = {q2.x, q2.y};
       // halo rows of the neighbours: my first 4 rows are the bottom halo of
       // rank - 1 (which owns R rows), my last 4 the top halo of rank + 1
       const bool to_up = rr.to_up && lr < 4;
