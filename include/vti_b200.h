@@ -100,9 +100,9 @@ uint64_t vti_ctx_kernel_launches(const vti_ctx* ctx);
 int vti_ctx_set_timing(vti_ctx* ctx, int enable);
 /* 2D traces (vti2d_synthetic) of a grid whose state fits the shared memory of
  * one thread-block cluster (up to 16 CTAs; (nnx-8) <= 1024 columns, e.g.
- * 461 x 261) run as one launch per shot with the wavefields resident on chip;
- * results are those of the per-step path. enable = 0 forces the per-step path
- * (default 1). */
+ * 461 x 261) run with the wavefields resident on chip, one cluster per shot
+ * (shots with disjoint receiver ranges in one launch); results are those of
+ * the per-step path. enable = 0 forces the per-step path (default 1). */
 int vti_ctx_set_2d_resident(vti_ctx* ctx, int enable);
 int vti_ctx_kernel_time(vti_ctx* ctx, const char* kernel, double* total_ms, uint64_t* count);
 

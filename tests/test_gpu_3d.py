@@ -163,6 +163,39 @@ def test_one_call_forms_keep_no_state_between_calls(ctx):
         np.testing.assert_array_equal(b, r)
 
 
+def test_one_call_plan_follows_the_geometry(ctx):
+    """A one-call form with another geometry (or flags) replaces the kept
+    plan; going back to the first geometry gives its results again."""
+    def case(nt):
+        s = S.small3d(nx=40, ny=36, nz=28, nt=nt, npad=6, rec_step=3, rate=2.1e-3)
+        true = S.small3d(nx=40, ny=36, nz=28, nt=nt, npad=6, seed=11)
+        return s, true
+
+    def run(s, true, flags):
+        n = s.nxyz
+        g = s.geom()
+        padb, randb = S.boundaries3d(s)
+        d = V.modelDataCij3d_f(ctx, g, s.souloc, [0], s.recloc, s.wavelet,
+                               *_split(true.cij(), n), flags=flags)
+        fg, mis = V.objFuncGradientCij3d_f(ctx, g, s.souloc, [0], s.recloc, s.wavelet, s.cij(),
+                                           padb, randb, d, flags=flags)
+        return d, fg, mis
+
+    a, b = case(110), case(90)
+    seq = [(a, 0), (b, 0), (a, V.OPT_FULL_STEPS), (a, 0)]
+    kept = [run(*c, f) for c, f in seq]
+    ctx.set_plan_cache(False)
+    try:
+        fresh = [run(*c, f) for c, f in seq]
+    finally:
+        ctx.set_plan_cache(True)
+    for k, r in zip(kept, fresh):
+        assert np.abs(r[0]).max() > 0 and r[2] > 0
+        for u, v in zip(k, r):
+            np.testing.assert_array_equal(u, v)
+    np.testing.assert_array_equal(kept[0][1], kept[3][1])
+
+
 def test_zero_residual_gives_zero_gradient(ctx):
     """Observed data modeled by the library itself: residual and gradient are 0."""
     s = S.small3d(nx=72, ny=64, nz=48, nt=130, npad=8, rec_step=2)

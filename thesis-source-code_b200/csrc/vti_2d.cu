@@ -172,14 +172,14 @@ struct Res2d {
   const float* c33;
   const float* taper;
   float idx2, idz2, dt2;
-  int src_x, src_z;
   float init_value;     // dt2 * wavelet[0], level 1 at the source before the taper
   const float* amp;     // amp[it]: source term of level it
   const int* rec_row;   // trace row recorded at level it, -1 none
-  const int* rx;        // receiver columns and rows
+  const int* shots;     // per shot (cluster): source x, source z, first receiver, receivers
+  const int* rx;        // receiver columns and rows (all receivers of the survey)
   const int* rz;
-  int nri;
-  float* data;          // rows x nri
+  int nr_total;
+  float* data;          // rows x nr_total, receiver-fastest
 };
 
 // 32-bit shared::cluster address of `p` (this CTA's shared memory) in the
@@ -198,13 +198,20 @@ __device__ __forceinline__ void st_cluster2(uint32_t addr, float2 v) {
                : "memory");
 }
 
+// Receivers of this shot in the CTA's rows: 0.5 (p + q) into trace row
+// `row` (recordData, kernels.cu:317-324); the CTA owning row 4 also writes 0
+// for receivers outside the update region (never updated, so 0 there), so
+// every receiver of the shot is written in every recorded row.
 __device__ __forceinline__ void res_record(const Res2d& a, int row, const float* p, const float* q,
-                                           int zr0, int nr) {
-  for (int ir = threadIdx.x; ir < a.nri; ir += blockDim.x) {
-    const int x = __ldg(a.rx + ir), lz = __ldg(a.rz + ir) - zr0;
-    // cells outside the update region stay 0, as the zeroed trace rows
-    if (lz >= 0 && lz < nr && x >= kHalo && x < a.nnx - kHalo)
-      a.data[(long long)row * a.nri + ir] = 0.5f * (p[lz * a.W + x] + q[(lz + 4) * a.W + x]);
+                                           int zr0, int nr, int ir0, int nri) {
+  for (int ir = threadIdx.x; ir < nri; ir += blockDim.x) {
+    const int x = __ldg(a.rx + ir0 + ir), z = __ldg(a.rz + ir0 + ir), lz = z - zr0;
+    const bool inside = x >= kHalo && x < a.nnx - kHalo && z >= kHalo && z < a.nnz - kHalo;
+    float* d = a.data + (long long)row * a.nr_total + ir0 + ir;
+    if (inside && lz >= 0 && lz < nr)
+      *d = 0.5f * (p[lz * a.W + x] + q[(lz + 4) * a.W + x]);
+    else if (!inside && zr0 == kHalo)
+      *d = 0.f;
   }
 }
 
@@ -308,6 +315,10 @@ __global__ void __launch_bounds__(kResThreads, 1)
   const int rank = (int)cl.block_rank();
   const int ncta = (int)cl.num_blocks();
   const int nnx = a.nnx, W = a.W;
+  // this cluster's shot
+  const int shot = blockIdx.x / ncta;
+  const int src_x = __ldg(a.shots + 4 * shot), src_z = __ldg(a.shots + 4 * shot + 1);
+  const int ir0 = __ldg(a.shots + 4 * shot + 2), nri = __ldg(a.shots + 4 * shot + 3);
   const int R = a.rows_per_cta;
   const int zr0 = kHalo + rank * R;
   const int nr = min(R, a.nnz - 2 * kHalo - rank * R);
@@ -324,10 +335,10 @@ __global__ void __launch_bounds__(kResThreads, 1)
   // level 1 (slot 1): the source after the taper (synthetic_f.cu:86-89); every
   // CTA writes its own copy, halo rows included
   if (threadIdx.x == 0) {
-    const float v = a.init_value * __ldg(a.taper + a.src_x + a.src_z * nnx);
-    const int lz = a.src_z - zr0;
-    if (lz >= 0 && lz < nr) sm[oP1 + lz * W + a.src_x] = v;
-    if (lz >= -4 && lz < nr + 4) sm[oQ1 + (lz + 4) * W + a.src_x] = v;
+    const float v = a.init_value * __ldg(a.taper + src_x + src_z * nnx);
+    const int lz = src_z - zr0;
+    if (lz >= 0 && lz < nr) sm[oP1 + lz * W + src_x] = v;
+    if (lz >= -4 && lz < nr + 4) sm[oQ1 + (lz + 4) * W + src_x] = v;
   }
   // this thread's column pair and rows
   const int NP = (nnx - 2 * kHalo + 1) / 2;
@@ -338,10 +349,10 @@ __global__ void __launch_bounds__(kResThreads, 1)
   const bool two = x + 1 < nnx - kHalo;  // the second column is updated
   const int r0 = seg * a.seg_rows;
   const int cnt = active ? max(0, min(a.seg_rows, nr - r0)) : 0;
-  const int src_e = a.src_x - x;  // 0 or 1 when the source is in this thread's columns
+  const int src_e = src_x - x;  // 0 or 1 when the source is in this thread's columns
   const bool src_mine = cnt > 0 && (src_e == 0 || (src_e == 1 && two)) &&
-                        a.src_z >= zr0 + r0 && a.src_z < zr0 + r0 + cnt;
-  const int src_row = src_mine ? a.src_z - zr0 : -1;  // owned row of the source
+                        src_z >= zr0 + r0 && src_z < zr0 + r0 + cnt;
+  const int src_row = src_mine ? src_z - zr0 : -1;  // owned row of the source
   // c11 and c33 of the thread's rows
   float2 m11[kResRows], m33[kResRows];
 #pragma unroll
@@ -359,7 +370,7 @@ __global__ void __launch_bounds__(kResThreads, 1)
   // every CTA of the cluster is running and initialised before any remote store
   cl.sync();
   if (a.nt > 1 && __ldg(a.rec_row + 1) >= 0)
-    res_record(a, __ldg(a.rec_row + 1), sm + oP1, sm + oQ1, zr0, nr);
+    res_record(a, __ldg(a.rec_row + 1), sm + oP1, sm + oQ1, zr0, nr, ir0, nri);
   int cur = 1;
   float amp_next = a.nt > 2 ? __ldg(a.amp + 2) : 0.f;
   for (int it = 2; it < a.nt; ++it) {
@@ -396,7 +407,7 @@ __global__ void __launch_bounds__(kResThreads, 1)
     cl.sync();
     const int row = __ldg(a.rec_row + it);
     if (row >= 0)
-      res_record(a, row, sm + (nxt ? oP1 : oP0), sm + (nxt ? oQ1 : oQ0), zr0, nr);
+      res_record(a, row, sm + (nxt ? oP1 : oP0), sm + (nxt ? oQ1 : oQ0), zr0, nr, ir0, nri);
     cur = nxt;
   }
   // no CTA leaves while a neighbour may still read its memory
@@ -483,9 +494,12 @@ bool resident_shape(vti_ctx* ctx, int nnx, int nnz, ResShape* out) {
   return false;
 }
 
-cudaError_t launch_resident(const ResShape& sh, const Res2d& a, cudaStream_t stream) {
+// One cluster of sh.ctas CTAs per shot; clusters that do not fit at once run
+// as earlier ones finish (no cluster waits for another).
+cudaError_t launch_resident(const ResShape& sh, const Res2d& a, int nshots,
+                            cudaStream_t stream) {
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(sh.ctas);
+  cfg.gridDim = dim3(sh.ctas * nshots);
   cfg.blockDim = dim3(kResThreads);
   cfg.dynamicSmemBytes = sh.smem;
   cfg.stream = stream;
@@ -505,6 +519,12 @@ cudaError_t launch_resident(const ResShape& sh, const Res2d& a, cudaStream_t str
 using namespace vti;
 
 namespace {
+
+#define VTI_TRY_RES(call)            \
+  do {                               \
+    const int st_ = (call);          \
+    if (st_ != VTI_OK) return st_;   \
+  } while (0)
 
 // The context's 2D scratch, grown (never shrunk) to `bytes`; freed with the
 // context.
@@ -598,38 +618,6 @@ int run2d(vti_ctx* ctx, const vti2d_geom* g, const float* c11, const float* c13,
     }
     CK(cudaMemsetAsync(d_data, 0, (size_t)nrows_out * nri * sizeof(float), ctx->stream));
   }
-  // Traces of a grid that fits one thread-block cluster: one launch runs all
-  // levels with the state in shared memory (k_synth2d_resident). The source
-  // must lie in the update region (a source outside it keeps its level-1
-  // value in one buffer only, which the per-step path below reproduces).
-  const int src_x = slocxz % nnx, src_z = slocxz / nnx;
-  ResShape shape;
-  if (mode == 0 && ctx->resident2d && src_x >= kHalo && src_x < nnx - kHalo && src_z >= kHalo &&
-      src_z < nnz - kHalo && resident_shape(ctx, nnx, nnz, &shape)) {
-    std::vector<int> hi(rec_row);
-    hi.resize(g->nt + 2 * (size_t)nri);
-    for (int ir = 0; ir < nri; ++ir) {
-      hi[g->nt + ir] = ridx[ir] % nnx;
-      hi[g->nt + nri + ir] = ridx[ir] / nnx;
-    }
-    CK(cudaMemcpyAsync(d_ints, hi.data(), hi.size() * sizeof(int), cudaMemcpyHostToDevice,
-                       ctx->stream));
-    Res2d a{nnx, nnz, g->nt, shape.W, shape.rows, shape.seg_rows, shape.segs, dc11, dc13, dc33, dtap,
-            1.f / dx2, 1.f / dz2, dt2, src_x, src_z, dt2 * wavelet[0], amps, d_ints,
-            d_ints + g->nt, d_ints + g->nt + nri, nri, d_data};
-    {
-      LaunchTimer tm(ctx, kTimedStep2d);
-      CK(launch_resident(shape, a, ctx->stream));
-    }
-    ctx->launches++;
-    CK(cudaGetLastError());
-    if (nri > 0)
-      CK(cudaMemcpy2DAsync(out + ir0, (size_t)nr_total * 4, d_data, (size_t)nri * 4,
-                           (size_t)nri * 4, nrows_out, cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    cleanup();
-    return VTI_OK;
-  }
   if (nrec > 0)
     CK(cudaMemcpyAsync(d_ridx, ridx.data(), nri * sizeof(int), cudaMemcpyHostToDevice,
                        ctx->stream));
@@ -710,6 +698,115 @@ int run2d(vti_ctx* ctx, const vti2d_geom* g, const float* c11, const float* c13,
   return VTI_OK;
 }
 
+// Traces of all shots of a grid that fits one thread-block cluster
+// (resident_shape) with every source in the update region: the model is
+// uploaded once and each shot runs in its own cluster of k_synth2d_resident
+// (all levels in shared memory). Shots whose receiver ranges are disjoint
+// share one launch; otherwise one launch per shot, in shot order, so a later
+// shot overwrites the receivers it shares with an earlier one (the per-shot
+// order of synthetic_f.cu:31-124). VTI_ERR_UNSUPPORTED: not eligible, the
+// caller runs the per-level path (nothing was computed).
+int synth2d_resident(vti_ctx* ctx, const vti2d_geom* g, const float* c11, const float* c13,
+                     const float* c33, const float* wavelet, const int* sloc, int ns,
+                     const int* rloc, int nr_total, const float* taper, float* out) {
+  if (!ctx->resident2d || ns < 1) return VTI_ERR_UNSUPPORTED;
+  const int nnx = g->nx + 2 * g->npad, nnz = g->nz + 2 * g->npad;
+  const long long nnxz = (long long)nnx * nnz;
+  if (nnx < 9 || nnz < 9 || g->nt < 2 || !(g->dt > 0) || !(g->rate > 0))
+    return VTI_ERR_UNSUPPORTED;
+  for (int is = 0; is < ns; ++is) {
+    const int* sh = sloc + 4 * is;
+    if (sh[0] < kHalo || sh[0] >= nnx - kHalo || sh[1] < kHalo || sh[1] >= nnz - kHalo)
+      return VTI_ERR_UNSUPPORTED;
+  }
+  const float dt = g->dt, dt2 = dt * dt;
+  const int ratio = (int)(g->rate / dt + 0.5f);
+  if (ratio < 1) return VTI_ERR_UNSUPPORTED;
+  VTI_CUDA(ctx, cudaSetDevice(ctx->device));
+  ResShape shape;
+  if (!resident_shape(ctx, nnx, nnz, &shape)) return VTI_ERR_UNSUPPORTED;
+  for (int ir = 0; ir < nr_total; ++ir) {
+    const int x = rloc[2 * ir], z = rloc[2 * ir + 1];
+    if (x < 0 || x >= nnx || z < 0 || z >= nnz)
+      return fail(ctx, VTI_ERR_ARG, "2D receiver outside the grid");
+  }
+  const int ntNeg = (int)std::round(std::fabs(g->ot) / dt);
+  // trace row taken at each level, -1 none (the arithmetic of run2d)
+  std::vector<int> hi(g->nt, -1);
+  if (ratio == 1 && g->ot == 0.f) hi[1] = 1;
+  for (int it = 2; it < g->nt; ++it) {
+    float t = it * dt + g->ot;
+    if (t >= 0.f && (it - ntNeg) % ratio == 0) hi[it] = (it - ntNeg) / ratio;
+  }
+  const long long nrows = (g->nt - ntNeg - 1) / ratio + 1;
+  // ints: trace rows, per-shot table, receiver columns, receiver rows
+  for (int is = 0; is < ns; ++is) {
+    const int* sh = sloc + 4 * is;
+    hi.push_back(sh[0]);
+    hi.push_back(sh[1]);
+    hi.push_back(sh[3]);
+    hi.push_back(sh[2]);
+  }
+  for (int ir = 0; ir < nr_total; ++ir) hi.push_back(rloc[2 * ir]);
+  for (int ir = 0; ir < nr_total; ++ir) hi.push_back(rloc[2 * ir + 1]);
+  const size_t nf = 4 * (size_t)nnxz + g->nt;
+  const size_t n_data = (size_t)nrows * nr_total;
+  float* buf = nullptr;
+  VTI_TRY_RES(scratch2d(ctx, (nf + hi.size() + n_data) * sizeof(float), &buf));
+  float *dc11 = buf, *dc13 = dc11 + nnxz, *dc33 = dc13 + nnxz, *dtap = dc33 + nnxz;
+  float* amps = dtap + nnxz;
+  int* d_ints = reinterpret_cast<int*>(buf + nf);
+  float* d_data = buf + nf + hi.size();
+  cudaStream_t s = ctx->stream;
+  VTI_CUDA(ctx, cudaMemcpyAsync(dc11, c11, nnxz * 4, cudaMemcpyHostToDevice, s));
+  VTI_CUDA(ctx, cudaMemcpyAsync(dc13, c13, nnxz * 4, cudaMemcpyHostToDevice, s));
+  VTI_CUDA(ctx, cudaMemcpyAsync(dc33, c33, nnxz * 4, cudaMemcpyHostToDevice, s));
+  VTI_CUDA(ctx, cudaMemcpyAsync(dtap, taper, nnxz * 4, cudaMemcpyHostToDevice, s));
+  std::vector<float> h_amp(g->nt, 0.f);
+  for (int it = 2; it < g->nt; ++it) h_amp[it] = dt2 * wavelet[it - 1];
+  VTI_CUDA(ctx, cudaMemcpyAsync(amps, h_amp.data(), g->nt * 4, cudaMemcpyHostToDevice, s));
+  VTI_CUDA(ctx, cudaMemcpyAsync(d_ints, hi.data(), hi.size() * sizeof(int),
+                                cudaMemcpyHostToDevice, s));
+  if (n_data) VTI_CUDA(ctx, cudaMemsetAsync(d_data, 0, n_data * sizeof(float), s));
+  // receiver ranges pairwise disjoint?
+  std::vector<std::pair<int, int>> rng;
+  for (int is = 0; is < ns; ++is)
+    if (sloc[4 * is + 2] > 0) rng.push_back({sloc[4 * is + 3], sloc[4 * is + 3] + sloc[4 * is + 2]});
+  std::sort(rng.begin(), rng.end());
+  bool disjoint = true;
+  for (size_t k = 1; k < rng.size(); ++k)
+    if (rng[k].first < rng[k - 1].second) disjoint = false;
+  const float dx2 = g->dx * g->dx, dz2 = g->dz * g->dz;
+  Res2d a{nnx, nnz, g->nt, shape.W, shape.rows, shape.seg_rows, shape.segs, dc11, dc13, dc33,
+          dtap, 1.f / dx2, 1.f / dz2, dt2, dt2 * wavelet[0], amps, d_ints, d_ints + g->nt,
+          d_ints + g->nt + 4 * ns, d_ints + g->nt + 4 * ns + nr_total, nr_total, d_data};
+  {
+    LaunchTimer tm(ctx, kTimedStep2d);
+    if (disjoint) {
+      VTI_CUDA(ctx, launch_resident(shape, a, ns, s));
+      ctx->launches++;
+    } else {
+      for (int is = 0; is < ns; ++is) {
+        Res2d b = a;
+        b.shots = a.shots + 4 * is;
+        VTI_CUDA(ctx, launch_resident(shape, b, 1, s));
+        ctx->launches++;
+      }
+    }
+  }
+  VTI_CUDA(ctx, cudaGetLastError());
+  // each shot's receiver columns into the caller's receiver-fastest rows
+  for (int is = 0; is < ns; ++is) {
+    const int nri = sloc[4 * is + 2], ir0 = sloc[4 * is + 3];
+    if (nri > 0)
+      VTI_CUDA(ctx, cudaMemcpy2DAsync(out + ir0, (size_t)nr_total * 4, d_data + ir0,
+                                      (size_t)nr_total * 4, (size_t)nri * 4, nrows,
+                                      cudaMemcpyDeviceToHost, s));
+  }
+  VTI_CUDA(ctx, cudaStreamSynchronize(s));
+  return VTI_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -723,6 +820,13 @@ int vti2d_synthetic(vti_ctx* ctx, const vti2d_geom* g, const float* c11, const f
     const int* s = sloc + 4 * is;
     if (s[2] < 0 || s[3] < 0 || s[3] + s[2] > nr)
       return fail(ctx, VTI_ERR_ARG, "2D shot receiver range exceeds rloc");
+  }
+  if (!c11 || !c13 || !c33 || !wavelet || !taper || !data) return VTI_ERR_ARG;
+  const int rst = synth2d_resident(ctx, g, c11, c13, c33, wavelet, sloc, ns, rloc, nr, taper,
+                                   data);
+  if (rst != VTI_ERR_UNSUPPORTED) return rst;
+  for (int is = 0; is < ns; ++is) {
+    const int* s = sloc + 4 * is;
     int st = run2d(ctx, g, c11, c13, c33, wavelet, taper, s[0] + s[1] * nnx, rloc, s[2], nr, s[3],
                    data, 0);
     if (st != VTI_OK) return st;
