@@ -146,7 +146,8 @@ __global__ void k_init2d(float* p, float* q, int src, float value, float taper_a
 
 // ---------------------------------------------------------------- resident
 // The whole 2D state of one shot held in the shared memory of one thread-block
-// cluster for all time steps (one launch per shot). CTA r of the cluster owns
+// cluster for all time steps (one cluster per shot, blockIdx.x / cluster size
+// picks the shot; any number of shots per launch). CTA r of the cluster owns
 // update rows z in [4 + r*R, 4 + r*R + nr) and keeps, in rows of W floats
 // (W = nnx rounded up to even), p at two levels (R rows each), q at two
 // levels with 4 halo rows above and below (R + 8 rows each), and the taper
@@ -158,7 +159,9 @@ __global__ void k_init2d(float* p, float* q, int src, float value, float taper_a
 // blockDim / NP segments) owns the columns x0 = 4 + 2*(t % NP) and x0 + 1
 // (when x0 + 1 < nnx - 4) over up to kResRows consecutive rows of its CTA:
 // 64-bit shared loads serve both columns, c11 and c33 stay in registers, q's z
-// stencil runs as a register queue.
+// stencil runs as a register queue, and the arithmetic of the two columns
+// runs on packed FP32 pairs (except the x stencil, whose neighbour pairs
+// straddle the loaded float2s).
 constexpr int kResThreads = 512, kResRows = 8, kResMaxCluster = 16;
 
 struct Res2d {
