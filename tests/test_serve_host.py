@@ -58,7 +58,8 @@ def test_lbfgs_driver_converges_on_a_quadratic():
     xs = rng.standard_normal(n) + 5.0
     x0 = np.full(n, 5.0, dtype=np.float32)
     shots = [None] * 3
-    drv = _Quadratic(None, x0, None, shots, iterations=25, step0=0.5, max_step=1.0)
+    drv = _Quadratic(None, x0, None, shots, iterations=25, step0=0.5, max_step=1.0,
+                     project_stiffness=False)
     jobs = drv.first()
     while jobs is not None:
         jobs = drv.update([_evaluate(j, A, xs, len(shots)) for j in jobs])
@@ -72,7 +73,8 @@ def test_lbfgs_step_is_capped_and_nonfinite_trials_are_rejected():
     A = np.eye(n)
     xs = np.full(n, 100.0)
     x0 = np.ones(n, dtype=np.float32)
-    drv = _Quadratic(None, x0, None, [None], iterations=2, step0=1000.0, max_step=0.02)
+    drv = _Quadratic(None, x0, None, [None], iterations=2, step0=1000.0, max_step=0.02,
+                     project_stiffness=False)
     jobs = drv.first()
     jobs = drv.update([_evaluate(j, A, xs, 1) for j in jobs])
     step = jobs[0] - x0
@@ -82,6 +84,38 @@ def test_lbfgs_step_is_capped_and_nonfinite_trials_are_rejected():
     nxt = drv.update([(np.zeros(n, dtype=np.float32), float("nan"))])
     assert drv.misfits[-1] == drv.misfits[0] and len(drv.misfits) == 1
     assert np.allclose(nxt[0] - drv.x, 0.5 * (before - drv.x))
+
+
+def test_lbfgs_never_accepts_an_increase():
+    """Trials that all raise the misfit: after max_halvings the driver keeps
+    the model (the misfit history repeats, never rises) and restarts from
+    steepest descent with a shorter step."""
+    n = 6
+    x0 = np.ones(n, dtype=np.float32)
+    drv = _Quadratic(None, x0, None, [None], iterations=3, step0=0.5, max_step=0.1,
+                     project_stiffness=False)
+    jobs = drv.first()
+    jobs = drv.update([(np.ones(n, dtype=np.float32), 1.0)])  # f(x0) = 1
+    tried = []
+    while jobs is not None:
+        tried.append(float(np.abs(jobs[0] - x0).max()))
+        jobs = drv.update([(np.ones(n, dtype=np.float32), 2.0)])  # every trial is worse
+    assert drv.misfits == [1.0, 1.0, 1.0, 1.0]
+    np.testing.assert_array_equal(drv.x, x0)
+    assert all(b < a for a, b in zip(tried, tried[1:]))
+
+
+def test_trial_models_keep_c13_inside_the_stable_range():
+    n = 5
+    c11 = np.full(n, 4.0, dtype=np.float32)
+    c33 = np.full(n, 9.0, dtype=np.float32)
+    c13 = np.array([0.0, 5.0, 5.99, 6.5, -7.0], dtype=np.float32)
+    drv = SV.FwiDriver(None, np.concatenate([c11, c13, c33]), None, [], iterations=1)
+    out = drv.project(np.concatenate([c11, c13, c33]))
+    lim = np.float32(0.99) * np.float32(6.0)
+    np.testing.assert_array_equal(out[:n], c11)
+    np.testing.assert_array_equal(out[2 * n:], c33)
+    np.testing.assert_allclose(out[n:2 * n], [0.0, 5.0, lim, lim, -lim], rtol=1e-6)
 
 
 def test_window_gradients_are_stacked_without_their_frames():

@@ -128,11 +128,14 @@ class FwiDriver:
     """L-BFGS on a 3D model (c11, c13, c33 stacked) with gradients from
     gradient requests on windows of the model, one request per shot and
     iteration; the next iteration is submitted when the last gradient of the
-    current one has arrived. A step that raises the misfit is halved and
-    re-evaluated (at most `max_halvings` times); a step never changes a
-    stiffness by more than `max_step` of the largest one, and a trial model
-    whose misfit is not finite (outside the scheme's stability range) counts
-    as an increase."""
+    current one has arrived. A step that raises the misfit (or whose misfit
+    is not finite) is halved and re-evaluated, at most `max_halvings` times;
+    if none lowers the misfit the iteration keeps the current model and
+    clears the L-BFGS memory (the next direction is steepest descent), so
+    the accepted misfits never increase. A step never changes a stiffness by
+    more than `max_step` of the largest one, and with `project_stiffness`
+    every trial model keeps |c13| <= 0.99 sqrt(c11 c33) (beyond it the VTI
+    system is not hyperbolic and wavefields grow without bound)."""
     g: object
     model: np.ndarray
     wavelet: np.ndarray
@@ -143,6 +146,7 @@ class FwiDriver:
     max_step: float = 0.02
     misfits: list = field(default_factory=list)
     step0: float = 0.0
+    project_stiffness: bool = True
 
     def __post_init__(self):
         self.s_hist, self.y_hist = [], []
@@ -152,6 +156,7 @@ class FwiDriver:
         self.f_cur = None
         self.trial = None
         self.halvings = 0
+        self.restarts = 0  # consecutive directions without a decrease
 
     def jobs(self, x):
         """One gradient job per shot on its window of model x; the random
@@ -216,6 +221,18 @@ class FwiDriver:
             q += np.float32(a - b) * s
         return -q
 
+    def project(self, x):
+        """Trial model clipped to |c13| <= 0.99 sqrt(c11 c33) (x = c11, c13, c33)."""
+        if not self.project_stiffness:
+            return x
+        n = x.size // 3
+        c11, c13, c33 = x[:n], x[n:2 * n], x[2 * n:]
+        lim = (np.float32(0.99) * np.sqrt(np.maximum(c11, 0) * np.maximum(c33, 0))).astype(
+            np.float32)
+        out = x.copy()
+        out[n:2 * n] = np.clip(c13, -lim, lim)
+        return out
+
     def first(self):
         self.trial = self.x
         return self.jobs(self.x)
@@ -225,8 +242,23 @@ class FwiDriver:
         f, grad = self.stack(results)
         if not np.isfinite(f) and self.f_cur is not None:
             f = np.inf  # a trial model outside the stable range: halve the step
-        if self.f_cur is None or f < self.f_cur or (self.halvings >= self.max_halvings and
-                                                    np.isfinite(f)):
+        if self.f_cur is not None and not f < self.f_cur and self.halvings >= self.max_halvings:
+            # no decrease along this direction: keep the model, restart L-BFGS
+            # with steepest descent, its step shortened 8x for each restart in a row
+            self.s_hist, self.y_hist = [], []
+            self.it += 1
+            self.misfits.append(self.f_cur)
+            self.halvings = 0
+            self.restarts += 1
+            if self.it >= self.iterations:
+                return None
+            self.p = self.direction(self.g_cur)
+            cap = self.max_step * float(np.abs(self.x).max())
+            pmax = float(np.abs(self.p).max())
+            self.alpha = (min(1.0, cap / pmax) if pmax > 0 else 1.0) * 0.125 ** self.restarts
+            self.trial = self.project(self.x + np.float32(self.alpha) * self.p)
+            return self.jobs(self.trial)
+        if self.f_cur is None or f < self.f_cur:
             if self.f_cur is not None:
                 s, y = self.trial - self.x, grad - self.g_cur
                 if _dot(s, y) > 0:
@@ -237,6 +269,7 @@ class FwiDriver:
             self.x, self.f_cur, self.g_cur = self.trial, f, grad
             self.misfits.append(f)
             self.halvings = 0
+            self.restarts = 0
             if self.it >= self.iterations:
                 return None
             self.p = self.direction(grad)
@@ -247,7 +280,7 @@ class FwiDriver:
         else:
             self.alpha *= 0.5
             self.halvings += 1
-        self.trial = self.x + np.float32(self.alpha) * self.p
+        self.trial = self.project(self.x + np.float32(self.alpha) * self.p)
         return self.jobs(self.trial)
 
 
