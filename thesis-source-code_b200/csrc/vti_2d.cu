@@ -569,13 +569,12 @@ int run2d(vti_ctx* ctx, const vti2d_geom* g, const float* c11, const float* c13,
   }
   VTI_CUDA(ctx, cudaSetDevice(ctx->device));
   // device buffers (the context's 2D scratch, kept between calls): 4
-  // model/taper + 4 wavefields + nt amplitudes, then ints (trace row per
-  // level, receiver columns and rows, or flat receiver indices), then the
-  // output rows
+  // model/taper + 4 wavefields + nt amplitudes, then the flat receiver
+  // indices, then the output rows
   const long long nrows_out = mode == 0 ? (g->nt - ntNeg - 1) / ratio + 1 : 0;
   const int nrec = mode == 0 ? std::max(nri, 0) : 0;
   const size_t nbuf = 8 * (size_t)nnxz + g->nt;
-  const size_t n_ints = (size_t)g->nt + 2 * (size_t)nrec;
+  const size_t n_ints = (size_t)nrec;
   const size_t n_data = (size_t)nrows_out * nrec;
   float* buf = nullptr;
   {
@@ -585,8 +584,7 @@ int run2d(vti_ctx* ctx, const vti2d_geom* g, const float* c11, const float* c13,
   float *dc11 = buf, *dc13 = dc11 + nnxz, *dc33 = dc13 + nnxz, *dtap = dc33 + nnxz;
   float* w[4] = {dtap + nnxz, dtap + 2 * nnxz, dtap + 3 * nnxz, dtap + 4 * nnxz};
   float* amps = dtap + 5 * nnxz;
-  int* d_ints = reinterpret_cast<int*>(buf + nbuf);
-  int* d_ridx = d_ints;
+  int* d_ridx = reinterpret_cast<int*>(buf + nbuf);
   float* d_data = nrec > 0 ? buf + nbuf + n_ints : nullptr;
   int st = VTI_OK;
   auto cleanup = [&]() { cudaStreamSynchronize(ctx->stream); };
