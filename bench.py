@@ -758,6 +758,27 @@ def run_forward2d(args):
     launches = ctx.launches - launches0
     snap = V.modeling_f(ctx, g, c11, c13, c33, s.wavelet, int(s.sloc[0] + s.sloc[1] * nnx),
                         s.taper)
+    # 14 shots of the same grid with disjoint receiver blocks: all shots in one
+    # launch (one cluster each) against the per-level path
+    sm = S.survey2d(nx=401, nz=201, nt=2000, npad=30, d=10.0, dt=1e-3, rate=2e-3, freq=15.0,
+                    src_z=20.0, rec_z=20.0, seed=1, ns=14)
+    sl = sm.sloc.reshape(-1, 4).copy()
+    nrb = (sm.rloc.size // 2) // len(sl)
+    sl[:, 2] = nrb
+    sl[:, 3] = np.arange(len(sl)) * nrb
+    multi = {"shots": len(sl), "receivers_per_shot": int(nrb)}
+    for key, res in (("resident_ms", True), ("per_level_ms", False)):
+        ctx.set_2d_resident(res)
+        V.synthetic_f(ctx, g, c11, c13, c33, sm.wavelet, sl.reshape(-1), sm.rloc, s.taper)
+        ctx.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(3):
+            V.synthetic_f(ctx, g, c11, c13, c33, sm.wavelet, sl.reshape(-1), sm.rloc, s.taper)
+        ctx.synchronize()
+        multi[key] = round((time.perf_counter() - t0) / 3 * 1e3, 2)
+    ctx.set_2d_resident(True)
+    multi["gpts_per_s"] = round(len(sl) * (s.nt - 2) * nnx * nnz / (multi["resident_ms"] / 1e3)
+                                / 1e9, 2)
     ctx.close()
     pts = (s.nt - 2) * nnx * nnz
     # CPU: the FP32 oracle of the same shot, all host threads
@@ -800,6 +821,7 @@ def run_forward2d(args):
                 "h2d_bytes_per_step": int(4 * (4 * nnx * nnz + s.nt)),
                 "d2h_bytes_per_step": int(tr.nbytes), "api": "vti2d_synthetic (host buffers)"},
         "gpu_launches": int(launches), "clocks": clk.summary(),
+        "multishot": multi,
     }
     print(json.dumps(res), flush=True)
     return res
