@@ -174,6 +174,16 @@ int vti3d_plan_objfunc(vti3d_plan* plan, const float* souloc, const int* shotid,
  * model; no sponge on the source wavefield. */
 int vti3d_plan_rtm(vti3d_plan* plan, const float* souloc, const int* shotid, int nshot,
                    const float* data, int data_mem, float* image, int image_mem);
+/* Offset-domain common-image gathers (odcig3d_f, lib/vti-fwi-3d/gpu/odcig3d_f.cu:15,
+ * with the imaging condition of extendedImagingKernel, wave3d.cu:1299-1313):
+ * the migration of vti3d_plan_rtm with, for every level, image[lag][p] +=
+ * (2/3 sx + 1/3 sz)(p) * sponge(p+lag) (2/3 lx + 1/3 lz)(p+lag) for
+ * |lag| <= nlag (x offsets; the reference fixes nlag = 32, wave3d.h:19), at
+ * x in [max(4,nlag), nx-max(4,nlag)), y in [4, ny-4), all z; zero elsewhere.
+ * image: (2*nlag+1) * nxyz floats, lag -nlag first; its lag-0 volume equals
+ * the vti3d_plan_rtm image on those x (bit for bit). 0 <= nlag <= 1024. */
+int vti3d_plan_odcig(vti3d_plan* plan, const float* souloc, const int* shotid, int nshot,
+                     const float* data, int data_mem, int nlag, float* image, int image_mem);
 /* Wavelet gradient (waveletGradientCij3d_f, lib/vti-fwi-3d/gpu/modelData3d_f.cu:858):
  * gwavelet (nt) = dt2 * sum over shots and levels of lambda_x + lambda_z at the
  * source, the adjoint wavefield driven by the traces `data` (nnt x nrec_total)

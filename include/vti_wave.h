@@ -77,6 +77,16 @@ void rtmVEpsDel(float* image, float* souloc, int ns, std::vector<int>& shotid, f
                 int ny, int nz, int nt, int npad, float ox, float oy, float oz, float ot,
                 float dx, float dy, float dz, float dt, float samplingRate, float wbottom);
 
+// wave3d.h:116 — offset-domain common-image gathers of all ns shots: the
+// migration of rtmCij3d_f (traces from data=, three floats per receiver,
+// devices from gpu=) from v, eps, del (c33 = v^2, c11 = c33 (1 + 2 eps),
+// c13 = c33 sqrt(1 + 2 del)), with x-offset lags |lag| <= 32 (NLAG,
+// wave3d.h:19); image holds 65 * nx*ny*nz floats, lag -32 first.
+void odcig3d_f(float* image, float* souloc, int ns, float* recloc, float* wavelet, float* v,
+               float* eps, float* del, int nx, int ny, int nz, int nt, int npad, float ox,
+               float oy, float oz, float ot, float dx, float dy, float dz, float dt,
+               float samplingRate);
+
 // wave3d.h:112 / :114 — gradient of the misfit w.r.t. the source wavelet (nt
 // floats), the adjoint driven by the traces in ddata (nnt*irbegin layout).
 void waveletGradient3d_f(float* gwavelet, const float* ddata, float* souloc, int ns,

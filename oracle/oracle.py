@@ -126,6 +126,26 @@ def rtm3d(g, c11, c13, c33, wavelet, souloc, shotid, recloc, data, dtype=np.floa
     return out
 
 
+def odcig3d(g, c11, c13, c33, wavelet, souloc, shotid, recloc, data, nlag, dtype=np.float64,
+            full_steps=False):
+    """Offset-domain gathers of rtmCij3d_f's migration with the extended
+    imaging condition of extendedImagingKernel (wave3d.cu:1299-1313):
+    (2 nlag + 1) x nxyz, lag -nlag first."""
+    ip, fp = _geo3(g, full_steps)
+    n = g.nx * g.ny * g.nz
+    out = np.zeros((2 * nlag + 1) * n, dtype=dtype)
+    suf = "f64" if dtype == np.float64 else "f32"
+    f = getattr(lib(), f"orc3d_odcig_{suf}")
+    f.argtypes = [VP] * 8 + [C.c_int, VP, VP, C.c_int, VP]
+    f.restype = C.c_int
+    shotid = _i32(shotid)
+    st = f(_p(ip), _p(fp), _p(_f32(c11)), _p(_f32(c13)), _p(_f32(c33)), _p(_f32(wavelet)),
+           _p(_f32(souloc)), _p(shotid), len(shotid), _p(_f32(recloc).reshape(-1)),
+           _p(_f32(data)), int(nlag), _p(out))
+    assert st == 0
+    return out.reshape(2 * nlag + 1, n)
+
+
 def wavelet_gradient3d(g, c11, c13, c33, souloc, shotid, recloc, data, dtype=np.float64,
                        full_steps=False):
     """waveletGradientCij3d_f restated: the gradient w.r.t. the wavelet (nt)."""

@@ -3,13 +3,15 @@
 // tests/golden/make_golden.py. TEST INFRASTRUCTURE ONLY: it produces golden
 // traces and gradients that pin the oracle; nothing in the library uses it.
 //
-// usage: ref3d <dir> model|grad|rtm|wgrad|modop [key=value ...] (modop: built with
-//   -DVTI_SHIM against libvti_wave.so, which provides ModelingOp3d)
+// usage: ref3d <dir> model|grad|rtm|wgrad|modop|odcig [key=value ...] (modop,
+//   odcig: built with -DVTI_SHIM against libvti_wave.so, which provides
+//   ModelingOp3d and a linkable odcig3d_f)
 //   <dir>/params.txt : nx ny nz nt npad ox oy oz ot dx dy dz dt rate ns nrec
 //   <dir>/{souloc,recloc,wavelet,cij,padb,randb,dobs}.bin (float32)
 //   writes <dir>/ref_ddata.bin (model), <dir>/ref_fgcij.bin (grad) or
 //   <dir>/ref_image.bin (rtm: the traces in dobs.bin migrated with cij) or
 //   <dir>/ref_wgrad.bin (wgrad: wavelet gradient driven by dobs.bin)
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
@@ -18,8 +20,13 @@
 
 #ifdef VTI_SHIM
 // built against libvti_wave.so: the source-inversion operator class
-// (ModelingOp3d.h) is available as well (mode modop)
+// (ModelingOp3d.h) and odcig3d_f (wave3d.h:116; the reference's own target
+// does not link) are available as well (modes modop, odcig)
 #include "vti_modeling_op3d.h"
+void odcig3d_f(float* image, float* souloc, int ns, float* recloc, float* wavelet, float* v,
+               float* eps, float* del, int nx, int ny, int nz, int nt, int npad, float ox,
+               float oy, float oz, float ot, float dx, float dy, float dz, float dt,
+               float samplingRate);
 #endif
 
 // Entry points of lib/vti-fwi-3d/gpu (wave3d.h:84-122) and lib/io/myio.cpp:15.
@@ -153,6 +160,24 @@ int main(int argc, char** argv) {
     save(dir + "/ref_modop_fwd_add.bin", d1.data(), d1.size());
     save(dir + "/ref_modop_adj.bin", m0.data(), m0.size());
     save(dir + "/ref_modop_adj_add.bin", m1.data(), m1.size());
+  } else if (mode == "odcig") {
+    // odcig3d_f of the traces in dobs.bin with v, eps, del derived from cij
+    // (c33 = v^2, c11 = c33 (1 + 2 eps), c13 = c33 sqrt(1 + 2 del)) ->
+    // ref_odcig.bin (65 lags x nxyz)
+    std::vector<float> v(n), eps(n), del(n);
+    for (size_t i = 0; i < n; ++i) {
+      const double c11 = cij[i], c13 = cij[n + i], c33 = cij[2 * n + i];
+      v[i] = (float)std::sqrt(c33);
+      eps[i] = (float)((c11 / c33 - 1.) / 2.);
+      del[i] = (float)(((c13 / c33) * (c13 / c33) - 1.) / 2.);
+    }
+    std::vector<float> rec3(3 * (size_t)nrec);
+    for (int ir = 0; ir < nrec; ++ir)
+      for (int k = 0; k < 3; ++k) rec3[3 * ir + k] = recloc[4 * ir + k];
+    std::vector<float> image(65 * n, 0.f);
+    odcig3d_f(image.data(), souloc.data(), ns, rec3.data(), wavelet.data(), v.data(), eps.data(),
+              del.data(), nx, ny, nz, nt, npad, ox, oy, oz, ot, dx, dy, dz, dt, rate);
+    save(dir + "/ref_odcig.bin", image.data(), image.size());
 #endif
   } else {
     std::fprintf(stderr, "unknown mode %s\n", mode.c_str());

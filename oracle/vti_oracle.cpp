@@ -474,17 +474,26 @@ void gradient3d(const Geo3& g, const float* cij_in, const float* padb, const flo
 // (2/3 sx + 1/3 sz)(2/3 lx + 1/3 lz) with both fields at the step's current
 // level, the receiver wavefield already damped by this step's sponge.
 // image is zeroed first and accumulates over shots (rtm3d_f.cu:175).
+// nlag >= 0: offset-domain gathers with the extended imaging condition of
+// extendedImagingKernel (lib/vti-fwi-3d/gpu/wave3d.cu:1299-1313): for
+// |lag| <= nlag, image[j + (lag+nlag)*n] += S[j] * R[j+lag] (x offsets) with
+// S = 2/3 sx + 1/3 sz and R the damped receiver term of the zero-lag image,
+// for x in [max(4,nlag), min(nx-4, nx-nlag)), y in [4, ny-4), all z. The 3D
+// reference driver (odcig3d_f.cu) does not link (its forwardKernel calls do
+// not match the declared kernel), so this restatement follows the kernel.
 template <typename T>
 void rtm3d(const Geo3& g, const float* c11, const float* c13, const float* c33,
            const float* wavelet, const float* souloc, const int* shotid, int nshot,
-           const float* recloc, const float* data, T* image) {
+           const float* recloc, const float* data, T* image, int nlag = -1) {
   const long n = g.nxyz(), nxy = g.nxy();
+  const long nimg = nlag >= 0 ? (2L * nlag + 1) * n : n;
   const float dt2 = g.dt * g.dt;
   const int st = sampling_step(g.rate, g.dt);
   const int nnt = (g.nt - 1) / st + 1;
   const int M = last_level(g);
-  std::fill(image, image + n, (T)0);
+  std::fill(image, image + nimg, (T)0);
   Damp3 damp(g);
+  const long xlo = std::max<long>(kHalf, nlag), xhi = std::min<long>(g.nx - kHalf, g.nx - nlag);
   std::vector<T> cx, cz, px, pz, lcx, lcz, lpx, lpz;
   for (int k = 0; k < nshot; ++k) {
     Shot3 s = make_shot3(g, souloc, recloc, shotid[k]);
@@ -517,15 +526,30 @@ void rtm3d(const Geo3& g, const float* c11, const float* c13, const float* c33,
         lpx[ri] += d * ((T)kTwoThird * inj);
         lpz[ri] += d * ((T)kOneThird * inj);
       }
+      if (nlag < 0) {
 #pragma omp parallel for collapse(2) schedule(static)
-      for (long iz = 0; iz < g.nz; ++iz)
-        for (long iy = kHalf; iy < g.ny - kHalf; ++iy)
-          for (long ix = kHalf; ix < g.nx - kHalf; ++ix) {
-            const long ixy = ix + iy * g.nx, j = ixy + iz * nxy;
-            const T d = (T)damp.at(ixy, (int)iz);
-            image[j] += ((T)kTwoThird * cx[j] + (T)kOneThird * cz[j]) *
-                        (d * ((T)kTwoThird * lcx[j] + (T)kOneThird * lcz[j]));
-          }
+        for (long iz = 0; iz < g.nz; ++iz)
+          for (long iy = kHalf; iy < g.ny - kHalf; ++iy)
+            for (long ix = kHalf; ix < g.nx - kHalf; ++ix) {
+              const long ixy = ix + iy * g.nx, j = ixy + iz * nxy;
+              const T d = (T)damp.at(ixy, (int)iz);
+              image[j] += ((T)kTwoThird * cx[j] + (T)kOneThird * cz[j]) *
+                          (d * ((T)kTwoThird * lcx[j] + (T)kOneThird * lcz[j]));
+            }
+      } else {
+#pragma omp parallel for collapse(2) schedule(static)
+        for (long iz = 0; iz < g.nz; ++iz)
+          for (long iy = kHalf; iy < g.ny - kHalf; ++iy)
+            for (long ix = xlo; ix < xhi; ++ix) {
+              const long ixy = ix + iy * g.nx, j = ixy + iz * nxy;
+              const T sv = (T)kTwoThird * cx[j] + (T)kOneThird * cz[j];
+              for (int lag = -nlag; lag <= nlag; ++lag) {
+                const T d = (T)damp.at(ixy + lag, (int)iz);
+                image[j + (lag + nlag) * n] +=
+                    sv * (d * ((T)kTwoThird * lcx[j + lag] + (T)kOneThird * lcz[j + lag]));
+              }
+            }
+      }
       std::swap(cx, px); std::swap(cz, pz);
       std::swap(lcx, lpx); std::swap(lcz, lpz);
     }
@@ -1380,6 +1404,19 @@ ORC3D_GRAD(float, f32)
   }
 ORC3D_RTM(double, f64)
 ORC3D_RTM(float, f32)
+
+#define ORC3D_ODCIG(T, SUF)                                                                    \
+  int orc3d_odcig_##SUF(const int* ip, const float* fp, const float* c11, const float* c13,     \
+                        const float* c33, const float* wavelet, const float* souloc,            \
+                        const int* shotid, int nshot, const float* recloc, const float* data,   \
+                        int nlag, T* image) {                                                   \
+    if (nlag < 0) return 1;                                                                     \
+    Geo3 g = unpack3(ip, fp);                                                                   \
+    rtm3d<T>(g, c11, c13, c33, wavelet, souloc, shotid, nshot, recloc, data, image, nlag);     \
+    return 0;                                                                                   \
+  }
+ORC3D_ODCIG(double, f64)
+ORC3D_ODCIG(float, f32)
 
 #define ORC3D_WGRAD(T, SUF)                                                                    \
   int orc3d_wavelet_gradient_##SUF(const int* ip, const float* fp, const float* c11,            \

@@ -106,3 +106,37 @@ def test_odcig2d_matches_oracle_and_reference(ctx, name):
     assert rel_l2(img, ref) < IMAGE_TOL
     # every offset panel carries signal
     assert all(np.abs(ref[h]).max() > 0 for h in range(2 * nhx + 1))
+
+
+@pytest.mark.parametrize("nlag", [3, 6])
+def test_odcig3d_lag0_is_the_rtm_image_and_matches_oracle(ctx, nlag):
+    """Offset-domain gathers (odcig3d_f's extended imaging condition): the
+    zero-lag gather is the RTM image bit for bit on the imaged x range
+    [max(4, nlag), nx - max(4, nlag)) and zero outside it; every lag matches
+    the FP64 oracle. nlag = 6 > 4 exercises the narrowed x range."""
+    c = K.case3d("g3_a")
+    s = c["s"]
+    g = s.geom()
+    n = s.nxyz
+    model = K.rtm_model3d(c)
+    dobs = load_golden("g3_a")["dobs"]
+    p = V.Plan3d(ctx, g)
+    try:
+        p.set_model(*_split(model, n))
+        p.set_wavelet(s.wavelet)
+        p.set_receivers(s.recloc)
+        img = p.rtm(s.souloc, c["shotid"], dobs)
+        gat = p.odcig(s.souloc, c["shotid"], dobs, nlag)
+    finally:
+        p.close()
+    assert gat.shape == (2 * nlag + 1, n)
+    lo = max(4, nlag)
+    mask = np.zeros((s.nz, s.ny, s.nx), dtype=bool)
+    mask[:, :, lo:s.nx - lo] = True
+    mask = mask.reshape(-1)
+    np.testing.assert_array_equal(gat[nlag][mask], img[mask])
+    assert not gat[:, ~mask].any()
+    o = O.odcig3d(g, *_split(model, n), s.wavelet, s.souloc, c["shotid"], s.recloc, dobs, nlag)
+    for k in range(2 * nlag + 1):
+        assert np.abs(o[k]).max() > 0, k
+        assert rel_l2(gat[k], o[k]) < IMAGE_TOL, k

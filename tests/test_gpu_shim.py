@@ -216,3 +216,38 @@ def test_shim_odcig2d_matches_reference(drivers, name):
         _run(drivers["2d"], d, "odcig", str(K.ODCIG_CASES2D[name]))
         img = np.fromfile(d / "ref_odcig.bin", dtype=np.float32)
     assert rel_l2(img, load_golden(f"{name}_odcig")["image"]) < 1e-4
+
+
+def test_shim_odcig3d_matches_the_plan(drivers, ctx):
+    """odcig3d_f through the drop-in (the reference's own target does not
+    link): v, eps, del derived from c_ij by the harness, 32 lags, equal to
+    the plan's gathers of the same model within the image tolerance (the
+    v/eps/del round trip moves c_ij by a few ulps)."""
+    import vtib200 as V
+    import vtib200.synth as S
+    s = S.small3d(nx=80, ny=28, nz=24, nt=110, npad=6, rec_step=3, rate=2.1e-3)
+    true = S.small3d(nx=80, ny=28, nz=24, nt=110, npad=6, seed=11)
+    g = s.geom()
+    n = s.nxyz
+    padb, randb = S.boundaries3d(s)
+    tc = true.cij()
+    dobs = V.modelDataCij3d_f(ctx, g, s.souloc, [0], s.recloc, s.wavelet, tc[:n], tc[n:2 * n],
+                              tc[2 * n:])
+    model = s.cij()
+    with tempfile.TemporaryDirectory() as td:
+        d = Path(td)
+        MG.write_inputs3d({"s": s, "padb": padb, "randb": randb}, d)
+        np.asarray(model, np.float32).tofile(d / "cij.bin")
+        np.asarray(dobs, np.float32).tofile(d / "dobs.bin")
+        _run(drivers["3d"], d, "odcig")
+        shim = np.fromfile(d / "ref_odcig.bin", dtype=np.float32).reshape(65, n)
+    p = V.Plan3d(ctx, g)
+    try:
+        p.set_model(model[:n], model[n:2 * n], model[2 * n:])
+        p.set_wavelet(s.wavelet)
+        p.set_receivers(s.recloc)
+        gat = p.odcig(s.souloc, [0], dobs, 32)
+    finally:
+        p.close()
+    assert np.abs(gat[32]).max() > 0
+    assert rel_l2(shim.reshape(-1), gat.reshape(-1)) < 1e-4

@@ -247,6 +247,12 @@ int launch_inject_residual(vti_ctx* ctx, float* lx, float* lz, const float* res,
 int launch_seed_adjoint(vti_ctx* ctx, float* lx, float* lz, const float* res, int nnt,
                         const long long* rec, const float* rec_damp, int nr, float dt2);
 int launch_set_point(vti_ctx* ctx, float* a, float* b, long long off, float value);
+// Offset-domain gathers of one backward level: image holds 2*nlag+1 volumes
+// of d.plane*d.nz floats (pitched rows, no z pad planes), lag -nlag first;
+// sx, sz, lx, lz are the level's current source and receiver wavefields.
+int launch_odcig3d(vti_ctx* ctx, const Dims3& d, const float* sx, const float* sz,
+                   const float* lx, const float* lz, const Damping& damp, int nlag,
+                   float* image);
 // res <- modeled - observed (dead receivers: modeled zeroed first);
 // acc[0] += sum(res^2) in FP64, reproducibly; acc must hold
 // 1 + residual_blocks(ctx) doubles. obs == nullptr: only zero dead traces.

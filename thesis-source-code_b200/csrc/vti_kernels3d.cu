@@ -215,6 +215,47 @@ __global__ void k_boundary_merge(Dims3 d, int npad, const float* full, const flo
   }
 }
 
+// Offset-domain image gathers of one backward level (extendedImagingKernel,
+// lib/vti-fwi-3d/gpu/wave3d.cu:1299-1313, on this library's RTM pair): with
+// S(p) = 2/3 sx + 1/3 sz and R(p) = sponge(p) (2/3 lx + 1/3 lz) at the step's
+// current level, evaluated with the operations of the zero-lag image of the
+// fused backward kernel, image[lag][p] = fma(S(p), R(p + lag), image[lag][p])
+// for |lag| <= nlag (x offsets) and x in [xlo, xhi). One block: 128 points
+// of one row; R of the row segment and its nlag-wide margins staged in
+// shared memory.
+constexpr int kOdcigTX = 128;
+constexpr float kTwoThirdF = (float)kTwoThird, kOneThirdF = (float)kOneThird;
+
+__global__ void __launch_bounds__(kOdcigTX)
+    k_odcig3d(Dims3 d, const float* sx, const float* sz, const float* lx, const float* lz,
+              const float* dampx, const float* dampy, const float* dampz, int nlag, int xlo,
+              int xhi, float* image, long long lag_stride) {
+  extern __shared__ float rs[];  // R at x0 - nlag .. x0 + kOdcigTX + nlag - 1
+  const int x0 = blockIdx.x * kOdcigTX;
+  const int y = kHalo + blockIdx.y;
+  const int z = blockIdx.z;
+  const float dz = dampz[z], dy = dampy[y];
+  const long long row = (long long)z * d.plane + (long long)y * d.pitch;
+  for (int t = threadIdx.x; t < kOdcigTX + 2 * nlag; t += kOdcigTX) {
+    const int xr = x0 - nlag + t;
+    float r = 0.f;
+    if (xr >= 0 && xr < d.nx) {
+      const float dd = (dampx[xr] * dy) * dz;
+      r = dd * fmaf(kTwoThirdF, lx[row + xr], kOneThirdF * lz[row + xr]);
+    }
+    rs[t] = r;
+  }
+  __syncthreads();
+  const int x = x0 + threadIdx.x;
+  if (x < xlo || x >= xhi) return;
+  const float sv = fmaf(kTwoThirdF, sx[row + x], kOneThirdF * sz[row + x]);
+  float* img = image + row + x;
+  for (int lag = -nlag; lag <= nlag; ++lag) {
+    float* q = img + (long long)(lag + nlag) * lag_stride;
+    *q = fmaf(sv, rs[threadIdx.x + nlag + lag], *q);
+  }
+}
+
 int zslab_for(vti_ctx* ctx, const Dims3& d, int tiles, int ctas_per_sm) {
   // choose the number of z slabs so the grid fills the GPU a few times over
   int target = ctx->sm_count * ctas_per_sm * 4;
@@ -228,6 +269,21 @@ int zslab_for(vti_ctx* ctx, const Dims3& d, int tiles, int ctas_per_sm) {
 }
 
 }  // namespace
+
+int launch_odcig3d(vti_ctx* ctx, const Dims3& d, const float* sx, const float* sz,
+                   const float* lx, const float* lz, const Damping& damp, int nlag,
+                   float* image) {
+  const int xlo = nlag > kHalo ? nlag : kHalo;
+  const int xhi = d.nx - xlo;
+  if (xhi <= xlo || d.ny <= 2 * kHalo || d.nz < 1) return VTI_OK;
+  dim3 grid((d.nx + kOdcigTX - 1) / kOdcigTX, d.ny - 2 * kHalo, d.nz);
+  const size_t smem = (kOdcigTX + 2 * (size_t)nlag) * sizeof(float);
+  k_odcig3d<<<grid, kOdcigTX, smem, ctx->stream>>>(d, sx, sz, lx, lz, damp.x, damp.y, damp.z,
+                                                   nlag, xlo, xhi, image,
+                                                   d.plane * (long long)d.nz);
+  VTI_LAUNCHED(ctx, "k_odcig3d");
+  return VTI_OK;
+}
 
 int launch_record(vti_ctx* ctx, float* trace, int nnt, int j, const float* cx, const float* cz,
                   const long long* rec, int nr) {

@@ -238,7 +238,10 @@ int forward_pass(vti3d_plan* p, const ShotGeom& s, bool sponge) {
 // sx[other] = level M-1 from pass 2, and the residual in d_trace.
 // rtm: the observed traces are in d_trace and the RTM image accumulates in
 // g11 (rtm3d_f.cu:470-620, same schedule).
-int backward_pass(vti3d_plan* p, const ShotGeom& s, bool rtm) {
+// ext (nlag >= 0, RTM only): offset-domain gathers of each level added after
+// its fused step, from the same current wavefields.
+int backward_pass(vti3d_plan* p, const ShotGeom& s, bool rtm, float* ext = nullptr,
+                  int nlag = 0) {
   vti_ctx* ctx = p->ctx;
   const vti3d_geom& g = p->g;
   const Dims3& d = p->d;
@@ -270,6 +273,9 @@ int backward_pass(vti3d_plan* p, const ShotGeom& s, bool rtm) {
         p->sz[SA].origin, p->lz[LA].origin, p->sx[SB].origin, p->sz[SB].origin,
         p->lx[LB].origin, p->lz[LB].origin, p->g11.origin, p->g13.origin, p->g33.origin, dmp,
         dt2, idx2, idy2, idz2, sxs, sys, szs, src, rtm));
+    if (ext)
+      VTI_TRY(launch_odcig3d(ctx, d, p->sx[SA].origin, p->sz[SA].origin, p->lx[LA].origin,
+                             p->lz[LA].origin, dmp, nlag, ext));
     // residual interpolated at it+1 (injectRecord3d.cu:60-78)
     const int ti = it + 1;
     float f = float(ti) / float(st);
@@ -499,7 +505,7 @@ int vti3d_plan_destroy(vti3d_plan* p) {
   vol_free(&p->g13);
   vol_free(&p->g33);
   void* ptrs[] = {p->dampx, p->d_rec, p->d_rec_damp, p->d_live, p->d_trace,
-                  p->d_obs, p->d_blist, p->d_acc, p->d_gw, p->d_part};
+                  p->d_obs, p->d_blist, p->d_acc, p->d_gw, p->d_part, p->d_ext};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   delete p;
@@ -670,6 +676,48 @@ int vti3d_plan_rtm(vti3d_plan* p, const float* souloc, const int* shotid, int ns
     VTI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   }
   VTI_TRY(vol_download(ctx, p->d, &p->g11, image, image_mem));
+  VTI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return check_device_status(ctx);
+}
+
+int vti3d_plan_odcig(vti3d_plan* p, const float* souloc, const int* shotid, int nshot,
+                     const float* data, int data_mem, int nlag, float* image, int image_mem) {
+  if (!p) return VTI_ERR_ARG;
+  vti_ctx* ctx = p->ctx;
+  if (!p->have_model) return fail(ctx, VTI_ERR_ARG, "model not set");
+  if ((int)p->wavelet.size() != p->g.nt) return fail(ctx, VTI_ERR_ARG, "wavelet not set");
+  if (!souloc || (nshot > 0 && !shotid) || !data || !image || nshot < 0)
+    return fail(ctx, VTI_ERR_ARG, "null pointer or negative shot count");
+  if (nlag < 0 || nlag > 1024) return fail(ctx, VTI_ERR_ARG, "nlag out of range (0..1024)");
+  VTI_CUDA(ctx, cudaSetDevice(ctx->device));
+  const Dims3& d = p->d;
+  const int nnt = nnt_of(p->g);
+  const int nl = 2 * nlag + 1;
+  const size_t vol = (size_t)d.plane * d.nz;  // one lag: pitched rows, no pad planes
+  VTI_TRY(ensure(ctx, &p->d_ext, &p->ext_cap, nl * vol));
+  VTI_CUDA(ctx, cudaMemsetAsync(p->d_ext, 0, nl * vol * sizeof(float), ctx->stream));
+  // the zero-lag image of the same passes accumulates in g11 (unused here)
+  VTI_TRY(vol_zero(ctx, d, &p->g11));
+  for (int k = 0; k < nshot; ++k) {
+    ShotGeom s;
+    VTI_TRY(shot_geom(p, souloc, shotid[k], &s));
+    VTI_TRY(upload_shot(p, s));
+    const float* obs = nullptr;
+    VTI_TRY(get_obs(p, s, data, data_mem, &obs));
+    if (s.nr > 0)
+      VTI_CUDA(ctx, cudaMemcpyAsync(p->d_trace, obs, (size_t)nnt * s.nr * sizeof(float),
+                                    cudaMemcpyDeviceToDevice, ctx->stream));
+    VTI_TRY(forward_pass(p, s, false));
+    VTI_TRY(backward_pass(p, s, true, p->d_ext, nlag));
+    VTI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  const cudaMemcpyKind kind =
+      image_mem == VTI_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  const size_t nxyz = (size_t)d.nx * d.ny * d.nz;
+  for (int l = 0; l < nl; ++l)
+    VTI_CUDA(ctx, cudaMemcpy2DAsync(image + l * nxyz, d.nx * sizeof(float), p->d_ext + l * vol,
+                                    d.pitch * sizeof(float), d.nx * sizeof(float),
+                                    (size_t)d.ny * d.nz, kind, ctx->stream));
   VTI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return check_device_status(ctx);
 }

@@ -49,6 +49,8 @@ struct vti3d_plan {
   double* d_acc = nullptr;
   float* d_gw = nullptr;  // wavelet gradient accumulator (nt)
   size_t gw_cap = 0;
+  float* d_ext = nullptr;  // offset-domain gathers ((2 nlag + 1) pitched volumes)
+  size_t ext_cap = 0;
   double* d_part = nullptr;  // per-trace AGC misfits
   size_t part_cap = 0;
   // misfit options of the gradient (objFuncGradient3d_f.cu:743-775)

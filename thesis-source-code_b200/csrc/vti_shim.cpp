@@ -912,6 +912,58 @@ void rtmVEpsDel(float* image, float* souloc, int ns, std::vector<int>& shotid, f
                 std::min<size_t>((size_t)nwbottom, (size_t)nz - npad) * nxy * sizeof(float));
 }
 
+// odcig3d_f (odcig3d_f.cu:15-543): all ns shots, v/eps/del converted with
+// unit scales (the c13 = c33 sqrt(1 + 2 del) of wave3d.cu:86), the migration
+// of rtmCij3d_f with the x-offset gathers of extendedImagingKernel
+// (wave3d.cu:1299-1313) for |lag| <= 32 (NLAG, wave3d.h:19). Images of the
+// devices' shots are summed.
+void odcig3d_f(float* image, float* souloc, int ns, float* recloc, float* wavelet, float* v,
+               float* eps, float* del, int nx, int ny, int nz, int nt, int npad, float ox,
+               float oy, float oz, float ot, float dx, float dy, float dz, float dt,
+               float samplingRate) {
+  constexpr int kNlag = 32;
+  const size_t n = (size_t)nx * ny * nz, nimg = (2 * kNlag + 1) * n;
+  std::memset(image, 0, nimg * sizeof(float));
+  std::vector<float> c(3 * n);
+  vti_vepsdel_to_cij(c.data(), c.data() + n, c.data() + 2 * n, v, eps, del, 1.f, 1.f, 1.f, n);
+  vti3d_geom g = geom3(nx, ny, nz, nt, npad, ox, oy, oz, ot, dx, dy, dz, dt, samplingRate);
+  std::vector<int> shotid(ns);
+  for (int i = 0; i < ns; ++i) shotid[i] = i;
+  const std::vector<int> gpus = gpus_from_argv();
+  const int nrec = total_receivers(souloc, shotid);
+  std::vector<float> rec4(4 * (size_t)nrec);
+  for (int ir = 0; ir < nrec; ++ir) {
+    for (int k = 0; k < 3; ++k) rec4[4 * (size_t)ir + k] = recloc[3 * (size_t)ir + k];
+    rec4[4 * (size_t)ir + 3] = 1.f;
+  }
+  std::vector<float> data;
+  int nr_read = 0;
+  if (!read_observed(souloc, shotid, g, &data, &nr_read)) return;
+  const unsigned flags = ref_flags(gpus.size());
+  std::vector<std::vector<float>> parts(gpus.size());
+  std::map<int, size_t> slot;
+  for (size_t i = 0; i < gpus.size(); ++i) slot[gpus[i]] = i;
+  over_gpus(gpus, shotid, [&](int id, const std::vector<int>& sub) {
+    Device* dev = device(id);
+    if (!dev) return false;
+    std::lock_guard<std::mutex> lk(dev->mu);
+    vti3d_plan* p = plan_for(dev, g, flags);
+    if (!p) return false;
+    std::vector<float>& img = parts[slot[id]];
+    img.assign(nimg, 0.f);
+    return report(dev->ctx, vti3d_plan_set_model(p, c.data(), c.data() + n, c.data() + 2 * n,
+                                                 nullptr, nullptr, VTI_MEM_HOST), "model") &&
+           report(dev->ctx, vti3d_plan_set_wavelet(p, wavelet, VTI_MEM_HOST), "wavelet") &&
+           report(dev->ctx, vti3d_plan_set_receivers(p, rec4.data(), nrec), "receivers") &&
+           report(dev->ctx, vti3d_plan_odcig(p, souloc, sub.data(), (int)sub.size(),
+                                             data.data(), VTI_MEM_HOST, kNlag, img.data(),
+                                             VTI_MEM_HOST), "odcig");
+  });
+  for (auto& img : parts)
+    if (!img.empty())
+      for (size_t i = 0; i < nimg; ++i) image[i] += img[i];
+}
+
 // rtm_f (rtm_f.cu:13-267): shots round-robin over the gpu= devices
 // (is = pass*nGPUs + i), per-device images summed.
 void rtm_f(float* image, const float* data, const float* c11, const float* c13, const float* c33,

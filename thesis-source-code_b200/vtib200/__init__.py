@@ -100,6 +100,7 @@ def _signatures():
                                           C.POINTER(C.c_double)]),
         "vti3d_plan_objfunc": (C.c_int, [P, P, P, C.c_int, P, C.c_int, C.POINTER(C.c_double)]),
         "vti3d_plan_rtm": (C.c_int, [P, P, P, C.c_int, P, C.c_int, P, C.c_int]),
+        "vti3d_plan_odcig": (C.c_int, [P, P, P, C.c_int, P, C.c_int, C.c_int, P, C.c_int]),
         "vti3d_plan_set_misfit": (C.c_int, [P, C.c_float, C.c_int, C.c_int]),
         "vti3d_rtm_cij": (C.c_int, [P, P, P, P, P, P, P, P, C.c_int, P, C.c_int, P, P, C.c_uint]),
         "vti3d_plan_wavefield": (VP, [P]),
@@ -334,6 +335,18 @@ class Plan3d:
         self.ctx.check(lib().vti3d_plan_rtm(self._h, _p(souloc), _p(shotid), len(shotid),
                                             _p(data), data_mem, _p(image), image_mem))
         return image
+
+    def odcig(self, souloc, shotid, data, nlag, data_mem=MEM_HOST):
+        """odcig3d_f on the resident model: (2 nlag + 1, nxyz) gathers, lag -nlag first."""
+        souloc, shotid = _f32(souloc).reshape(-1), _i32(shotid)
+        if data_mem == MEM_HOST:
+            data = _f32(data)
+        n = self.g.nx * self.g.ny * self.g.nz
+        image = np.zeros((2 * nlag + 1) * n, dtype=np.float32)
+        self.ctx.check(lib().vti3d_plan_odcig(self._h, _p(souloc), _p(shotid), len(shotid),
+                                              _p(data), data_mem, int(nlag), _p(image),
+                                              MEM_HOST))
+        return image.reshape(2 * nlag + 1, n)
 
     def objfunc(self, souloc, shotid, dobs, dobs_mem=MEM_HOST):
         souloc, shotid = _f32(souloc).reshape(-1), _i32(shotid)
