@@ -173,6 +173,34 @@ def test_oracle_rtm3d_matches_reference(name):
     assert rel_l2(o, gold["image"]) < 1e-4
 
 
+def test_oracle_odcig3d_zero_lag_is_the_pinned_rtm_image():
+    """3D offset gathers (the reference's odcig3d_f target does not link, so
+    the gathers are pinned through the RTM image the reference does produce):
+    the zero-lag gather of the FP64 restatement is its RTM image bit for bit
+    on the imaged x range and zero elsewhere, that image matches the
+    reference's, and a trace-free shot gives empty gathers."""
+    name = K.RTM_CASES3D[0]
+    c = K.case3d(name)
+    s = c["s"]
+    g = s.geom()
+    n = s.nxyz
+    model = K.rtm_model3d(c)
+    dobs = load_golden(name)["dobs"]
+    img = O.rtm3d(g, *_split(model, n), s.wavelet, s.souloc, c["shotid"], s.recloc, dobs)
+    assert rel_l2(img, load_golden(f"{name}_rtm")["image"]) < 1e-4
+    nlag = 5
+    gat = O.odcig3d(g, *_split(model, n), s.wavelet, s.souloc, c["shotid"], s.recloc, dobs, nlag)
+    mask = np.zeros((s.nz, s.ny, s.nx), dtype=bool)
+    mask[:, :, nlag:s.nx - nlag] = True
+    mask = mask.reshape(-1)
+    np.testing.assert_array_equal(gat[nlag][mask], img[mask])
+    assert not gat[:, ~mask].any()
+    assert all(np.abs(gat[k]).max() > 0 for k in range(2 * nlag + 1))
+    empty = O.odcig3d(g, *_split(model, n), s.wavelet, s.souloc, c["shotid"], s.recloc,
+                      np.zeros_like(dobs), nlag)
+    assert not empty.any()
+
+
 @pytest.mark.parametrize("name", K.RTM_CASES2D)
 def test_oracle_rtm2d_matches_reference(name):
     """rtm_f restated (FP64) against the reference's own image."""
