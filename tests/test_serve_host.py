@@ -118,6 +118,26 @@ def test_trial_models_keep_c13_inside_the_stable_range():
     np.testing.assert_allclose(out[n:2 * n], [0.0, 5.0, lim, lim, -lim], rtol=1e-6)
 
 
+def test_trial_steps_that_break_the_leapfrog_bound_are_shortened():
+    """A step whose trial model would violate dt^2 lambda_max < 4 is halved
+    on the host before any gradient is evaluated."""
+    g = V.geom3d(12, 10, 8, 10, 2, 10.0, 10.0, 10.0, 1e-3, 2e-3)
+    n = 12 * 10 * 8
+    v2 = np.float32(3700.0 ** 2)  # dt^2 lambda_max near 3, so doubling breaks the bound
+    c = np.concatenate([np.full(n, 1.2 * v2), np.full(n, 1.05 * v2), np.full(n, v2)]).astype(
+        np.float32)
+    base = V.cfl_number(g, c[:n], c[n:2 * n], c[2 * n:])
+    assert 2.5 < base < 3.9
+    drv = SV.FwiDriver(g, c, None, [], iterations=1)
+    drv.x, drv.p, drv.alpha = c, c.copy(), 1.0  # alpha = 1 would double every stiffness
+    t = drv.stable_trial()
+    assert drv.alpha < 1.0
+    assert V.cfl_number(g, t[:n], t[n:2 * n], t[2 * n:]) < drv.cfl_limit
+    drv.p, drv.alpha = 1e-3 * c, 1.0  # a small step is kept as it is
+    np.testing.assert_array_equal(drv.stable_trial(), drv.project(c + np.float32(1e-3) * c))
+    assert drv.alpha == 1.0
+
+
 def test_window_gradients_are_stacked_without_their_frames():
     """Window (x0, y0, nx, ny) contributes x in [x0 + pad, x0 + nx - pad) and
     likewise in y, except that a frame lying on the model's edge counts."""

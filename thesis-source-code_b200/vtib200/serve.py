@@ -20,8 +20,8 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import (JOB_GRADIENT, JOB_MODEL, OPT_FULL_STEPS, Context, Engine3d, Plan3d, geom3d,
-               get_boundary, objFuncGradient_f, synthetic_f, vepsdel_to_cij)
+from . import (JOB_GRADIENT, JOB_MODEL, OPT_FULL_STEPS, Context, Engine3d, Plan3d, cfl_number,
+               geom3d, get_boundary, objFuncGradient_f, synthetic_f, vepsdel_to_cij)
 from . import synth as S
 
 
@@ -135,7 +135,9 @@ class FwiDriver:
     the accepted misfits never increase. A step never changes a stiffness by
     more than `max_step` of the largest one, and with `project_stiffness`
     every trial model keeps |c13| <= 0.99 sqrt(c11 c33) (beyond it the VTI
-    system is not hyperbolic and wavefields grow without bound)."""
+    system is not hyperbolic and wavefields grow without bound) and a step
+    whose trial model breaks the leapfrog bound (dt^2 lambda_max >=
+    `cfl_limit`, vti3d_cfl_number) is halved before it is evaluated."""
     g: object
     model: np.ndarray
     wavelet: np.ndarray
@@ -147,6 +149,7 @@ class FwiDriver:
     misfits: list = field(default_factory=list)
     step0: float = 0.0
     project_stiffness: bool = True
+    cfl_limit: float = 3.9
 
     def __post_init__(self):
         self.s_hist, self.y_hist = [], []
@@ -233,6 +236,19 @@ class FwiDriver:
         out[n:2 * n] = np.clip(c13, -lim, lim)
         return out
 
+    def stable_trial(self):
+        """x + alpha p projected; alpha halved (at most 30 times) while the
+        trial model breaks the leapfrog bound."""
+        for _ in range(30):
+            t = self.project(self.x + np.float32(self.alpha) * self.p)
+            if not self.project_stiffness or self.g is None:
+                return t
+            n = t.size // 3
+            if cfl_number(self.g, t[:n], t[n:2 * n], t[2 * n:]) < self.cfl_limit:
+                return t
+            self.alpha *= 0.5
+        return t
+
     def first(self):
         self.trial = self.x
         return self.jobs(self.x)
@@ -256,7 +272,7 @@ class FwiDriver:
             cap = self.max_step * float(np.abs(self.x).max())
             pmax = float(np.abs(self.p).max())
             self.alpha = (min(1.0, cap / pmax) if pmax > 0 else 1.0) * 0.125 ** self.restarts
-            self.trial = self.project(self.x + np.float32(self.alpha) * self.p)
+            self.trial = self.stable_trial()
             return self.jobs(self.trial)
         if self.f_cur is None or f < self.f_cur:
             if self.f_cur is not None:
@@ -280,7 +296,7 @@ class FwiDriver:
         else:
             self.alpha *= 0.5
             self.halvings += 1
-        self.trial = self.project(self.x + np.float32(self.alpha) * self.p)
+        self.trial = self.stable_trial()
         return self.jobs(self.trial)
 
 
