@@ -30,6 +30,20 @@ def test_binding_declares_only_header_symbols():
     assert set(V.exported_symbols()) <= set(header_functions())
 
 
+@pytest.mark.parametrize("lang", [("gcc", "c", "-std=c99"), ("g++", "c++", "-std=c++17")])
+def test_c_abi_header_is_plain_c(lang, tmp_path):
+    """include/vti_b200.h compiles as strict C99 (pedantic, warnings as
+    errors) and as C++: no C++ or CUDA types in the boundary."""
+    import subprocess
+    cc, x, std = lang
+    src = tmp_path / "use.c"
+    src.write_text('#include "vti_b200.h"\nint main(void) { return VTI_OK; }\n')
+    r = subprocess.run([cc, std, "-Wall", "-Wextra", "-pedantic", "-Werror", "-fsyntax-only",
+                        "-x", x, "-I", str(ROOT / "include"), str(src)],
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr[-2000:]
+
+
 @pytest.mark.parametrize("dim", ["3d", "2d"])
 def test_reference_harness_links_against_the_shim(dim, tmp_path):
     """The harness that drives the reference's C++ entry points and operator
