@@ -16,10 +16,10 @@ class GNHessianOpCij : public Operator {
                  int nx, int nz, int nt, int npad, float dx, float dz, float dt, float rate,
                  float ot, float wbottom, float* m)
       : Operator(3 * (nx + 2 * npad) * (nz + 2 * npad), 3 * (nx + 2 * npad) * (nz + 2 * npad)),
-        _d0(d0), _c11(c11), _c13(c13), _c33(c33), _c110(c110), _c130(c130), _c330(c330),
-        _wavelet(wavelet), _sloc(sloc), _rloc(rloc), _taper(taper), _ns(ns), _nr(nr), _nx(nx),
-        _nz(nz), _nt(nt), _npad(npad), _dx(dx), _dz(dz), _dt(dt), _rate(rate), _ot(ot),
-        _wbottom(wbottom), _m(m) {}
+        _sloc(sloc), _rloc(rloc), _d0(d0), _c11(c11), _c13(c13), _c33(c33), _wavelet(wavelet),
+        _taper(taper), _m(m), _ns(ns), _nr(nr), _nx(nx), _nz(nz), _nt(nt), _npad(npad),
+        _c110(c110), _c130(c130), _c330(c330), _dx(dx), _dz(dz), _dt(dt), _rate(rate), _ot(ot),
+        _wbottom(wbottom) {}
   void forward(bool add, const float* model, float* data);
   void adjoint(bool add, float* model, const float* data);
   int *_sloc, *_rloc;
@@ -35,10 +35,10 @@ class GNHessianOpVEpsDel : public Operator {
                      float* taper, int nx, int nz, int nt, int npad, float dx, float dz, float dt,
                      float rate, float ot, float wbottom, float* m)
       : Operator(3 * (nx + 2 * npad) * (nz + 2 * npad), 3 * (nx + 2 * npad) * (nz + 2 * npad)),
-        _d0(d0), _v(v), _eps(eps), _del(del), _v0(v0), _eps0(eps0), _del0(del0),
-        _wavelet(wavelet), _sloc(sloc), _rloc(rloc), _taper(taper), _ns(ns), _nr(nr), _nx(nx),
-        _nz(nz), _nt(nt), _npad(npad), _dx(dx), _dz(dz), _dt(dt), _rate(rate), _ot(ot),
-        _wbottom(wbottom), _m(m) {}
+        _sloc(sloc), _rloc(rloc), _d0(d0), _v(v), _eps(eps), _del(del), _wavelet(wavelet),
+        _taper(taper), _m(m), _ns(ns), _nr(nr), _nx(nx), _nz(nz), _nt(nt), _npad(npad), _v0(v0),
+        _eps0(eps0), _del0(del0), _dx(dx), _dz(dz), _dt(dt), _rate(rate), _ot(ot),
+        _wbottom(wbottom) {}
   void forward(bool add, const float* model, float* data);
   void adjoint(bool add, float* model, const float* data);
   int *_sloc, *_rloc;

@@ -44,6 +44,18 @@ def test_c_abi_header_is_plain_c(lang, tmp_path):
     assert r.returncode == 0, r.stderr[-2000:]
 
 
+@pytest.mark.parametrize("header", sorted(p.name for p in (ROOT / "include").glob("*.h")))
+def test_every_header_compiles_on_its_own(header, tmp_path):
+    """Each header of include/ is self-contained C++ (warnings as errors)."""
+    import subprocess
+    src = tmp_path / "use.cpp"
+    src.write_text(f'#include "{header}"\nint main() {{ return 0; }}\n')
+    r = subprocess.run(["g++", "-std=c++17", "-Wall", "-Wextra", "-Werror", "-fsyntax-only",
+                        "-I", str(ROOT / "include"), str(src)],
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr[-2000:]
+
+
 @pytest.mark.parametrize("dim", ["3d", "2d"])
 def test_reference_harness_links_against_the_shim(dim, tmp_path):
     """The harness that drives the reference's C++ entry points and operator
