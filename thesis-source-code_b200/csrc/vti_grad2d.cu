@@ -35,9 +35,6 @@ __device__ __forceinline__ float lap9(const float* r, int s) {
 
 struct Grid2 {
   int nnx, nnz;
-  __device__ bool inner(int ix, int iz) const {
-    return ix >= kHalo && ix < nnx - kHalo && iz >= kHalo && iz < nnz - kHalo;
-  }
 };
 
 // Forward level of the background (and Born) field, forwardC semantics

@@ -256,18 +256,6 @@ __global__ void __launch_bounds__(kOdcigTX)
   }
 }
 
-int zslab_for(vti_ctx* ctx, const Dims3& d, int tiles, int ctas_per_sm) {
-  // choose the number of z slabs so the grid fills the GPU a few times over
-  int target = ctx->sm_count * ctas_per_sm * 4;
-  int nslab = (target + tiles - 1) / tiles;
-  int maxslab = (d.nz + 3) / 4;
-  if (nslab > maxslab) nslab = maxslab;
-  if (nslab < 1) nslab = 1;
-  int zs = (d.nz + nslab - 1) / nslab;
-  zs = (zs + 3) & ~3;
-  return zs;
-}
-
 }  // namespace
 
 int launch_odcig3d(vti_ctx* ctx, const Dims3& d, const float* sx, const float* sz,
