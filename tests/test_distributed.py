@@ -5,7 +5,6 @@ import os
 import socket
 
 import numpy as np
-import pytest
 import torch.multiprocessing as mp
 
 from vtib200.distributed import shard
