@@ -86,6 +86,22 @@ def test_lbfgs_step_is_capped_and_nonfinite_trials_are_rejected():
     assert np.allclose(nxt[0] - drv.x, 0.5 * (before - drv.x))
 
 
+def test_lbfgs_first_step_without_step0_moves_by_the_cap():
+    """With step0 left at its default the first direction is scaled to the
+    max_step cap, so the first trial differs from the starting model."""
+    n = 8
+    A = np.eye(n)
+    xs = np.full(n, 3.0)
+    x0 = np.ones(n, dtype=np.float32)
+    drv = _Quadratic(None, x0, None, [None], iterations=2, max_step=0.05,
+                     project_stiffness=False)
+    jobs = drv.first()
+    jobs = drv.update([_evaluate(j, A, xs, 1) for j in jobs])
+    step = np.abs(jobs[0] - x0).max()
+    assert 0 < step <= 0.05 * np.abs(x0).max() * (1 + 1e-6)
+    assert np.isclose(step, 0.05, rtol=1e-5)
+
+
 def test_lbfgs_never_accepts_an_increase():
     """Trials that all raise the misfit: after max_halvings the driver keeps
     the model (the misfit history repeats, never rises) and restarts from

@@ -77,3 +77,75 @@ def test_noalloc_rejects_calls_beyond_its_array(ctx):
     # the context stays usable
     s = K.case2d("g2_a")["s"]
     assert np.abs(_traces(ctx, "vti2d_synthetic_noalloc", s.geom(), s)).max() > 0
+
+
+def _big_case(nx=980, nz=980, npad=10, nt=40, nrec=10):
+    """A padded 1000 x 1000 grid: its 8 volumes (32 MB) are larger than any
+    2D scratch the other tests grow, and still fit the static array."""
+    n = (nx + 2 * npad) * (nz + 2 * npad)
+    c33 = np.full(n, 4.0e6, dtype=np.float32)
+    c11 = np.float32(1.2) * c33
+    c13 = np.float32(1.05) * c33
+    taper = np.ones(n, dtype=np.float32)
+    wavelet = np.zeros(nt, dtype=np.float32)
+    wavelet[:8] = np.hanning(8)
+    sloc = np.array([500, 20, nrec, 0], dtype=np.int32)
+    rloc = np.stack([np.arange(400, 400 + 10 * nrec, 10), np.full(nrec, 20)], 1)
+    rloc = rloc.astype(np.int32).reshape(-1)
+    g = V.Geom2d(nx=nx, nz=nz, nt=nt, npad=npad, dx=10.0, dz=10.0, dt=1e-3, rate=2e-3, ot=0.0)
+    return g, (c11, c13, c33, wavelet, sloc, rloc, taper), nrec
+
+
+def _call(ctx, g, arrays, nrec, rows):
+    c11, c13, c33, wavelet, sloc, rloc, taper = arrays
+    out = np.zeros(rows * nrec, dtype=np.float32)
+    st = V.lib().vti2d_synthetic_noalloc(ctx.handle, C.byref(g), V._p(c11), V._p(c13),
+                                         V._p(c33), V._p(wavelet), V._p(sloc), 1, V._p(rloc),
+                                         nrec, V._p(taper), V._p(out))
+    return st, out
+
+
+def test_noalloc_allocates_no_device_memory(ctx):
+    """The point of the entry point: after the first call on the device (which
+    loads the kernels and looks up the array's address), a call on a grid
+    larger than any earlier one leaves the device's free memory unchanged."""
+    cudart = C.CDLL("libcudart.so.12")
+    free, total = C.c_size_t(0), C.c_size_t(0)
+
+    def free_bytes():
+        assert cudart.cudaMemGetInfo(C.byref(free), C.byref(total)) == 0
+        return free.value
+
+    g, arrays, nrec = _big_case()
+    rows = (g.nt - 1) // 2 + 1
+    st, warm = _call(ctx, g, arrays, nrec, rows)
+    assert st == V.VTI_OK
+    before = free_bytes()
+    st, again = _call(ctx, g, arrays, nrec, rows)
+    after = free_bytes()
+    assert st == V.VTI_OK
+    np.testing.assert_array_equal(again, warm)
+    # an allocating path would take >= 32 MB here
+    assert abs(before - after) < (1 << 21), (before, after)
+
+
+def test_noalloc_rejects_a_record_before_time_zero(ctx):
+    """|ot| beyond the whole record leaves no trace rows: rejected before any
+    work is queued, and the context stays usable."""
+    s = K.case2d("g2_a")["s"]
+    g = s.geom()
+    g.ot = -float(g.nt + 50) * g.dt
+    sloc = V._i32(s.sloc).reshape(-1)
+    rloc = V._i32(s.rloc).reshape(-1)
+    out = np.zeros(4, dtype=np.float32)
+    for name in ("vti2d_synthetic_noalloc", "vti2d_synthetic"):
+        st = getattr(V.lib(), name)(ctx.handle, C.byref(g), V._p(V._f32(s.c11)),
+                                    V._p(V._f32(s.c13)), V._p(V._f32(s.c33)),
+                                    V._p(V._f32(s.wavelet)), V._p(sloc), sloc.size // 4,
+                                    V._p(rloc), rloc.size // 2, V._p(V._f32(s.taper)),
+                                    V._p(out))
+        assert st == V.VTI_ERR_ARG, name
+        assert b"before time zero" in V.lib().vti_ctx_last_error(ctx.handle)
+    g2 = s.geom()
+    assert np.abs(_traces(ctx, "vti2d_synthetic_noalloc", g2, s)).max() > 0
+

@@ -450,13 +450,16 @@ struct ResShape {
   size_t smem = 0;
 };
 bool attr_res[64] = {};
+std::mutex attr_res_mu;  // first calls from several threads set the attributes once
 
 bool resident_shape(vti_ctx* ctx, int nnx, int nnz, ResShape* out) {
   constexpr size_t kMaxSmem = 227 * 1024;
   const int NP = (nnx - 2 * kHalo + 1) / 2, rows = nnz - 2 * kHalo;
   const int W = (nnx + 1) & ~1;
   if (NP < 1 || rows < 4 || NP > kResThreads) return false;
-  if (ctx->device < 64 && !attr_res[ctx->device]) {
+  if (ctx->device < 0 || ctx->device >= 64) return false;
+  std::lock_guard<std::mutex> lk(attr_res_mu);
+  if (!attr_res[ctx->device]) {
     if (cudaFuncSetAttribute(k_synth2d_resident, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)kMaxSmem) != cudaSuccess ||
         cudaFuncSetAttribute(k_synth2d_resident,
@@ -572,6 +575,8 @@ int run2d(vti_ctx* ctx, const vti2d_geom* g, const float* c11, const float* c13,
   // model/taper + 4 wavefields + nt amplitudes, then the flat receiver
   // indices, then the output rows
   const long long nrows_out = mode == 0 ? (g->nt - ntNeg - 1) / ratio + 1 : 0;
+  if (mode == 0 && nrows_out < 1)
+    return fail(ctx, VTI_ERR_ARG, "the whole record lies before time zero (|ot| too large)");
   const int nrec = mode == 0 ? std::max(nri, 0) : 0;
   const size_t nbuf = 8 * (size_t)nnxz + g->nt;
   const size_t n_ints = (size_t)nrec;
@@ -740,6 +745,8 @@ int synth2d_resident(vti_ctx* ctx, const vti2d_geom* g, const float* c11, const 
     if (t >= 0.f && (it - ntNeg) % ratio == 0) hi[it] = (it - ntNeg) / ratio;
   }
   const long long nrows = (g->nt - ntNeg - 1) / ratio + 1;
+  if (nrows < 1)
+    return fail(ctx, VTI_ERR_ARG, "the whole record lies before time zero (|ot| too large)");
   // ints: trace rows, per-shot table, receiver columns, receiver rows
   for (int is = 0; is < ns; ++is) {
     const int* sh = sloc + 4 * is;
@@ -919,6 +926,8 @@ extern "C" int vti2d_synthetic_noalloc(vti_ctx* ctx, const vti2d_geom* g, const 
   if (ratio < 1) return fail(ctx, VTI_ERR_ARG, "rate < dt");
   const int ntNeg = (int)std::round(std::fabs(g->ot) / dt);
   const long long rows = (g->nt - ntNeg - 1) / ratio + 1;
+  if (rows < 1)
+    return fail(ctx, VTI_ERR_ARG, "the whole record lies before time zero (|ot| too large)");
   // validate every shot and size the largest before queuing anything
   long long max_nri = 0;
   for (int is = 0; is < ns; ++is) {
@@ -942,37 +951,57 @@ extern "C" int vti2d_synthetic_noalloc(vti_ctx* ctx, const vti2d_geom* g, const 
                   need, kNoAllocFloats);
     return fail(ctx, VTI_ERR_ARG, msg);
   }
+  // the caller's current device is restored on every return
+  int caller_dev = -1;
+  VTI_CUDA(ctx, cudaGetDevice(&caller_dev));
+  struct DeviceRestore {
+    int dev;
+    ~DeviceRestore() {
+      if (dev >= 0) cudaSetDevice(dev);
+    }
+  } restore{caller_dev};
   VTI_CUDA(ctx, cudaSetDevice(ctx->device));
   float* buf = nullptr;
   int st = noalloc_scratch(ctx, &buf);
   if (st != VTI_OK) return st;
+  cudaStream_t sm = ctx->stream;
+  // From the first queued operation on, an error return first waits for the
+  // work already queued on the shared array, so no call returns while its
+  // copies or kernels can still touch it.
+#define NK(call)                                \
+  do {                                          \
+    cudaError_t e_ = (call);                    \
+    if (e_ != cudaSuccess) {                    \
+      st = cuda_check(ctx, e_, #call);          \
+      cudaStreamSynchronize(sm);                \
+      return st;                                \
+    }                                           \
+  } while (0)
   float *dc11 = buf, *dc13 = dc11 + nnxz, *dc33 = dc13 + nnxz, *dtap = dc33 + nnxz;
   float* w[4] = {dtap + nnxz, dtap + 2 * nnxz, dtap + 3 * nnxz, dtap + 4 * nnxz};
   float* amps = dtap + 5 * nnxz;
   int* d_ridx = reinterpret_cast<int*>(amps + g->nt);
   float* d_rows = amps + g->nt + max_nri;
-  cudaStream_t sm = ctx->stream;
-  VTI_CUDA(ctx, cudaMemcpyAsync(dc11, c11, nnxz * 4, cudaMemcpyHostToDevice, sm));
-  VTI_CUDA(ctx, cudaMemcpyAsync(dc13, c13, nnxz * 4, cudaMemcpyHostToDevice, sm));
-  VTI_CUDA(ctx, cudaMemcpyAsync(dc33, c33, nnxz * 4, cudaMemcpyHostToDevice, sm));
-  VTI_CUDA(ctx, cudaMemcpyAsync(dtap, taper, nnxz * 4, cudaMemcpyHostToDevice, sm));
+  NK(cudaMemcpyAsync(dc11, c11, nnxz * 4, cudaMemcpyHostToDevice, sm));
+  NK(cudaMemcpyAsync(dc13, c13, nnxz * 4, cudaMemcpyHostToDevice, sm));
+  NK(cudaMemcpyAsync(dc33, c33, nnxz * 4, cudaMemcpyHostToDevice, sm));
+  NK(cudaMemcpyAsync(dtap, taper, nnxz * 4, cudaMemcpyHostToDevice, sm));
   std::vector<float> h_amp(g->nt, 0.f);
   for (int it = 2; it < g->nt; ++it) h_amp[it] = dt2 * wavelet[it - 1];
-  VTI_CUDA(ctx, cudaMemcpyAsync(amps, h_amp.data(), g->nt * 4, cudaMemcpyHostToDevice, sm));
+  NK(cudaMemcpyAsync(amps, h_amp.data(), g->nt * 4, cudaMemcpyHostToDevice, sm));
   const float idx2 = 1.f / (g->dx * g->dx), idz2 = 1.f / (g->dz * g->dz);
   const dim3 block(BX, BZ), grid((nnx - 8 + BX - 1) / BX, (nnz - 8 + BZ - 1) / BZ);
   std::vector<int> ridx;
   for (int is = 0; is < ns; ++is) {
     const int* s = sloc + 4 * is;
     const int slocxz = s[0] + s[1] * nnx, nri = s[2], ir0 = s[3];
-    VTI_CUDA(ctx, cudaMemsetAsync(w[0], 0, 4 * nnxz * 4, sm));  // wavefields start at zero
+    NK(cudaMemsetAsync(w[0], 0, 4 * nnxz * 4, sm));  // wavefields start at zero
     if (nri > 0) {
       ridx.resize(nri);
       for (int ir = 0; ir < nri; ++ir)
         ridx[ir] = rloc[2 * (ir0 + ir)] + rloc[2 * (ir0 + ir) + 1] * nnx;
-      VTI_CUDA(ctx, cudaMemcpyAsync(d_ridx, ridx.data(), nri * sizeof(int),
-                                    cudaMemcpyHostToDevice, sm));
-      VTI_CUDA(ctx, cudaMemsetAsync(d_rows, 0, (size_t)rows * nri * 4, sm));  // row 0 stays 0
+      NK(cudaMemcpyAsync(d_ridx, ridx.data(), nri * sizeof(int), cudaMemcpyHostToDevice, sm));
+      NK(cudaMemsetAsync(d_rows, 0, (size_t)rows * nri * 4, sm));  // row 0 stays 0
     }
     // time level 1: source then taper (synthetic_f.cu:86-89)
     k_init2d<<<1, 1, 0, sm>>>(w[2], w[3], slocxz, dt2 * wavelet[0], taper[slocxz]);
@@ -995,11 +1024,12 @@ extern "C" int vti2d_synthetic_noalloc(vti_ctx* ctx, const vti2d_geom* g, const 
       std::swap(p0, p1);
       std::swap(q0, q1);
     }
-    VTI_CUDA(ctx, cudaGetLastError());
+    NK(cudaGetLastError());
     if (nri > 0)  // the caller's receiver-fastest layout, as vti2d_synthetic
-      VTI_CUDA(ctx, cudaMemcpy2DAsync(data + ir0, (size_t)nr * 4, d_rows, (size_t)nri * 4,
-                                      (size_t)nri * 4, rows, cudaMemcpyDeviceToHost, sm));
+      NK(cudaMemcpy2DAsync(data + ir0, (size_t)nr * 4, d_rows, (size_t)nri * 4,
+                           (size_t)nri * 4, rows, cudaMemcpyDeviceToHost, sm));
   }
-  VTI_CUDA(ctx, cudaStreamSynchronize(sm));
+  NK(cudaStreamSynchronize(sm));
+#undef NK
   return VTI_OK;
 }

@@ -29,6 +29,7 @@
 // read-modify-write per point per block instead of a compensation term per
 // step).
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <vector>
 
@@ -665,12 +666,14 @@ struct VolB {
   TileMaps m;
 };
 
-bool attr_born[64] = {}, attr_adj[64] = {};
+// once per device and kernel (atomic flags: first calls may come from
+// several host threads)
+std::atomic<bool> attr_born[64], attr_adj[64];
 
-int smem_attr(vti_ctx* ctx, const void* kern, bool* done) {
-  if (ctx->device < 64 && done[ctx->device]) return VTI_OK;
-  VTI_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, G_SMEM));
-  if (ctx->device < 64) done[ctx->device] = true;
+int smem_attr(vti_ctx* ctx, const void* kern, std::atomic<bool>* done, int bytes = G_SMEM) {
+  if (ctx->device < 64 && done[ctx->device].load(std::memory_order_acquire)) return VTI_OK;
+  VTI_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  if (ctx->device < 64) done[ctx->device].store(true, std::memory_order_release);
   return VTI_OK;
 }
 
@@ -822,14 +825,13 @@ int launch_adj(GnState& S, int im, int cur, int slot) {
   return VTI_OK;
 }
 
-bool attr_adjb[64] = {};
+std::atomic<bool> attr_adjb[64];
 
 int launch_adj_b16(GnState& S, int im, int cur, int slot) {
   vti_ctx* ctx = S.ctx;
-  if (!(ctx->device < 64 && attr_adjb[ctx->device])) {
-    VTI_CUDA(ctx, cudaFuncSetAttribute(k_adj3d_b16, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       A_SMEM));
-    if (ctx->device < 64) attr_adjb[ctx->device] = true;
+  {
+    const int st = smem_attr(ctx, (const void*)k_adj3d_b16, attr_adjb, A_SMEM);
+    if (st != VTI_OK) return st;
   }
   const int nx_ = 1 - cur;
   const VolB& ax = S.segb[2 * slot];

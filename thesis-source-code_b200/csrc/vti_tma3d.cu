@@ -27,6 +27,7 @@
 // the reference is lib/vti-fwi-3d/gpu/kernel3d.cu:3-74,222-298 and
 // abc3d.cu:82-126.
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <vector>
 
@@ -767,11 +768,13 @@ Sched sched_with_seg(const Dims3& d, int seg) {
   return s;
 }
 
+// Once per device and kernel; the flags are atomic because first calls may
+// come from several host threads (setting the attribute twice is harmless).
 template <typename K>
-int set_smem_attr(vti_ctx* ctx, K kern, int bytes, bool* done) {
-  if (ctx->device < 64 && done[ctx->device]) return VTI_OK;
+int set_smem_attr(vti_ctx* ctx, K kern, int bytes, std::atomic<bool>* done) {
+  if (ctx->device < 64 && done[ctx->device].load(std::memory_order_acquire)) return VTI_OK;
   VTI_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-  if (ctx->device < 64) done[ctx->device] = true;
+  if (ctx->device < 64) done[ctx->device].store(true, std::memory_order_release);
   return VTI_OK;
 }
 
@@ -790,8 +793,7 @@ FwdCommon fwd_common(const Dims3& d, const Sched& sc, const Damping* damp, float
   return c;
 }
 
-bool attr_fwd[3][64] = {}, attr_bwd[2][64] = {}, attr_fwd_batch[64] = {},
-     attr_bwd_batch[64] = {};
+std::atomic<bool> attr_fwd[3][64], attr_bwd[2][64], attr_fwd_batch[64], attr_bwd_batch[64];
 
 }  // namespace
 

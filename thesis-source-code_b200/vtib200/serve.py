@@ -218,7 +218,10 @@ class FwiDriver:
             s, y = self.s_hist[-1], self.y_hist[-1]
             q *= np.float32(_dot(s, y) / _dot(y, y))
         else:
-            q *= np.float32(self.step0 / max(float(np.abs(q).max()), 1e-300))
+            # no curvature pair yet: the first step's largest change is step0,
+            # or (step0 <= 0) the max_step cap relative to the largest stiffness
+            s0 = self.step0 if self.step0 > 0 else self.max_step * float(np.abs(self.x).max())
+            q *= np.float32(s0 / max(float(np.abs(q).max()), 1e-300))
         for (s, y), a in zip(zip(self.s_hist, self.y_hist), reversed(al)):
             b = _dot(y, q) / _dot(y, s)
             q += np.float32(a - b) * s
