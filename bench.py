@@ -33,20 +33,23 @@ import numpy as np
 
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT / "thesis-source-code_b200"))
+# the oracle (test infrastructure) is used only by the cpu_baseline, error and
+# reference legs below, never inside the timed GPU region
+sys.path.insert(0, str(ROOT / "oracle"))
 
-CONFIGS = {
-    # name: survey3d kwargs
-    "gradient400": dict(nx=400, ny=400, nz=200, nt=3000, npad=40, d=12.5, dt=1e-3, rate=4e-3,
-                        freq=12.0, rec_step=2, rec_start=0, rec_depth=25.0, src_depth=25.0,
-                        smooth_m=250.0),
-    "small": dict(nx=128, ny=128, nz=96, nt=402, npad=16, d=12.5, dt=1e-3, rate=4e-3,
-                  freq=12.0, rec_step=2, rec_start=0, rec_depth=25.0, src_depth=25.0,
-                  smooth_m=100.0),
-    # profiling case: every volume (34 MB) x 14 inputs exceeds the 126 MB L2
-    "mid": dict(nx=256, ny=256, nz=128, nt=130, npad=24, d=12.5, dt=1e-3, rate=4e-3,
-                freq=12.0, rec_step=2, rec_start=0, rec_depth=25.0, src_depth=25.0,
-                smooth_m=100.0),
-}
+
+def _configs():
+    import vtib200.synth as S
+    return {
+        # name: survey3d kwargs
+        "gradient400": dict(S.GRADIENT400),
+        "small": dict(S.GRADIENT400, nx=128, ny=128, nz=96, nt=402, npad=16, smooth_m=100.0),
+        # profiling case: every volume (34 MB) x 14 inputs exceeds the 126 MB L2
+        "mid": dict(S.GRADIENT400, nx=256, ny=256, nz=128, nt=130, npad=24, smooth_m=100.0),
+    }
+
+
+CONFIGS = _configs()
 BWD_BYTES_PER_POINT = 84  # 14 reads + 7 writes of FP32 per point (fused backward)
 FWD_BYTES_PER_POINT = 36  # 7 reads + 2 writes
 
@@ -105,29 +108,117 @@ class ClockSampler:
                 "samples": len(self.rows)}
 
 
-def make_inputs(cfg, rank):
-    import vtib200 as V
+def make_inputs(cfg, rank, nt=None):
     import vtib200.synth as S
     kw = dict(CONFIGS[cfg])
-    nx, ny = kw["nx"], kw["ny"]
-    # each rank's shot at its own position (weak scaling)
-    off = [(0, 0), (40, 0), (0, 40), (40, 40), (-40, 0), (0, -40), (-40, -40), (40, -40)]
-    dx, dy = off[rank % len(off)]
-    kw["src_xy"] = (nx // 2 + dx * nx // 400, ny // 2 + dy * ny // 400)
-    s = S.survey3d(**kw)
-    padb, randb = S.boundaries3d(s)
-    tv, te, td = s.extra["true"]
-    ctrue = s.cij(tv, te, td)
-    n = s.nxyz
-    # observed data use the pad boundary of the true model in the sponge pass
-    ctrue = np.concatenate([V.put_boundary(padb[k * s.nb:(k + 1) * s.nb],
-                                           ctrue[k * n:(k + 1) * n], s.nx, s.ny, s.nz, s.npad)
-                            for k in range(3)])
-    return s, s.cij(), ctrue, padb, randb
+    if nt:
+        kw["nt"] = nt
+    return S.gradient_inputs(kw, rank)
 
 
 def levels(g, flags):
     return g.nt - 1 if flags & 1 else 1 + 64 * ((g.nt - 2) // 64)
+
+
+GRADIENT_METRIC = "3D VTI fwd+adjoint gradient throughput (grid-point updates/s)"
+CPU_SAMPLE_NT = 66   # time samples of one CPU sample of the gradient (65 levels)
+CHECK_NT = 130       # time samples of the full-grid check against the FP64 oracle
+
+
+def gradient_config(cfg, s, M, nrec):
+    """The workload description both arms print (identical object)."""
+    return {"workload": f"3D VTI L2-misfit gradient, {cfg}: {s.nx}x{s.ny}x{s.nz} grid "
+                        f"(pad {s.npad}), nt={s.nt}, {M} levels, {nrec} receivers, "
+                        "1 shot per GPU",
+            "grid": [s.nx, s.ny, s.nz], "nt": s.nt, "levels": M, "receivers": nrec,
+            "shots_per_gpu": 1,
+            "points": "nx*ny*nz per wavefield-pair update, 4 updates per level (pass 1, "
+                      "pass 2, pass 3 source and adjoint); the 4-cell x/y frame the scheme "
+                      "never updates is 4% of them",
+            "l2": "wavefields (133 MB each) larger than L2 (126 MB); no flush"}
+
+
+def shortened(s, nt):
+    """The same survey over its first nt time samples (the Ricker wavelet is
+    evaluated per sample, so it is the first nt values)."""
+    import dataclasses
+    return dataclasses.replace(s, nt=nt, wavelet=np.ascontiguousarray(s.wavelet[:nt]))
+
+
+def first_samples(dobs, nrec, nnt_full, nnt):
+    """Trace-major traces ([receiver][sample]) cut to their first nnt samples."""
+    return np.ascontiguousarray(np.asarray(dobs, dtype=np.float32).reshape(nrec, nnt_full)
+                                [:, :nnt]).reshape(-1)
+
+
+class OracleGeom:
+    """Geometry attributes the oracle reads (no library needed)."""
+
+    def __init__(self, s):
+        self.nx, self.ny, self.nz, self.nt, self.npad = s.nx, s.ny, s.nz, s.nt, s.npad
+        self.ox = self.oy = self.oz = s.o
+        self.ot = 0.0
+        self.dx = self.dy = self.dz = s.d
+        self.dt, self.sampling_rate = s.dt, s.rate
+
+
+def oracle_gradient_sample(s, cstart, padb, randb, dobs):
+    """One timed CPU sample: the FP32 oracle's whole three-pass gradient
+    (REFERENCE mode, all levels) of survey s on its full grid, all host
+    threads. Returns (Gpts/s counted as the GPU arm counts, seconds)."""
+    import oracle as O
+    g = OracleGeom(s)
+    t0 = time.perf_counter()
+    O.gradient3d(g, cstart, padb, randb, s.wavelet, s.souloc, [0], s.recloc, dobs,
+                 dtype=np.float32, full_steps=True)
+    sec = time.perf_counter() - t0
+    M = s.nt - 1
+    return 4.0 * (M - 1) * s.nxyz / sec / 1e9, sec
+
+
+def cpu_sample_desc(s, threads):
+    return (f"the FP32 oracle's whole gradient (pass 1 with traces and misfit, pass 2, "
+            f"pass 3) on the full {s.nx}x{s.ny}x{s.nz} grid over the first {s.nt} time "
+            f"samples ({s.nt - 1} levels) of the same shot, {threads} OpenMP threads")
+
+
+def oracle_errors(ctx, s, cstart, ctrue, padb, randb, nt):
+    """GPU vs the FP64 oracle on the full grid over the first nt samples:
+    modeled traces, misfit and the three gradients through the host-buffer
+    C ABI (VTI_OPT_FULL_STEPS); the FP32 oracle's own error against FP64 is
+    the FP32 noise level for comparison."""
+    import oracle as O
+    import vtib200 as V
+    t0 = time.perf_counter()
+    sh = shortened(s, nt)
+    g = sh.geom()
+    n = sh.nxyz
+    flags = V.OPT_FULL_STEPS
+    sp = lambda c: (c[:n], c[n:2 * n], c[2 * n:])  # noqa: E731
+    dobs = V.modelDataCij3d_f(ctx, g, sh.souloc, [0], sh.recloc, sh.wavelet, *sp(ctrue),
+                              flags=flags)
+    dmod = V.modelDataCij3d_f(ctx, g, sh.souloc, [0], sh.recloc, sh.wavelet, *sp(cstart),
+                              flags=flags)
+    fg, mis = V.objFuncGradientCij3d_f(ctx, g, sh.souloc, [0], sh.recloc, sh.wavelet, cstart,
+                                       padb, randb, dobs, flags=flags)
+    og = OracleGeom(sh)
+    o64, m64 = O.gradient3d(og, cstart, padb, randb, sh.wavelet, sh.souloc, [0], sh.recloc,
+                            dobs, dtype=np.float64, full_steps=True, want_modeled=True)
+    o32 = O.gradient3d(og, cstart, padb, randb, sh.wavelet, sh.souloc, [0], sh.recloc, dobs,
+                       dtype=np.float32, full_steps=True)
+
+    def rl2(a, b):
+        a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+        return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+    part = lambda f, k: f[1 + k * n:1 + (k + 1) * n]  # noqa: E731
+    return {"nt": nt, "levels": nt - 1, "grid": [sh.nx, sh.ny, sh.nz],
+            "api": "vti3d_model_data_cij + vti3d_gradient_cij (host buffers)",
+            "traces_rel_l2": rl2(dmod, m64), "misfit_rel": abs(mis - o64[0]) / o64[0],
+            "gradient_rel_l2": [rl2(part(fg, k), part(o64, k)) for k in range(3)],
+            "fp32_oracle_gradient_rel_l2": [rl2(part(o32, k), part(o64, k)) for k in range(3)],
+            "tolerance": {"traces": 1e-5, "misfit": 1e-5, "gradient": 1e-4},
+            "seconds": round(time.perf_counter() - t0, 1)}
 
 
 def run_b200(args):
@@ -174,8 +265,9 @@ def run_b200(args):
         dist.barrier()
     torch.cuda.synchronize()
     launches0 = ctx.launches
-    ctx.set_timing(True)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # the timed steps run without per-kernel events; the kernel times come
+    # from one further step with events on each launch
     with ClockSampler(local) as clk:
         e0.record(stream)
         for _ in range(args.steps):
@@ -183,10 +275,13 @@ def run_b200(args):
         e1.record(stream)
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
+    launches = ctx.launches - launches0
+    ctx.set_timing(True)
+    step()
+    torch.cuda.synchronize()
     bwd_ms, bwd_n = ctx.kernel_time("bwd3d")
     fwd_ms, fwd_n = ctx.kernel_time("fwd3d")
     ctx.set_timing(False)
-    launches = ctx.launches - launches0
     if world > 1:
         t = torch.tensor([ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -201,8 +296,9 @@ def run_b200(args):
     bwd_avg = bwd_ms / max(bwd_n, 1) / 1e3
     fwd_avg = fwd_ms / max(fwd_n, 1) / 1e3
     achieved = BWD_BYTES_PER_POINT * upd / bwd_avg / 1e9 if bwd_n else None
-    # DRAM bytes per updated point from an ncu capture of a smaller grid
-    # (traffic grows with the points updated), scaled to this launch
+    # DRAM bytes per updated point from an ncu capture of in-loop launches on
+    # a smaller grid (traffic grows with the points updated), scaled to this
+    # launch
     traffic = None
     tf = ROOT / "profiles" / "k_bwd3d_tma_traffic.json"
     if tf.exists():
@@ -211,19 +307,25 @@ def run_b200(args):
     out = None
     if rank == 0:
         e2e = run_e2e(args, ctx, s, cstart, padb, randb, dobs.cpu().numpy(), flags)
-        cpu = None if args.no_cpu else cpu_baseline(s, cstart, args)
+        errors = None if args.no_check else oracle_errors(ctx, s, cstart, ctrue, padb, randb,
+                                                          CHECK_NT)
+        cpu = None
+        if not args.no_cpu:
+            import oracle as O
+            sh = shortened(s, CPU_SAMPLE_NT)
+            d_s = first_samples(dobs.cpu().numpy(), nrec, nnt, V.nnt3d(sh.geom()))
+            val, sec = oracle_gradient_sample(sh, cstart, padb, randb, d_s)
+            cpu = {"value": round(val, 4), "unit": "Gpts/s", "cores": O.max_threads(),
+                   "kind": "port", "sample": cpu_sample_desc(sh, O.max_threads()),
+                   "seconds": round(sec, 2)}
         out = {
-            "metric": "3D VTI fwd+adjoint gradient throughput (grid-point updates/s)",
+            "metric": GRADIENT_METRIC,
             "value": round(value, 3), "unit": "Gpts/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded layered VTI model + GRF, Ricker source)",
-            "config": {"workload": f"3D VTI L2-misfit gradient, {args.config}: "
-                                   f"{s.nx}x{s.ny}x{s.nz} grid (pad {s.npad}), nt={s.nt}, "
-                                   f"{M} levels, {nrec} receivers, 1 shot per GPU",
-                       "grid": [s.nx, s.ny, s.nz], "nt": s.nt, "levels": M,
-                       "receivers": nrec, "shots_per_gpu": 1, "misfit": mis,
-                       "l2": "wavefields (128 MB each) larger than L2 (126 MB)"},
+            "config": gradient_config(args.config, s, M, nrec),
+            "misfit": mis,
             "roofline": {"bound": "hbm", "kernel": "k_bwd3d_tma",
                          "achieved": round(achieved, 1) if achieved else None, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s",
@@ -231,11 +333,13 @@ def run_b200(args):
                          "traffic": traffic,
                          "bytes_per_point": BWD_BYTES_PER_POINT,
                          "avg_launch_ms": round(bwd_avg * 1e3, 4),
+                         "timing": "CUDA events around each launch on the library's stream, "
+                                   "one gradient after the timed steps",
                          "fwd3d": {"achieved": round(FWD_BYTES_PER_POINT * upd / fwd_avg / 1e9, 1)
                                    if fwd_n else None,
                                    "avg_launch_ms": round(fwd_avg * 1e3, 4)}},
-            "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": launches,
-            "clocks": clk.summary(),
+            "e2e": e2e, "cpu_baseline": cpu, "error_vs_fp64_oracle": errors,
+            "gpu_launches": launches, "clocks": clk.summary(),
         }
         print(json.dumps(out), flush=True)
     plan.close()
@@ -297,32 +401,22 @@ def run_e2e(args, ctx, s, cstart, padb, randb, dobs, flags):
                    "between calls of the same geometry)"}
 
 
-def cpu_baseline(s, cstart, args, target_s=15.0):
-    """FP32 oracle (C++/OpenMP restatement of the reference path) on the same
-    grid: per level 2 forward steps + 1 fused backward step."""
-    sys.path.insert(0, str(ROOT / "oracle"))
+def run_parity(args):
+    """The full-grid comparison against the FP64 oracle over --nt time samples
+    (default: the whole 3000): one GPU gradient, the oracle's FP64 and FP32
+    gradients on the host cores; prints one JSON line."""
+    import vtib200 as V
+    nt = args.nt or CONFIGS[args.config]["nt"]
+    s, cstart, ctrue, padb, randb = make_inputs(args.config, 0)
+    ctx = V.Context(0)
+    try:
+        res = oracle_errors(ctx, s, cstart, ctrue, padb, randb, nt)
+    finally:
+        ctx.close()
     import oracle as O
-    g = s.geom()
-    n = s.nxyz
-    c = (cstart[:n], cstart[n:2 * n], cstart[2 * n:])
-    t0 = time.perf_counter()
-    thr = O.time_forward_f32(g, *c, 1)
-    tf1 = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    O.time_backward_f32(g, *c, 1)
-    tb1 = time.perf_counter() - t0
-    k = max(1, int(target_s / (2 * tf1 + tb1)))
-    t0 = time.perf_counter()
-    O.time_forward_f32(g, *c, 2 * k)
-    tf = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    O.time_backward_f32(g, *c, k)
-    tb = time.perf_counter() - t0
-    val = 4.0 * k * n / (tf + tb) / 1e9
-    return {"value": round(val, 4), "unit": "Gpts/s", "cores": int(thr), "kind": "port",
-            "sample": f"{k} gradient levels (2k forward + k fused backward steps) on the "
-                      f"{s.nx}x{s.ny}x{s.nz} grid, FP32, {thr} OpenMP threads",
-            "seconds": round(tf + tb, 2)}
+    res["threads"] = O.max_threads()
+    print(json.dumps({"workload": "parity", "config": args.config, **res}), flush=True)
+    return res
 
 
 def run_batched(args):
@@ -828,43 +922,51 @@ def run_forward2d(args):
 
 
 def run_reference(args):
-    """Reference arm: the reference algorithm's CPU implementation (the FP32
-    oracle port; the reference's own CPU path needs ISPC and TBB, absent
-    here), all host threads, bounded samples of the same workload."""
+    """Reference arm: the reference algorithm's CPU implementation on the host
+    cores (the FP32 oracle port: the reference's own CPU path needs ISPC and
+    TBB, absent here), all host threads. Each step is one bounded sample of
+    the same workload: the whole three-pass gradient of the same shot on the
+    full grid over the first CPU_SAMPLE_NT time samples. Inputs are built
+    with numpy and the oracle only; the B200 library is never loaded."""
     rank = int(os.environ.get("RANK", 0))
     if rank != 0:
         return None
-    sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
     import vtib200.synth as S
     kw = dict(CONFIGS[args.config])
-    s = S.survey3d(**kw)
-    cstart = s.cij()
-    g = s.geom()
-    n = s.nxyz
-    c = (cstart[:n], cstart[n:2 * n], cstart[2 * n:])
-    k = 1
+    host = dict(get_boundary=O.get_boundary, put_boundary=O.put_boundary,
+                vepsdel_to_cij=O.vepsdel_to_cij)
+    s, cstart, ctrue, padb, randb = S.gradient_inputs(kw, 0, **host)
+    nrec = s.recloc.size // 4
+    M = levels(OracleGeom(s), 1)
+    sh = shortened(s, CPU_SAMPLE_NT)
+    n = sh.nxyz
+    # observed data of the sample: the FP32 oracle's traces of the true model
+    dobs = O.model_data3d(OracleGeom(sh), ctrue[:n], ctrue[n:2 * n], ctrue[2 * n:], sh.wavelet,
+                          sh.souloc, [0], sh.recloc, dtype=np.float32, full_steps=True)
+    dobs = np.asarray(dobs, dtype=np.float32)
     for _ in range(args.warmup):
-        O.time_forward_f32(g, *c, 1)
-    t0 = time.perf_counter()
-    thr = 0
+        oracle_gradient_sample(sh, cstart, padb, randb, dobs)
+    secs = []
     for _ in range(args.steps):
-        thr = O.time_forward_f32(g, *c, 2 * k)
-        O.time_backward_f32(g, *c, k)
-    sec = time.perf_counter() - t0
-    val = 4.0 * k * n * args.steps / sec / 1e9
-    out = {"metric": "3D VTI fwd+adjoint gradient throughput (grid-point updates/s)",
+        secs.append(oracle_gradient_sample(sh, cstart, padb, randb, dobs)[1])
+    sec = sum(secs)
+    pts = 4.0 * (sh.nt - 2) * n * args.steps
+    val = pts / sec / 1e9
+    thr = O.max_threads()
+    import vtib200
+    assert vtib200._lib is None, "the reference arm must not load the B200 library"
+    out = {"metric": GRADIENT_METRIC,
            "value": round(val, 4), "unit": "Gpts/s", "n_gpus": int(os.environ.get(
                "WORLD_SIZE", 1)), "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": round(sec / args.steps * 1e3, 2), "higher_is_better": True,
-           "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic (seeded layered VTI model + GRF, Ricker source)",
            "impl": "reference",
-           "config": {"workload": f"3D VTI L2-misfit gradient, {args.config}: "
-                                  f"{s.nx}x{s.ny}x{s.nz} grid; each step = {k} gradient level "
-                                  "(2 forward + 1 fused backward step)"},
-           "cpu_baseline": {"value": round(val, 4), "unit": "Gpts/s", "cores": int(thr),
+           "config": gradient_config(args.config, s, M, nrec),
+           "cpu_baseline": {"value": round(val, 4), "unit": "Gpts/s", "cores": thr,
                             "kind": "port",
-                            "sample": f"{k} level(s) per step on the full grid, FP32"},
+                            "sample": "each step: " + cpu_sample_desc(sh, thr)},
            "e2e": {"value": round(val, 4), "unit": "Gpts/s", "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
@@ -879,13 +981,16 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default="gradient400", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-check", action="store_true",
+                    help="skip the full-grid check against the FP64 oracle")
     ap.add_argument("--workload", default="gradient",
-                    choices=["gradient", "batched", "served", "gnhv", "forward2d"],
+                    choices=["gradient", "batched", "served", "gnhv", "forward2d", "parity"],
                     help="batched: many shots on their own windows vs the plain loop")
     ap.add_argument("--shots", type=int, default=64, help="batched workload: shots")
     ap.add_argument("--plain-shots", type=int, default=3,
                     help="batched workload: shots timed in the plain per-shot loop")
-    ap.add_argument("--nt", type=int, default=0, help="batched workload: time samples")
+    ap.add_argument("--nt", type=int, default=0,
+                    help="batched / parity workloads: time samples")
     ap.add_argument("--requests", type=int, default=40, help="served workload: requests")
     ap.add_argument("--budget-gib", type=float, default=100.0,
                     help="served workload: engine device-memory budget (GiB)")
@@ -913,6 +1018,8 @@ def main():
         run_batched(args)
     elif args.workload == "served" and args.impl == "b200":
         run_served(args)
+    elif args.workload == "parity" and args.impl == "b200":
+        run_parity(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

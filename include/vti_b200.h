@@ -53,7 +53,11 @@ typedef enum {
  * reference pipeline's 2 + 64*floor((nt-2)/64) levels
  * (objFuncGradient3d_f.cu:538-542), so results match it for every nt. */
 #define VTI_OPT_FULL_STEPS 1u
-/* Check wavefields for NaN/Inf after each pass (VTI_ERR_NONFINITE). */
+/* 3D plans: after each pass the wavefields of its last two levels (a NaN or
+ * Inf propagates into every later level), the traces of pass 1 and the
+ * gradients of pass 3 are scanned for NaN/Inf, and so is the misfit; the
+ * call then returns VTI_ERR_NONFINITE. Costs one read of those volumes per
+ * pass. */
 #define VTI_OPT_CHECK_FINITE 2u
 /* Without VTI_OPT_FULL_STEPS the 3D time levels and the recorded trace
  * samples follow the reference pipeline run on G GPUs (G = its GPUs.size(),
@@ -105,11 +109,26 @@ int vti_ctx_set_timing(vti_ctx* ctx, int enable);
  * the per-step path. enable = 0 forces the per-step path (default 1). */
 int vti_ctx_set_2d_resident(vti_ctx* ctx, int enable);
 int vti_ctx_kernel_time(vti_ctx* ctx, const char* kernel, double* total_ms, uint64_t* count);
+/* Diagnostic (no counterpart in the reference): one CTA waits on a shared-
+ * memory mbarrier that nothing arrives at, through the bounded wait of the
+ * TMA pipeline kernels but with at most `polls` polls (1..65536). The wait
+ * gives up, the kernel sets the context's status word and returns, and this
+ * call reports VTI_ERR_TIMEOUT: the path every pipeline stall takes, shown
+ * without stalling a real kernel. */
+int vti_ctx_check_bounded_wait(vti_ctx* ctx, unsigned polls);
 
 /* ------------------------------------------------------------- host glue */
 /* Stability bound of the leapfrog scheme: largest dt^2 * lambda_max(M) over
- * the model, M = [[c11 Kh, c13 Kz],[c13 Kh, c33 Kz]]. Stable iff < 4. */
+ * the model, M = [[c11 Kh, c13 Kz],[c13 Kh, c33 Kz]]. Stable iff < 4 (NaN if
+ * the model holds a NaN). Every entry point that takes a model refuses one
+ * whose number is not below 4 with VTI_ERR_CFL before it computes anything
+ * (the reference runs such a model and returns growing garbage). */
 double vti3d_cfl_number(const vti3d_geom* g, const float* c11, const float* c13,
+                        const float* c33);
+/* The same number for a 2D model on its padded (nx+2npad) x (nz+2npad) grid
+ * (lib/vti-fwi-2d/kernels.h:4-8 stencil). New entry point, no counterpart in
+ * the reference. */
+double vti2d_cfl_number(const vti2d_geom* g, const float* c11, const float* c13,
                         const float* c33);
 /* getBoundary / putBoundary / zeroBoundary (boundary.cpp:10-117). */
 void vti3d_get_boundary(float* boundary, const float* v, int nx, int ny, int nz, int npad);
@@ -374,6 +393,11 @@ int vti3d_engine_submit(vti3d_engine* e, const vti3d_job* job, int* id);
 /* Enqueues up to `ticks` time levels of every admitted job; *active = jobs
  * still running. */
 int vti3d_engine_step(vti3d_engine* e, int ticks, int* active);
+/* Drops an admitted job (running or finished, result not collected): waits
+ * for the launches already queued, then releases its device state and its
+ * share of the byte budget; the jobs beside it continue unchanged. For
+ * request loops that cancel requests; no counterpart in the reference. */
+int vti3d_engine_cancel(vti3d_engine* e, int id);
 /* Ids of finished jobs whose results are ready (non-blocking). */
 int vti3d_engine_poll(vti3d_engine* e, int* ids, int max_ids, int* n_done);
 /* Result of a finished job, then its device state is released: modeling:

@@ -40,6 +40,7 @@ def lib():
             f = getattr(L, f"orc2d_forward_{suf}")
             f.argtypes = [VP] * 7 + [C.c_int, VP, C.c_int, VP, VP, C.c_int]
             f.restype = C.c_int
+        L.orc_max_threads.restype = C.c_int
         L.orc3d_damping.argtypes = [C.c_int] * 4 + [VP]
         L.orc3d_last_level.argtypes = [VP, VP]
         L.orc3d_last_level.restype = C.c_int
@@ -203,6 +204,44 @@ def exact_gnhv3d(g, c11, c13, c33, wavelet, souloc, shotid, recloc, dc):
     return exact_adjoint3d(g, c11, c13, c33, wavelet, souloc, shotid, recloc, bd)
 
 
+# ------------------------------------------------------------ host glue
+# numpy restatements of the reference's host helpers, so that inputs can be
+# built with the oracle alone (the reference leg of the benchmark)
+def _pad_mask(nx, ny, nz, npad):
+    m = np.ones((nz, ny, nx), dtype=bool)
+    m[npad:nz - npad, npad:ny - npad, npad:nx - npad] = False
+    return m
+
+
+def get_boundary(v, nx, ny, nz, npad):
+    """getBoundary (lib/vti-fwi-3d/gpu/boundary.cpp:10-46): the pad-region
+    cells in index order (top planes, then per middle plane the npad full
+    rows, both npad-wide ends of each middle row, the npad full rows, then
+    the bottom planes): the cells of the pad mask in raster order."""
+    return _f32(v).reshape(nz, ny, nx)[_pad_mask(nx, ny, nz, npad)].copy()
+
+
+def put_boundary(b, v, nx, ny, nz, npad):
+    """putBoundary (boundary.cpp:48-84): the inverse of get_boundary."""
+    out = np.array(v, dtype=np.float32, copy=True).reshape(nz, ny, nx)
+    out[_pad_mask(nx, ny, nz, npad)] = _f32(b)
+    return out.reshape(-1)
+
+
+def vepsdel_to_cij(v, eps, dl, v0=1.0, eps0=1.0, del0=1.0):
+    """VEpsDel2Cij (lib/vti-fwi-2d/conversions.cpp:42-50) with its float /
+    double mix: c33 = v0 v0 v v in float; c11 = c33 (1. + 2 eps0 eps) and
+    c13 = c33 sqrt(1. + 2 del0 del) in double, stored as float."""
+    f = np.float32
+    v, eps, dl = _f32(v), _f32(eps), _f32(dl)
+    c33 = (f(v0) * f(v0) * v * v).astype(np.float32)
+    te = 1.0 + ((f(2) * f(eps0)) * eps).astype(np.float64)
+    td = np.sqrt(1.0 + ((f(2) * f(del0)) * dl).astype(np.float64))
+    c11 = (c33.astype(np.float64) * te).astype(np.float32)
+    c13 = (c33.astype(np.float64) * td).astype(np.float32)
+    return c11, c13, c33
+
+
 def damping3d(nx, ny, nz, npad):
     out = np.zeros(nx * ny + nz, dtype=np.float32)
     lib().orc3d_damping(nx, ny, nz, npad, _p(out))
@@ -241,6 +280,11 @@ def forward2d(g, c11, c13, c33, wavelet, sloc, rloc, taper, mode=0, slocxz=None,
         _p(ip), _p(fp), _p(_f32(c11)), _p(_f32(c13)), _p(_f32(c33)), _p(_f32(wavelet)), _p(s), 1,
         None, 0, _p(_f32(taper)), _p(out), 1)
     return out.reshape(rows, nnxz)
+
+
+def max_threads():
+    """OpenMP threads of the oracle's parallel loops."""
+    return lib().orc_max_threads()
 
 
 def time_forward_f32(g, c11, c13, c33, nsteps):

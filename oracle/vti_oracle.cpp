@@ -159,37 +159,53 @@ struct Damp3 {
 // damp != nullptr selects the sponge with the block-order reading rule.
 // Optional imaging (kernel3d.cu:291-293) uses lam_x/lam_z at time t-1.
 template <typename T, bool kForwardForm>
-void step3d(const Geo3& g, const float* c11, const float* c13, const float* c33, const T* cx,
-            const T* cz, T* px, T* pz, const Damp3* damp, const T* lamx, const T* lamz, T* g11,
-            T* g13, T* g33) {
+void step3d(const Geo3& g, const float* c11, const float* c13, const float* c33,
+            const T* __restrict cx, const T* __restrict cz, T* __restrict px, T* __restrict pz,
+            const Damp3* damp, const T* __restrict lamx, const T* __restrict lamz,
+            T* __restrict g11, T* __restrict g13, T* __restrict g33) {
   const long nx = g.nx, ny = g.ny, nz = g.nz, nxy = g.nxy();
   const float dx2 = g.dx * g.dx, dy2 = g.dy * g.dy, dz2 = g.dz * g.dz, dt2 = g.dt * g.dt;
   const float sx = dt2 / dx2, sy = dt2 / dy2, sz = dt2 / dz2;
   const T C[5] = {(T)k3C0, (T)k3C1, (T)k3C2, (T)k3C3, (T)k3C4};
+  // Rows used in place of planes outside [0, nz) (zeros) and of the damping
+  // factors of undamped planes (ones): multiplying by (T)(1.0f * 1.0f) keeps
+  // the value exact, so every point evaluates the same expressions as the
+  // plain per-point form while the x loop stays free of branches.
+  const std::vector<T> zeros(nx, (T)0);
+  const std::vector<float> ones(nx, 1.f);
 #pragma omp parallel for collapse(2) schedule(static)
   for (long iz = 0; iz < nz; ++iz) {
     for (long iy = kHalf; iy < ny - kHalf; ++iy) {
       const long blk = iz / kHalf;
+      const long row = iy * nx;
+      const T* zr[9];
+      const float* dr[9];
+      float zf[9];
+      for (int k = -4; k <= 4; ++k) {
+        const long z2 = iz + k;
+        const bool in = z2 >= 0 && z2 < nz;
+        // the block-order rule: planes of the blocks above were damped as cur
+        const bool dm = in && damp && z2 / kHalf < blk;
+        zr[k + 4] = in ? cz + row + z2 * nxy : zeros.data();
+        dr[k + 4] = dm ? damp->xy.data() + row : ones.data();
+        zf[k + 4] = dm ? damp->z[z2] : 1.f;
+      }
+      const float* dc = damp ? damp->xy.data() + row : ones.data();
+      const float zc = damp ? damp->z[iz] : 1.f;
+      const long base = row + iz * nxy;
+#pragma omp simd
       for (long ix = kHalf; ix < nx - kHalf; ++ix) {
-        const long ixy = ix + iy * nx, i = ixy + iz * nxy;
+        const long i = base + ix;
         T lxx = C[0] * cx[i], lyy = C[0] * cx[i];
         for (int k = 1; k <= 4; ++k) {
           lxx += C[k] * (cx[i - k] + cx[i + k]);
           lyy += C[k] * (cx[i - k * nx] + cx[i + k * nx]);
         }
         T zv[9];
-        for (int k = -4; k <= 4; ++k) {
-          long z2 = iz + k;
-          T v = 0;
-          if (z2 >= 0 && z2 < nz) {
-            v = cz[ixy + z2 * nxy];
-            if (damp && z2 / kHalf < blk) v *= (T)damp->at(ixy, (int)z2);
-          }
-          zv[k + 4] = v;
-        }
+        for (int k = 0; k < 9; ++k) zv[k] = zr[k][ix] * (T)(dr[k][ix] * zf[k]);
         T lzz = C[0] * zv[4];
         for (int k = 1; k <= 4; ++k) lzz += C[k] * (zv[4 - k] + zv[4 + k]);
-        const T d = damp ? (T)damp->at(ixy, (int)iz) : (T)1;
+        const T d = (T)(dc[ix] * zc);
         T nxv, nzv, lxy_u = 0, lz_u = 0;
         if (kForwardForm) {
           const T lxy = lxx * (T)sx + lyy * (T)sy, lz = lzz * (T)sz;
@@ -1520,6 +1536,9 @@ int orc3d_time_backward_f32(const int* ip, const float* fp, const float* c11, co
   }
   return omp_get_max_threads();
 }
+
+// OpenMP threads the oracle's parallel loops use.
+int orc_max_threads() { return omp_get_max_threads(); }
 
 #define ORC2D_FWD(T, SUF)                                                                      \
   int orc2d_forward_##SUF(const int* ip, const float* fp, const float* c11, const float* c13,   \

@@ -1,0 +1,64 @@
+"""Parity on the full grid of the headline gradient workload.
+
+The benchmark's gradient runs on a 400 x 400 x 200 grid (40-cell pad inside)
+with the layered VTI + Gaussian-random-field model, a 12 Hz Ricker source at
+the centre and a 200 x 200 receiver grid. Here the same grid, model, source
+and receivers run with the time axis cut to nt = 130 (129 levels of each
+pass) so that the FP64 oracle finishes in seconds of host time; every tile,
+z-segment and boundary path of the full-size launches is exercised. The calls
+go through the host-buffer C ABI (vti3d_model_data_cij, vti3d_gradient_cij)
+with VTI_OPT_FULL_STEPS, as the benchmark runs them.
+
+Tolerances (relative L2): FP32 traces and misfit 1e-5, gradients 1e-4, against
+the FP64 oracle; the FP32 oracle (the same arithmetic precision as the GPU)
+is held to the same bars.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import rel_l2
+
+import vtib200 as V
+import vtib200.synth as S
+
+pytestmark = pytest.mark.gpu
+
+TRACE_TOL = 1e-5
+GRAD_TOL = 1e-4
+NT = 130
+
+
+@pytest.fixture(scope="module")
+def headline():
+    s, cstart, ctrue, padb, randb = S.gradient_inputs(dict(S.GRADIENT400, nt=NT))
+    return s, cstart, ctrue, padb, randb
+
+
+def _split(c, n):
+    return c[:n], c[n:2 * n], c[2 * n:]
+
+
+def test_headline_grid_traces_misfit_and_gradient_match_the_oracle(ctx, headline):
+    s, cstart, ctrue, padb, randb = headline
+    g = s.geom()
+    n = s.nxyz
+    assert (s.nx, s.ny, s.nz, s.npad) == (400, 400, 200, 40)
+    flags = V.OPT_FULL_STEPS
+    dobs = V.modelDataCij3d_f(ctx, g, s.souloc, [0], s.recloc, s.wavelet, *_split(ctrue, n),
+                              flags=flags)
+    dmod = V.modelDataCij3d_f(ctx, g, s.souloc, [0], s.recloc, s.wavelet, *_split(cstart, n),
+                              flags=flags)
+    fg, mis = V.objFuncGradientCij3d_f(ctx, g, s.souloc, [0], s.recloc, s.wavelet, cstart, padb,
+                                       randb, dobs, flags=flags)
+    assert np.isfinite(fg).all()
+    for dtype in (np.float64, np.float32):
+        o, mod = O.gradient3d(g, cstart, padb, randb, s.wavelet, s.souloc, [0], s.recloc, dobs,
+                              dtype=dtype, full_steps=True, want_modeled=True)
+        assert np.abs(mod).max() > 0 and o[0] > 0
+        assert rel_l2(dmod, mod) < TRACE_TOL, dtype
+        assert abs(mis - o[0]) / o[0] < TRACE_TOL, dtype
+        for k in range(3):
+            a, b = fg[1 + k * n:1 + (k + 1) * n], o[1 + k * n:1 + (k + 1) * n]
+            assert np.abs(b).max() > 0
+            assert rel_l2(a, b) < GRAD_TOL, (dtype, k, rel_l2(a, b))

@@ -178,6 +178,31 @@ def test_cfl_number_matches_eigenvalues():
     assert abs(cfl - lam * dt2) / (lam * dt2) < 1e-9
 
 
+def test_cfl_number_2d_and_nonfinite_models():
+    rng = np.random.default_rng(5)
+    nx, nz, npad = 7, 5, 2
+    n = (nx + 2 * npad) * (nz + 2 * npad)
+    c33 = rng.uniform(1.5e3, 4.5e3, n).astype(np.float32) ** 2
+    c11 = (c33 * rng.uniform(1.0, 1.4, n)).astype(np.float32)
+    c13 = (c33 * rng.uniform(1.0, 1.2, n)).astype(np.float32)
+    g = V.geom2d(nx, nz, 10, npad, 10.0, 8.0, 1e-3, 2e-3)
+    cfl = V.cfl_number2d(g, c11, c13, c33)
+    C = np.array([-2.84722222222, 1.6, -0.2, 0.02539682539, -0.00178571428])
+    s = abs(C[0] + 2 * sum(C[k] * (-1) ** k for k in range(1, 5)))
+    kh, kz = s / 10.0**2, s / 8.0**2
+    lam = max(np.linalg.eigvals(np.array([[a * kh, b * kz], [b * kh, c * kz]])).real.max()
+              for a, b, c in zip(c11.astype(np.float64), c13.astype(np.float64),
+                                 c33.astype(np.float64)))
+    dt2 = float(np.float32(1e-3)) ** 2
+    assert abs(cfl - lam * dt2) / (lam * dt2) < 1e-9
+    # a NaN anywhere in the model gives NaN (which every entry point refuses)
+    c11[n // 2] = np.nan
+    assert np.isnan(V.cfl_number2d(g, c11, c13, c33))
+    g3 = V.geom3d(nx, nz, 1, 10, 0, 10.0, 10.0, 8.0, 1e-3, 2e-3)
+    g3.nx, g3.ny, g3.nz = n, 1, 1
+    assert np.isnan(V.cfl_number(g3, c11, c13, c33))
+
+
 def test_taper2d_profile():
     nx, nz, npad = 20, 10, 5
     t = V.init_taper2d(nx, nz, npad).reshape(nz + 2 * npad, nx + 2 * npad)
@@ -225,3 +250,36 @@ def test_random_boundary_matches_reference_generator(name):
     assert r.max() <= 1.0 and r.min() > 0.2 / 3
     if inner is not None:
         assert np.all(r[inner == 1] == 1.0)
+
+
+def test_oracle_host_helpers_equal_the_library():
+    """The oracle's numpy restatements of getBoundary / putBoundary /
+    VEpsDel2Cij give the library's arrays bit for bit, so inputs built with
+    the oracle alone (the reference leg of the benchmark) are the same."""
+    import oracle as O
+    rng = np.random.default_rng(0)
+    nx, ny, nz, npad = 23, 19, 17, 5
+    n = nx * ny * nz
+    v = rng.uniform(1500, 4500, n).astype(np.float32)
+    e = rng.uniform(0, 0.2, n).astype(np.float32)
+    d = rng.uniform(0, 0.1, n).astype(np.float32)
+    for a, b in zip(O.vepsdel_to_cij(v, e, d), V.vepsdel_to_cij(v, e, d)):
+        np.testing.assert_array_equal(a, b)
+    for a, b in zip(O.vepsdel_to_cij(v, e, d, 1.1, 0.9, 1.3), V.vepsdel_to_cij(v, e, d, 1.1, 0.9, 1.3)):
+        np.testing.assert_array_equal(a, b)
+    bo, bl = O.get_boundary(v, nx, ny, nz, npad), V.get_boundary(v, nx, ny, nz, npad)
+    np.testing.assert_array_equal(bo, bl)
+    w = rng.uniform(0, 1, n).astype(np.float32)
+    np.testing.assert_array_equal(O.put_boundary(bo, w, nx, ny, nz, npad),
+                                  V.put_boundary(bl, w, nx, ny, nz, npad))
+
+
+def test_gradient_inputs_built_by_the_oracle_equal_the_library_ones():
+    import oracle as O
+    import vtib200.synth as S
+    kw = dict(S.GRADIENT400, nx=48, ny=40, nz=32, nt=50, npad=8, smooth_m=60.0)
+    a = S.gradient_inputs(kw)
+    b = S.gradient_inputs(kw, get_boundary=O.get_boundary, put_boundary=O.put_boundary,
+                          vepsdel_to_cij=O.vepsdel_to_cij)
+    for x, y in zip(a[1:], b[1:]):
+        np.testing.assert_array_equal(x, y)

@@ -174,3 +174,129 @@ def test_window_gradients_are_stacked_without_their_frames():
                       (3, 15): 0}
             for (y, x), v in expect.items():
                 assert a[c, z, y, x] == v, (c, z, y, x)
+
+
+# ------------------------------------------------------------------ failures
+# The serving loop's failure handling, driven on the CPU with a stand-in for
+# the GPU engine: refused admissions are retried, cancelled requests are
+# dropped wherever they are, and an engine failure between ticks (a simulated
+# worker death) rebuilds the engine and re-queues what it held.
+from types import SimpleNamespace
+
+
+class _FakeEngine:
+    """Engine3d stand-in: at most `slots` jobs at once; a job is finished
+    `ticks` engine ticks after admission; its result is (value, 0.0)."""
+
+    made = []
+
+    def __init__(self, slots=2, ticks=3, on_step=None):
+        self.slots, self.ticks, self.on_step = slots, ticks, on_step
+        self.jobs, self.next = {}, 1
+        self.cancelled, self.closed, self.tick = [], False, 0
+        _FakeEngine.made.append(self)
+
+    def submit(self, job):
+        if len(self.jobs) >= self.slots:
+            return None
+        jid = self.next
+        self.next += 1
+        self.jobs[jid] = [job, 0]
+        return jid
+
+    def step(self, n):
+        self.tick += 1
+        if self.on_step:
+            self.on_step(self)
+        for v in self.jobs.values():
+            v[1] += 1
+        return sum(v[1] < self.ticks for v in self.jobs.values())
+
+    def poll(self):
+        return [j for j, v in self.jobs.items() if v[1] >= self.ticks]
+
+    def result(self, jid):
+        job, _ = self.jobs.pop(jid)
+        return np.full(3, job.value, dtype=np.float32), 0.0
+
+    def cancel(self, jid):
+        self.jobs.pop(jid)
+        self.cancelled.append(jid)
+
+    def close(self):
+        self.closed = True
+
+
+def _job(value, n=16):
+    return SimpleNamespace(g=SimpleNamespace(nx=n, ny=n, nz=n, nt=10), kind=V.JOB_MODEL,
+                           value=value)
+
+
+def _requests(n3, n2=0):
+    reqs = [SV.Request(i, 3, "model", 0.0, (lambda v=i: _job(v))) for i in range(n3)]
+    reqs += [SV.Request(n3 + k, 2, "model", 0.0,
+                        (lambda v=n3 + k: (lambda ctx: np.full(2, v, np.float32))))
+             for k in range(n2)]
+    return reqs
+
+
+def _server(**kw):
+    eng = {k: kw.pop(k) for k in ("slots", "ticks", "on_step") if k in kw}
+    _FakeEngine.made = []
+    return SV.Server(engine_factory=lambda: _FakeEngine(**eng), ctx2=object(), chunk=1, **kw)
+
+
+def test_refused_admissions_are_retried():
+    srv = _server(slots=1, ticks=2, policy="fifo")
+    reqs = _requests(4)
+    out = srv.run(reqs, t_limit=30.0)
+    assert out["done"] == 4 and out["failed"] == 0 and out["cancelled"] == 0
+    assert out["refused_admissions"] > 0
+    assert all(float(r.result[0][0]) == r.rid for r in reqs)
+
+
+def test_cancelled_requests_are_dropped_wherever_they_are():
+    srv = None
+
+    def on_step(eng):
+        if eng.tick == 1:
+            srv.cancel(0)  # on the engine by now
+            srv.cancel(3)  # still waiting for a slot
+            srv.cancel(5)  # a 2D request
+
+    srv = _server(slots=2, ticks=3, on_step=on_step, policy="fifo")
+    reqs = _requests(4, 2)
+    srv.cancel(4)  # cancelled before it ever runs
+    out = srv.run(reqs, t_limit=30.0)
+    assert out["cancelled"] + out["done"] == 6
+    assert {0, 3, 4} <= {r.rid for r in reqs if r.result is None}
+    assert _FakeEngine.made[0].cancelled  # the running job was released on the engine
+    for r in reqs:
+        if r.result is not None:
+            assert float(np.asarray(r.result[0] if r.dim == 3 else r.result)[0]) == r.rid
+
+
+def test_worker_death_rebuilds_the_engine_and_requeues_its_jobs():
+    def fault(tick):
+        if tick == 2:
+            raise SV.WorkerFault("simulated worker death")
+
+    srv = _server(slots=2, ticks=3, fault=fault, policy="fifo")
+    reqs = _requests(5)
+    out = srv.run(reqs, t_limit=30.0)
+    assert out["done"] == 5 and out["failed"] == 0
+    assert out["engine_restarts"] == 1 and out["requeued"] == 2
+    assert len(_FakeEngine.made) == 2 and _FakeEngine.made[0].closed
+    # every result is the one the request would have had without the fault
+    assert all(float(r.result[0][0]) == r.rid for r in reqs)
+
+
+def test_requests_fail_after_max_fail_attempts():
+    def fault(tick):
+        raise SV.WorkerFault("the engine keeps failing")
+
+    srv = _server(slots=2, ticks=3, fault=fault, policy="fifo", max_fail=3)
+    reqs = _requests(3)
+    out = srv.run(reqs, t_limit=30.0)
+    assert out["done"] == 0 and out["failed"] == 3
+    assert all(isinstance(r.result, SV.WorkerFault) for r in reqs)

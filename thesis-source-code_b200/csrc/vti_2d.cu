@@ -830,6 +830,7 @@ int vti2d_synthetic(vti_ctx* ctx, const vti2d_geom* g, const float* c11, const f
       return fail(ctx, VTI_ERR_ARG, "2D shot receiver range exceeds rloc");
   }
   if (!c11 || !c13 || !c33 || !wavelet || !taper || !data) return VTI_ERR_ARG;
+  VTI_TRY_RES(check_cfl2d(ctx, g, c11, c13, c33));
   const int rst = synth2d_resident(ctx, g, c11, c13, c33, wavelet, sloc, ns, rloc, nr, taper,
                                    data);
   if (rst != VTI_ERR_UNSUPPORTED) return rst;
@@ -845,6 +846,7 @@ int vti2d_synthetic(vti_ctx* ctx, const vti2d_geom* g, const float* c11, const f
 int vti2d_modeling(vti_ctx* ctx, const vti2d_geom* g, const float* c11, const float* c13,
                    const float* c33, const float* wavelet, int slocxz, const float* taper,
                    float* wavefield) {
+  if (ctx && g && c11 && c13 && c33) VTI_TRY_RES(check_cfl2d(ctx, g, c11, c13, c33));
   return run2d(ctx, g, c11, c13, c33, wavelet, taper, slocxz, nullptr, 0, 0, 0, wavefield, 1);
 }
 
@@ -942,6 +944,10 @@ extern "C" int vti2d_synthetic_noalloc(vti_ctx* ctx, const vti2d_geom* g, const 
         return fail(ctx, VTI_ERR_ARG, "2D receiver outside the grid");
     }
     max_nri = std::max<long long>(max_nri, s[2]);
+  }
+  {
+    const int cst = check_cfl2d(ctx, g, c11, c13, c33);
+    if (cst != VTI_OK) return cst;
   }
   const long long need = 8 * nnxz + g->nt + max_nri + rows * max_nri;
   if (need > (long long)kNoAllocFloats) {

@@ -553,7 +553,13 @@ int vti3d_batch_set_model(vti3d_batch* b, const float* c11, const float* c13, co
                                   ctx->stream));
   VTI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   b->model_version++;
-  return VTI_OK;
+  // the model as stored: x-fastest rows of nx floats, no z pad planes
+  Dims3 flat = make_dims(b->g.nx, b->g.ny, b->g.nz);
+  flat.pitch = b->g.nx;
+  flat.plane = (long long)b->g.nx * b->g.ny;
+  double num = 0;
+  VTI_TRY(cfl3d_device(ctx, b->g, flat, b->d_model, b->d_model + n, b->d_model + 2 * n, &num));
+  return cfl_verdict(ctx, num, "batch model");
 }
 
 int vti3d_batch_set_wavelet(vti3d_batch* b, const float* wavelet, int mem) {
@@ -1096,6 +1102,7 @@ int vti3d_engine_submit(vti3d_engine* e, const vti3d_job* job, int* id) {
       (job->nrec > 0 && !job->recloc) || (job->kind == VTI_JOB_GRADIENT && !job->dobs))
     return fail(ctx, VTI_ERR_ARG, "null job array");
   VTI_TRY(check_geom(ctx, &job->g));
+  VTI_TRY(cfl_verdict(ctx, vti3d_cfl_number(&job->g, job->c11, job->c13, job->c33), "job model"));
   const size_t bytes = vti3d_engine_job_bytes(job);
   if (e->used + bytes > e->max_bytes)
     return fail(ctx, VTI_ERR_BUSY, "engine memory budget full; submit again later");
@@ -1296,6 +1303,23 @@ int vti3d_engine_result(vti3d_engine* e, int id, float* out, double* misfit) {
   engine_free_job(e, j);
   e->dirty = true;
   return check_device_status(ctx);
+}
+
+int vti3d_engine_cancel(vti3d_engine* e, int id) {
+  if (!e) return VTI_ERR_ARG;
+  vti_ctx* ctx = e->ctx;
+  EngineJob* j = engine_find(e, id);
+  if (!j) return fail(ctx, VTI_ERR_ARG, "unknown job id");
+  VTI_CUDA(ctx, cudaSetDevice(ctx->device));
+  // nothing of the job may be in flight when its memory goes: the launches
+  // that advanced it are on the context stream, its result copies on the
+  // copy stream
+  VTI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  VTI_CUDA(ctx, cudaStreamSynchronize(e->copy));
+  e->jobs.erase(std::find(e->jobs.begin(), e->jobs.end(), j));
+  engine_free_job(e, j);
+  e->dirty = true;
+  return VTI_OK;
 }
 
 int vti3d_engine_stats(vti3d_engine* e, size_t* used_bytes, int* jobs, int* tick) {

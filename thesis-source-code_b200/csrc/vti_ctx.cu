@@ -1,4 +1,6 @@
 // Context, status strings and pitched device volumes.
+#include <cmath>
+#include <cstdio>
 #include <cstring>
 
 #include "vti_internal.h"
@@ -15,6 +17,47 @@ int cuda_check(vti_ctx* ctx, cudaError_t e, const char* what) {
   std::string m = std::string(what) + ": " + cudaGetErrorString(e);
   int st = (e == cudaErrorMemoryAllocation) ? VTI_ERR_OOM : VTI_ERR_DEVICE;
   return fail(ctx, st, m);
+}
+
+double nyquist_factor(double h) {
+  // lib/vti-fwi-3d/gpu/wave3d.h:8-12 coefficients
+  const double C[5] = {-2.84722222222, 1.6, -0.2, 0.02539682539, -0.00178571428};
+  double s = C[0];
+  for (int k = 1; k <= 4; ++k) s += 2.0 * C[k] * ((k & 1) ? -1.0 : 1.0);
+  return std::fabs(s) / (h * h);
+}
+
+int cfl3d_device(vti_ctx* ctx, const vti3d_geom& g, const Dims3& d, const float* c11,
+                 const float* c13, const float* c33, double* number) {
+  const double s = nyquist_factor(1.0);
+  const double kh = s / ((double)g.dx * g.dx) + (g.ny > 1 ? s / ((double)g.dy * g.dy) : 0.0);
+  const double kz = s / ((double)g.dz * g.dz);
+  VTI_CUDA(ctx, cudaMemsetAsync(ctx->d_cfl, 0, sizeof(unsigned long long), ctx->stream));
+  const int st = launch_cfl_max(ctx, d, c11, c13, c33, kh, kz, ctx->d_cfl);
+  if (st != VTI_OK) return st;
+  unsigned long long bits = 0;
+  VTI_CUDA(ctx, cudaMemcpyAsync(&bits, ctx->d_cfl, sizeof bits, cudaMemcpyDeviceToHost,
+                                ctx->stream));
+  VTI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  double lam;
+  std::memcpy(&lam, &bits, sizeof lam);
+  *number = lam * (double)g.dt * g.dt;
+  return VTI_OK;
+}
+
+int check_cfl2d(vti_ctx* ctx, const vti2d_geom* g, const float* c11, const float* c13,
+                const float* c33) {
+  return cfl_verdict(ctx, vti2d_cfl_number(g, c11, c13, c33), "2D model");
+}
+
+int cfl_verdict(vti_ctx* ctx, double number, const char* what) {
+  if (number < 4.0) return VTI_OK;  // false for NaN as well
+  char msg[256];
+  std::snprintf(msg, sizeof msg,
+                "%s: dt^2 * lambda_max = %.4g is not below 4, the leapfrog stability bound of "
+                "the 8th-order scheme (reduce dt or the stiffnesses)",
+                what, number);
+  return fail(ctx, VTI_ERR_CFL, msg);
 }
 
 Dims3 make_dims(int nx, int ny, int nz) {
@@ -73,6 +116,8 @@ int check_device_status(vti_ctx* ctx) {
   VTI_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream));
   if (h & (1 << VTI_ERR_TIMEOUT))
     return fail(ctx, VTI_ERR_TIMEOUT, "a device-side pipeline wait timed out");
+  if (h & (1 << VTI_ERR_NONFINITE))
+    return fail(ctx, VTI_ERR_NONFINITE, "a wavefield, trace or gradient holds NaN or Inf");
   return fail(ctx, VTI_ERR_DEVICE, "device status word " + std::to_string(h));
 }
 
@@ -153,11 +198,12 @@ int vti_ctx_create(int device, vti_ctx** out) {
       cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device) !=
           cudaSuccess ||
-      cudaMalloc((void**)&c->d_status, sizeof(int)) != cudaSuccess ||
-      cudaMemset(c->d_status, 0, sizeof(int)) != cudaSuccess) {
+      cudaMalloc((void**)&c->d_status, 16) != cudaSuccess ||
+      cudaMemset(c->d_status, 0, 16) != cudaSuccess) {
     delete c;
     return VTI_ERR_DEVICE;
   }
+  c->d_cfl = reinterpret_cast<unsigned long long*>(reinterpret_cast<char*>(c->d_status) + 8);
   *out = c;
   return VTI_OK;
 }
@@ -176,6 +222,11 @@ int vti_ctx_destroy(vti_ctx* ctx) {
   if (ctx->scratch2d) cudaFree(ctx->scratch2d);
   delete ctx;
   return VTI_OK;
+}
+
+int vti_ctx_check_bounded_wait(vti_ctx* ctx, unsigned polls) {
+  if (!ctx) return VTI_ERR_ARG;
+  return wait_selftest(ctx, polls);
 }
 
 int vti_ctx_set_2d_resident(vti_ctx* ctx, int enable) {

@@ -910,6 +910,7 @@ int vti3d_gnhv_exact(vti_ctx* ctx, const vti3d_geom* g, const float* c11, const 
     return fail(ctx, VTI_ERR_ARG, "null input");
   if ((hv || born) && !dc) return fail(ctx, VTI_ERR_ARG, "H dc / Born traces need dc");
   if ((grad || misfit) && !dobs) return fail(ctx, VTI_ERR_ARG, "the gradient needs dobs");
+  VTI_TRY(cfl_verdict(ctx, vti3d_cfl_number(g, c11, c13, c33), "model"));
   VTI_CUDA(ctx, cudaSetDevice(ctx->device));
   const unsigned flags = VTI_OPT_FULL_STEPS;
   // the per-shot helpers of the plan: receivers, schedule, damping tables

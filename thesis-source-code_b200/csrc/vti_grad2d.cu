@@ -313,6 +313,12 @@ int run_grad2d(vti_ctx* ctx, const vti2d_geom* g, float* gc11, float* gc13, floa
   if (nnx < 9 || nnz < 9 || ratio < 1 || g->nt < 3 || (g->nt - 1) / ratio + 1 < 3)
     return fail(ctx, VTI_ERR_ARG, "2D gradient needs nt >= 2*ratio+1 and a grid of 9x9 or more");
   const int nnt_data = (g->nt - ntNeg - 1) / ratio + 1;
+  if (nnt_data < 1)
+    return fail(ctx, VTI_ERR_ARG, "the whole record lies before time zero (|ot| too large)");
+  {
+    const int cst = check_cfl2d(ctx, g, c11, c13, c33);
+    if (cst != VTI_OK) return cst;
+  }
   VTI_CUDA(ctx, cudaSetDevice(ctx->device));
   std::vector<std::vector<Pair>> sched(ns);
   {

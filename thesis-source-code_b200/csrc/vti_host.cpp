@@ -44,6 +44,34 @@ void walk_boundary(int nx, int ny, int nz, int npad, F&& run) {
 
 const float kDamper2d = 0.95f;  // lib/vti-fwi-2d/init.h:11
 
+// |C0 + 2 sum (-1)^k C_k| of the 8th-order second derivative
+// (lib/vti-fwi-3d/gpu/wave3d.h:8-12): its symbol at the Nyquist wavenumber
+// times h^2.
+double nyq() {
+  const double C[5] = {-2.84722222222, 1.6, -0.2, 0.02539682539, -0.00178571428};
+  double s = C[0];
+  for (int k = 1; k <= 4; ++k) s += 2.0 * C[k] * ((k & 1) ? -1.0 : 1.0);
+  return std::fabs(s);
+}
+
+// max over the points of the largest eigenvalue of
+// [[c11 kh, c13 kz], [c13 kh, c33 kz]]; a NaN value makes the result NaN.
+double max_symbol(const float* c11, const float* c13, const float* c33, size_t n, double kh,
+                  double kz) {
+  double worst = 0.0;
+  int bad = 0;
+#pragma omp parallel for reduction(max : worst) reduction(| : bad)
+  for (size_t i = 0; i < n; ++i) {
+    double a = c11[i] * kh, b = c13[i] * kz, c = c13[i] * kh, d = c33[i] * kz;
+    double tr = a + d, det = a * d - b * c;
+    double disc = tr * tr * 0.25 - det;
+    double lam = tr * 0.5 + std::sqrt(disc > 0 ? disc : 0.0);
+    if (std::isnan(lam)) bad = 1;
+    else if (lam > worst) worst = lam;
+  }
+  return bad ? std::nan("") : worst;
+}
+
 }  // namespace
 
 extern "C" {
@@ -160,23 +188,21 @@ void vti2d_init_taper(float* taper, int nx, int nz, int npad) {
 // (coefficients of lib/vti-fwi-3d/gpu/wave3d.h:8-12).
 double vti3d_cfl_number(const vti3d_geom* g, const float* c11, const float* c13,
                         const float* c33) {
-  const double C[5] = {-2.84722222222, 1.6, -0.2, 0.02539682539, -0.00178571428};
-  double s = C[0];
-  for (int k = 1; k <= 4; ++k) s += 2.0 * C[k] * ((k & 1) ? -1.0 : 1.0);
-  s = std::fabs(s);
+  const double s = nyq();
   const double kh = s / ((double)g->dx * g->dx) + (g->ny > 1 ? s / ((double)g->dy * g->dy) : 0.0);
   const double kz = s / ((double)g->dz * g->dz);
   const size_t n = (size_t)g->nx * g->ny * g->nz;
-  double worst = 0.0;
-#pragma omp parallel for reduction(max : worst)
-  for (size_t i = 0; i < n; ++i) {
-    double a = c11[i] * kh, b = c13[i] * kz, c = c13[i] * kh, d = c33[i] * kz;
-    double tr = a + d, det = a * d - b * c;
-    double disc = tr * tr * 0.25 - det;
-    double lam = tr * 0.5 + std::sqrt(disc > 0 ? disc : 0.0);
-    if (lam > worst) worst = lam;
-  }
-  return worst * (double)g->dt * g->dt;
+  return max_symbol(c11, c13, c33, n, kh, kz) * (double)g->dt * g->dt;
+}
+
+// The same bound for the 2D scheme (x and z second derivatives of the same
+// 8th-order stencil, lib/vti-fwi-2d/kernels.h:4-8) on the padded grid.
+double vti2d_cfl_number(const vti2d_geom* g, const float* c11, const float* c13,
+                        const float* c33) {
+  const double s = nyq();
+  const double kh = s / ((double)g->dx * g->dx), kz = s / ((double)g->dz * g->dz);
+  const size_t n = (size_t)(g->nx + 2 * g->npad) * (g->nz + 2 * g->npad);
+  return max_symbol(c11, c13, c33, n, kh, kz) * (double)g->dt * g->dt;
 }
 
 }  // extern "C"

@@ -57,8 +57,10 @@ struct vti_ctx {
   std::string last_error;
   uint64_t launches = 0;
   int sm_count = 0;
-  // device status word written by kernels (0 = ok)
+  // device status word written by kernels (0 = ok); the same allocation holds
+  // the stability-number reduction slot at byte 8
   int* d_status = nullptr;
+  unsigned long long* d_cfl = nullptr;
   // optional per-kernel timing: event pairs recorded around timed launches
   bool timing = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events[vti::kNumTimed];
@@ -234,6 +236,8 @@ void step_batch_free(StepBatch* b);
 // Sets the batched kernels' launch attributes (before any stream capture).
 int prepare_batch_kernels(vti_ctx* ctx);
 
+// k_wait_selftest with `polls` polls; returns the status it leaves.
+int wait_selftest(vti_ctx* ctx, unsigned polls);
 // Reads (and clears) the device status word; VTI_ERR_TIMEOUT if a bounded
 // device-side wait gave up since the last check.
 int check_device_status(vti_ctx* ctx);
@@ -268,5 +272,25 @@ int launch_agc_adjoint(vti_ctx* ctx, float* trace, const float* obs, int nnt, in
                        double* part, double* acc);
 int launch_boundary_merge(vti_ctx* ctx, const Dims3& d, int npad, const float* full,
                           const float* blist, float* out);
+// VTI_ERR_NONFINITE bit of the status word if a[0, n) holds a NaN or Inf.
+int launch_check_finite(vti_ctx* ctx, const float* a, long long n);
+// *out (zeroed by the caller) <- bits of max over the volume of the largest
+// eigenvalue of [[c11 kh, c13 kz], [c13 kh, c33 kz]]; dt^2 times it is the
+// number vti3d_cfl_number returns.
+int launch_cfl_max(vti_ctx* ctx, const Dims3& d, const float* c11, const float* c13,
+                   const float* c33, double kh, double kz, unsigned long long* out);
+// Nyquist symbol factors of the 8th-order second derivative per axis:
+// |C0 + 2 sum (-1)^k C_k| / h^2 (0 for an absent axis).
+double nyquist_factor(double h);
+// Stability number of a device-resident pitched model (three volumes at
+// their origin planes) of geometry g: dt^2 * max lambda over the grid.
+int cfl3d_device(vti_ctx* ctx, const vti3d_geom& g, const Dims3& d, const float* c11,
+                 const float* c13, const float* c33, double* number);
+// cfl_verdict of vti2d_cfl_number for a 2D model (non-null arrays).
+int check_cfl2d(vti_ctx* ctx, const vti2d_geom* g, const float* c11, const float* c13,
+                const float* c33);
+// VTI_ERR_CFL (with the number in the context's message) when
+// dt^2 lambda_max >= 4, the leapfrog bound; VTI_OK otherwise.
+int cfl_verdict(vti_ctx* ctx, double number, const char* what);
 
 }  // namespace vti

@@ -349,6 +349,66 @@ int launch_agc_adjoint(vti_ctx* ctx, float* trace, const float* obs, int nnt, in
   return VTI_OK;
 }
 
+namespace {
+// dt^2-free stability number of every point: the largest eigenvalue of
+// [[c11 kh, c13 kz], [c13 kh, c33 kz]] (the symbol of the scheme at the
+// Nyquist wavenumber, as vti3d_cfl_number evaluates it), in double; the
+// maximum is reduced with an atomic max on the bit pattern (non-negative
+// doubles order like their bits; a NaN model value wins and is rejected).
+__global__ void k_cfl_max(Dims3 d, const float* c11, const float* c13, const float* c33,
+                          double kh, double kz, unsigned long long* out) {
+  const long long n = (long long)d.nx * d.ny * d.nz;
+  double worst = 0.0;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(t % d.nx);
+    const long long yz = t / d.nx;
+    const long long o = (yz / d.ny) * d.plane + (yz % d.ny) * d.pitch + x;
+    const double a = c11[o] * kh, b = c13[o] * kz, c = c13[o] * kh, e = c33[o] * kz;
+    const double tr = a + e, det = a * e - b * c;
+    const double disc = tr * tr * 0.25 - det;
+    const double lam = tr * 0.5 + sqrt(disc > 0 ? disc : 0.0);
+    if (!(lam <= worst)) worst = lam;
+  }
+  unsigned long long bits = __double_as_longlong(worst);
+  for (int k = 16; k > 0; k >>= 1) {
+    const unsigned long long other = __shfl_xor_sync(0xffffffffu, bits, k);
+    bits = other > bits ? other : bits;
+  }
+  if ((threadIdx.x & 31) == 0) atomicMax(out, bits);
+}
+}  // namespace
+
+namespace {
+// Sets the VTI_ERR_NONFINITE bit of the status word if any of a[0, n) is NaN
+// or infinite.
+__global__ void k_check_finite(const float* a, long long n, int* status) {
+  bool bad = false;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    bad |= !isfinite(a[i]);
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0)
+    atomicOr(status, 1 << VTI_ERR_NONFINITE);
+}
+}  // namespace
+
+int launch_check_finite(vti_ctx* ctx, const float* a, long long n) {
+  if (n <= 0) return VTI_OK;
+  const int blocks = (int)std::min<long long>((n + 255) / 256, (long long)ctx->sm_count * 8);
+  k_check_finite<<<blocks, 256, 0, ctx->stream>>>(a, n, ctx->d_status);
+  VTI_LAUNCHED(ctx, "k_check_finite");
+  return VTI_OK;
+}
+
+int launch_cfl_max(vti_ctx* ctx, const Dims3& d, const float* c11, const float* c13,
+                   const float* c33, double kh, double kz, unsigned long long* out) {
+  const long long n = (long long)d.nx * d.ny * d.nz;
+  const int blocks = (int)std::min<long long>((n + 255) / 256, (long long)ctx->sm_count * 8);
+  k_cfl_max<<<blocks, 256, 0, ctx->stream>>>(d, c11, c13, c33, kh, kz, out);
+  VTI_LAUNCHED(ctx, "k_cfl_max");
+  return VTI_OK;
+}
+
 int launch_boundary_merge(vti_ctx* ctx, const Dims3& d, int npad, const float* full,
                           const float* blist, float* out) {
   long long n = d.npoints();

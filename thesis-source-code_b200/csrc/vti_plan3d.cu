@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <initializer_list>
 
 #include "vti_plan3d.h"
 
@@ -191,6 +192,18 @@ int upload_shot(vti3d_plan* p, const ShotGeom& s) {
   return VTI_OK;
 }
 
+// VTI_OPT_CHECK_FINITE: the volumes (whole allocations, zero padding
+// included) are scanned for NaN / Inf; a hit sets the status word's
+// VTI_ERR_NONFINITE bit, which the call's final status check reports. A
+// non-finite value propagates through every later level, so checking the
+// last two levels of each pass catches one that arose anywhere in it.
+int check_finite(vti3d_plan* p, std::initializer_list<const Vol*> vols) {
+  if (!(p->flags & VTI_OPT_CHECK_FINITE)) return VTI_OK;
+  for (const Vol* v : vols)
+    VTI_TRY(launch_check_finite(p->ctx, v->alloc, (long long)(v->bytes / sizeof(float))));
+  return VTI_OK;
+}
+
 // Forward propagation of one shot. sponge: pass 1 (pad-boundary model, sponge,
 // traces recorded into d_trace). Otherwise pass 2 (random-boundary model, no
 // sponge). On return sx[last_cur] holds level M and the other buffer M-1.
@@ -230,7 +243,9 @@ int forward_pass(vti3d_plan* p, const ShotGeom& s, bool sponge) {
                             p->sz[A].origin, p->d_rec, s.nr));
   }
   p->last_cur = A;
-  return VTI_OK;
+  if (sponge && s.nr > 0 && (p->flags & VTI_OPT_CHECK_FINITE))
+    VTI_TRY(launch_check_finite(ctx, p->d_trace, (long long)nnt * s.nr));
+  return check_finite(p, {&p->sx[0], &p->sx[1], &p->sz[0], &p->sz[1]});
 }
 
 // Time-reversed source wavefield + adjoint + imaging (pass 3,
@@ -287,7 +302,8 @@ int backward_pass(vti3d_plan* p, const ShotGeom& s, bool rtm, float* ext = nullp
     std::swap(SA, SB);
     std::swap(LA, LB);
   }
-  return VTI_OK;
+  return check_finite(p, {&p->sx[0], &p->sx[1], &p->sz[0], &p->sz[1], &p->lx[0], &p->lx[1],
+                          &p->lz[0], &p->lz[1], &p->g11, &p->g13, &p->g33});
 }
 
 int check_geom(vti_ctx* ctx, const vti3d_geom* g) {
@@ -549,6 +565,18 @@ int vti3d_plan_set_model(vti3d_plan* p, const float* c11, const float* c13, cons
     }
   }
   VTI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  p->have_model = false;
+  // refuse a model the scheme cannot step stably (the random boundary only
+  // lowers velocities, but a caller's list may not)
+  double num = 0;
+  VTI_TRY(cfl3d_device(ctx, p->g, d, p->cpad[0].origin, p->cpad[1].origin, p->cpad[2].origin,
+                       &num));
+  VTI_TRY(cfl_verdict(ctx, num, "model"));
+  if (randb) {
+    VTI_TRY(cfl3d_device(ctx, p->g, d, p->crand[0].origin, p->crand[1].origin,
+                         p->crand[2].origin, &num));
+    VTI_TRY(cfl_verdict(ctx, num, "model with the random boundary"));
+  }
   p->have_rand = randb != nullptr;
   p->have_model = true;
   return VTI_OK;

@@ -399,6 +399,10 @@ extern "C" int vti2d_wavelet_gradient(vti_ctx* ctx, const vti2d_geom* g, float* 
   const long long nnxz = (long long)nnx * nnz;
   if (nnx < 9 || nnz < 9 || g->nt < 3 || !(g->dt > 0) || !(g->rate > 0))
     return fail(ctx, VTI_ERR_ARG, "2D geometry out of range");
+  {
+    const int cst = check_cfl2d(ctx, g, c11, c13, c33);
+    if (cst != VTI_OK) return cst;
+  }
   const float dt = g->dt, dt2 = dt * dt;
   const int ratio = (int)(g->rate / dt + 0.5);  // objFuncGradient_f.cu:375 (double 0.5)
   if (ratio < 1) return fail(ctx, VTI_ERR_ARG, "rate < dt");

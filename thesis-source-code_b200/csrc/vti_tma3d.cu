@@ -672,6 +672,20 @@ __global__ void __launch_bounds__(NTHREADS, 2) k_bwd3d_batch(const __grid_consta
 
 static_assert(sizeof(FwdBatch) <= 32000 && sizeof(BwdBatch) <= 32000, "kernel parameter size");
 
+// vti_ctx_check_bounded_wait: thread 0 waits on an mbarrier (expected count
+// 1) that no thread arrives at and no copy completes, with a poll limit; the
+// wait gives up and sets the status word. Nothing is in flight, so the CTA
+// simply returns.
+__global__ void k_wait_selftest(int* status, unsigned polls) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) mbar_wait(&bar, 0, status, polls);
+}
+
 }  // namespace
 
 // ------------------------------------------------------------ host side
@@ -1021,6 +1035,15 @@ int step_batch_launch(vti_ctx* ctx, StepBatch* b, int tick) {
     }
   }
   return VTI_OK;
+}
+
+int wait_selftest(vti_ctx* ctx, unsigned polls) {
+  if (polls < 1 || polls > 65536) return fail(ctx, VTI_ERR_ARG, "polls must be in [1, 65536]");
+  VTI_CUDA(ctx, cudaSetDevice(ctx->device));
+  k_wait_selftest<<<1, 32, 0, ctx->stream>>>(ctx->d_status, polls);
+  VTI_LAUNCHED(ctx, "k_wait_selftest");
+  VTI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return check_device_status(ctx);
 }
 
 int step_batch_launches(const StepBatch* b) {

@@ -74,9 +74,11 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait; false (and the status word set) if the phase never completes.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* status) {
-  for (unsigned i = 0; i < kSpinLimit; ++i)
+// Bounded wait; false (and the status word set) if the phase never completes
+// within `limit` polls.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* status,
+                                          unsigned limit = kSpinLimit) {
+  for (unsigned i = 0; i < limit; ++i)
     if (mbar_try_wait(bar, parity)) return true;
   atomicOr(status, 1 << VTI_ERR_TIMEOUT);
   return false;

@@ -83,6 +83,8 @@ def _signatures():
         "vti_ctx_kernel_time": (C.c_int, [P, C.c_char_p, C.POINTER(C.c_double),
                                           C.POINTER(C.c_uint64)]),
         "vti3d_cfl_number": (C.c_double, [P, P, P, P]),
+        "vti2d_cfl_number": (C.c_double, [P, P, P, P]),
+        "vti_ctx_check_bounded_wait": (C.c_int, [P, C.c_uint]),
         "vti3d_get_boundary": (None, [P, P, C.c_int, C.c_int, C.c_int, C.c_int]),
         "vti3d_put_boundary": (None, [P, P, C.c_int, C.c_int, C.c_int, C.c_int]),
         "vti3d_zero_boundary": (None, [P, C.c_int, C.c_int, C.c_int, C.c_int]),
@@ -144,6 +146,7 @@ def _signatures():
         "vti3d_engine_step": (C.c_int, [P, C.c_int, C.POINTER(C.c_int)]),
         "vti3d_engine_poll": (C.c_int, [P, P, C.c_int, C.POINTER(C.c_int)]),
         "vti3d_engine_result": (C.c_int, [P, C.c_int, P, C.POINTER(C.c_double)]),
+        "vti3d_engine_cancel": (C.c_int, [P, C.c_int]),
         "vti3d_engine_stats": (C.c_int, [P, C.POINTER(C.c_size_t), C.POINTER(C.c_int),
                                          C.POINTER(C.c_int)]),
     }
@@ -504,6 +507,11 @@ class Engine3d:
         self.ctx.check(lib().vti3d_engine_result(self._h, jid, _p(out), C.byref(mis)))
         return out, mis.value
 
+    def cancel(self, jid):
+        """Drops an admitted job (vti3d_engine_cancel)."""
+        self.ctx.check(lib().vti3d_engine_cancel(self._h, int(jid)))
+        self._jobs.pop(jid, None)
+
     def stats(self):
         u, n, t = C.c_size_t(0), C.c_int(0), C.c_int(0)
         self.ctx.check(lib().vti3d_engine_stats(self._h, C.byref(u), C.byref(n), C.byref(t)))
@@ -732,6 +740,11 @@ def grad_cij_to_vepsdel(gc11, gc13, gc33, v, eps, dl, v0=1.0, eps0=1.0, del0=1.0
 
 def cfl_number(g: Geom3d, c11, c13, c33):
     return lib().vti3d_cfl_number(C.byref(g), _p(_f32(c11)), _p(_f32(c13)), _p(_f32(c33)))
+
+
+def cfl_number2d(g: Geom2d, c11, c13, c33):
+    """vti2d_cfl_number: dt^2 lambda_max of a 2D model on its padded grid."""
+    return lib().vti2d_cfl_number(C.byref(g), _p(_f32(c11)), _p(_f32(c13)), _p(_f32(c33)))
 
 
 def random_boundary_ref(v, n1, n2, n3, pad, pct_g=0.9, seed=2017, bval=1.0, eval_=0.2):

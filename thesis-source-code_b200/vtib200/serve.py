@@ -20,8 +20,8 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import (JOB_GRADIENT, JOB_MODEL, OPT_FULL_STEPS, Context, Engine3d, Plan3d, cfl_number,
-               geom3d, get_boundary, objFuncGradient_f, synthetic_f, vepsdel_to_cij)
+from . import (JOB_GRADIENT, JOB_MODEL, OPT_FULL_STEPS, Context, Engine3d, Plan3d, VtiError,
+               cfl_number, geom3d, get_boundary, objFuncGradient_f, synthetic_f, vepsdel_to_cij)
 from . import synth as S
 
 
@@ -341,34 +341,79 @@ def _summary(res):
             mis[-1] if mis else None)
 
 
+class WorkerFault(RuntimeError):
+    """The engine failed between ticks (raised by a fault hook to simulate a
+    worker death, or standing for a device error reported by the engine)."""
+
+
+# Attempts per request before it is reported failed: the reference's job farm
+# resubmits a failed job up to MAX_FAIL = 5 times (lib/vti-fwi-3d/gpu/cluster.h:4,
+# objFuncGradient3d_f.cu:60-64).
+MAX_FAIL = 5
+
+
 class Server:
-    """Continuous-batching request loop on one GPU."""
+    """Continuous-batching request loop on one GPU.
+
+    Failure handling (all on the host, between ticks): a request can be
+    cancelled at any time (`cancel`); an admission the engine refuses for
+    lack of memory is retried on later ticks; if the engine fails (an error
+    from a step, or a `fault` hook raising WorkerFault before a tick), the
+    engine is torn down and rebuilt and every request it held is queued again
+    from its start, up to `max_fail` attempts, after which it is reported
+    failed."""
 
     def __init__(self, device=0, max_bytes=64 << 30, chunk=16, keep_results=True, log=None,
-                 policy="sjf", max_active_points=24_000_000):
+                 policy="sjf", max_active_points=24_000_000, engine_factory=None, ctx2=None,
+                 fault=None, max_fail=MAX_FAIL):
         """policy "sjf": waiting 3D jobs are admitted shortest (grid points x
         time steps x passes) first, and only while the grid points of the
         jobs in flight stay within max_active_points (a larger job runs
         alone): a launch that already fills the GPU gains nothing from more
         jobs, which would only share its time. policy "fifo": arrival order,
-        no cap (memory budget only)."""
-        self.ctx3 = Context(device)
-        self.ctx2 = Context(device)
-        self.engine = Engine3d(self.ctx3, max_bytes)
+        no cap (memory budget only). engine_factory / ctx2 replace the GPU
+        engine and the 2D context (tests drive the loop with stand-ins);
+        fault(tick) is called before every engine step that has jobs in flight,
+        with the number of that step (1, 2, ...)."""
+        self._own = engine_factory is None
+        if self._own:
+            self.ctx3 = Context(device)
+            self.ctx2 = Context(device)
+            engine_factory = lambda: Engine3d(self.ctx3, max_bytes)  # noqa: E731
+        else:
+            self.ctx2 = ctx2
+        self._factory = engine_factory
+        self.engine = engine_factory()
         self.chunk = chunk
         self.keep_results = keep_results
         self.log = log
         self.policy = policy
         self.max_active_points = max_active_points
+        self.fault = fault
+        self.max_fail = max_fail
+        self._lock = threading.Lock()
+        self._cancel = set()
 
     def _log(self, msg):
         if self.log:
             self.log(msg)
 
+    def cancel(self, rid):
+        """Cancels request `rid` (thread-safe): it is dropped wherever it is
+        (not yet arrived, waiting, on the engine, or queued for the 2D
+        worker); a request already done is unaffected."""
+        with self._lock:
+            self._cancel.add(rid)
+
+    def _cancelled(self, rid):
+        with self._lock:
+            return rid in self._cancel
+
     def close(self):
         self.engine.close()
-        self.ctx3.close()
-        self.ctx2.close()
+        if self._own:
+            self.ctx3.close()
+            self.ctx2.close()
 
     def run(self, requests, fwi: FwiDriver | None = None, t_limit=3600.0):
         t0 = time.perf_counter()
@@ -379,6 +424,9 @@ class Server:
         inflight = {}
         done = []
         fwi_reqs = []
+        cancelled, failed = [], []
+        counts = {"requeued": 0, "engine_restarts": 0, "refused_admissions": 0}
+        tick = 0
 
         ready = {}  # request id -> prepared 3D job (built off the stepping thread)
         q3 = queue.Queue()
@@ -398,6 +446,10 @@ class Server:
                 r = q2.get()
                 if r is None:
                     return
+                if self._cancelled(r.rid):
+                    r.t_done = now()
+                    cancelled.append(r)
+                    continue
                 r.t_admit = now()
                 res = r.make()(self.ctx2)
                 r.result = res if self.keep_results else _summary(res)
@@ -419,7 +471,46 @@ class Server:
             submit_fwi(fwi.first())
         fwi_batch = {}
         n2 = sum(r.dim == 2 for r in requests)
+
+        def drop_cancelled():
+            with self._lock:
+                cset = set(self._cancel)
+            if not cset:
+                return
+            for lst in (pending, waiting):
+                for r in [r for r in lst if r.rid >= 0 and r.rid in cset]:
+                    lst.remove(r)
+                    r.t_done = now()
+                    cancelled.append(r)
+            for jid in [j for j, r in inflight.items() if r.rid >= 0 and r.rid in cset]:
+                r = inflight.pop(jid)
+                self.engine.cancel(jid)
+                r.t_done = now()
+                cancelled.append(r)
+
+        def worker_death(err):
+            """Tear the engine down and rebuild it; its requests start again."""
+            counts["engine_restarts"] += 1
+            self._log(f"engine failed at tick {tick}: {err}; restarting it with "
+                      f"{len(inflight)} request(s) re-queued")
+            try:
+                self.engine.close()
+            except Exception as e:  # the old engine may be unusable
+                self._log(f"closing the failed engine: {e}")
+            self.engine = self._factory()
+            for r in sorted(inflight.values(), key=lambda x: x.t_admit, reverse=True):
+                r.attempts = getattr(r, "attempts", 0) + 1
+                if r.attempts >= self.max_fail:
+                    r.t_done = now()
+                    r.result = err
+                    failed.append(r)
+                else:
+                    counts["requeued"] += 1
+                    waiting.appendleft(r)
+            inflight.clear()
+
         while now() < t_limit:
+            drop_cancelled()
             t = now()
             while pending and pending[0].arrival <= t:
                 r = pending.popleft()
@@ -448,16 +539,27 @@ class Server:
                     break
                 jid = self.engine.submit(r._job)
                 if jid is None:
-                    refused = True
+                    # retried on a later tick; with nothing in flight the job
+                    # can never fit the budget
+                    refused = not inflight
+                    counts["refused_admissions"] += 1
                     break
                 waiting.remove(r)
                 r.t_admit = now()
                 inflight[jid] = r
                 active_pts += pts
-            active = self.engine.step(self.chunk) if inflight else 0
-            for jid in self.engine.poll():
+            try:
+                if inflight:
+                    tick += 1
+                    if self.fault is not None:
+                        self.fault(tick)
+                active = self.engine.step(self.chunk) if inflight else 0
+                finished = [(jid, self.engine.result(jid)) for jid in self.engine.poll()]
+            except (WorkerFault, VtiError) as err:
+                worker_death(err)
+                continue
+            for jid, res in finished:
                 r = inflight[jid]
-                res = self.engine.result(jid)
                 del inflight[jid]
                 r.t_done = now()
                 del r._job
@@ -476,7 +578,7 @@ class Server:
                     submit_fwi(nxt)
                 else:
                     fwi = None
-            n_done = sum(r.rid >= 0 for r in done)
+            n_done = sum(r.rid >= 0 for r in done + cancelled + failed)
             if n_done == len(requests) and fwi is None and not inflight and not waiting:
                 break
             if not active and not inflight:
@@ -487,7 +589,7 @@ class Server:
                     continue
                 if pending:
                     time.sleep(max(0.0, min(pending[0].arrival - now(), 0.05)))
-                elif len(done) < len(requests):
+                elif n_done < len(requests):
                     time.sleep(0.002)
         q2.put(None)
         q3.put(None)
@@ -504,4 +606,7 @@ class Server:
             "makespan_s": last - first,
             "requests_per_s": len(lat) / max(last - first, 1e-9),
             "fwi_requests": len(fwi_reqs),
+            "cancelled": sum(r.rid >= 0 for r in cancelled),
+            "failed": sum(r.rid >= 0 for r in failed),
+            **counts,
         }

@@ -187,6 +187,41 @@ def survey3d(nx=400, ny=400, nz=200, nt=3010, npad=40, d=12.5, dt=1e-3, rate=4e-
                     wavelet, souloc.reshape(-1), recloc.reshape(-1), extra={"true": true})
 
 
+# The headline gradient workload: a 400 x 400 x 200 grid at 12.5 m with a
+# 40-cell pad inside it, dt 1 ms, nt 3000, 12 Hz Ricker, a 200 x 200 receiver
+# grid at 25 m spacing and 25 m depth, 4 ms trace sampling, gradient at the
+# true model smoothed by a 250 m Gaussian.
+GRADIENT400 = dict(nx=400, ny=400, nz=200, nt=3000, npad=40, d=12.5, dt=1e-3, rate=4e-3,
+                   freq=12.0, rec_step=2, rec_start=0, rec_depth=25.0, src_depth=25.0,
+                   smooth_m=250.0)
+
+
+def gradient_inputs(kw, rank=0, get_boundary=None, put_boundary=None, vepsdel_to_cij=None):
+    """Inputs of one shot of a gradient workload (kwargs of survey3d): the
+    survey, the starting c_ij, the true c_ij with the pad boundary of the true
+    model (what observed data are modeled with), and the pad and random
+    boundary lists. Each rank's shot sits at its own offset from the centre.
+    The three host functions default to the library's; any implementation of
+    boundary.cpp:10-46 and conversions.cpp:42-50 gives the same arrays."""
+    if get_boundary is None or put_boundary is None or vepsdel_to_cij is None:
+        from . import get_boundary as gb, put_boundary as pb, vepsdel_to_cij as vc
+        get_boundary, put_boundary, vepsdel_to_cij = (get_boundary or gb, put_boundary or pb,
+                                                      vepsdel_to_cij or vc)
+    kw = dict(kw)
+    nx, ny = kw["nx"], kw["ny"]
+    off = [(0, 0), (40, 0), (0, 40), (40, 40), (-40, 0), (0, -40), (-40, -40), (40, -40)]
+    dx, dy = off[rank % len(off)]
+    kw["src_xy"] = (nx // 2 + dx * nx // 400, ny // 2 + dy * ny // 400)
+    s = survey3d(**kw)
+    padb, randb = boundaries3d(s, get_boundary=get_boundary, vepsdel_to_cij=vepsdel_to_cij)
+    n = s.nxyz
+    cstart = np.concatenate(vepsdel_to_cij(s.v, s.eps, s.dl))
+    ctrue = np.concatenate(vepsdel_to_cij(*s.extra["true"]))
+    ctrue = np.concatenate([put_boundary(padb[k * s.nb:(k + 1) * s.nb], ctrue[k * n:(k + 1) * n],
+                                         s.nx, s.ny, s.nz, s.npad) for k in range(3)])
+    return s, cstart.astype(np.float32), ctrue.astype(np.float32), padb, randb
+
+
 def small3d(nx=48, ny=44, nz=40, nt=130, npad=8, d=10.0, dt=7e-4, rate=1.4e-3, freq=25.0,
             seed=3, rec_step=3, nshot=1):
     """A reduced 3D survey for parity tests (CFL-safe: dt^2 lambda_max < 4)."""
@@ -206,10 +241,14 @@ def small3d(nx=48, ny=44, nz=40, nt=130, npad=8, d=10.0, dt=7e-4, rate=1.4e-3, f
     return s
 
 
-def boundaries3d(s: Survey3d, v_true=None, seed=4):
+def boundaries3d(s: Survey3d, v_true=None, seed=4, get_boundary=None, vepsdel_to_cij=None):
     """pad and random boundary lists of c11,c13,c33 (3*nb floats each) built
-    the way objFuncGradientVEpsDel does (objFuncGradient3d_f.cu:261-269)."""
-    from . import get_boundary, vepsdel_to_cij
+    the way objFuncGradientVEpsDel does (objFuncGradient3d_f.cu:261-269).
+    get_boundary / vepsdel_to_cij default to the library's host functions."""
+    if get_boundary is None or vepsdel_to_cij is None:
+        from . import get_boundary as gb, vepsdel_to_cij as vc
+        get_boundary = get_boundary or gb
+        vepsdel_to_cij = vepsdel_to_cij or vc
     v = s.v if v_true is None else v_true
     bv = get_boundary(v, s.nx, s.ny, s.nz, s.npad)
     be = get_boundary(s.eps, s.nx, s.ny, s.nz, s.npad)
