@@ -1,6 +1,6 @@
 #!/usr/bin/env bash
 # Compiles the reference's own VTI GPU path from its sources where they lie
-# under /root/reference (read-only; nothing is copied) into oracle/_ref/:
+# in the reference tree ($REF, read-only; nothing is copied) into oracle/_ref/:
 #   ref3d : lib/vti-fwi-3d/gpu 3D modeling, gradient, RTM (+ the host glue they link)
 #   ref2d : lib/vti-fwi-2d synthetic_f / modeling_f / objFuncGradient_f / GNhessian_f / rtm_f
 #   ref_randb : lib/random-boundary's generator (CPU)

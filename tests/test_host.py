@@ -283,3 +283,32 @@ def test_gradient_inputs_built_by_the_oracle_equal_the_library_ones():
                           vepsdel_to_cij=O.vepsdel_to_cij)
     for x, y in zip(a[1:], b[1:]):
         np.testing.assert_array_equal(x, y)
+
+
+def test_reference_callers_link_against_the_shim():
+    """The reference's own FWI and RTM executables (3D fwi3d-lbfgsc, 3D
+    rtm3d-cij-shot, 2D fwi-lbfgs-c-param with its objFuncGradient.cu glue),
+    compiled from the reference tree with its own headers, link against
+    libvti_wave.so with none of the reference's GPU objects: the entries they
+    call (objFuncGradientVEpsDel, rtmCij3d_f, objFuncGradient_f) are the
+    shim's. Needs the reference tree (oracle/link_callers.sh); nothing runs."""
+    import subprocess
+    r = subprocess.run(["bash", str(ROOT / "oracle" / "link_callers.sh")], capture_output=True,
+                       text=True, timeout=900)
+    if "skipping" in r.stderr:
+        pytest.skip("reference tree not present")
+    assert r.returncode == 0, r.stderr[-3000:]
+    out = ROOT / "oracle" / "_ref" / "callers"
+    for exe in ("fwi3d-lbfgsc", "rtm3d-cij-shot", "fwi-lbfgs-c-param"):
+        assert (out / exe).exists()
+    shim = V.LIB_PATH.parent / "libvti_wave.so"
+    exported = subprocess.run(["nm", "-D", "--defined-only", str(shim)], capture_output=True,
+                              text=True).stdout
+    for obj, sym in (("fwi3d-lbfgsc.cu.o", "objFuncGradientVEpsDel"),
+                     ("rtm3d-cij-shot.cu.o", "rtmCij3d_f"),
+                     ("objFuncGradient.cu.o", "objFuncGradient_f")):
+        undef = subprocess.run(["nm", "-u", "-C", str(out / obj)], capture_output=True,
+                               text=True).stdout
+        assert sym in undef, (obj, sym)          # the caller needs it from outside
+        assert sym in subprocess.run(["c++filt"], input=exported, capture_output=True,
+                                     text=True).stdout, sym  # and the shim exports it

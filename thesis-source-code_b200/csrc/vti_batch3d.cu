@@ -648,6 +648,7 @@ int vti3d_batch_set_options(vti3d_batch* b, int use_graph, int seg_fwd, int seg_
 int vti3d_batch_gradient(vti3d_batch* b, const float* dobs, int dobs_mem, float* fgcij,
                          int fgcij_mem, double* misfit) {
   if (!b) return VTI_ERR_ARG;
+  NvtxRange nv("vti3d batched gradient");
   vti_ctx* ctx = b->ctx;
   VTI_TRY(check_ready(b));
   if (!dobs) return fail(ctx, VTI_ERR_ARG, "null observed data");
@@ -1221,6 +1222,7 @@ int vti3d_engine_submit(vti3d_engine* e, const vti3d_job* job, int* id) {
 
 int vti3d_engine_step(vti3d_engine* e, int ticks, int* active) {
   if (!e || ticks < 0) return VTI_ERR_ARG;
+  NvtxRange nv("vti3d engine ticks");
   vti_ctx* ctx = e->ctx;
   VTI_CUDA(ctx, cudaSetDevice(ctx->device));
   for (int i = 0; i < ticks; ++i) {

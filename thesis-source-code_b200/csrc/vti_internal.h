@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <cstdint>
 #include <cstdio>
 #include <string>
@@ -78,6 +79,15 @@ struct vti_ctx {
 };
 
 namespace vti {
+// NVTX range for the lifetime of the object (header-only NVTX v3: a no-op
+// unless a profiler is attached). Names the passes and calls of the path in
+// timeline tools.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 // Brackets one launch with events on ctx->stream when timing is enabled.
 struct LaunchTimer {
   vti_ctx* ctx;

@@ -208,6 +208,7 @@ int check_finite(vti3d_plan* p, std::initializer_list<const Vol*> vols) {
 // traces recorded into d_trace). Otherwise pass 2 (random-boundary model, no
 // sponge). On return sx[last_cur] holds level M and the other buffer M-1.
 int forward_pass(vti3d_plan* p, const ShotGeom& s, bool sponge) {
+  NvtxRange nv(sponge ? "vti3d pass 1 (sponge, traces)" : "vti3d pass 2 (random boundary)");
   vti_ctx* ctx = p->ctx;
   const vti3d_geom& g = p->g;
   const Dims3& d = p->d;
@@ -257,6 +258,7 @@ int forward_pass(vti3d_plan* p, const ShotGeom& s, bool sponge) {
 // its fused step, from the same current wavefields.
 int backward_pass(vti3d_plan* p, const ShotGeom& s, bool rtm, float* ext = nullptr,
                   int nlag = 0) {
+  NvtxRange nv(rtm ? "vti3d RTM back-propagation" : "vti3d pass 3 (reconstruction, adjoint, imaging)");
   vti_ctx* ctx = p->ctx;
   const vti3d_geom& g = p->g;
   const Dims3& d = p->d;
@@ -339,6 +341,7 @@ int get_obs(vti3d_plan* p, const ShotGeom& s, const float* dobs, int mem, const 
 int run_gradient(vti3d_plan* p, const float* souloc, const int* shotid, int nshot,
                  const float* dobs, int dobs_mem, float* fgcij, int fgcij_mem, double* misfit,
                  bool misfit_only) {
+  NvtxRange nv(misfit_only ? "vti3d misfit" : "vti3d gradient");
   vti_ctx* ctx = p->ctx;
   if (!p->have_model) return fail(ctx, VTI_ERR_ARG, "model not set");
   if ((int)p->wavelet.size() != p->g.nt) return fail(ctx, VTI_ERR_ARG, "wavelet not set");
