@@ -309,6 +309,7 @@ def run_b200(args):
         e2e = run_e2e(args, ctx, s, cstart, padb, randb, dobs.cpu().numpy(), flags)
         errors = None if args.no_check else oracle_errors(ctx, s, cstart, ctrue, padb, randb,
                                                           CHECK_NT)
+        served = None if args.no_served else served_block(args.served_requests, local)
         cpu = None
         if not args.no_cpu:
             import oracle as O
@@ -338,7 +339,7 @@ def run_b200(args):
                          "fwd3d": {"achieved": round(FWD_BYTES_PER_POINT * upd / fwd_avg / 1e9, 1)
                                    if fwd_n else None,
                                    "avg_launch_ms": round(fwd_avg * 1e3, 4)}},
-            "e2e": e2e, "cpu_baseline": cpu, "error_vs_fp64_oracle": errors,
+            "e2e": e2e, "cpu_baseline": cpu, "error_vs_fp64_oracle": errors, "served": served,
             "gpu_launches": launches, "clocks": clk.summary(),
         }
         print(json.dumps(out), flush=True)
@@ -550,6 +551,78 @@ def run_batched(args):
     return out
 
 
+def serve_requests(n, budget, chunk, policy, log=None, fwi=None, with_requests=True,
+                   device=0):
+    """The served form: `n` seeded requests (Poisson 20/s, seed 7) through the
+    continuous-batching server; returns its statistics."""
+    import vtib200.serve as SV
+    srv = SV.Server(device=device, max_bytes=budget, chunk=chunk, keep_results=False, log=log,
+                    policy=policy)
+    t0 = time.perf_counter()
+    st = srv.run(SV.make_requests(n, rate=20.0, seed=7) if with_requests else [], fwi=fwi)
+    st["wall_s"] = time.perf_counter() - t0
+    st["launches"] = srv.ctx3.launches + srv.ctx2.launches
+    srv.close()
+    return st
+
+
+def plain_requests_run(n, log=None, device=0):
+    """The plain form of the same requests: one at a time in arrival order on
+    one stream (3D through vti3d_plan_*, 2D the same calls)."""
+    import vtib200 as V
+    import vtib200.serve as SV
+    ctx = V.Context(device)
+    reqs_p = SV.make_requests(n, rate=20.0, seed=7)
+    t0 = time.perf_counter()
+    lat = []
+    for r in reqs_p:
+        now = time.perf_counter() - t0
+        if r.arrival > now:
+            time.sleep(r.arrival - now)
+        if r.dim == 2:
+            r.make()(ctx)
+        else:
+            job = r.make()
+            if job.kind == V.JOB_MODEL:
+                jc11, jc13, jc33, jw, jso, jrec = job._keep[:6]
+                p = V.Plan3d(ctx, job.g, V.OPT_FULL_STEPS)
+                p.set_model(jc11, jc13, jc33)
+                p.set_wavelet(jw)
+                p.set_receivers(jrec)
+                p.model_data(jso, [0])
+                p.close()
+            else:
+                SV.plain_gradient(ctx, job)
+        lat.append(time.perf_counter() - t0 - r.arrival)
+        if log:
+            log(f"plain request {r.rid} done at {time.perf_counter() - t0:.2f} s")
+    span = time.perf_counter() - t0 - min(r.arrival for r in reqs_p)
+    launches = ctx.launches
+    ctx.close()
+    return {"requests_per_s": round(len(lat) / span, 4), "makespan_s": span,
+            "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "launches": launches}
+
+
+def served_block(n, device=0):
+    """The served half of the headline metric, for the default bench line:
+    `n` requests served (continuous batching, shortest-first) and the same
+    requests one at a time (plain), each request a shot (modeling or
+    gradient) of its own grid."""
+    served = serve_requests(n, 100 << 30, 32, "sjf", device=device)
+    plain = plain_requests_run(n, device=device)
+    return {"requests": n,
+            "workload": f"{n} requests, Poisson 20/s (seed 7): half 2D 201x401..401x801, half "
+                        "3D 128^3..200x400x400, half modeling / half gradient, nt U{2000..4000}, "
+                        "Ricker U[10,15] Hz",
+            "shots_per_s": round(served["requests_per_s"], 4),
+            "p50_s": round(served["p50_s"], 3), "p99_s": round(served["p99_s"], 3),
+            "plain_shots_per_s": plain["requests_per_s"],
+            "plain_p50_s": round(plain["p50_s"], 3), "plain_p99_s": round(plain["p99_s"], 3),
+            "ratio_vs_plain": round(served["requests_per_s"] / plain["requests_per_s"], 3),
+            "wall_s": round(served["wall_s"] + plain["makespan_s"], 1)}
+
+
 def run_served(args):
     """Served workload: Poisson arrivals (mean 20 req/s, seed 7) of mixed
     modeling and gradient requests, half 2D (201x401 .. 401x801) and half 3D
@@ -601,46 +674,11 @@ def run_served(args):
     budget = int(args.budget_gib * (1 << 30))
 
     def serve(fwi=None):
-        srv = SV.Server(max_bytes=budget, chunk=args.chunk, keep_results=False, log=log,
-                        policy=args.policy)
-        t0 = time.perf_counter()
-        st = srv.run(SV.make_requests(args.requests, rate=20.0, seed=7) if fwi is None or
-                     args.requests_with_fwi else [], fwi=fwi)
-        st["wall_s"] = time.perf_counter() - t0
-        st["launches"] = srv.ctx3.launches + srv.ctx2.launches
-        srv.close()
-        return st
+        return serve_requests(args.requests, budget, args.chunk, args.policy, log, fwi=fwi,
+                              with_requests=fwi is None or args.requests_with_fwi)
 
     def plain_requests():
-        """One request at a time in arrival order, one stream."""
-        ctx = V.Context(0)
-        reqs_p = SV.make_requests(args.requests, rate=20.0, seed=7)
-        t0 = time.perf_counter()
-        lat = []
-        for r in reqs_p:
-            now = time.perf_counter() - t0
-            if r.arrival > now:
-                time.sleep(r.arrival - now)
-            if r.dim == 2:
-                r.make()(ctx)
-            else:
-                job = r.make()
-                if job.kind == V.JOB_MODEL:
-                    jc11, jc13, jc33, jw, jso, jrec = job._keep[:6]
-                    p = V.Plan3d(ctx, job.g, V.OPT_FULL_STEPS)
-                    p.set_model(jc11, jc13, jc33)
-                    p.set_wavelet(jw)
-                    p.set_receivers(jrec)
-                    p.model_data(jso, [0])
-                    p.close()
-                else:
-                    SV.plain_gradient(ctx, job)
-            lat.append(time.perf_counter() - t0 - r.arrival)
-            log(f"plain request {r.rid} done at {time.perf_counter() - t0:.2f} s")
-        span = time.perf_counter() - t0 - min(r.arrival for r in reqs_p)
-        ctx.close()
-        return {"requests_per_s": round(len(lat) / span, 4), "makespan_s": span,
-                "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99))}
+        return plain_requests_run(args.requests, log)
 
     with ClockSampler(0) as clk:
         served = serve()
@@ -983,6 +1021,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-check", action="store_true",
                     help="skip the full-grid check against the FP64 oracle")
+    ap.add_argument("--no-served", action="store_true",
+                    help="skip the served-vs-plain block of the gradient line")
+    ap.add_argument("--served-requests", type=int, default=40,
+                    help="gradient line: requests of the served-vs-plain block")
     ap.add_argument("--workload", default="gradient",
                     choices=["gradient", "batched", "served", "gnhv", "forward2d", "parity"],
                     help="batched: many shots on their own windows vs the plain loop")

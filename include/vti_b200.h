@@ -415,11 +415,14 @@ int vti3d_engine_stats(vti3d_engine* e, size_t* used_bytes, int* jobs, int* tick
  * levels (0: 64), recomputed per block in the backward pass; with
  * VTI_GNHV_BF16 the recomputed levels the imaging reads are kept as BF16
  * with one FP32 scale per z plane (half the segment memory; checkpoints
- * stay FP32, so the recomputation is exact).
+ * stay FP32, so the recomputation is exact), rounded to nearest, or
+ * stochastically with VTI_GNHV_BF16_SR (each stored value unbiased,
+ * independent errors from level to level).
  * Outputs (host, each may be NULL): hv = H dc (3*nxyz), grad = dJ/dc of
  * J = 1/2|d - dobs|^2 (3*nxyz; needs dobs), misfit = J, traces d and Born
  * traces (nnt*nrec each). souloc: 5 floats (x, y, z, nrec, 0). */
 #define VTI_GNHV_BF16 1u /* background levels of the imaging stored as BF16 + plane scales */
+#define VTI_GNHV_BF16_SR 2u /* with VTI_GNHV_BF16: stochastic instead of nearest rounding */
 int vti3d_gnhv_exact(vti_ctx* ctx, const vti3d_geom* g, const float* c11, const float* c13,
                      const float* c33, const float* dc, const float* wavelet, const float* souloc,
                      const float* recloc, int nrec, const float* dobs, int checkpoint_every,

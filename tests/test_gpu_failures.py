@@ -65,7 +65,7 @@ def test_plan_refuses_an_unstable_model(ctx):
     assert e.value.status == V.VTI_ERR_CFL
     # a stable call on the same context still works
     d = V.modelDataCij3d_f(ctx, g, s.souloc, [0], s.recloc, s.wavelet, c[:n], c[n:2 * n],
-                           c[2 * n:])
+                           c[2 * n:], flags=V.OPT_FULL_STEPS)
     assert np.isfinite(d).all() and np.abs(d).max() > 0
 
 
@@ -143,5 +143,5 @@ def test_bounded_wait_gives_up_and_reports_a_timeout(ctx):
     n = s.nxyz
     c = s.cij()
     d = V.modelDataCij3d_f(ctx, s.geom(), s.souloc, [0], s.recloc, s.wavelet, c[:n],
-                           c[n:2 * n], c[2 * n:])
+                           c[n:2 * n], c[2 * n:], flags=V.OPT_FULL_STEPS)
     assert np.isfinite(d).all() and np.abs(d).max() > 0

@@ -362,7 +362,40 @@ __global__ void __launch_bounds__(NTHREADS, 2)
 // The background levels the adjoint images against are stored as bfloat16
 // with one FP32 scale per z plane (value = bf16 * scale[z + kZPad]; the
 // scale is the plane's largest magnitude, pad planes hold 0).
-__global__ void k_pack_bf16(const float* src, Dims3 d, __nv_bfloat16* dst, float* scale) {
+//
+// Rounding: nearest by default. Stochastic rounding (VTI_GNHV_BF16_SR;
+// Connolly, Higham & Mary, "Stochastic rounding and its probabilistic
+// backward error analysis", SIAM J. Sci. Comput. 43(1), 2021) rounds x up to
+// the next BF16 value with probability (x - lower) / ulp, so each stored
+// value is unbiased and the errors of different levels are independent. It
+// pays when round-to-nearest errors add coherently over the imaging sum; on
+// the reduced config-4 case they do not, and stochastic rounding's larger
+// per-value variance (ulp^2/6 against ulp^2/12) gives about twice the image
+// error, so nearest stays the default. Implemented on the bits: the
+// FP32 pattern plus 16 random low bits, truncated to its upper 16 bits
+// (carries into the exponent round the magnitude up across a binade, as
+// they should). The random bits are a counter hash of (level, plane, cell),
+// so a run is reproducible.
+__device__ __forceinline__ uint32_t mix32(uint32_t x) {
+  // xorshift-multiply integer hash (constants of a published low-bias
+  // 32-bit mixer)
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
+}
+
+__device__ __forceinline__ __nv_bfloat16 bf16_stochastic(float x, uint32_t r) {
+  const uint32_t b = __float_as_uint(x) + (r & 0xffffu);
+  __nv_bfloat16_raw raw;
+  raw.x = (unsigned short)(b >> 16);
+  return __nv_bfloat16(raw);
+}
+
+__global__ void k_pack_bf16(const float* src, Dims3 d, __nv_bfloat16* dst, float* scale,
+                            uint32_t seed, int stochastic) {
   const int z = blockIdx.x;
   const float* s = src + (long long)z * d.plane;
   __nv_bfloat16* o = dst + (long long)z * d.plane;
@@ -383,8 +416,11 @@ __global__ void k_pack_bf16(const float* src, Dims3 d, __nv_bfloat16* dst, float
   const float sc = wm[0] > 0.f ? wm[0] : 1.f;
   const float inv = 1.f / sc;
   if (threadIdx.x == 0) scale[z + kZPad] = sc;
-  for (int i = threadIdx.x; i < n; i += blockDim.x)
-    o[i] = __float2bfloat16_rn(i % d.pitch < d.nx ? s[i] * inv : 0.f);
+  const uint32_t zs = mix32(seed ^ (0x9e3779b9u * (uint32_t)(z + 1)));
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const float x = i % d.pitch < d.nx ? s[i] * inv : 0.f;
+    o[i] = stochastic ? bf16_stochastic(x, mix32(zs + (uint32_t)i)) : __float2bfloat16_rn(x);
+  }
 }
 
 __device__ __forceinline__ float2 ldb2(const __nv_bfloat16* p) {
@@ -684,6 +720,7 @@ struct GnState {
   vti3d_geom g{};
   Dims3 d{};
   int M = 0, K = 0;
+  bool stochastic = false;  // BF16 packing: stochastic rounding (else nearest)
   VolM c[3], dc[3];
   VolM a[2][2], b[2][2];       // [buffer][x, z]
   std::vector<VolM> ck;        // checkpoint k: levels k*K (x, z), k*K+1 (x, z)
@@ -879,8 +916,11 @@ int launch_adj_b16(GnState& S, int im, int cur, int slot) {
   return VTI_OK;
 }
 
-int pack(GnState& S, const VolM& src, VolB& dst) {
-  k_pack_bf16<<<S.d.nz, 256, 0, S.ctx->stream>>>(src.v.origin, S.d, dst.origin, dst.scale);
+// level: time level of the packed field, component: 0 x, 1 z (random bits)
+int pack(GnState& S, const VolM& src, VolB& dst, int level, int component) {
+  const uint32_t seed = (uint32_t)level * 2u + (uint32_t)component;
+  k_pack_bf16<<<S.d.nz, 256, 0, S.ctx->stream>>>(src.v.origin, S.d, dst.origin, dst.scale, seed,
+                                                 S.stochastic ? 1 : 0);
   VTI_LAUNCHED(S.ctx, "k_pack_bf16");
   return VTI_OK;
 }
@@ -905,6 +945,8 @@ int vti3d_gnhv_exact(vti_ctx* ctx, const vti3d_geom* g, const float* c11, const 
                      float* born) {
   if (!ctx || !g) return VTI_ERR_ARG;
   const bool b16 = (gn_flags & VTI_GNHV_BF16) != 0;
+  if ((gn_flags & VTI_GNHV_BF16_SR) && !b16)
+    return fail(ctx, VTI_ERR_ARG, "VTI_GNHV_BF16_SR needs VTI_GNHV_BF16");
   VTI_TRY(p3d::check_geom(ctx, g));
   if (!c11 || !c13 || !c33 || !wavelet || !souloc || (nrec > 0 && !recloc))
     return fail(ctx, VTI_ERR_ARG, "null input");
@@ -928,6 +970,7 @@ int vti3d_gnhv_exact(vti_ctx* ctx, const vti3d_geom* g, const float* c11, const 
   VTI_TRY(p3d::upload_shot(p, sg));
   GnState S;
   S.ctx = ctx;
+  S.stochastic = (gn_flags & VTI_GNHV_BF16_SR) != 0;
   S.g = *g;
   S.d = p->d;
   S.M = p3d::last_level(*g, flags);
@@ -1060,8 +1103,8 @@ int vti3d_gnhv_exact(vti_ctx* ctx, const vti3d_geom* g, const float* c11, const 
     }
     if (b16)
       for (int f = 0; f < 2; ++f) {
-        VTI_TRY(pack(S, lvl(k0 - 1)[f], S.segb[f]));
-        VTI_TRY(pack(S, lvl(k0)[f], S.segb[2 + f]));
+        VTI_TRY(pack(S, lvl(k0 - 1)[f], S.segb[f], k0 - 1, f));
+        VTI_TRY(pack(S, lvl(k0)[f], S.segb[2 + f], k0, f));
       }
     Damping dmp{S.damp, S.damp + g->nx, S.damp + g->nx + g->ny};
     for (int t = k0 + 1; t <= k1; ++t) {
@@ -1075,8 +1118,8 @@ int vti3d_gnhv_exact(vti_ctx* ctx, const vti3d_geom* g, const float* c11, const 
                                sxs, sys, szs, ps, Probe(), true));
       if (b16) {
         const int sl = t - (k0 - 1);
-        VTI_TRY(pack(S, nx_[0], S.segb[2 * sl]));
-        VTI_TRY(pack(S, nx_[1], S.segb[2 * sl + 1]));
+        VTI_TRY(pack(S, nx_[0], S.segb[2 * sl], t, 0));
+        VTI_TRY(pack(S, nx_[1], S.segb[2 * sl + 1], t, 1));
       }
     }
     for (int tm1 = k1; tm1 >= k0; --tm1) {

@@ -530,6 +530,7 @@ class Engine3d:
 
 
 GNHV_BF16 = 1
+GNHV_BF16_SR = 2  # with GNHV_BF16: stochastic rounding (default: nearest)
 
 
 def gnhv_exact(ctx, g: Geom3d, c11, c13, c33, wavelet, souloc, recloc, dc=None, dobs=None,
