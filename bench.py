@@ -204,8 +204,8 @@ def oracle_errors(ctx, s, cstart, ctrue, padb, randb, nt):
     og = OracleGeom(sh)
     o64, m64 = O.gradient3d(og, cstart, padb, randb, sh.wavelet, sh.souloc, [0], sh.recloc,
                             dobs, dtype=np.float64, full_steps=True, want_modeled=True)
-    o32 = O.gradient3d(og, cstart, padb, randb, sh.wavelet, sh.souloc, [0], sh.recloc, dobs,
-                       dtype=np.float32, full_steps=True)
+    o32, m32 = O.gradient3d(og, cstart, padb, randb, sh.wavelet, sh.souloc, [0], sh.recloc,
+                            dobs, dtype=np.float32, full_steps=True, want_modeled=True)
 
     def rl2(a, b):
         a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
@@ -217,6 +217,7 @@ def oracle_errors(ctx, s, cstart, ctrue, padb, randb, nt):
             "traces_rel_l2": rl2(dmod, m64), "misfit_rel": abs(mis - o64[0]) / o64[0],
             "gradient_rel_l2": [rl2(part(fg, k), part(o64, k)) for k in range(3)],
             "fp32_oracle_gradient_rel_l2": [rl2(part(o32, k), part(o64, k)) for k in range(3)],
+            "fp32_oracle_traces_rel_l2": rl2(m32, m64),
             "tolerance": {"traces": 1e-5, "misfit": 1e-5, "gradient": 1e-4},
             "seconds": round(time.perf_counter() - t0, 1)}
 
@@ -492,6 +493,37 @@ def run_batched(args):
     area = sum(w[2] * w[3] for w in wins)
     pts = 4.0 * (M - 1) * area * s.nz
     upd = sum((w[2] - 8) * (w[3] - 8) for w in wins) * s.nz
+    # windowed plain: the same windows (the batch's own window models and
+    # random boundaries), one shot at a time through vti3d_plan_gradient; a
+    # sample of the windows is timed and the total scaled by window area
+    nwin = max(1, min(args.plain_shots, args.shots))
+    pick = sorted(set(int(round(i * (args.shots - 1) / max(nwin - 1, 1))) for i in range(nwin)))
+    win_ms, win_area = 0.0, 0
+    for j in pick:
+        x0, y0, wx, wy = wins[j]
+        gs = V.geom3d(wx, wy, g.nz, g.nt, g.npad, g.dx, g.dy, g.dz, g.dt, g.sampling_rate,
+                      ox=g.ox + x0 * g.dx, oy=g.oy + y0 * g.dy, oz=g.oz, ot=g.ot)
+        ns = wx * wy * g.nz
+        cpad, crand = b.shot_models(j)
+        randb = np.concatenate([V.get_boundary(crand[k * ns:(k + 1) * ns], wx, wy, g.nz, g.npad)
+                                for k in range(3)])
+        pw = V.Plan3d(ctx, gs, flags)
+        pw.set_model(cpad[:ns], cpad[ns:2 * ns], cpad[2 * ns:], randb=randb)
+        pw.set_wavelet(s.wavelet)
+        pw.set_receivers(recloc)
+        fgw = torch.zeros(1 + 3 * ns, dtype=torch.float32, device="cuda")
+        so = souloc[5 * j:5 * j + 5]
+        pw.gradient(so, [0], dobs.data_ptr(), V.MEM_DEVICE, fgw.data_ptr(), V.MEM_DEVICE)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        pw.gradient(so, [0], dobs.data_ptr(), V.MEM_DEVICE, fgw.data_ptr(), V.MEM_DEVICE)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        win_ms += e0.elapsed_time(e1)
+        win_area += wx * wy
+        pw.close()
+        del fgw
+    windowed_ms = win_ms * area / win_area  # all windows, one at a time
     b.close()
     # plain per-shot loop on the full model
     padb, randb = S.boundaries3d(s)
@@ -534,6 +566,12 @@ def run_batched(args):
                   "gpts": round(4.0 * (M - 1) * n / (plain_ms / 1e3) / 1e9, 2),
                   "api": "vti3d_plan_gradient, full model, one shot at a time"},
         "speedup_vs_plain": round(shots_s / plain_s, 3),
+        "windowed_plain": {"value": round(args.shots / (windowed_ms / 1e3), 4), "unit": "shots/s",
+                           "windows_timed": len(pick), "timed_ms": round(win_ms, 1),
+                           "api": "vti3d_plan_gradient on each shot's own window (the batch's "
+                                  "window models), one at a time; total scaled from the timed "
+                                  "windows by window area"},
+        "speedup_vs_windowed_plain": round(shots_s / (args.shots / (windowed_ms / 1e3)), 3),
         "roofline": {"bound": "hbm", "kernel": "k_bwd3d_tma (batched)",
                      "achieved": round(achieved, 1) if achieved else None, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s",
@@ -758,6 +796,11 @@ def run_gnhv(args):
         ct = s.cij(vt, s.eps, s.dl)
         return s, c, ct, dc
 
+    bf16 = args.gn_mode == "bf16"
+    gflags = V.GNHV_BF16 if bf16 else 0
+    # FP32 background: the whole segment of K+1 levels is FP32, so K is chosen
+    # near sqrt(2 M) (segment and checkpoint memory balanced)
+    gk = args.gn_k if (bf16 or args.gn_k != 126) else max(16, int(round(np.sqrt(2.0 * (nt - 1)))))
     ctx = V.Context(0)
     s, c, ct, dc = case(nx, ny, nz, nt, 40)
     g = s.geom()
@@ -768,14 +811,14 @@ def run_gnhv(args):
     log = lambda m: print(m, file=sys.stderr, flush=True)  # noqa: E731
     log("model ready")
     dobs = V.gnhv_exact(ctx, g, *[ct[k * n:(k + 1) * n] for k in range(3)], s.wavelet, so,
-                        s.recloc, checkpoint_every=args.gn_k, want=("traces",))["traces"]
+                        s.recloc, checkpoint_every=gk, want=("traces",))["traces"]
     log("observed traces ready")
     launches0 = ctx.launches
     ctx.set_timing(True)
     with ClockSampler(0) as clk:
         t0 = time.perf_counter()
         out = V.gnhv_exact(ctx, g, *cs, s.wavelet, so, s.recloc, dc=dc, dobs=dobs,
-                           checkpoint_every=args.gn_k, want=("hv", "grad"), flags=V.GNHV_BF16)
+                           checkpoint_every=gk, want=("hv", "grad"), flags=gflags)
         wall = time.perf_counter() - t0
     adj_ms, adj_n = ctx.kernel_time("bwd3d")
     fwd_ms, fwd_n = ctx.kernel_time("fwd3d")
@@ -788,7 +831,8 @@ def run_gnhv(args):
     upd = (nx - 8) * (ny - 8) * nz
     peak, peak_kind = peaks()
     adj_avg = adj_ms / max(adj_n, 1) / 1e3
-    achieved = 80 * upd / adj_avg / 1e9 if adj_n else None
+    adj_bytes = 80 if bf16 else 84
+    achieved = adj_bytes * upd / adj_avg / 1e9 if adj_n else None
     log("reduced grid vs the FP64 oracle")
     r = args.gn_check
     sr, cr, ctr, dcr = case(r[0], r[1], r[2], args.gn_check_nt, 8)
@@ -802,7 +846,7 @@ def run_gnhv(args):
     dob = O.exact_forward3d(gr, *[ctr[k * nr_:(k + 1) * nr_].astype(np.float64)
                                   for k in range(3)], sr.wavelet, sor, [0], sr.recloc)
     gpu = V.gnhv_exact(ctx, gr, *csr, sr.wavelet, sor, sr.recloc, dc=dcr,
-                       dobs=dob.astype(np.float32), checkpoint_every=16, flags=V.GNHV_BF16)
+                       dobs=dob.astype(np.float32), checkpoint_every=16, flags=gflags)
     ctx.close()
     tr = O.exact_forward3d(gr, *c64, sr.wavelet, sor, [0], sr.recloc)
     bo = O.exact_born3d(gr, *c64, sr.wavelet, sor, [0], sr.recloc, dcr)
@@ -822,18 +866,20 @@ def run_gnhv(args):
         "metric": "3D exact-mode Gauss-Newton H*v + gradient (grid-point updates/s)",
         "value": round(pts / wall / 1e9, 3), "unit": "Gpts/s", "n_gpus": 1, "steps": 1,
         "warmup": 0, "ms_per_step": round(wall * 1e3, 1), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (BF16 stored background)",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 (BF16 stored background)" if bf16 else "f32",
         "data": "synthetic (seeded layered VTI + GRF model, GRF input vector)",
         "config": {"workload": f"GN H*v + gradient, {nx}x{ny}x{nz} at 10 m, nt={nt}, dt=0.75 ms, "
-                               f"checkpoints every {args.gn_k} levels, BF16 background",
+                               f"checkpoints every {gk} levels, "
+                               f"{'BF16' if bf16 else 'FP32'} background",
                    "grid": [nx, ny, nz], "nt": nt, "receivers": int(s.recloc.size // 4),
-                   "checkpoint_every": args.gn_k, "misfit": out["misfit"],
+                   "checkpoint_every": gk, "background": args.gn_mode, "misfit": out["misfit"],
                    "updates_per_level": "5 (background+Born, recomputation, 2 adjoints)"},
-        "roofline": {"bound": "hbm", "kernel": "k_adj3d_b16",
+        "roofline": {"bound": "hbm", "kernel": "k_adj3d_b16" if bf16 else "k_adj3d_tma",
                      "achieved": round(achieved, 1) if achieved else None, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": round(achieved / peak, 4) if achieved else None, "traffic": None,
-                     "bytes_per_point": 80, "avg_launch_ms": round(adj_avg * 1e3, 4),
+                     "bytes_per_point": adj_bytes, "avg_launch_ms": round(adj_avg * 1e3, 4),
                      "forward_kernels_ms": round(fwd_ms, 1), "forward_launches": int(fwd_n)},
         "error_vs_fp64_oracle": errs,
         "e2e": {"value": round(pts / wall / 1e9, 3), "unit": "Gpts/s",
@@ -1048,6 +1094,8 @@ def main():
     ap.add_argument("--gn-grid", type=int, nargs=3, default=[600, 600, 300],
                     help="gnhv workload: nx ny nz")
     ap.add_argument("--gn-k", type=int, default=126, help="gnhv workload: checkpoint interval")
+    ap.add_argument("--gn-mode", default="bf16", choices=["bf16", "fp32"],
+                    help="gnhv workload: storage of the recomputed background levels")
     ap.add_argument("--gn-check", type=int, nargs=3, default=[44, 56, 40],
                     help="gnhv workload: reduced grid of the FP64 oracle check")
     ap.add_argument("--gn-check-nt", type=int, default=300)

@@ -378,13 +378,19 @@ struct BwdArgs {
   int* status;
 };
 
-constexpr int B_STAGES = 3;
-// stage: [sigma_x halo][lambda_x halo][sz+4][lz+4][spx][spz][lpx][lpz][c11 c13 c33][g11 g13 g33]
+constexpr int B_STAGES = 4;
+// stage: [sigma_x halo][lambda_x halo][sz+4][lz+4][spx][spz][lpx][lpz][c11 c13 c33]
+// The gradient tiles are not staged: each consumer thread reads its own
+// g11/g13/g33 pair with plain loads issued before it waits for the plane's
+// stage (it alone reads and writes those cells), which keeps a stage at
+// 26 KB so that four stages of two CTAs fit one SM (three stages in flight
+// per CTA instead of two).
 constexpr int B_OFF_SH = 0;
 constexpr int B_OFF_LH = HALO_BYTES;
-constexpr int B_OFF_P = 2 * HALO_BYTES;  // 10 plain tiles from here
-constexpr int B_STAGE_BYTES = B_OFF_P + 12 * PLAIN_BYTES;  // 32256
+constexpr int B_OFF_P = 2 * HALO_BYTES;  // 9 plain tiles from here
+constexpr int B_STAGE_BYTES = B_OFF_P + 9 * PLAIN_BYTES;  // 26112
 constexpr int B_SMEM = B_STAGES * B_STAGE_BYTES + 1024 + 2 * B_STAGES * 8;
+static_assert(2 * B_SMEM <= 228 * 1024, "two backward CTAs per SM");
 
 struct BwdMaps {
   CUtensorMap scx, scz, spx, spz, lcx, lcz, lpx, lpz, c11, c13, c33, g11, g13, g33;
@@ -407,7 +413,7 @@ __device__ __forceinline__ bool bwd_produce(const BwdCommon& a, const BwdMaps& m
     const int zp = z + kZPad;
     unsigned char* st = smem + s * B_STAGE_BYTES;
     unsigned char* pl = st + B_OFF_P;
-    mbar_arrive_expect_tx(&full[s], kRtm ? B_STAGE_BYTES - 2 * PLAIN_BYTES : B_STAGE_BYTES);
+    mbar_arrive_expect_tx(&full[s], B_STAGE_BYTES);
     tma_load(st + B_OFF_SH, &m.scx, &full[s], x0 - kHalo, y0 - kHalo, zp);
     tma_load(st + B_OFF_LH, &m.lcx, &full[s], x0 - kHalo, y0 - kHalo, zp);
     tma_load(pl + 0 * PLAIN_BYTES, &m.scz, &full[s], x0, y0, zp + kHalo);
@@ -419,11 +425,6 @@ __device__ __forceinline__ bool bwd_produce(const BwdCommon& a, const BwdMaps& m
     tma_load(pl + 6 * PLAIN_BYTES, &m.c11, &full[s], x0, y0, zp);
     tma_load(pl + 7 * PLAIN_BYTES, &m.c13, &full[s], x0, y0, zp);
     tma_load(pl + 8 * PLAIN_BYTES, &m.c33, &full[s], x0, y0, zp);
-    tma_load(pl + 9 * PLAIN_BYTES, &m.g11, &full[s], x0, y0, zp);
-    if (!kRtm) {
-      tma_load(pl + 10 * PLAIN_BYTES, &m.g13, &full[s], x0, y0, zp);
-      tma_load(pl + 11 * PLAIN_BYTES, &m.g33, &full[s], x0, y0, zp);
-    }
   }
   return true;
 }
@@ -474,9 +475,22 @@ __device__ __forceinline__ bool bwd_consume(const BwdCommon& a, const BwdPar& bp
 #pragma unroll
   for (int j = 0; j < 4; ++j) dzr[j] = z0 - 4 + j >= 0 ? a.dampz[z0 - 4 + j] : 1.f;
   float dz_next = a.dampz[z0];
+  // this thread's gradient pair of a plane (read with plain loads)
+  const bool anyv = v0 || v1;
+  auto gload = [&](int zz, float2& r11, float2& r13, float2& r33) {
+    const long long i = (long long)zz * a.d.plane + off;
+    const float2 zero = make_float2(0.f, 0.f);
+    r11 = anyv ? __ldg(reinterpret_cast<const float2*>(a.g11 + i)) : zero;
+    r13 = (anyv && !kRtm) ? __ldg(reinterpret_cast<const float2*>(a.g13 + i)) : zero;
+    r33 = (anyv && !kRtm) ? __ldg(reinterpret_cast<const float2*>(a.g33 + i)) : zero;
+  };
   for (int z = z0; z < z1; ++z, ++k) {
     const float dz = dz_next;
     if (z + 1 < z1) dz_next = a.dampz[z + 1];
+    // issued before the stage wait: the loads complete while the stage
+    // arrives and the stencils are evaluated
+    float2 g11o, g13o, g33o;
+    gload(z, g11o, g13o, g33o);
 #pragma unroll
     for (int j = 0; j < 3; ++j) dzr[j] = dzr[j + 1];
     dzr[3] = dz;
@@ -522,9 +536,6 @@ __device__ __forceinline__ bool bwd_consume(const BwdCommon& a, const BwdPar& bp
     const float2 spx = ld2(pl + 2 * T), spz = ld2(pl + 3 * T);
     const float2 lpx = ld2(pl + 4 * T), lpz = ld2(pl + 5 * T);
     const float2 c11 = ld2(pl + 6 * T), c13 = ld2(pl + 7 * T), c33 = ld2(pl + 8 * T);
-    const float2 g11o = ld2(pl + 9 * T);
-    const float2 g13o = kRtm ? make_float2(0.f, 0.f) : ld2(pl + 10 * T);
-    const float2 g33o = kRtm ? make_float2(0.f, 0.f) : ld2(pl + 11 * T);
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[s]);
     float snx[2], snz[2], lnx[2], lnz[2], g11[2], g13[2], g33[2];
