@@ -154,6 +154,7 @@ struct Probe {
 struct TileMaps {
   alignas(64) unsigned char plain[128];
   alignas(64) unsigned char halo[128];
+  const float* origin = nullptr;  // plane 0 of the volume (FP32 volumes; kernels that read it directly)
 };
 int make_tile_maps(vti_ctx* ctx, const Dims3& d, const Vol& v, TileMaps* out);
 // The same over a volume of `elem_bytes` (4: float, 2: bfloat16) elements

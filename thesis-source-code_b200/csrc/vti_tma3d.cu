@@ -59,6 +59,9 @@ struct FwdCommon {
   PointSource src;     // amp: single launches only
   const float* amp;    // batched: source amplitude per step
   int t0;              // batched: tick of the job's step 0
+  const float* c11;    // the model, read per point with read-only loads
+  const float* c13;
+  const float* c33;
 };
 struct FwdPar {
   const float* cz;  // cur sigma_z (queue initialisation)
@@ -72,19 +75,33 @@ struct FwdArgs {
   int* status;
 };
 
-constexpr int F_STAGES = 4;
-// stage layout: [halo x][z+4][prev x][prev z][c11][c13][c33]
+constexpr int F_STAGES = 6;
+// stage layout: [halo x][z+4][prev x][prev z]. The model (c11, c13, c33) is
+// not staged: each consumer thread reads its own pair with read-only loads
+// issued before it waits for the plane's stage, so a stage is 10 KB and six
+// of them per CTA fit three CTAs per SM (five stages in flight per CTA).
 constexpr int F_OFF_H = 0;
 constexpr int F_OFF_Z = HALO_BYTES;
 constexpr int F_OFF_PX = F_OFF_Z + PLAIN_BYTES;
 constexpr int F_OFF_PZ = F_OFF_PX + PLAIN_BYTES;
-constexpr int F_OFF_C = F_OFF_PZ + PLAIN_BYTES;
-constexpr int F_STAGE_BYTES = F_OFF_C + 3 * PLAIN_BYTES;  // 15872
+constexpr int F_STAGE_BYTES = F_OFF_PZ + PLAIN_BYTES;  // 9984
 constexpr int F_SMEM = F_STAGES * F_STAGE_BYTES + 1024 + 2 * F_STAGES * 8;
+static_assert(3 * F_SMEM <= 228 * 1024, "three forward CTAs per SM");
 
 struct FwdMaps {
-  CUtensorMap cx, cz, px, pz, c11, c13, c33;
+  CUtensorMap cx, cz, px, pz;
 };
+
+// The model pair of one thread at plane z (zeros where neither point is in
+// the update region; x + 1 < pitch always).
+__device__ __forceinline__ void model_pair(const float* c11, const float* c13, const float* c33,
+                                           long long i, bool any, float2& a11, float2& a13,
+                                           float2& a33) {
+  const float2 zero = make_float2(0.f, 0.f);
+  a11 = any ? __ldg(reinterpret_cast<const float2*>(c11 + i)) : zero;
+  a13 = any ? __ldg(reinterpret_cast<const float2*>(c13 + i)) : zero;
+  a33 = any ? __ldg(reinterpret_cast<const float2*>(c33 + i)) : zero;
+}
 
 // Producer side of one item: TMA loads of every plane of the item's range.
 __device__ __forceinline__ bool fwd_produce(const FwdCommon& a, const FwdMaps& m, int* status,
@@ -104,9 +121,6 @@ __device__ __forceinline__ bool fwd_produce(const FwdCommon& a, const FwdMaps& m
     tma_load(st + F_OFF_Z, &m.cz, &full[s], x0, y0, zp + kHalo);
     tma_load(st + F_OFF_PX, &m.px, &full[s], x0, y0, zp);
     tma_load(st + F_OFF_PZ, &m.pz, &full[s], x0, y0, zp);
-    tma_load(st + F_OFF_C, &m.c11, &full[s], x0, y0, zp);
-    tma_load(st + F_OFF_C + PLAIN_BYTES, &m.c13, &full[s], x0, y0, zp);
-    tma_load(st + F_OFF_C + 2 * PLAIN_BYTES, &m.c33, &full[s], x0, y0, zp);
   }
   return true;
 }
@@ -172,11 +186,14 @@ __device__ __forceinline__ bool fwd_consume(const FwdCommon& a, const FwdPar& bp
 #pragma unroll
     for (int j = 0; j < 3; ++j) dzr[j] = dzr[j + 1];
     dzr[3] = dz;
+    // the model pair: loads issued before the stage wait
+    float2 c11, c13, c33;
+    model_pair(a.c11, a.c13, a.c33, (long long)z * a.d.plane + off, v0 || v1, c11, c13, c33);
     const int s = (int)(k % F_STAGES);
     if (!mbar_wait(&full[s], (uint32_t)((k / F_STAGES) & 1), status)) return false;
     const unsigned char* st = smem + s * F_STAGE_BYTES;
     const float* sh = (const float*)(st + F_OFF_H) + sr;
-    const float* pl = (const float*)(st + F_OFF_Z) + pi;  // [z+4][prev x][prev z][c11][c13][c33]
+    const float* pl = (const float*)(st + F_OFF_Z) + pi;  // [z+4][prev x][prev z]
     constexpr int T = TX * TY;
 #pragma unroll
     for (int kk = 0; kk < 8; ++kk) {
@@ -201,7 +218,6 @@ __device__ __forceinline__ bool fwd_consume(const FwdCommon& a, const FwdPar& bp
       yp[j] = ld2(sh + (j + 1) * HX);
     }
     const float2 px = ld2(pl + T), pz = ld2(pl + 2 * T);
-    const float2 c11 = ld2(pl + 3 * T), c13 = ld2(pl + 4 * T), c33 = ld2(pl + 5 * T);
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[s]);
     float nxv[2], nzv[2];
@@ -363,6 +379,9 @@ struct BwdCommon {
   PointSource src;
   const float* amp;
   int t0;
+  const float* c11;  // the model, read per point with read-only loads
+  const float* c13;
+  const float* c33;
 };
 struct BwdPar {
   const float* scz;  // cur sigma_z, lambda_z (queue initialisation)
@@ -378,22 +397,22 @@ struct BwdArgs {
   int* status;
 };
 
-constexpr int B_STAGES = 4;
-// stage: [sigma_x halo][lambda_x halo][sz+4][lz+4][spx][spz][lpx][lpz][c11 c13 c33]
-// The gradient tiles are not staged: each consumer thread reads its own
-// g11/g13/g33 pair with plain loads issued before it waits for the plane's
-// stage (it alone reads and writes those cells), which keeps a stage at
-// 26 KB so that four stages of two CTAs fit one SM (three stages in flight
-// per CTA instead of two).
+constexpr int B_STAGES = 5;
+// stage: [sigma_x halo][lambda_x halo][sz+4][lz+4][spx][spz][lpx][lpz]
+// The model and gradient tiles are not staged: each consumer thread reads
+// its own c11/c13/c33 and g11/g13/g33 pairs with plain loads issued before
+// it waits for the plane's stage (it alone writes those gradient cells),
+// which keeps a stage at 20 KB so that five stages of two CTAs fit one SM
+// (four stages in flight per CTA).
 constexpr int B_OFF_SH = 0;
 constexpr int B_OFF_LH = HALO_BYTES;
-constexpr int B_OFF_P = 2 * HALO_BYTES;  // 9 plain tiles from here
-constexpr int B_STAGE_BYTES = B_OFF_P + 9 * PLAIN_BYTES;  // 26112
+constexpr int B_OFF_P = 2 * HALO_BYTES;  // 6 plain tiles from here
+constexpr int B_STAGE_BYTES = B_OFF_P + 6 * PLAIN_BYTES;  // 19968
 constexpr int B_SMEM = B_STAGES * B_STAGE_BYTES + 1024 + 2 * B_STAGES * 8;
 static_assert(2 * B_SMEM <= 228 * 1024, "two backward CTAs per SM");
 
 struct BwdMaps {
-  CUtensorMap scx, scz, spx, spz, lcx, lcz, lpx, lpz, c11, c13, c33, g11, g13, g33;
+  CUtensorMap scx, scz, spx, spz, lcx, lcz, lpx, lpz;
 };
 
 // wave3d.h:5-6 recording / imaging weights, as float
@@ -422,9 +441,6 @@ __device__ __forceinline__ bool bwd_produce(const BwdCommon& a, const BwdMaps& m
     tma_load(pl + 3 * PLAIN_BYTES, &m.spz, &full[s], x0, y0, zp);
     tma_load(pl + 4 * PLAIN_BYTES, &m.lpx, &full[s], x0, y0, zp);
     tma_load(pl + 5 * PLAIN_BYTES, &m.lpz, &full[s], x0, y0, zp);
-    tma_load(pl + 6 * PLAIN_BYTES, &m.c11, &full[s], x0, y0, zp);
-    tma_load(pl + 7 * PLAIN_BYTES, &m.c13, &full[s], x0, y0, zp);
-    tma_load(pl + 8 * PLAIN_BYTES, &m.c33, &full[s], x0, y0, zp);
   }
   return true;
 }
@@ -489,8 +505,9 @@ __device__ __forceinline__ bool bwd_consume(const BwdCommon& a, const BwdPar& bp
     if (z + 1 < z1) dz_next = a.dampz[z + 1];
     // issued before the stage wait: the loads complete while the stage
     // arrives and the stencils are evaluated
-    float2 g11o, g13o, g33o;
+    float2 g11o, g13o, g33o, c11, c13, c33;
     gload(z, g11o, g13o, g33o);
+    model_pair(a.c11, a.c13, a.c33, (long long)z * a.d.plane + off, anyv, c11, c13, c33);
 #pragma unroll
     for (int j = 0; j < 3; ++j) dzr[j] = dzr[j + 1];
     dzr[3] = dz;
@@ -535,7 +552,6 @@ __device__ __forceinline__ bool bwd_consume(const BwdCommon& a, const BwdPar& bp
     }
     const float2 spx = ld2(pl + 2 * T), spz = ld2(pl + 3 * T);
     const float2 lpx = ld2(pl + 4 * T), lpz = ld2(pl + 5 * T);
-    const float2 c11 = ld2(pl + 6 * T), c13 = ld2(pl + 7 * T), c33 = ld2(pl + 8 * T);
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[s]);
     float snx[2], snz[2], lnx[2], lnz[2], g11[2], g13[2], g33[2];
@@ -746,7 +762,9 @@ Sched make_sched(vti_ctx* ctx, const Dims3& d, int ctas_per_sm) {
 
 
 int make_tile_maps(vti_ctx* ctx, const Dims3& d, const Vol& v, TileMaps* out) {
-  return make_tile_maps_typed(ctx, d, v.alloc, 4, out);
+  const int st = make_tile_maps_typed(ctx, d, v.alloc, 4, out);
+  out->origin = v.origin;
+  return st;
 }
 
 int make_tile_maps_typed(vti_ctx* ctx, const Dims3& d, void* alloc, int elem_bytes,
@@ -804,8 +822,12 @@ int set_smem_attr(vti_ctx* ctx, K kern, int bytes, std::atomic<bool>* done) {
 }
 
 FwdCommon fwd_common(const Dims3& d, const Sched& sc, const Damping* damp, float sx, float sy,
-                     float sz, PointSource src) {
+                     float sz, PointSource src, const TileMaps& c11, const TileMaps& c13,
+                     const TileMaps& c33) {
   FwdCommon c{};
+  c.c11 = c11.origin;
+  c.c13 = c13.origin;
+  c.c33 = c33.origin;
   c.d = d;
   c.sc = sc;
   c.dampx = damp ? damp->x : nullptr;
@@ -835,9 +857,8 @@ int launch_fwd3d_tma(vti_ctx* ctx, const Dims3& d, const TileMaps& cx, const Til
   VTI_TRY_ST(set_smem_attr(ctx, kern, F_SMEM, attr_fwd[variant]));
   FwdMaps m;
   m.cx = *H(cx); m.cz = *P(cz); m.px = *P(px); m.pz = *P(pz);
-  m.c11 = *P(c11); m.c13 = *P(c13); m.c33 = *P(c33);
   FwdArgs a{};
-  a.c = fwd_common(d, make_sched(ctx, d, 3), damp, sx, sy, sz, src);
+  a.c = fwd_common(d, make_sched(ctx, d, 3), damp, sx, sy, sz, src, c11, c13, c33);
   a.p = FwdPar{cz_ptr, px_ptr, pz_ptr};
   a.probe = probe;
   a.status = ctx->d_status;
@@ -864,13 +885,12 @@ int launch_bwd3d_tma(vti_ctx* ctx, const Dims3& d, const TileMaps& scx, const Ti
   BwdMaps m;
   m.scx = *H(scx); m.scz = *P(scz); m.spx = *P(spx); m.spz = *P(spz);
   m.lcx = *H(lcx); m.lcz = *P(lcz); m.lpx = *P(lpx); m.lpz = *P(lpz);
-  m.c11 = *P(c11); m.c13 = *P(c13); m.c33 = *P(c33);
-  m.g11 = *P(g11); m.g13 = *P(g13); m.g33 = *P(g33);
   BwdArgs a{};
   BwdCommon& c = a.c;
   c.d = d;
   c.sc = make_sched(ctx, d, 2);
   c.g11 = g11_ptr; c.g13 = g13_ptr; c.g33 = g33_ptr;
+  c.c11 = c11.origin; c.c13 = c13.origin; c.c33 = c33.origin;
   c.dampx = damp.x; c.dampy = damp.y; c.dampz = damp.z;
   c.dt2 = dt2; c.idx2 = idx2; c.idy2 = idy2; c.idz2 = idz2;
   c.sx = sx; c.sy = sy; c.sz = sz;
@@ -929,7 +949,8 @@ int fwd_batch_build(vti_ctx* ctx, const FwdJobSpec* spec, int njobs, StepBatch**
       const Sched sc = sp.seg > 0 ? sched_with_seg(sp.d, sp.seg) : make_sched(ctx, sp.d, 3);
       PointSource src;
       src.x = sp.src_x; src.y = sp.src_y; src.z = sp.src_z;
-      B.c[j] = fwd_common(sp.d, sc, sp.damp, sp.sx, sp.sy, sp.sz, src);
+      B.c[j] = fwd_common(sp.d, sc, sp.damp, sp.sx, sp.sy, sp.sz, src, *sp.c[0], *sp.c[1],
+                          *sp.c[2]);
       B.c[j].amp = sp.amp;
       B.c[j].t0 = sp.t0;
       for (int par = 0; par < 2; ++par) {
@@ -937,7 +958,6 @@ int fwd_batch_build(vti_ctx* ctx, const FwdJobSpec* spec, int njobs, StepBatch**
         FwdMaps& m = maps[2 * j + par];
         m.cx = *H(*sp.cx[par]); m.cz = *P(*sp.cz[par]); m.px = *P(*sp.px[par]);
         m.pz = *P(*sp.pz[par]);
-        m.c11 = *P(*sp.c[0]); m.c13 = *P(*sp.c[1]); m.c33 = *P(*sp.c[2]);
       }
       B.base[j] = items;
       items += sc.items;
@@ -981,6 +1001,7 @@ int bwd_batch_build(vti_ctx* ctx, const BwdJobSpec* spec, int njobs, StepBatch**
       c.d = sp.d;
       c.sc = sc;
       c.g11 = sp.g_ptr[0]; c.g13 = sp.g_ptr[1]; c.g33 = sp.g_ptr[2];
+      c.c11 = sp.c[0]->origin; c.c13 = sp.c[1]->origin; c.c33 = sp.c[2]->origin;
       c.dampx = sp.damp.x; c.dampy = sp.damp.y; c.dampz = sp.damp.z;
       c.dt2 = sp.dt2; c.idx2 = sp.idx2; c.idy2 = sp.idy2; c.idz2 = sp.idz2;
       c.sx = sp.sx; c.sy = sp.sy; c.sz = sp.sz;
@@ -995,8 +1016,6 @@ int bwd_batch_build(vti_ctx* ctx, const BwdJobSpec* spec, int njobs, StepBatch**
         m.spz = *P(*sp.spz[par]);
         m.lcx = *H(*sp.lcx[par]); m.lcz = *P(*sp.lcz[par]); m.lpx = *P(*sp.lpx[par]);
         m.lpz = *P(*sp.lpz[par]);
-        m.c11 = *P(*sp.c[0]); m.c13 = *P(*sp.c[1]); m.c33 = *P(*sp.c[2]);
-        m.g11 = *P(*sp.g[0]); m.g13 = *P(*sp.g[1]); m.g33 = *P(*sp.g[2]);
       }
       B.base[j] = items;
       items += sc.items;
