@@ -957,6 +957,23 @@ def run_forward2d(args):
     ctx.set_2d_resident(True)
     multi["gpts_per_s"] = round(len(sl) * (s.nt - 2) * nnx * nnz / (multi["resident_ms"] / 1e3)
                                 / 1e9, 2)
+    # the 2D adjoint gradient of the same shot (objFuncGradient_f: forward with
+    # checkpoints, exact adjoint with imaging), observed data from the shot
+    # itself scaled by 0.9 so the residual is not zero
+    dobs = (0.9 * tr).astype(np.float32)
+    V.objFuncGradient_f(ctx, g, dobs, c11, c13, c33, s.wavelet, s.sloc, s.rloc, s.taper)
+    ctx.synchronize()
+    l0 = ctx.launches
+    t0 = time.perf_counter()
+    for _ in range(3):
+        V.objFuncGradient_f(ctx, g, dobs, c11, c13, c33, s.wavelet, s.sloc, s.rloc, s.taper)
+    ctx.synchronize()
+    gms = (time.perf_counter() - t0) / 3 * 1e3
+    grad2d = {"ms_per_shot": round(gms, 2), "levels": 2 * (s.nt - 2),
+              "us_per_level": round(gms * 1e3 / (2 * (s.nt - 2)), 2),
+              "launches_per_shot": (ctx.launches - l0) // 3,
+              "api": "vti2d_gradient (host buffers), per-level kernels launched as "
+                     "programmatic dependents"}
     ctx.close()
     pts = (s.nt - 2) * nnx * nnz
     # CPU: the FP32 oracle of the same shot, all host threads
@@ -999,7 +1016,7 @@ def run_forward2d(args):
                 "h2d_bytes_per_step": int(4 * (4 * nnx * nnz + s.nt)),
                 "d2h_bytes_per_step": int(tr.nbytes), "api": "vti2d_synthetic (host buffers)"},
         "gpu_launches": int(launches), "clocks": clk.summary(),
-        "multishot": multi,
+        "multishot": multi, "gradient2d": grad2d,
     }
     print(json.dumps(res), flush=True)
     return res

@@ -417,25 +417,6 @@ __global__ void __launch_bounds__(kResThreads, 1)
   cl.sync();
 }
 
-// Launch with programmatic stream serialization: the kernel may start while
-// the previous kernel of the stream runs; its griddepcontrol.wait orders its
-// dependent reads and writes after that kernel.
-template <typename... KArgs, typename... Args>
-cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, cudaStream_t s,
-                       Args&&... args) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = grid;
-  cfg.blockDim = block;
-  cfg.dynamicSmemBytes = 0;
-  cfg.stream = s;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  at[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = at;
-  cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
-}
-
 struct Dev2d {
   float* buf = nullptr;  // c11 c13 c33 taper p0 q0 p1 q1 amps
   size_t n = 0;

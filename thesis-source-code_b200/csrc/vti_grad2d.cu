@@ -56,6 +56,10 @@ struct Fwd2 {
 };
 
 __global__ void __launch_bounds__(BX* BZ) k_fwd2d(Fwd2 a) {
+  // launched as programmatic dependents (launch_pdl): wait for the previous
+  // kernel of the stream before touching anything
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   __shared__ float sp[BZ][BX + 8], sq[BZ + 8][BX];
   __shared__ float sdp[BZ][BX + 8], sdq[BZ + 8][BX];
   const int tx = threadIdx.x, tz = threadIdx.y;
@@ -117,6 +121,10 @@ __global__ void __launch_bounds__(BX* BZ) k_fwd2d(Fwd2 a) {
 // D kernel (kernels.cu:345-387): checkpoint of (Dxx p / dx2, Dzz q / dz2).
 __global__ void __launch_bounds__(BX* BZ) k_dop2d(Grid2 g, const float* p, const float* q,
                                                   float* tp, float* tq, float idx2, float idz2) {
+  // launched as programmatic dependents (launch_pdl): wait for the previous
+  // kernel of the stream before touching anything
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   __shared__ float sp[BZ][BX + 8], sq[BZ + 8][BX];
   const int tx = threadIdx.x, tz = threadIdx.y;
   const int ix = kHalo + blockIdx.x * BX + tx, iz = kHalo + blockIdx.y * BZ + tz;
@@ -156,6 +164,10 @@ struct Adj2 {
 };
 
 __global__ void __launch_bounds__(BX* BZ) k_adj2d(Adj2 a) {
+  // launched as programmatic dependents (launch_pdl): wait for the previous
+  // kernel of the stream before touching anything
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   __shared__ float su[BZ][BX + 8], sw[BZ + 8][BX];
   const int tx = threadIdx.x, tz = threadIdx.y;
   const int ix = kHalo + blockIdx.x * BX + tx, iz = kHalo + blockIdx.y * BZ + tz;
@@ -213,6 +225,10 @@ __global__ void __launch_bounds__(BX* BZ) k_adj2d(Adj2 a) {
 // injectData (kernels.cu:208-217) into a tapered level: taper factor applied.
 __global__ void k_inject2d(float* p, float* q, const float* b0, const float* b1, float f,
                            const int* ridx, const float* taper, int nr, float dt2, int scale) {
+  // launched as programmatic dependents (launch_pdl): wait for the previous
+  // kernel of the stream before touching anything
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   int ir = blockIdx.x * blockDim.x + threadIdx.x;
   if (ir < nr) {
     const int i = ridx[ir];
@@ -226,6 +242,10 @@ __global__ void k_inject2d(float* p, float* q, const float* b0, const float* b1,
 
 __global__ void k_record_rows(float* rec, int row, const float* p, const float* q,
                               const int* ridx, int nr) {
+  // launched as programmatic dependents (launch_pdl): wait for the previous
+  // kernel of the stream before touching anything
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   int ir = blockIdx.x * blockDim.x + threadIdx.x;
   if (ir < nr) {
     int i = ridx[ir];
@@ -234,6 +254,10 @@ __global__ void k_record_rows(float* rec, int row, const float* p, const float* 
 }
 
 __global__ void k_set2(float* a, float* b, int i, float v) {
+  // launched as programmatic dependents (launch_pdl): wait for the previous
+  // kernel of the stream before touching anything
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   a[i] = v;
   b[i] = v;
 }
@@ -408,15 +432,16 @@ int run_grad2d(vti_ctx* ctx, const vti2d_geom* g, float* gc11, float* gc13, floa
     if (born) VTI_CUDA(ctx, cudaMemsetAsync(dp0, 0, 4 * nnxz * 4, s));
     float *P0 = p0, *Q0 = q0, *P1 = p1, *Q1 = q1;
     float *DP0 = dp0, *DQ0 = dq0, *DP1 = dp1, *DQ1 = dq1;
-    k_set2<<<1, 1, 0, s>>>(P1, Q1, sxz, dt2 * wavelet[0]);  // no taper at level 1
+    VTI_CUDA(ctx, launch_pdl(k_set2, dim3(1), dim3(1), s, P1, Q1, sxz,
+                             dt2 * wavelet[0]));  // no taper at level 1
     ctx->launches++;
-    auto checkpoint = [&](int t, const float* p, const float* q) {
+    auto checkpoint = [&](int t, const float* p, const float* q) -> cudaError_t {
       const long label = (long)is * (g->nt + 1) + t;
-      if (!slot.count(label)) return;
-      k_dop2d<<<grid, block, 0, s>>>(G, p, q, ckp(label), ckq(label), idx2, idz2);
+      if (!slot.count(label)) return cudaSuccess;
       ctx->launches++;
+      return launch_pdl(k_dop2d, grid, block, s, G, p, q, ckp(label), ckq(label), idx2, idz2);
     };
-    checkpoint(1, P1, Q1);
+    VTI_CUDA(ctx, checkpoint(1, P1, Q1));
     for (int it = 2; it < g->nt; ++it) {
       const float t = it * dt + g->ot;
       Fwd2 a{G,   P1,  Q1,  P0,  Q0,   DP1,  DQ1, DP0, DQ0, d11, d13, d33, e11,
@@ -426,13 +451,13 @@ int run_grad2d(vti_ctx* ctx, const vti2d_geom* g, float* gc11, float* gc13, floa
         a.bdp = stale_p;
         a.bdq = stale_q;
       }
-      k_fwd2d<<<grid, block, 0, s>>>(a);
+      VTI_CUDA(ctx, launch_pdl(k_fwd2d, grid, block, s, a));
       ctx->launches++;
-      checkpoint(it, P0, Q0);
+      VTI_CUDA(ctx, checkpoint(it, P0, Q0));
       if (t >= 0.f && (it - ntNeg) % ratio == 0 && nri > 0) {
-        k_record_rows<<<(nri + 127) / 128, 128, 0, s>>>(recb.p, (it - ntNeg) / ratio,
-                                                        born ? DP0 : P0, born ? DQ0 : Q0,
-                                                        d_ridx, nri);
+        VTI_CUDA(ctx, launch_pdl(k_record_rows, dim3((nri + 127) / 128), dim3(128), s, recb.p,
+                                 (it - ntNeg) / ratio, (const float*)(born ? DP0 : P0),
+                                 (const float*)(born ? DQ0 : Q0), d_ridx, nri));
         ctx->launches++;
       }
       std::swap(P0, P1);
@@ -441,7 +466,8 @@ int run_grad2d(vti_ctx* ctx, const vti2d_geom* g, float* gc11, float* gc13, floa
       std::swap(DQ0, DQ1);
     }
     if (born) {  // D of the last Born level, read by the next shot's first step
-      k_dop2d<<<grid, block, 0, s>>>(G, DP1, DQ1, stale_p, stale_q, idx2, idz2);
+      VTI_CUDA(ctx, launch_pdl(k_dop2d, grid, block, s, G, (const float*)DP1,
+                               (const float*)DQ1, stale_p, stale_q, idx2, idz2));
       ctx->launches++;
     }
     if (!born && nri > 0) {
@@ -460,13 +486,14 @@ int run_grad2d(vti_ctx* ctx, const vti2d_geom* g, float* gc11, float* gc13, floa
     // ---- backward
     VTI_CUDA(ctx, cudaMemsetAsync(p0, 0, 4 * nnxz * 4, s));
     P0 = p0; Q0 = q0; P1 = p1; Q1 = q1;
-    float* b0 = b01.p;
-    float* b1 = b01.p + std::max(nri, 1);
-    VTI_CUDA(ctx, cudaMemsetAsync(b01.p, 0, 2 * std::max(nri, 1) * sizeof(float), s));
+    // the two trace rows interpolated between (injectData): pointers into the
+    // recorded rows, starting with the last row and a row of zeros
+    VTI_CUDA(ctx, cudaMemsetAsync(b01.p, 0, std::max(nri, 1) * sizeof(float), s));
+    const float* b0 = recb.p + (size_t)(nnt_data - 1) * std::max(nri, 1);
+    const float* b1 = b01.p;
     if (nri > 0) {
-      VTI_CUDA(ctx, cudaMemcpyAsync(b0, recb.p + (size_t)(nnt_data - 1) * nri,
-                                    nri * sizeof(float), cudaMemcpyDeviceToDevice, s));
-      k_inject2d<<<(nri + 127) / 128, 128, 0, s>>>(P0, Q0, b0, b1, 0.f, d_ridx, tap, nri, dt2, 0);
+      VTI_CUDA(ctx, launch_pdl(k_inject2d, dim3((nri + 127) / 128), dim3(128), s, P0, Q0, b0,
+                               b1, 0.f, d_ridx, (const float*)tap, nri, dt2, 0));
       ctx->launches++;
     }
     int step = 0;  // sched[step] images the current adjoint
@@ -474,18 +501,17 @@ int run_grad2d(vti_ctx* ctx, const vti2d_geom* g, float* gc11, float* gc13, floa
       const Pair& pr = sched[is][step];
       Adj2 a{G,      P0,  Q0,  P1,  Q1,  d11, d13, d33, tap,  idx2, idz2, dt2, born ? 0 : 1,
              ckp(pr.a), ckq(pr.a), ckp(pr.b), ckq(pr.b), pr.f, 1, g11, g13, g33};
-      k_adj2d<<<grid, block, 0, s>>>(a);
+      VTI_CUDA(ctx, launch_pdl(k_adj2d, grid, block, s, a));
       ctx->launches++;
       if (it >= ntNeg && nri > 0) {
         float f = (it - ntNeg + 1.) / ratio;
         int i1 = (int)f;
-        if ((it - ntNeg + 2) % ratio == 0) {
-          VTI_CUDA(ctx, cudaMemcpyAsync(b1, recb.p + (size_t)i1 * nri, nri * sizeof(float),
-                                        cudaMemcpyDeviceToDevice, s));
+        if ((it - ntNeg + 2) % ratio == 0) {  // row i1 enters, the older row leaves
+          b1 = recb.p + (size_t)i1 * nri;
           std::swap(b0, b1);
         }
-        k_inject2d<<<(nri + 127) / 128, 128, 0, s>>>(P1, Q1, b0, b1, f - i1, d_ridx, tap, nri,
-                                                      dt2, 1);
+        VTI_CUDA(ctx, launch_pdl(k_inject2d, dim3((nri + 127) / 128), dim3(128), s, P1, Q1, b0,
+                                 b1, f - i1, d_ridx, (const float*)tap, nri, dt2, 1));
         ctx->launches++;
       }
       std::swap(P0, P1);
@@ -495,7 +521,7 @@ int run_grad2d(vti_ctx* ctx, const vti2d_geom* g, float* gc11, float* gc13, floa
       const Pair& pr = sched[is][step];
       Adj2 a{G,      P0,  Q0,  nullptr, nullptr, d11, d13, d33, tap,  idx2, idz2, dt2, 1,
              ckp(pr.a), ckq(pr.a), ckp(pr.b), ckq(pr.b), pr.f, 1, g11, g13, g33};
-      k_adj2d<<<grid, block, 0, s>>>(a);
+      VTI_CUDA(ctx, launch_pdl(k_adj2d, grid, block, s, a));
       ctx->launches++;
     }
     VTI_CUDA(ctx, cudaGetLastError());
