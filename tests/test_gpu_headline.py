@@ -70,3 +70,35 @@ def test_headline_grid_traces_misfit_and_gradient_match_the_oracle(ctx, headline
             a, b = fg[1 + k * n:1 + (k + 1) * n], o[1 + k * n:1 + (k + 1) * n]
             assert np.abs(b).max() > 0
             assert rel_l2(a, b) < GRAD_TOL, (dtype, k, rel_l2(a, b))
+
+
+def test_headline_gradient_is_bitwise_reproducible(ctx, headline):
+    """Every launch of the step kernels computes each cell once, from its own
+    stage of a TMA ring; the same inputs therefore give the same bits, call
+    after call. The time-reversed reconstruction amplifies any read of a
+    wrong stage row by orders of magnitude within a few dozen levels, so a
+    race between the consumers' shared-memory reads and the ring's refill
+    shows here (it did, once per ~1000 backward launches, before the stage
+    release carried a proxy fence)."""
+    s, cstart, ctrue, padb, randb = headline
+    g = s.geom()
+    n = s.nxyz
+    flags = V.OPT_FULL_STEPS
+    p = V.Plan3d(ctx, g, flags)
+    try:
+        p.set_wavelet(s.wavelet)
+        p.set_receivers(s.recloc)
+        nr = s.recloc.size // 4
+        p.set_model(*_split(ctrue, n), padb=padb, randb=randb)
+        dobs = p.model_data(s.souloc, [0], nrec_total=nr)
+        p.set_model(*_split(cstart, n), padb=padb, randb=randb)
+        runs = [p.gradient(s.souloc, [0], dobs) for _ in range(4)]
+        images = [p.rtm(s.souloc, [0], dobs) for _ in range(3)]
+    finally:
+        p.close()
+    for fg, mis in runs[1:]:
+        assert mis == runs[0][1]
+        np.testing.assert_array_equal(fg, runs[0][0])
+    for im in images[1:]:
+        np.testing.assert_array_equal(im, images[0])
+

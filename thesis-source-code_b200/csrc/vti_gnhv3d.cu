@@ -202,8 +202,7 @@ __global__ void __launch_bounds__(NTHREADS, 2)
       const float2 bpx = ld2(pl + 4 * T), bpz = ld2(pl + 5 * T);
       const float2 c11 = ld2(pl + 6 * T), c13 = ld2(pl + 7 * T), c33 = ld2(pl + 8 * T);
       const float2 d11 = ld2(pl + 9 * T), d13 = ld2(pl + 10 * T), d33 = ld2(pl + 11 * T);
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&empty[s]);
+      stage_release(&empty[s], lane);
       float anx[2], anz[2], bnx[2], bnz[2];
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
@@ -321,8 +320,7 @@ __global__ void __launch_bounds__(NTHREADS, 2)
       const float2 m2x = ld2(pl + 4 * T), m2z = ld2(pl + 5 * T);
       const float2 c11 = ld2(pl + 6 * T), c13 = ld2(pl + 7 * T), c33 = ld2(pl + 8 * T);
       const float2 g11o = ld2(pl + 9 * T), g13o = ld2(pl + 10 * T), g33o = ld2(pl + 11 * T);
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&empty[s]);
+      stage_release(&empty[s], lane);
       float mx[2], mz[2], wx[2], wzv[2], g11[2], g13[2], g33[2];
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
@@ -557,8 +555,7 @@ __global__ void __launch_bounds__(NTHREADS, 2)
       const float2 m2x = ld2(pr + 2 * T), m2z = ld2(pr + 3 * T);
       const float2 c11 = ld2(pr + 4 * T), c13 = ld2(pr + 5 * T), c33 = ld2(pr + 6 * T);
       const float2 g11o = ld2(pr + 7 * T), g13o = ld2(pr + 8 * T), g33o = ld2(pr + 9 * T);
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&empty[s]);
+      stage_release(&empty[s], lane);
       float mx[2], mz[2], wx[2], wzv[2], g11[2], g13[2], g33[2];
 #pragma unroll
       for (int e = 0; e < 2; ++e) {

@@ -218,8 +218,7 @@ __device__ __forceinline__ bool fwd_consume(const FwdCommon& a, const FwdPar& bp
       yp[j] = ld2(sh + (j + 1) * HX);
     }
     const float2 px = ld2(pl + T), pz = ld2(pl + 2 * T);
-    __syncwarp();
-    if (lane == 0) mbar_arrive(&empty[s]);
+    stage_release(&empty[s], lane);
     float nxv[2], nzv[2];
 #pragma unroll
     for (int e = 0; e < 2; ++e) {
@@ -552,8 +551,7 @@ __device__ __forceinline__ bool bwd_consume(const BwdCommon& a, const BwdPar& bp
     }
     const float2 spx = ld2(pl + 2 * T), spz = ld2(pl + 3 * T);
     const float2 lpx = ld2(pl + 4 * T), lpz = ld2(pl + 5 * T);
-    __syncwarp();
-    if (lane == 0) mbar_arrive(&empty[s]);
+    stage_release(&empty[s], lane);
     float snx[2], snz[2], lnx[2], lnz[2], g11[2], g13[2], g33[2];
 #pragma unroll
     for (int e = 0; e < 2; ++e) {
@@ -733,8 +731,9 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 // CTA, waves * (seg + restart), where a wave is one item per resident slot
 // and a restart (8 queue planes read with plain loads, pipeline refill) costs
 // about kRestart plane-steps.
+constexpr long long kRestart = 4;
+
 Sched make_sched(vti_ctx* ctx, const Dims3& d, int ctas_per_sm) {
-  constexpr long long kRestart = 4;
   Sched s;
   s.gx = (d.nx - kHalo + TX - 1) / TX;  // x origins 0, 32, ...; updated x < nx-4
   s.gy = (d.ny - 2 * kHalo + TY - 1) / TY;
@@ -760,6 +759,13 @@ Sched make_sched(vti_ctx* ctx, const Dims3& d, int ctas_per_sm) {
   return s;
 }
 
+long long step_sched_cost(vti_ctx* ctx, const Dims3& d, int ctas_per_sm, long long* work) {
+  const Sched s = make_sched(ctx, d, ctas_per_sm);
+  const long long slots = (long long)ctx->sm_count * ctas_per_sm;
+  const long long waves = (s.items + slots - 1) / slots;
+  if (work) *work = (long long)s.gx * s.gy * s.nz;
+  return waves * (s.seg + kRestart) * slots;
+}
 
 int make_tile_maps(vti_ctx* ctx, const Dims3& d, const Vol& v, TileMaps* out) {
   const int st = make_tile_maps_typed(ctx, d, v.alloc, 4, out);

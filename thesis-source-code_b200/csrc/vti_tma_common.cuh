@@ -64,6 +64,18 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t by
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
+// Release of a consumed stage by one consumer warp. The stage was read with
+// ordinary shared-memory loads (generic proxy) and is refilled by TMA (async
+// proxy) once the producer sees the release: each lane's proxy fence orders
+// its reads before those writes, so no lane can read a row of the next
+// plane's tile. Without the fence an unlucky half-warp read was observed to
+// see the refill (about once per thousand backward launches of a 400^2 x 200
+// grid).
+__device__ __forceinline__ void stage_release(uint64_t* bar, int lane) {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  __syncwarp();
+  if (lane == 0) mbar_arrive(bar);
+}
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
