@@ -425,9 +425,12 @@ def run_batched(args):
     """Batched multi-shot gradient (the batching workload): `--shots` shots on
     the 400x400x200 model, each on its own window with apertures per side drawn
     from U{160..400} (seed 5), receivers every 25 m inside each window, all
-    shots advanced together by vti3d_batch_gradient (CUDA-graph time loops,
-    autotuned segment lengths). Compared with the plain per-shot loop on the
-    same GPU: vti3d_plan_gradient of one shot at a time on the full model.
+    shots in one vti3d_batch_gradient call under the schedule
+    vti3d_batch_autotune times faster (side by side: one launch per level
+    over all windows, CUDA-graph time loops, autotuned segment lengths; per
+    shot: each window through the single-grid passes in turn); the other
+    schedule is timed once beside it. Compared with the plain per-shot loop on
+    the same GPU: vti3d_plan_gradient of one shot at a time on the full model.
     Observed traces are zero (the residual is the modeled data); the work per
     step does not depend on the data values."""
     import torch
@@ -455,7 +458,9 @@ def run_batched(args):
     b.set_wavelet(s.wavelet)
     b.set_receivers(recloc)
     b.set_shots(souloc, wins, seed=4)
-    seg_f, seg_b = b.autotune()
+    seg_f, seg_b = b.autotune()  # segment lengths, then the faster schedule
+    schedule = b.schedule
+    sched_name = {V.BATCH_SIDE_BY_SIDE: "side_by_side", V.BATCH_PER_SHOT: "per_shot"}
     dobs = torch.zeros(nnt * nrec, dtype=torch.float32, device="cuda")
     fg = torch.zeros(1 + 3 * n, dtype=torch.float32, device="cuda")
 
@@ -483,6 +488,19 @@ def run_batched(args):
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
     launches = (ctx.launches - launches0) // args.steps
+    # the schedule autotune did not choose, one gradient, for the record
+    other = V.BATCH_PER_SHOT if schedule == V.BATCH_SIDE_BY_SIDE else V.BATCH_SIDE_BY_SIDE
+    other_ms = None
+    if args.steps > 0 and not args.no_check:
+        b.set_schedule(other)
+        grad()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        grad()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        other_ms = e0.elapsed_time(e1)
+        b.set_schedule(V.BATCH_AUTO)
     # end to end: pinned host traces in, host gradient out
     h_dobs = torch.zeros(nnt * nrec, dtype=torch.float32).pin_memory()
     h_fg = torch.zeros(1 + 3 * n, dtype=torch.float32).pin_memory()
@@ -546,8 +564,12 @@ def run_batched(args):
     peak, peak_kind = peaks()
     bwd_avg = bwd_ms / max(bwd_n, 1) / 1e3
     fwd_avg = fwd_ms / max(fwd_n, 1) / 1e3
-    fwd_upd = 2 * upd  # pass 1 and pass 2 of every shot per forward launch
-    achieved = BWD_BYTES_PER_POINT * upd / bwd_avg / 1e9 if bwd_n else None
+    # bytes over the summed device time of all step launches of one gradient:
+    # side by side, every launch covers all windows; per shot, one window
+    achieved = (BWD_BYTES_PER_POINT * upd * (M - 1) / (bwd_ms / 1e3) / 1e9
+                if bwd_n else None)
+    fwd_achieved = (FWD_BYTES_PER_POINT * 2 * upd * (M - 1) / (fwd_ms / 1e3) / 1e9
+                    if fwd_n else None)
     shots_s = args.shots / (ms / 1e3)
     plain_s = 1.0 / (plain_ms / 1e3)
     out = {
@@ -558,8 +580,13 @@ def run_batched(args):
         "data": "synthetic (seeded layered VTI model + GRF; zero observed traces)",
         "config": {"workload": f"{args.shots} shots, 400x400x200 model, windows U{{160..400}} "
                                f"per side (seed 5), nt={s.nt}, {M} levels, {nrec} receivers",
-                   "windows": wins, "segments": [seg_f, seg_b], "graph": True,
-                   "misfit": mis},
+                   "windows": wins, "segments": [seg_f, seg_b],
+                   "graph": schedule == V.BATCH_SIDE_BY_SIDE,
+                   "schedule": sched_name[schedule], "misfit": mis},
+        "schedules": {sched_name[schedule]: round(ms, 1),
+                      sched_name[other]: round(other_ms, 1) if other_ms else None,
+                      "unit": "ms per gradient of all shots",
+                      "chosen_by": "vti3d_batch_autotune (one level of each, timed)"},
         "gpts": round(pts / (ms / 1e3) / 1e9, 2),
         "plain": {"value": round(plain_s, 4), "unit": "shots/s",
                   "ms_per_shot": round(plain_ms, 1), "shots_timed": nplain,
@@ -572,14 +599,16 @@ def run_batched(args):
                                   "window models), one at a time; total scaled from the timed "
                                   "windows by window area"},
         "speedup_vs_windowed_plain": round(shots_s / (args.shots / (windowed_ms / 1e3)), 3),
-        "roofline": {"bound": "hbm", "kernel": "k_bwd3d_tma (batched)",
+        "roofline": {"bound": "hbm",
+                     "kernel": ("k_bwd3d_batch" if schedule == V.BATCH_SIDE_BY_SIDE
+                                else "k_bwd3d_tma (one window per launch)"),
                      "achieved": round(achieved, 1) if achieved else None, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": round(achieved / peak, 4) if achieved else None,
                      "traffic": None, "bytes_per_point": BWD_BYTES_PER_POINT,
-                     "avg_launch_ms": round(bwd_avg * 1e3, 4),
-                     "fwd3d": {"achieved": round(FWD_BYTES_PER_POINT * fwd_upd / fwd_avg / 1e9, 1)
-                               if fwd_n else None, "avg_launch_ms": round(fwd_avg * 1e3, 4)}},
+                     "avg_launch_ms": round(bwd_avg * 1e3, 4), "launches": bwd_n,
+                     "fwd3d": {"achieved": round(fwd_achieved, 1) if fwd_achieved else None,
+                               "avg_launch_ms": round(fwd_avg * 1e3, 4), "launches": fwd_n}},
         "e2e": {"value": round(args.shots / (e2e_ms / 1e3), 4), "unit": "shots/s",
                 "h2d_bytes_per_step": int(4 * nnt * nrec), "d2h_bytes_per_step": int(4 * (1 + 3 * n)),
                 "ms_per_step": round(e2e_ms, 1), "api": "vti3d_batch_gradient (host buffers)"},

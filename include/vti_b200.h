@@ -349,7 +349,25 @@ int vti3d_batch_set_shots(vti3d_batch* b, int nshot, const float* souloc,
 /* use_graph != 0: the time loops are captured once as CUDA graphs and
  * replayed. seg_fwd/seg_bwd: z planes per work item (0: default schedule). */
 int vti3d_batch_set_options(vti3d_batch* b, int use_graph, int seg_fwd, int seg_bwd);
-/* Times candidate segment lengths on the current shots and keeps the fastest. */
+/* Schedules of vti3d_batch_gradient. Side by side: every level is one
+ * forward launch over passes 1 and 2 of all shots and one backward launch
+ * over pass 3 of all shots. Per shot: the shots run one after another, each
+ * with the single-grid launches of vti3d_plan_gradient (windows that fill the
+ * GPU alone lose nothing to this and keep the single-grid kernels' higher
+ * bandwidth). Auto: per shot when every window alone fills every SM with at
+ * least kBatchPerShotWaves waves of full-depth columns (vti3d_batch_autotune
+ * replaces this rule by timing both). The gradient is the same under every
+ * schedule. */
+#define VTI_BATCH_AUTO 0
+#define VTI_BATCH_SIDE_BY_SIDE 1
+#define VTI_BATCH_PER_SHOT 2
+int vti3d_batch_set_schedule(vti3d_batch* b, int schedule);
+/* The schedule the next gradient runs (VTI_BATCH_SIDE_BY_SIDE or
+ * VTI_BATCH_PER_SHOT): the one set, or what auto resolves to. */
+int vti3d_batch_get_schedule(vti3d_batch* b, int* schedule);
+/* Times candidate segment lengths on the current shots and keeps the
+ * fastest; under VTI_BATCH_AUTO also times one level of each schedule and
+ * keeps the faster. */
 int vti3d_batch_autotune(vti3d_batch* b, int* seg_fwd, int* seg_bwd);
 /* Gradient of all shots: dobs as vti3d_plan_gradient (trace-major, global
  * receiver order); fgcij = [misfit/2, gc11, gc13, gc33] over the full model,

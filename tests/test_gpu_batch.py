@@ -158,6 +158,43 @@ def test_batch_graph_and_segments_give_the_same_gradient(ctx, survey):
         assert m_ == m0
 
 
+def test_batch_per_shot_schedule_gives_the_same_gradient(ctx, survey):
+    """The per-shot schedule (each window through the single-grid passes, one
+    shot after another) computes every shot with the same arithmetic as the
+    side-by-side launches; the misfit sums the same per-shot residuals in the
+    same order."""
+    k = survey
+    dobs = _observed(ctx, k)
+    b = _batch(ctx, k)
+    try:
+        # three windows of at most 64 x 60 cells cannot fill the GPU alone
+        assert b.schedule == V.BATCH_SIDE_BY_SIDE
+        b.set_schedule(V.BATCH_SIDE_BY_SIDE)
+        base, m0 = b.gradient(dobs)
+        b.set_schedule(V.BATCH_PER_SHOT)
+        assert b.schedule == V.BATCH_PER_SHOT
+        g1, m1 = b.gradient(dobs)
+        g2, m2 = b.gradient(dobs)  # again, from the state the first left
+        b.set_schedule(V.BATCH_AUTO)
+        b.autotune()
+        assert b.schedule in (V.BATCH_SIDE_BY_SIDE, V.BATCH_PER_SHOT)
+        g3, m3 = b.gradient(dobs)
+        with pytest.raises(V.VtiError):
+            b.set_schedule(7)
+    finally:
+        b.close()
+    np.testing.assert_array_equal(g1, g2)
+    assert m1 == m2
+    assert abs(m1 - m0) / m0 < 1e-12
+    assert abs(m3 - m0) / m0 < 1e-12
+    n = k["n"]
+    for c in range(3):
+        a, ref = g1[1 + c * n:1 + (c + 1) * n], base[1 + c * n:1 + (c + 1) * n]
+        assert np.abs(ref).max() > 0
+        assert rel_l2(a, ref) < 1e-6, (c, np.abs(a - ref).max())
+        assert rel_l2(g3[1 + c * n:1 + (c + 1) * n], ref) < 1e-6, c
+
+
 def test_batch_shot_matches_fp64_oracle(ctx, survey):
     """One shot of the batch against the FP64 oracle on its window."""
     k = survey

@@ -9,6 +9,13 @@
 // launch per step over the receivers of all shots. The time loops can be
 // captured once as CUDA graphs and replayed on every later call.
 //
+// Under the per-shot schedule the shots instead run one after another, each
+// with the plan's own single-grid passes (fwd_level / bwd_level), which is the
+// better order when every window alone fills the GPU: the single-grid step
+// kernels keep their parameters in the constant bank and their neighbouring
+// columns in step, and reach a higher fraction of HBM bandwidth than the
+// side-by-side launches.
+//
 // Per shot the arithmetic is exactly that of vti3d_plan_gradient on a plan
 // whose grid is the window (the same kernels' item bodies, the same source,
 // recording and injection schedule), so a shot's gradient is the plan's; the
@@ -200,6 +207,8 @@ struct vti3d_batch {
   cudaGraphExec_t graph_fwd = nullptr, graph_bwd = nullptr;
   double* d_acc = nullptr;
   float* d_full = nullptr;  // stacked gradient, 3 * nxyz
+  int schedule = VTI_BATCH_AUTO;
+  int tuned = 0;  // schedule measured by vti3d_batch_autotune (0: none yet)
 };
 
 namespace {
@@ -230,6 +239,7 @@ void free_shots(vti3d_batch* b) {
   b->d_entries = nullptr;
   b->tables_ok = false;
   b->cut_version = -1;
+  b->tuned = 0;
 }
 
 int levels(const vti3d_batch* b) { return last_level(b->g, b->flags); }
@@ -424,32 +434,81 @@ int cut_windows(vti3d_batch* b) {
   return VTI_OK;
 }
 
-int forward_loop(vti3d_batch* b) {
+// One side-by-side forward level (passes 1 and 2 of every shot) and its
+// recording.
+int fwd_tick(vti3d_batch* b, int tick) {
   vti_ctx* ctx = b->ctx;
-  const int M = levels(b);
-  const int rgrid = (b->nentries + 255) / 256;
-  for (int tick = 0; tick < M - 1; ++tick) {
-    VTI_TRY(step_batch_launch(ctx, b->fwd, tick));
-    if (b->nentries > 0) {
-      k_record_batch<<<rgrid, 256, 0, ctx->stream>>>(b->d_recjobs, b->d_entries, b->nentries,
-                                                     tick);
-      VTI_LAUNCHED(ctx, "k_record_batch");
-    }
+  VTI_TRY(step_batch_launch(ctx, b->fwd, tick));
+  if (b->nentries > 0) {
+    k_record_batch<<<(b->nentries + 255) / 256, 256, 0, ctx->stream>>>(
+        b->d_recjobs, b->d_entries, b->nentries, tick);
+    VTI_LAUNCHED(ctx, "k_record_batch");
   }
   return VTI_OK;
 }
 
-int backward_loop(vti3d_batch* b) {
+// One side-by-side backward level (pass 3 of every shot) and its injection.
+int bwd_tick(vti3d_batch* b, int tick) {
   vti_ctx* ctx = b->ctx;
+  VTI_TRY(step_batch_launch(ctx, b->bwd, tick));
+  if (b->nentries > 0) {
+    k_inject_batch<<<(b->nentries + 255) / 256, 256, 0, ctx->stream>>>(
+        b->d_recjobs, b->d_entries, b->nentries, tick);
+    VTI_LAUNCHED(ctx, "k_inject_batch");
+  }
+  return VTI_OK;
+}
+
+int forward_loop(vti3d_batch* b) {
   const int M = levels(b);
-  const int rgrid = (b->nentries + 255) / 256;
-  for (int tick = 0; tick < M - 1; ++tick) {
-    VTI_TRY(step_batch_launch(ctx, b->bwd, tick));
-    if (b->nentries > 0) {
-      k_inject_batch<<<rgrid, 256, 0, ctx->stream>>>(b->d_recjobs, b->d_entries, b->nentries,
-                                                     tick);
-      VTI_LAUNCHED(ctx, "k_inject_batch");
-    }
+  for (int tick = 0; tick < M - 1; ++tick) VTI_TRY(fwd_tick(b, tick));
+  return VTI_OK;
+}
+
+int backward_loop(vti3d_batch* b) {
+  const int M = levels(b);
+  for (int tick = 0; tick < M - 1; ++tick) VTI_TRY(bwd_tick(b, tick));
+  return VTI_OK;
+}
+
+// Ratio of the side-by-side step kernels' HBM bandwidth to the single-grid
+// kernels' (measured on windows of 160..400 x 160..400 x 200 cells: 0.64 and
+// 0.81 of the copy bandwidth for the backward step), and the gap between two
+// single-grid launches in CTA-slot plane-steps (about 3 us; one plane-step
+// of a 32 x 16 column is about 2 us).
+constexpr double kSideBySideRel = 0.79;
+constexpr long long kLaunchGap = 2;
+
+// The schedule of the next gradient: the one set; under auto the one
+// vti3d_batch_autotune measured faster, else per shot when the single-grid
+// schedules of the windows (backward step, two CTAs per SM, launch gaps
+// included) keep the SMs busy at least kSideBySideRel of the time.
+int resolve_schedule(vti3d_batch* b) {
+  if (b->schedule != VTI_BATCH_AUTO) return b->schedule;
+  if (b->tuned) return b->tuned;
+  vti_ctx* ctx = b->ctx;
+  long long work = 0, cost = 0;
+  for (vti3d_plan* p : b->plans) {
+    long long w = 0;
+    cost += step_sched_cost(ctx, p->d, 2, &w) + kLaunchGap * ctx->sm_count * 2;
+    work += w;
+  }
+  return cost > 0 && (double)work >= kSideBySideRel * (double)cost ? VTI_BATCH_PER_SHOT
+                                                                   : VTI_BATCH_SIDE_BY_SIDE;
+}
+
+// Shot k's window gradient added into the full-model gradient.
+int add_window(vti3d_batch* b, int k) {
+  vti_ctx* ctx = b->ctx;
+  const size_t n = (size_t)b->g.nx * b->g.ny * b->g.nz;
+  vti3d_plan* p = b->plans[k];
+  const vti3d_window& w = b->win[k];
+  const Vol* gv[3] = {&p->g11, &p->g13, &p->g33};
+  const int grid = grid_for(ctx, p->d.npoints());
+  for (int c = 0; c < 3; ++c) {
+    k_add_window<<<grid, 256, 0, ctx->stream>>>(gv[c]->origin, p->d, p->g.npad, w.x0, w.y0,
+                                                b->g.nx, b->g.ny, b->d_full + c * n);
+    VTI_LAUNCHED(ctx, "k_add_window");
   }
   return VTI_OK;
 }
@@ -645,6 +704,21 @@ int vti3d_batch_set_options(vti3d_batch* b, int use_graph, int seg_fwd, int seg_
   return VTI_OK;
 }
 
+int vti3d_batch_set_schedule(vti3d_batch* b, int schedule) {
+  if (!b) return VTI_ERR_ARG;
+  if (schedule != VTI_BATCH_AUTO && schedule != VTI_BATCH_SIDE_BY_SIDE &&
+      schedule != VTI_BATCH_PER_SHOT)
+    return fail(b->ctx, VTI_ERR_ARG, "unknown batch schedule");
+  b->schedule = schedule;
+  return VTI_OK;
+}
+
+int vti3d_batch_get_schedule(vti3d_batch* b, int* schedule) {
+  if (!b || !schedule) return VTI_ERR_ARG;
+  *schedule = resolve_schedule(b);
+  return VTI_OK;
+}
+
 int vti3d_batch_gradient(vti3d_batch* b, const float* dobs, int dobs_mem, float* fgcij,
                          int fgcij_mem, double* misfit) {
   if (!b) return VTI_ERR_ARG;
@@ -657,49 +731,56 @@ int vti3d_batch_gradient(vti3d_batch* b, const float* dobs, int dobs_mem, float*
   const int nnt = nnt_of(b->g);
   const float dt2 = b->g.dt * b->g.dt;
   VTI_TRY(cut_windows(b));
-  if (!b->tables_ok) VTI_TRY(build_tables(b));
   if (!b->d_acc) VTI_CUDA(ctx, cudaMalloc((void**)&b->d_acc, (1 + residual_blocks(ctx)) * sizeof(double)));
-  // passes 1 and 2 of every shot, side by side
-  for (int k = 0; k < S; ++k) {
-    vti3d_plan* p = b->plans[k];
-    const ShotGeom& sg = b->geo[k];
-    VTI_TRY(zero_shot_fields(p, true, true, true));
-    const long long o = p->d.off(sg.sx, sg.sy, sg.sz);
-    // "injecting source at time 0 to wavefields at time 1" (objFuncGradient3d_f.cu:605-608)
-    VTI_TRY(launch_set_point(ctx, p->lx[0].origin, p->lz[0].origin, o, dt2 * b->wavelet[0]));
-    VTI_TRY(launch_set_point(ctx, p->sx[0].origin, p->sz[0].origin, o, dt2 * b->wavelet[0]));
-    if (sg.nr > 0)
-      VTI_CUDA(ctx, cudaMemsetAsync(p->d_trace, 0, (size_t)nnt * sg.nr * sizeof(float),
-                                    ctx->stream));
-  }
-  VTI_TRY(run_loop(b, forward_loop, &b->graph_fwd));
-  // residuals and misfit (objFuncGradient3d_f.cu:735-771), shots in order
-  VTI_CUDA(ctx, cudaMemsetAsync(b->d_acc, 0, sizeof(double), ctx->stream));
-  for (int k = 0; k < S; ++k) {
-    vti3d_plan* p = b->plans[k];
-    const ShotGeom& sg = b->geo[k];
-    const float* obs = nullptr;
-    VTI_TRY(get_obs(p, sg, dobs, dobs_mem, &obs));
-    VTI_TRY(launch_residual(ctx, p->d_trace, obs, p->d_live, nnt, sg.nr, b->d_acc));
-    VTI_TRY(zero_shot_fields(p, false, true, false));
-    VTI_TRY(launch_seed_adjoint(ctx, p->lx[0].origin, p->lz[0].origin, p->d_trace, nnt,
-                                p->d_rec + p->rec_cap, p->d_rec_damp, sg.nr, dt2));
-  }
-  VTI_TRY(run_loop(b, backward_loop, &b->graph_bwd));
-  // stack the window gradients
   const size_t n = (size_t)b->g.nx * b->g.ny * b->g.nz;
   if (!b->d_full) VTI_CUDA(ctx, cudaMalloc((void**)&b->d_full, 3 * n * sizeof(float)));
   VTI_CUDA(ctx, cudaMemsetAsync(b->d_full, 0, 3 * n * sizeof(float), ctx->stream));
-  for (int k = 0; k < S; ++k) {
-    vti3d_plan* p = b->plans[k];
-    const vti3d_window& w = b->win[k];
-    const Vol* gv[3] = {&p->g11, &p->g13, &p->g33};
-    const int grid = grid_for(ctx, p->d.npoints());
-    for (int c = 0; c < 3; ++c) {
-      k_add_window<<<grid, 256, 0, ctx->stream>>>(gv[c]->origin, p->d, p->g.npad, w.x0, w.y0,
-                                                  b->g.nx, b->g.ny, b->d_full + c * n);
-      VTI_LAUNCHED(ctx, "k_add_window");
+  VTI_CUDA(ctx, cudaMemsetAsync(b->d_acc, 0, sizeof(double), ctx->stream));
+  if (resolve_schedule(b) == VTI_BATCH_PER_SHOT) {
+    // one shot after another, the plan's passes on its window
+    // (objFuncGradient3d_f.cu:600-1078 per shot)
+    for (int k = 0; k < S; ++k) {
+      vti3d_plan* p = b->plans[k];
+      const ShotGeom& sg = b->geo[k];
+      VTI_TRY(zero_shot_fields(p, false, false, true));
+      VTI_TRY(forward_pass(p, sg, true));
+      const float* obs = nullptr;
+      VTI_TRY(get_obs(p, sg, dobs, dobs_mem, &obs));
+      VTI_TRY(launch_residual(ctx, p->d_trace, obs, p->d_live, nnt, sg.nr, b->d_acc));
+      VTI_TRY(forward_pass(p, sg, false));
+      VTI_TRY(backward_pass(p, sg, false));
+      VTI_TRY(add_window(b, k));
     }
+  } else {
+    if (!b->tables_ok) VTI_TRY(build_tables(b));
+    // passes 1 and 2 of every shot, side by side
+    for (int k = 0; k < S; ++k) {
+      vti3d_plan* p = b->plans[k];
+      const ShotGeom& sg = b->geo[k];
+      VTI_TRY(zero_shot_fields(p, true, true, true));
+      const long long o = p->d.off(sg.sx, sg.sy, sg.sz);
+      // "injecting source at time 0 to wavefields at time 1" (objFuncGradient3d_f.cu:605-608)
+      VTI_TRY(launch_set_point(ctx, p->lx[0].origin, p->lz[0].origin, o, dt2 * b->wavelet[0]));
+      VTI_TRY(launch_set_point(ctx, p->sx[0].origin, p->sz[0].origin, o, dt2 * b->wavelet[0]));
+      if (sg.nr > 0)
+        VTI_CUDA(ctx, cudaMemsetAsync(p->d_trace, 0, (size_t)nnt * sg.nr * sizeof(float),
+                                      ctx->stream));
+    }
+    VTI_TRY(run_loop(b, forward_loop, &b->graph_fwd));
+    // residuals and misfit (objFuncGradient3d_f.cu:735-771), shots in order
+    for (int k = 0; k < S; ++k) {
+      vti3d_plan* p = b->plans[k];
+      const ShotGeom& sg = b->geo[k];
+      const float* obs = nullptr;
+      VTI_TRY(get_obs(p, sg, dobs, dobs_mem, &obs));
+      VTI_TRY(launch_residual(ctx, p->d_trace, obs, p->d_live, nnt, sg.nr, b->d_acc));
+      VTI_TRY(zero_shot_fields(p, false, true, false));
+      VTI_TRY(launch_seed_adjoint(ctx, p->lx[0].origin, p->lz[0].origin, p->d_trace, nnt,
+                                  p->d_rec + p->rec_cap, p->d_rec_damp, sg.nr, dt2));
+    }
+    VTI_TRY(run_loop(b, backward_loop, &b->graph_bwd));
+    // stack the window gradients
+    for (int k = 0; k < S; ++k) VTI_TRY(add_window(b, k));
   }
   double acc = 0;
   VTI_CUDA(ctx, cudaMemcpyAsync(&acc, b->d_acc, sizeof(double), cudaMemcpyDeviceToHost,
@@ -783,10 +864,40 @@ int vti3d_batch_autotune(vti3d_batch* b, int* seg_fwd, int* seg_bwd) {
     if (which == 0) b->seg_fwd = best[0];
     else b->seg_bwd = best[1];
   }
+  VTI_TRY(build_tables(b));
+  if (b->schedule == VTI_BATCH_AUTO) {
+    // one level of each schedule (both forward passes, the backward pass and
+    // the receiver work of every shot), timed over `reps` levels after one
+    // untimed level
+    auto side = [&](int t) -> int {
+      VTI_TRY(fwd_tick(b, t));
+      return bwd_tick(b, t);
+    };
+    auto per_shot = [&](int) -> int {
+      for (size_t k = 0; k < b->plans.size(); ++k) {
+        vti3d_plan* p = b->plans[k];
+        const ShotGeom& sg = b->geo[k];
+        VTI_TRY(fwd_level(p, sg, true, 0, 1, 2));
+        VTI_TRY(fwd_level(p, sg, false, 0, 1, 2));
+        VTI_TRY(bwd_level(p, sg, false, 0, 1, 0, 1, 0));
+      }
+      return VTI_OK;
+    };
+    float t[2] = {0.f, 0.f};
+    for (int which = 0; which < 2; ++which) {
+      auto one = [&](int tick) { return which == 0 ? side(tick) : per_shot(tick); };
+      VTI_TRY(one(0));
+      VTI_CUDA(ctx, cudaEventRecord(e0, ctx->stream));
+      for (int r = 0; r < reps; ++r) VTI_TRY(one(r));
+      VTI_CUDA(ctx, cudaEventRecord(e1, ctx->stream));
+      VTI_CUDA(ctx, cudaEventSynchronize(e1));
+      VTI_CUDA(ctx, cudaEventElapsedTime(&t[which], e0, e1));
+    }
+    b->tuned = t[1] < t[0] ? VTI_BATCH_PER_SHOT : VTI_BATCH_SIDE_BY_SIDE;
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   VTI_TRY(check_device_status(ctx));
-  VTI_TRY(build_tables(b));
   if (seg_fwd) *seg_fwd = b->seg_fwd;
   if (seg_bwd) *seg_bwd = b->seg_bwd;
   return VTI_OK;

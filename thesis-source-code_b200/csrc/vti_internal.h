@@ -177,6 +177,10 @@ struct TileMaps {
   const float* origin = nullptr;  // plane 0 of the volume (FP32 volumes; kernels that read it directly)
 };
 int make_tile_maps(vti_ctx* ctx, const Dims3& d, const Vol& v, TileMaps* out);
+// Single-grid step schedule of d with ctas_per_sm resident CTAs: returns its
+// modelled duration in CTA-slot plane-steps (waves x (segment + restart) x
+// slots); *work = the plane-steps of useful work (columns x planes).
+long long step_sched_cost(vti_ctx* ctx, const Dims3& d, int ctas_per_sm, long long* work);
 // The same over a volume of `elem_bytes` (4: float, 2: bfloat16) elements
 // with the layout of Vol (alloc = start of the pad planes).
 int make_tile_maps_typed(vti_ctx* ctx, const Dims3& d, void* alloc, int elem_bytes,

@@ -204,6 +204,31 @@ int check_finite(vti3d_plan* p, std::initializer_list<const Vol*> vols) {
   return VTI_OK;
 }
 
+// One forward level (objFuncGradient3d_f.cu:610-700): level `it` from
+// sx[A] (level it-1) and sx[B] (level it-2) into sx[B], then, for pass 1, the
+// traces of the new level. Pass 1 (sponge) runs on the pad-boundary model,
+// pass 2 on the random-boundary model when the plan has one.
+int fwd_level(vti3d_plan* p, const ShotGeom& s, bool sponge, int A, int B, int it) {
+  vti_ctx* ctx = p->ctx;
+  const vti3d_geom& g = p->g;
+  const float dt2 = g.dt * g.dt;
+  const TileMaps* cm = (sponge || !p->have_rand) ? p->m_cpad : p->m_crand;
+  Damping dmp{p->dampx, p->dampy, p->dampz};
+  PointSource src;
+  src.x = s.sx;
+  src.y = s.sy;
+  src.z = s.sz;
+  src.amp = dt2 * p->wavelet[it - 1];
+  VTI_TRY(launch_fwd3d_tma(ctx, p->d, p->m_sx[A], p->m_sz[A], p->m_sx[B], p->m_sz[B], cm[0],
+                           cm[1], cm[2], p->sz[A].origin, p->sx[B].origin, p->sz[B].origin,
+                           sponge ? &dmp : nullptr, dt2 / (g.dx * g.dx), dt2 / (g.dy * g.dy),
+                           dt2 / (g.dz * g.dz), src));
+  if (sponge && it < (int)s.rec_at.size() && s.rec_at[it] >= 0)
+    VTI_TRY(launch_record(ctx, p->d_trace, nnt_of(g), s.rec_at[it], p->sx[B].origin,
+                          p->sz[B].origin, p->d_rec, s.nr));
+  return VTI_OK;
+}
+
 // Forward propagation of one shot. sponge: pass 1 (pad-boundary model, sponge,
 // traces recorded into d_trace). Otherwise pass 2 (random-boundary model, no
 // sponge). On return sx[last_cur] holds level M and the other buffer M-1.
@@ -212,11 +237,8 @@ int forward_pass(vti3d_plan* p, const ShotGeom& s, bool sponge) {
   vti_ctx* ctx = p->ctx;
   const vti3d_geom& g = p->g;
   const Dims3& d = p->d;
-  const float dx2 = g.dx * g.dx, dy2 = g.dy * g.dy, dz2 = g.dz * g.dz, dt2 = g.dt * g.dt;
-  const float sxs = dt2 / dx2, sys = dt2 / dy2, szs = dt2 / dz2;
+  const float dt2 = g.dt * g.dt;
   const int nnt = nnt_of(g), M = last_level(g, p->flags);
-  const TileMaps* cm = (sponge || !p->have_rand) ? p->m_cpad : p->m_crand;
-  Damping dmp{p->dampx, p->dampy, p->dampz};
   for (int k = 0; k < 2; ++k) {
     VTI_TRY(vol_zero(ctx, d, &p->sx[k]));
     VTI_TRY(vol_zero(ctx, d, &p->sz[k]));
@@ -229,24 +251,49 @@ int forward_pass(vti3d_plan* p, const ShotGeom& s, bool sponge) {
   if (sponge && s.nr > 0)
     VTI_CUDA(ctx,
              cudaMemsetAsync(p->d_trace, 0, (size_t)nnt * s.nr * sizeof(float), ctx->stream));
-  PointSource src;
-  src.x = s.sx;
-  src.y = s.sy;
-  src.z = s.sz;
   for (int it = 2; it <= M; ++it) {
-    src.amp = dt2 * p->wavelet[it - 1];
-    VTI_TRY(launch_fwd3d_tma(ctx, d, p->m_sx[A], p->m_sz[A], p->m_sx[B], p->m_sz[B], cm[0],
-                             cm[1], cm[2], p->sz[A].origin, p->sx[B].origin, p->sz[B].origin,
-                             sponge ? &dmp : nullptr, sxs, sys, szs, src));
+    VTI_TRY(fwd_level(p, s, sponge, A, B, it));
     std::swap(A, B);
-    if (sponge && it < (int)s.rec_at.size() && s.rec_at[it] >= 0)
-      VTI_TRY(launch_record(ctx, p->d_trace, nnt, s.rec_at[it], p->sx[A].origin,
-                            p->sz[A].origin, p->d_rec, s.nr));
   }
   p->last_cur = A;
   if (sponge && s.nr > 0 && (p->flags & VTI_OPT_CHECK_FINITE))
     VTI_TRY(launch_check_finite(ctx, p->d_trace, (long long)nnt * s.nr));
   return check_finite(p, {&p->sx[0], &p->sx[1], &p->sz[0], &p->sz[1]});
+}
+
+// Backward step i of pass 3 (objFuncGradient3d_f.cu:920-1060): the source
+// field reconstructed from sx[SA] (current) and sx[SB] (next, overwritten),
+// the adjoint from lx[LA] and lx[LB] (overwritten) and the imaging terms
+// added into g11/g13/g33 (the RTM image into g11), then the residual of time
+// nt-2-i injected into the new adjoint level (injectRecord3d.cu:60-78).
+int bwd_level(vti3d_plan* p, const ShotGeom& s, bool rtm, int SA, int SB, int LA, int LB,
+              int i) {
+  vti_ctx* ctx = p->ctx;
+  const vti3d_geom& g = p->g;
+  const float dx2 = g.dx * g.dx, dy2 = g.dy * g.dy, dz2 = g.dz * g.dz, dt2 = g.dt * g.dt;
+  const int st = sampling_step(g), nnt = nnt_of(g);
+  const TileMaps* cm = p->have_rand ? p->m_crand : p->m_cpad;
+  Damping dmp{p->dampx, p->dampy, p->dampz};
+  const int it = g.nt - 3 - i;
+  PointSource src;
+  src.x = s.sx;
+  src.y = s.sy;
+  src.z = s.sz;
+  src.amp = dt2 * p->wavelet[it + 1];
+  VTI_TRY(launch_bwd3d_tma(
+      ctx, p->d, p->m_sx[SA], p->m_sz[SA], p->m_sx[SB], p->m_sz[SB], p->m_lx[LA], p->m_lz[LA],
+      p->m_lx[LB], p->m_lz[LB], cm[0], cm[1], cm[2], p->m_g[0], p->m_g[1], p->m_g[2],
+      p->sz[SA].origin, p->lz[LA].origin, p->sx[SB].origin, p->sz[SB].origin,
+      p->lx[LB].origin, p->lz[LB].origin, p->g11.origin, p->g13.origin, p->g33.origin, dmp,
+      dt2, 1.f / dx2, 1.f / dy2, 1.f / dz2, dt2 / dx2, dt2 / dy2, dt2 / dz2, src, rtm));
+  // residual interpolated at it+1 (injectRecord3d.cu:60-78)
+  const int ti = it + 1;
+  float f = float(ti) / float(st);
+  int i0 = (int)f;
+  int clamp = i0 >= nnt - 1;
+  f = f - i0;
+  return launch_inject_residual(ctx, p->lx[LB].origin, p->lz[LB].origin, p->d_trace, nnt,
+                                clamp ? 0 : i0, f, clamp, p->d_rec, p->d_rec_damp, s.nr, dt2);
 }
 
 // Time-reversed source wavefield + adjoint + imaging (pass 3,
@@ -256,17 +303,13 @@ int forward_pass(vti3d_plan* p, const ShotGeom& s, bool sponge) {
 // g11 (rtm3d_f.cu:470-620, same schedule).
 // ext (nlag >= 0, RTM only): offset-domain gathers of each level added after
 // its fused step, from the same current wavefields.
-int backward_pass(vti3d_plan* p, const ShotGeom& s, bool rtm, float* ext = nullptr,
-                  int nlag = 0) {
+int backward_pass(vti3d_plan* p, const ShotGeom& s, bool rtm, float* ext, int nlag) {
   NvtxRange nv(rtm ? "vti3d RTM back-propagation" : "vti3d pass 3 (reconstruction, adjoint, imaging)");
   vti_ctx* ctx = p->ctx;
   const vti3d_geom& g = p->g;
   const Dims3& d = p->d;
-  const float dx2 = g.dx * g.dx, dy2 = g.dy * g.dy, dz2 = g.dz * g.dz, dt2 = g.dt * g.dt;
-  const float sxs = dt2 / dx2, sys = dt2 / dy2, szs = dt2 / dz2;
-  const float idx2 = 1.f / dx2, idy2 = 1.f / dy2, idz2 = 1.f / dz2;
-  const int st = sampling_step(g), nnt = nnt_of(g), M = last_level(g, p->flags);
-  const TileMaps* cm = p->have_rand ? p->m_crand : p->m_cpad;
+  const float dt2 = g.dt * g.dt;
+  const int nnt = nnt_of(g), M = last_level(g, p->flags);
   Damping dmp{p->dampx, p->dampy, p->dampz};
   // flip (objFuncGradient3d_f.cu:912-914): cur = level M-1, prev = level M
   int SA = 1 - p->last_cur, SB = p->last_cur;
@@ -277,30 +320,13 @@ int backward_pass(vti3d_plan* p, const ShotGeom& s, bool rtm, float* ext = nullp
   int LA = 0, LB = 1;
   VTI_TRY(launch_seed_adjoint(ctx, p->lx[LA].origin, p->lz[LA].origin, p->d_trace, nnt,
                               p->d_rec + p->rec_cap, p->d_rec_damp, s.nr, dt2));
-  PointSource src;
-  src.x = s.sx;
-  src.y = s.sy;
-  src.z = s.sz;
   for (int i = 0; i < M - 1; ++i) {
-    const int it = g.nt - 3 - i;
-    src.amp = dt2 * p->wavelet[it + 1];
-    VTI_TRY(launch_bwd3d_tma(
-        ctx, d, p->m_sx[SA], p->m_sz[SA], p->m_sx[SB], p->m_sz[SB], p->m_lx[LA], p->m_lz[LA],
-        p->m_lx[LB], p->m_lz[LB], cm[0], cm[1], cm[2], p->m_g[0], p->m_g[1], p->m_g[2],
-        p->sz[SA].origin, p->lz[LA].origin, p->sx[SB].origin, p->sz[SB].origin,
-        p->lx[LB].origin, p->lz[LB].origin, p->g11.origin, p->g13.origin, p->g33.origin, dmp,
-        dt2, idx2, idy2, idz2, sxs, sys, szs, src, rtm));
+    VTI_TRY(bwd_level(p, s, rtm, SA, SB, LA, LB, i));
+    // the gathers read the current levels sx[SA], lx[LA]; the step and the
+    // injection write only sx[SB], lx[LB]
     if (ext)
       VTI_TRY(launch_odcig3d(ctx, d, p->sx[SA].origin, p->sz[SA].origin, p->lx[LA].origin,
                              p->lz[LA].origin, dmp, nlag, ext));
-    // residual interpolated at it+1 (injectRecord3d.cu:60-78)
-    const int ti = it + 1;
-    float f = float(ti) / float(st);
-    int i0 = (int)f;
-    int clamp = i0 >= nnt - 1;
-    f = f - i0;
-    VTI_TRY(launch_inject_residual(ctx, p->lx[LB].origin, p->lz[LB].origin, p->d_trace, nnt,
-                                   clamp ? 0 : i0, f, clamp, p->d_rec, p->d_rec_damp, s.nr, dt2));
     std::swap(SA, SB);
     std::swap(LA, LB);
   }

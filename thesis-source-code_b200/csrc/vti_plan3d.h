@@ -89,6 +89,21 @@ int shot_geom(vti3d_plan* p, const float* souloc, int is, ShotGeom* s);
 int upload_shot(vti3d_plan* p, const ShotGeom& s);
 // Device pointer to the shot's observed traces (copied from the host if needed).
 int get_obs(vti3d_plan* p, const ShotGeom& s, const float* dobs, int mem, const float** out);
+// One forward level `it` of pass 1 (sponge: pad model, traces) or pass 2
+// (random-boundary model): sx[A] = level it-1, sx[B] = level it-2 in, level
+// it out in sx[B].
+int fwd_level(vti3d_plan* p, const ShotGeom& s, bool sponge, int A, int B, int it);
+// Backward step i of pass 3 with its residual injection: source fields
+// sx[SA] (current) / sx[SB] (overwritten), adjoint lx[LA] / lx[LB]
+// (overwritten), imaging into g11/g13/g33.
+int bwd_level(vti3d_plan* p, const ShotGeom& s, bool rtm, int SA, int SB, int LA, int LB,
+              int i);
+// Whole passes: forward_pass leaves level M in sx[last_cur] and M-1 in the
+// other buffer; backward_pass runs the M-1 backward steps from there (nlag
+// offset-domain gathers into ext when ext is given).
+int forward_pass(vti3d_plan* p, const ShotGeom& s, bool sponge);
+int backward_pass(vti3d_plan* p, const ShotGeom& s, bool rtm, float* ext = nullptr,
+                  int nlag = 0);
 
 template <typename T>
 int ensure(vti_ctx* ctx, T** ptr, size_t* cap, size_t n) {

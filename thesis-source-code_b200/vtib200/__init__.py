@@ -7,6 +7,7 @@ raises. Arrays are numpy float32/int32 (host) or raw device pointers
 """
 from __future__ import annotations
 
+import atexit
 import ctypes as C
 import weakref
 from pathlib import Path
@@ -32,6 +33,10 @@ MEM_HOST = 0
 MEM_DEVICE = 1
 OPT_FULL_STEPS = 1
 OPT_CHECK_FINITE = 2
+# schedules of Batch3d.gradient
+BATCH_AUTO = 0
+BATCH_SIDE_BY_SIDE = 1
+BATCH_PER_SHOT = 2
 
 
 class VtiError(RuntimeError):
@@ -135,6 +140,8 @@ def _signatures():
         "vti3d_batch_set_shots": (C.c_int, [P, C.c_int, P, P, C.c_uint]),
         "vti3d_batch_set_options": (C.c_int, [P, C.c_int, C.c_int, C.c_int]),
         "vti3d_batch_autotune": (C.c_int, [P, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+        "vti3d_batch_set_schedule": (C.c_int, [P, C.c_int]),
+        "vti3d_batch_get_schedule": (C.c_int, [P, C.POINTER(C.c_int)]),
         "vti3d_batch_gradient": (C.c_int, [P, P, C.c_int, P, C.c_int, C.POINTER(C.c_double)]),
         "vti3d_batch_get_shot_models": (C.c_int, [P, C.c_int, P, P]),
         "vti3d_gnhv_exact": (C.c_int, [P] * 9 + [C.c_int, P, C.c_int, C.c_uint, P, P,
@@ -198,6 +205,22 @@ def _i32(a):
     return np.ascontiguousarray(a, dtype=np.int32)
 
 
+_contexts = weakref.WeakSet()
+
+
+@atexit.register
+def _close_contexts():
+    """Closes every live context (its plans, batches and engines first) while
+    the interpreter and the CUDA runtime are still whole; left to garbage
+    collection at shutdown, a handle could be destroyed after the library
+    that owns it."""
+    for c in list(_contexts):
+        try:
+            c.close()
+        except Exception:
+            pass
+
+
 class Context:
     """One CUDA device. Mirrors vti_ctx_create/destroy."""
 
@@ -207,6 +230,7 @@ class Context:
         st = lib().vti_ctx_create(device, C.byref(self._h))
         if st != VTI_OK:
             raise VtiError(st, "vti_ctx_create failed (no CUDA device?)")
+        _contexts.add(self)
 
     @property
     def handle(self):
@@ -416,6 +440,17 @@ class Batch3d:
         a, b = C.c_int(0), C.c_int(0)
         self.ctx.check(lib().vti3d_batch_autotune(self._h, C.byref(a), C.byref(b)))
         return a.value, b.value
+
+    def set_schedule(self, schedule):
+        """BATCH_AUTO, BATCH_SIDE_BY_SIDE or BATCH_PER_SHOT."""
+        self.ctx.check(lib().vti3d_batch_set_schedule(self._h, int(schedule)))
+
+    @property
+    def schedule(self):
+        """The schedule the next gradient runs (auto resolved)."""
+        v = C.c_int(0)
+        self.ctx.check(lib().vti3d_batch_get_schedule(self._h, C.byref(v)))
+        return v.value
 
     def gradient(self, dobs, dobs_mem=MEM_HOST, fgcij=None, fgcij_mem=MEM_HOST):
         if dobs_mem == MEM_HOST:
