@@ -182,6 +182,32 @@ int vti3d_plan_gradient(vti3d_plan* plan, const float* souloc, const int* shotid
  * misfit-only entry (vti3d_plan_objfunc) stays plain L2, as objFuncCij3d_f.
  * Defaults: 0, 0, 20. */
 int vti3d_plan_set_misfit(vti3d_plan* plan, float tpow, int objtype, int halfwidth);
+/* Observed traces in flight as 16 bits. VTI_TRACES_F32 (default): dobs /
+ * data arguments are FP32 traces as the reference passes them. VTI_TRACES_F16:
+ * they point to a packed block of vti_traces_f16_bytes(nr_total, nnt)
+ * bytes made by vti_traces_pack_f16 (host or device memory, per the call's
+ * mem argument), which moves half the bytes; each shot's traces are expanded
+ * to FP32 on the device before the misfit; the results are bitwise those of
+ * the FP32 traces the block stands for (vti_traces_unpack_f16). Plane scales
+ * keep every sample at FP16's full relative precision (2^-11). The gradient
+ * is linear in the residual, so against the gradient of the original FP32
+ * traces it moves by about |dq - d| / |residual| (relative L2, dq the
+ * unpacked data): measured 4e-6 with a residual of 91 % of the data and 1e-3
+ * with 13 % — a format for early FWI iterations, not for late ones. BF16
+ * values move it 12x more and are not offered. */
+#define VTI_TRACES_F32 0
+#define VTI_TRACES_F16 1
+int vti3d_plan_set_trace_format(vti3d_plan* plan, int format);
+/* Bytes of a packed block of nr traces of nnt samples: nnt FP32 scales (one
+ * per time sample, the maximum |value| over all nr traces at that sample, 1
+ * where it is 0) followed by nr*nnt IEEE half values, trace-major. */
+size_t vti_traces_f16_bytes(int nr, int nnt);
+/* Packs nr FP32 traces of nnt samples (trace-major, host) into a block
+ * (host): value / scale rounded to the nearest half (ties to even). Returns
+ * VTI_ERR_NONFINITE if a sample is NaN or Inf. */
+int vti_traces_pack_f16(const float* traces, int nr, int nnt, void* block);
+/* The FP32 traces a block stands for (host). */
+int vti_traces_unpack_f16(const void* block, int nr, int nnt, float* traces);
 /* Misfit only (objFuncCij3d_f, objFuncGradient3d_f.cu:1272). */
 int vti3d_plan_objfunc(vti3d_plan* plan, const float* souloc, const int* shotid, int nshot,
                        const float* dobs, int dobs_mem, double* misfit);
@@ -362,6 +388,10 @@ int vti3d_batch_set_options(vti3d_batch* b, int use_graph, int seg_fwd, int seg_
 #define VTI_BATCH_SIDE_BY_SIDE 1
 #define VTI_BATCH_PER_SHOT 2
 int vti3d_batch_set_schedule(vti3d_batch* b, int schedule);
+/* Observed traces of vti3d_batch_gradient as FP32 (default) or as a
+ * VTI_TRACES_F16 block over all nr_total receivers (see
+ * vti3d_plan_set_trace_format). */
+int vti3d_batch_set_trace_format(vti3d_batch* b, int format);
 /* The schedule the next gradient runs (VTI_BATCH_SIDE_BY_SIDE or
  * VTI_BATCH_PER_SHOT): the one set, or what auto resolves to. */
 int vti3d_batch_get_schedule(vti3d_batch* b, int* schedule);

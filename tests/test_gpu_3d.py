@@ -269,3 +269,59 @@ def test_gradient_misfit_options_match_oracle_and_reference(ctx, name, key):
     l2 = O.gradient3d(g, c["cij"], c["padb"], c["randb"], s.wavelet, s.souloc, c["shotid"],
                       s.recloc, dobs, misfit_only=True)
     assert abs(plain - l2[0]) / l2[0] < TRACE_TOL
+
+
+def test_f16_traces_in_flight(ctx):
+    """Observed traces passed as a VTI_TRACES_F16 block (FP16 values, one FP32
+    scale per time sample): the plan expands each shot's traces on the device
+    to exactly the FP32 traces the block stands for, from host or device
+    memory, so the gradient is bitwise that of those traces and within the
+    FP32 bar of the FP64 oracle run on them. Against the gradient of the
+    original FP32 traces it moves by the quantisation of the data relative to
+    the residual (the gradient is linear in the residual): here the residual
+    is 13 % of the data and the move is 1e-3."""
+    import torch
+    c = K.case3d("g3_a")
+    s = c["s"]
+    g = s.geom()
+    n = s.nxyz
+    gold = load_golden("g3_a")
+    nnt = O.nnt3d(g)
+    nr = s.recloc.size // 4
+    dobs = np.asarray(gold["dobs"], dtype=np.float32)
+    block = V.pack_traces_f16(dobs, nnt)
+    assert block.nbytes < 0.51 * dobs.nbytes + 4 * nnt
+    dq = V.unpack_traces_f16(block, nr, nnt)
+    assert 0 < rel_l2(dq, dobs) < 1e-3
+    p = V.Plan3d(ctx, g)
+    try:
+        p.set_model(*_split(c["cij"], n), padb=c["padb"], randb=c["randb"])
+        p.set_wavelet(s.wavelet)
+        p.set_receivers(s.recloc)
+        fq, mq = p.gradient(s.souloc, c["shotid"], dq)
+        iq = p.rtm(s.souloc, c["shotid"], dq)
+        p.set_trace_format(V.TRACES_F16)
+        fh, mh = p.gradient(s.souloc, c["shotid"], block)
+        ih = p.rtm(s.souloc, c["shotid"], block)
+        bd = torch.from_numpy(block).cuda()
+        fd, md = p.gradient(s.souloc, c["shotid"], bd.data_ptr(), V.MEM_DEVICE)
+        torch.cuda.synchronize()
+        with pytest.raises(V.VtiError):
+            p.set_trace_format(5)
+    finally:
+        p.close()
+    np.testing.assert_array_equal(fh, fq)
+    np.testing.assert_array_equal(fd, fq)
+    np.testing.assert_array_equal(ih, iq)
+    assert mh == mq and md == mq
+    oq = O.gradient3d(g, c["cij"], c["padb"], c["randb"], s.wavelet, s.souloc, c["shotid"],
+                      s.recloc, dq)
+    for a, b in zip(_parts(fh, n), _parts(oq, n)):
+        assert np.abs(b).max() > 0
+        assert rel_l2(a, b) < GRAD_TOL
+    o = O.gradient3d(g, c["cij"], c["padb"], c["randb"], s.wavelet, s.souloc, c["shotid"],
+                     s.recloc, dobs)
+    mod = O.model_data3d(g, *_split(c["cij"], n), s.wavelet, s.souloc, c["shotid"], s.recloc)
+    bound = np.linalg.norm(dq - dobs) / np.linalg.norm(mod - dobs)
+    for a, b in zip(_parts(fh, n), _parts(o, n)):
+        assert rel_l2(a, b) < 1.5 * bound + GRAD_TOL

@@ -312,3 +312,42 @@ def test_reference_callers_link_against_the_shim():
         assert sym in undef, (obj, sym)          # the caller needs it from outside
         assert sym in subprocess.run(["c++filt"], input=exported, capture_output=True,
                                      text=True).stdout, sym  # and the shim exports it
+
+
+def _pack_f16_numpy(t, nnt):
+    """The packing the library documents, restated with numpy: per time
+    sample the largest |value| over all traces (1 where 0), values times the
+    FP32 reciprocal of it rounded to the nearest half."""
+    a = np.asarray(t, dtype=np.float32).reshape(-1, nnt)
+    sc = np.abs(a).max(axis=0, initial=np.float32(0))
+    sc = np.where(sc > 0, sc, np.float32(1)).astype(np.float32)
+    inv = (np.float32(1) / sc).astype(np.float32)
+    h = (a * inv).astype(np.float16)
+    return sc, h
+
+
+@pytest.mark.parametrize("nr,nnt", [(7, 33), (40, 8), (1, 1), (0, 5), (300, 751)])
+def test_traces_f16_block_matches_the_documented_packing(nr, nnt):
+    rng = np.random.default_rng(nr * 1000 + nnt)
+    decay = np.exp(-np.arange(nnt) / max(nnt / 6, 1)).astype(np.float32)
+    t = (rng.standard_normal((nr, nnt)) * decay).astype(np.float32)
+    if nr > 2:
+        t[:, nnt // 2] = 0.0  # an all-zero time plane packs with scale 1
+    block = V.pack_traces_f16(t, nnt)
+    assert block.size == V.traces_f16_bytes(nr, nnt) == 4 * nnt + 2 * nr * nnt
+    sc, h = _pack_f16_numpy(t, nnt)
+    np.testing.assert_array_equal(block[:4 * nnt].view(np.float32), sc)
+    np.testing.assert_array_equal(block[4 * nnt:].view(np.float16).reshape(nr, nnt), h)
+    back = V.unpack_traces_f16(block, nr, nnt)
+    np.testing.assert_array_equal(back, (h.astype(np.float32) * sc).reshape(-1))
+    if nr:
+        # every sample keeps the half's relative precision against its plane
+        err = np.abs(back.reshape(nr, nnt) - t) / sc
+        assert err.max() <= 2.0 ** -11 * 1.0001
+
+
+def test_traces_f16_packing_refuses_nonfinite_samples():
+    t = np.ones((3, 5), dtype=np.float32)
+    t[1, 2] = np.nan
+    with pytest.raises(V.VtiError):
+        V.pack_traces_f16(t, 5)

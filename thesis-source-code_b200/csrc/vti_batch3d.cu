@@ -209,6 +209,7 @@ struct vti3d_batch {
   float* d_full = nullptr;  // stacked gradient, 3 * nxyz
   int schedule = VTI_BATCH_AUTO;
   int tuned = 0;  // schedule measured by vti3d_batch_autotune (0: none yet)
+  int trace_format = VTI_TRACES_F32;
 };
 
 namespace {
@@ -672,6 +673,7 @@ int vti3d_batch_set_shots(vti3d_batch* b, int nshot, const float* souloc,
       return st;
     }
     b->plans.push_back(p);
+    p->trace_format = b->trace_format;
     p->wavelet = b->wavelet;
     p->recloc = b->recloc;
     p->nrec_total = b->nrec_total;
@@ -701,6 +703,15 @@ int vti3d_batch_set_options(vti3d_batch* b, int use_graph, int seg_fwd, int seg_
   b->use_graph = use_graph != 0;
   b->seg_fwd = seg_fwd;
   b->seg_bwd = seg_bwd;
+  return VTI_OK;
+}
+
+int vti3d_batch_set_trace_format(vti3d_batch* b, int format) {
+  if (!b) return VTI_ERR_ARG;
+  if (format != VTI_TRACES_F32 && format != VTI_TRACES_F16)
+    return fail(b->ctx, VTI_ERR_ARG, "unknown trace format");
+  b->trace_format = format;
+  for (vti3d_plan* p : b->plans) p->trace_format = format;
   return VTI_OK;
 }
 

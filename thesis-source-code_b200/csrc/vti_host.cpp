@@ -206,3 +206,77 @@ double vti2d_cfl_number(const vti2d_geom* g, const float* c11, const float* c13,
 }
 
 }  // extern "C"
+
+// ------------------------------------------------ 16-bit traces in flight
+// Block layout: nnt FP32 plane scales, then nr * nnt IEEE halves
+// (trace-major). The scale of time sample t is the largest |value| of any
+// trace at t, so every sample is packed at the half's full relative
+// precision (F16C conversions, round to nearest even).
+#include <immintrin.h>
+
+#include <algorithm>
+#include <vector>
+
+extern "C" {
+
+size_t vti_traces_f16_bytes(int nr, int nnt) {
+  if (nr < 0 || nnt < 0) return 0;
+  return (size_t)nnt * sizeof(float) + (size_t)nr * nnt * sizeof(uint16_t);
+}
+
+int vti_traces_pack_f16(const float* traces, int nr, int nnt, void* block) {
+  if ((!traces && nr > 0) || !block || nr < 0 || nnt < 1) return VTI_ERR_ARG;
+  float* scale = static_cast<float*>(block);
+  uint16_t* h = reinterpret_cast<uint16_t*>(scale + nnt);
+  std::vector<float> mx((size_t)nnt, 0.f);
+  int bad = 0;
+#pragma omp parallel
+  {
+    std::vector<float> local((size_t)nnt, 0.f);
+    int lbad = 0;
+#pragma omp for nowait
+    for (int r = 0; r < nr; ++r) {
+      const float* t = traces + (size_t)r * nnt;
+      for (int i = 0; i < nnt; ++i) {
+        const float a = std::fabs(t[i]);
+        if (!std::isfinite(a)) lbad = 1;
+        local[i] = std::max(local[i], a);
+      }
+    }
+#pragma omp critical
+    {
+      bad |= lbad;
+      for (int i = 0; i < nnt; ++i) mx[i] = std::max(mx[i], local[i]);
+    }
+  }
+  if (bad) return VTI_ERR_NONFINITE;
+  for (int i = 0; i < nnt; ++i) scale[i] = mx[i] > 0.f ? mx[i] : 1.f;
+  std::vector<float> inv((size_t)nnt);
+  for (int i = 0; i < nnt; ++i) inv[i] = 1.f / scale[i];
+#pragma omp parallel for
+  for (int r = 0; r < nr; ++r) {
+    const float* t = traces + (size_t)r * nnt;
+    uint16_t* o = h + (size_t)r * nnt;
+    int i = 0;
+    for (; i + 8 <= nnt; i += 8) {
+      const __m256 v = _mm256_mul_ps(_mm256_loadu_ps(t + i), _mm256_loadu_ps(inv.data() + i));
+      _mm_storeu_si128(reinterpret_cast<__m128i*>(o + i),
+                       _mm256_cvtps_ph(v, _MM_FROUND_TO_NEAREST_INT));
+    }
+    for (; i < nnt; ++i) o[i] = _cvtss_sh(t[i] * inv[i], _MM_FROUND_TO_NEAREST_INT);
+  }
+  return VTI_OK;
+}
+
+int vti_traces_unpack_f16(const void* block, int nr, int nnt, float* traces) {
+  if (!block || (!traces && nr > 0) || nr < 0 || nnt < 1) return VTI_ERR_ARG;
+  const float* scale = static_cast<const float*>(block);
+  const uint16_t* h = reinterpret_cast<const uint16_t*>(scale + nnt);
+#pragma omp parallel for
+  for (int r = 0; r < nr; ++r)
+    for (int i = 0; i < nnt; ++i)
+      traces[(size_t)r * nnt + i] = _cvtsh_ss(h[(size_t)r * nnt + i]) * scale[i];
+  return VTI_OK;
+}
+
+}  // extern "C"

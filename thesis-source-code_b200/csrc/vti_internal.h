@@ -309,6 +309,10 @@ int launch_boundary_merge(vti_ctx* ctx, const Dims3& d, int npad, const float* f
                           const float* blist, float* out);
 // VTI_ERR_NONFINITE bit of the status word if a[0, n) holds a NaN or Inf.
 int launch_check_finite(vti_ctx* ctx, const float* a, long long n);
+// nr traces of nnt FP16 samples (trace-major) times the per-sample scales
+// into FP32 traces.
+int launch_unpack_traces_f16(vti_ctx* ctx, const uint16_t* src, const float* scale, int nnt,
+                             int nr, float* dst);
 // *out (zeroed by the caller) <- bits of max over the volume of the largest
 // eigenvalue of [[c11 kh, c13 kz], [c13 kh, c33 kz]]; dt^2 times it is the
 // number vti3d_cfl_number returns.

@@ -19,6 +19,8 @@
 // The step kernels themselves (TMA-staged 2.5D blocking) are in
 // vti_tma3d.cu; this file holds the sparse per-receiver kernels and the
 // device side of the boundary merge and the misfit.
+#include <cuda_fp16.h>
+
 #include "vti_internal.h"
 
 namespace vti {
@@ -397,6 +399,26 @@ int launch_check_finite(vti_ctx* ctx, const float* a, long long n) {
   const int blocks = (int)std::min<long long>((n + 255) / 256, (long long)ctx->sm_count * 8);
   k_check_finite<<<blocks, 256, 0, ctx->stream>>>(a, n, ctx->d_status);
   VTI_LAUNCHED(ctx, "k_check_finite");
+  return VTI_OK;
+}
+
+namespace {
+// 16-bit traces in flight: sample t of every trace is h * scale[t], h an
+// IEEE half. One block per trace, threads along time (contiguous).
+__global__ void k_unpack_traces_f16(const __half* src, const float* scale, int nnt,
+                                    float* dst) {
+  const long long row = (long long)blockIdx.x * nnt;
+  for (int t = threadIdx.x; t < nnt; t += blockDim.x)
+    dst[row + t] = __half2float(src[row + t]) * scale[t];
+}
+}  // namespace
+
+int launch_unpack_traces_f16(vti_ctx* ctx, const uint16_t* src, const float* scale, int nnt,
+                             int nr, float* dst) {
+  if (nr <= 0) return VTI_OK;
+  k_unpack_traces_f16<<<nr, 256, 0, ctx->stream>>>(reinterpret_cast<const __half*>(src), scale,
+                                                  nnt, dst);
+  VTI_LAUNCHED(ctx, "k_unpack_traces_f16");
   return VTI_OK;
 }
 

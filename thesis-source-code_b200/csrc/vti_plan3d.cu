@@ -352,6 +352,26 @@ int check_geom(vti_ctx* ctx, const vti3d_geom* g) {
 int get_obs(vti3d_plan* p, const ShotGeom& s, const float* dobs, int mem, const float** out) {
   const int nnt = nnt_of(p->g);
   const size_t n = (size_t)nnt * s.nr;
+  if (p->trace_format == VTI_TRACES_F16) {
+    // block: nnt plane scales, then the halves of every trace
+    vti_ctx* ctx = p->ctx;
+    const float* scale = dobs;
+    const uint16_t* h = reinterpret_cast<const uint16_t*>(dobs + nnt) + (size_t)nnt * s.irbegin;
+    VTI_TRY(ensure(ctx, &p->d_obs, &p->obs_cap, n));
+    if (mem != VTI_MEM_DEVICE) {
+      VTI_TRY(ensure(ctx, &p->d_obs16, &p->obs16_cap, n));
+      VTI_TRY(ensure(ctx, &p->d_obs_scale, &p->obs_scale_cap, (size_t)nnt));
+      VTI_CUDA(ctx, cudaMemcpyAsync(p->d_obs16, h, n * sizeof(uint16_t),
+                                    cudaMemcpyHostToDevice, ctx->stream));
+      VTI_CUDA(ctx, cudaMemcpyAsync(p->d_obs_scale, scale, (size_t)nnt * sizeof(float),
+                                    cudaMemcpyHostToDevice, ctx->stream));
+      h = p->d_obs16;
+      scale = p->d_obs_scale;
+    }
+    VTI_TRY(launch_unpack_traces_f16(ctx, h, scale, nnt, s.nr, p->d_obs));
+    *out = p->d_obs;
+    return VTI_OK;
+  }
   const float* src = dobs + (size_t)nnt * s.irbegin;
   if (mem == VTI_MEM_DEVICE) {
     *out = src;
@@ -550,7 +570,8 @@ int vti3d_plan_destroy(vti3d_plan* p) {
   vol_free(&p->g13);
   vol_free(&p->g33);
   void* ptrs[] = {p->dampx, p->d_rec, p->d_rec_damp, p->d_live, p->d_trace,
-                  p->d_obs, p->d_blist, p->d_acc, p->d_gw, p->d_part, p->d_ext};
+                  p->d_obs, p->d_blist, p->d_acc, p->d_gw, p->d_part, p->d_ext,
+                  p->d_obs16, p->d_obs_scale};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   delete p;
@@ -663,6 +684,14 @@ int vti3d_plan_set_misfit(vti3d_plan* p, float tpow, int objtype, int halfwidth)
   p->tpow = tpow;
   p->objtype = objtype;
   p->halfwidth = halfwidth;
+  return VTI_OK;
+}
+
+int vti3d_plan_set_trace_format(vti3d_plan* p, int format) {
+  if (!p) return VTI_ERR_ARG;
+  if (format != VTI_TRACES_F32 && format != VTI_TRACES_F16)
+    return fail(p->ctx, VTI_ERR_ARG, "unknown trace format");
+  p->trace_format = format;
   return VTI_OK;
 }
 

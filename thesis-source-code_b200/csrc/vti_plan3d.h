@@ -44,6 +44,11 @@ struct vti3d_plan {
   size_t trace_cap = 0;
   float* d_obs = nullptr;
   size_t obs_cap = 0;
+  int trace_format = VTI_TRACES_F32;  // observed traces as passed by the caller
+  uint16_t* d_obs16 = nullptr;        // FP16 traces of one shot (host blocks)
+  size_t obs16_cap = 0;
+  float* d_obs_scale = nullptr;       // their plane scales
+  size_t obs_scale_cap = 0;
   float* d_blist = nullptr;
   size_t blist_cap = 0;
   double* d_acc = nullptr;
@@ -87,7 +92,8 @@ int check_geom(vti_ctx* ctx, const vti3d_geom* g);
 int shot_geom(vti3d_plan* p, const float* souloc, int is, ShotGeom* s);
 // Receiver tables of s into the plan's device scratch; trace buffer sized.
 int upload_shot(vti3d_plan* p, const ShotGeom& s);
-// Device pointer to the shot's observed traces (copied from the host if needed).
+// Device pointer to the shot's observed traces as FP32 (copied from the host
+// if needed; a VTI_TRACES_F16 block is expanded on the device).
 int get_obs(vti3d_plan* p, const ShotGeom& s, const float* dobs, int mem, const float** out);
 // One forward level `it` of pass 1 (sponge: pad model, traces) or pass 2
 // (random-boundary model): sx[A] = level it-1, sx[B] = level it-2 in, level

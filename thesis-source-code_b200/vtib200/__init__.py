@@ -33,6 +33,9 @@ MEM_HOST = 0
 MEM_DEVICE = 1
 OPT_FULL_STEPS = 1
 OPT_CHECK_FINITE = 2
+# observed-trace formats of Plan3d / Batch3d (set_trace_format)
+TRACES_F32 = 0
+TRACES_F16 = 1
 # schedules of Batch3d.gradient
 BATCH_AUTO = 0
 BATCH_SIDE_BY_SIDE = 1
@@ -141,6 +144,11 @@ def _signatures():
         "vti3d_batch_set_options": (C.c_int, [P, C.c_int, C.c_int, C.c_int]),
         "vti3d_batch_autotune": (C.c_int, [P, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "vti3d_batch_set_schedule": (C.c_int, [P, C.c_int]),
+        "vti3d_batch_set_trace_format": (C.c_int, [P, C.c_int]),
+        "vti3d_plan_set_trace_format": (C.c_int, [P, C.c_int]),
+        "vti_traces_f16_bytes": (C.c_size_t, [C.c_int, C.c_int]),
+        "vti_traces_pack_f16": (C.c_int, [P, C.c_int, C.c_int, P]),
+        "vti_traces_unpack_f16": (C.c_int, [P, C.c_int, C.c_int, P]),
         "vti3d_batch_get_schedule": (C.c_int, [P, C.POINTER(C.c_int)]),
         "vti3d_batch_gradient": (C.c_int, [P, P, C.c_int, P, C.c_int, C.POINTER(C.c_double)]),
         "vti3d_batch_get_shot_models": (C.c_int, [P, C.c_int, P, P]),
@@ -203,6 +211,39 @@ def _f32(a):
 
 def _i32(a):
     return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _obs(a):
+    """Observed traces for a plan or batch call: FP32 traces, or a packed
+    16-bit block (uint8 array from pack_traces_f16) passed through as is."""
+    if isinstance(a, np.ndarray) and a.dtype == np.uint8:
+        return np.ascontiguousarray(a)
+    return _f32(a)
+
+
+def traces_f16_bytes(nr: int, nnt: int) -> int:
+    return int(lib().vti_traces_f16_bytes(nr, nnt))
+
+
+def pack_traces_f16(traces, nnt: int):
+    """FP32 traces (nr x nnt, trace-major) -> a VTI_TRACES_F16 block (uint8):
+    nnt FP32 plane scales, then the traces as IEEE halves."""
+    t = _f32(traces).reshape(-1)
+    nr = t.size // nnt
+    block = np.zeros(traces_f16_bytes(nr, nnt), dtype=np.uint8)
+    st = lib().vti_traces_pack_f16(_p(t), nr, nnt, _p(block))
+    if st != VTI_OK:
+        raise VtiError(st, "vti_traces_pack_f16 failed")
+    return block
+
+
+def unpack_traces_f16(block, nr: int, nnt: int):
+    """The FP32 traces (nr * nnt) a VTI_TRACES_F16 block stands for."""
+    out = np.zeros(nr * nnt, dtype=np.float32)
+    st = lib().vti_traces_unpack_f16(_p(np.ascontiguousarray(block)), nr, nnt, _p(out))
+    if st != VTI_OK:
+        raise VtiError(st, "vti_traces_unpack_f16 failed")
+    return out
 
 
 _contexts = weakref.WeakSet()
@@ -337,7 +378,7 @@ class Plan3d:
     def gradient(self, souloc, shotid, dobs, dobs_mem=MEM_HOST, fgcij=None, fgcij_mem=MEM_HOST):
         souloc, shotid = _f32(souloc).reshape(-1), _i32(shotid)
         if dobs_mem == MEM_HOST:
-            dobs = _f32(dobs)
+            dobs = _obs(dobs)
         n = self.g.nx * self.g.ny * self.g.nz
         if fgcij is None:
             fgcij = np.zeros(1 + 3 * n, dtype=np.float32)
@@ -346,6 +387,11 @@ class Plan3d:
                                                  _p(dobs), dobs_mem, _p(fgcij), fgcij_mem,
                                                  C.byref(mis)))
         return fgcij, mis.value
+
+    def set_trace_format(self, fmt):
+        """TRACES_F32 (default) or TRACES_F16: observed data passed as a block
+        from pack_traces_f16 (host or device memory)."""
+        self.ctx.check(lib().vti3d_plan_set_trace_format(self._h, int(fmt)))
 
     def set_misfit(self, tpow=0.0, objtype=0, halfwidth=20):
         """tpow gain / AGC misfit of the gradient (the reference's tpow=,
@@ -356,7 +402,7 @@ class Plan3d:
         """rtmCij3d_f on the resident model: the image (nxyz)."""
         souloc, shotid = _f32(souloc).reshape(-1), _i32(shotid)
         if data_mem == MEM_HOST:
-            data = _f32(data)
+            data = _obs(data)
         if image is None:
             image = np.zeros(self.g.nx * self.g.ny * self.g.nz, dtype=np.float32)
         self.ctx.check(lib().vti3d_plan_rtm(self._h, _p(souloc), _p(shotid), len(shotid),
@@ -367,7 +413,7 @@ class Plan3d:
         """odcig3d_f on the resident model: (2 nlag + 1, nxyz) gathers, lag -nlag first."""
         souloc, shotid = _f32(souloc).reshape(-1), _i32(shotid)
         if data_mem == MEM_HOST:
-            data = _f32(data)
+            data = _obs(data)
         n = self.g.nx * self.g.ny * self.g.nz
         image = np.zeros((2 * nlag + 1) * n, dtype=np.float32)
         self.ctx.check(lib().vti3d_plan_odcig(self._h, _p(souloc), _p(shotid), len(shotid),
@@ -378,7 +424,7 @@ class Plan3d:
     def objfunc(self, souloc, shotid, dobs, dobs_mem=MEM_HOST):
         souloc, shotid = _f32(souloc).reshape(-1), _i32(shotid)
         if dobs_mem == MEM_HOST:
-            dobs = _f32(dobs)
+            dobs = _obs(dobs)
         mis = C.c_double(0)
         self.ctx.check(lib().vti3d_plan_objfunc(self._h, _p(souloc), _p(shotid), len(shotid),
                                                 _p(dobs), dobs_mem, C.byref(mis)))
@@ -441,6 +487,11 @@ class Batch3d:
         self.ctx.check(lib().vti3d_batch_autotune(self._h, C.byref(a), C.byref(b)))
         return a.value, b.value
 
+    def set_trace_format(self, fmt):
+        """TRACES_F32 (default) or TRACES_F16 (a pack_traces_f16 block over all
+        receivers)."""
+        self.ctx.check(lib().vti3d_batch_set_trace_format(self._h, int(fmt)))
+
     def set_schedule(self, schedule):
         """BATCH_AUTO, BATCH_SIDE_BY_SIDE or BATCH_PER_SHOT."""
         self.ctx.check(lib().vti3d_batch_set_schedule(self._h, int(schedule)))
@@ -454,7 +505,7 @@ class Batch3d:
 
     def gradient(self, dobs, dobs_mem=MEM_HOST, fgcij=None, fgcij_mem=MEM_HOST):
         if dobs_mem == MEM_HOST:
-            dobs = _f32(dobs)
+            dobs = _obs(dobs)
         n = self.g.nx * self.g.ny * self.g.nz
         if fgcij is None:
             fgcij = np.zeros(1 + 3 * n, dtype=np.float32)
