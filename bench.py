@@ -458,7 +458,9 @@ def run_batched(args):
     b.set_wavelet(s.wavelet)
     b.set_receivers(recloc)
     b.set_shots(souloc, wins, seed=4)
-    seg_f, seg_b = b.autotune()  # segment lengths, then the faster schedule
+    b.set_schedule({"auto": V.BATCH_AUTO, "side": V.BATCH_SIDE_BY_SIDE,
+                    "per_shot": V.BATCH_PER_SHOT}[args.schedule])
+    seg_f, seg_b = b.autotune()  # segment lengths, then (auto) the faster schedule
     schedule = b.schedule
     sched_name = {V.BATCH_SIDE_BY_SIDE: "side_by_side", V.BATCH_PER_SHOT: "per_shot"}
     dobs = torch.zeros(nnt * nrec, dtype=torch.float32, device="cuda")
@@ -500,7 +502,7 @@ def run_batched(args):
         e1.record(stream)
         torch.cuda.synchronize()
         other_ms = e0.elapsed_time(e1)
-        b.set_schedule(V.BATCH_AUTO)
+        b.set_schedule(schedule)
     # end to end: pinned host traces in, host gradient out
     h_dobs = torch.zeros(nnt * nrec, dtype=torch.float32).pin_memory()
     h_fg = torch.zeros(1 + 3 * n, dtype=torch.float32).pin_memory()
@@ -586,7 +588,8 @@ def run_batched(args):
         "schedules": {sched_name[schedule]: round(ms, 1),
                       sched_name[other]: round(other_ms, 1) if other_ms else None,
                       "unit": "ms per gradient of all shots",
-                      "chosen_by": "vti3d_batch_autotune (one level of each, timed)"},
+                      "chosen_by": ("vti3d_batch_autotune (one level of each, timed)"
+                                    if args.schedule == "auto" else "--schedule")},
         "gpts": round(pts / (ms / 1e3) / 1e9, 2),
         "plain": {"value": round(plain_s, 4), "unit": "shots/s",
                   "ms_per_shot": round(plain_ms, 1), "shots_timed": nplain,
@@ -1121,6 +1124,8 @@ def main():
                     choices=["gradient", "batched", "served", "gnhv", "forward2d", "parity"],
                     help="batched: many shots on their own windows vs the plain loop")
     ap.add_argument("--shots", type=int, default=64, help="batched workload: shots")
+    ap.add_argument("--schedule", default="auto", choices=["auto", "side", "per_shot"],
+                    help="batched workload: schedule (auto: the one autotune times faster)")
     ap.add_argument("--plain-shots", type=int, default=3,
                     help="batched workload: shots timed in the plain per-shot loop")
     ap.add_argument("--nt", type=int, default=0,
@@ -1140,8 +1145,9 @@ def main():
     ap.add_argument("--gn-grid", type=int, nargs=3, default=[600, 600, 300],
                     help="gnhv workload: nx ny nz")
     ap.add_argument("--gn-k", type=int, default=126, help="gnhv workload: checkpoint interval")
-    ap.add_argument("--gn-mode", default="bf16", choices=["bf16", "fp32"],
-                    help="gnhv workload: storage of the recomputed background levels")
+    ap.add_argument("--gn-mode", default="fp32", choices=["bf16", "fp32"],
+                    help="gnhv workload: storage of the recomputed background levels (fp32 "
+                         "meets the 1e-4 error budget; bf16 halves the segment memory)")
     ap.add_argument("--gn-check", type=int, nargs=3, default=[44, 56, 40],
                     help="gnhv workload: reduced grid of the FP64 oracle check")
     ap.add_argument("--gn-check-nt", type=int, default=300)
