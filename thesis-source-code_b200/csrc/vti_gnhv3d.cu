@@ -61,27 +61,56 @@ struct BornArgs {
 struct BornMaps {
   CUtensorMap ax, bx, az, bz, apx, apz, bpx, bpz, c11, c13, c33, d11, d13, d33;
 };
-constexpr int G_STAGES = 3;
+// Born step stage: two halo tiles (x fields) and 12 plain tiles (the two z
+// fields 4 planes below, the four previous-level tiles, the model and the
+// perturbation), three stages. Reading the model and the perturbation with
+// read-only loads instead (as the adjoint does) measured 4 % slower here:
+// the kernel already spills at 96 registers and the six pairs held across
+// the stage wait add to it.
+constexpr int GB_STAGES = 3;
 constexpr int G_OFF_P = 2 * HALO_BYTES;
-constexpr int G_STAGE_BYTES = G_OFF_P + 12 * PLAIN_BYTES;  // 32256
+constexpr int GB_STAGE_BYTES = G_OFF_P + 12 * PLAIN_BYTES;  // 32256
+constexpr int GB_SMEM = GB_STAGES * GB_STAGE_BYTES + 1024 + 2 * GB_STAGES * 8;
+static_assert(2 * GB_SMEM <= 228 * 1024, "two Born CTAs per SM");
+// Adjoint step stage: two halo tiles and 6 plain tiles (the two z fields 4
+// planes below, the four previous-level tiles). The model and the images are
+// not staged: each consumer thread reads its own float2 pairs with read-only
+// loads issued before it waits for the plane's stage, which keeps a stage at
+// 20 KB and five stages of two CTAs on one SM (0.583 -> 0.514 ms per
+// 400x400x200 launch).
+constexpr int G_STAGES = 5;
+constexpr int G_STAGE_BYTES = G_OFF_P + 6 * PLAIN_BYTES;  // 19968
 constexpr int G_SMEM = G_STAGES * G_STAGE_BYTES + 1024 + 2 * G_STAGES * 8;
+static_assert(2 * G_SMEM <= 228 * 1024, "two Gauss-Newton CTAs per SM");
 
-// Loads of one item: two halo tiles (x fields) and 12 plain tiles per plane.
-template <typename Maps, int kNumPlain>
+// Three float2 pairs of one thread at plane offset i (zeros where neither
+// point is updated).
+__device__ __forceinline__ void ldg3(const float* p0, const float* p1, const float* p2,
+                                     long long i, bool any, float2& r0, float2& r1, float2& r2) {
+  const float2 zero = make_float2(0.f, 0.f);
+  r0 = any ? __ldg(reinterpret_cast<const float2*>(p0 + i)) : zero;
+  r1 = any ? __ldg(reinterpret_cast<const float2*>(p1 + i)) : zero;
+  r2 = any ? __ldg(reinterpret_cast<const float2*>(p2 + i)) : zero;
+}
+
+// Loads of one item: two halo tiles (x fields) and kNumPlain plain tiles per
+// plane, into a ring of kStages stages of kStageBytes.
+template <typename Maps, int kNumPlain, int kStages, int kStageBytes>
 __device__ __forceinline__ bool produce14(const Sched& sc, const Maps& m, int* status, int li,
                                           unsigned char* smem, uint64_t* full, uint64_t* empty,
                                           long long& k) {
   static_assert(sizeof(Maps) == (2 + kNumPlain) * sizeof(CUtensorMap), "map layout");
+  static_assert(2 * HALO_BYTES + kNumPlain * PLAIN_BYTES <= kStageBytes, "stage size");
   const CUtensorMap* maps = reinterpret_cast<const CUtensorMap*>(&m);
   int bx, by, z0, z1;
   item(sc, li, bx, by, z0, z1);
   const int x0 = bx * TX, y0 = kHalo + by * TY;
   for (int z = z0; z < z1; ++z, ++k) {
-    const int s = (int)(k % G_STAGES);
-    if (k >= G_STAGES && !mbar_wait(&empty[s], (uint32_t)(((k / G_STAGES) & 1) ^ 1), status))
+    const int s = (int)(k % kStages);
+    if (k >= kStages && !mbar_wait(&empty[s], (uint32_t)(((k / kStages) & 1) ^ 1), status))
       return false;
     const int zp = z + kZPad;
-    unsigned char* st = smem + s * G_STAGE_BYTES;
+    unsigned char* st = smem + s * kStageBytes;
     mbar_arrive_expect_tx(&full[s], 2 * HALO_BYTES + kNumPlain * PLAIN_BYTES);
     tma_load(st, &maps[0], &full[s], x0 - kHalo, y0 - kHalo, zp);
     tma_load(st + HALO_BYTES, &maps[1], &full[s], x0 - kHalo, y0 - kHalo, zp);
@@ -155,13 +184,15 @@ __global__ void __launch_bounds__(NTHREADS, 2)
     k_born3d_tma(const __grid_constant__ BornMaps m, const __grid_constant__ BornArgs a) {
   extern __shared__ unsigned char smem_raw[];
   uint64_t *full, *empty;
-  unsigned char* smem = ring_init<G_STAGES, G_STAGE_BYTES>(smem_raw, full, empty);
+  unsigned char* smem = ring_init<GB_STAGES, GB_STAGE_BYTES>(smem_raw, full, empty);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   long long k = 0;
   if (warp == NCW) {
     if (lane == 0)
       for (int it = blockIdx.x; it < a.sc.items; it += gridDim.x)
-        if (!produce14<BornMaps, 12>(a.sc, m, a.status, it, smem, full, empty, k)) break;
+        if (!produce14<BornMaps, 12, GB_STAGES, GB_STAGE_BYTES>(a.sc, m, a.status, it, smem,
+                                                               full, empty, k))
+          break;
     return;
   }
   const int ry = warp * 2 + (lane >> 4);
@@ -185,12 +216,12 @@ __global__ void __launch_bounds__(NTHREADS, 2)
     bool ok = true;
     for (int z = z0; z < z1; ++z, ++k) {
       const float dz = a.dampz[z];
-      const int s = (int)(k % G_STAGES);
-      if (!mbar_wait(&full[s], (uint32_t)((k / G_STAGES) & 1), a.status)) {
+      const int s = (int)(k % GB_STAGES);
+      if (!mbar_wait(&full[s], (uint32_t)((k / GB_STAGES) & 1), a.status)) {
         ok = false;
         break;
       }
-      const unsigned char* st = smem + s * G_STAGE_BYTES;
+      const unsigned char* st = smem + s * GB_STAGE_BYTES;
       const float* pl = (const float*)(st + G_OFF_P) + pi;
       constexpr int T = TX * TY;
       queue_push(aq, ld2(pl));
@@ -264,9 +295,12 @@ struct AdjArgs {
   const float* dampz;
   float sx, sy, sz;
   int* status;
+  const float* c11;  // the model, read per point with read-only loads
+  const float* c13;
+  const float* c33;
 };
 struct AdjMaps {
-  CUtensorMap wx, ax, wz, az, m1x, m1z, mpx, mpz, c11, c13, c33, g11, g13, g33;
+  CUtensorMap wx, ax, wz, az, m1x, m1z, mpx, mpz;
 };
 
 __global__ void __launch_bounds__(NTHREADS, 2)
@@ -279,7 +313,9 @@ __global__ void __launch_bounds__(NTHREADS, 2)
   if (warp == NCW) {
     if (lane == 0)
       for (int it = blockIdx.x; it < a.sc.items; it += gridDim.x)
-        if (!produce14<AdjMaps, 12>(a.sc, m, a.status, it, smem, full, empty, k)) break;
+        if (!produce14<AdjMaps, 6, G_STAGES, G_STAGE_BYTES>(a.sc, m, a.status, it, smem, full,
+                                                            empty, k))
+          break;
     return;
   }
   const int ry = warp * 2 + (lane >> 4);
@@ -301,8 +337,14 @@ __global__ void __launch_bounds__(NTHREADS, 2)
     dxy[0] = v0 ? a.dampx[x] * a.dampy[y] : 1.f;
     dxy[1] = v1 ? a.dampx[x + 1] * a.dampy[y] : 1.f;
     bool ok = true;
+    const bool any = v0 || v1;
     for (int z = z0; z < z1; ++z, ++k) {
       const float dz = a.dampz[z];
+      // issued before the stage wait; this thread alone writes its image cells
+      float2 c11, c13, c33, g11o, g13o, g33o;
+      const long long gi = (long long)z * a.d.plane + off;
+      ldg3(a.c11, a.c13, a.c33, gi, any, c11, c13, c33);
+      ldg3(a.g11, a.g13, a.g33, gi, any, g11o, g13o, g33o);
       const int s = (int)(k % G_STAGES);
       if (!mbar_wait(&full[s], (uint32_t)((k / G_STAGES) & 1), a.status)) {
         ok = false;
@@ -318,8 +360,6 @@ __global__ void __launch_bounds__(NTHREADS, 2)
       sa.load((const float*)(st + HALO_BYTES) + sr);
       const float2 m1x = ld2(pl + 2 * T), m1z = ld2(pl + 3 * T);
       const float2 m2x = ld2(pl + 4 * T), m2z = ld2(pl + 5 * T);
-      const float2 c11 = ld2(pl + 6 * T), c13 = ld2(pl + 7 * T), c33 = ld2(pl + 8 * T);
-      const float2 g11o = ld2(pl + 9 * T), g13o = ld2(pl + 10 * T), g33o = ld2(pl + 11 * T);
       stage_release(&empty[s], lane);
       float mx[2], mz[2], wx[2], wzv[2], g11[2], g13[2], g33[2];
 #pragma unroll
@@ -426,13 +466,15 @@ __device__ __forceinline__ float2 ldb2(const __nv_bfloat16* p) {
 }
 
 // Adjoint step imaging against a BF16 background (stage: w halo FP32, a halo
-// BF16, w_z FP32, a_z BF16, then mu_{t+1}, mu_{t+2}, C, image FP32).
+// BF16, w_z FP32, a_z BF16, then mu_{t+1} and mu_{t+2}; the model and the
+// image by read-only loads as in the FP32 step).
 constexpr int A_OFF_AH = HALO_BYTES;
 constexpr int A_OFF_P = A_OFF_AH + HXB * HY * 2;  // BF16 halo tile, HXB x HY
 constexpr int A_OFF_AZ = A_OFF_P + PLAIN_BYTES;
 constexpr int A_OFF_R = A_OFF_AZ + PLAIN_BYTES / 2;
-constexpr int A_STAGE_BYTES = A_OFF_R + 10 * PLAIN_BYTES;  // 29696
+constexpr int A_STAGE_BYTES = A_OFF_R + 4 * PLAIN_BYTES;  // 17408
 constexpr int A_SMEM = G_STAGES * A_STAGE_BYTES + 1024 + 2 * G_STAGES * 8;
+static_assert(2 * A_SMEM <= 228 * 1024, "two BF16 adjoint CTAs per SM");
 static_assert(A_OFF_AH % 128 == 0 && A_OFF_P % 128 == 0 && A_OFF_AZ % 128 == 0 &&
                   A_OFF_R % 128 == 0 && A_STAGE_BYTES % 128 == 0,
               "TMA destinations on 128-byte boundaries");
@@ -475,7 +517,7 @@ __global__ void __launch_bounds__(NTHREADS, 2)
           tma_load(st + A_OFF_P, &maps[2], &full[s], x0, y0, zp + kHalo);
           tma_load(st + A_OFF_AZ, &maps[3], &full[s], x0, y0, zp + kHalo);
 #pragma unroll
-          for (int j = 0; j < 10; ++j)
+          for (int j = 0; j < 4; ++j)
             tma_load(st + A_OFF_R + j * PLAIN_BYTES, &maps[4 + j], &full[s], x0, y0, zp);
         }
         if (!ok) break;
@@ -512,10 +554,16 @@ __global__ void __launch_bounds__(NTHREADS, 2)
     dxy[0] = v0 ? a.dampx[x] * a.dampy[y] : 1.f;
     dxy[1] = v1 ? a.dampx[x + 1] * a.dampy[y] : 1.f;
     bool ok = true;
+    const bool any = v0 || v1;
     for (int z = z0; z < z1; ++z, ++k) {
       const float dz = a.dampz[z];
       const float scx = b.sxs[z + kZPad];
       const float scz = b.szs[z + kHalo + kZPad];
+      // issued before the stage wait; this thread alone writes its image cells
+      float2 c11, c13, c33, g11o, g13o, g33o;
+      const long long gi = (long long)z * a.d.plane + off;
+      ldg3(a.c11, a.c13, a.c33, gi, any, c11, c13, c33);
+      ldg3(a.g11, a.g13, a.g33, gi, any, g11o, g13o, g33o);
       const int s = (int)(k % G_STAGES);
       if (!mbar_wait(&full[s], (uint32_t)((k / G_STAGES) & 1), a.status)) {
         ok = false;
@@ -553,8 +601,6 @@ __global__ void __launch_bounds__(NTHREADS, 2)
       }
       const float2 m1x = ld2(pr), m1z = ld2(pr + T);
       const float2 m2x = ld2(pr + 2 * T), m2z = ld2(pr + 3 * T);
-      const float2 c11 = ld2(pr + 4 * T), c13 = ld2(pr + 5 * T), c33 = ld2(pr + 6 * T);
-      const float2 g11o = ld2(pr + 7 * T), g13o = ld2(pr + 8 * T), g33o = ld2(pr + 9 * T);
       stage_release(&empty[s], lane);
       float mx[2], mz[2], wx[2], wzv[2], g11[2], g13[2], g33[2];
 #pragma unroll
@@ -772,7 +818,7 @@ struct GnState {
 
 int launch_born(GnState& S, int cur, const p3d::ShotGeom& sg, float amp) {
   vti_ctx* ctx = S.ctx;
-  VTI_TRY(smem_attr(ctx, (const void*)k_born3d_tma, attr_born));
+  VTI_TRY(smem_attr(ctx, (const void*)k_born3d_tma, attr_born, GB_SMEM));
   const int nxt = 1 - cur;
   BornMaps m;
   m.ax = HM(S.a[cur][0].m);
@@ -805,7 +851,7 @@ int launch_born(GnState& S, int cur, const p3d::ShotGeom& sg, float amp) {
   x.status = ctx->d_status;
   {
     LaunchTimer tm(ctx, kTimedFwd3d);
-    k_born3d_tma<<<x.sc.grid, NTHREADS, G_SMEM, ctx->stream>>>(m, x);
+    k_born3d_tma<<<x.sc.grid, NTHREADS, GB_SMEM, ctx->stream>>>(m, x);
   }
   VTI_LAUNCHED(ctx, "k_born3d_tma");
   return VTI_OK;
@@ -829,10 +875,9 @@ int launch_adj(GnState& S, int im, int cur, int slot) {
   m.m1z = PM(S.mu[im][cur][1].m);
   m.mpx = PM(S.mu[im][nx_][0].m);
   m.mpz = PM(S.mu[im][nx_][1].m);
-  m.c11 = PM(S.c[0].m); m.c13 = PM(S.c[1].m); m.c33 = PM(S.c[2].m);
-  m.g11 = PM(S.img[im][0].m); m.g13 = PM(S.img[im][1].m); m.g33 = PM(S.img[im][2].m);
   const float dt2 = S.g.dt * S.g.dt;
   AdjArgs x{};
+  x.c11 = S.c[0].v.origin; x.c13 = S.c[1].v.origin; x.c33 = S.c[2].v.origin;
   x.d = S.d;
   x.sc = make_sched(ctx, S.d, 2);
   x.wz = S.w[im][cur][1].v.origin;
@@ -879,11 +924,10 @@ int launch_adj_b16(GnState& S, int im, int cur, int slot) {
   m.m1z = PM(S.mu[im][cur][1].m);
   m.mpx = PM(S.mu[im][nx_][0].m);
   m.mpz = PM(S.mu[im][nx_][1].m);
-  m.c11 = PM(S.c[0].m); m.c13 = PM(S.c[1].m); m.c33 = PM(S.c[2].m);
-  m.g11 = PM(S.img[im][0].m); m.g13 = PM(S.img[im][1].m); m.g33 = PM(S.img[im][2].m);
   const float dt2 = S.g.dt * S.g.dt;
   AdjArgsB b{};
   AdjArgs& x = b.f;
+  x.c11 = S.c[0].v.origin; x.c13 = S.c[1].v.origin; x.c33 = S.c[2].v.origin;
   x.d = S.d;
   x.sc = make_sched(ctx, S.d, 2);
   x.wz = S.w[im][cur][1].v.origin;
