@@ -142,7 +142,7 @@ __device__ __forceinline__ bool fwd_consume(const FwdCommon& a, const FwdPar& bp
   const int xo = 2 * (lane & 15);
   const int sr = (ry + kHalo) * HX + xo + kHalo;  // centre in the halo tile
   const int pi = ry * TX + xo;                    // centre in a plain tile
-  float q[2][9];
+  float2 q[9];  // z queue of the pair: planes z-4 .. z+4
   float dxy[2];
   int bx, by, z0, z1;
   item(a.sc, li, bx, by, z0, z1);
@@ -158,7 +158,7 @@ __device__ __forceinline__ bool fwd_consume(const FwdCommon& a, const FwdPar& bp
   dxy[0] = (damp && v0) ? a.dampx[x] * a.dampy[y] : 1.f;
   dxy[1] = (damp && v1) ? a.dampx[x + 1] * a.dampy[y] : 1.f;
   // start the queue: planes z0-4 .. z0+3 from global
-  q[0][0] = q[1][0] = 0.f;
+  q[0] = make_float2(0.f, 0.f);
 #pragma unroll
   for (int kk = 1; kk < 9; ++kk) {
     const int zz = z0 - 5 + kk;
@@ -170,8 +170,7 @@ __device__ __forceinline__ bool fwd_consume(const FwdCommon& a, const FwdPar& bp
       v.x *= dxy[0] * a.dampz[zz];
       v.y *= dxy[1] * a.dampz[zz];
     }
-    q[0][kk] = v.x;
-    q[1][kk] = v.y;
+    q[kk] = v;
   }
   // z damping factors in registers: dzr holds planes z-3..z once plane z
   // is entered (the block transition rescales those four queue entries);
@@ -196,13 +195,8 @@ __device__ __forceinline__ bool fwd_consume(const FwdCommon& a, const FwdPar& bp
     const float* pl = (const float*)(st + F_OFF_Z) + pi;  // [z+4][prev x][prev z]
     constexpr int T = TX * TY;
 #pragma unroll
-    for (int kk = 0; kk < 8; ++kk) {
-      q[0][kk] = q[0][kk + 1];
-      q[1][kk] = q[1][kk + 1];
-    }
-    const float2 zq = ld2(pl);
-    q[0][8] = zq.x;
-    q[1][8] = zq.y;
+    for (int kk = 0; kk < 8; ++kk) q[kk] = q[kk + 1];
+    q[8] = ld2(pl);
     // the row x-4 .. x+5 and the column pairs y +- 1..4
     float r[10];
 #pragma unroll
@@ -220,41 +214,68 @@ __device__ __forceinline__ bool fwd_consume(const FwdCommon& a, const FwdPar& bp
     const float2 px = ld2(pl + T), pz = ld2(pl + 2 * T);
     stage_release(&empty[s], lane);
     float nxv[2], nzv[2];
+    if (kExact) {
 #pragma unroll
-    for (int e = 0; e < 2; ++e) {
-      auto pick = [e](float2 v) { return e ? v.y : v.x; };
-      const float c = r[4 + e];
-      const float lxx = lap9(c, r[3 + e], r[5 + e], r[2 + e], r[6 + e], r[1 + e], r[7 + e],
-                             r[e], r[8 + e]);
-      const float lyy = lap9(c, pick(ym[0]), pick(yp[0]), pick(ym[1]), pick(yp[1]),
-                             pick(ym[2]), pick(yp[2]), pick(ym[3]), pick(yp[3]));
-      const float lzz = lap9(q[e][4], q[e][3], q[e][5], q[e][2], q[e][6], q[e][1], q[e][7],
-                             q[e][0], q[e][8]);
-      const float lxy = fmaf(lyy, a.sy, lxx * a.sx);
-      const float lz = lzz * a.sz;
-      const float dd = dxy[e] * dz;
-      const float a11 = pick(c11), a13 = pick(c13), a33 = pick(c33);
-      if (kExact) {
+      for (int e = 0; e < 2; ++e) {
+        auto pick = [e](float2 v) { return e ? v.y : v.x; };
+        const float c = r[4 + e];
+        const float lxx = lap9(c, r[3 + e], r[5 + e], r[2 + e], r[6 + e], r[1 + e], r[7 + e],
+                               r[e], r[8 + e]);
+        const float lyy = lap9(c, pick(ym[0]), pick(yp[0]), pick(ym[1]), pick(yp[1]),
+                               pick(ym[2]), pick(yp[2]), pick(ym[3]), pick(yp[3]));
+        const float lzz = lap9(pick(q[4]), pick(q[3]), pick(q[5]), pick(q[2]), pick(q[6]),
+                               pick(q[1]), pick(q[7]), pick(q[0]), pick(q[8]));
+        const float lxy = fmaf(lyy, a.sy, lxx * a.sx);
+        const float lz = lzz * a.sz;
+        const float dd = dxy[e] * dz;
+        const float a11 = pick(c11), a13 = pick(c13), a33 = pick(c33);
         // centred damping: D (C L cur + 2 cur + src) - (2D - 1) prev
         nxv[e] = fmaf(a11, lxy, fmaf(a13, lz, 2.f * c));
-        nzv[e] = fmaf(a13, lxy, fmaf(a33, lz, 2.f * q[e][4]));
+        nzv[e] = fmaf(a13, lxy, fmaf(a33, lz, 2.f * pick(q[4])));
         if (src_e == e && z == a.src.z) {
           nxv[e] += amp;
           nzv[e] += amp;
         }
         nxv[e] = fmaf(dd, nxv[e], -(2.f * dd - 1.f) * pick(px));
         nzv[e] = fmaf(dd, nzv[e], -(2.f * dd - 1.f) * pick(pz));
-      } else {
-        nxv[e] = fmaf(a11, lxy, fmaf(a13, lz, 2.f * c - dd * pick(px)));
-        nzv[e] = fmaf(a13, lxy, fmaf(a33, lz, 2.f * q[e][4] - dd * pick(pz)));
-        if (kProbe && prb_e == e && z == probe.z) *probe.out += nxv[e] + nzv[e];
-        if (src_e == e && z == a.src.z) {
-          nxv[e] += amp;
-          nzv[e] += amp;
-        }
-        nxv[e] *= dd;
-        nzv[e] *= dd;
       }
+    } else {
+      // the y and z stencils and the update of both points as packed FP32
+      // pairs (each lane rounded as the scalar operation); the x stencil per
+      // point, its neighbour pairs straddling the loaded float2s
+      const float2 c2 = make_float2(r[4], r[5]);
+      float2 lxx;
+      lxx.x = lap9(r[4], r[3], r[5], r[2], r[6], r[1], r[7], r[0], r[8]);
+      lxx.y = lap9(r[5], r[4], r[6], r[3], r[7], r[2], r[8], r[1], r[9]);
+      const float2 lyy = lap9_2(c2, ym[0], yp[0], ym[1], yp[1], ym[2], yp[2], ym[3], yp[3]);
+      const float2 lzz = lap9_2(q[4], q[3], q[5], q[2], q[6], q[1], q[7], q[0], q[8]);
+      const float2 lxy = fma2(lyy, splat(a.sy), mul2(lxx, splat(a.sx)));
+      const float2 lz = mul2(lzz, splat(a.sz));
+      const float2 dd = mul2(make_float2(dxy[0], dxy[1]), splat(dz));
+      const float2 ndd = mul2(dd, splat(-1.f));
+      // 2 cur - dd prev, rounded once
+      float2 nx = fma2(c11, lxy, fma2(c13, lz, fma2(ndd, px, mul2(splat(2.f), c2))));
+      float2 nz = fma2(c13, lxy, fma2(c33, lz, fma2(ndd, pz, mul2(splat(2.f), q[4]))));
+      if (kProbe && z == probe.z) {
+        if (prb_e == 0) *probe.out += nx.x + nz.x;
+        if (prb_e == 1) *probe.out += nx.y + nz.y;
+      }
+      if (z == a.src.z) {
+        if (src_e == 0) {
+          nx.x += amp;
+          nz.x += amp;
+        }
+        if (src_e == 1) {
+          nx.y += amp;
+          nz.y += amp;
+        }
+      }
+      nx = mul2(nx, dd);
+      nz = mul2(nz, dd);
+      nxv[0] = nx.x;
+      nxv[1] = nx.y;
+      nzv[0] = nz.x;
+      nzv[1] = nz.y;
     }
     const long long i = (long long)z * a.d.plane + off;
     if (v0 && v1) {
@@ -273,13 +294,11 @@ __device__ __forceinline__ bool fwd_consume(const FwdCommon& a, const FwdPar& bp
     // entering the next plane: if it starts a new 4-plane block of the same
     // column, the four planes of the block just finished become "damped cur"
     if (!kExact && damp && ((z + 1) & 3) == 0 && z + 1 < a.d.nz) {
+      // after the shift at z+1, entries 0..3 hold planes z-3..z; they are
+      // entries 1..4 now
 #pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        // after the shift at z+1, entries 0..3 hold planes z-3..z; they are
-        // entries 1..4 now
-#pragma unroll
-        for (int kk = 0; kk < 4; ++kk) q[e][kk + 1] *= dxy[e] * dzr[kk];
-      }
+      for (int kk = 0; kk < 4; ++kk)
+        q[kk + 1] = mul2(q[kk + 1], make_float2(dxy[0] * dzr[kk], dxy[1] * dzr[kk]));
     }
   }
   return true;
@@ -454,7 +473,7 @@ __device__ __forceinline__ bool bwd_consume(const BwdCommon& a, const BwdPar& bp
   const int xo = 2 * (lane & 15);
   const int sr = (ry + kHalo) * HX + xo + kHalo;
   const int pi = ry * TX + xo;
-  float sq[2][9], lq[2][9];
+  float2 sq[9], lq[9];  // z queues of the pair (source, adjoint): planes z-4 .. z+4
   float dxy[2];
   int bx, by, z0, z1;
   item(a.sc, li, bx, by, z0, z1);
@@ -467,7 +486,7 @@ __device__ __forceinline__ bool bwd_consume(const BwdCommon& a, const BwdPar& bp
   dxy[0] = v0 ? a.dampx[x] * a.dampy[y] : 1.f;
   dxy[1] = v1 ? a.dampx[x + 1] * a.dampy[y] : 1.f;
   // start the queues: planes z0-4 .. z0+3 from global
-  sq[0][0] = sq[1][0] = lq[0][0] = lq[1][0] = 0.f;
+  sq[0] = lq[0] = make_float2(0.f, 0.f);
 #pragma unroll
   for (int kk = 1; kk < 9; ++kk) {
     const int zz = z0 - 5 + kk;
@@ -480,10 +499,8 @@ __device__ __forceinline__ bool bwd_consume(const BwdCommon& a, const BwdPar& bp
       lv.x *= dxy[0] * a.dampz[zz];
       lv.y *= dxy[1] * a.dampz[zz];
     }
-    sq[0][kk] = sv.x;
-    sq[1][kk] = sv.y;
-    lq[0][kk] = lv.x;
-    lq[1][kk] = lv.y;
+    sq[kk] = sv;
+    lq[kk] = lv;
   }
   // z damping factors in registers (see the forward kernel)
   float dzr[4];
@@ -519,18 +536,11 @@ __device__ __forceinline__ bool bwd_consume(const BwdCommon& a, const BwdPar& bp
     constexpr int T = TX * TY;
 #pragma unroll
     for (int kk = 0; kk < 8; ++kk) {
-      sq[0][kk] = sq[0][kk + 1];
-      sq[1][kk] = sq[1][kk + 1];
-      lq[0][kk] = lq[0][kk + 1];
-      lq[1][kk] = lq[1][kk + 1];
+      sq[kk] = sq[kk + 1];
+      lq[kk] = lq[kk + 1];
     }
-    {
-      const float2 s8 = ld2(pl), l8 = ld2(pl + T);
-      sq[0][8] = s8.x;
-      sq[1][8] = s8.y;
-      lq[0][8] = l8.x;
-      lq[1][8] = l8.y;
-    }
+    sq[8] = ld2(pl);
+    lq[8] = ld2(pl + T);
     // x rows (x-4 .. x+5) and y column pairs of both halo fields
     float rs[10], rl[10];
 #pragma unroll
@@ -552,84 +562,74 @@ __device__ __forceinline__ bool bwd_consume(const BwdCommon& a, const BwdPar& bp
     const float2 spx = ld2(pl + 2 * T), spz = ld2(pl + 3 * T);
     const float2 lpx = ld2(pl + 4 * T), lpz = ld2(pl + 5 * T);
     stage_release(&empty[s], lane);
-    float snx[2], snz[2], lnx[2], lnz[2], g11[2], g13[2], g33[2];
-#pragma unroll
-    for (int e = 0; e < 2; ++e) {
-      auto pick = [e](float2 v) { return e ? v.y : v.x; };
-      const float a11 = pick(c11), a13 = pick(c13), a33 = pick(c33);
-      // source wavefield back one level (gradient form)
-      const float sc = rs[4 + e];
-      const float sxx = lap9(sc, rs[3 + e], rs[5 + e], rs[2 + e], rs[6 + e], rs[1 + e],
-                             rs[7 + e], rs[e], rs[8 + e]);
-      const float syy = lap9(sc, pick(sym[0]), pick(syp[0]), pick(sym[1]), pick(syp[1]),
-                             pick(sym[2]), pick(syp[2]), pick(sym[3]), pick(syp[3]));
-      const float szz = lap9(sq[e][4], sq[e][3], sq[e][5], sq[e][2], sq[e][6], sq[e][1],
-                             sq[e][7], sq[e][0], sq[e][8]);
-      const float sxy_u = fmaf(syy, a.idy2, sxx * a.idx2);
-      const float sz_u = szz * a.idz2;
-      snx[e] = fmaf(a.dt2, fmaf(a11, sxy_u, a13 * sz_u), 2.f * sc - pick(spx));
-      snz[e] = fmaf(a.dt2, fmaf(a13, sxy_u, a33 * sz_u), 2.f * sq[e][4] - pick(spz));
-      if (x + e == a.src.x && y == a.src.y && z == a.src.z) {
-        snx[e] += amp;
-        snz[e] += amp;
-      }
-      // imaging with the current adjoint
-      const float lc = rl[4 + e];
-      const float lz0 = lq[e][4];
-      const float dd = dxy[e] * dz;
-      if (kRtm) {
-        g11[e] = fmaf(fmaf(kTwoThirdF, sc, kOneThirdF * sq[e][4]),
-                      dd * fmaf(kTwoThirdF, lc, kOneThirdF * lz0), pick(g11o));
-      } else {
-        g11[e] = fmaf(lc, sxy_u, pick(g11o));
-        g33[e] = fmaf(lz0, sz_u, pick(g33o));
-        g13[e] = fmaf(lz0, sxy_u, fmaf(lc, sz_u, pick(g13o)));
-      }
-      // adjoint, forward form with the sponge
-      const float lxx = lap9(lc, rl[3 + e], rl[5 + e], rl[2 + e], rl[6 + e], rl[1 + e],
-                             rl[7 + e], rl[e], rl[8 + e]);
-      const float lyy = lap9(lc, pick(lym[0]), pick(lyp[0]), pick(lym[1]), pick(lyp[1]),
-                             pick(lym[2]), pick(lyp[2]), pick(lym[3]), pick(lyp[3]));
-      const float lzz = lap9(lz0, lq[e][3], lq[e][5], lq[e][2], lq[e][6], lq[e][1], lq[e][7],
-                             lq[e][0], lq[e][8]);
-      const float lxy = fmaf(lyy, a.sy, lxx * a.sx);
-      const float lzs = lzz * a.sz;
-      lnx[e] = dd * fmaf(a11, lxy, fmaf(a13, lzs, 2.f * lc - dd * pick(lpx)));
-      lnz[e] = dd * fmaf(a13, lxy, fmaf(a33, lzs, 2.f * lz0 - dd * pick(lpz)));
-    }
+    // the y and z stencils, the updates and the imaging of both points as
+    // packed FP32 pairs (each lane rounded as the scalar operation); the x
+    // stencils per point, their neighbour pairs straddling the loaded float2s
+    const float2 two = splat(2.f);
+    // source wavefield back one level (gradient form)
+    // every stencil first (the y columns and x rows die as they are used)
+    const float2 sc = make_float2(rs[4], rs[5]);
+    const float2 lc = make_float2(rl[4], rl[5]);
+    const float2 syy = lap9_2(sc, sym[0], syp[0], sym[1], syp[1], sym[2], syp[2], sym[3], syp[3]);
+    const float2 lyy = lap9_2(lc, lym[0], lyp[0], lym[1], lyp[1], lym[2], lyp[2], lym[3], lyp[3]);
+    float2 sxx, lxx;
+    sxx.x = lap9(rs[4], rs[3], rs[5], rs[2], rs[6], rs[1], rs[7], rs[0], rs[8]);
+    sxx.y = lap9(rs[5], rs[4], rs[6], rs[3], rs[7], rs[2], rs[8], rs[1], rs[9]);
+    lxx.x = lap9(rl[4], rl[3], rl[5], rl[2], rl[6], rl[1], rl[7], rl[0], rl[8]);
+    lxx.y = lap9(rl[5], rl[4], rl[6], rl[3], rl[7], rl[2], rl[8], rl[1], rl[9]);
+    const float2 szz = lap9_2(sq[4], sq[3], sq[5], sq[2], sq[6], sq[1], sq[7], sq[0], sq[8]);
+    const float2 lzz = lap9_2(lq[4], lq[3], lq[5], lq[2], lq[6], lq[1], lq[7], lq[0], lq[8]);
+    const float2 sxy_u = fma2(syy, splat(a.idy2), mul2(sxx, splat(a.idx2)));
+    const float2 sz_u = mul2(szz, splat(a.idz2));
     const long long i = (long long)z * a.d.plane + off;
-    if (v0 && v1) {
-      *reinterpret_cast<float2*>(bp.spx + i) = make_float2(snx[0], snx[1]);
-      *reinterpret_cast<float2*>(bp.spz + i) = make_float2(snz[0], snz[1]);
-      *reinterpret_cast<float2*>(bp.lpx + i) = make_float2(lnx[0], lnx[1]);
-      *reinterpret_cast<float2*>(bp.lpz + i) = make_float2(lnz[0], lnz[1]);
-      *reinterpret_cast<float2*>(a.g11 + i) = make_float2(g11[0], g11[1]);
-      if (!kRtm) {
-        *reinterpret_cast<float2*>(a.g13 + i) = make_float2(g13[0], g13[1]);
-        *reinterpret_cast<float2*>(a.g33 + i) = make_float2(g33[0], g33[1]);
+    // each result pair is stored as soon as it is complete (shorter live
+    // ranges: the whole step fits the 96 registers of two CTAs per SM)
+    auto store2 = [&](float* f, float2 v) {
+      if (v0 && v1) {
+        *reinterpret_cast<float2*>(f + i) = v;
+      } else {
+        if (v0) f[i] = v.x;
+        if (v1) f[i + 1] = v.y;
       }
-    } else {
-#pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        if (e ? v1 : v0) {
-          bp.spx[i + e] = snx[e];
-          bp.spz[i + e] = snz[e];
-          bp.lpx[i + e] = lnx[e];
-          bp.lpz[i + e] = lnz[e];
-          a.g11[i + e] = g11[e];
-          if (!kRtm) {
-            a.g13[i + e] = g13[e];
-            a.g33[i + e] = g33[e];
-          }
-        }
+    };
+    const float2 dt2 = splat(a.dt2);
+    float2 snx = fma2(dt2, fma2(c11, sxy_u, mul2(c13, sz_u)), sub2(mul2(two, sc), spx));
+    float2 snz = fma2(dt2, fma2(c13, sxy_u, mul2(c33, sz_u)), sub2(mul2(two, sq[4]), spz));
+    if (y == a.src.y && z == a.src.z) {
+      if (x == a.src.x) {
+        snx.x += amp;
+        snz.x += amp;
+      }
+      if (x + 1 == a.src.x) {
+        snx.y += amp;
+        snz.y += amp;
       }
     }
+    store2(bp.spx, snx);
+    store2(bp.spz, snz);
+    // imaging with the current adjoint
+    const float2 lz0 = lq[4];
+    const float2 dd = mul2(make_float2(dxy[0], dxy[1]), splat(dz));
+    if (kRtm) {
+      store2(a.g11, fma2(fma2(splat(kTwoThirdF), sc, mul2(splat(kOneThirdF), sq[4])),
+                         mul2(dd, fma2(splat(kTwoThirdF), lc, mul2(splat(kOneThirdF), lz0))),
+                         g11o));
+    } else {
+      store2(a.g11, fma2(lc, sxy_u, g11o));
+      store2(a.g33, fma2(lz0, sz_u, g33o));
+      store2(a.g13, fma2(lz0, sxy_u, fma2(lc, sz_u, g13o)));
+    }
+    // adjoint, forward form with the sponge
+    const float2 lxy = fma2(lyy, splat(a.sy), mul2(lxx, splat(a.sx)));
+    const float2 lzs = mul2(lzz, splat(a.sz));
+    const float2 ndd = mul2(dd, splat(-1.f));
+    // 2 cur - dd prev, rounded once
+    store2(bp.lpx, mul2(dd, fma2(c11, lxy, fma2(c13, lzs, fma2(ndd, lpx, mul2(two, lc))))));
+    store2(bp.lpz, mul2(dd, fma2(c13, lxy, fma2(c33, lzs, fma2(ndd, lpz, mul2(two, lz0))))));
     if (((z + 1) & 3) == 0 && z + 1 < a.d.nz) {
 #pragma unroll
-      for (int e = 0; e < 2; ++e) {
-#pragma unroll
-        for (int kk = 0; kk < 4; ++kk) lq[e][kk + 1] *= dxy[e] * dzr[kk];
-      }
+      for (int kk = 0; kk < 4; ++kk)
+        lq[kk + 1] = mul2(lq[kk + 1], make_float2(dxy[0] * dzr[kk], dxy[1] * dzr[kk]));
     }
   }
   return true;

@@ -10,6 +10,7 @@
 #include <cudaTypedefs.h>
 
 #include "vti_internal.h"
+#include "vti_pair.cuh"
 
 namespace vti {
 
@@ -42,6 +43,18 @@ __device__ __forceinline__ float lap9(float c, float m1, float p1, float m2, flo
   s = fmaf(kC2, m2 + p2, s);
   s = fmaf(kC3, m3 + p3, s);
   s = fmaf(kC4, m4 + p4, s);
+  return s;
+}
+
+// lap9 of two adjacent points as packed FP32 pairs: each lane is rounded as
+// the scalar lap9 (the same operation sequence).
+__device__ __forceinline__ float2 lap9_2(float2 c, float2 m1, float2 p1, float2 m2, float2 p2,
+                                         float2 m3, float2 p3, float2 m4, float2 p4) {
+  float2 s = mul2(splat(kC0), c);
+  s = fma2(splat(kC1), add2(m1, p1), s);
+  s = fma2(splat(kC2), add2(m2, p2), s);
+  s = fma2(splat(kC3), add2(m3, p3), s);
+  s = fma2(splat(kC4), add2(m4, p4), s);
   return s;
 }
 
