@@ -195,6 +195,33 @@ def test_batch_per_shot_schedule_gives_the_same_gradient(ctx, survey):
         assert rel_l2(g3[1 + c * n:1 + (c + 1) * n], ref) < 1e-6, c
 
 
+def test_batch_f16_traces_equal_the_unpacked_traces(ctx, survey):
+    """Observed traces of all shots as one VTI_TRACES_F16 block: each shot's
+    slice is expanded on the device to exactly the FP32 traces the block
+    stands for, under both schedules."""
+    k = survey
+    dobs = _observed(ctx, k)
+    g = k["g"]
+    nnt = V.nnt3d(g)
+    nr = k["recloc"].size // 4
+    block = V.pack_traces_f16(dobs, nnt)
+    dq = V.unpack_traces_f16(block, nr, nnt)
+    b = _batch(ctx, k)
+    try:
+        out = {}
+        for sched in (V.BATCH_SIDE_BY_SIDE, V.BATCH_PER_SHOT):
+            b.set_schedule(sched)
+            b.set_trace_format(V.TRACES_F32)
+            out[sched, 32] = b.gradient(dq)
+            b.set_trace_format(V.TRACES_F16)
+            out[sched, 16] = b.gradient(block)
+    finally:
+        b.close()
+    for sched in (V.BATCH_SIDE_BY_SIDE, V.BATCH_PER_SHOT):
+        np.testing.assert_array_equal(out[sched, 16][0], out[sched, 32][0])
+        assert out[sched, 16][1] == out[sched, 32][1]
+
+
 def test_batch_shot_matches_fp64_oracle(ctx, survey):
     """One shot of the batch against the FP64 oracle on its window."""
     k = survey
