@@ -3,8 +3,12 @@
 // These are O(n) host operations around the device time loops; their
 // arithmetic (including the float/double mix) is kept as the reference
 // writes it so that drop-in callers see identical numbers.
+#include <immintrin.h>
+
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "vti_b200.h"
 
@@ -212,11 +216,6 @@ double vti2d_cfl_number(const vti2d_geom* g, const float* c11, const float* c13,
 // (trace-major). The scale of time sample t is the largest |value| of any
 // trace at t, so every sample is packed at the half's full relative
 // precision (F16C conversions, round to nearest even).
-#include <immintrin.h>
-
-#include <algorithm>
-#include <vector>
-
 extern "C" {
 
 size_t vti_traces_f16_bytes(int nr, int nnt) {
