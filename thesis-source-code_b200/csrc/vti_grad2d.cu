@@ -53,7 +53,23 @@ struct Fwd2 {
   // when set, the Born stencil reads these D values instead of D(dp1): the
   // reference never clears its Born D buffer between shots (hessian_f.cu)
   const float *bdp, *bdq;
+  // non-null: store D of the current level (k_dop2d's checkpoint of level
+  // it-1, the same expressions as tp / tq below)
+  float *ckp, *ckq;
+  // receiver of each cell (-1: none); with rec_row >= 0 the new level
+  // (Born field for the Gauss-Newton product) is recorded into that row
+  const int* rmap;
+  float* rec;
+  int rec_row, nri;
 };
+
+// injectData value of one receiver (kernels.cu:208-217): dt2 times half
+// the residual interpolated between rows b0 and b1.
+__device__ __forceinline__ float inject_value(const float* b0, const float* b1, int ir, float f,
+                                              float dt2) {
+  const float s = 0.5f * __fadd_rn(__fmul_rn(1.f - f, b0[ir]), __fmul_rn(f, b1[ir]));
+  return __fmul_rn(dt2, s);
+}
 
 __global__ void __launch_bounds__(BX* BZ) k_fwd2d(Fwd2 a) {
   // launched as programmatic dependents (launch_pdl): wait for the previous
@@ -96,6 +112,10 @@ __global__ void __launch_bounds__(BX* BZ) k_fwd2d(Fwd2 a) {
   const int i = ix + iz * nnx;
   const float tp = lap9(&sp[tz][tx + 4], 1) * a.idx2;
   const float tq = lap9(&sq[tz + 4][tx], BX) * a.idz2;
+  if (a.ckp) {
+    a.ckp[i] = tp;
+    a.ckq[i] = tq;
+  }
   const float t = a.taper[i];
   const float c11 = a.c11[i], c13 = a.c13[i], c33 = a.c33[i];
   float pn = fmaf(a.dt2, fmaf(c11, tp, c13 * tq), 2.f * sp[tz][tx + 4] - t * a.p0[i]);
@@ -104,8 +124,12 @@ __global__ void __launch_bounds__(BX* BZ) k_fwd2d(Fwd2 a) {
     pn += a.amp;
     qn += a.amp;
   }
-  a.p0[i] = t * pn;
-  a.q0[i] = t * qn;
+  // the stored products, rounded before they are recorded (no contraction)
+  const float pv = __fmul_rn(t, pn), qv = __fmul_rn(t, qn);
+  a.p0[i] = pv;
+  a.q0[i] = qv;
+  const int ir = (a.rec_row >= 0 && !born) ? a.rmap[i] : -1;
+  if (ir >= 0) a.rec[(long long)a.rec_row * a.nri + ir] = 0.5f * (pv + qv);
   if (born) {
     const float dtp = a.bdp ? a.bdp[i] : lap9(&sdp[tz][tx + 4], 1) * a.idx2;
     const float dtq = a.bdq ? a.bdq[i] : lap9(&sdq[tz + 4][tx], BX) * a.idz2;
@@ -113,8 +137,11 @@ __global__ void __launch_bounds__(BX* BZ) k_fwd2d(Fwd2 a) {
     float dqn = fmaf(a.dt2, fmaf(c13, dtp, c33 * dtq), 2.f * sdq[tz + 4][tx] - t * a.dq0[i]);
     dpn = fmaf(a.dt2, fmaf(a.dc11[i], tp, a.dc13[i] * tq), dpn);
     dqn = fmaf(a.dt2, fmaf(a.dc13[i], tp, a.dc33[i] * tq), dqn);
-    a.dp0[i] = t * dpn;
-    a.dq0[i] = t * dqn;
+    const float dpv = __fmul_rn(t, dpn), dqv = __fmul_rn(t, dqn);
+    a.dp0[i] = dpv;
+    a.dq0[i] = dqv;
+    const int irb = a.rec_row >= 0 ? a.rmap[i] : -1;
+    if (irb >= 0) a.rec[(long long)a.rec_row * a.nri + irb] = 0.5f * (dpv + dqv);
   }
 }
 
@@ -161,6 +188,12 @@ struct Adj2 {
   float f;
   int image;
   float *g11, *g13, *g33;
+  // receiver of each cell (-1: none); with inject, the residual rows b0/b1
+  // interpolated at fi are injected into the new level (k_inject2d, scaled)
+  const int* rmap;
+  const float *b0, *b1;
+  float fi;
+  int inject;
 };
 
 __global__ void __launch_bounds__(BX* BZ) k_adj2d(Adj2 a) {
@@ -218,8 +251,17 @@ __global__ void __launch_bounds__(BX* BZ) k_adj2d(Adj2 a) {
     pn = fmaf(a.dt2, fmaf(a.c11[i], tp, a.c13[i] * tq), 2.f * p - t * a.p1[i]);
     qn = fmaf(a.dt2, fmaf(a.c13[i], tp, a.c33[i] * tq), 2.f * q - t * a.q1[i]);
   }
-  a.p1[i] = t * pn;
-  a.q1[i] = t * qn;
+  // the stored products, rounded before the injection adds to them (the
+  // arithmetic of a store followed by k_inject2d)
+  float pv = __fmul_rn(t, pn), qv = __fmul_rn(t, qn);
+  const int ir = a.inject ? a.rmap[i] : -1;
+  if (ir >= 0) {
+    const float v = __fmul_rn(inject_value(a.b0, a.b1, ir, a.fi, a.dt2), t);
+    pv += v;
+    qv += v;
+  }
+  a.p1[i] = pv;
+  a.q1[i] = qv;
 }
 
 // injectData (kernels.cu:208-217) into a tapered level: taper factor applied.
@@ -232,9 +274,8 @@ __global__ void k_inject2d(float* p, float* q, const float* b0, const float* b1,
   int ir = blockIdx.x * blockDim.x + threadIdx.x;
   if (ir < nr) {
     const int i = ridx[ir];
-    float s = 0.5f * ((1.f - f) * b0[ir] + f * b1[ir]);
-    float v = dt2 * s;
-    if (scale) v *= taper[i];
+    float v = inject_value(b0, b1, ir, f, dt2);
+    if (scale) v = __fmul_rn(v, taper[i]);
     p[i] += v;
     q[i] += v;
   }
@@ -418,10 +459,28 @@ int run_grad2d(vti_ctx* ctx, const vti2d_geom* g, float* gc11, float* gc13, floa
         return fail(ctx, VTI_ERR_ARG, "2D receiver outside the grid");
       ridx[ir] = x + z * nnx;
     }
-    Buf rb, recb, obsb, live, b01;
+    Buf rb, recb, obsb, live, b01, rmapb;
     VTI_CUDA(ctx, cudaMalloc((void**)&rb.p, ridx.size() * sizeof(int)));
     VTI_CUDA(ctx, cudaMemcpyAsync(rb.p, ridx.data(), ridx.size() * sizeof(int),
                                   cudaMemcpyHostToDevice, s));
+    // receiver of each cell: the step kernels record and inject themselves
+    // (one launch per level instead of two); a cell holding two receivers
+    // keeps the separate receiver kernels
+    std::vector<int> rmh;
+    bool fuse = nri > 0;
+    if (fuse) {
+      rmh.assign(nnxz, -1);
+      for (int ir = 0; ir < nri && fuse; ++ir) {
+        if (rmh[ridx[ir]] >= 0) fuse = false;
+        rmh[ridx[ir]] = ir;
+      }
+    }
+    if (fuse) {
+      VTI_CUDA(ctx, cudaMalloc((void**)&rmapb.p, nnxz * sizeof(int)));
+      VTI_CUDA(ctx, cudaMemcpyAsync(rmapb.p, rmh.data(), nnxz * sizeof(int),
+                                    cudaMemcpyHostToDevice, s));
+    }
+    const int* d_rmap = fuse ? (const int*)rmapb.p : nullptr;
     const size_t nrec = (size_t)nnt_data * std::max(nri, 1);
     VTI_CUDA(ctx, cudaMalloc((void**)&recb.p, nrec * sizeof(float)));
     VTI_CUDA(ctx, cudaMemsetAsync(recb.p, 0, nrec * sizeof(float), s));
@@ -441,7 +500,6 @@ int run_grad2d(vti_ctx* ctx, const vti2d_geom* g, float* gc11, float* gc13, floa
       ctx->launches++;
       return launch_pdl(k_dop2d, grid, block, s, G, p, q, ckp(label), ckq(label), idx2, idz2);
     };
-    VTI_CUDA(ctx, checkpoint(1, P1, Q1));
     for (int it = 2; it < g->nt; ++it) {
       const float t = it * dt + g->ot;
       Fwd2 a{G,   P1,  Q1,  P0,  Q0,   DP1,  DQ1, DP0, DQ0, d11, d13, d33, e11,
@@ -451,10 +509,20 @@ int run_grad2d(vti_ctx* ctx, const vti2d_geom* g, float* gc11, float* gc13, floa
         a.bdp = stale_p;
         a.bdq = stale_q;
       }
+      // the checkpoint of the current level it-1 (k_dop2d's D of P1, Q1)
+      {
+        const long label = (long)is * (g->nt + 1) + (it - 1);
+        a.ckp = slot.count(label) ? ckp(label) : nullptr;
+        a.ckq = slot.count(label) ? ckq(label) : nullptr;
+      }
+      const bool record = t >= 0.f && (it - ntNeg) % ratio == 0 && nri > 0;
+      a.rmap = d_rmap;
+      a.rec = recb.p;
+      a.rec_row = (fuse && record) ? (it - ntNeg) / ratio : -1;
+      a.nri = nri;
       VTI_CUDA(ctx, launch_pdl(k_fwd2d, grid, block, s, a));
       ctx->launches++;
-      VTI_CUDA(ctx, checkpoint(it, P0, Q0));
-      if (t >= 0.f && (it - ntNeg) % ratio == 0 && nri > 0) {
+      if (record && !fuse) {
         VTI_CUDA(ctx, launch_pdl(k_record_rows, dim3((nri + 127) / 128), dim3(128), s, recb.p,
                                  (it - ntNeg) / ratio, (const float*)(born ? DP0 : P0),
                                  (const float*)(born ? DQ0 : Q0), d_ridx, nri));
@@ -465,6 +533,8 @@ int run_grad2d(vti_ctx* ctx, const vti2d_geom* g, float* gc11, float* gc13, floa
       std::swap(DP0, DP1);
       std::swap(DQ0, DQ1);
     }
+    // the last level has no next step to carry its checkpoint
+    VTI_CUDA(ctx, checkpoint(g->nt - 1, P1, Q1));
     if (born) {  // D of the last Born level, read by the next shot's first step
       VTI_CUDA(ctx, launch_pdl(k_dop2d, grid, block, s, G, (const float*)DP1,
                                (const float*)DQ1, stale_p, stale_q, idx2, idz2));
@@ -499,19 +569,31 @@ int run_grad2d(vti_ctx* ctx, const vti2d_geom* g, float* gc11, float* gc13, floa
     int step = 0;  // sched[step] images the current adjoint
     for (int it = g->nt - 3; it >= 0; --it, ++step) {
       const Pair& pr = sched[is][step];
-      Adj2 a{G,      P0,  Q0,  P1,  Q1,  d11, d13, d33, tap,  idx2, idz2, dt2, born ? 0 : 1,
-             ckp(pr.a), ckq(pr.a), ckp(pr.b), ckq(pr.b), pr.f, 1, g11, g13, g33};
-      VTI_CUDA(ctx, launch_pdl(k_adj2d, grid, block, s, a));
-      ctx->launches++;
-      if (it >= ntNeg && nri > 0) {
+      // the residual rows injected into the new level (injectData), chosen
+      // before the step
+      const bool inject = it >= ntNeg && nri > 0;
+      float fi = 0.f;
+      if (inject) {
         float f = (it - ntNeg + 1.) / ratio;
         int i1 = (int)f;
         if ((it - ntNeg + 2) % ratio == 0) {  // row i1 enters, the older row leaves
           b1 = recb.p + (size_t)i1 * nri;
           std::swap(b0, b1);
         }
+        fi = f - i1;
+      }
+      Adj2 a{G,      P0,  Q0,  P1,  Q1,  d11, d13, d33, tap,  idx2, idz2, dt2, born ? 0 : 1,
+             ckp(pr.a), ckq(pr.a), ckp(pr.b), ckq(pr.b), pr.f, 1, g11, g13, g33};
+      a.rmap = d_rmap;
+      a.b0 = b0;
+      a.b1 = b1;
+      a.fi = fi;
+      a.inject = (inject && fuse) ? 1 : 0;
+      VTI_CUDA(ctx, launch_pdl(k_adj2d, grid, block, s, a));
+      ctx->launches++;
+      if (inject && !fuse) {
         VTI_CUDA(ctx, launch_pdl(k_inject2d, dim3((nri + 127) / 128), dim3(128), s, P1, Q1, b0,
-                                 b1, f - i1, d_ridx, (const float*)tap, nri, dt2, 1));
+                                 b1, fi, d_ridx, (const float*)tap, nri, dt2, 1));
         ctx->launches++;
       }
       std::swap(P0, P1);
